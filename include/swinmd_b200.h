@@ -1,0 +1,195 @@
+/* swinmd_b200.h — C ABI of the B200 force + integration path for SwinMD.
+ *
+ * One opaque context holds one system on one GPU.  Every entry point returns
+ * an int status (SMD_OK = 0) and never exits the process; the reference's
+ * ERRORMSG/exit() paths (src/Errors.h:53-62) become non-zero codes, with the
+ * message available from smd_last_error().  Arrays cross the boundary as
+ * plain host pointers in the reference's layout: per-atom Vector3 values are
+ * three consecutive doubles in atom order (Atom::position / velocity /
+ * force, src/Atom.h:422-429); units are the reference's (nm, ps, amu,
+ * kJ/mol, e; src/NEMD_defs.h:97-108).
+ *
+ * Each entry point names the reference interface it stands in for.
+ */
+#ifndef SWINMD_B200_H
+#define SWINMD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct smd_ctx smd_ctx;
+
+/* status codes */
+enum {
+    SMD_OK = 0,
+    SMD_ERR_ARG = 1,          /* bad argument or call order */
+    SMD_ERR_CUDA = 2,         /* a CUDA call failed */
+    SMD_ERR_LIST_OVERFLOW = 3,/* a site has more neighbours than the list holds */
+    SMD_ERR_NH_ITER = 4,      /* "NH iteration Error" (LFIntegrator.cpp:606-608) */
+    SMD_ERR_SHAKE = 5,        /* SHAKE did not converge (LFIntegrator.cpp:1798-1812) */
+    SMD_ERR_NAN = 6,          /* non-finite force or position */
+    SMD_ERR_CG = 7,           /* dipole solve did not converge */
+    SMD_ERR_NO_DEVICE = 8     /* no CUDA device / extension unusable */
+};
+
+/* arithmetic of the pair, reciprocal and dipole-field kernels */
+enum {
+    SMD_PREC_FP64 = 0,   /* FP64 math, 64-bit fixed-point accumulation */
+    SMD_PREC_MIXED = 1   /* FP32 math on exact fixed-point displacements,
+                            64-bit fixed-point accumulation */
+};
+
+/* force terms for smd_compute_forces (bit mask) */
+enum {
+    SMD_TERM_VDW = 1,        /* LJForce / MieForce / BMH pair term */
+    SMD_TERM_EWALD_REAL = 2, /* EwaldForce::compute() real space + intra + self */
+    SMD_TERM_EWALD_LONG = 4, /* EwaldForce::compute_long() */
+    SMD_TERM_ALL = 0xffff
+};
+
+/* energy components returned by smd_compute_forces, indices into energy[] */
+enum {
+    SMD_E_VDW = 0,       /* myEnergy.ljEnergy (incl. long-range correction) */
+    SMD_E_REAL = 1,      /* myEnergy.realEnergy */
+    SMD_E_LONG = 2,      /* myEnergy.longEnergy */
+    SMD_E_CORRECT = 3,   /* myEnergy.correctEnergy (self + net charge) */
+    SMD_E_MOLCORRECT = 4,/* myEnergy.molCorrectEnergy */
+    SMD_E_SURF = 5,      /* myEnergy.surfCorrectEnergy */
+    SMD_E_COUNT = 8
+};
+
+/* vdW kinds for smd_set_vdw */
+enum { SMD_VDW_NONE = 0, SMD_VDW_LJ = 1, SMD_VDW_MIE = 2, SMD_VDW_BMH = 3 };
+
+/* thermostat kinds */
+enum { SMD_THERMO_NONE = 0, SMD_THERMO_NOSE_HOOVER = 1 };
+
+/* Leap-frog integrator settings: the config.txt fields that
+ * LFIntegrator / Integrator read (src/Integrator.cpp:14-99). */
+typedef struct {
+    double timestep;       /* ps */
+    double temperature;    /* K */
+    double coupl_const;    /* Nose-Hoover tau (ps) */
+    int thermostat;        /* SMD_THERMO_* */
+    int atom_thermo;       /* 1: atomic kinetic energy drives zeta; 0: molecular */
+    int constraint;        /* 0 none, 2 SHAKE (rigid 3-site water) */
+    int long_steps;        /* reciprocal term every long_steps steps */
+    double shake_tol;      /* SHAKE tolerance */
+    int shake_max_iter;    /* SHAKE maxCount */
+    int atom_ndf;          /* degrees of freedom (Integrator.cpp:22-27) */
+    int mol_ndf;
+    double strain_rate;    /* SLLOD planar Couette rate (1/ps); 0: equilibrium */
+} smd_integrator_params;
+
+/* Per-step observables the reference keeps in Ensemble/Integrator members. */
+typedef struct {
+    int64_t step;            /* currentSteps */
+    int64_t list_updates;    /* numUpdates */
+    double energy[SMD_E_COUNT];
+    double e_potential;      /* sum of energy[] (myEnergy.totEnergy without bonded terms) */
+    double ke_atom;          /* myEnergy.atomKinEnergy = 0.5 sum m v^2 */
+    double ke_mol;           /* myEnergy.molKinEnergy */
+    double t_atom, t_mol;    /* atomTemp, molTemp (K) */
+    double zeta;             /* fnh */
+    double virial[9];        /* myEnsemble->virial (+ longVirial) */
+    double atom_pressure[9]; /* Ensemble::atomPressure (kJ/mol/nm^3) */
+    double mol_pressure[9];  /* Ensemble::molPressure */
+    double volume;
+    int64_t pairs_in_cutoff; /* unordered pairs inside the short-range cutoff */
+    uint32_t status;
+    uint32_t pad;
+} smd_observables;
+
+/* ---- lifetime -------------------------------------------------------- */
+/* Creates a context on CUDA device `device` (the Simulation/Ensemble pair of
+ * Simulation::setup_simulation, src/Simulation.cpp:171-263). */
+int smd_create(int device, smd_ctx **out);
+void smd_destroy(smd_ctx *ctx);
+const char *smd_last_error(const smd_ctx *ctx);
+
+/* ---- system (Ensemble::set_mol_system, src/Ensemble.cpp:140-227) ---- */
+/* atom_type[n], mol_id[n], mass[n] (amu), scaled_charge[n] (charge times
+ * SQRTCOULOMBCONSTANT, Atom::scaledCharge, src/Ensemble.cpp:183). */
+int smd_set_topology(smd_ctx *ctx, int n_atoms, int n_types, const int32_t *atom_type,
+                     const int32_t *mol_id, const double *mass, const double *scaled_charge);
+/* Exclusion table (Ensemble::build_exclusion_table, src/Ensemble.cpp:323-367)
+ * as CSR: partners of atom i are excl[offsets[i] .. offsets[i+1]). */
+int smd_set_exclusions(smd_ctx *ctx, const int32_t *offsets, const int32_t *partners);
+/* Box edges (Ensemble::boxLx..., src/Ensemble.cpp:370-420). */
+int smd_set_box(smd_ctx *ctx, double lx, double ly, double lz);
+/* Pair list (Ensemble::set_pairlist, src/Ensemble.cpp:454-473): list radius
+ * cutoff + cut_buffer, cell list when use_cells and >= 3 cells per edge
+ * (CellManager::set_cellManager, src/utils/CellManager.cpp:43-84). */
+int smd_set_pairlist(smd_ctx *ctx, double cutoff, double cut_buffer, int use_cells);
+/* Short-range pair term.  params: ntypes*ntypes rows of 4 doubles, meaning
+ * per kind (LJ: sigma^2, 4 eps as Parameters::set_lj_param stores them,
+ * src/Parameters.cpp:1360-1372; MIE: sigma, Cn*eps, n, m as MieForce derives
+ * them, src/forces/MieForce.cpp:26-35,122-124; BMH: A, 1/rho, C, D).
+ * LJ shifts the energy at the cutoff when switch_on (LJForce.cpp:152-168);
+ * MIE and BMH apply the 5th-order switch from sqrt(switch_dist2) to the
+ * cutoff (MieForce.cpp:145-154).  e_lrc/v_lrc: long-range correction energy
+ * and virial added once per evaluation (LJForce.cpp:232-235). */
+int smd_set_vdw(smd_ctx *ctx, int kind, const double *params, int switch_on,
+                double switch_dist2, double e_lrc, double v_lrc);
+/* Ewald summation for point charges (EwaldForce ctor + set_up,
+ * src/forces/EwaldForce.cpp:22-257): alpha (1/nm), kcut (1/nm), real-space
+ * cutoff.  long_steps: reciprocal term every long_steps steps. */
+int smd_set_ewald(smd_ctx *ctx, double alpha, double kcut, double real_cut);
+int smd_set_precision(smd_ctx *ctx, int mode);
+/* Pair-kernel threads per site (1..32, power of two); 0 lets the library pick. */
+int smd_set_tuning(smd_ctx *ctx, int threads_per_site);
+
+/* ---- state ------------------------------------------------------------ */
+int smd_upload_positions(smd_ctx *ctx, const double *pos);
+/* vel: Atom::velocity; vtminus may be NULL (then set by smd_integrator_start) */
+int smd_upload_velocities(smd_ctx *ctx, const double *vel, const double *vtminus);
+int smd_download_state(smd_ctx *ctx, double *pos, double *vel, double *vtminus);
+
+/* ---- forces (Force::compute / compute_long, src/Force.h:59) ----------
+ * Rebuilds the pair list from the current positions, evaluates the selected
+ * terms and returns: force[3n] (the terms' contribution to Atom::force),
+ * energy[SMD_E_COUNT] (NULL allowed), virial[9] (contribution to
+ * Ensemble::virial + longVirial, i.e. +sum r_ij f_ij; NULL allowed). */
+int smd_compute_forces(smd_ctx *ctx, uint32_t terms, double *force, double *energy,
+                       double *virial);
+/* Unordered pairs of the current Verlet list as (i < j) int32 pairs, the set
+ * CellManager::update_pair_list builds (src/utils/CellManager.cpp:216-314).
+ * cap: room in pairs[] for `cap` pairs; *count receives the number found. */
+int smd_get_pairs(smd_ctx *ctx, int32_t *pairs, int64_t cap, int64_t *count);
+/* k-vector count of the Ewald reciprocal set (EwaldForce::set_up). */
+int smd_ewald_nk(smd_ctx *ctx, int *nk);
+
+/* ---- integration (LFIntegrator, src/integrators/LFIntegrator.cpp) ------ */
+int smd_set_integrator(smd_ctx *ctx, const smd_integrator_params *p);
+/* LFIntegrator::start (LFIntegrator.cpp:991-1174): F(0) and
+ * vtMinus = v - dt/2 F/m. */
+int smd_integrator_start(smd_ctx *ctx);
+/* LFIntegrator::run(nsteps) (LFIntegrator.cpp:252-942) without file output. */
+int smd_run(smd_ctx *ctx, int nsteps);
+int smd_get_observables(smd_ctx *ctx, smd_observables *out);
+/* Per-step samples recorded during smd_run (e_potential, ke_atom, t_atom, zeta,
+ * atom-pressure trace/3) for the last min(nsteps, cap) steps: out[5*cap]. */
+int smd_set_series_capacity(smd_ctx *ctx, int cap);
+int smd_get_series(smd_ctx *ctx, double *out, int cap, int *count);
+
+/* ---- measurement ------------------------------------------------------- */
+/* Average device time (ms, CUDA events on the context's stream) of each
+ * stage of one step, each launched `reps` times on its own:
+ * out[0] pair kernel, out[1] reciprocal kernels, out[2] integrate kernel,
+ * out[3] a forced pair-list rebuild.  Leaves forces and state unchanged
+ * except for the rebuilt list. */
+int smd_profile_stages(smd_ctx *ctx, int reps, double *out);
+/* smd_run with the device time of the nsteps graph launches (CUDA events on
+ * the context's stream, synchronized on both sides) returned in *device_ms. */
+int smd_run_timed(smd_ctx *ctx, int nsteps, double *device_ms);
+/* Number of kernel launches in one step of smd_run (kernel nodes of the
+ * step's CUDA graph). */
+int smd_step_kernel_count(smd_ctx *ctx, int *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,123 @@
+"""ctypes binding of the CPU restatement in oracle/smd_oracle.c.
+
+Test infrastructure only: tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline call it as the checker; the product never imports it.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+_lib = None
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int32)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        src = os.path.join(HERE, "smd_oracle.c")
+        if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
+            subprocess.run(["make", "-C", HERE, "-s", "lib"], check=True)
+        _lib = ctypes.CDLL(LIB)
+        _lib.or_pairlist.restype = ctypes.c_int64
+        _lib.or_pairlist.argtypes = [ctypes.c_int, _D, _D, ctypes.c_double, _I, _I, _I, ctypes.c_int64]
+        _lib.or_lj.restype = ctypes.c_double
+        _lib.or_lj.argtypes = [ctypes.c_int, _D, _I, _I, _D, ctypes.c_int, _D, _D, ctypes.c_double,
+                               ctypes.c_int, ctypes.c_double, ctypes.c_double, _I, ctypes.c_int64, _D, _D]
+        _lib.or_lj_md.restype = ctypes.c_int
+        _lib.or_lj_md.argtypes = [ctypes.c_int, _D, _D, _D, _D, _I, _I, _D, ctypes.c_int, _D, _D,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_int, _D, _D, _D]
+        _lib.or_ewald_real.restype = ctypes.c_double
+        _lib.or_ewald_real.argtypes = [ctypes.c_int, _D, _D, _D, ctypes.c_double, ctypes.c_double,
+                                       _I, ctypes.c_int64, _D, _D]
+        _lib.or_ewald_recip.restype = ctypes.c_double
+        _lib.or_ewald_recip.argtypes = [ctypes.c_int, _D, _D, _D, ctypes.c_double, ctypes.c_double,
+                                        _D, _D, ctypes.POINTER(ctypes.c_int)]
+    return _lib
+
+
+def d(a):
+    return np.ascontiguousarray(a, np.float64).ctypes.data_as(_D)
+
+
+def i32(a):
+    return np.ascontiguousarray(a, np.int32).ctypes.data_as(_I)
+
+
+def _excl_csr(system):
+    ex = system.exclusion_table()
+    off = np.zeros(system.n_atoms + 1, np.int32)
+    off[1:] = np.cumsum([len(e) for e in ex])
+    flat = np.array([j for e in ex for j in e] or [0], np.int32)
+    return off, flat
+
+
+def pairlist(system, pos, box):
+    c = system.config
+    rl = c.cutoff + c.cut_buffer
+    L = np.array([box] * 3, np.float64)
+    off, flat = _excl_csr(system)
+    pos = np.ascontiguousarray(pos, np.float64)
+    n = system.n_atoms
+    cap = n * 600
+    out = np.zeros(2 * cap, np.int32)
+    k = lib().or_pairlist(n, d(pos), d(L), rl * rl, i32(off), i32(flat), i32(out), cap)
+    assert k <= cap
+    return out[:2 * k].reshape(-1, 2)
+
+
+def lj(system, pos, box, pairs, e_lrc=0.0, v_lrc=0.0):
+    s2, e4 = system.lj_table()
+    L = np.array([box] * 3, np.float64)
+    f = np.zeros(3 * system.n_atoms)
+    w = np.zeros(9)
+    pairs = np.ascontiguousarray(pairs, np.int32)
+    e = lib().or_lj(system.n_atoms, d(pos), i32(system.atom_type), i32(system.mol_id), d(L),
+                    len(system.atom_types), d(s2), d(e4), system.config.cutoff,
+                    int(system.config.switch_on), e_lrc, v_lrc, i32(pairs), len(pairs),
+                    f.ctypes.data_as(_D), w.ctypes.data_as(_D))
+    return f.reshape(-1, 3), e, w
+
+
+def lj_md(system, pos, vel, box, nsteps, e_lrc=0.0, v_lrc=0.0):
+    c = system.config
+    s2, e4 = system.lj_table()
+    L = np.array([box] * 3, np.float64)
+    pos = np.array(pos, np.float64).reshape(-1).copy()
+    vel = np.array(vel, np.float64).reshape(-1).copy()
+    vtm = np.zeros_like(vel)
+    ep, tt, zz = np.zeros(nsteps), np.zeros(nsteps), np.zeros(nsteps)
+    r = lib().or_lj_md(system.n_atoms, pos.ctypes.data_as(_D), vel.ctypes.data_as(_D),
+                       vtm.ctypes.data_as(_D), d(system.masses()), i32(system.atom_type),
+                       i32(system.mol_id), d(L), len(system.atom_types), d(s2), d(e4), c.cutoff,
+                       c.cut_buffer, int(c.switch_on), e_lrc, v_lrc, c.timestep, c.temperature,
+                       c.coupl_const, nsteps, ep.ctypes.data_as(_D), tt.ctypes.data_as(_D),
+                       zz.ctypes.data_as(_D))
+    assert r == 0, r
+    return {"pos": pos.reshape(-1, 3), "vel": vel.reshape(-1, 3), "vtminus": vtm.reshape(-1, 3),
+            "epot": ep, "temp": tt, "zeta": zz}
+
+
+def ewald(system, pos, box, pairs):
+    c = system.config
+    L = np.array([box] * 3, np.float64)
+    q = system.scaled_charges()
+    n = system.n_atoms
+    f = np.zeros(3 * n)
+    w = np.zeros(9)
+    pairs = np.ascontiguousarray(pairs, np.int32)
+    er = lib().or_ewald_real(n, d(pos), d(q), d(L), c.alpha, c.cutoff, i32(pairs), len(pairs),
+                             f.ctypes.data_as(_D), w.ctypes.data_as(_D))
+    fl = np.zeros(3 * n)
+    wl = np.zeros(9)
+    nk = ctypes.c_int()
+    el = lib().or_ewald_recip(n, d(pos), d(q), d(L), c.alpha, c.k_cutoff, fl.ctypes.data_as(_D),
+                              wl.ctypes.data_as(_D), ctypes.byref(nk))
+    return {"real_force": f.reshape(-1, 3), "real_energy": er, "real_virial": w,
+            "long_force": fl.reshape(-1, 3), "long_energy": el, "long_virial": wl, "nk": nk.value}

@@ -1,0 +1,304 @@
+// ref_dump — drives the reference SwinMD objects (built by oracle/Makefile)
+// and writes their FP64 results as text records, one per line:
+//     <name> <count> v0 v1 ... v(count-1)
+// Test infrastructure only: the checker that pins this project's CPU
+// restatement and its CUDA path.  It never runs inside the product.
+//
+// Usage (run inside a case directory holding config.txt, sysData.in and the
+// coordinate file the config names):
+//     ref_dump forces <out>        one force evaluation of every term the
+//                                  config enables, each term on its own
+//     ref_dump run <nsteps> <out>  LFIntegrator::start() then nsteps x run(1)
+//     ref_dump mie <out>           MieForce::compute() on its own
+//     ref_dump buck <out>          BuckinghamForce::compute() on its own
+//
+// Setup follows Simulation::setup_simulation (src/Simulation.cpp:171-263)
+// without the output files.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <ctime>
+#include <cstdint>
+#include <iostream>
+#include <iomanip>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+#include <set>
+#include <map>
+#include <algorithm>
+#include <utility>
+#include <limits>
+#include "mpi.h"
+// Several members the checker reads (LFIntegrator::vtMinus, the force
+// objects' virial) are private; widen access for this translation unit only.
+#define class struct
+#define private public
+#define protected public
+#include "Ensemble.h"
+#include "Parameters.h"
+#include "SimConfiguration.h"
+#include "Integrator.h"
+#include "integrators/LFIntegrator.h"
+#include "forces/LJForce.h"
+#include "forces/MieForce.h"
+#include "forces/BuckinghamForce.h"
+#include "forces/BuffvdWForce.h"
+#include "forces/EwaldForce.h"
+#include "forces/Multipole.h"
+#include "forces/Induction.h"
+#undef class
+#undef private
+#undef protected
+
+int mpi_size_g = 1;
+int mpi_rank_g = 0;
+
+static FILE *g_out = nullptr;
+
+static void rec(const char *name, const std::vector<double> &v) {
+    fprintf(g_out, "%s %zu", name, v.size());
+    for (double x : v) fprintf(g_out, " %.17g", x);
+    fputc('\n', g_out);
+}
+static void rec1(const char *name, double x) { rec(name, std::vector<double>{x}); }
+
+struct Setup {
+    SimConfiguration *cfg;
+    Parameters *params;
+    Ensemble *ens;
+};
+
+static Setup build() {
+    Setup s;
+    s.cfg = new SimConfiguration((char *)"config.txt");
+    s.cfg->read_config_file();
+    s.params = new Parameters(s.cfg->get_sysData_file());
+    s.ens = new Ensemble();
+    s.ens->set_mol_system(s.params);
+    s.ens->set_configuration(s.cfg);
+    s.ens->compute_bound_box();
+    s.ens->set_pairlist();
+    s.ens->set_sysdata_file(new std::ofstream("sysData.out", std::ios::out));
+    s.ens->set_result_file(new std::ofstream("result.out", std::ios::out));
+    return s;
+}
+
+static void dump_state(Ensemble *e, const char *tag) {
+    int n = e->nAtoms;
+    std::vector<double> p(3 * n), v(3 * n);
+    for (int i = 0; i < n; i++) {
+        p[3 * i] = e->atoms[i].position.x;
+        p[3 * i + 1] = e->atoms[i].position.y;
+        p[3 * i + 2] = e->atoms[i].position.z;
+        v[3 * i] = e->atoms[i].velocity.x;
+        v[3 * i + 1] = e->atoms[i].velocity.y;
+        v[3 * i + 2] = e->atoms[i].velocity.z;
+    }
+    std::string a = std::string(tag) + "_pos", b = std::string(tag) + "_vel";
+    rec(a.c_str(), p);
+    rec(b.c_str(), v);
+}
+
+static void dump_pairs(Ensemble *e) {
+    std::vector<double> pr;
+    for (int i = 0; i < e->nAtoms; i++) {
+        Atom *a = &e->atoms[i];
+        for (int k = 0; k < a->get_list_size(); k++) {
+            int j = a->myPairList[k]->atomID;
+            pr.push_back(std::min(i, j));
+            pr.push_back(std::max(i, j));
+        }
+    }
+    rec("pairs", pr);
+}
+
+static void zero(Ensemble *e) {
+    for (int i = 0; i < e->nAtoms; i++) e->atoms[i].force = 0.0;
+    for (int k = 0; k < 9; k++) {
+        e->virial[k] = 0.0;
+        e->longVirial[k] = 0.0;
+    }
+    std::memset(&e->myEnergy, 0, sizeof(e->myEnergy));
+}
+
+static void dump_forces(Ensemble *e, const char *tag) {
+    int n = e->nAtoms;
+    std::vector<double> f(3 * n);
+    for (int i = 0; i < n; i++) {
+        f[3 * i] = e->atoms[i].force.x;
+        f[3 * i + 1] = e->atoms[i].force.y;
+        f[3 * i + 2] = e->atoms[i].force.z;
+    }
+    std::string a = std::string(tag) + "_force";
+    rec(a.c_str(), f);
+    std::string b = std::string(tag) + "_virial";
+    rec(b.c_str(), std::vector<double>(e->virial, e->virial + 9));
+    std::string c = std::string(tag) + "_longvirial";
+    rec(c.c_str(), std::vector<double>(e->longVirial, e->longVirial + 9));
+    const Energy &E = e->myEnergy;
+    std::string d = std::string(tag) + "_energy";
+    // order: lj real long correct molCorrect surfCorrect realPol longPol
+    //        correctPol molCorrectPol surfacePol
+    rec(d.c_str(), {E.ljEnergy, E.realEnergy, E.longEnergy, E.correctEnergy,
+                    E.molCorrectEnergy, E.surfCorrectEnergy, E.realPolEnergy,
+                    E.longPolEnergy, E.correctPolEnergy, E.molCorrectPolEnergy,
+                    E.surfacePolEnergy});
+}
+
+static void header(Setup &s) {
+    Ensemble *e = s.ens;
+    rec("box", {e->boxLx, e->boxLy, e->boxLz});
+    rec1("natoms", e->nAtoms);
+    rec1("pair_cutoff2", e->pairCutOff);
+    std::vector<double> m(e->nAtoms), q(e->nAtoms), t(e->nAtoms), mol(e->nAtoms);
+    for (int i = 0; i < e->nAtoms; i++) {
+        m[i] = e->atoms[i].mass;
+        q[i] = e->atoms[i].scaledCharge;
+        t[i] = e->atoms[i].atomType;
+        mol[i] = e->atoms[i].molID;
+    }
+    rec("mass", m);
+    rec("scaled_charge", q);
+    rec("type", t);
+    rec("molid", mol);
+    dump_state(e, "init");
+    dump_pairs(e);
+}
+
+static int mode_forces(const char *out) {
+    Setup s = build();
+    g_out = fopen(out, "w");
+    header(s);
+    Ensemble *e = s.ens;
+    SimConfiguration *c = s.cfg;
+    if (c->compute_buffamoeba()) {
+        zero(e);
+        BuffvdWForce f(e);
+        f.compute();
+        dump_forces(e, "buff");
+    } else {
+        zero(e);
+        LJForce f(e);
+        f.compute();
+        dump_forces(e, "lj");
+    }
+    if (c->compute_ewald_force()) {
+        zero(e);
+        EwaldForce f(e);
+        f.compute();
+        dump_forces(e, "ewald_short");
+        zero(e);
+        f.compute_long();
+        dump_forces(e, "ewald_long");
+        rec1("ewald_nk", (double)f.kVector.size());
+    }
+    if (c->compute_multipol()) {
+        zero(e);
+        Multipole mp(e);
+        mp.compute();
+        dump_forces(e, "mp_short");
+        zero(e);
+        mp.compute_long();
+        dump_forces(e, "mp_long");
+        if (c->compute_induction()) {
+            zero(e);
+            Induction ind(e);
+            ind.compute();
+            dump_forces(e, "ind_short");
+            zero(e);
+            ind.compute_long();
+            dump_forces(e, "ind_long");
+        }
+    }
+    fclose(g_out);
+    return 0;
+}
+
+static int mode_single(const char *which, const char *out) {
+    Setup s = build();
+    g_out = fopen(out, "w");
+    header(s);
+    Ensemble *e = s.ens;
+    zero(e);
+    if (!strcmp(which, "mie")) {
+        MieForce f(e);
+        f.compute();
+        dump_forces(e, "mie");
+    } else {
+        BuckinghamForce f(e);
+        f.compute();
+        dump_forces(e, "buck");
+    }
+    fclose(g_out);
+    return 0;
+}
+
+static int mode_run(int nsteps, const char *out) {
+    Setup s = build();
+    g_out = fopen(out, "w");
+    header(s);
+    Ensemble *e = s.ens;
+    LFIntegrator *lf = new LFIntegrator(e, s.cfg);  // runs start(): F(0), vtMinus
+    dump_forces(e, "start");
+    {
+        std::vector<double> vm(3 * e->nAtoms);
+        for (int i = 0; i < e->nAtoms; i++) {
+            vm[3 * i] = lf->vtMinus[i].x;
+            vm[3 * i + 1] = lf->vtMinus[i].y;
+            vm[3 * i + 2] = lf->vtMinus[i].z;
+        }
+        rec("start_vtminus", vm);
+    }
+    std::vector<double> epot, ekin, atemp, zeta, press, nupd;
+    std::vector<double> ptensor;
+    double run_seconds = 0.0;
+    for (int k = 0; k < nsteps; k++) {
+        timespec t0, t1;
+        clock_gettime(CLOCK_MONOTONIC, &t0);
+        lf->run(1);
+        clock_gettime(CLOCK_MONOTONIC, &t1);
+        run_seconds += (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec);
+        const Energy &E = e->myEnergy;
+        epot.push_back(E.totEnergy);
+        ekin.push_back(E.atomKinEnergy);
+        atemp.push_back(e->atomTemp);
+        zeta.push_back(lf->fnh);
+        nupd.push_back(lf->numUpdates);
+        for (int q = 0; q < 9; q++) ptensor.push_back(e->atomPressure[q]);
+    }
+    rec("step_epot", epot);
+    rec("step_ekin", ekin);
+    rec("step_atomtemp", atemp);
+    rec("step_zeta", zeta);
+    rec("step_nupdates", nupd);
+    rec("step_atompressure", ptensor);
+    rec1("run_seconds", run_seconds);
+    dump_state(e, "final");
+    dump_forces(e, "final");
+    {
+        std::vector<double> vm(3 * e->nAtoms);
+        for (int i = 0; i < e->nAtoms; i++) {
+            vm[3 * i] = lf->vtMinus[i].x;
+            vm[3 * i + 1] = lf->vtMinus[i].y;
+            vm[3 * i + 2] = lf->vtMinus[i].z;
+        }
+        rec("final_vtminus", vm);
+    }
+    fclose(g_out);
+    return 0;
+}
+
+int main(int argc, char **argv) {
+    if (argc < 3) {
+        fprintf(stderr, "usage: ref_dump forces|mie|buck <out> | run <nsteps> <out>\n");
+        return 2;
+    }
+    if (!strcmp(argv[1], "forces")) return mode_forces(argv[2]);
+    if (!strcmp(argv[1], "mie") || !strcmp(argv[1], "buck")) return mode_single(argv[1], argv[2]);
+    if (!strcmp(argv[1], "run") && argc >= 4) return mode_run(atoi(argv[2]), argv[3]);
+    fprintf(stderr, "unknown mode\n");
+    return 2;
+}

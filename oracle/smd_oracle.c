@@ -1,0 +1,254 @@
+/* smd_oracle.c — CPU restatement of the SwinMD force/integration path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product links or calls this
+ * file; tests/, __graft_entry__.smoke() and bench.py's CPU baseline use it
+ * as the checker of the CUDA path.  It restates, in plain C and FP64, the
+ * reference's algorithms for the functions the CUDA path replaces; each
+ * function cites the reference lines it follows.  It is pinned against the
+ * reference's own outputs (tests/golden/*.npz, made by running the
+ * reference's C++ through oracle/_ref/ref_dump) by tests/test_oracle.py.
+ *
+ * Conventions: positions/forces are n x 3 row-major doubles (nm, kJ/mol/nm),
+ * r_ij = r_j - r_i, f_i += f_ij, the returned virial is the contribution to
+ * Ensemble::virial (= -sum f_ij (x) r_ij, row-major).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define OR_PI 3.14159265358979323846
+#define OR_SQRT_PI 1.7724538509055160273
+#define OR_KB 0.0083145112
+
+/* Ensemble::apply_pbc (src/Ensemble.h:319-334) */
+static void pbc(double *d, const double *L) {
+    for (int k = 0; k < 3; k++) {
+        double h = L[k] / 2.0;
+        while (d[k] >= h) d[k] -= L[k];
+        while (d[k] < -h) d[k] += L[k];
+    }
+}
+
+static int excluded(int i, int j, const int32_t *off, const int32_t *ex) {
+    for (int e = off[i]; e < off[i + 1]; e++)
+        if (ex[e] == j) return 1;
+    return 0;
+}
+
+/* Ensemble::build_pairlist (src/Ensemble.cpp:492-525): all i < j not in the
+ * exclusion table with |pbc(r_j - r_i)|^2 < (rc + skin)^2.  Writes pairs as
+ * (i, j) into out (capacity cap pairs); returns the number of pairs. */
+int64_t or_pairlist(int n, const double *pos, const double *L, double rl2, const int32_t *off,
+                    const int32_t *ex, int32_t *out, int64_t cap) {
+    int64_t k = 0;
+    for (int i = 0; i < n - 1; i++)
+        for (int j = i + 1; j < n; j++) {
+            if (excluded(i, j, off, ex)) continue;
+            double d[3] = {pos[3 * j] - pos[3 * i], pos[3 * j + 1] - pos[3 * i + 1],
+                           pos[3 * j + 2] - pos[3 * i + 2]};
+            pbc(d, L);
+            double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+            if (r2 < rl2) {
+                if (k < cap) { out[2 * k] = i; out[2 * k + 1] = j; }
+                k++;
+            }
+        }
+    return k;
+}
+
+static void vir_add(double *w, const double *f, const double *r) {
+    /* local virial[XY] += f.y * r.x (LJForce.cpp:206-214), stored negated */
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) w[3 * a + b] -= f[b] * r[a];
+}
+
+/* LJForce::compute (src/forces/LJForce.cpp:58-255) over a given pair list:
+ * same-molecule pairs skipped, r*r <= rc^2 with r = |r_ij|, energy shifted
+ * by U(rc) when shift != 0, long-range correction e_lrc / v_lrc added. */
+double or_lj(int n, const double *pos, const int32_t *type, const int32_t *mol, const double *L,
+             int nt, const double *sig2, const double *eps4, double rc, int shift, double e_lrc,
+             double v_lrc, const int32_t *pairs, int64_t np, double *f, double *w) {
+    double rc2 = rc * rc, rcut_2 = 1.0 / rc2, energy = 0.0;
+    memset(f, 0, sizeof(double) * 3 * n);
+    memset(w, 0, sizeof(double) * 9);
+    for (int64_t p = 0; p < np; p++) {
+        int i = pairs[2 * p], j = pairs[2 * p + 1];
+        if (mol[i] == mol[j]) continue;
+        double d[3] = {pos[3 * j] - pos[3 * i], pos[3 * j + 1] - pos[3 * i + 1],
+                       pos[3 * j + 2] - pos[3 * i + 2]};
+        pbc(d, L);
+        double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        double rij2 = r * r;
+        if (rij2 > rc2) continue;
+        int t = type[i] * nt + type[j];
+        double r_1 = 1.0 / r, rij_2 = r_1 * r_1;
+        double sr2 = sig2[t] * rij_2, sr6 = sr2 * sr2 * sr2, sr12 = sr6 * sr6;
+        double e = eps4[t] * (sr12 - sr6);
+        double fs = (sr12 + sr12 - sr6) * 6 * eps4[t] * rij_2;
+        if (shift) {
+            double c2 = sig2[t] * rcut_2, c6 = c2 * c2 * c2;
+            e -= eps4[t] * (c6 * c6 - c6);
+        }
+        energy += e;
+        double fij[3] = {-fs * d[0], -fs * d[1], -fs * d[2]};
+        for (int k = 0; k < 3; k++) { f[3 * i + k] += fij[k]; f[3 * j + k] -= fij[k]; }
+        vir_add(w, fij, d);
+    }
+    w[0] -= v_lrc; w[4] -= v_lrc; w[8] -= v_lrc;
+    return energy + e_lrc;
+}
+
+/* Leap-frog Nose-Hoover MD of a Lennard-Jones system: LFIntegrator::start
+ * (LFIntegrator.cpp:1172-1173) then nsteps of LFIntegrator::run
+ * (:278-941) with the unconstrained update (:588-642), zeta update
+ * (:688-722), COM drift removal (:359-379), molecule wrap (:897-912) and
+ * brute-force list rebuild when a displacement exceeds skin/2.
+ * Monatomic molecules (mol[i] == i) only.  out_epot/out_temp/out_zeta:
+ * per-step potential energy (at the step's start), atomic temperature and
+ * zeta.  pos/vel are updated in place; vtm receives v(t - dt/2). */
+int or_lj_md(int n, double *pos, double *vel, double *vtm, const double *mass,
+             const int32_t *type, const int32_t *mol, const double *L, int nt, const double *sig2,
+             const double *eps4, double rc, double skin, int shift, double e_lrc, double v_lrc,
+             double dt, double T, double tau, int nsteps, double *out_epot, double *out_temp,
+             double *out_zeta) {
+    int64_t cap = (int64_t)n * 400;
+    int32_t *pairs = (int32_t *)malloc(sizeof(int32_t) * 2 * cap);
+    int32_t *off = (int32_t *)calloc(n + 1, sizeof(int32_t));
+    double *f = (double *)malloc(sizeof(double) * 3 * n);
+    double *disp = (double *)calloc(3 * n, sizeof(double));
+    double w[9];
+    double rl = rc + skin, rl2 = rl * rl, drmax = skin * skin / 4.0;
+    int64_t np = or_pairlist(n, pos, L, rl2, off, NULL, pairs, cap);
+    if (np > cap) return -1;
+    or_lj(n, pos, type, mol, L, nt, sig2, eps4, rc, shift, e_lrc, v_lrc, pairs, np, f, w);
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < 3; k++) vtm[3 * i + k] = vel[3 * i + k] - 0.5 * dt * (1.0 / mass[i]) * f[3 * i + k];
+    int ndf = 3 * n - 3;
+    double fnh = 0, fnhmi = 0, mtot = 0;
+    for (int i = 0; i < n; i++) mtot += mass[i];
+    for (int s = 0; s < nsteps; s++) {
+        int upd = 0;
+        for (int i = 0; i < n && !upd; i++)
+            if (disp[3 * i] * disp[3 * i] + disp[3 * i + 1] * disp[3 * i + 1] + disp[3 * i + 2] * disp[3 * i + 2] > drmax) upd = 1;
+        if (upd) {
+            memset(disp, 0, sizeof(double) * 3 * n);
+            np = or_pairlist(n, pos, L, rl2, off, NULL, pairs, cap);
+            if (np > cap) return -1;
+        }
+        double vom[3] = {0, 0, 0};
+        for (int i = 0; i < n; i++)
+            for (int k = 0; k < 3; k++) vom[k] += vtm[3 * i + k] * mass[i];
+        for (int k = 0; k < 3; k++) vom[k] /= mtot;
+        if (fabs(vom[0]) > 1e-11 || fabs(vom[1]) > 1e-11 || fabs(vom[2]) > 1e-11)
+            for (int i = 0; i < n; i++)
+                for (int k = 0; k < 3; k++) { vtm[3 * i + k] -= vom[k]; vel[3 * i + k] -= vom[k]; }
+        out_epot[s] = or_lj(n, pos, type, mol, L, nt, sig2, eps4, rc, shift, e_lrc, v_lrc, pairs, np, f, w);
+        double ke = 0;
+        for (int i = 0; i < n; i++) {
+            double mr = 1.0 / mass[i], vp[3], *v = &vel[3 * i], *vm = &vtm[3 * i];
+            double velcheck = 1.0;
+            int cnt = 0;
+            while (velcheck > 1e-10 && cnt < 11) {
+                for (int k = 0; k < 3; k++) vp[k] = vm[k] + dt * (mr * f[3 * i + k] - fnh * v[k]);
+                double dd = 0;
+                for (int k = 0; k < 3; k++) {
+                    double nv = (vp[k] + vm[k]) * 0.5;
+                    dd += (nv - v[k]) * (nv - v[k]);
+                    v[k] = nv;
+                }
+                velcheck = sqrt(dd);
+                cnt++;
+            }
+            if (cnt == 10) return -2;
+            for (int k = 0; k < 3; k++) {
+                double dr = dt * vp[k];
+                pos[3 * i + k] += dr;
+                disp[3 * i + k] += dr;
+                v[k] = (vp[k] + vm[k]) * 0.5;
+                vm[k] = vp[k];
+            }
+            ke += (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) * mass[i];
+            /* monatomic molecule: wrap the atom into the box */
+            double c[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]}, o[3] = {c[0], c[1], c[2]};
+            pbc(c, L);
+            for (int k = 0; k < 3; k++) pos[3 * i + k] += c[k] - o[k];
+        }
+        double qq = ndf * OR_KB * T * tau * tau;
+        double fnhpl = fnhmi + dt * (1.0 / qq) * (ke - ndf * OR_KB * T);
+        fnh = 0.5 * (fnhpl + fnhmi);
+        fnhmi = fnhpl;
+        out_temp[s] = ke / (ndf * OR_KB);
+        out_zeta[s] = fnh;
+    }
+    free(pairs); free(off); free(f); free(disp);
+    return 0;
+}
+
+/* Ewald real-space term (EwaldForce::real_term, src/forces/EwaldForce.cpp:
+ * 296-527) over a pair list: q_i q_j erfc(a r)/r for r^2 < rc^2 (scaled
+ * charges), all listed pairs.  Returns the real-space energy. */
+double or_ewald_real(int n, const double *pos, const double *q, const double *L, double alpha,
+                     double rc, const int32_t *pairs, int64_t np, double *f, double *w) {
+    double rc2 = rc * rc, a2 = alpha * alpha, a2pi = 2.0 * alpha / OR_SQRT_PI, energy = 0;
+    for (int64_t p = 0; p < np; p++) {
+        int i = pairs[2 * p], j = pairs[2 * p + 1];
+        double d[3] = {pos[3 * j] - pos[3 * i], pos[3 * j + 1] - pos[3 * i + 1],
+                       pos[3 * j + 2] - pos[3 * i + 2]};
+        pbc(d, L);
+        double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+        if (!(r2 < rc2)) continue;
+        double qij = q[i] * q[j], r = sqrt(r2);
+        double e = erfc(alpha * r) / r;
+        double fs = (e + a2pi * exp(-a2 * r2)) / r2;
+        energy += qij * e;
+        double fij[3] = {-qij * fs * d[0], -qij * fs * d[1], -qij * fs * d[2]};
+        for (int k = 0; k < 3; k++) { f[3 * i + k] += fij[k]; f[3 * j + k] -= fij[k]; }
+        vir_add(w, fij, d);
+    }
+    return energy;
+}
+
+/* Ewald reciprocal term (EwaldForce::set_up + reciprocal_term,
+ * src/forces/EwaldForce.cpp:198-257, 529-698): half-space k set with
+ * k^2 < kcut^2.  Adds forces into f, the long virial into w (all nine
+ * components), returns the energy; *nk receives the k count. */
+double or_ewald_recip(int n, const double *pos, const double *q, const double *L, double alpha,
+                      double kcut, double *f, double *w, int *nk_out) {
+    double kc2 = kcut * kcut, aR4 = 1.0 / (4.0 * alpha * alpha);
+    int nmax[3];
+    for (int d = 0; d < 3; d++) nmax[d] = (int)(kcut * L[d] / (2 * OR_PI));
+    double v[3] = {2.0 * OR_PI / L[0], 2.0 * OR_PI / L[1], 2.0 * OR_PI / L[2]};
+    double vol = L[0] * L[1] * L[2], pi4V = 4.0 * OR_PI * (1.0 / vol), pi8V = 2.0 * pi4V;
+    double *sc = (double *)malloc(sizeof(double) * 2 * n), pe = 0;
+    int nk = 0;
+    for (int nx = 0; nx <= nmax[0]; nx++)
+        for (int ny = (nx == 0 ? 0 : -nmax[1]); ny <= nmax[1]; ny++)
+            for (int nz = ((nx == 0 && ny == 0) ? 1 : -nmax[2]); nz <= nmax[2]; nz++) {
+                double k[3] = {nx * v[0], ny * v[1], nz * v[2]};
+                double k2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
+                if (!(k2 < kc2)) continue;
+                nk++;
+                double expK = exp(-k2 * aR4) / k2, ss = 0, cs = 0;
+                for (int i = 0; i < n; i++) {
+                    double a = pos[3 * i] * k[0] + pos[3 * i + 1] * k[1] + pos[3 * i + 2] * k[2];
+                    sc[2 * i] = q[i] * sin(a);
+                    sc[2 * i + 1] = q[i] * cos(a);
+                    ss += sc[2 * i];
+                    cs += sc[2 * i + 1];
+                }
+                double e = pi4V * expK * (ss * ss + cs * cs);
+                pe += e;
+                double coeff = 2.0 * (aR4 + 1.0 / k2);
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) w[3 * a + b] += (a == b ? e : 0.0) - e * coeff * k[a] * k[b];
+                double b = pi8V * expK;
+                for (int i = 0; i < n; i++) {
+                    double val = b * (sc[2 * i] * cs - sc[2 * i + 1] * ss);
+                    for (int d = 0; d < 3; d++) f[3 * i + d] += k[d] * val;
+                }
+            }
+    free(sc);
+    if (nk_out) *nk_out = nk;
+    return pe;
+}

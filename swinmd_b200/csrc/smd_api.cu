@@ -1,0 +1,724 @@
+// C-ABI entry points (declared in include/swinmd_b200.h): context lifetime,
+// topology and parameter upload, force evaluation and the integration loop.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <new>
+#include "smd_ctx.cuh"
+
+using namespace smd;
+
+struct smd_ctx {
+    Ctx c;
+};
+
+namespace {
+
+int fail(smd_ctx *x, int code, const std::string &msg) {
+    if (x) x->c.err = msg;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(x, SMD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t count) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc((void **)p, count * sizeof(T));
+}
+
+int status_to_code(unsigned st) {
+    if (st & ST_LIST_OVERFLOW) return SMD_ERR_LIST_OVERFLOW;
+    if (st & ST_NAN) return SMD_ERR_NAN;
+    if (st & (ST_SHAKE_ITER | ST_SHAKE_GEOM)) return SMD_ERR_SHAKE;
+    if (st & ST_NH_ITER) return SMD_ERR_NH_ITER;
+    if (st & ST_CG_ITER) return SMD_ERR_CG;
+    return SMD_OK;
+}
+
+const char *status_text(unsigned st) {
+    if (st & ST_LIST_OVERFLOW) return "pair list overflow: a site has more neighbours than the list holds";
+    if (st & ST_NAN) return "non-finite position";
+    if (st & ST_SHAKE_GEOM) return "SHAKE geometric failure";
+    if (st & ST_SHAKE_ITER) return "SHAKE did not converge within maxCount";
+    if (st & ST_NH_ITER) return "NH iteration Error";
+    if (st & ST_CG_ITER) return "dipole solve did not converge";
+    return "";
+}
+
+// Cell grid as CellManager::set_cellManager (src/utils/CellManager.cpp:43-84).
+void setup_grid(Ctx &c, int use_cells) {
+    CellGrid &g = c.grid;
+    double len = c.cutoff + c.cut_buffer;
+    g.use_cells = use_cells;
+    for (int d = 0; d < 3; d++)
+        if (len <= 0 || len > c.box.L[d] / 3.0) g.use_cells = 0;
+    if (!g.use_cells) {
+        g.ncell = 0;
+        for (int d = 0; d < 3; d++) { g.n[d] = 0; g.len[d] = g.rlen[d] = g.origin[d] = 0; }
+        return;
+    }
+    for (int d = 0; d < 3; d++) {
+        g.n[d] = (int)(c.box.L[d] / len);
+        g.len[d] = c.box.L[d] / g.n[d];
+        g.rlen[d] = 1.0 / g.len[d];
+        g.origin[d] = -c.box.L[d] / 2.0;
+    }
+    g.ncell = g.n[0] * g.n[1] * g.n[2];
+}
+
+int alloc_list(smd_ctx *x) {
+    Ctx &c = x->c;
+    if (c.n == 0 || c.box.L[0] <= 0) return SMD_OK;
+    double rl = c.cutoff + c.cut_buffer;
+    double vol = c.box.L[0] * c.box.L[1] * c.box.L[2];
+    double dens = c.n / vol;
+    double expect = 4.18879020478639 * rl * rl * rl * dens;
+    int cap = (int)(expect * 1.6 + 64);
+    cap = (cap + 31) & ~31;
+    cap = std::min(cap, c.n);
+    cap = std::max(cap, 32);
+    if (cap != c.pl.max_nbr || !c.pl.nbr) {
+        c.pl.max_nbr = cap;
+        CK(dalloc(&c.pl.nbr, (size_t)cap * c.n));
+    }
+    int ncell = std::max(c.grid.ncell, 1);
+    if (ncell > c.pl.cell_cap) {
+        CK(dalloc(&c.pl.cell_count, ncell));
+        CK(dalloc(&c.pl.cell_start, ncell + 1));
+        CK(cudaMemset(c.pl.cell_count, 0, ncell * sizeof(int)));
+        c.pl.cell_cap = ncell;
+    }
+    c.list_valid = 0;
+    c.graph_dirty = 1;
+    return SMD_OK;
+}
+
+int sync_status(smd_ctx *x) {
+    Ctx &c = x->c;
+    CK(cudaStreamSynchronize(c.stream));
+    CK(cudaGetLastError());
+    unsigned st = 0;
+    CK(cudaMemcpy(&st, c.status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    int code = status_to_code(st);
+    if (code != SMD_OK) return fail(x, code, status_text(st));
+    return SMD_OK;
+}
+
+void enqueue_forces(Ctx &c) {
+    launch_pair(c);
+    if (c.ewald_on) launch_recip(c);
+}
+
+void enqueue_step(Ctx &c) {
+    launch_nlist(c, false);
+    enqueue_forces(c);
+    launch_integrate(c);
+}
+
+}  // namespace
+
+extern "C" {
+
+int smd_create(int device, smd_ctx **out) {
+    smd_ctx *x = nullptr;
+    if (!out) return SMD_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return SMD_ERR_NO_DEVICE;
+    if (device < 0 || device >= ndev) return SMD_ERR_ARG;
+    x = new (std::nothrow) smd_ctx();
+    if (!x) return SMD_ERR_ARG;
+    Ctx &c = x->c;
+    c.device = device;
+    if (cudaSetDevice(device) != cudaSuccess) { delete x; return SMD_ERR_CUDA; }
+    if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete x;
+        return SMD_ERR_CUDA;
+    }
+    if (dalloc(&c.acc, ACC_COUNT) != cudaSuccess || dalloc(&c.scal, 8) != cudaSuccess ||
+        dalloc(&c.ticket, 1) != cudaSuccess || dalloc(&c.status, 1) != cudaSuccess ||
+        dalloc(&c.flags, 4) != cudaSuccess || dalloc(&c.obs, 1) != cudaSuccess) {
+        delete x;
+        return SMD_ERR_CUDA;
+    }
+    cudaMemset(c.acc, 0, ACC_COUNT * sizeof(long long));
+    cudaMemset(c.scal, 0, 8 * sizeof(double));
+    cudaMemset(c.ticket, 0, sizeof(unsigned));
+    cudaMemset(c.status, 0, sizeof(unsigned));
+    cudaMemset(c.flags, 0, 4 * sizeof(int));
+    cudaMemset(c.obs, 0, sizeof(smd_observables));
+    *out = x;
+    return SMD_OK;
+}
+
+void smd_destroy(smd_ctx *x) {
+    if (!x) return;
+    Ctx &c = x->c;
+    cudaSetDevice(c.device);
+    if (c.step_graph) cudaGraphExecDestroy(c.step_graph);
+    void *ptrs[] = {c.type, c.mol, c.mol_off, c.mol_atoms, c.excl_off, c.excl, c.mass,
+                    c.pair_par, c.pair_par_f, c.type_q, c.pos4, c.vel4, c.vtm4, c.disp4, c.fixq,
+                    c.frc, c.acc, c.scal, c.partials, c.ticket, c.status, c.flags, c.obs,
+                    c.series, c.pl.nbr, c.pl.nnbr, c.pl.cell_of, c.pl.cell_slot,
+                    c.pl.cell_count, c.pl.cell_start, c.pl.cell_atoms, c.rc.kn, c.rc.kcoef,
+                    c.rc.sk, c.rc.kvec};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (c.stream) cudaStreamDestroy(c.stream);
+    delete x;
+}
+
+const char *smd_last_error(const smd_ctx *x) { return x ? x->c.err.c_str() : "null context"; }
+
+int smd_set_topology(smd_ctx *x, int n, int ntypes, const int32_t *atom_type,
+                     const int32_t *mol_id, const double *mass, const double *scaled_charge) {
+    if (!x || n <= 0 || ntypes <= 0 || ntypes > 8 || !atom_type || !mol_id || !mass || !scaled_charge)
+        return fail(x, SMD_ERR_ARG, "smd_set_topology: bad arguments (ntypes must be 1..8)");
+    Ctx &c = x->c;
+    CK(cudaSetDevice(c.device));
+    c.n = n;
+    c.ntypes = ntypes;
+    c.h_type.assign(atom_type, atom_type + n);
+    c.h_mol.assign(mol_id, mol_id + n);
+    c.h_mass.assign(mass, mass + n);
+    c.h_charge.assign(scaled_charge, scaled_charge + n);
+    int nmol = 0;
+    for (int i = 0; i < n; i++) {
+        if (atom_type[i] < 0 || atom_type[i] >= ntypes || mol_id[i] < 0)
+            return fail(x, SMD_ERR_ARG, "smd_set_topology: atom type or molecule id out of range");
+        nmol = std::max(nmol, mol_id[i] + 1);
+    }
+    c.nmol = nmol;
+    // molecule -> atoms in atom order (Molecule::add_atom, src/Ensemble.cpp:216-222)
+    c.h_mol_off.assign(nmol + 1, 0);
+    for (int i = 0; i < n; i++) c.h_mol_off[mol_id[i] + 1]++;
+    for (int m = 0; m < nmol; m++) c.h_mol_off[m + 1] += c.h_mol_off[m];
+    c.h_mol_atoms.assign(n, 0);
+    std::vector<int> fill(c.h_mol_off.begin(), c.h_mol_off.end() - 1);
+    for (int i = 0; i < n; i++) c.h_mol_atoms[fill[mol_id[i]]++] = i;
+    for (int m = 0; m < nmol; m++)
+        if (c.h_mol_off[m + 1] == c.h_mol_off[m])
+            return fail(x, SMD_ERR_ARG, "smd_set_topology: molecule ids must be contiguous from 0");
+    // charge per type (Atom::scaledCharge is a per-type parameter)
+    c.h_type_charge.assign(ntypes, 0.0);
+    std::vector<int> seen(ntypes, 0);
+    for (int i = 0; i < n; i++) {
+        int t = atom_type[i];
+        if (!seen[t]) { c.h_type_charge[t] = scaled_charge[i]; seen[t] = 1; }
+        else if (c.h_type_charge[t] != scaled_charge[i])
+            return fail(x, SMD_ERR_ARG, "smd_set_topology: charges must be per atom type");
+    }
+    c.total_mass = 0;
+    for (int i = 0; i < n; i++) c.total_mass += mass[i];
+
+    CK(dalloc(&c.type, n)); CK(dalloc(&c.mol, n)); CK(dalloc(&c.mass, n));
+    CK(dalloc(&c.mol_off, nmol + 1)); CK(dalloc(&c.mol_atoms, n));
+    CK(dalloc(&c.type_q, ntypes));
+    CK(dalloc(&c.pos4, n)); CK(dalloc(&c.vel4, n)); CK(dalloc(&c.vtm4, n));
+    CK(dalloc(&c.disp4, n)); CK(dalloc(&c.fixq, n));
+    CK(dalloc(&c.frc, 3 * (size_t)n));
+    CK(dalloc(&c.pl.nnbr, n)); CK(dalloc(&c.pl.cell_of, n)); CK(dalloc(&c.pl.cell_slot, n));
+    CK(dalloc(&c.pl.cell_atoms, n));
+    int nb = (nmol + 127) / 128;
+    CK(dalloc(&c.partials, (size_t)nb * 32));
+    CK(cudaMemcpy(c.type, atom_type, n * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.mol, mol_id, n * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.mass, mass, n * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.mol_off, c.h_mol_off.data(), (nmol + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.mol_atoms, c.h_mol_atoms.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.type_q, c.h_type_charge.data(), ntypes * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemset(c.disp4, 0, n * sizeof(double4)));
+    CK(cudaMemset(c.frc, 0, 3 * (size_t)n * sizeof(long long)));
+    // velocity arrays carry 1/m and m in .w
+    std::vector<double4> v(n), vm(n);
+    for (int i = 0; i < n; i++) {
+        v[i] = make_double4(0, 0, 0, 1.0 / mass[i]);
+        vm[i] = make_double4(0, 0, 0, mass[i]);
+    }
+    CK(cudaMemcpy(c.vel4, v.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.vtm4, vm.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
+    // no exclusions until smd_set_exclusions
+    std::vector<int> off(n + 1, 0);
+    c.h_excl_off = off;
+    c.h_excl.clear();
+    CK(dalloc(&c.excl_off, n + 1)); CK(dalloc(&c.excl, 1));
+    CK(cudaMemcpy(c.excl_off, off.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    // default pair parameters: none
+    CK(dalloc(&c.pair_par, (size_t)ntypes * ntypes * 4));
+    CK(cudaMemset(c.pair_par, 0, (size_t)ntypes * ntypes * 4 * sizeof(double)));
+    c.list_valid = 0;
+    c.graph_dirty = 1;
+    return alloc_list(x);
+}
+
+int smd_set_exclusions(smd_ctx *x, const int32_t *offsets, const int32_t *partners) {
+    if (!x || !offsets || x->c.n == 0) return fail(x, SMD_ERR_ARG, "smd_set_exclusions: bad arguments");
+    Ctx &c = x->c;
+    int n = c.n;
+    int tot = offsets[n];
+    if (offsets[0] != 0 || tot < 0 || (tot > 0 && !partners))
+        return fail(x, SMD_ERR_ARG, "smd_set_exclusions: bad CSR offsets");
+    for (int i = 0; i < n; i++)
+        if (offsets[i + 1] < offsets[i]) return fail(x, SMD_ERR_ARG, "smd_set_exclusions: offsets decrease");
+    for (int k = 0; k < tot; k++)
+        if (partners[k] < 0 || partners[k] >= n) return fail(x, SMD_ERR_ARG, "smd_set_exclusions: partner out of range");
+    c.h_excl_off.assign(offsets, offsets + n + 1);
+    c.h_excl.assign(partners, partners + tot);
+    CK(dalloc(&c.excl, std::max(tot, 1)));
+    CK(cudaMemcpy(c.excl_off, offsets, (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    if (tot) CK(cudaMemcpy(c.excl, partners, tot * sizeof(int), cudaMemcpyHostToDevice));
+    c.list_valid = 0;
+    c.graph_dirty = 1;
+    return SMD_OK;
+}
+
+int smd_set_box(smd_ctx *x, double lx, double ly, double lz) {
+    if (!x || !(lx > 0) || !(ly > 0) || !(lz > 0)) return fail(x, SMD_ERR_ARG, "smd_set_box: edges must be > 0");
+    Ctx &c = x->c;
+    c.box.L[0] = lx; c.box.L[1] = ly; c.box.L[2] = lz;
+    for (int d = 0; d < 3; d++) {
+        c.box.half[d] = 0.5 * c.box.L[d];
+        c.box.inv[d] = 1.0 / c.box.L[d];
+    }
+    setup_grid(c, c.want_cells);
+    if (c.ewald_on) {
+        int r = setup_recip(c);
+        if (r) return fail(x, r, "smd_set_box: reciprocal set-up failed");
+    }
+    return alloc_list(x);
+}
+
+int smd_set_pairlist(smd_ctx *x, double cutoff, double cut_buffer, int use_cells) {
+    if (!x || !(cutoff > 0) || cut_buffer < 0) return fail(x, SMD_ERR_ARG, "smd_set_pairlist: bad cutoff");
+    Ctx &c = x->c;
+    c.cutoff = cutoff;
+    c.cut_buffer = cut_buffer;
+    double pc = cutoff + cut_buffer;   // Ensemble::set_pairlist, src/Ensemble.cpp:456-457
+    pc *= pc;
+    c.pl.rl2 = pc;
+    c.pl.drmax = cut_buffer * cut_buffer / 4.0;  // Integrator.cpp:36
+    c.vdw_rc2 = cutoff * cutoff;
+    c.want_cells = use_cells;
+    setup_grid(c, use_cells);
+    return alloc_list(x);
+}
+
+int smd_set_vdw(smd_ctx *x, int kind, const double *params, int switch_on, double switch_dist2,
+                double e_lrc, double v_lrc) {
+    if (!x || kind < 0 || kind > 3 || (kind != SMD_VDW_NONE && !params) || x->c.ntypes == 0)
+        return fail(x, SMD_ERR_ARG, "smd_set_vdw: bad arguments");
+    Ctx &c = x->c;
+    int nt = c.ntypes;
+    std::vector<double> p((size_t)nt * nt * 4, 0.0);
+    if (params) std::memcpy(p.data(), params, p.size() * sizeof(double));
+    c.vdw = kind;
+    c.switch_on = switch_on;
+    c.e_lrc = e_lrc;
+    c.v_lrc = v_lrc;
+    double rc2 = c.vdw_rc2;
+    if (kind == SMD_VDW_LJ) {
+        // energy at the cutoff (LJForce.cpp:159-166)
+        double rcut_2 = 1.0 / rc2;
+        for (int k = 0; k < nt * nt; k++) {
+            double sr2 = p[4 * k] * rcut_2;
+            double sr6 = sr2 * sr2 * sr2;
+            double sr12 = sr6 * sr6;
+            p[4 * k + 2] = p[4 * k + 1] * (sr12 - sr6);
+        }
+    }
+    // 5th-order switch constants (MieForce.cpp:26-46)
+    c.sw_rs2 = rc2;
+    if (switch_on) c.sw_rs2 = switch_dist2;
+    if (switch_on && rc2 > c.sw_rs2) {
+        double c1 = 1.0 / (rc2 - c.sw_rs2);
+        c.sw_c1 = c1 * c1 * c1;
+        c.sw_c2 = rc2 - 3.0 * c.sw_rs2;
+        c.sw_c3 = 4 * c.sw_c1;
+    } else {
+        c.sw_c1 = c.sw_c2 = c.sw_c3 = 0.0;
+        if (kind != SMD_VDW_LJ) c.sw_rs2 = rc2;  // switch inactive
+    }
+    CK(cudaMemcpy(c.pair_par, p.data(), p.size() * sizeof(double), cudaMemcpyHostToDevice));
+    c.graph_dirty = 1;
+    return SMD_OK;
+}
+
+int smd_set_ewald(smd_ctx *x, double alpha, double kcut, double real_cut) {
+    if (!x || !(alpha > 0) || !(kcut > 0) || !(real_cut > 0) || x->c.n == 0)
+        return fail(x, SMD_ERR_ARG, "smd_set_ewald: bad arguments");
+    Ctx &c = x->c;
+    c.ewald_on = 1;
+    c.ew_alpha = alpha;
+    c.ew_kcut = kcut;
+    c.ew_rc2 = real_cut * real_cut;
+    // self and net-charge energies (EwaldForce.cpp:63-79)
+    double qsum = 0, q2sum = 0;
+    for (int i = 0; i < c.n; i++) {
+        qsum += c.h_charge[i];
+        q2sum += c.h_charge[i] * c.h_charge[i];
+    }
+    const double PI = 3.14159265358979323846, SQRT_PI = 1.7724538509055160273;
+    c.e_self = -q2sum * alpha / SQRT_PI;
+    if (std::fabs(qsum) > 1.0e-5) {
+        double vol = c.box.L[0] * c.box.L[1] * c.box.L[2];
+        c.e_self += -PI * qsum * qsum / (2.0 * vol * alpha * alpha);
+    }
+    int r = setup_recip(c);
+    if (r) return fail(x, r, "smd_set_ewald: reciprocal set-up failed");
+    c.graph_dirty = 1;
+    return SMD_OK;
+}
+
+int smd_set_precision(smd_ctx *x, int mode) {
+    if (!x || (mode != SMD_PREC_FP64 && mode != SMD_PREC_MIXED))
+        return fail(x, SMD_ERR_ARG, "smd_set_precision: unknown mode");
+    x->c.precision = mode;
+    x->c.graph_dirty = 1;
+    return SMD_OK;
+}
+
+int smd_set_tuning(smd_ctx *x, int tpp) {
+    if (!x) return SMD_ERR_ARG;
+    if (tpp == 0) tpp = 8;
+    if (tpp < 1 || tpp > 32 || (tpp & (tpp - 1)))
+        return fail(x, SMD_ERR_ARG, "smd_set_tuning: threads per site must be a power of two <= 32");
+    x->c.tpp = tpp;
+    x->c.graph_dirty = 1;
+    return SMD_OK;
+}
+
+int smd_upload_positions(smd_ctx *x, const double *pos) {
+    if (!x || !pos || x->c.n == 0) return fail(x, SMD_ERR_ARG, "smd_upload_positions: bad arguments");
+    Ctx &c = x->c;
+    std::vector<double4> p(c.n);
+    for (int i = 0; i < c.n; i++)
+        p[i] = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], (double)c.h_type[i]);
+    CK(cudaMemcpyAsync(c.pos4, p.data(), c.n * sizeof(double4), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaMemsetAsync(c.disp4, 0, c.n * sizeof(double4), c.stream));
+    int one = 1;  // the next step rebuilds the pair list from these positions
+    CK(cudaMemcpyAsync(c.flags, &one, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    c.list_valid = 0;
+    return SMD_OK;
+}
+
+int smd_upload_velocities(smd_ctx *x, const double *vel, const double *vtminus) {
+    if (!x || !vel || x->c.n == 0) return fail(x, SMD_ERR_ARG, "smd_upload_velocities: bad arguments");
+    Ctx &c = x->c;
+    std::vector<double4> v(c.n), vm(c.n);
+    for (int i = 0; i < c.n; i++) {
+        v[i] = make_double4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], 1.0 / c.h_mass[i]);
+        const double *s = vtminus ? vtminus : vel;
+        vm[i] = make_double4(s[3 * i], s[3 * i + 1], s[3 * i + 2], c.h_mass[i]);
+    }
+    CK(cudaMemcpyAsync(c.vel4, v.data(), c.n * sizeof(double4), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaMemcpyAsync(c.vtm4, vm.data(), c.n * sizeof(double4), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return SMD_OK;
+}
+
+int smd_download_state(smd_ctx *x, double *pos, double *vel, double *vtminus) {
+    if (!x || x->c.n == 0) return fail(x, SMD_ERR_ARG, "smd_download_state: bad arguments");
+    Ctx &c = x->c;
+    std::vector<double4> h(c.n);
+    double *outs[3] = {pos, vel, vtminus};
+    double4 *srcs[3] = {c.pos4, c.vel4, c.vtm4};
+    for (int q = 0; q < 3; q++) {
+        if (!outs[q]) continue;
+        CK(cudaMemcpyAsync(h.data(), srcs[q], c.n * sizeof(double4), cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+        for (int i = 0; i < c.n; i++) {
+            outs[q][3 * i] = h[i].x;
+            outs[q][3 * i + 1] = h[i].y;
+            outs[q][3 * i + 2] = h[i].z;
+        }
+    }
+    return SMD_OK;
+}
+
+int smd_compute_forces(smd_ctx *x, uint32_t terms, double *force, double *energy, double *virial) {
+    if (!x || x->c.n == 0 || x->c.box.L[0] <= 0) return fail(x, SMD_ERR_ARG, "smd_compute_forces: system not set up");
+    Ctx &c = x->c;
+    CK(cudaSetDevice(c.device));
+    CK(cudaMemsetAsync(c.status, 0, sizeof(unsigned), c.stream));
+    launch_nlist(c, true);
+    c.list_valid = 1;
+    CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
+    CK(cudaMemsetAsync(c.frc, 0, 3 * (size_t)c.n * sizeof(long long), c.stream));
+    const int save_vdw = c.vdw, save_ew = c.ewald_on;
+    if (!(terms & SMD_TERM_VDW)) c.vdw = VDW_NONE;
+    bool want_real = (terms & SMD_TERM_EWALD_REAL) && c.ewald_on;
+    bool want_long = (terms & SMD_TERM_EWALD_LONG) && c.ewald_on;
+    c.ewald_on = want_real ? 1 : 0;
+    launch_pair(c);
+    c.ewald_on = save_ew;
+    if (want_long) launch_recip(c);
+    c.vdw = save_vdw;
+    double *dforce = nullptr;
+    if (force) {
+        CK(cudaMalloc(&dforce, 3 * (size_t)c.n * sizeof(double)));
+        launch_finalize_forces(c, dforce);
+    }
+    long long hacc[ACC_COUNT];
+    CK(cudaMemcpyAsync(hacc, c.acc, sizeof(hacc), cudaMemcpyDeviceToHost, c.stream));
+    if (force) CK(cudaMemcpyAsync(force, dforce, 3 * (size_t)c.n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    int rs = sync_status(x);
+    if (dforce) cudaFree(dforce);
+    if (rs) return rs;
+    const bool vdw = (terms & SMD_TERM_VDW) && c.vdw != VDW_NONE;
+    if (energy) {
+        for (int q = 0; q < SMD_E_COUNT; q++) energy[q] = 0;
+        energy[SMD_E_VDW] = (double)hacc[ACC_E_VDW] * ACC_INV + (vdw ? c.e_lrc : 0.0);
+        energy[SMD_E_REAL] = (double)hacc[ACC_E_REAL] * ACC_INV;
+        energy[SMD_E_LONG] = (double)hacc[ACC_E_LONG] * ACC_INV;
+        energy[SMD_E_CORRECT] = want_real ? c.e_self : 0.0;
+        energy[SMD_E_MOLCORRECT] = (double)hacc[ACC_E_INTRA] * ACC_INV;
+        energy[SMD_E_SURF] = (double)hacc[ACC_E_SURF] * ACC_INV;
+    }
+    if (virial) {
+        for (int q = 0; q < 9; q++) {
+            virial[q] = ((double)hacc[ACC_VIR + q] + (double)hacc[ACC_LVIR + q]) * ACC_INV;
+            if (vdw && (q == 0 || q == 4 || q == 8)) virial[q] -= c.v_lrc;
+        }
+    }
+    return SMD_OK;
+}
+
+int smd_get_pairs(smd_ctx *x, int32_t *pairs, int64_t cap, int64_t *count) {
+    if (!x || !count || x->c.n == 0) return fail(x, SMD_ERR_ARG, "smd_get_pairs: bad arguments");
+    Ctx &c = x->c;
+    if (!c.list_valid) {
+        CK(cudaMemsetAsync(c.status, 0, sizeof(unsigned), c.stream));
+        launch_nlist(c, true);
+        c.list_valid = 1;
+        int rs = sync_status(x);
+        if (rs) return rs;
+    }
+    std::vector<int> nn(c.n);
+    std::vector<int> nb((size_t)c.pl.max_nbr * c.n);
+    CK(cudaMemcpy(nn.data(), c.pl.nnbr, c.n * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(nb.data(), c.pl.nbr, nb.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    int64_t k = 0;
+    for (int i = 0; i < c.n; i++)
+        for (int q = 0; q < nn[i]; q++) {
+            int j = nb[(size_t)q * c.n + i] & 0x7fffffff;
+            if (i < j) {
+                if (pairs && k < cap) { pairs[2 * k] = i; pairs[2 * k + 1] = j; }
+                k++;
+            }
+        }
+    *count = k;
+    return SMD_OK;
+}
+
+int smd_ewald_nk(smd_ctx *x, int *nk) {
+    if (!x || !nk) return SMD_ERR_ARG;
+    *nk = x->c.rc.nk;
+    return SMD_OK;
+}
+
+int smd_set_integrator(smd_ctx *x, const smd_integrator_params *p) {
+    if (!x || !p || !(p->timestep > 0) || x->c.n == 0)
+        return fail(x, SMD_ERR_ARG, "smd_set_integrator: bad arguments");
+    if (p->constraint != 0)
+        return fail(x, SMD_ERR_ARG, "smd_set_integrator: constraint mode not available in this build");
+    if (p->long_steps > 1)
+        return fail(x, SMD_ERR_ARG, "smd_set_integrator: long_steps > 1 not supported");
+    Ctx &c = x->c;
+    c.ip = *p;
+    if (c.ip.atom_ndf <= 0) c.ip.atom_ndf = 3 * c.n - 3;
+    if (c.ip.mol_ndf <= 0) c.ip.mol_ndf = 3 * c.nmol - 3;
+    c.integrator_ready = 1;
+    c.graph_dirty = 1;
+    return SMD_OK;
+}
+
+int smd_integrator_start(smd_ctx *x) {
+    if (!x || !x->c.integrator_ready) return fail(x, SMD_ERR_ARG, "smd_integrator_start: call smd_set_integrator first");
+    Ctx &c = x->c;
+    CK(cudaSetDevice(c.device));
+    CK(cudaMemsetAsync(c.status, 0, sizeof(unsigned), c.stream));
+    CK(cudaMemsetAsync(c.obs, 0, sizeof(smd_observables), c.stream));
+    CK(cudaMemsetAsync(c.ticket, 0, sizeof(unsigned), c.stream));
+    launch_nlist(c, true);
+    c.list_valid = 1;
+    CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
+    enqueue_forces(c);
+    launch_start_velocities(c);
+    c.steps_done = 0;
+    return sync_status(x);
+}
+
+int smd_run(smd_ctx *x, int nsteps) {
+    if (!x || !x->c.integrator_ready || nsteps < 0) return fail(x, SMD_ERR_ARG, "smd_run: integrator not set");
+    Ctx &c = x->c;
+    CK(cudaSetDevice(c.device));
+    if (c.graph_dirty || !c.step_graph) {
+        if (c.step_graph) { cudaGraphExecDestroy(c.step_graph); c.step_graph = nullptr; }
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_step(c);
+        CK(cudaStreamEndCapture(c.stream, &g));
+        cudaError_t e = cudaGraphInstantiate(&c.step_graph, g, 0);
+        cudaGraphDestroy(g);
+        CK(e);
+        c.graph_dirty = 0;
+    }
+    for (int s = 0; s < nsteps; s++) CK(cudaGraphLaunch(c.step_graph, c.stream));
+    c.steps_done += nsteps;
+    return sync_status(x);
+}
+
+int smd_profile_stages(smd_ctx *x, int reps, double *out) {
+    if (!x || !out || reps <= 0 || !x->c.integrator_ready)
+        return fail(x, SMD_ERR_ARG, "smd_profile_stages: set up the integrator first");
+    Ctx &c = x->c;
+    CK(cudaSetDevice(c.device));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    // keep the state: the integrate stage runs on a copy of the step inputs
+    std::vector<long long> save_acc(ACC_COUNT);
+    float ms = 0;
+    auto timed = [&](auto &&fn) -> double {
+        fn();  // warm
+        cudaEventRecord(e0, c.stream);
+        for (int r = 0; r < reps; r++) fn();
+        cudaEventRecord(e1, c.stream);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);
+        return (double)ms / reps;
+    };
+    out[0] = timed([&] { launch_pair(c); });
+    out[1] = c.ewald_on ? timed([&] { launch_recip(c); }) : 0.0;
+    // integrate on scratch copies of the moving state
+    size_t nb = (size_t)c.n * sizeof(double4);
+    double4 *b_pos, *b_vel, *b_vtm, *b_disp;
+    CK(cudaMalloc(&b_pos, nb)); CK(cudaMalloc(&b_vel, nb));
+    CK(cudaMalloc(&b_vtm, nb)); CK(cudaMalloc(&b_disp, nb));
+    CK(cudaMemcpyAsync(b_pos, c.pos4, nb, cudaMemcpyDeviceToDevice, c.stream));
+    CK(cudaMemcpyAsync(b_vel, c.vel4, nb, cudaMemcpyDeviceToDevice, c.stream));
+    CK(cudaMemcpyAsync(b_vtm, c.vtm4, nb, cudaMemcpyDeviceToDevice, c.stream));
+    CK(cudaMemcpyAsync(b_disp, c.disp4, nb, cudaMemcpyDeviceToDevice, c.stream));
+    smd_observables o_save;
+    CK(cudaMemcpyAsync(&o_save, c.obs, sizeof(o_save), cudaMemcpyDeviceToHost, c.stream));
+    double sc_save[8];
+    CK(cudaMemcpyAsync(sc_save, c.scal, sizeof(sc_save), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    std::swap(c.pos4, b_pos); std::swap(c.vel4, b_vel); std::swap(c.vtm4, b_vtm); std::swap(c.disp4, b_disp);
+    out[2] = timed([&] { launch_integrate(c); });
+    std::swap(c.pos4, b_pos); std::swap(c.vel4, b_vel); std::swap(c.vtm4, b_vtm); std::swap(c.disp4, b_disp);
+    CK(cudaMemcpyAsync(c.obs, &o_save, sizeof(o_save), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaMemcpyAsync(c.scal, sc_save, sizeof(sc_save), cudaMemcpyHostToDevice, c.stream));
+    out[3] = timed([&] { launch_nlist(c, true); });
+    // forces for the current positions again, accumulators clear
+    CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
+    enqueue_forces(c);
+    CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    cudaFree(b_pos); cudaFree(b_vel); cudaFree(b_vtm); cudaFree(b_disp);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return sync_status(x);
+}
+
+int smd_step_kernel_count(smd_ctx *x, int *count) {
+    if (!x || !count) return SMD_ERR_ARG;
+    Ctx &c = x->c;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(c);
+    CK(cudaStreamEndCapture(c.stream, &g));
+    size_t nn = 0;
+    CK(cudaGraphGetNodes(g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    CK(cudaGraphGetNodes(g, nodes.data(), &nn));
+    int k = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        cudaGraphNodeGetType(nd, &t);
+        if (t == cudaGraphNodeTypeKernel) k++;
+    }
+    cudaGraphDestroy(g);
+    *count = k;
+    return SMD_OK;
+}
+
+int smd_run_timed(smd_ctx *x, int nsteps, double *device_ms) {
+    if (!x || !device_ms || !x->c.integrator_ready || nsteps < 0)
+        return fail(x, SMD_ERR_ARG, "smd_run_timed: integrator not set");
+    Ctx &c = x->c;
+    CK(cudaSetDevice(c.device));
+    if (c.graph_dirty || !c.step_graph) {
+        int r = smd_run(x, 0);
+        if (r) return r;
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaStreamSynchronize(c.stream));
+    CK(cudaEventRecord(e0, c.stream));
+    for (int s = 0; s < nsteps; s++) CK(cudaGraphLaunch(c.step_graph, c.stream));
+    CK(cudaEventRecord(e1, c.stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    *device_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c.steps_done += nsteps;
+    return sync_status(x);
+}
+
+int smd_get_observables(smd_ctx *x, smd_observables *out) {
+    if (!x || !out) return SMD_ERR_ARG;
+    Ctx &c = x->c;
+    CK(cudaMemcpyAsync(out, c.obs, sizeof(smd_observables), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return SMD_OK;
+}
+
+int smd_set_series_capacity(smd_ctx *x, int cap) {
+    if (!x || cap < 0) return SMD_ERR_ARG;
+    Ctx &c = x->c;
+    if (c.series) { cudaFree(c.series); c.series = nullptr; }
+    c.series_cap = cap;
+    if (cap > 0) {
+        CK(cudaMalloc(&c.series, (size_t)cap * 5 * sizeof(double)));
+        CK(cudaMemset(c.series, 0, (size_t)cap * 5 * sizeof(double)));
+    }
+    c.graph_dirty = 1;
+    return SMD_OK;
+}
+
+int smd_get_series(smd_ctx *x, double *out, int cap, int *count) {
+    if (!x || !out || !count) return SMD_ERR_ARG;
+    Ctx &c = x->c;
+    smd_observables o;
+    int r = smd_get_observables(x, &o);
+    if (r) return r;
+    long long steps = o.step;
+    int have = (int)std::min<long long>(steps, c.series_cap);
+    have = std::min(have, cap);
+    std::vector<double> all((size_t)c.series_cap * 5);
+    if (c.series_cap) CK(cudaMemcpy(all.data(), c.series, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    // oldest first
+    for (int k = 0; k < have; k++) {
+        long long stepno = steps - have + k;  // 0-based step index
+        long long slot = stepno % c.series_cap;
+        for (int q = 0; q < 5; q++) out[5 * k + q] = all[slot * 5 + q];
+    }
+    *count = have;
+    return SMD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,106 @@
+// Shared device-side definitions of the SwinMD B200 force/integration path.
+//
+// Data layout in HBM (one system, N sites, M molecules):
+//   pos4   double4[N]  x, y, z (nm) and the scaled charge q*sqrt(ke)   FP64 master
+//   fixq   int4[N]     x, y, z as 32-bit fractions of the box edge and the
+//                      site type: the FP32 pair kernels take exact integer
+//                      minimum-image differences from it
+//   vel4   double4[N]  on-step velocity, w = 1/m
+//   vtm4   double4[N]  leap-frog half-step velocity v(t - dt/2), w = m
+//   disp4  double4[N]  displacement since the last pair-list build,
+//                      w = unwrapped-position offset bookkeeping (unused)
+//   frc    long long[3][N]  forces, 64-bit fixed point (FRC_SCALE units),
+//                      SoA so every kernel's owner-thread read-modify-write
+//                      is coalesced; integer adds make the total independent
+//                      of kernel and thread order
+//   acc    long long[ACC_COUNT]  energies and virial, 64-bit fixed point
+//   nbr    int[max_nbr][N] full (both directions) Verlet list, column-major
+//                      so a warp of consecutive sites reads one row coalesced
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace smd {
+
+// ---- fixed point -----------------------------------------------------------
+// Forces: 2^32 units per kJ/mol/nm (resolution 2.3e-10, range +-2.1e9).
+constexpr double FRC_SCALE = 4294967296.0;
+constexpr double FRC_INV = 1.0 / 4294967296.0;
+// Energies and virial terms: 2^28 units per kJ/mol (range +-3.4e10).
+constexpr double ACC_SCALE = 268435456.0;
+constexpr double ACC_INV = 1.0 / 268435456.0;
+
+__device__ __forceinline__ long long to_fix(double v, double scale) {
+    return __double2ll_rn(v * scale);
+}
+
+// ---- accumulator slots (acc[]) ---------------------------------------------
+enum AccSlot {
+    ACC_E_VDW = 0,      // LJ / Mie / BMH / buffered 14-7 pair energy
+    ACC_E_REAL = 1,     // Ewald real-space energy
+    ACC_E_LONG = 2,     // Ewald reciprocal energy
+    ACC_E_INTRA = 3,    // Ewald intramolecular correction
+    ACC_E_SURF = 4,     // surface-dipole correction
+    ACC_E_MP_REAL = 5,  // multipole real space
+    ACC_E_MP_LONG = 6,  // multipole reciprocal
+    ACC_E_POL = 7,      // induction energy
+    ACC_VIR = 8,        // 9 short-range virial components (XX XY XZ YX .. ZZ)
+    ACC_LVIR = 17,      // 9 long-range virial components
+    ACC_NPAIR = 26,     // pairs inside the short-range cutoff (both directions)
+    ACC_COUNT = 27
+};
+
+// ---- status word bits (ctx->status on device) --------------------------------
+enum StatusBits {
+    ST_LIST_OVERFLOW = 1,    // a site had more neighbours than the list holds
+    ST_NH_ITER = 2,          // Nose-Hoover implicit velocity iteration hit its cap
+    ST_SHAKE_ITER = 4,       // SHAKE did not converge within maxCount
+    ST_NAN = 8,              // non-finite force or position
+    ST_CELL_RANGE = 16,      // site outside the cell grid after clamping
+    ST_CG_ITER = 32,         // dipole solver did not converge
+    ST_SHAKE_GEOM = 64       // SHAKE geometric failure (reference LFIntegrator.cpp:1758)
+};
+
+struct Box {
+    double L[3];      // edges (nm)
+    double half[3];   // L/2
+    double inv[3];    // 1/L
+};
+
+// Minimum image as the reference's Ensemble::apply_pbc (src/Ensemble.h:319-334):
+// while-loops on [-L/2, L/2); positions stay within one box of each other, so
+// at most one correction per axis is ever taken.
+// The loops are capped: a non-finite coordinate leaves them after a few
+// passes instead of spinning (the integrator flags it as ST_NAN).
+__device__ __forceinline__ double pbc1(double d, double L, double h) {
+    for (int k = 0; k < 8 && d >= h; k++) d -= L;
+    for (int k = 0; k < 8 && d < -h; k++) d += L;
+    return d;
+}
+
+// Box fraction of a coordinate as an unsigned 32-bit fixed-point number;
+// the difference of two, read as a signed int, is the exact minimum image.
+__device__ __forceinline__ int frac32(double x, double invL) {
+    double f = x * invL;
+    f -= floor(f);
+    long long v = __double2ll_rn(f * 4294967296.0);
+    return (int)(unsigned int)(v & 0xffffffffLL);
+}
+
+// Warp helpers ---------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum over `width` consecutive lanes (power of two), result in every lane.
+template <int width, typename T>
+__device__ __forceinline__ T group_sum(T v) {
+#pragma unroll
+    for (int o = width / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, width);
+    return v;
+}
+
+}  // namespace smd

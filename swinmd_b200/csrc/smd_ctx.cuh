@@ -1,0 +1,112 @@
+// Host-side context of one simulated system and the launchers of its kernels.
+// The C-ABI in include/swinmd_b200.h hands callers an opaque pointer to this.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include "smd_common.cuh"
+#include "../../include/swinmd_b200.h"
+
+namespace smd {
+
+enum VdwKind { VDW_NONE = 0, VDW_LJ = 1, VDW_MIE = 2, VDW_BMH = 3 };
+
+// Per type pair parameters of the short-range pair term (ntypes^2 rows of 8).
+//   LJ : p0 sigma^2, p1 4 eps, p2 energy at the cutoff (shift), p3 unused
+//   MIE: p0 sigma, p1 Cn*eps, p2 n, p3 m
+//   BMH: p0 A, p1 1/rho, p2 C, p3 D
+struct CellGrid {
+    int use_cells;
+    int n[3];
+    int ncell;
+    double len[3], rlen[3], origin[3];
+};
+
+struct PairList {
+    int max_nbr = 0;
+    int *nbr = nullptr;      // [max_nbr][N]; bit 31 set = same molecule
+    int *nnbr = nullptr;     // [N]
+    int *cell_of = nullptr, *cell_slot = nullptr, *cell_count = nullptr;
+    int *cell_start = nullptr, *cell_atoms = nullptr;
+    int cell_cap = 0;
+    double rl2 = 0;          // (cutoff + cutBuff)^2
+    double drmax = 0;        // cutBuff^2 / 4
+};
+
+struct Recip {               // Ewald reciprocal space (k half-space, k^2 < kcut^2)
+    int nk = 0;
+    int *kn = nullptr;       // [3][nk] integer lattice indices
+    double *kcoef = nullptr; // [nk] 4 pi/V * exp(-k^2/4a^2)/k^2
+    long long *sk = nullptr; // [2][nk] structure factor, fixed point (SK_SCALE)
+    double *kvec = nullptr;  // [3][nk] k in 1/nm
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    // sizes
+    int n = 0, nmol = 0, ntypes = 0;
+    // host topology
+    std::vector<int> h_type, h_mol, h_mol_off, h_mol_atoms, h_excl_off, h_excl;
+    std::vector<double> h_mass, h_charge;
+    std::vector<double> h_type_charge;
+    double total_mass = 0;
+    // device topology
+    int *type = nullptr, *mol = nullptr, *mol_off = nullptr, *mol_atoms = nullptr;
+    int *excl_off = nullptr, *excl = nullptr;
+    double *mass = nullptr;
+    double *pair_par = nullptr;    // [ntypes*ntypes*4]
+    float *pair_par_f = nullptr;
+    double *type_q = nullptr;      // scaled charge per type
+    // state
+    double4 *pos4 = nullptr, *vel4 = nullptr, *vtm4 = nullptr, *disp4 = nullptr;
+    int4 *fixq = nullptr;
+    long long *frc = nullptr;      // [3][N]
+    long long *acc = nullptr;      // [ACC_COUNT]
+    double *scal = nullptr;        // integrator scalars (see smd_integrate.cu)
+    double *partials = nullptr;    // per-block reduction partials
+    unsigned int *ticket = nullptr;
+    unsigned int *status = nullptr;
+    int *flags = nullptr;          // [0] rebuild list, [1] list builds so far
+    smd_observables *obs = nullptr;  // observables of the last step, on device
+    double *series = nullptr;      // recorded per-step samples
+    int series_cap = 0;
+    // configuration
+    Box box{};
+    CellGrid grid{};
+    PairList pl;
+    Recip rc;
+    int precision = SMD_PREC_FP64;
+    int want_cells = 1;
+    int vdw = VDW_NONE;
+    double cutoff = 1.0, cut_buffer = 0.1;
+    double vdw_rc2 = 1.0, sw_rs2 = 0.0, sw_c1 = 0, sw_c2 = 0, sw_c3 = 0;
+    int switch_on = 0;
+    double e_lrc = 0, v_lrc = 0;
+    int ewald_on = 0;
+    double ew_alpha = 0, ew_kcut = 0, ew_rc2 = 0, e_self = 0;
+    int long_steps = 1;
+    smd_integrator_params ip{};
+    int integrator_ready = 0;
+    int tpp = 8;                    // threads per site in the pair kernel
+    int nb_blocks = 0;              // blocks of the integrate kernel
+    long long steps_done = 0;
+    int list_valid = 0;
+    // CUDA graph of one step
+    cudaGraphExec_t step_graph = nullptr;
+    int graph_dirty = 1;
+};
+
+// launchers (each enqueues on ctx.stream)
+void launch_fixq(Ctx &c);
+void launch_nlist(Ctx &c, bool force_rebuild);
+void launch_pair(Ctx &c);
+void launch_recip(Ctx &c);
+void launch_integrate(Ctx &c);
+void launch_start_velocities(Ctx &c);
+void launch_finalize_forces(Ctx &c, double *f_out_dev);
+int setup_recip(Ctx &c);
+
+}  // namespace smd

@@ -1,0 +1,244 @@
+// Verlet pair list on the GPU.
+//
+// Same pair set as CellManager::update_pair_list (src/utils/CellManager.cpp:
+// 216-314) and Ensemble::build_pairlist (src/Ensemble.cpp:492-525): all
+// unordered pairs (i, j) not in the exclusion table whose minimum-image FP64
+// distance squared, computed as the reference computes it, is below
+// (cutoff + cutBuff)^2.  Sites are binned with the reference's cell formula
+// (CellManager::find_cell, CellManager.h:75-102, clamping included), and the
+// 27-cell stencil around each site's cell is the symmetric closure of the
+// reference's own-cell + 13-cell half shell, so the list holds each pair in
+// both directions ("full list"): every site's forces are then summed by the
+// threads that own it, with no atomics.
+//
+// The list is rebuilt only when flags[0] is set (the integrate kernel raises
+// it when a displacement since the last build exceeds cutBuff/2,
+// LFIntegrator.cpp:307-341); every kernel here reads the flag and returns at
+// once otherwise, so the step can run as one fixed CUDA graph.
+#include "smd_ctx.cuh"
+
+namespace smd {
+
+__device__ __forceinline__ int ref_cell(const double4 &p, const CellGrid &g) {
+    int c[3];
+    const double pp[3] = {p.x, p.y, p.z};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        double delta = pp[d] - g.origin[d];
+        int x = (int)(delta * g.rlen[d]);
+        if (x >= g.n[d]) x = g.n[d] - 1;
+        else if (x < 0) x = 0;
+        c[d] = x;
+    }
+    return (c[2] * g.n[1] + c[1]) * g.n[0] + c[0];
+}
+
+__global__ void k_bin(int n, const double4 *__restrict__ pos4, CellGrid g, int *cell_of,
+                      int *cell_slot, int *cell_count, double4 *disp4, const int *flags) {
+    if (!flags[0]) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (g.use_cells) {
+        int c = ref_cell(pos4[i], g);
+        cell_of[i] = c;
+        cell_slot[i] = atomicAdd(&cell_count[c], 1);
+    }
+    disp4[i] = make_double4(0, 0, 0, 0);
+}
+
+// Exclusive scan of the cell counts in one block; zeroes the counts for the
+// next build.  ncell is small (a few thousand at most for one system).
+__global__ void k_scan(int ncell, int *cell_count, int *cell_start, const int *flags) {
+    if (!flags[0]) return;
+    __shared__ int carry;
+    __shared__ int warp_tot[32];
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < ncell; base += blockDim.x) {
+        int c = base + threadIdx.x;
+        int v = c < ncell ? cell_count[c] : 0;
+        int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        int x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_tot[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            int t = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            warp_tot[lane] = t;
+        }
+        __syncthreads();
+        int excl = x - v + (w > 0 ? warp_tot[w - 1] : 0) + carry;
+        if (c < ncell) {
+            cell_start[c] = excl;
+            cell_count[c] = 0;
+        }
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) cell_start[ncell] = carry;
+}
+
+__global__ void k_fill(int n, const int *cell_of, const int *cell_slot, const int *cell_start,
+                       int *cell_atoms, const int *flags) {
+    if (!flags[0]) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    cell_atoms[cell_start[cell_of[i]] + cell_slot[i]] = i;
+}
+
+// One warp per cell: order the cell's sites by index (rank sort), so the
+// list rows, and with them every per-thread partial sum, come out the same
+// on every run.
+__global__ void k_sort_cells(int ncell, const int *cell_start, int *cell_atoms, int *scratch,
+                             const int *flags) {
+    if (!flags[0]) return;
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (warp >= ncell) return;
+    int s = cell_start[warp], e = cell_start[warp + 1];
+    for (int k = s + lane; k < e; k += 32) scratch[k] = cell_atoms[k];
+    __syncwarp();
+    for (int k = s + lane; k < e; k += 32) {
+        int v = scratch[k], r = 0;
+        for (int q = s; q < e; q++) r += scratch[q] < v;
+        cell_atoms[s + r] = v;
+    }
+}
+
+struct BuildArgs {
+    int n, max_nbr;
+    const double4 *pos4;
+    const int *mol, *excl_off, *excl;
+    const int *cell_of, *cell_start, *cell_atoms;
+    CellGrid g;
+    Box box;
+    double rl2;
+    int *nbr, *nnbr;
+    unsigned int *status;
+    const int *flags;
+};
+
+// r^2 of the reference's pair test, without contraction into FMA
+// (x86-64 -O2 builds of the reference use separate multiply and add).
+__device__ __forceinline__ double ref_r2(const double4 &a, const double4 &b, const Box &bx,
+                                         bool pbc) {
+    double dx = __dsub_rn(b.x, a.x), dy = __dsub_rn(b.y, a.y), dz = __dsub_rn(b.z, a.z);
+    if (pbc) {
+        dx = pbc1(dx, bx.L[0], bx.half[0]);
+        dy = pbc1(dy, bx.L[1], bx.half[1]);
+        dz = pbc1(dz, bx.L[2], bx.half[2]);
+    }
+    return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+// One warp per site i; candidates are tested 32 at a time and appended in
+// candidate order (ballot + popc), so the row order is deterministic.
+__global__ void k_build(BuildArgs a) {
+    if (!a.flags[0]) return;
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (i >= a.n) return;
+    const double4 pi = a.pos4[i];
+    const int mi = a.mol[i];
+    const int e0 = a.excl_off[i], e1 = a.excl_off[i + 1];
+    int count = 0;
+    auto consider = [&](int j, bool pbc, bool valid) {
+        bool take = valid && j != i;
+        if (take) {
+            for (int e = e0; e < e1; e++)
+                if (a.excl[e] == j) { take = false; break; }
+        }
+        if (take) take = ref_r2(pi, a.pos4[j], a.box, pbc) < a.rl2;
+        unsigned m = __ballot_sync(0xffffffffu, take);
+        if (take) {
+            int slot = count + __popc(m & ((1u << lane) - 1));
+            int v = j | (a.mol[j] == mi ? (int)0x80000000 : 0);
+            if (slot < a.max_nbr) a.nbr[(size_t)slot * a.n + i] = v;
+        }
+        count += __popc(m);
+    };
+    if (a.g.use_cells) {
+        int c = a.cell_of[i];
+        int cx = c % a.g.n[0], cy = (c / a.g.n[0]) % a.g.n[1], cz = c / (a.g.n[0] * a.g.n[1]);
+        for (int dz = -1; dz <= 1; dz++) {
+            int z = cz + dz; z = z < 0 ? z + a.g.n[2] : (z >= a.g.n[2] ? z - a.g.n[2] : z);
+            for (int dy = -1; dy <= 1; dy++) {
+                int y = cy + dy; y = y < 0 ? y + a.g.n[1] : (y >= a.g.n[1] ? y - a.g.n[1] : y);
+                for (int dx = -1; dx <= 1; dx++) {
+                    int x = cx + dx; x = x < 0 ? x + a.g.n[0] : (x >= a.g.n[0] ? x - a.g.n[0] : x);
+                    int nc = (z * a.g.n[1] + y) * a.g.n[0] + x;
+                    // same-cell pairs are tested without minimum image, as the
+                    // reference does (CellManager.cpp:246-262)
+                    bool pbc = nc != c;
+                    int s = a.cell_start[nc], e = a.cell_start[nc + 1];
+                    for (int k = s; k < e; k += 32) {
+                        int kk = k + lane;
+                        consider(kk < e ? a.cell_atoms[kk] : -1, pbc, kk < e);
+                    }
+                }
+            }
+        }
+    } else {
+        for (int k = 0; k < a.n; k += 32) {
+            int j = k + lane;
+            consider(j < a.n ? j : -1, true, j < a.n);
+        }
+    }
+    if (lane == 0) {
+        if (count > a.max_nbr) {
+            atomicOr(a.status, ST_LIST_OVERFLOW);
+            count = a.max_nbr;
+        }
+        a.nnbr[i] = count;
+    }
+}
+
+__global__ void k_list_done(int *flags) {
+    if (flags[0]) {
+        flags[1] += 1;
+        flags[0] = 0;
+    }
+}
+
+void launch_nlist(Ctx &c, bool force_rebuild) {
+    if (force_rebuild) {
+        int one = 1;
+        cudaMemcpyAsync(c.flags, &one, sizeof(int), cudaMemcpyHostToDevice, c.stream);
+    }
+    const int T = 256;
+    int nb = (c.n + T - 1) / T;
+    if (c.grid.use_cells) {
+        k_bin<<<nb, T, 0, c.stream>>>(c.n, c.pos4, c.grid, c.pl.cell_of, c.pl.cell_slot,
+                                      c.pl.cell_count, c.disp4, c.flags);
+        k_scan<<<1, 1024, 0, c.stream>>>(c.grid.ncell, c.pl.cell_count, c.pl.cell_start, c.flags);
+        k_fill<<<nb, T, 0, c.stream>>>(c.n, c.pl.cell_of, c.pl.cell_slot, c.pl.cell_start,
+                                       c.pl.cell_atoms, c.flags);
+        int nw = (c.grid.ncell * 32 + T - 1) / T;
+        k_sort_cells<<<nw, T, 0, c.stream>>>(c.grid.ncell, c.pl.cell_start, c.pl.cell_atoms,
+                                             c.pl.cell_slot /* reused as scratch after fill */,
+                                             c.flags);
+    } else {
+        k_bin<<<nb, T, 0, c.stream>>>(c.n, c.pos4, c.grid, c.pl.cell_of, c.pl.cell_slot,
+                                      c.pl.cell_count, c.disp4, c.flags);
+    }
+    BuildArgs a;
+    a.n = c.n; a.max_nbr = c.pl.max_nbr; a.pos4 = c.pos4; a.mol = c.mol;
+    a.excl_off = c.excl_off; a.excl = c.excl; a.cell_of = c.pl.cell_of;
+    a.cell_start = c.pl.cell_start; a.cell_atoms = c.pl.cell_atoms; a.g = c.grid; a.box = c.box;
+    a.rl2 = c.pl.rl2; a.nbr = c.pl.nbr; a.nnbr = c.pl.nnbr; a.status = c.status; a.flags = c.flags;
+    int nbw = (c.n * 32 + T - 1) / T;
+    k_build<<<nbw, T, 0, c.stream>>>(a);
+    k_list_done<<<1, 1, 0, c.stream>>>(c.flags);
+}
+
+}  // namespace smd

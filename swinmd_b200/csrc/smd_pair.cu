@@ -1,0 +1,332 @@
+// Short-range pair kernel: LJ / Mie n-m / Born-Mayer-Huggins fused with the
+// Ewald real-space term, over the full Verlet list.
+//
+// Reference terms (per pair inside the cutoff, r_ij = r_j - r_i, f_i += f_ij):
+//   LJ   LJForce::compute (src/forces/LJForce.cpp:92-229): skips same-molecule
+//        pairs, U = 4eps (sr12 - sr6) minus U(rc) when switchOn, force unshifted,
+//        cutoff test on r*r <= rc^2 with r = |r_ij|.
+//   MIE  MieForce::compute (src/forces/MieForce.cpp:89-196): Cn eps (s^n - s^m),
+//        5th-order switch between switchDist and the cutoff.
+//   BMH  A exp(-r/rho) - C r^-6 - D r^-8 with the same switch (no reference
+//        code for this form; structure of BuckinghamForce.cpp:150-182).
+//   real EwaldForce::real_term (src/forces/EwaldForce.cpp:296-527):
+//        q_i q_j erfc(a r)/r for r^2 < realCut^2, all listed pairs.
+//
+// Layout: TPP consecutive threads own one site i and split its list row;
+// their partial forces are combined with shuffles in a fixed tree, so the
+// result does not depend on scheduling.  The list holds each pair twice, so
+// the energy and virial sums are halved.  Energies and the virial go to
+// 64-bit fixed-point accumulators (one atomic per block and slot); forces
+// are written as fixed point by the owner threads.
+//
+// Two arithmetic paths:
+//   double: positions from pos4 (FP64), minimum image as Ensemble::apply_pbc.
+//   float : positions from fixq (32-bit box fractions); the minimum-image
+//           displacement is an exact integer difference and r^2 an exact
+//           64-bit integer sum (cubic box), so the only roundings are the
+//           FP32 pair arithmetic itself.
+#include "smd_ctx.cuh"
+
+namespace smd {
+
+struct PairArgs {
+    int n, max_nbr, ntypes;
+    const int *nbr, *nnbr;
+    const double4 *pos4;
+    const int4 *fixq;
+    Box box;
+    int cubic;
+    double r2scale;     // (L/2^32)^2, cubic boxes
+    float dscale[3];    // L/2^32 per axis
+    const double *par;  // [ntypes^2][4]
+    const double *type_q;
+    double vdw_rc2;
+    int switch_on;
+    double sw_rs2, sw_c1, sw_c2, sw_c3;
+    double alpha, alpha2, alpha2pi, ew_rc2;
+    long long *frc;
+    long long *acc;
+};
+
+constexpr int PAIR_BLOCK = 256;
+constexpr int MAX_TYPES = 8;
+
+template <typename R, int VDW>
+__device__ __forceinline__ void vdw_pair(R r2, R &e, R &fs, const R *p, const PairArgs &a,
+                                         bool same) {
+    // fs: scalar with f_ij = -fs * r_ij
+    e = R(0);
+    fs = R(0);
+    if (VDW == VDW_NONE || same) return;
+    if (VDW == VDW_LJ) {
+        R r = sqrt(r2);
+        R rr = r * r;
+        if (rr <= R(a.vdw_rc2)) {
+            R r_1 = R(1) / r;
+            R rij_2 = r_1 * r_1;
+            R sr2 = p[0] * rij_2;
+            R sr6 = sr2 * sr2 * sr2;
+            R sr12 = sr6 * sr6;
+            e = p[1] * (sr12 - sr6);
+            fs = (sr12 + sr12 - sr6) * R(6) * p[1] * rij_2;
+            if (a.switch_on) e -= p[2];
+        }
+    } else {
+        R r = sqrt(r2);
+        R rr = r * r;
+        if (rr <= R(a.vdw_rc2)) {
+            R r_1 = R(1) / r;
+            R rij_2 = r_1 * r_1;
+            if (VDW == VDW_MIE) {
+                R s = p[0] * r_1;
+                R srn = pow(s, p[2]);
+                R srm = pow(s, p[3]);
+                e = p[1] * (srn - srm);
+                fs = p[1] * (p[2] * srn - p[3] * srm) * rij_2;
+            } else {  // BMH
+                R ex = p[0] * exp(-r * p[1]);
+                R r6 = rij_2 * rij_2 * rij_2;
+                R r8 = r6 * rij_2;
+                e = ex - p[2] * r6 - p[3] * r8;
+                fs = ex * p[1] * r_1 - R(6) * p[2] * r8 - R(8) * p[3] * r8 * rij_2;
+            }
+            if (a.switch_on && rr > R(a.sw_rs2)) {
+                R c = R(a.vdw_rc2) - rr;
+                R c4 = c * (R(2) * rr + R(a.sw_c2));
+                R sv = c * c4 * R(a.sw_c1);
+                R dsv = R(a.sw_c3) * (c * c - c4);
+                fs = fs * sv - e * dsv;
+                e *= sv;
+            }
+        }
+    }
+}
+
+// FP32 LJ with the rounding of r^2 and of 1/r^2 corrected to first order:
+// r2f is r^2 rounded to float, dr2 = (r^2 - r2f)/r2f from the exact integer
+// r^2.  With ir2 = 1/r2f (rounded) the true 1/r^2 = ir2 (1 + eps) with
+// eps = (1 - r2f ir2) - dr2 (the first term exact by FMA); the r^-14 and
+// r^-8 force terms and the r^-12 / r^-6 energy terms then take the factors
+// (1 + 7 eps), (1 + 4 eps), (1 + 6 eps), (1 + 3 eps).  Without it the
+// seven-fold amplification of the two roundings dominates the FP32 error.
+__device__ __forceinline__ void lj_pair_f(float r2f, float dr2, float &e, float &fs,
+                                          const float *p, const PairArgs &a, bool same) {
+    e = 0.f;
+    fs = 0.f;
+    if (same || !(r2f <= (float)a.vdw_rc2)) return;
+    const float ir2 = __frcp_rn(r2f);
+    const float eps = fmaf(-r2f, ir2, 1.0f) - dr2;
+    const float sr2 = p[0] * ir2;
+    const float sr6 = sr2 * sr2 * sr2;
+    const float sr12 = sr6 * sr6;
+    const float t1 = 12.f * p[1] * sr12 * ir2;
+    const float t2 = 6.f * p[1] * sr6 * ir2;
+    fs = (t1 - t2) + eps * (7.f * t1 - 4.f * t2);
+    e = p[1] * (sr12 - sr6) + eps * (p[1] * (6.f * sr12 - 3.f * sr6));
+    if (a.switch_on) e -= p[2];
+}
+
+template <typename R, int VDW, bool EWALD, int TPP>
+__global__ void __launch_bounds__(PAIR_BLOCK) k_pair(PairArgs a) {
+    __shared__ R s_par[MAX_TYPES * MAX_TYPES * 4];
+    __shared__ R s_q[MAX_TYPES];
+    __shared__ double s_red[PAIR_BLOCK / 32][11];
+    const int nt2 = a.ntypes * a.ntypes;
+    for (int k = threadIdx.x; k < nt2 * 4; k += blockDim.x) s_par[k] = R(a.par[k]);
+    for (int k = threadIdx.x; k < a.ntypes; k += blockDim.x) s_q[k] = R(a.type_q[k]);
+    __syncthreads();
+
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gt / TPP;
+    const int t = gt % TPP;
+    double fx = 0, fy = 0, fz = 0;
+    R evdw = 0, ereal = 0;
+    int npair = 0;
+    R vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
+    if (i < a.n) {
+        const int cnt = a.nnbr[i];
+        double4 pi64;
+        int4 pif;
+        int ti;
+        if (sizeof(R) == 8) {
+            pi64 = a.pos4[i];
+            ti = (int)pi64.w;
+        } else {
+            pif = a.fixq[i];
+            ti = pif.w;
+        }
+        const R qi = s_q[ti];
+        for (int k = t; k < cnt; k += TPP) {
+            const int raw = a.nbr[(size_t)k * a.n + i];
+            const int j = raw & 0x7fffffff;
+            const bool same = raw < 0;
+            R dx, dy, dz, r2;
+            float r2c = 0.f;
+            int tj;
+            if (sizeof(R) == 8) {
+                const double4 pj = a.pos4[j];
+                dx = pbc1(pj.x - pi64.x, a.box.L[0], a.box.half[0]);
+                dy = pbc1(pj.y - pi64.y, a.box.L[1], a.box.half[1]);
+                dz = pbc1(pj.z - pi64.z, a.box.L[2], a.box.half[2]);
+                r2 = dx * dx + dy * dy + dz * dz;
+                tj = (int)pj.w;
+            } else {
+                const int4 pj = a.fixq[j];
+                const int ix = pj.x - pif.x, iy = pj.y - pif.y, iz = pj.z - pif.z;
+                dx = R(ix) * R(a.dscale[0]);
+                dy = R(iy) * R(a.dscale[1]);
+                dz = R(iz) * R(a.dscale[2]);
+                float dr2 = 0.f;
+                if (a.cubic) {
+                    unsigned long long s2 = (unsigned long long)((long long)ix * ix) +
+                                            (unsigned long long)((long long)iy * iy) +
+                                            (unsigned long long)((long long)iz * iz);
+                    const double r2d = (double)s2 * a.r2scale;
+                    r2 = R(r2d);
+                    dr2 = (float)((r2d - (double)r2) / r2d);
+                } else {
+                    r2 = dx * dx + dy * dy + dz * dz;
+                }
+                tj = pj.w;
+                r2c = dr2;
+            }
+            R e, fs;
+            if (sizeof(R) == 4 && VDW == VDW_LJ)
+                lj_pair_f((float)r2, r2c, *(float *)&e, *(float *)&fs,
+                          (const float *)&s_par[(ti * a.ntypes + tj) * 4], a, same);
+            else
+                vdw_pair<R, VDW>(r2, e, fs, &s_par[(ti * a.ntypes + tj) * 4], a, same);
+            evdw += e;
+            npair += (r2 <= R(a.vdw_rc2) || (EWALD && r2 < R(a.ew_rc2))) ? 1 : 0;
+            if (EWALD) {
+                if (r2 < R(a.ew_rc2)) {
+                    const R qij = qi * s_q[tj];
+                    const R r = sqrt(r2);
+                    const R ee = erfc(R(a.alpha) * r) / r;
+                    const R ff = (ee + R(a.alpha2pi) * exp(-R(a.alpha2) * r2)) / r2;
+                    ereal += qij * ee;
+                    fs += qij * ff;
+                }
+            }
+            const R fijx = -fs * dx, fijy = -fs * dy, fijz = -fs * dz;
+            fx += (double)fijx;
+            fy += (double)fijy;
+            fz += (double)fijz;
+            vxx += fijx * dx; vxy += fijy * dx; vxz += fijz * dx;
+            vyy += fijy * dy; vyz += fijz * dy; vzz += fijz * dz;
+        }
+    }
+    fx = group_sum<TPP>(fx);
+    fy = group_sum<TPP>(fy);
+    fz = group_sum<TPP>(fz);
+    if (i < a.n && t == 0) {
+        a.frc[i] = to_fix(fx, FRC_SCALE);
+        a.frc[a.n + i] = to_fix(fy, FRC_SCALE);
+        a.frc[2 * a.n + i] = to_fix(fz, FRC_SCALE);
+    }
+    // energies and virial: warp, then block, then one fixed-point atomic each
+    double v[8] = {(double)evdw, (double)ereal, (double)vxx, (double)vxy,
+                   (double)vxz,  (double)vyy,   (double)vyz, (double)vzz};
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    {
+        int np = warp_sum(npair);
+        if (lane == 0 && np) atomicAdd((unsigned long long *)&a.acc[ACC_NPAIR], (unsigned long long)np);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        double s = warp_sum(v[q]);
+        if (lane == 0) s_red[w][q] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        double s = 0;
+        for (int q = 0; q < PAIR_BLOCK / 32; q++) s += s_red[q][threadIdx.x];
+        s *= 0.5;  // each pair appears twice in the full list
+        // local virial convention of the reference (sum f_ij r_ij) has the
+        // opposite sign of Ensemble::virial; store the Ensemble sign.
+        int slot;
+        switch (threadIdx.x) {
+            case 0: slot = ACC_E_VDW; break;
+            case 1: slot = ACC_E_REAL; break;
+            case 2: slot = ACC_VIR + 0; break;
+            case 3: slot = ACC_VIR + 1; break;
+            case 4: slot = ACC_VIR + 2; break;
+            case 5: slot = ACC_VIR + 4; break;
+            case 6: slot = ACC_VIR + 5; break;
+            default: slot = ACC_VIR + 8; break;
+        }
+        if (threadIdx.x >= 2) s = -s;
+        if (s != 0.0) atomicAdd((unsigned long long *)&a.acc[slot],
+                                (unsigned long long)to_fix(s, ACC_SCALE));
+        // the virial of central pair forces is symmetric
+        if (threadIdx.x == 3) atomicAdd((unsigned long long *)&a.acc[ACC_VIR + 3], (unsigned long long)to_fix(s, ACC_SCALE));
+        if (threadIdx.x == 4) atomicAdd((unsigned long long *)&a.acc[ACC_VIR + 6], (unsigned long long)to_fix(s, ACC_SCALE));
+        if (threadIdx.x == 6) atomicAdd((unsigned long long *)&a.acc[ACC_VIR + 7], (unsigned long long)to_fix(s, ACC_SCALE));
+    }
+}
+
+template <typename R, int VDW, bool EWALD>
+static void dispatch_tpp(Ctx &c, const PairArgs &a) {
+    int tpp = c.tpp;
+    long long threads = (long long)c.n * tpp;
+    int nb = (int)((threads + PAIR_BLOCK - 1) / PAIR_BLOCK);
+    switch (tpp) {
+        case 1: k_pair<R, VDW, EWALD, 1><<<nb, PAIR_BLOCK, 0, c.stream>>>(a); break;
+        case 2: k_pair<R, VDW, EWALD, 2><<<nb, PAIR_BLOCK, 0, c.stream>>>(a); break;
+        case 4: k_pair<R, VDW, EWALD, 4><<<nb, PAIR_BLOCK, 0, c.stream>>>(a); break;
+        case 8: k_pair<R, VDW, EWALD, 8><<<nb, PAIR_BLOCK, 0, c.stream>>>(a); break;
+        case 16: k_pair<R, VDW, EWALD, 16><<<nb, PAIR_BLOCK, 0, c.stream>>>(a); break;
+        default: k_pair<R, VDW, EWALD, 32><<<nb, PAIR_BLOCK, 0, c.stream>>>(a); break;
+    }
+}
+
+template <typename R, bool EWALD>
+static void dispatch_vdw(Ctx &c, const PairArgs &a) {
+    switch (c.vdw) {
+        case VDW_LJ: dispatch_tpp<R, VDW_LJ, EWALD>(c, a); break;
+        case VDW_MIE: dispatch_tpp<R, VDW_MIE, EWALD>(c, a); break;
+        case VDW_BMH: dispatch_tpp<R, VDW_BMH, EWALD>(c, a); break;
+        default: dispatch_tpp<R, VDW_NONE, EWALD>(c, a); break;
+    }
+}
+
+// Converts FP64 master positions to box fractions for the FP32 path.
+__global__ void k_fixq(int n, const double4 *pos4, int4 *fixq, Box b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 p = pos4[i];
+    fixq[i] = make_int4(frac32(p.x, b.inv[0]), frac32(p.y, b.inv[1]), frac32(p.z, b.inv[2]),
+                        (int)p.w);
+}
+
+void launch_fixq(Ctx &c) {
+    k_fixq<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.pos4, c.fixq, c.box);
+}
+
+void launch_pair(Ctx &c) {
+    PairArgs a;
+    a.n = c.n; a.max_nbr = c.pl.max_nbr; a.ntypes = c.ntypes;
+    a.nbr = c.pl.nbr; a.nnbr = c.pl.nnbr; a.pos4 = c.pos4; a.fixq = c.fixq;
+    a.box = c.box;
+    a.cubic = (c.box.L[0] == c.box.L[1] && c.box.L[1] == c.box.L[2]);
+    double s = c.box.L[0] / 4294967296.0;
+    a.r2scale = s * s;
+    for (int d = 0; d < 3; d++) a.dscale[d] = (float)(c.box.L[d] / 4294967296.0);
+    a.par = c.pair_par; a.type_q = c.type_q;
+    a.vdw_rc2 = c.vdw_rc2; a.switch_on = c.switch_on;
+    a.sw_rs2 = c.sw_rs2; a.sw_c1 = c.sw_c1; a.sw_c2 = c.sw_c2; a.sw_c3 = c.sw_c3;
+    a.alpha = c.ew_alpha; a.alpha2 = c.ew_alpha * c.ew_alpha;
+    a.alpha2pi = 2.0 * c.ew_alpha / 1.7724538509055160273;
+    a.ew_rc2 = c.ew_rc2;
+    a.frc = c.frc; a.acc = c.acc;
+    if (c.precision == SMD_PREC_MIXED) {
+        launch_fixq(c);
+        if (c.ewald_on) dispatch_vdw<float, true>(c, a);
+        else dispatch_vdw<float, false>(c, a);
+    } else {
+        if (c.ewald_on) dispatch_vdw<double, true>(c, a);
+        else dispatch_vdw<double, false>(c, a);
+    }
+}
+
+}  // namespace smd

@@ -1,0 +1,356 @@
+"""Host side of the B200 path, mirroring the reference's plugin interface.
+
+``GpuEnsemble`` plays the part of SwinMD's ``Ensemble`` (src/Ensemble.h):
+it owns one system's topology, box, pair list and state on the GPU.  The
+force classes mirror ``Force`` subclasses (src/Force.h:30-72): ``compute()``
+evaluates the term and leaves its energy and virial in the object, and
+``compute_long()`` does the reciprocal part where the reference has one.
+``LFIntegrator`` mirrors the leap-frog integrator's ``start()``/``run(n)``
+(src/integrators/LFIntegrator.cpp).  Every call goes through the C ABI of
+``libswinmd_b200.so``; nothing here computes forces or moves atoms.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from typing import Dict, Optional
+
+import numpy as np
+
+from . import _lib as L
+from .systems import BOLTZMAN, System, reference_box
+
+
+# ---------------------------------------------------------------------------
+# reference set-up arithmetic (host, once per run)
+# ---------------------------------------------------------------------------
+
+class _RefLCG:
+    """``Ensemble::drand`` (src/Ensemble.cpp:1851-1864): 20-bit LCG whose state
+    is a function-level static seeded once from the config seed."""
+
+    def __init__(self, seed: float):
+        self.s = int(seed) & 0xFFFFFFFF
+
+    def drand(self) -> float:
+        self.s = (self.s * 1029 + 221591) % 1048576
+        return float(self.s) / 1048576
+
+    def gauss(self) -> float:
+        """``Ensemble::gauss`` (src/Ensemble.cpp:1826-1849): sum of 12 uniforms
+        mapped through an odd polynomial (Allen & Tildesley's GAUSS)."""
+        a1, a3, a5, a7, a9 = 3.949846138, 0.252408784, 0.076542912, 0.008355968, 0.029899776
+        s = 0.0
+        for _ in range(12):
+            s += self.drand()
+        r = (s - 6.0) / 4.0
+        r2 = r * r
+        return ((((a9 * r2 + a7) * r2 + a5) * r2 + a3) * r2 + a1) * r
+
+
+def init_velocity(s: System) -> np.ndarray:
+    """``Ensemble::init_velocity`` (src/Ensemble.cpp:1752-1823): Gaussian
+    momenta from the seeded LCG, zero total momentum, scaled to T."""
+    c = s.config
+    rng = _RefLCG(c.seed)
+    nb, na = len(s.bonds), len(s.angles)
+    if c.atom_thermo:
+        n = s.n_atoms
+        ndf = 3 * n - nb - na - 3 if c.constraint else 3 * n - 3
+        mass = s.masses()
+    else:
+        n = s.n_mols
+        ndf = 3 * n - 3
+        mass = np.zeros(n)
+        np.add.at(mass, s.mol_id, s.masses())
+    p = np.zeros((n, 3))
+    for i in range(n):
+        p[i, 0] = rng.gauss()
+        p[i, 1] = rng.gauss()
+        p[i, 2] = rng.gauss()
+    avg = [0.0, 0.0, 0.0]
+    for i in range(n):
+        for d in range(3):
+            avg[d] += p[i, d]
+    avg = [a / n for a in avg]
+    tavg = 0.0
+    for i in range(n):
+        for d in range(3):
+            p[i, d] -= avg[d]
+        x, y, z = p[i]
+        tavg += (x * x + y * y + z * z) / mass[i]
+    tavg /= (ndf * BOLTZMAN)
+    scale = math.sqrt(c.temperature / tavg)
+    if c.atom_thermo:
+        mom = scale * p
+        return mom / mass[:, None]
+    v = np.zeros((s.n_atoms, 3))
+    for m in range(n):
+        vm = (scale * p[m]) / mass[m]
+        v[s.mol_id == m] = vm
+    return v
+
+
+def lj_long_range_correction(s: System) -> tuple:
+    """``LJForce::long_range_correct`` (src/forces/LJForce.cpp:260-337):
+    energy and virial corrections of the dispersion tail."""
+    s2, e4 = s.lj_table()
+    nt = len(s.atom_types)
+    counts = np.bincount(s.atom_type, minlength=nt)
+    rc = s.config.cutoff
+    vol = reference_box(s) ** 3
+    csix, npair, nexcl = 0.0, 0, 0
+    for i in range(nt):
+        for j in range(i, nt):
+            sig6 = s2[i, j] ** 3
+            nij = int(counts[i] * counts[j]) if i != j else int(counts[i] * (counts[i] - 1) * 0.5)
+            csix += nij * e4[i, j] * sig6
+            npair += nij
+    excl = s.exclusion_table()
+    for i in range(s.n_atoms):
+        for j in excl[i]:
+            if j >= i:
+                sig6 = s2[s.atom_type[i], s.atom_type[j]] ** 3
+                csix -= e4[s.atom_type[i], s.atom_type[j]] * sig6
+                nexcl += 1
+    csix = 0.0 if npair - nexcl <= 0 else csix / (npair - nexcl)
+    n = s.n_atoms
+    e_lrc = -2.0 * math.pi * n * n * (1.0 / vol) * csix / (3.0 * rc ** 3)
+    return e_lrc, -2.0 * e_lrc
+
+
+# ---------------------------------------------------------------------------
+# the GPU system
+# ---------------------------------------------------------------------------
+
+class GpuEnsemble:
+    """One system on one GPU behind the C ABI (the role of ``Ensemble``)."""
+
+    def __init__(self, system: System, precision: str = "fp64", device: int = 0,
+                 threads_per_site: int = 0, velocities: Optional[np.ndarray] = None,
+                 box: Optional[float] = None):
+        self.lib = L.load()
+        self.system = s = system
+        self.n = s.n_atoms
+        ctx = ctypes.c_void_p()
+        code = self.lib.smd_create(device, ctypes.byref(ctx))
+        if code != L.SMD_OK:
+            raise L.SmdError(code, "smd_create failed (no CUDA device?)")
+        self.ctx = ctx
+        c = s.config
+        self.box = box if box is not None else reference_box(s)
+        types = np.ascontiguousarray(s.atom_type, np.int32)
+        mol = np.ascontiguousarray(s.mol_id, np.int32)
+        self.mass = s.masses()
+        self.charge = s.scaled_charges()
+        self._chk(self.lib.smd_set_topology(ctx, self.n, len(s.atom_types), L.iptr(types),
+                                            L.iptr(mol), L.dptr(self.mass), L.dptr(self.charge)))
+        excl = s.exclusion_table()
+        off = np.zeros(self.n + 1, np.int32)
+        off[1:] = np.cumsum([len(e) for e in excl])
+        flat = np.array([j for e in excl for j in e] or [0], np.int32)
+        self._chk(self.lib.smd_set_exclusions(ctx, L.iptr(off), L.iptr(flat)))
+        self._chk(self.lib.smd_set_box(ctx, self.box, self.box, self.box))
+        self._chk(self.lib.smd_set_pairlist(ctx, c.cutoff, c.cut_buffer, int(c.use_cell_list)))
+        self._setup_vdw()
+        if c.compute_ewald:
+            self._chk(self.lib.smd_set_ewald(ctx, c.alpha, c.k_cutoff, c.cutoff))
+        self.set_precision(precision)
+        if threads_per_site:
+            self._chk(self.lib.smd_set_tuning(ctx, threads_per_site))
+        self.upload_positions(np.asarray(s.pos, np.float64))
+        v = velocities if velocities is not None else init_velocity(s)
+        self.upload_velocities(v)
+
+    # -- plumbing -------------------------------------------------------
+    def _chk(self, code):
+        L.check(self.ctx, code)
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.smd_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_precision(self, precision: str):
+        self.precision = precision
+        self._chk(self.lib.smd_set_precision(self.ctx, L.PREC_MIXED if precision == "mixed" else L.PREC_FP64))
+
+    def _setup_vdw(self):
+        s, c = self.system, self.system.config
+        nt = len(s.atom_types)
+        par = np.zeros((nt, nt, 4))
+        kind = L.VDW_NONE
+        e_lrc = v_lrc = 0.0
+        if s.bmh is not None:
+            kind = L.VDW_BMH
+            par[..., 0] = s.bmh["A"]
+            par[..., 1] = 1.0 / s.bmh["rho"]
+            par[..., 2] = s.bmh["C"]
+            par[..., 3] = s.bmh["D"]
+        elif c.compute_mie:
+            # MieForce: sigma = sqrt(sigma^2), eps = 4eps/4, Cn (MieForce.cpp:26-35,122-124)
+            kind = L.VDW_MIE
+            s2, e4 = s.lj_table()
+            n_, m_ = float(c.n_mie), float(c.m_mie)
+            cn = (n_ / (n_ - m_)) * math.pow(n_ / m_, m_ / (n_ - m_))
+            par[..., 0] = np.sqrt(s2)
+            par[..., 1] = cn * 0.25 * e4
+            par[..., 2] = n_
+            par[..., 3] = m_
+        elif not c.compute_buff:
+            kind = L.VDW_LJ
+            s2, e4 = s.lj_table()
+            par[..., 0] = s2
+            par[..., 1] = e4
+            if c.long_correct:
+                e_lrc, v_lrc = lj_long_range_correction(s)
+        self.vdw_kind = kind
+        p = np.ascontiguousarray(par.reshape(-1))
+        self._chk(self.lib.smd_set_vdw(self.ctx, kind, L.dptr(p), int(c.switch_on),
+                                       c.switch_dist ** 2, e_lrc, v_lrc))
+
+    # -- state ----------------------------------------------------------
+    def upload_positions(self, pos: np.ndarray):
+        p = np.ascontiguousarray(pos, np.float64).reshape(-1)
+        self._chk(self.lib.smd_upload_positions(self.ctx, L.dptr(p)))
+
+    def upload_velocities(self, vel: np.ndarray, vtminus: Optional[np.ndarray] = None):
+        v = np.ascontiguousarray(vel, np.float64).reshape(-1)
+        vm = None if vtminus is None else np.ascontiguousarray(vtminus, np.float64).reshape(-1)
+        self._chk(self.lib.smd_upload_velocities(self.ctx, L.dptr(v), L.dptr(vm)))
+
+    def state(self) -> Dict[str, np.ndarray]:
+        pos = np.zeros(3 * self.n); vel = np.zeros(3 * self.n); vtm = np.zeros(3 * self.n)
+        self._chk(self.lib.smd_download_state(self.ctx, L.dptr(pos), L.dptr(vel), L.dptr(vtm)))
+        return {"pos": pos.reshape(-1, 3), "vel": vel.reshape(-1, 3), "vtminus": vtm.reshape(-1, 3)}
+
+    # -- forces ---------------------------------------------------------
+    def compute_forces(self, terms: int = L.TERM_ALL):
+        f = np.zeros(3 * self.n)
+        e = np.zeros(L.E_COUNT)
+        w = np.zeros(9)
+        self._chk(self.lib.smd_compute_forces(self.ctx, terms, L.dptr(f), L.dptr(e), L.dptr(w)))
+        return f.reshape(-1, 3), e, w
+
+    def pairs(self) -> np.ndarray:
+        cnt = ctypes.c_int64()
+        self._chk(self.lib.smd_get_pairs(self.ctx, None, 0, ctypes.byref(cnt)))
+        out = np.zeros(2 * cnt.value, np.int32)
+        self._chk(self.lib.smd_get_pairs(self.ctx, L.iptr(out), cnt.value, ctypes.byref(cnt)))
+        return out.reshape(-1, 2)
+
+    def ewald_nk(self) -> int:
+        nk = ctypes.c_int()
+        self._chk(self.lib.smd_ewald_nk(self.ctx, ctypes.byref(nk)))
+        return nk.value
+
+
+# ---------------------------------------------------------------------------
+# Force plugin mirrors (Force::compute / compute_long)
+# ---------------------------------------------------------------------------
+
+class GpuForce:
+    """Base of the force mirrors: after ``compute()`` the object holds
+    ``force`` (this term's contribution to Atom::force), ``energy`` and
+    ``virial`` (its contribution to Ensemble::virial, row-major 3x3)."""
+    terms = 0
+    energy_index = L.E_VDW
+
+    def __init__(self, ensemble: GpuEnsemble):
+        self.ens = ensemble
+        self.force = None
+        self.energy = 0.0
+        self.energies = None
+        self.virial = np.zeros(9)
+
+    def compute(self):
+        self.force, self.energies, self.virial = self.ens.compute_forces(self.terms)
+        self.energy = float(self.energies[self.energy_index])
+
+    def get_energy(self):
+        return self.energy
+
+    def get_virial(self):
+        return self.virial.copy()
+
+
+class LJForce(GpuForce):
+    """``LJForce::compute`` (src/forces/LJForce.cpp:58-255); also serves the
+    Mie and BMH kinds the ensemble was configured with."""
+    terms = L.TERM_VDW
+    energy_index = L.E_VDW
+
+
+class EwaldForce(GpuForce):
+    """``EwaldForce::compute`` (real space + self/charged energies,
+    src/forces/EwaldForce.cpp:127-172) and ``compute_long`` (reciprocal,
+    :174-196)."""
+    terms = L.TERM_EWALD_REAL
+    energy_index = L.E_REAL
+
+    def compute_long(self):
+        f, e, w = self.ens.compute_forces(L.TERM_EWALD_LONG)
+        self.long_force, self.long_energy, self.long_virial = f, float(e[L.E_LONG]), w
+        return f
+
+
+# ---------------------------------------------------------------------------
+# integrator mirror
+# ---------------------------------------------------------------------------
+
+class LFIntegrator:
+    """``LFIntegrator`` (src/integrators/LFIntegrator.cpp): ``start()`` is
+    LFIntegrator::start (F(0), vtMinus), ``run(n)`` advances n steps."""
+
+    def __init__(self, ensemble: GpuEnsemble, series_capacity: int = 0):
+        self.ens = ensemble
+        s, c = ensemble.system, ensemble.system.config
+        p = L.IntegratorParams()
+        p.timestep = c.timestep
+        p.temperature = c.temperature
+        p.coupl_const = c.coupl_const
+        p.thermostat = L.THERMO_NOSE_HOOVER if c.thermostat == "NoseHoover" else L.THERMO_NONE
+        p.atom_thermo = int(c.atom_thermo)
+        p.constraint = int(c.constraint)
+        p.long_steps = int(c.long_steps)
+        p.shake_tol = c.tolerance
+        p.shake_max_iter = int(c.max_count)
+        # degrees of freedom (Integrator.cpp:22-27)
+        p.mol_ndf = 3 * s.n_mols - 3
+        p.atom_ndf = 6 * s.n_mols - 3 if c.constraint else 3 * s.n_atoms - 3
+        p.strain_rate = c.rate if c.test_mode == 2 else 0.0
+        self.params = p
+        L.check(ensemble.ctx, ensemble.lib.smd_set_integrator(ensemble.ctx, ctypes.byref(p)))
+        if series_capacity:
+            L.check(ensemble.ctx, ensemble.lib.smd_set_series_capacity(ensemble.ctx, series_capacity))
+        self.series_capacity = series_capacity
+
+    def start(self):
+        L.check(self.ens.ctx, self.ens.lib.smd_integrator_start(self.ens.ctx))
+
+    def run(self, nsteps: int):
+        L.check(self.ens.ctx, self.ens.lib.smd_run(self.ens.ctx, int(nsteps)))
+
+    def run_timed(self, nsteps: int) -> float:
+        """run(n) returning the device time in ms (CUDA events)."""
+        ms = ctypes.c_double()
+        L.check(self.ens.ctx, self.ens.lib.smd_run_timed(self.ens.ctx, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
+    def observables(self) -> L.Observables:
+        o = L.Observables()
+        L.check(self.ens.ctx, self.ens.lib.smd_get_observables(self.ens.ctx, ctypes.byref(o)))
+        return o
+
+    def series(self) -> np.ndarray:
+        out = np.zeros(5 * max(self.series_capacity, 1))
+        cnt = ctypes.c_int()
+        L.check(self.ens.ctx, self.ens.lib.smd_get_series(self.ens.ctx, L.dptr(out),
+                                                          self.series_capacity, ctypes.byref(cnt)))
+        return out[:5 * cnt.value].reshape(-1, 5)
