@@ -164,6 +164,10 @@ int smd_ewald_nk(smd_ctx *ctx, int *nk);
 
 /* ---- integration (LFIntegrator, src/integrators/LFIntegrator.cpp) ------ */
 int smd_set_integrator(smd_ctx *ctx, const smd_integrator_params *p);
+/* SHAKE targets (LFIntegrator::initialise, LFIntegrator.cpp:141-167):
+ * len2[3*m + k] = squared length of the k-th cyclic distance of molecule m
+ * (sites 0-1, 1-2, 2-0 of a 3-site molecule; 0-1, 1-2 of a chain). */
+int smd_set_constraints(smd_ctx *ctx, const double *len2);
 /* LFIntegrator::start (LFIntegrator.cpp:991-1174): F(0) and
  * vtMinus = v - dt/2 F/m. */
 int smd_integrator_start(smd_ctx *ctx);

@@ -39,6 +39,10 @@ def lib():
         _lib.or_ewald_recip.restype = ctypes.c_double
         _lib.or_ewald_recip.argtypes = [ctypes.c_int, _D, _D, _D, ctypes.c_double, ctypes.c_double,
                                         _D, _D, ctypes.POINTER(ctypes.c_int)]
+        _lib.or_vdw.restype = ctypes.c_double
+        _lib.or_vdw.argtypes = [ctypes.c_int, ctypes.c_int, _D, _I, _I, _D, ctypes.c_int, _D,
+                                ctypes.c_double, ctypes.c_int, ctypes.c_double, _I, ctypes.c_int64,
+                                _D, _D]
     return _lib
 
 
@@ -121,3 +125,64 @@ def ewald(system, pos, box, pairs):
                               wl.ctypes.data_as(_D), ctypes.byref(nk))
     return {"real_force": f.reshape(-1, 3), "real_energy": er, "real_virial": w,
             "long_force": fl.reshape(-1, 3), "long_energy": el, "long_virial": wl, "nk": nk.value}
+
+
+def vdw_table(system):
+    """The per-type-pair table the pair term uses (kind, params[nt, nt, 4])."""
+    import math
+    c = system.config
+    nt = len(system.atom_types)
+    par = np.zeros((nt, nt, 4))
+    if system.bmh is not None:
+        b = system.bmh
+        par[..., 0], par[..., 1], par[..., 2], par[..., 3] = b["A"], 1.0 / b["rho"], b["C"], b["D"]
+        return 3, par
+    s2, e4 = system.lj_table()
+    n_, m_ = float(c.n_mie), float(c.m_mie)
+    cn = (n_ / (n_ - m_)) * math.pow(n_ / m_, m_ / (n_ - m_))
+    par[..., 0], par[..., 1], par[..., 2], par[..., 3] = np.sqrt(s2), cn * 0.25 * e4, n_, m_
+    return 2, par
+
+
+def vdw(system, pos, box, pairs):
+    c = system.config
+    kind, par = vdw_table(system)
+    L = np.array([box] * 3, np.float64)
+    n = system.n_atoms
+    f = np.zeros(3 * n)
+    w = np.zeros(9)
+    pairs = np.ascontiguousarray(pairs, np.int32)
+    e = lib().or_vdw(kind, n, d(pos), i32(system.atom_type), i32(system.mol_id), d(L),
+                     len(system.atom_types), d(par), c.cutoff, int(c.switch_on), c.switch_dist ** 2,
+                     i32(pairs), len(pairs), f.ctypes.data_as(_D), w.ctypes.data_as(_D))
+    return f.reshape(-1, 3), e, w
+
+
+def water_md(system, pos, vel, box, nsteps):
+    from swinmd_b200.systems import constraint_lengths
+    import math
+    c = system.config
+    lb = lib()
+    lb.or_water_md.restype = ctypes.c_int
+    lb.or_water_md.argtypes = [ctypes.c_int, _D, _D, _D, _I, _I, _D, _D, ctypes.c_int, _D, _D,
+                               ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                               ctypes.c_double, ctypes.c_double, _I, _I, _D, ctypes.c_double,
+                               ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                               ctypes.c_int, _D, _D, _D]
+    s2, e4 = system.lj_table()
+    L = np.array([box] * 3, np.float64)
+    q = system.scaled_charges()
+    e_self = -float((q * q).sum()) * c.alpha / math.sqrt(math.pi)
+    off, flat = _excl_csr(system)
+    pos = np.array(pos, np.float64).reshape(-1).copy()
+    vel = np.array(vel, np.float64).reshape(-1).copy()
+    ep, tt, zz = np.zeros(nsteps), np.zeros(nsteps), np.zeros(nsteps)
+    cl = constraint_lengths(system)[0].copy()
+    r = lb.or_water_md(system.n_mols, pos.ctypes.data_as(_D), vel.ctypes.data_as(_D),
+                       d(system.masses()), i32(system.atom_type), i32(system.mol_id), d(q), d(L),
+                       len(system.atom_types), d(s2), d(e4), c.cutoff, c.cut_buffer, int(c.switch_on),
+                       c.alpha, c.k_cutoff, e_self, i32(off), i32(flat), d(cl), c.tolerance,
+                       int(c.max_count), c.timestep, c.temperature, c.coupl_const, nsteps,
+                       ep.ctypes.data_as(_D), tt.ctypes.data_as(_D), zz.ctypes.data_as(_D))
+    assert r == 0, r
+    return {"pos": pos.reshape(-1, 3), "vel": vel.reshape(-1, 3), "epot": ep, "temp": tt, "zeta": zz}

@@ -252,3 +252,216 @@ double or_ewald_recip(int n, const double *pos, const double *q, const double *L
     if (nk_out) *nk_out = nk;
     return pe;
 }
+
+/* Mie n-m and Born-Mayer-Huggins pair terms over a pair list, with the
+ * 5th-order switch of MieForce::compute (src/forces/MieForce.cpp:89-196,
+ * switch constants :26-46) applied between sqrt(rs2) and rc when sw != 0.
+ * kind 2 (Mie): par = {sigma, Cn*eps, n, m} per type pair, as MieForce
+ * derives them from the LJ table (:26-35, :122-124).
+ * kind 3 (BMH, no reference code): par = {A, 1/rho, C, D},
+ * U = A exp(-r/rho) - C r^-6 - D r^-8.
+ * Same-molecule pairs are skipped (:111).  Returns the energy. */
+double or_vdw(int kind, int n, const double *pos, const int32_t *type, const int32_t *mol,
+              const double *L, int nt, const double *par, double rc, int sw, double rs2,
+              const int32_t *pairs, int64_t np, double *f, double *w) {
+    double rc2 = rc * rc, energy = 0;
+    double c1 = 0, c2 = 0, c3 = 0;
+    if (sw && rc2 > rs2) {
+        c1 = 1.0 / (rc2 - rs2);
+        c1 = c1 * c1 * c1;
+        c2 = rc2 - 3.0 * rs2;
+        c3 = 4 * c1;
+    }
+    memset(f, 0, sizeof(double) * 3 * n);
+    memset(w, 0, sizeof(double) * 9);
+    for (int64_t p = 0; p < np; p++) {
+        int i = pairs[2 * p], j = pairs[2 * p + 1];
+        if (mol[i] == mol[j]) continue;
+        double d[3] = {pos[3 * j] - pos[3 * i], pos[3 * j + 1] - pos[3 * i + 1],
+                       pos[3 * j + 2] - pos[3 * i + 2]};
+        pbc(d, L);
+        double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        double rij2 = r * r;
+        if (rij2 > rc2) continue;
+        const double *q = &par[4 * (type[i] * nt + type[j])];
+        double r_1 = 1.0 / r, rij_2 = r_1 * r_1, e, fs;
+        if (kind == 2) {
+            double s = q[0] * r_1, srn = pow(s, q[2]), srm = pow(s, q[3]);
+            e = q[1] * (srn - srm);
+            fs = q[1] * (q[2] * srn - q[3] * srm) * rij_2;
+        } else {
+            double ex = q[0] * exp(-r * q[1]), r6 = rij_2 * rij_2 * rij_2, r8 = r6 * rij_2;
+            e = ex - q[2] * r6 - q[3] * r8;
+            fs = ex * q[1] * r_1 - 6.0 * q[2] * r8 - 8.0 * q[3] * r8 * rij_2;
+        }
+        if (sw && rij2 > rs2) {
+            double c = rc2 - rij2, c4 = c * (2 * rij2 + c2);
+            double sv = c * c4 * c1, dsv = c3 * (c * c - c4);
+            fs = fs * sv - e * dsv;
+            e *= sv;
+        }
+        energy += e;
+        double fij[3] = {-fs * d[0], -fs * d[1], -fs * d[2]};
+        for (int k = 0; k < 3; k++) { f[3 * i + k] += fij[k]; f[3 * j + k] -= fij[k]; }
+        vir_add(w, fij, d);
+    }
+    return energy;
+}
+
+/* EwaldForce::intraMolCorrect energy (src/forces/EwaldForce.cpp:709-813) for
+ * molecules of consecutive sites (ns per molecule): -sum over excluded
+ * intramolecular pairs of q_i q_j erf(a r)/r.  Forces only when !constrained
+ * (the reference applies none under constraints). */
+double or_ewald_intra(int nmol, int ns, const double *pos, const double *q, const double *L,
+                      double alpha, const int32_t *off, const int32_t *ex, int constrained,
+                      double *f) {
+    double en = 0, a2 = alpha * alpha, a2pi = 2.0 * alpha / OR_SQRT_PI;
+    for (int m = 0; m < nmol; m++)
+        for (int a = 0; a < ns; a++)
+            for (int b = a + 1; b < ns; b++) {
+                int i = m * ns + a, j = m * ns + b;
+                if (!excluded(i, j, off, ex)) continue;
+                double d[3] = {pos[3 * j] - pos[3 * i], pos[3 * j + 1] - pos[3 * i + 1],
+                               pos[3 * j + 2] - pos[3 * i + 2]};
+                pbc(d, L);
+                double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2], r = sqrt(r2);
+                double qij = q[i] * q[j], e = erf(alpha * r) / r;
+                en += qij * e;
+                if (!constrained) {
+                    double dudr = e - a2pi * exp(-a2 * r2);
+                    for (int k = 0; k < 3; k++) {
+                        double fij = qij * dudr / r2 * d[k];
+                        f[3 * i + k] += fij;
+                        f[3 * j + k] -= fij;
+                    }
+                }
+            }
+    return -en;
+}
+
+/* Rigid 3-site water MD: LJ (LJForce) + Ewald (real, reciprocal, intra
+ * energy, self) forces, then LFIntegrator::shake (LFIntegrator.cpp:1678-1827,
+ * NVT branch with the Nose-Hoover term -zeta P_mol/ns) for every molecule
+ * and the step's molecular bookkeeping and zeta update (:646-722), molecule
+ * wrap (:897-912), drift removal (:359-379) and list rebuild (:307-341).
+ * Molecules are consecutive triples (H O H); clen2[3] the squared
+ * constraint distances.  out_*: per-step potential energy, temperature. */
+int or_water_md(int nmol, double *pos, double *vel, const double *mass, const int32_t *type,
+                const int32_t *mol, const double *q, const double *L, int nt, const double *sig2,
+                const double *eps4, double rc, double skin, int shift, double alpha, double kcut,
+                double e_self, const int32_t *off, const int32_t *ex, const double *clen2,
+                double tol, int maxcount, double dt, double T, double tau, int nsteps,
+                double *out_epot, double *out_temp, double *out_zeta) {
+    int n = 3 * nmol;
+    int64_t cap = (int64_t)n * 600;
+    int32_t *pairs = (int32_t *)malloc(sizeof(int32_t) * 2 * cap);
+    double *f = (double *)malloc(sizeof(double) * 3 * n), *f2 = (double *)malloc(sizeof(double) * 3 * n);
+    double *vtm = (double *)malloc(sizeof(double) * 3 * n);
+    double *disp = (double *)calloc(3 * n, sizeof(double));
+    double *P = (double *)calloc(3 * nmol, sizeof(double));
+    double w[9];
+    double rl = rc + skin, rl2 = rl * rl, drmax = skin * skin / 4.0;
+    int64_t np = or_pairlist(n, pos, L, rl2, off, ex, pairs, cap);
+    if (np > cap) return -1;
+#define OR_FORCES(E)                                                                          \
+    do {                                                                                      \
+        double e_ = or_lj(n, pos, type, mol, L, nt, sig2, eps4, rc, shift, 0.0, 0.0, pairs, np, f, w); \
+        memset(w, 0, sizeof(w));                                                              \
+        e_ += or_ewald_real(n, pos, q, L, alpha, rc, pairs, np, f, w);                        \
+        e_ += or_ewald_intra(nmol, 3, pos, q, L, alpha, off, ex, 1, f);                       \
+        e_ += or_ewald_recip(n, pos, q, L, alpha, kcut, f, w, NULL) + e_self;                 \
+        E = e_;                                                                               \
+    } while (0)
+    double e0;
+    OR_FORCES(e0);
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < 3; k++) vtm[3 * i + k] = vel[3 * i + k] - 0.5 * dt * (1.0 / mass[i]) * f[3 * i + k];
+    int ndf = 6 * nmol - 3;
+    double fnh = 0, fnhmi = 0, mtot = 0;
+    for (int i = 0; i < n; i++) mtot += mass[i];
+    for (int s = 0; s < nsteps; s++) {
+        int upd = 0;
+        for (int i = 0; i < n && !upd; i++)
+            if (disp[3 * i] * disp[3 * i] + disp[3 * i + 1] * disp[3 * i + 1] + disp[3 * i + 2] * disp[3 * i + 2] > drmax) upd = 1;
+        if (upd) {
+            memset(disp, 0, sizeof(double) * 3 * n);
+            np = or_pairlist(n, pos, L, rl2, off, ex, pairs, cap);
+        }
+        double vom[3] = {0, 0, 0};
+        for (int i = 0; i < n; i++)
+            for (int k = 0; k < 3; k++) vom[k] += vtm[3 * i + k] * mass[i];
+        for (int k = 0; k < 3; k++) vom[k] /= mtot;
+        if (fabs(vom[0]) > 1e-11 || fabs(vom[1]) > 1e-11 || fabs(vom[2]) > 1e-11)
+            for (int i = 0; i < n; i++)
+                for (int k = 0; k < 3; k++) { vtm[3 * i + k] -= vom[k]; vel[3 * i + k] -= vom[k]; }
+        OR_FORCES(out_epot[s]);
+        double ke = 0;
+        for (int m = 0; m < nmol; m++) {
+            double ro[3][3], rn[3][3], mr[3];
+            for (int a = 0; a < 3; a++) {
+                int i = 3 * m + a;
+                mr[a] = 1.0 / mass[i];
+                for (int k = 0; k < 3; k++) {
+                    double vp = vtm[3 * i + k] + dt * mr[a] * (f[3 * i + k] - fnh * P[3 * m + k] / 3);
+                    ro[a][k] = pos[3 * i + k];
+                    rn[a][k] = ro[a][k] + dt * vp;
+                }
+            }
+            int count = 0, done = 0;
+            while (!done && count < maxcount) {
+                done = 1;
+                for (int b = 0; b < 3; b++) {
+                    int nx = (b + 1) % 3;
+                    double dn[3] = {rn[b][0] - rn[nx][0], rn[b][1] - rn[nx][1], rn[b][2] - rn[nx][2]};
+                    pbc(dn, L);
+                    double r2 = dn[0] * dn[0] + dn[1] * dn[1] + dn[2] * dn[2];
+                    double diff = clen2[b] - r2;
+                    if (fabs(diff) > clen2[b] * 2 * tol) {
+                        double dold[3] = {ro[b][0] - ro[nx][0], ro[b][1] - ro[nx][1], ro[b][2] - ro[nx][2]};
+                        pbc(dold, L);
+                        double rr = dold[0] * dn[0] + dold[1] * dn[1] + dold[2] * dn[2];
+                        if (rr < clen2[b] * tol) return -3;
+                        double factor = diff / (2 * rr * (mr[b] + mr[nx]));
+                        for (int k = 0; k < 3; k++) {
+                            rn[b][k] += factor * dold[k] * mr[b];
+                            rn[nx][k] -= factor * dold[k] * mr[nx];
+                        }
+                        done = 0;
+                    }
+                }
+                count++;
+            }
+            if (!done) return -4;
+            double Pm[3] = {0, 0, 0}, com[3] = {0, 0, 0}, M = 0;
+            for (int a = 0; a < 3; a++) {
+                int i = 3 * m + a;
+                for (int k = 0; k < 3; k++) {
+                    double dr = rn[a][k] - pos[3 * i + k];
+                    pos[3 * i + k] += dr;
+                    disp[3 * i + k] += dr;
+                    double vp = dr / dt;
+                    vel[3 * i + k] = (vp + vtm[3 * i + k]) * 0.5;
+                    vtm[3 * i + k] = vp;
+                    Pm[k] += vel[3 * i + k] * mass[i];
+                    com[k] += mass[i] * pos[3 * i + k];
+                }
+                M += mass[i];
+                ke += (vel[3 * i] * vel[3 * i] + vel[3 * i + 1] * vel[3 * i + 1] + vel[3 * i + 2] * vel[3 * i + 2]) * mass[i];
+            }
+            for (int k = 0; k < 3; k++) { P[3 * m + k] = Pm[k]; com[k] /= M; }
+            double c[3] = {com[0], com[1], com[2]};
+            pbc(c, L);
+            for (int a = 0; a < 3; a++)
+                for (int k = 0; k < 3; k++) pos[3 * (3 * m + a) + k] += c[k] - com[k];
+        }
+        double qq = ndf * OR_KB * T * tau * tau;
+        double fnhpl = fnhmi + dt * (1.0 / qq) * (ke - ndf * OR_KB * T);
+        fnh = 0.5 * (fnhpl + fnhmi);
+        fnhmi = fnhpl;
+        out_temp[s] = ke / (ndf * OR_KB);
+        out_zeta[s] = fnh;
+    }
+#undef OR_FORCES
+    free(pairs); free(f); free(f2); free(vtm); free(disp); free(P);
+    return 0;
+}

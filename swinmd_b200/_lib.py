@@ -73,6 +73,7 @@ SIGNATURES = {
     "smd_get_pairs": (ctypes.c_int, [_P, _I, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "smd_ewald_nk": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
     "smd_set_integrator": (ctypes.c_int, [_P, ctypes.POINTER(IntegratorParams)]),
+    "smd_set_constraints": (ctypes.c_int, [_P, _D]),
     "smd_integrator_start": (ctypes.c_int, [_P]),
     "smd_run": (ctypes.c_int, [_P, ctypes.c_int]),
     "smd_get_observables": (ctypes.c_int, [_P, ctypes.POINTER(Observables)]),

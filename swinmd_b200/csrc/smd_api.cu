@@ -115,12 +115,20 @@ int sync_status(smd_ctx *x) {
 
 void enqueue_forces(Ctx &c) {
     launch_pair(c);
-    if (c.ewald_on) launch_recip(c);
+    if (c.ewald_on) {
+        launch_intra(c);
+        launch_recip(c);
+    }
 }
 
+// One MD step: in the FP32 path the integrate kernel of the previous step
+// (or smd_integrator_start / smd_upload_positions) has already written the
+// box fractions the pair kernel reads.
 void enqueue_step(Ctx &c) {
     launch_nlist(c, false);
+    c.fixq_from_integrate = 1;
     enqueue_forces(c);
+    c.fixq_from_integrate = 0;
     launch_integrate(c);
 }
 
@@ -170,7 +178,7 @@ void smd_destroy(smd_ctx *x) {
                     c.frc, c.acc, c.scal, c.partials, c.ticket, c.status, c.flags, c.obs,
                     c.series, c.pl.nbr, c.pl.nnbr, c.pl.cell_of, c.pl.cell_slot,
                     c.pl.cell_count, c.pl.cell_start, c.pl.cell_atoms, c.rc.kn, c.rc.kcoef,
-                    c.rc.sk, c.rc.kvec};
+                    c.rc.sk, c.rc.kvec, c.clen2};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -217,6 +225,9 @@ int smd_set_topology(smd_ctx *x, int n, int ntypes, const int32_t *atom_type,
         else if (c.h_type_charge[t] != scaled_charge[i])
             return fail(x, SMD_ERR_ARG, "smd_set_topology: charges must be per atom type");
     }
+    c.has_multisite = 0;
+    for (int m = 0; m < nmol; m++)
+        if (c.h_mol_off[m + 1] - c.h_mol_off[m] > 1) c.has_multisite = 1;
     c.total_mass = 0;
     for (int i = 0; i < n; i++) c.total_mass += mass[i];
 
@@ -229,7 +240,7 @@ int smd_set_topology(smd_ctx *x, int n, int ntypes, const int32_t *atom_type,
     CK(dalloc(&c.pl.nnbr, n)); CK(dalloc(&c.pl.cell_of, n)); CK(dalloc(&c.pl.cell_slot, n));
     CK(dalloc(&c.pl.cell_atoms, n));
     int nb = (nmol + 127) / 128;
-    CK(dalloc(&c.partials, (size_t)nb * 32));
+    CK(dalloc(&c.partials, (size_t)nb * 40));  // per block: NPART (35) partial sums
     CK(cudaMemcpy(c.type, atom_type, n * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.mol, mol_id, n * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.mass, mass, n * sizeof(double), cudaMemcpyHostToDevice));
@@ -382,6 +393,7 @@ int smd_set_precision(smd_ctx *x, int mode) {
     if (!x || (mode != SMD_PREC_FP64 && mode != SMD_PREC_MIXED))
         return fail(x, SMD_ERR_ARG, "smd_set_precision: unknown mode");
     x->c.precision = mode;
+    if (x->c.n > 0 && x->c.pos4) launch_fixq(x->c);
     x->c.graph_dirty = 1;
     return SMD_OK;
 }
@@ -406,6 +418,7 @@ int smd_upload_positions(smd_ctx *x, const double *pos) {
     CK(cudaMemsetAsync(c.disp4, 0, c.n * sizeof(double4), c.stream));
     int one = 1;  // the next step rebuilds the pair list from these positions
     CK(cudaMemcpyAsync(c.flags, &one, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+    launch_fixq(c);
     CK(cudaStreamSynchronize(c.stream));
     c.list_valid = 0;
     return SMD_OK;
@@ -460,6 +473,7 @@ int smd_compute_forces(smd_ctx *x, uint32_t terms, double *force, double *energy
     bool want_long = (terms & SMD_TERM_EWALD_LONG) && c.ewald_on;
     c.ewald_on = want_real ? 1 : 0;
     launch_pair(c);
+    if (want_real) launch_intra(c);
     c.ewald_on = save_ew;
     if (want_long) launch_recip(c);
     c.vdw = save_vdw;
@@ -529,8 +543,12 @@ int smd_ewald_nk(smd_ctx *x, int *nk) {
 int smd_set_integrator(smd_ctx *x, const smd_integrator_params *p) {
     if (!x || !p || !(p->timestep > 0) || x->c.n == 0)
         return fail(x, SMD_ERR_ARG, "smd_set_integrator: bad arguments");
-    if (p->constraint != 0)
-        return fail(x, SMD_ERR_ARG, "smd_set_integrator: constraint mode not available in this build");
+    if (p->constraint != 0 && p->constraint != 2)
+        return fail(x, SMD_ERR_ARG, "smd_set_integrator: constraint must be 0 (none) or 2 (SHAKE)");
+    if (p->constraint == 2 && !x->c.clen2)
+        return fail(x, SMD_ERR_ARG, "smd_set_integrator: SHAKE needs smd_set_constraints first");
+    if (p->constraint == 2 && (p->shake_max_iter <= 0 || !(p->shake_tol > 0)))
+        return fail(x, SMD_ERR_ARG, "smd_set_integrator: SHAKE tolerance and maxCount must be > 0");
     if (p->long_steps > 1)
         return fail(x, SMD_ERR_ARG, "smd_set_integrator: long_steps > 1 not supported");
     Ctx &c = x->c;
@@ -538,6 +556,22 @@ int smd_set_integrator(smd_ctx *x, const smd_integrator_params *p) {
     if (c.ip.atom_ndf <= 0) c.ip.atom_ndf = 3 * c.n - 3;
     if (c.ip.mol_ndf <= 0) c.ip.mol_ndf = 3 * c.nmol - 3;
     c.integrator_ready = 1;
+    c.graph_dirty = 1;
+    return SMD_OK;
+}
+
+int smd_set_constraints(smd_ctx *x, const double *len2) {
+    if (!x || !len2 || x->c.nmol == 0) return fail(x, SMD_ERR_ARG, "smd_set_constraints: bad arguments");
+    Ctx &c = x->c;
+    for (int m = 0; m < c.nmol; m++) {
+        int ns = c.h_mol_off[m + 1] - c.h_mol_off[m];
+        if (ns > 8) return fail(x, SMD_ERR_ARG, "smd_set_constraints: molecules of more than 8 sites");
+        for (int q = 0; q < 3; q++)
+            if (ns > 1 && !(len2[3 * m + q] > 0))
+                return fail(x, SMD_ERR_ARG, "smd_set_constraints: squared lengths must be > 0");
+    }
+    CK(dalloc(&c.clen2, 3 * (size_t)c.nmol));
+    CK(cudaMemcpy(c.clen2, len2, 3 * (size_t)c.nmol * sizeof(double), cudaMemcpyHostToDevice));
     c.graph_dirty = 1;
     return SMD_OK;
 }

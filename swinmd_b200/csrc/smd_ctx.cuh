@@ -80,6 +80,9 @@ struct Ctx {
     Recip rc;
     int precision = SMD_PREC_FP64;
     int want_cells = 1;
+    int has_multisite = 0;          // some molecule has more than one site
+    double *clen2 = nullptr;        // [nmol][3] squared SHAKE distances
+    int fixq_from_integrate = 0;    // step graph: integrate writes fixq
     int vdw = VDW_NONE;
     double cutoff = 1.0, cut_buffer = 0.1;
     double vdw_rc2 = 1.0, sw_rs2 = 0.0, sw_c1 = 0, sw_c2 = 0, sw_c3 = 0;
@@ -107,6 +110,7 @@ void launch_recip(Ctx &c);
 void launch_integrate(Ctx &c);
 void launch_start_velocities(Ctx &c);
 void launch_finalize_forces(Ctx &c, double *f_out_dev);
+void launch_intra(Ctx &c);
 int setup_recip(Ctx &c);
 
 }  // namespace smd

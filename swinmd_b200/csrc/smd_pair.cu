@@ -126,6 +126,50 @@ __device__ __forceinline__ void lj_pair_f(float r2f, float dr2, float &e, float 
     if (a.switch_on) e -= p[2];
 }
 
+// FP32 Mie n-m and Born-Mayer-Huggins with the same first-order correction
+// of the rounding of r^2, 1/r^2 and the power/exponent bases (eps as in
+// lj_pair_f): s^n = b^(n/2) with b = sigma^2/r^2, and exp(-r/rho) whose
+// argument error is amplified by r/rho (about 10 for NaCl).
+template <int VDW>
+__device__ __forceinline__ void vdw_pair_f(float r2f, float dr2, float &e, float &fs,
+                                           const float *p, const PairArgs &a, bool same) {
+    e = 0.f;
+    fs = 0.f;
+    if (same || !(r2f <= (float)a.vdw_rc2)) return;
+    const float ir2 = __frcp_rn(r2f);
+    const float eps = fmaf(-r2f, ir2, 1.0f) - dr2;   // 1/r^2 = ir2 (1 + eps)
+    if (VDW == VDW_MIE) {
+        const float s2 = p[0] * p[0];
+        const float b = s2 * ir2;
+        const float db = fmaf(s2, ir2, -b) / b + eps;  // b_exact = b (1 + db)
+        const float hn = 0.5f * p[2], hm = 0.5f * p[3];
+        const float srn = powf(b, hn), srm = powf(b, hm);
+        const float cn = 1.f + hn * db, cm = 1.f + hm * db;
+        e = p[1] * (srn * cn - srm * cm);
+        fs = p[1] * (p[2] * srn * cn - p[3] * srm * cm) * ir2 * (1.f + eps);
+    } else {
+        // r = sqrt(r^2) with the rounding of the root and of r^2 corrected
+        const float r = sqrtf(r2f);
+        const float dr = 0.5f * (fmaf(-r, r, r2f) / r2f + dr2);   // r_exact = r (1 + dr)
+        const float x = r * p[1];
+        const float dx = fmaf(r, p[1], -x) + x * dr;              // x_exact = x + dx
+        const float ex = p[0] * expf(-x) * (1.f - dx);
+        const float r6 = ir2 * ir2 * ir2, r8 = r6 * ir2;
+        const float c6 = 1.f + 3.f * eps, c8 = 1.f + 4.f * eps, c10 = 1.f + 5.f * eps;
+        e = ex - p[2] * r6 * c6 - p[3] * r8 * c8;
+        fs = ex * p[1] * (1.f - dr) / r - 6.f * p[2] * r8 * c8 - 8.f * p[3] * r8 * ir2 * c10;
+    }
+    const float rr = r2f;
+    if (a.switch_on && rr > (float)a.sw_rs2) {
+        const float c = (float)a.vdw_rc2 - rr;
+        const float c4 = c * (2.f * rr + (float)a.sw_c2);
+        const float sv = c * c4 * (float)a.sw_c1;
+        const float dsv = (float)a.sw_c3 * (c * c - c4);
+        fs = fs * sv - e * dsv;
+        e *= sv;
+    }
+}
+
 template <typename R, int VDW, bool EWALD, int TPP>
 __global__ void __launch_bounds__(PAIR_BLOCK) k_pair(PairArgs a) {
     __shared__ R s_par[MAX_TYPES * MAX_TYPES * 4];
@@ -194,6 +238,9 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_pair(PairArgs a) {
             if (sizeof(R) == 4 && VDW == VDW_LJ)
                 lj_pair_f((float)r2, r2c, *(float *)&e, *(float *)&fs,
                           (const float *)&s_par[(ti * a.ntypes + tj) * 4], a, same);
+            else if (sizeof(R) == 4 && (VDW == VDW_MIE || VDW == VDW_BMH))
+                vdw_pair_f<VDW>((float)r2, r2c, *(float *)&e, *(float *)&fs,
+                                (const float *)&s_par[(ti * a.ntypes + tj) * 4], a, same);
             else
                 vdw_pair<R, VDW>(r2, e, fs, &s_par[(ti * a.ntypes + tj) * 4], a, same);
             evdw += e;
@@ -320,7 +367,7 @@ void launch_pair(Ctx &c) {
     a.ew_rc2 = c.ew_rc2;
     a.frc = c.frc; a.acc = c.acc;
     if (c.precision == SMD_PREC_MIXED) {
-        launch_fixq(c);
+        if (!c.fixq_from_integrate) launch_fixq(c);
         if (c.ewald_on) dispatch_vdw<float, true>(c, a);
         else dispatch_vdw<float, false>(c, a);
     } else {

@@ -24,6 +24,19 @@ constexpr int RK_THREADS = 128;   // k vectors per structure-factor block
 constexpr int RK_CHUNKS = 16;     // site chunks (partial sums per k)
 constexpr int RF_TPS = 4;         // threads per site in the force pass
 
+// sin and cos of 2 pi ph / 2^32 for a 32-bit phase: the top 24 bits go
+// through sincospif exactly (they fit a float), the low 8 bits (an angle
+// below 4e-7 rad) are added to first order, so the argument carries no
+// rounding at all.
+__device__ __forceinline__ void sincos_phase(int ph, float &s, float &c) {
+    const int hi = ph & ~0xff;
+    const float b = (float)(ph & 0xff) * 1.4629180792671596e-09f;  // pi / 2^31
+    float sh, ch;
+    sincospif((float)hi * 4.656612873077393e-10f, &sh, &ch);
+    s = fmaf(b, ch, sh);
+    c = fmaf(-b, sh, ch);
+}
+
 // partial[ch][2][nk]
 template <typename R>
 __global__ void __launch_bounds__(RK_THREADS) k_sk_partial(int n, int nk, const double4 *pos4,
@@ -67,7 +80,7 @@ __global__ void __launch_bounds__(RK_THREADS) k_sk_partial(int n, int nk, const 
                     const int ph = (int)((unsigned)nx * (unsigned)f.x + (unsigned)ny * (unsigned)f.y +
                                          (unsigned)nz * (unsigned)f.z);
                     float sf, cf;
-                    sincospif((float)ph * 4.656612873077393e-10f, &sf, &cf);  // ph / 2^31
+                    sincos_phase(ph, sf, cf);
                     s = sf; c = cf;
                     qi = (R)tq[f.w];
                 }
@@ -136,8 +149,10 @@ __global__ void __launch_bounds__(256) k_recip_force(int n, int nk, const double
                                                      const double *sk, const double *tq,
                                                      long long *frc) {
     __shared__ int s_n[3][256];
-    __shared__ R s_k[3][256];
-    __shared__ R s_b[256], s_c[256], s_s[256];
+    // k vectors, prefactors and S(k) stay FP64; only the phase and its
+    // sine/cosine follow R (the FP32 path's cost is in sincospif)
+    __shared__ double s_k[3][256];
+    __shared__ double s_b[256], s_c[256], s_s[256];
     const int gt = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = gt / RF_TPS, t = gt % RF_TPS;
     double4 p64 = make_double4(0, 0, 0, 0);
@@ -153,21 +168,20 @@ __global__ void __launch_bounds__(256) k_recip_force(int n, int nk, const double
         const int k = base + threadIdx.x;
         if (k < nk) {
             s_n[0][threadIdx.x] = kn[k]; s_n[1][threadIdx.x] = kn[nk + k]; s_n[2][threadIdx.x] = kn[2 * nk + k];
-            s_k[0][threadIdx.x] = (R)kvec[k]; s_k[1][threadIdx.x] = (R)kvec[nk + k];
-            s_k[2][threadIdx.x] = (R)kvec[2 * nk + k];
-            s_b[threadIdx.x] = (R)(2.0 * kcoef[k]);
-            s_c[threadIdx.x] = (R)sk[k];
-            s_s[threadIdx.x] = (R)sk[nk + k];
+            s_k[0][threadIdx.x] = kvec[k]; s_k[1][threadIdx.x] = kvec[nk + k];
+            s_k[2][threadIdx.x] = kvec[2 * nk + k];
+            s_b[threadIdx.x] = 2.0 * kcoef[k];
+            s_c[threadIdx.x] = sk[k];
+            s_s[threadIdx.x] = sk[nk + k];
         }
         __syncthreads();
         const int cnt = min(256, nk - base);
         if (i < n) {
-            R ax = 0, ay = 0, az = 0;
+            double ax = 0, ay = 0, az = 0;
             for (int q = t; q < cnt; q += RF_TPS) {
                 R s, c;
                 if (sizeof(R) == 8) {
-                    const double a = p64.x * (double)s_k[0][q] + p64.y * (double)s_k[1][q] +
-                                     p64.z * (double)s_k[2][q];
+                    const double a = p64.x * s_k[0][q] + p64.y * s_k[1][q] + p64.z * s_k[2][q];
                     double sd, cd;
                     sincos(a, &sd, &cd);
                     s = (R)sd; c = (R)cd;
@@ -176,15 +190,16 @@ __global__ void __launch_bounds__(256) k_recip_force(int n, int nk, const double
                                          (unsigned)s_n[1][q] * (unsigned)pf.y +
                                          (unsigned)s_n[2][q] * (unsigned)pf.z);
                     float sf, cf;
-                    sincospif((float)ph * 4.656612873077393e-10f, &sf, &cf);
+                    sincos_phase(ph, sf, cf);
                     s = sf; c = cf;
                 }
-                const R val = s_b[q] * (qi * s * s_c[q] - qi * c * s_s[q]);
+                const double qs = (double)(qi * s), qc = (double)(qi * c);
+                const double val = s_b[q] * (qs * s_c[q] - qc * s_s[q]);
                 ax += s_k[0][q] * val;
                 ay += s_k[1][q] * val;
                 az += s_k[2][q] * val;
             }
-            fx += (double)ax; fy += (double)ay; fz += (double)az;
+            fx += ax; fy += ay; fz += az;
         }
     }
     fx = group_sum<RF_TPS>(fx);

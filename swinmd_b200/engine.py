@@ -155,6 +155,10 @@ class GpuEnsemble:
         self._setup_vdw()
         if c.compute_ewald:
             self._chk(self.lib.smd_set_ewald(ctx, c.alpha, c.k_cutoff, c.cutoff))
+        if c.constraint == 2:
+            from .systems import constraint_lengths
+            cl = np.ascontiguousarray(constraint_lengths(s).reshape(-1))
+            self._chk(self.lib.smd_set_constraints(ctx, L.dptr(cl)))
         self.set_precision(precision)
         if threads_per_site:
             self._chk(self.lib.smd_set_tuning(ctx, threads_per_site))

@@ -324,3 +324,148 @@ def lj_fluid(ncell: int = 10, rho_star: float = 0.8442, t_star: float = 0.722,
                   atom_types=[AtomType(AR_MASS, 0.0, AR_EPS, AR_SIGMA, name="Ar", long_name="Argon")],
                   atom_type=np.zeros(n, np.int32), mol_id=np.arange(n, dtype=np.int32),
                   mol_type_names=[("AR", 1)], mol_type=np.zeros(n, np.int32), config=cfg)
+
+
+# Tosi-Fumi (1964) Born-Mayer-Huggins parameters for NaCl, converted to
+# kJ/mol and nm: phi = A exp(-r/rho) - C r^-6 - D r^-8 with
+# A = A_ij b exp((s_i + s_j)/rho), b = 0.338e-19 J, rho = 0.317 A.
+_TF_B = 0.338e-19 * 6.02214076e23 / 1000.0
+_TF_RHO = 0.0317
+_TF_S = {"Na": 0.117, "Cl": 0.1585}
+_TF_A = {("Na", "Na"): 1.25, ("Na", "Cl"): 1.00, ("Cl", "Cl"): 0.75}
+_TF_C = {("Na", "Na"): 1.68, ("Na", "Cl"): 11.2, ("Cl", "Cl"): 116.0}   # 1e-79 J m^6
+_TF_D = {("Na", "Na"): 0.8, ("Na", "Cl"): 13.9, ("Cl", "Cl"): 233.0}    # 1e-99 J m^8
+
+
+def nacl_bmh_tables():
+    names = ["Na", "Cl"]
+    A = np.zeros((2, 2)); C = np.zeros((2, 2)); D = np.zeros((2, 2))
+    for i, a in enumerate(names):
+        for j, b in enumerate(names):
+            key = (a, b) if (a, b) in _TF_A else (b, a)
+            A[i, j] = _TF_A[key] * _TF_B * math.exp((_TF_S[a] + _TF_S[b]) / _TF_RHO)
+            C[i, j] = _TF_C[key] * 6.02214076e-5
+            D[i, j] = _TF_D[key] * 6.02214076e-7
+    return {"A": A, "rho": np.full((2, 2), _TF_RHO), "C": C, "D": D}
+
+
+def nacl_melt(ncell: int = 20, density_gcc: float = 1.55, temperature: float = 1200.0,
+              seed: int = 1, jitter: float = 0.02, cutoff: float = 1.1, skin: float = 0.1,
+              alpha: float = 2.8, kmax: int = 10, potential: str = "bmh",
+              dt: float = 0.001, n_steps: int = 1000) -> System:
+    """Rock-salt NaCl with ``ncell^3`` ions (ncell even), +-1 e, at the given
+    mass density, each ion displaced uniformly by up to ``jitter`` nm from its
+    lattice site (seeded).  potential: "bmh" (Tosi-Fumi Born-Mayer-Huggins) or
+    "mie" (Mie 14-7 with Joung-Cheatham-like sigma/eps through the LJ table,
+    as the reference's MieForce reads it).  Ewald with |n| < kmax."""
+    assert ncell % 2 == 0
+    n = ncell ** 3
+    m_na, m_cl = 22.98977, 35.453
+    mass_g = (n // 2) * (m_na + m_cl) / 6.02214076e23
+    L = (mass_g / density_gcc) ** (1.0 / 3.0) * 1e7  # cm -> nm
+    a = L / ncell
+    g = np.stack(np.meshgrid(np.arange(ncell), np.arange(ncell), np.arange(ncell),
+                             indexing="ij"), -1).reshape(-1, 3)
+    typ = (g.sum(1) % 2).astype(np.int32)   # 0 Na, 1 Cl alternate
+    rng = np.random.default_rng(seed)
+    pos = (g + 0.5) * a - L / 2 + rng.uniform(-jitter, jitter, (n, 3))
+    pos = _wrap(pos, L)
+    # |k| cutoff strictly between kmax-1 and kmax shells: n^2 < kmax^2
+    kcut = 2 * math.pi * math.sqrt(kmax * kmax - 0.5) / L
+    cfg = Config(seed=seed, timestep=dt, n_steps=n_steps, temperature=temperature,
+                 coupl_const=0.5, cutoff=cutoff, cutoff_ew=cutoff, cut_buffer=skin,
+                 compute_ewald=True, alpha=alpha, k_cutoff=kcut, switch_on=True,
+                 switch_dist=cutoff - 0.1, compute_mie=(potential == "mie"), n_mie=14, m_mie=7)
+    types = [AtomType(m_na, 1.0, 0.3658, 0.2439, name="Na", long_name="Sodium"),
+             AtomType(m_cl, -1.0, 0.1489, 0.4478, name="Cl", long_name="Chloride")]
+    s = System(name=f"nacl{n}", pos=pos, box=(L, L, L), atom_types=types, atom_type=typ,
+               mol_id=np.arange(n, dtype=np.int32), mol_type_names=[("ION", 1)],
+               mol_type=np.zeros(n, np.int32), config=cfg)
+    if potential == "bmh":
+        s.bmh = nacl_bmh_tables()
+    return s
+
+
+def _random_rotation(rng):
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    a, b, c, d = q
+    return np.array([[a * a + b * b - c * c - d * d, 2 * (b * c - a * d), 2 * (b * d + a * c)],
+                     [2 * (b * c + a * d), a * a - b * b + c * c - d * d, 2 * (c * d - a * b)],
+                     [2 * (b * d - a * c), 2 * (c * d + a * b), a * a - b * b - c * c + d * d]])
+
+
+def _place_waters(nmol, L, r_oh, theta_deg, rng, masses, min_dist=0.2):
+    """Molecule centres on a cubic grid (first nmol of g^3 points), random
+    orientations (seeded), re-drawn while any site of a molecule comes
+    closer than min_dist to a site of an already placed molecule."""
+    g = int(math.ceil(nmol ** (1.0 / 3.0) - 1e-9))
+    a = L / g
+    th = math.radians(theta_deg)
+    # H O H in the molecule frame, centre of mass at the origin
+    body = np.array([[r_oh * math.sin(th / 2), r_oh * math.cos(th / 2), 0.0],
+                     [0.0, 0.0, 0.0],
+                     [-r_oh * math.sin(th / 2), r_oh * math.cos(th / 2), 0.0]])
+    com = (masses[:, None] * body).sum(0) / masses.sum()
+    body -= com
+    idx = np.stack(np.meshgrid(np.arange(g), np.arange(g), np.arange(g), indexing="ij"), -1).reshape(-1, 3)
+    order = rng.permutation(len(idx))[:nmol]
+    centres = (idx[np.sort(order)] + 0.5) * a - L / 2
+    pos = np.zeros((nmol, 3, 3))
+    for m in range(nmol):
+        for _ in range(200):
+            cand = centres[m] + body @ _random_rotation(rng).T
+            if m == 0:
+                break
+            prev = pos[:m].reshape(-1, 3)
+            d = cand[:, None, :] - prev[None, :, :]
+            d -= L * np.round(d / L)
+            if np.sqrt((d ** 2).sum(-1)).min() >= min_dist:
+                break
+        pos[m] = cand
+    return pos.reshape(-1, 3)
+
+
+def spce_water(nmol: int = 2160, box: float = 4.03, seed: int = 1, temperature: float = 298.0,
+               cutoff: float = 1.0, skin: float = 0.1, alpha: float = 3.1, kmax: int = 9,
+               dt: float = 0.002, tol: float = 1e-8, n_steps: int = 1000) -> System:
+    """Rigid SPC/E-like water: H O H sites (molecule name WAT so the
+    reference applies its 3-site SHAKE), q_O = -0.8476 e, r_OH = 0.1 nm,
+    HOH = 109.47 deg, LJ on O only (sigma 0.3166 nm, eps 0.650 kJ/mol),
+    Ewald with |n| < kmax, SHAKE, Nose-Hoover."""
+    rng = np.random.default_rng(seed)
+    m_h, m_o = 1.008, 15.9994
+    pos = _place_waters(nmol, box, 0.1, 109.47, rng, np.array([m_h, m_o, m_h]))
+    pos = _wrap(pos, box)
+    n = 3 * nmol
+    typ = np.tile(np.array([0, 1, 0], np.int32), nmol)
+    mol = np.repeat(np.arange(nmol, dtype=np.int32), 3)
+    bonds = np.array([[3 * m + a, 3 * m + b, 0] for m in range(nmol) for a, b in ((0, 1), (1, 2))], np.int32)
+    angles = np.array([[3 * m, 3 * m + 1, 3 * m + 2, 0] for m in range(nmol)], np.int32)
+    kcut = 2 * math.pi * math.sqrt(kmax * kmax - 0.5) / box
+    cfg = Config(seed=seed, timestep=dt, n_steps=n_steps, temperature=temperature, coupl_const=0.5,
+                 cutoff=cutoff, cutoff_ew=cutoff, cut_buffer=skin, compute_ewald=True, alpha=alpha,
+                 k_cutoff=kcut, switch_on=True, switch_dist=cutoff, constraint=2, tolerance=tol,
+                 max_count=1000, long_correct=True)
+    types = [AtomType(m_h, 0.4238, 0.0, 0.1, name="H", long_name="Hydrogen"),
+             AtomType(m_o, -0.8476, 0.650, 0.3166, name="O", long_name="Oxygen")]
+    return System(name=f"spce{nmol}", pos=pos, box=(box, box, box), atom_types=types,
+                  atom_type=typ, mol_id=mol, mol_type_names=[("WAT", 3)],
+                  mol_type=np.zeros(nmol, np.int32), config=cfg, bonds=bonds, angles=angles,
+                  bond_params=[(0, 1, 0.1, 345000.0)], angle_params=[(0, 1, 0, 109.47, 383.0)])
+
+
+def constraint_lengths(s: System) -> np.ndarray:
+    """Squared constraint lengths per molecule for the cyclic 3-site SHAKE
+    (LFIntegrator::initialise, src/integrators/LFIntegrator.cpp:156-167):
+    bond 0-1, bond 1-2, and the 0..2 distance from the two bonds and the
+    angle (Parameters::get_bond_length(a1,a2,a3), src/Parameters.h:219-226)."""
+    (t1, t2, r0, _), = s.bond_params[:1]
+    out = np.zeros((s.n_mols, 3))
+    theta = s.angle_params[0][3] * 2 * math.pi / 360.0
+    l1 = l2 = r0
+    l3 = math.sqrt(l1 * l1 + l2 * l2 - 2 * l1 * l2 * math.cos(theta))
+    out[:, 0] = l1 * l1
+    out[:, 1] = l2 * l2
+    out[:, 2] = l3 * l3
+    return out

@@ -30,7 +30,17 @@ def lj500():
     return s, [("forces",), ("run", 20)]
 
 
-CASES = {"lj500": lj500}
+def nacl1000_mie():
+    s = systems.nacl_melt(ncell=10, potential="mie", kmax=6, seed=5)
+    return s, [("forces",), ("mie",)]
+
+
+def spce512():
+    s = systems.spce_water(nmol=512, box=2.4953, cutoff=0.9, kmax=6, seed=11, n_steps=20)
+    return s, [("forces",), ("run", 20)]
+
+
+CASES = {"lj500": lj500, "nacl1000_mie": nacl1000_mie, "spce512": spce512}
 
 
 def pack(name, s, results):
@@ -50,6 +60,10 @@ def pack(name, s, results):
             continue
         else:
             out["f_" + k] = v
+    if "mie" in results:
+        for k, v in results["mie"].items():
+            if k.startswith("mie_"):
+                out["m_" + k] = v
     if "run" in results:
         for k, v in results["run"].items():
             if k.startswith(("step_", "final_", "start_")):
