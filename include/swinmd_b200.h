@@ -47,6 +47,10 @@ enum {
     SMD_TERM_VDW = 1,        /* LJForce / MieForce / BMH pair term */
     SMD_TERM_EWALD_REAL = 2, /* EwaldForce::compute() real space + intra + self */
     SMD_TERM_EWALD_LONG = 4, /* EwaldForce::compute_long() */
+    SMD_TERM_MP_SHORT = 8,   /* Multipole::compute(): self + real + intramolecular */
+    SMD_TERM_MP_LONG = 16,   /* Multipole::compute_long() */
+    SMD_TERM_IND_SHORT = 32, /* Induction::compute(): dipole solve, self, real, intra */
+    SMD_TERM_IND_LONG = 64,  /* Induction::compute_long() (solves the dipoles too) */
     SMD_TERM_ALL = 0xffff
 };
 
@@ -58,11 +62,22 @@ enum {
     SMD_E_CORRECT = 3,   /* myEnergy.correctEnergy (self + net charge) */
     SMD_E_MOLCORRECT = 4,/* myEnergy.molCorrectEnergy */
     SMD_E_SURF = 5,      /* myEnergy.surfCorrectEnergy */
-    SMD_E_COUNT = 8
+    SMD_E_POL_REAL = 6,  /* myEnergy.realPolEnergy */
+    SMD_E_POL_LONG = 7,  /* myEnergy.longPolEnergy */
+    SMD_E_POL_SELF = 8,  /* myEnergy.correctPolEnergy */
+    SMD_E_POL_INTRA = 9, /* myEnergy.molCorrectPolEnergy */
+    SMD_E_COUNT = 12
 };
 
 /* vdW kinds for smd_set_vdw */
-enum { SMD_VDW_NONE = 0, SMD_VDW_LJ = 1, SMD_VDW_MIE = 2, SMD_VDW_BMH = 3 };
+enum { SMD_VDW_NONE = 0, SMD_VDW_LJ = 1, SMD_VDW_MIE = 2, SMD_VDW_BMH = 3, SMD_VDW_BUFF = 4 };
+
+/* initial guess of the induced-dipole solve */
+enum {
+    SMD_GUESS_DIRECT = 0,   /* p0 = alpha E0 (first-order induction) */
+    SMD_GUESS_PREVIOUS = 1, /* p0 = the previous solve's dipoles */
+    SMD_GUESS_LEARNED = 2   /* p0 from the per-site network (smd_mlp_*) */
+};
 
 /* thermostat kinds */
 enum { SMD_THERMO_NONE = 0, SMD_THERMO_NOSE_HOOVER = 1 };
@@ -138,6 +153,32 @@ int smd_set_vdw(smd_ctx *ctx, int kind, const double *params, int switch_on,
  * src/forces/EwaldForce.cpp:22-257): alpha (1/nm), kcut (1/nm), real-space
  * cutoff.  long_steps: reciprocal term every long_steps steps. */
 int smd_set_ewald(smd_ctx *ctx, double alpha, double kcut, double real_cut);
+/* Buffered 14-7 pair term (BuffvdWForce, src/forces/BuffvdWForce.cpp):
+ * params: ntypes*ntypes rows of {sigma, eps} as set_buff_param mixes them
+ * (:392-433); n, m, delta, gamma; h_factor pulls type-0 (H) sites towards
+ * their molecule's second site (O) (:358-385); taper c[6] from switch_dist
+ * to the cutoff (:60-73); e_lrc / v_lrc the tail correction (:468-601). */
+int smd_set_buff(smd_ctx *ctx, const double *params, double n, double m, double delta,
+                 double gamma, double h_factor, int switch_on, double switch_dist,
+                 const double *taper_c, double e_lrc, double v_lrc);
+/* Polarisable multipole model (Multipole + Induction, src/forces/Multipole.cpp,
+ * src/forces/Induction.cpp) for 3-site H O H molecules.  type_mp: per type
+ * local-frame dipole (3) and traceless quadrupole (xx xy xz yy yz zz) as in
+ * the !AtomParams section; polar: per type polarisability (nm^3); alpha,
+ * kcut: Ewald splitting and |k| cutoff (1/nm); real_cut: cutoffEw;
+ * induction: solve for induced dipoles; ind_cut: cutoffInd; thole_a. */
+int smd_set_multipole(smd_ctx *ctx, const double *type_mp, const double *polar, double alpha,
+                      double kcut, double real_cut, int induction, double ind_cut, double thole_a);
+/* Dipole solver: RMS change tolerance (e nm), iteration cap, initial guess. */
+int smd_set_solver(smd_ctx *ctx, double tol, int max_iter, int guess);
+/* Solver statistics of the last solve: iterations and final RMS change. */
+int smd_solver_stats(smd_ctx *ctx, int *iterations, double *rms_change);
+/* Lab-frame dipoles, quadrupoles, permanent field and induced dipoles of the
+ * last evaluation, per site (each pointer may be NULL): mu[3n], quad[6n]
+ * (xx xy xz yy yz zz, the reference's /3 convention), e0[3n], p[3n]. */
+int smd_get_polarization(smd_ctx *ctx, double *mu, double *quad, double *e0, double *p);
+/* Induced dipoles to start the next solve from (SMD_GUESS_PREVIOUS/LEARNED). */
+int smd_set_induced(smd_ctx *ctx, const double *p);
 int smd_set_precision(smd_ctx *ctx, int mode);
 /* Pair-kernel threads per site (1..32, power of two); 0 lets the library pick. */
 int smd_set_tuning(smd_ctx *ctx, int threads_per_site);

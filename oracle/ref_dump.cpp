@@ -200,6 +200,24 @@ static int mode_forces(const char *out) {
         Multipole mp(e);
         mp.compute();
         dump_forces(e, "mp_short");
+        {
+            int n = e->nAtoms;
+            std::vector<double> dip(3 * n), quad(6 * n);
+            for (int i = 0; i < n; i++) {
+                dip[3 * i] = mp.myL2G->dip[i].x;
+                dip[3 * i + 1] = mp.myL2G->dip[i].y;
+                dip[3 * i + 2] = mp.myL2G->dip[i].z;
+                quad[6 * i] = mp.myL2G->Qxx[i];
+                quad[6 * i + 1] = mp.myL2G->Qxy[i];
+                quad[6 * i + 2] = mp.myL2G->Qxz[i];
+                quad[6 * i + 3] = mp.myL2G->Qyy[i];
+                quad[6 * i + 4] = mp.myL2G->Qyz[i];
+                quad[6 * i + 5] = mp.myL2G->Qzz[i];
+            }
+            rec("mp_dip", dip);
+            rec("mp_quad", quad);
+            rec("mp_parts", {mp.selfEnergy, mp.realEnergy, mp.intraMolEnergy});
+        }
         zero(e);
         mp.compute_long();
         dump_forces(e, "mp_long");
@@ -208,6 +226,10 @@ static int mode_forces(const char *out) {
             Induction ind(e);
             ind.compute();
             dump_forces(e, "ind_short");
+            int n3 = 3 * e->nAtoms;
+            rec("ind_E0", std::vector<double>(ind.Ei0, ind.Ei0 + n3));
+            rec("ind_P", std::vector<double>(ind.Pi, ind.Pi + n3));
+            rec("ind_parts", {ind.selfEnergy, ind.realEnergy, ind.intraMolEnergy});
             zero(e);
             ind.compute_long();
             dump_forces(e, "ind_long");

@@ -17,8 +17,11 @@ ERRORS = {1: "SMD_ERR_ARG", 2: "SMD_ERR_CUDA", 3: "SMD_ERR_LIST_OVERFLOW", 4: "S
           5: "SMD_ERR_SHAKE", 6: "SMD_ERR_NAN", 7: "SMD_ERR_CG", 8: "SMD_ERR_NO_DEVICE"}
 PREC_FP64, PREC_MIXED = 0, 1
 TERM_VDW, TERM_EWALD_REAL, TERM_EWALD_LONG, TERM_ALL = 1, 2, 4, 0xFFFF
-E_VDW, E_REAL, E_LONG, E_CORRECT, E_MOLCORRECT, E_SURF, E_COUNT = 0, 1, 2, 3, 4, 5, 8
-VDW_NONE, VDW_LJ, VDW_MIE, VDW_BMH = 0, 1, 2, 3
+TERM_MP_SHORT, TERM_MP_LONG, TERM_IND_SHORT, TERM_IND_LONG = 8, 16, 32, 64
+E_VDW, E_REAL, E_LONG, E_CORRECT, E_MOLCORRECT, E_SURF = 0, 1, 2, 3, 4, 5
+E_POL_REAL, E_POL_LONG, E_POL_SELF, E_POL_INTRA, E_COUNT = 6, 7, 8, 9, 12
+VDW_NONE, VDW_LJ, VDW_MIE, VDW_BMH, VDW_BUFF = 0, 1, 2, 3, 4
+GUESS_DIRECT, GUESS_PREVIOUS, GUESS_LEARNED = 0, 1, 2
 THERMO_NONE, THERMO_NOSE_HOOVER = 0, 1
 
 
@@ -82,6 +85,16 @@ SIGNATURES = {
     "smd_profile_stages": (ctypes.c_int, [_P, ctypes.c_int, _D]),
     "smd_step_kernel_count": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
     "smd_run_timed": (ctypes.c_int, [_P, ctypes.c_int, _D]),
+    "smd_set_buff": (ctypes.c_int, [_P, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                    _D, ctypes.c_double, ctypes.c_double]),
+    "smd_set_multipole": (ctypes.c_int, [_P, _D, _D, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_double]),
+    "smd_set_solver": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
+    "smd_solver_stats": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), _D]),
+    "smd_get_polarization": (ctypes.c_int, [_P, _D, _D, _D, _D]),
+    "smd_set_induced": (ctypes.c_int, [_P, _D]),
 }
 
 _lib = None

@@ -113,12 +113,30 @@ int sync_status(smd_ctx *x) {
     return SMD_OK;
 }
 
+// Polarisable model, in the order LFIntegrator::run calls the reference's
+// terms (LFIntegrator.cpp:440-458): multipoles short and long, then the
+// induced dipoles (solved once per step) short and long; all torques are
+// mapped onto the sites at the end (the mapping is linear in the torques).
+void enqueue_polar(Ctx &c, bool mp_short, bool mp_long, bool ind_short, bool ind_long) {
+    launch_frames(c);
+    launch_torques_begin(c);
+    if (mp_short) launch_mp_short(c);
+    if (mp_long) launch_mp_long(c);
+    if (c.ind_on && (ind_short || ind_long)) {
+        launch_ind_solve(c);
+        if (ind_short) launch_ind_short(c);
+        if (ind_long) launch_ind_long(c);
+    }
+    launch_torques_end(c);
+}
+
 void enqueue_forces(Ctx &c) {
     launch_pair(c);
     if (c.ewald_on) {
         launch_intra(c);
         launch_recip(c);
     }
+    if (c.mp_on) enqueue_polar(c, true, true, true, true);
 }
 
 // One MD step: in the FP32 path the integrate kernel of the previous step
@@ -178,7 +196,8 @@ void smd_destroy(smd_ctx *x) {
                     c.frc, c.acc, c.scal, c.partials, c.ticket, c.status, c.flags, c.obs,
                     c.series, c.pl.nbr, c.pl.nnbr, c.pl.cell_of, c.pl.cell_slot,
                     c.pl.cell_count, c.pl.cell_start, c.pl.cell_atoms, c.rc.kn, c.rc.kcoef,
-                    c.rc.sk, c.rc.kvec, c.clen2};
+                    c.rc.sk, c.rc.kvec, c.clen2, c.type_mp, c.type_polar, c.mu, c.qd, c.trq, c.e0,
+                    c.pind, c.cgw, c.cgs, c.cg_bar, c.vpos4, c.vfixq, c.fv};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -301,7 +320,7 @@ int smd_set_box(smd_ctx *x, double lx, double ly, double lz) {
         c.box.inv[d] = 1.0 / c.box.L[d];
     }
     setup_grid(c, c.want_cells);
-    if (c.ewald_on) {
+    if (c.ewald_on || c.mp_on) {
         int r = setup_recip(c);
         if (r) return fail(x, r, "smd_set_box: reciprocal set-up failed");
     }
@@ -386,6 +405,124 @@ int smd_set_ewald(smd_ctx *x, double alpha, double kcut, double real_cut) {
     int r = setup_recip(c);
     if (r) return fail(x, r, "smd_set_ewald: reciprocal set-up failed");
     c.graph_dirty = 1;
+    return SMD_OK;
+}
+
+int smd_set_buff(smd_ctx *x, const double *params, double n, double m, double delta, double gamma,
+                 double h_factor, int switch_on, double switch_dist, const double *taper_c, double e_lrc,
+                 double v_lrc) {
+    if (!x || !params || x->c.ntypes == 0 || !(n > m) || !(m > 0))
+        return fail(x, SMD_ERR_ARG, "smd_set_buff: bad arguments");
+    Ctx &c = x->c;
+    const int nt = c.ntypes;
+    std::vector<double> p((size_t)nt * nt * 4, 0.0);
+    for (int k = 0; k < nt * nt; k++) {
+        p[4 * k] = params[2 * k];
+        p[4 * k + 1] = params[2 * k + 1];
+    }
+    CK(cudaMemcpy(c.pair_par, p.data(), p.size() * sizeof(double), cudaMemcpyHostToDevice));
+    c.vdw = VDW_BUFF;
+    c.buff_on = 1;
+    c.buff_n = n; c.buff_m = m; c.buff_delta = delta; c.buff_gamma = gamma; c.buff_h = h_factor;
+    c.switch_on = switch_on;
+    c.buff_sw = switch_dist;
+    for (int q = 0; q < 6; q++) c.buff_c[q] = taper_c ? taper_c[q] : 0.0;
+    c.e_lrc = e_lrc;
+    c.v_lrc = v_lrc;
+    CK(dalloc(&c.vpos4, c.n));
+    CK(dalloc(&c.vfixq, c.n));
+    CK(dalloc(&c.fv, 3 * (size_t)c.n));
+    c.graph_dirty = 1;
+    return SMD_OK;
+}
+
+int smd_set_multipole(smd_ctx *x, const double *type_mp, const double *polar, double alpha, double kcut,
+                      double real_cut, int induction, double ind_cut, double thole_a) {
+    if (!x || !type_mp || !polar || !(alpha > 0) || !(kcut > 0) || !(real_cut > 0) || x->c.n == 0)
+        return fail(x, SMD_ERR_ARG, "smd_set_multipole: bad arguments");
+    Ctx &c = x->c;
+    for (int m = 0; m < c.nmol; m++)
+        if (c.h_mol_off[m + 1] - c.h_mol_off[m] != 3)
+            return fail(x, SMD_ERR_ARG, "smd_set_multipole: molecules must be H O H triples");
+    if (real_cut > c.cutoff + 1e-12 || (induction && ind_cut > c.cutoff + 1e-12))
+        return fail(x, SMD_ERR_ARG, "smd_set_multipole: real-space and induction cutoffs must not exceed the pair-list cutoff");
+    c.mp_on = 1;
+    c.ind_on = induction ? 1 : 0;
+    c.ew_alpha = alpha;
+    c.ew_kcut = kcut;
+    c.mp_rc2 = real_cut * real_cut;
+    c.ind_cut2 = ind_cut * ind_cut;
+    c.thole_a = thole_a;
+    c.h_type_polar.assign(polar, polar + c.ntypes);
+    CK(dalloc(&c.type_mp, 9 * (size_t)c.ntypes));
+    CK(cudaMemcpy(c.type_mp, type_mp, 9 * (size_t)c.ntypes * sizeof(double), cudaMemcpyHostToDevice));
+    CK(dalloc(&c.type_polar, c.ntypes));
+    CK(cudaMemcpy(c.type_polar, polar, c.ntypes * sizeof(double), cudaMemcpyHostToDevice));
+    const size_t n = c.n;
+    CK(dalloc(&c.mu, 3 * n)); CK(dalloc(&c.qd, 6 * n)); CK(dalloc(&c.trq, 3 * n));
+    CK(dalloc(&c.e0, 3 * n)); CK(dalloc(&c.pind, 3 * n)); CK(dalloc(&c.cgw, 12 * n));
+    CK(cudaMemset(c.pind, 0, 3 * n * sizeof(double)));
+    CK(cudaMemset(c.e0, 0, 3 * n * sizeof(double)));
+    int r = setup_cg(c);
+    if (r) return fail(x, r, "smd_set_multipole: solver set-up failed");
+    CK(dalloc(&c.cgs, 8 + 4 * (size_t)c.cg_blocks));
+    CK(cudaMemset(c.cgs, 0, (8 + 4 * (size_t)c.cg_blocks) * sizeof(double)));
+    CK(dalloc(&c.cg_bar, 1));
+    r = setup_recip(c);
+    if (r) return fail(x, r, "smd_set_multipole: reciprocal set-up failed");
+    c.graph_dirty = 1;
+    return SMD_OK;
+}
+
+int smd_set_solver(smd_ctx *x, double tol, int max_iter, int guess) {
+    if (!x || !(tol > 0) || max_iter <= 0 || guess < 0 || guess > 2)
+        return fail(x, SMD_ERR_ARG, "smd_set_solver: bad arguments");
+    x->c.cg_tol = tol;
+    x->c.cg_max_iter = max_iter;
+    x->c.cg_guess = guess;
+    x->c.graph_dirty = 1;
+    return SMD_OK;
+}
+
+int smd_solver_stats(smd_ctx *x, int *iterations, double *rms_change) {
+    if (!x || !x->c.cgs) return fail(x, SMD_ERR_ARG, "smd_solver_stats: no dipole solver");
+    double s[2];
+    CK(cudaMemcpyAsync(s, x->c.cgs, sizeof(s), cudaMemcpyDeviceToHost, x->c.stream));
+    CK(cudaStreamSynchronize(x->c.stream));
+    if (iterations) *iterations = (int)s[0];
+    if (rms_change) *rms_change = s[1];
+    return SMD_OK;
+}
+
+int smd_get_polarization(smd_ctx *x, double *mu, double *quad, double *e0, double *p) {
+    if (!x || !x->c.mp_on) return fail(x, SMD_ERR_ARG, "smd_get_polarization: multipoles not set up");
+    Ctx &c = x->c;
+    const int n = c.n;
+    std::vector<double> h(6 * (size_t)n);
+    auto get = [&](const double *src, int comps, double *dst) -> int {
+        if (!dst) return SMD_OK;
+        CK(cudaMemcpyAsync(h.data(), src, comps * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+        for (int i = 0; i < n; i++)
+            for (int d = 0; d < comps; d++) dst[comps * i + d] = h[(size_t)d * n + i];
+        return SMD_OK;
+    };
+    int r;
+    if ((r = get(c.mu, 3, mu))) return r;
+    if ((r = get(c.qd, 6, quad))) return r;
+    if ((r = get(c.e0, 3, e0))) return r;
+    if ((r = get(c.pind, 3, p))) return r;
+    return SMD_OK;
+}
+
+int smd_set_induced(smd_ctx *x, const double *p) {
+    if (!x || !p || !x->c.mp_on) return fail(x, SMD_ERR_ARG, "smd_set_induced: multipoles not set up");
+    Ctx &c = x->c;
+    const int n = c.n;
+    std::vector<double> h(3 * (size_t)n);
+    for (int i = 0; i < n; i++)
+        for (int d = 0; d < 3; d++) h[(size_t)d * n + i] = p[3 * i + d];
+    CK(cudaMemcpy(c.pind, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
     return SMD_OK;
 }
 
@@ -477,6 +614,9 @@ int smd_compute_forces(smd_ctx *x, uint32_t terms, double *force, double *energy
     c.ewald_on = save_ew;
     if (want_long) launch_recip(c);
     c.vdw = save_vdw;
+    if (c.mp_on && (terms & (SMD_TERM_MP_SHORT | SMD_TERM_MP_LONG | SMD_TERM_IND_SHORT | SMD_TERM_IND_LONG)))
+        enqueue_polar(c, terms & SMD_TERM_MP_SHORT, terms & SMD_TERM_MP_LONG, terms & SMD_TERM_IND_SHORT,
+                      terms & SMD_TERM_IND_LONG);
     double *dforce = nullptr;
     if (force) {
         CK(cudaMalloc(&dforce, 3 * (size_t)c.n * sizeof(double)));
@@ -494,9 +634,13 @@ int smd_compute_forces(smd_ctx *x, uint32_t terms, double *force, double *energy
         energy[SMD_E_VDW] = (double)hacc[ACC_E_VDW] * ACC_INV + (vdw ? c.e_lrc : 0.0);
         energy[SMD_E_REAL] = (double)hacc[ACC_E_REAL] * ACC_INV;
         energy[SMD_E_LONG] = (double)hacc[ACC_E_LONG] * ACC_INV;
-        energy[SMD_E_CORRECT] = want_real ? c.e_self : 0.0;
+        energy[SMD_E_CORRECT] = (want_real ? c.e_self : 0.0) + (double)hacc[ACC_E_SELF] * ACC_INV;
         energy[SMD_E_MOLCORRECT] = (double)hacc[ACC_E_INTRA] * ACC_INV;
         energy[SMD_E_SURF] = (double)hacc[ACC_E_SURF] * ACC_INV;
+        energy[SMD_E_POL_REAL] = (double)hacc[ACC_E_POL_REAL] * ACC_INV;
+        energy[SMD_E_POL_LONG] = (double)hacc[ACC_E_POL_LONG] * ACC_INV;
+        energy[SMD_E_POL_SELF] = (double)hacc[ACC_E_POL_SELF] * ACC_INV;
+        energy[SMD_E_POL_INTRA] = (double)hacc[ACC_E_POL_INTRA] * ACC_INV;
     }
     if (virial) {
         for (int q = 0; q < 9; q++) {

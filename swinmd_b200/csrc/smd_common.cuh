@@ -37,17 +37,19 @@ __device__ __forceinline__ long long to_fix(double v, double scale) {
 // ---- accumulator slots (acc[]) ---------------------------------------------
 enum AccSlot {
     ACC_E_VDW = 0,      // LJ / Mie / BMH / buffered 14-7 pair energy
-    ACC_E_REAL = 1,     // Ewald real-space energy
-    ACC_E_LONG = 2,     // Ewald reciprocal energy
+    ACC_E_REAL = 1,     // Ewald (point-charge or multipole) real-space energy
+    ACC_E_LONG = 2,     // Ewald (point-charge or multipole) reciprocal energy
     ACC_E_INTRA = 3,    // Ewald intramolecular correction
     ACC_E_SURF = 4,     // surface-dipole correction
-    ACC_E_MP_REAL = 5,  // multipole real space
-    ACC_E_MP_LONG = 6,  // multipole reciprocal
-    ACC_E_POL = 7,      // induction energy
+    ACC_E_SELF = 5,     // multipole self energy (point-charge self energy is a constant)
+    ACC_E_POL_SELF = 6, // induced-dipole self energy
+    ACC_E_POL_REAL = 7, // induced-dipole real-space energy
     ACC_VIR = 8,        // 9 short-range virial components (XX XY XZ YX .. ZZ)
     ACC_LVIR = 17,      // 9 long-range virial components
     ACC_NPAIR = 26,     // pairs inside the short-range cutoff (both directions)
-    ACC_COUNT = 27
+    ACC_E_POL_LONG = 27,  // induced-dipole reciprocal energy
+    ACC_E_POL_INTRA = 28, // induced-dipole intramolecular correction
+    ACC_COUNT = 29
 };
 
 // ---- status word bits (ctx->status on device) --------------------------------

@@ -10,7 +10,7 @@
 
 namespace smd {
 
-enum VdwKind { VDW_NONE = 0, VDW_LJ = 1, VDW_MIE = 2, VDW_BMH = 3 };
+enum VdwKind { VDW_NONE = 0, VDW_LJ = 1, VDW_MIE = 2, VDW_BMH = 3, VDW_BUFF = 4 };
 
 // Per type pair parameters of the short-range pair term (ntypes^2 rows of 8).
 //   LJ : p0 sigma^2, p1 4 eps, p2 energy at the cutoff (shift), p3 unused
@@ -80,6 +80,34 @@ struct Ctx {
     Recip rc;
     int precision = SMD_PREC_FP64;
     int want_cells = 1;
+    // polarisable multipole model (Multipole / Induction / BuffvdWForce)
+    int mp_on = 0, ind_on = 0;
+    double mp_rc2 = 0;              // real-space cutoff^2 (cutoffEw)
+    double ind_cut2 = 0;            // cutoffInd^2
+    double thole_a = 0.39;
+    double *type_mp = nullptr;      // [ntypes][9] local dipole (3) + quadrupole (6)
+    double *type_polar = nullptr;   // [ntypes] polarisabilities (nm^3)
+    std::vector<double> h_type_polar;
+    double *mu = nullptr;           // [3][N] lab-frame dipoles (e nm)
+    double *qd = nullptr;           // [6][N] lab-frame quadrupoles (already /3)
+    long long *trq = nullptr;       // [3][N] torques, fixed point
+    double *e0 = nullptr;           // [3][N] permanent field at the sites
+    double *pind = nullptr;         // [3][N] induced dipoles
+    double *cgw = nullptr;          // CG work vectors: r, z, v, s  [4][3][N]
+    double *cgs = nullptr;          // CG scalars / partials
+    int cg_max_iter = 500;
+    double cg_tol = 2.0819e-8;      // RMS dipole change tolerance (e nm); 1e-6 D
+    int cg_guess = 0;               // 0: alpha E0, 1: previous step, 2: learned (MLP)
+    int cg_blocks = 0;
+    unsigned int *cg_bar = nullptr; // grid-barrier counter
+    // buffered 14-7 with virtual H sites
+    int buff_on = 0;
+    double buff_n = 14, buff_m = 7, buff_delta = 0.07, buff_gamma = 0.12, buff_h = 0.91;
+    double buff_c[6] = {0, 0, 0, 0, 0, 0};
+    double buff_sw = 0;             // taper start (nm)
+    double4 *vpos4 = nullptr;       // virtual site positions
+    int4 *vfixq = nullptr;          // their 32-bit box fractions
+    long long *fv = nullptr;        // [3][N] forces on the virtual sites
     int has_multisite = 0;          // some molecule has more than one site
     double *clen2 = nullptr;        // [nmol][3] squared SHAKE distances
     int fixq_from_integrate = 0;    // step graph: integrate writes fixq
@@ -111,6 +139,17 @@ void launch_integrate(Ctx &c);
 void launch_start_velocities(Ctx &c);
 void launch_finalize_forces(Ctx &c, double *f_out_dev);
 void launch_intra(Ctx &c);
+// polarisable model: term groups (each maps its own torques to forces)
+void launch_mp_short(Ctx &c);
+void launch_mp_long(Ctx &c);
+void launch_ind_solve(Ctx &c);
+void launch_ind_short(Ctx &c);
+void launch_ind_long(Ctx &c);
+void launch_torques_begin(Ctx &c);
+void launch_torques_end(Ctx &c);
+void launch_frames(Ctx &c);
+void launch_buff(Ctx &c);
+int setup_cg(Ctx &c);
 int setup_recip(Ctx &c);
 
 }  // namespace smd

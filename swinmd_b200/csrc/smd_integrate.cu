@@ -349,11 +349,15 @@ __global__ void __launch_bounds__(INT_BLOCK) k_integrate(IntArgs a) {
         o.energy[SMD_E_VDW] = (double)__ldcg(&acc[ACC_E_VDW]) * ACC_INV + a.e_lrc;
         o.energy[SMD_E_REAL] = (double)__ldcg(&acc[ACC_E_REAL]) * ACC_INV;
         o.energy[SMD_E_LONG] = (double)__ldcg(&acc[ACC_E_LONG]) * ACC_INV;
-        o.energy[SMD_E_CORRECT] = a.e_self;
+        o.energy[SMD_E_CORRECT] = a.e_self + (double)__ldcg(&acc[ACC_E_SELF]) * ACC_INV;
         o.energy[SMD_E_MOLCORRECT] = (double)__ldcg(&acc[ACC_E_INTRA]) * ACC_INV;
         o.energy[SMD_E_SURF] = (double)__ldcg(&acc[ACC_E_SURF]) * ACC_INV;
+        o.energy[SMD_E_POL_REAL] = (double)__ldcg(&acc[ACC_E_POL_REAL]) * ACC_INV;
+        o.energy[SMD_E_POL_LONG] = (double)__ldcg(&acc[ACC_E_POL_LONG]) * ACC_INV;
+        o.energy[SMD_E_POL_SELF] = (double)__ldcg(&acc[ACC_E_POL_SELF]) * ACC_INV;
+        o.energy[SMD_E_POL_INTRA] = (double)__ldcg(&acc[ACC_E_POL_INTRA]) * ACC_INV;
         double ep = 0;
-        for (int q = 0; q < 6; q++) ep += o.energy[q];
+        for (int q = 0; q < 10; q++) ep += o.energy[q];
         o.e_potential = ep;
         // virial and pressure tensors (Integrator::computePressure; SHAKE
         // virial added afterwards to the atomic tensor, LFIntegrator.cpp:805-814)

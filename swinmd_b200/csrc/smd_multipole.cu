@@ -1,0 +1,558 @@
+// Permanent multipole electrostatics of the polarisable water model
+// (Multipole::compute / compute_long, src/forces/Multipole.cpp) and the
+// torque-to-force mapping shared with the induction terms.
+//
+// Sites carry a charge, a dipole and a traceless quadrupole given in a
+// molecular local frame.  Per step:
+//   k_frames      local -> lab frame rotation (Local2Global::FrameofReference,
+//                 src/utils/Local2Global.cpp:90-225); quadrupoles are /3
+//   k_mp_real     Ewald real space over the full Verlet list with the B_n
+//                 erfc recursion and the G_n multipole invariants
+//                 (Multipole::real_term, Multipole.cpp:398-913): energy,
+//                 force and torque on the owning site
+//   k_mp_mol      self energy (:338-396) and the intramolecular erf
+//                 correction energy (:1290-1713; under constraints the
+//                 reference applies no intramolecular force or torque)
+//   k_mp_sk_* / k_mp_recip_force  reciprocal sum with the charge-quadrupole
+//                 and dipole structure factors (:951-1245)
+//   k_torque2force  torques mapped onto the H-O-H sites
+//                 (Multipole::torques2forces, :1946-2134)
+// All sums are FP64; forces and torques accumulate in 64-bit fixed point.
+#include "smd_ctx.cuh"
+#include "smd_polar.cuh"
+
+namespace smd {
+
+constexpr double COULOMBS = 138.93548501;            // src/NEMD_defs.h:98
+constexpr double SQRTCOULOMB = 11.78708976;          // src/NEMD_defs.h:97
+constexpr double SQRT_PI_D = 1.7724538509055160273;
+
+__device__ __forceinline__ V3 ld3(const double *a, int n, int i) { return v3(a[i], a[n + i], a[2 * n + i]); }
+__device__ __forceinline__ Q6 ldq(const double *a, int n, int i) {
+    return {a[i], a[n + i], a[2 * n + i], a[3 * n + i], a[4 * n + i], a[5 * n + i]};
+}
+
+// ---------------------------------------------------------------------------
+// frames
+// ---------------------------------------------------------------------------
+// Local axes per site of an H O H molecule: H sites take z along O - H and x
+// from the lab x axis (lab y when |z.x| > 0.866); O takes z along the sum of
+// the unit O->H vectors and x from the unit O->H2 vector; then
+// u = x - (x.z) z normalised, v = z x u (Local2Global.cpp:100-150).
+__global__ void k_frames(int nmol, int n, const int *mol_off, const int *mol_atoms,
+                         const double4 *pos4, const double *type_mp, double *mu, double *qd) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nmol) return;
+    const int s = mol_off[m];
+    if (mol_off[m + 1] - s != 3) return;
+    const int ih1 = mol_atoms[s], io = mol_atoms[s + 1], ih2 = mol_atoms[s + 2];
+    const double4 a = pos4[ih1], b = pos4[io], c = pos4[ih2];
+    const V3 rh1 = v3(a.x, a.y, a.z), ro = v3(b.x, b.y, b.z), rh2 = v3(c.x, c.y, c.z);
+    V3 p1[3], p2[3];
+    p1[0] = ro - rh1;
+    p2[0] = fabs(p1[0].x / len(p1[0])) > 0.8660 ? v3(0, 1, 0) : v3(1, 0, 0);
+    V3 t1 = rh1 - ro, t2 = rh2 - ro;
+    t1 = (1.0 / len(t1)) * t1;
+    t2 = (1.0 / len(t2)) * t2;
+    p1[1] = t1 + t2;
+    p2[1] = t2;
+    p1[2] = ro - rh2;
+    p2[2] = fabs(p1[2].x / len(p1[2])) > 0.8660 ? v3(0, 1, 0) : v3(1, 0, 0);
+    const int ids[3] = {ih1, io, ih2};
+    for (int q = 0; q < 3; q++) {
+        const V3 w = (1.0 / len(p1[q])) * p1[q];
+        const V3 ss = p2[q] - dot(p2[q], w) * w;
+        const V3 u = (1.0 / len(ss)) * ss;
+        const V3 v = crs(w, u);
+        const int id = ids[q];
+        const double *tp = type_mp + 9 * (int)pos4[id].w;
+        const double dx = tp[0], dy = tp[1], dz = tp[2];
+        mu[id] = u.x * dx + v.x * dy + w.x * dz;
+        mu[n + id] = u.y * dx + v.y * dy + w.y * dz;
+        mu[2 * n + id] = u.z * dx + v.z * dy + w.z * dz;
+        // Q' = R Q R^T / 3 with R = [u v w] (columns)
+        const double L[3][3] = {{tp[3], tp[4], tp[5]}, {tp[4], tp[6], tp[7]}, {tp[5], tp[7], tp[8]}};
+        const double R[3][3] = {{u.x, v.x, w.x}, {u.y, v.y, w.y}, {u.z, v.z, w.z}};
+        double G[3][3];
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) {
+                double t = 0;
+                for (int k = 0; k < 3; k++) {
+                    double inner = 0;
+                    for (int l = 0; l < 3; l++) inner += R[j][l] * L[k][l];
+                    t += R[i][k] * inner;
+                }
+                G[i][j] = t / 3.0;
+            }
+        qd[id] = G[0][0];
+        qd[n + id] = G[0][1];
+        qd[2 * n + id] = G[0][2];
+        qd[3 * n + id] = G[1][1];
+        qd[4 * n + id] = G[1][2];
+        qd[5 * n + id] = G[2][2];
+    }
+}
+
+void launch_frames(Ctx &c) {
+    k_frames<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.n, c.mol_off, c.mol_atoms, c.pos4,
+                                                         c.type_mp, c.mu, c.qd);
+}
+
+// ---------------------------------------------------------------------------
+// pair invariants of the multipole-multipole interaction (r = r_i - r_j)
+// ---------------------------------------------------------------------------
+struct MPPair {
+    double G[5];
+    V3 gG[5];   // gradients of G1..G4 (gG[0] unused)
+};
+
+__device__ __forceinline__ void mp_invariants(double qi, V3 mi, const Q6 &Qi, double qj, V3 mj,
+                                              const Q6 &Qj, V3 r, MPPair &P) {
+    const double QiI = qtr(Qi), QjI = qtr(Qj);
+    const V3 Qir = qv(Qi, r), Qjr = qv(Qj, r);
+    const double QiRij = dot(r, Qir), QjRij = dot(r, Qjr);
+    const double mir = dot(mi, r), mjr = dot(mj, r);
+    P.G[0] = qi * qj;
+    P.G[1] = qj * mir - qi * mjr - dot(mi, mj) + qj * QiI + qi * QjI;
+    P.G[2] = qj * QiRij + qi * QjRij - mir * mjr - mjr * QiI + mir * QjI - 2 * dot(mj, Qir) +
+             2 * dot(mi, Qjr) + QiI * QjI + 2 * qdd(Qi, Qj);
+    P.G[3] = mir * QjRij - mjr * QiRij + QiI * QjRij + QjI * QiRij + 4 * dot(Qir, Qjr);
+    P.G[4] = QiRij * QjRij;
+    P.gG[1] = qj * mi - qi * mj;
+    P.gG[2] = (2 * qj) * Qir - mjr * mi - mir * mj - 2.0 * qv(Qi, mj) - QiI * mj + (2 * qi) * Qjr +
+              2.0 * qv(Qj, mi) + QjI * mi;
+    P.gG[3] = (-QiRij) * mj - (2 * mjr) * Qir + QjRij * mi + (2 * mir) * Qjr + (2 * QiI) * Qjr +
+              (2 * QjI) * Qir + 4.0 * qv(Qi, Qjr) + 4.0 * qv(Qj, Qir);
+    P.gG[4] = (2 * QjRij) * Qir + (2 * QiRij) * Qjr;
+}
+
+// torque coefficients on site i (Multipole.cpp real_term, Gt1i..Gt4i)
+__device__ __forceinline__ void mp_torque_i(double qj, V3 mi, const Q6 &Qi, V3 mj, const Q6 &Qj,
+                                            V3 r, V3 Gt[5]) {
+    const V3 Qir = qv(Qi, r), Qjr = qv(Qj, r);
+    const double QjI = qtr(Qj), QjRij = dot(r, Qjr), mjr = dot(mj, r);
+    const V3 rxmi = crs(r, mi);
+    const V3 RxQi = crs(r, Qir);
+    Gt[1] = qj * rxmi - crs(mj, mi);
+    Gt[2] = (-mjr) * rxmi + 2.0 * crs(Qjr, mi) + QjI * rxmi + (2 * qj) * RxQi -
+            2.0 * crs(mj, Qir) - 2.0 * crs(r, qv(Qi, mj)) + 4.0 * qcross(Qj, Qi);
+    Gt[3] = QjRij * rxmi - (2 * mjr) * RxQi + (2 * QjI) * RxQi + 4.0 * crs(r, qv(Qi, Qjr)) +
+            4.0 * crs(Qjr, Qir);
+    Gt[4] = (2 * QjRij) * RxQi;
+}
+
+// B_n of erfc(a r)/r (Multipole.cpp:632-637); D_n of erf(a r)/r (:1495-1500)
+__device__ __forceinline__ void bn_erfc(double r2, double alpha, double B[6]) {
+    const double a2 = alpha * alpha, a2pi = 2.0 * alpha / SQRT_PI_D;
+    const double r = sqrt(r2), ex = exp(-a2 * r2);
+    B[0] = erfc(alpha * r) / r;
+    B[1] = (-B[0] - a2pi * ex) / r2;
+    B[2] = (-3 * B[1] + 2 * a2pi * a2 * ex) / r2;
+    B[3] = (-5 * B[2] - 4 * a2pi * a2 * a2 * ex) / r2;
+    B[4] = (-7 * B[3] + 8 * a2pi * a2 * a2 * a2 * ex) / r2;
+    B[5] = (-9 * B[4] - 16 * a2pi * a2 * a2 * a2 * a2 * ex) / r2;
+}
+__device__ __forceinline__ void dn_erf(double r2, double alpha, double D[6]) {
+    const double a2 = alpha * alpha, a2pi = 2.0 * alpha / SQRT_PI_D;
+    const double r = sqrt(r2), ex = exp(-a2 * r2);
+    D[0] = erf(alpha * r) / r;
+    D[1] = (-D[0] + a2pi * ex) / r2;
+    D[2] = (-3 * D[1] - 2 * a2pi * a2 * ex) / r2;
+    D[3] = (-5 * D[2] + 4 * a2pi * a2 * a2 * ex) / r2;
+    D[4] = (-7 * D[3] - 8 * a2pi * a2 * a2 * a2 * ex) / r2;
+    D[5] = (-9 * D[4] + 16 * a2pi * a2 * a2 * a2 * a2 * ex) / r2;
+}
+
+// ---------------------------------------------------------------------------
+// real space
+// ---------------------------------------------------------------------------
+struct MPArgs {
+    int n;
+    const int *nbr, *nnbr;
+    const double4 *pos4;
+    const double *mu, *qd, *tq;
+    Box box;
+    double alpha, rc2;
+    long long *frc, *trq, *acc;
+};
+
+template <int TPP>
+__global__ void __launch_bounds__(256) k_mp_real(MPArgs a) {
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gt / TPP, t = gt % TPP;
+    V3 f = v3(0, 0, 0), tau = v3(0, 0, 0);
+    double en = 0, w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (i < a.n) {
+        const double4 pi = a.pos4[i];
+        const double qi = a.tq[(int)pi.w] / SQRTCOULOMB;
+        const V3 mi = ld3(a.mu, a.n, i);
+        const Q6 Qi = ldq(a.qd, a.n, i);
+        const int cnt = a.nnbr[i];
+        for (int k = t; k < cnt; k += TPP) {
+            const int j = a.nbr[(size_t)k * a.n + i] & 0x7fffffff;
+            const double4 pj = a.pos4[j];
+            V3 r = v3(pbc1(pi.x - pj.x, a.box.L[0], a.box.half[0]),
+                      pbc1(pi.y - pj.y, a.box.L[1], a.box.half[1]),
+                      pbc1(pi.z - pj.z, a.box.L[2], a.box.half[2]));
+            const double r2 = dot(r, r);
+            if (!(r2 < a.rc2)) continue;
+            const double qj = a.tq[(int)pj.w] / SQRTCOULOMB;
+            const V3 mj = ld3(a.mu, a.n, j);
+            const Q6 Qj = ldq(a.qd, a.n, j);
+            MPPair P;
+            mp_invariants(qi, mi, Qi, qj, mj, Qj, r, P);
+            double B[6];
+            bn_erfc(r2, a.alpha, B);
+            en += P.G[0] * B[0] + P.G[1] * B[1] + P.G[2] * B[2] + P.G[3] * B[3] + P.G[4] * B[4];
+            const double radial = P.G[0] * B[1] + P.G[1] * B[2] + P.G[2] * B[3] + P.G[3] * B[4] + P.G[4] * B[5];
+            const V3 fij = -(B[1] * P.gG[1] + B[2] * P.gG[2] + B[3] * P.gG[3] + B[4] * P.gG[4]) - radial * r;
+            f = f + fij;
+            // Ensemble virial gets -sum fij_b r_a (reference omits COULOMBS here)
+            const double fr[3] = {fij.x, fij.y, fij.z}, rr[3] = {r.x, r.y, r.z};
+            for (int p = 0; p < 3; p++)
+                for (int q = 0; q < 3; q++) w[3 * p + q] -= 0.5 * fr[q] * rr[p];
+            V3 Gt[5];
+            mp_torque_i(qj, mi, Qi, mj, Qj, r, Gt);
+            tau = tau + (B[1] * Gt[1] + B[2] * Gt[2] + B[3] * Gt[3] + B[4] * Gt[4]);
+        }
+    }
+    f.x = group_sum<TPP>(f.x); f.y = group_sum<TPP>(f.y); f.z = group_sum<TPP>(f.z);
+    tau.x = group_sum<TPP>(tau.x); tau.y = group_sum<TPP>(tau.y); tau.z = group_sum<TPP>(tau.z);
+    if (i < a.n && t == 0) {
+        add_fix3(a.frc, a.n, i, f, COULOMBS);
+        add_fix3(a.trq, a.n, i, tau, COULOMBS);
+    }
+    __shared__ double s_r[8][10];
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    double vals[10] = {0.5 * en * COULOMBS, w[0], w[1], w[2], w[3], w[4], w[5], w[6], w[7], w[8]};
+    for (int q = 0; q < 10; q++) {
+        double s = warp_sum(vals[q]);
+        if (lane == 0) s_r[wp][q] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < 10) {
+        double s = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) s += s_r[q][threadIdx.x];
+        const int slot = threadIdx.x == 0 ? ACC_E_REAL : ACC_VIR + threadIdx.x - 1;
+        if (s != 0.0) atomicAdd((unsigned long long *)&a.acc[slot], (unsigned long long)to_fix(s, ACC_SCALE));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// self energy and intramolecular correction (energy only: rigid molecules)
+// ---------------------------------------------------------------------------
+__global__ void k_mp_mol(int nmol, int n, const int *mol_off, const int *mol_atoms,
+                         const int *excl_off, const int *excl, const double4 *pos4, const double *tq,
+                         const double *mu, const double *qd, Box box, double alpha, long long *acc) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    double eself = 0, eintra = 0;
+    if (m < nmol) {
+        const double a2 = alpha * alpha, a2pi = 2.0 * alpha / SQRT_PI_D;
+        const int s = mol_off[m], e = mol_off[m + 1];
+        for (int p = s; p < e; p++) {
+            const int i = mol_atoms[p];
+            const double4 pi = pos4[i];
+            const double qi = tq[(int)pi.w] / SQRTCOULOMB;
+            const V3 mi = ld3(mu, n, i);
+            const Q6 Qi = ldq(qd, n, i);
+            const double QiI = qtr(Qi), QiQi = qdd(Qi, Qi);
+            const double selfterm = qi * qi * a2pi + (dot(mi, mi) - 2 * qi * QiI) * 2 * a2pi * a2 / 3 +
+                                    (QiI * QiI + 2 * QiQi) * 4 * a2pi * a2 * a2 / 5;
+            eself += -0.5 * selfterm * COULOMBS;
+            for (int q = p + 1; q < e; q++) {
+                const int j = mol_atoms[q];
+                bool ex = false;
+                for (int k = excl_off[i]; k < excl_off[i + 1]; k++)
+                    if (excl[k] == j) { ex = true; break; }
+                if (!ex) continue;
+                const double4 pj = pos4[j];
+                V3 r = v3(pbc1(pi.x - pj.x, box.L[0], box.half[0]), pbc1(pi.y - pj.y, box.L[1], box.half[1]),
+                          pbc1(pi.z - pj.z, box.L[2], box.half[2]));
+                const double r2 = dot(r, r);
+                MPPair P;
+                mp_invariants(qi, mi, Qi, tq[(int)pj.w] / SQRTCOULOMB, ld3(mu, n, j), ldq(qd, n, j), r, P);
+                double D[6];
+                dn_erf(r2, alpha, D);
+                eintra += P.G[0] * D[0] + P.G[1] * D[1] + P.G[2] * D[2] + P.G[3] * D[3] + P.G[4] * D[4];
+            }
+        }
+    }
+    __shared__ double s_r[2][4];
+    double v0 = warp_sum(eself), v1 = warp_sum(-eintra * COULOMBS);
+    if ((threadIdx.x & 31) == 0) { s_r[0][threadIdx.x >> 5] = v0; s_r[1][threadIdx.x >> 5] = v1; }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double t = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += s_r[threadIdx.x][q];
+        atomicAdd((unsigned long long *)&acc[threadIdx.x == 0 ? ACC_E_SELF : ACC_E_INTRA],
+                  (unsigned long long)to_fix(t, ACC_SCALE));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// reciprocal space: structure factors of (q - k.Q.k) and (mu.k)
+// ---------------------------------------------------------------------------
+constexpr int MK_THREADS = 128;
+constexpr int MK_CHUNKS = 16;
+
+// partial[ch][NS][nk]; NS = 4 (qQ cos/sin, m cos/sin) or 6 (+ induced p cos/sin)
+template <int NS>
+__global__ void __launch_bounds__(MK_THREADS) k_mp_sk_partial(int n, int nk, const double4 *pos4,
+                                                              const double *kvec, const double *tq,
+                                                              const double *mu, const double *qd,
+                                                              const double *pind, double *partial) {
+    __shared__ double s_d[MK_THREADS][NS == 6 ? 14 : 11];
+    const int k = blockIdx.x * MK_THREADS + threadIdx.x;
+    const int ch = blockIdx.y;
+    const int per = (n + MK_CHUNKS - 1) / MK_CHUNKS;
+    const int s0 = ch * per, s1 = min(n, s0 + per);
+    V3 kk = v3(0, 0, 0);
+    if (k < nk) kk = v3(kvec[k], kvec[nk + k], kvec[2 * nk + k]);
+    double acc[NS];
+    for (int q = 0; q < NS; q++) acc[q] = 0;
+    for (int base = s0; base < s1; base += MK_THREADS) {
+        const int i = base + threadIdx.x;
+        __syncthreads();
+        if (i < s1) {
+            const double4 p = pos4[i];
+            s_d[threadIdx.x][0] = p.x; s_d[threadIdx.x][1] = p.y; s_d[threadIdx.x][2] = p.z;
+            s_d[threadIdx.x][3] = tq[(int)p.w] / SQRTCOULOMB;
+            s_d[threadIdx.x][4] = mu[i]; s_d[threadIdx.x][5] = mu[n + i]; s_d[threadIdx.x][6] = mu[2 * n + i];
+            // k.Q.k needs the 6 components; store them after the dipole
+            for (int q = 0; q < 6 && 7 + q < (NS == 6 ? 14 : 11); q++) s_d[threadIdx.x][7 + q] = 0;
+        }
+        __syncthreads();
+        const int cnt = min(MK_THREADS, s1 - base);
+        if (k < nk) {
+            for (int q = 0; q < cnt; q++) {
+                const int id = base + q;
+                const double a = s_d[q][0] * kk.x + s_d[q][1] * kk.y + s_d[q][2] * kk.z;
+                double sn, cs;
+                sincos(a, &sn, &cs);
+                const Q6 Qi = ldq(qd, n, id);
+                const double qk = s_d[q][3] - dot(kk, qv(Qi, kk));
+                const double mk = s_d[q][4] * kk.x + s_d[q][5] * kk.y + s_d[q][6] * kk.z;
+                acc[0] += qk * cs; acc[1] += qk * sn;
+                acc[2] += mk * cs; acc[3] += mk * sn;
+                if (NS == 6) {
+                    const double pk = pind[id] * kk.x + pind[n + id] * kk.y + pind[2 * n + id] * kk.z;
+                    acc[4] += pk * cs; acc[5] += pk * sn;
+                }
+            }
+        }
+    }
+    if (k < nk)
+        for (int q = 0; q < NS; q++) partial[((size_t)ch * NS + q) * nk + k] = acc[q];
+}
+
+// Sums over chunks in a fixed order; per-k energy and long virial.
+// mode 0: permanent (UqQ + 2 UmqQ + Umm); mode 1: induction (UmqQ' + Ump)
+template <int NS>
+__global__ void k_mp_sk_reduce(int nk, const double *partial, const double *kcoef, const double *kvec,
+                               double alphaR4, double *sk, long long *acc, int slot_e) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0, vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
+    if (k < nk) {
+        double S[NS];
+        for (int q = 0; q < NS; q++) {
+            double t = 0;
+            for (int ch = 0; ch < MK_CHUNKS; ch++) t += partial[((size_t)ch * NS + q) * nk + k];
+            S[q] = t;
+            sk[(size_t)q * nk + k] = t;
+        }
+        const double c = kcoef[k];  // 4 pi/V exp(-k^2/4a^2)/k^2
+        if (NS == 4) {
+            const double UqQ = c * (S[0] * S[0] + S[1] * S[1]);
+            const double UmqQ = c * (S[1] * S[2] - S[0] * S[3]);
+            const double Umm = c * (S[2] * S[2] + S[3] * S[3]);
+            e = (UqQ + 2 * UmqQ + Umm) * COULOMBS;
+        } else {
+            const double UmqQ = c * (S[1] * S[4] - S[0] * S[5]);
+            const double Ump = c * (S[4] * S[2] + S[5] * S[3]);
+            e = (UmqQ + Ump) * COULOMBS;
+        }
+        const double kx = kvec[k], ky = kvec[nk + k], kz = kvec[2 * nk + k];
+        const double k2 = kx * kx + ky * ky + kz * kz;
+        const double coeff = 2.0 * (alphaR4 + 1.0 / k2);
+        vxx = e - e * coeff * kx * kx;
+        vyy = e - e * coeff * ky * ky;
+        vzz = e - e * coeff * kz * kz;
+        vxy = -e * coeff * kx * ky;
+        vxz = -e * coeff * kx * kz;
+        vyz = -e * coeff * ky * kz;
+    }
+    __shared__ double s_r[7][8];
+    double v[7] = {e, vxx, vxy, vxz, vyy, vyz, vzz};
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int q = 0; q < 7; q++) {
+        double t = warp_sum(v[q]);
+        if (lane == 0) s_r[q][w] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < 7) {
+        double t = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += s_r[threadIdx.x][q];
+        const int slots[7][2] = {{slot_e, -1}, {ACC_LVIR + 0, -1}, {ACC_LVIR + 1, ACC_LVIR + 3},
+                                 {ACC_LVIR + 2, ACC_LVIR + 6}, {ACC_LVIR + 4, -1},
+                                 {ACC_LVIR + 5, ACC_LVIR + 7}, {ACC_LVIR + 8, -1}};
+        const long long fx = to_fix(t, ACC_SCALE);
+        atomicAdd((unsigned long long *)&acc[slots[threadIdx.x][0]], (unsigned long long)fx);
+        if (slots[threadIdx.x][1] >= 0)
+            atomicAdd((unsigned long long *)&acc[slots[threadIdx.x][1]], (unsigned long long)fx);
+    }
+}
+
+// Per-site reciprocal force and torque; 4 threads split the k set.
+template <int NS>
+__global__ void __launch_bounds__(256) k_mp_recip_force(int n, int nk, const double4 *pos4,
+                                                        const double *kvec, const double *kcoef,
+                                                        const double *sk, const double *tq,
+                                                        const double *mu, const double *qd,
+                                                        const double *pind, long long *frc,
+                                                        long long *trq) {
+    constexpr int TPS = 4;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gt / TPS, t = gt % TPS;
+    V3 f = v3(0, 0, 0), tau = v3(0, 0, 0);
+    if (i < n) {
+        const double4 p = pos4[i];
+        const double qi = tq[(int)p.w] / SQRTCOULOMB;
+        const V3 mi = ld3(mu, n, i);
+        const Q6 Qi = ldq(qd, n, i);
+        V3 pi = v3(0, 0, 0);
+        if (NS == 6) pi = ld3(pind, n, i);
+        for (int k = t; k < nk; k += TPS) {
+            const V3 kk = v3(kvec[k], kvec[nk + k], kvec[2 * nk + k]);
+            const double a = p.x * kk.x + p.y * kk.y + p.z * kk.z;
+            double sn, cs;
+            sincos(a, &sn, &cs);
+            const V3 Qk = qv(Qi, kk);
+            const double qk = qi - dot(kk, Qk);
+            const double c1 = qk * cs, s1 = qk * sn;
+            const double mk = dot(mi, kk), mkc = mk * cs, mks = mk * sn;
+            const double b = 2.0 * kcoef[k];
+            const double CqQ = sk[k], SqQ = sk[nk + k], Cm = sk[2 * (size_t)nk + k], Sm = sk[3 * (size_t)nk + k];
+            const V3 kxm = crs(kk, mi), KQ = crs(kk, Qk);
+            double val;
+            if (NS == 4) {
+                val = b * ((s1 * CqQ - c1 * SqQ) + (mkc * CqQ + mks * SqQ) - (c1 * Cm + s1 * Sm) +
+                           (mks * Cm - mkc * Sm));
+                tau = tau + b * ((SqQ * cs - CqQ * sn) * kxm + (Cm * cs + Sm * sn) * kxm -
+                                 2.0 * (CqQ * cs + SqQ * sn) * KQ + 2.0 * (Sm * cs - Cm * sn) * KQ);
+            } else {
+                const double Cp = sk[4 * (size_t)nk + k], Sp = sk[5 * (size_t)nk + k];
+                const double pk = dot(pi, kk), pkc = pk * cs, pks = pk * sn;
+                val = b * ((pkc * CqQ + pks * SqQ) - (c1 * Cp + s1 * Sp) +
+                           (pks * (Cm + Cp) - pkc * (Sm + Sp)) + (mks * Cp - mkc * Sp));
+                tau = tau + b * ((cs * Cp + sn * Sp) * kxm + 2.0 * (cs * Sp - sn * Cp) * KQ);
+            }
+            f = f + val * kk;
+        }
+    }
+    f.x = group_sum<TPS>(f.x); f.y = group_sum<TPS>(f.y); f.z = group_sum<TPS>(f.z);
+    tau.x = group_sum<TPS>(tau.x); tau.y = group_sum<TPS>(tau.y); tau.z = group_sum<TPS>(tau.z);
+    if (i < n && t == 0) {
+        add_fix3(frc, n, i, f, COULOMBS);
+        add_fix3(trq, n, i, tau, COULOMBS);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// torques -> forces on the H O H sites (Multipole::torques2forces)
+// ---------------------------------------------------------------------------
+__global__ void k_torque2force(int nmol, int n, const int *mol_off, const int *mol_atoms,
+                               const double4 *pos4, const long long *trq, long long *frc) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nmol) return;
+    const int s = mol_off[m];
+    if (mol_off[m + 1] - s != 3) return;
+    const int h1 = mol_atoms[s], o = mol_atoms[s + 1], h2 = mol_atoms[s + 2];
+    const double4 a = pos4[h1], b = pos4[o], c = pos4[h2];
+    const V3 rh1 = v3(a.x, a.y, a.z), ro = v3(b.x, b.y, b.z), rh2 = v3(c.x, c.y, c.z);
+    auto tq = [&](int id) {
+        return v3((double)trq[id] * FRC_INV, (double)trq[n + id] * FRC_INV, (double)trq[2 * n + id] * FRC_INV);
+    };
+    V3 fh1 = v3(0, 0, 0), fo = v3(0, 0, 0), fh2 = v3(0, 0, 0);
+    // H sites: u along H - O, v the lab x (or y) axis
+    auto hsite = [&](V3 rh, V3 tau, V3 &fh) {
+        V3 u = rh - ro;
+        const double ul = len(u);
+        V3 v = fabs(u.x / ul) > 0.8666 ? v3(0, 1, 0) : v3(1, 0, 0);
+        V3 w = crs(u, v);
+        const double wl = len(w);
+        u = (1.0 / ul) * u;
+        w = (1.0 / wl) * w;
+        const V3 vxu = crs(v, u), wxu = crs(w, u);
+        const double vxuL = len(vxu), wxuL = len(wxu);
+        const V3 dUdu = (-dot(v, tau) / (vxuL * vxuL * ul)) * vxu + (-dot(w, tau) / (wxuL * wxuL * ul)) * wxu;
+        fh = fh - dUdu;
+        fo = fo + dUdu;
+    };
+    hsite(rh1, tq(h1), fh1);
+    {   // O site: u = O - H1, v = O - H2, half weight on the w rotation
+        const V3 tau = tq(o);
+        V3 u = ro - rh1, v = ro - rh2;
+        V3 w = crs(u, v);
+        const double ul = len(u), vl = len(v), wl = len(w);
+        u = (1.0 / ul) * u;
+        v = (1.0 / vl) * v;
+        w = (1.0 / wl) * w;
+        const V3 vxu = crs(v, u), wxu = crs(w, u), wxv = crs(w, v);
+        const double vxuL = len(vxu), wxuL = len(wxu), wxvL = len(wxv);
+        const V3 dUdu = (-dot(v, tau) / (vxuL * vxuL * ul)) * vxu + (0.5 * -dot(w, tau) / (wxuL * wxuL * ul)) * wxu;
+        const V3 dUdv = (-dot(u, tau) / (vxuL * vxuL * vl)) * (-vxu) + (0.5 * -dot(w, tau) / (wxvL * wxvL * vl)) * wxv;
+        fo = fo - dUdu - dUdv;
+        fh1 = fh1 + dUdu;
+        fh2 = fh2 + dUdv;
+    }
+    hsite(rh2, tq(h2), fh2);
+    add_fix3(frc, n, h1, fh1, 1.0);
+    add_fix3(frc, n, o, fo, 1.0);
+    add_fix3(frc, n, h2, fh2, 1.0);
+}
+
+void launch_torques_begin(Ctx &c) {
+    cudaMemsetAsync(c.trq, 0, 3 * (size_t)c.n * sizeof(long long), c.stream);
+}
+
+void launch_torques_end(Ctx &c) {
+    k_torque2force<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.n, c.mol_off, c.mol_atoms,
+                                                                c.pos4, c.trq, c.frc);
+}
+
+// real space + self + intramolecular (Multipole::compute)
+void launch_mp_short(Ctx &c) {
+    MPArgs a;
+    a.n = c.n; a.nbr = c.pl.nbr; a.nnbr = c.pl.nnbr; a.pos4 = c.pos4; a.mu = c.mu; a.qd = c.qd;
+    a.tq = c.type_q; a.box = c.box; a.alpha = c.ew_alpha; a.rc2 = c.mp_rc2;
+    a.frc = c.frc; a.trq = c.trq; a.acc = c.acc;
+    const int tpp = 8;
+    const int nb = (int)(((long long)c.n * tpp + 255) / 256);
+    k_mp_real<tpp><<<nb, 256, 0, c.stream>>>(a);
+    k_mp_mol<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.n, c.mol_off, c.mol_atoms, c.excl_off,
+                                                         c.excl, c.pos4, c.type_q, c.mu, c.qd, c.box,
+                                                         c.ew_alpha, c.acc);
+}
+
+// reciprocal space (Multipole::compute_long); NS = 6 adds the induced dipoles
+template <int NS>
+static void mp_recip(Ctx &c, int slot_e) {
+    const int nk = c.rc.nk;
+    if (nk == 0) return;
+    double *partial = (double *)c.rc.sk;
+    double *sk = partial + (size_t)6 * nk * MK_CHUNKS;
+    dim3 g1((nk + MK_THREADS - 1) / MK_THREADS, MK_CHUNKS);
+    k_mp_sk_partial<NS><<<g1, MK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.rc.kvec, c.type_q, c.mu, c.qd,
+                                                        c.pind, partial);
+    k_mp_sk_reduce<NS><<<(nk + 255) / 256, 256, 0, c.stream>>>(nk, partial, c.rc.kcoef, c.rc.kvec,
+                                                               1.0 / (4.0 * c.ew_alpha * c.ew_alpha), sk,
+                                                               c.acc, slot_e);
+    const int nb = (int)(((long long)c.n * 4 + 255) / 256);
+    k_mp_recip_force<NS><<<nb, 256, 0, c.stream>>>(c.n, nk, c.pos4, c.rc.kvec, c.rc.kcoef, sk, c.type_q,
+                                                  c.mu, c.qd, c.pind, c.frc, c.trq);
+}
+
+void launch_mp_long(Ctx &c) { mp_recip<4>(c, ACC_E_LONG); }
+void launch_ind_long(Ctx &c) { mp_recip<6>(c, ACC_E_POL_LONG); }
+
+}  // namespace smd

@@ -44,6 +44,8 @@ struct PairArgs {
     int switch_on;
     double sw_rs2, sw_c1, sw_c2, sw_c3;
     double alpha, alpha2, alpha2pi, ew_rc2;
+    // buffered 14-7 (BuffvdWForce): exponents, buffers, taper
+    double bn, bm, bdelta, bgamma, bc[6], bsw2;
     long long *frc;
     long long *acc;
 };
@@ -58,6 +60,37 @@ __device__ __forceinline__ void vdw_pair(R r2, R &e, R &fs, const R *p, const Pa
     e = R(0);
     fs = R(0);
     if (VDW == VDW_NONE || same) return;
+    if (VDW == VDW_BUFF) {
+        // BuffvdWForce::compute (src/forces/BuffvdWForce.cpp:186-240):
+        // U = eps ((1+d)/(rho+d))^(n-m) ((1+g)/(rho^m+g) - 2), rho = r/sigma,
+        // 5th-order taper in r beyond the switch distance
+        const R r = sqrt(r2);
+        const R rr = r * r;
+        if (!(rr <= R(a.vdw_rc2)) || p[1] == R(0)) return;
+        const R inv_s = R(1) / p[0];
+        const R rho = r * inv_s;
+        const R rho_m = pow(rho, R(a.bm)), rho_m1 = pow(rho, R(a.bm) - R(1));
+        const R nm = R(a.bn) - R(a.bm);
+        const R par1 = (R(1) + R(a.bdelta)) / (rho + R(a.bdelta));
+        const R par2 = (R(1) + R(a.bgamma)) / (rho_m + R(a.bgamma));
+        const R par1_nm = pow(par1, nm);
+        R tmpE = p[1] * par1_nm * (par2 - R(2));
+        R tmpf = -p[1] * nm * par1_nm * (par2 - R(2)) * inv_s / (rho + R(a.bdelta)) -
+                 p[1] * par1_nm * par2 * R(a.bm) * rho_m1 * inv_s / (rho_m + R(a.bgamma));
+        if (a.switch_on && rr > R(a.bsw2)) {
+            const R r3 = rr * r, r4 = rr * rr, r5 = rr * r3;
+            const R sv = R(a.bc[5]) * r5 + R(a.bc[4]) * r4 + R(a.bc[3]) * r3 + R(a.bc[2]) * rr +
+                         R(a.bc[1]) * r + R(a.bc[0]);
+            const R dsv = R(5) * R(a.bc[5]) * r4 + R(4) * R(a.bc[4]) * r3 + R(3) * R(a.bc[3]) * rr +
+                          R(2) * R(a.bc[2]) * r + R(a.bc[1]);
+            tmpf = tmpf * sv + tmpE * dsv;
+            tmpE *= sv;
+        }
+        // the reference's f_ij = -tmpf (r_i - r_j)/r = -fs (r_j - r_i)
+        e = tmpE;
+        fs = -tmpf / r;
+        return;
+    }
     if (VDW == VDW_LJ) {
         R r = sqrt(r2);
         R rr = r * r;
@@ -333,6 +366,7 @@ static void dispatch_vdw(Ctx &c, const PairArgs &a) {
         case VDW_LJ: dispatch_tpp<R, VDW_LJ, EWALD>(c, a); break;
         case VDW_MIE: dispatch_tpp<R, VDW_MIE, EWALD>(c, a); break;
         case VDW_BMH: dispatch_tpp<R, VDW_BMH, EWALD>(c, a); break;
+        case VDW_BUFF: dispatch_tpp<R, VDW_BUFF, EWALD>(c, a); break;
         default: dispatch_tpp<R, VDW_NONE, EWALD>(c, a); break;
     }
 }
@@ -344,6 +378,52 @@ __global__ void k_fixq(int n, const double4 *pos4, int4 *fixq, Box b) {
     double4 p = pos4[i];
     fixq[i] = make_int4(frac32(p.x, b.inv[0]), frac32(p.y, b.inv[1]), frac32(p.z, b.inv[2]),
                         (int)p.w);
+}
+
+// Virtual sites of the buffered 14-7 term (BuffvdWForce::VirtualPositions,
+// src/forces/BuffvdWForce.cpp:358-385): a type-0 (H) site moves to
+// f r_H + (1 - f) r_O, with O the molecule's second site; others stay.
+__global__ void k_virtual(int nmol, const int *mol_off, const int *mol_atoms, const double4 *pos4,
+                          double f, Box b, double4 *vpos4, int4 *vfixq) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nmol) return;
+    const int s = mol_off[m], e = mol_off[m + 1];
+    const double4 po = pos4[mol_atoms[s + (e - s > 1 ? 1 : 0)]];
+    for (int k = s; k < e; k++) {
+        const int i = mol_atoms[k];
+        double4 p = pos4[i];
+        if ((int)p.w == 0 && e - s > 1) {
+            p.x = f * p.x + (1.0 - f) * po.x;
+            p.y = f * p.y + (1.0 - f) * po.y;
+            p.z = f * p.z + (1.0 - f) * po.z;
+        }
+        vpos4[i] = p;
+        vfixq[i] = make_int4(frac32(p.x, b.inv[0]), frac32(p.y, b.inv[1]), frac32(p.z, b.inv[2]), (int)p.w);
+    }
+}
+
+// Force on a virtual H site: f on H, (1 - f) on the molecule's O
+// (BuffvdWForce.cpp:257-274).  Writes the molecule's forces (first term).
+__global__ void k_buff_distribute(int nmol, int n, const int *mol_off, const int *mol_atoms,
+                                  const double4 *pos4, double f, const long long *fv, long long *frc) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nmol) return;
+    const int s = mol_off[m], e = mol_off[m + 1];
+    const int o = mol_atoms[s + (e - s > 1 ? 1 : 0)];
+    double acc[3] = {0, 0, 0};
+    for (int k = s; k < e; k++) {
+        const int i = mol_atoms[k];
+        if ((int)pos4[i].w == 0 && e - s > 1) {
+            for (int d = 0; d < 3; d++) {
+                const double v = (double)fv[d * n + i] * FRC_INV;
+                frc[d * n + i] = to_fix(f * v, FRC_SCALE);
+                acc[d] += (1.0 - f) * v;
+            }
+        } else {
+            for (int d = 0; d < 3; d++) frc[d * n + i] = fv[d * n + i];
+        }
+    }
+    for (int d = 0; d < 3; d++) frc[d * n + o] += to_fix(acc[d], FRC_SCALE);
 }
 
 void launch_fixq(Ctx &c) {
@@ -366,6 +446,19 @@ void launch_pair(Ctx &c) {
     a.alpha2pi = 2.0 * c.ew_alpha / 1.7724538509055160273;
     a.ew_rc2 = c.ew_rc2;
     a.frc = c.frc; a.acc = c.acc;
+    a.bn = c.buff_n; a.bm = c.buff_m; a.bdelta = c.buff_delta; a.bgamma = c.buff_gamma;
+    for (int q = 0; q < 6; q++) a.bc[q] = c.buff_c[q];
+    a.bsw2 = c.buff_sw * c.buff_sw;
+    const bool buff = c.vdw == VDW_BUFF;
+    if (buff) {
+        // the pair term acts between the virtual sites; their forces are
+        // handed to the real sites afterwards
+        k_virtual<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.mol_off, c.mol_atoms, c.pos4,
+                                                               c.buff_h, c.box, c.vpos4, c.vfixq);
+        a.pos4 = c.vpos4;
+        a.fixq = c.vfixq;
+        a.frc = c.fv;
+    }
     if (c.precision == SMD_PREC_MIXED) {
         if (!c.fixq_from_integrate) launch_fixq(c);
         if (c.ewald_on) dispatch_vdw<float, true>(c, a);
@@ -374,6 +467,9 @@ void launch_pair(Ctx &c) {
         if (c.ewald_on) dispatch_vdw<double, true>(c, a);
         else dispatch_vdw<double, false>(c, a);
     }
+    if (buff)
+        k_buff_distribute<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.n, c.mol_off, c.mol_atoms,
+                                                                       c.pos4, c.buff_h, c.fv, c.frc);
 }
 
 }  // namespace smd

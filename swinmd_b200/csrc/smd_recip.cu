@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(256) k_recip_force(int n, int nk, const double
 
 int setup_recip(Ctx &c) {
     const double PI = 3.14159265358979323846;
-    if (!c.ewald_on || c.box.L[0] <= 0) return 0;
+    if (!(c.ewald_on || c.mp_on) || c.box.L[0] <= 0) return 0;
     const double kCut = c.ew_kcut, kCut2 = kCut * kCut;
     const double alpha2 = c.ew_alpha * c.ew_alpha, alphaR4 = 1.0 / (4.0 * alpha2);
     const int nxMax = (int)(kCut * c.box.L[0] / (2 * PI));
@@ -254,7 +254,7 @@ int setup_recip(Ctx &c) {
         return cudaMalloc((void **)p, (cnt ? cnt : 1) * sizeof(**p)) == cudaSuccess;
     };
     if (!realloc(&c.rc.kn, 3 * (size_t)nk) || !realloc(&c.rc.kvec, 3 * (size_t)nk) ||
-        !realloc(&c.rc.kcoef, (size_t)nk) || !realloc(&c.rc.sk, 2 * (size_t)nk * RK_CHUNKS + 2 * (size_t)nk))
+        !realloc(&c.rc.kcoef, (size_t)nk) || !realloc(&c.rc.sk, 6 * (size_t)nk * RK_CHUNKS + 6 * (size_t)nk))
         return SMD_ERR_CUDA;
     if (nk) {
         cudaMemcpy(c.rc.kn, kn.data(), kn.size() * sizeof(int), cudaMemcpyHostToDevice);

@@ -119,6 +119,95 @@ def lj_long_range_correction(s: System) -> tuple:
     return e_lrc, -2.0 * e_lrc
 
 
+def buff_table(s: System) -> np.ndarray:
+    """Pair parameters of the buffered 14-7 term as
+    ``BuffvdWForce::set_buff_param`` mixes them (src/forces/BuffvdWForce.cpp:
+    392-433): cubic-mean sigma, HHG epsilon; pairs with a zero epsilon get
+    sigma 1e-7 and epsilon 0.  Returns [nt, nt, 2] = (sigma, eps)."""
+    nt = len(s.atom_types)
+    out = np.zeros((nt, nt, 2))
+    for i, a in enumerate(s.atom_types):
+        for j, b in enumerate(s.atom_types):
+            if a.eps == 0 or b.eps == 0:
+                out[i, j] = (0.0000001, 0.0)
+                continue
+            si2, sj2 = a.sigma * a.sigma, b.sigma * b.sigma
+            es = math.sqrt(a.eps) + math.sqrt(b.eps)
+            out[i, j, 0] = (si2 * a.sigma + sj2 * b.sigma) / (si2 + sj2)
+            out[i, j, 1] = (4.0 * a.eps * b.eps) / (es * es)
+    return out
+
+
+def buff_taper(rc: float, sd: float) -> np.ndarray:
+    """Coefficients c0..c5 of the 5th-order taper in r
+    (BuffvdWForce.cpp:60-73)."""
+    rc2, sd2 = rc * rc, sd * sd
+    off = rc - sd
+    den = off ** 5
+    return np.array([rc * rc2 * (rc2 - 5.0 * rc * sd + 10.0 * sd2) / den,
+                     -30.0 * rc2 * sd2 / den,
+                     30.0 * (rc2 * sd + rc * sd2) / den,
+                     -10.0 * (rc2 + 4.0 * rc * sd + sd2) / den,
+                     15.0 * (rc + sd) / den,
+                     -6.0 / den])
+
+
+def _buff_pot(r, sigma, eps, n, m, delta, gamma):
+    """BuffvdWForce::potFunc (BuffvdWForce.cpp:435-463) on an array of r."""
+    if eps == 0:
+        return np.zeros_like(r), np.zeros_like(r)
+    inv = 1.0 / sigma
+    rho = r * inv
+    rho_m, rho_m1 = rho ** m, rho ** (m - 1.0)
+    nm = n - m
+    par1 = (1.0 + delta) / (rho + delta)
+    par2 = (1.0 + gamma) / (rho_m + gamma)
+    p1 = par1 ** nm
+    e = eps * p1 * (par2 - 2.0)
+    f = -eps * nm * p1 * (par2 - 2.0) * inv / (rho + delta) - eps * p1 * par2 * m * rho_m1 * inv / (rho_m + gamma)
+    return e, f
+
+
+def buff_long_range_correction(s: System, box: float) -> tuple:
+    """``BuffvdWForce::long_range_correct`` (BuffvdWForce.cpp:468-601): the
+    trapezoid rule with 2^20 intervals of r^2 U(r) and r^3 U'(r) from the
+    cutoff to 5000 nm, averaged over type pairs.  Returns (e_lrc, v_lrc)."""
+    c = s.config
+    tab = buff_table(s)
+    nt = len(s.atom_types)
+    counts = np.bincount(s.atom_type, minlength=nt)
+    rc = c.cutoff
+    vol = box ** 3
+    level = 20
+    h = (5000.0 - rc) / 2.0 ** level
+    k = np.arange(1, 2 ** level, dtype=np.float64)
+    r_in = rc + k * h
+    U = P = 0.0
+    npair = 0
+    for i in range(nt):
+        for j in range(i, nt):
+            nij = int(counts[i] * counts[j]) if i != j else int(counts[i] * (counts[i] - 1) * 0.5)
+            npair += nij
+            sig, eps = tab[i, j]
+            e0, f0 = _buff_pot(np.array([rc]), sig, eps, c.n_buff, c.m_buff, c.delta_buff, c.gamma_buff)
+            e1, f1 = _buff_pot(np.array([5000.0]), sig, eps, c.n_buff, c.m_buff, c.delta_buff, c.gamma_buff)
+            ei, fi = _buff_pot(r_in, sig, eps, c.n_buff, c.m_buff, c.delta_buff, c.gamma_buff)
+            sumU = 0.5 * h * rc * rc * e0[0] + float(np.sum(h * r_in * r_in * ei)) + \
+                0.5 * h * 5000.0 ** 2 * e1[0]
+            sumP = 0.5 * h * rc * rc * rc * f0[0] + float(np.sum(h * r_in * r_in * r_in * fi)) + \
+                0.5 * h * 5000.0 ** 3 * f1[0]
+            U += nij * sumU
+            P += nij * sumP
+    if npair <= 0:
+        return 0.0, 0.0
+    U /= npair
+    P /= npair
+    N = s.n_atoms
+    e_lrc = 2.0 * math.pi * N * N / vol * U
+    dU = 2.0 * math.pi * N * N / (vol * vol) * P / 3.0
+    return e_lrc, dU * vol
+
+
 # ---------------------------------------------------------------------------
 # the GPU system
 # ---------------------------------------------------------------------------
@@ -159,6 +248,19 @@ class GpuEnsemble:
             from .systems import constraint_lengths
             cl = np.ascontiguousarray(constraint_lengths(s).reshape(-1))
             self._chk(self.lib.smd_set_constraints(ctx, L.dptr(cl)))
+        if c.compute_buff:
+            tab = np.ascontiguousarray(buff_table(s).reshape(-1))
+            tap = buff_taper(c.cutoff, c.switch_dist)
+            e_lrc, v_lrc = buff_long_range_correction(s, self.box) if c.long_correct else (0.0, 0.0)
+            self._chk(self.lib.smd_set_buff(ctx, L.dptr(tab), float(c.n_buff), float(c.m_buff),
+                                            c.delta_buff, c.gamma_buff, c.h_factor, int(c.switch_on),
+                                            c.switch_dist, L.dptr(tap), e_lrc, v_lrc))
+        if c.compute_multipole:
+            mp = np.ascontiguousarray([[*t.dip, *t.quad] for t in s.atom_types], np.float64).reshape(-1)
+            pol = np.ascontiguousarray([t.polar for t in s.atom_types], np.float64)
+            self._chk(self.lib.smd_set_multipole(ctx, L.dptr(mp), L.dptr(pol), c.alpha, c.k_cutoff,
+                                                 c.cutoff_ew, int(c.compute_induction), c.cutoff_ind,
+                                                 c.a_damping))
         self.set_precision(precision)
         if threads_per_site:
             self._chk(self.lib.smd_set_tuning(ctx, threads_per_site))
@@ -253,6 +355,26 @@ class GpuEnsemble:
         nk = ctypes.c_int()
         self._chk(self.lib.smd_ewald_nk(self.ctx, ctypes.byref(nk)))
         return nk.value
+
+    def set_solver(self, tol: float = 2.0819e-8, max_iter: int = 500, guess: int = L.GUESS_DIRECT):
+        self._chk(self.lib.smd_set_solver(self.ctx, tol, max_iter, guess))
+
+    def solver_stats(self):
+        it = ctypes.c_int()
+        rms = ctypes.c_double()
+        self._chk(self.lib.smd_solver_stats(self.ctx, ctypes.byref(it), ctypes.byref(rms)))
+        return it.value, rms.value
+
+    def polarization(self):
+        n = self.n
+        mu, q, e0, p = np.zeros(3 * n), np.zeros(6 * n), np.zeros(3 * n), np.zeros(3 * n)
+        self._chk(self.lib.smd_get_polarization(self.ctx, L.dptr(mu), L.dptr(q), L.dptr(e0), L.dptr(p)))
+        return {"mu": mu.reshape(-1, 3), "quad": q.reshape(-1, 6), "e0": e0.reshape(-1, 3),
+                "p": p.reshape(-1, 3)}
+
+    def set_induced(self, p: np.ndarray):
+        pp = np.ascontiguousarray(p, np.float64).reshape(-1)
+        self._chk(self.lib.smd_set_induced(self.ctx, L.dptr(pp)))
 
 
 # ---------------------------------------------------------------------------
@@ -358,3 +480,33 @@ class LFIntegrator:
         L.check(self.ens.ctx, self.ens.lib.smd_get_series(self.ens.ctx, L.dptr(out),
                                                           self.series_capacity, ctypes.byref(cnt)))
         return out[:5 * cnt.value].reshape(-1, 5)
+
+
+class BuffvdWForce(GpuForce):
+    """``BuffvdWForce::compute`` (src/forces/BuffvdWForce.cpp:93-343)."""
+    terms = L.TERM_VDW
+    energy_index = L.E_VDW
+
+
+class Multipole(GpuForce):
+    """``Multipole::compute`` (self + real + intramolecular,
+    src/forces/Multipole.cpp:163-205) and ``compute_long`` (:207-222)."""
+    terms = L.TERM_MP_SHORT
+    energy_index = L.E_REAL
+
+    def compute_long(self):
+        f, e, w = self.ens.compute_forces(L.TERM_MP_LONG)
+        self.long_force, self.long_energy, self.long_virial = f, float(e[L.E_LONG]), w
+        return f
+
+
+class Induction(GpuForce):
+    """``Induction::compute`` (dipole solve, self, real, intramolecular,
+    src/forces/Induction.cpp:486-565) and ``compute_long`` (:567-590)."""
+    terms = L.TERM_IND_SHORT
+    energy_index = L.E_POL_REAL
+
+    def compute_long(self):
+        f, e, w = self.ens.compute_forces(L.TERM_IND_LONG)
+        self.long_force, self.long_energy, self.long_virial = f, float(e[L.E_POL_LONG]), w
+        return f

@@ -455,6 +455,47 @@ def spce_water(nmol: int = 2160, box: float = 4.03, seed: int = 1, temperature: 
                   bond_params=[(0, 1, 0.1, 345000.0)], angle_params=[(0, 1, 0, 109.47, 383.0)])
 
 
+def polarizable_water(nmol: int = 4096, density_gcc: float = 0.997, seed: int = 1,
+                      temperature: float = 298.0, cutoff: float = 0.9, skin: float = 0.1,
+                      switch: float = 0.8, alpha: float = 3.5, kmax: int = 20, dt: float = 0.001,
+                      tol: float = 1e-8, a_damping: float = 0.39, n_steps: int = 1000) -> System:
+    """Rigid polarisable multipole water with the site parameters of the
+    reference's shipped test model (charges, local-frame dipoles and
+    traceless quadrupoles, isotropic polarisabilities, buffered 14-7 on O and
+    H with the H sites pulled towards O by 0.91): H O H sites, molecule name
+    WAT, SHAKE on r_OH = 0.09572 nm and HOH = 108.5 deg, Ewald for the
+    multipoles with |n| < kmax, Thole-damped induction solved each step."""
+    rng = np.random.default_rng(seed)
+    m_h, m_o = 1.008, 15.999
+    mass_g = nmol * (2 * m_h + m_o) / 6.02214076e23
+    box = (mass_g / density_gcc) ** (1.0 / 3.0) * 1e7
+    pos = _place_waters(nmol, box, 0.09572, 108.5, rng, np.array([m_h, m_o, m_h]), min_dist=0.18)
+    pos = _wrap(pos, box)
+    typ = np.tile(np.array([0, 1, 0], np.int32), nmol)
+    mol = np.repeat(np.arange(nmol, dtype=np.int32), 3)
+    bonds = np.array([[3 * m + a, 3 * m + b, 0] for m in range(nmol) for a, b in ((0, 1), (1, 2))], np.int32)
+    angles = np.array([[3 * m, 3 * m + 1, 3 * m + 2, 0] for m in range(nmol)], np.int32)
+    kcut = 2 * math.pi * math.sqrt(kmax * kmax - 0.5) / box
+    cfg = Config(seed=seed, timestep=dt, n_steps=n_steps, temperature=temperature, coupl_const=0.5,
+                 cutoff=cutoff, cutoff_ew=cutoff, cut_buffer=skin, compute_ewald=False,
+                 alpha=alpha, k_cutoff=kcut, switch_on=True, switch_dist=switch, constraint=2,
+                 tolerance=tol, max_count=1000, long_correct=True, compute_multipole=True,
+                 compute_induction=True, compute_torques=True, damp_induction=True,
+                 induction_min=True, damp_amoeba=False, cutoff_ind=cutoff, a_damping=a_damping,
+                 compute_buff=True, n_buff=14, m_buff=7, delta_buff=0.07, gamma_buff=0.12,
+                 h_factor=0.91)
+    types = [AtomType(m_h, 0.25983, 0.0565245, 0.2655, dip=(-0.002042095, 0.0, -0.003078753),
+                      quad=(-0.0001028545, 0.0, -5.684578967e-06, -0.000300723, 0.0, 0.0004035771),
+                      polar=0.000496, name="H", long_name="Hydrogen"),
+             AtomType(m_o, -0.51966, 0.46057, 0.3405, dip=(0.0, 0.0, 0.0075561214),
+                      quad=(0.0010620922, 0.0, 0.0, -0.00117077124, 0.0, 0.000108679),
+                      polar=0.000837, name="O", long_name="Oxygen")]
+    return System(name=f"polwater{nmol}", pos=pos, box=(box, box, box), atom_types=types,
+                  atom_type=typ, mol_id=mol, mol_type_names=[("WAT", 3)],
+                  mol_type=np.zeros(nmol, np.int32), config=cfg, bonds=bonds, angles=angles,
+                  bond_params=[(0, 1, 0.09572, 221743.52)], angle_params=[(0, 1, 0, 108.5, 142.56735)])
+
+
 def constraint_lengths(s: System) -> np.ndarray:
     """Squared constraint lengths per molecule for the cyclic 3-site SHAKE
     (LFIntegrator::initialise, src/integrators/LFIntegrator.cpp:156-167):

@@ -40,7 +40,14 @@ def spce512():
     return s, [("forces",), ("run", 20)]
 
 
-CASES = {"lj500": lj500, "nacl1000_mie": nacl1000_mie, "spce512": spce512}
+def polwater216():
+    s = systems.polarizable_water(nmol=216, cutoff=0.9, switch=0.8, alpha=3.5, kmax=7, seed=3,
+                                  n_steps=10)
+    return s, [("forces",), ("run", 10)]
+
+
+CASES = {"lj500": lj500, "nacl1000_mie": nacl1000_mie, "spce512": spce512,
+         "polwater216": polwater216}
 
 
 def pack(name, s, results):
