@@ -179,6 +179,33 @@ int smd_solver_stats(smd_ctx *ctx, int *iterations, double *rms_change);
 int smd_get_polarization(smd_ctx *ctx, double *mu, double *quad, double *e0, double *p);
 /* Induced dipoles to start the next solve from (SMD_GUESS_PREVIOUS/LEARNED). */
 int smd_set_induced(smd_ctx *ctx, const double *p);
+
+/* ---- learned initial guess of the induced dipoles (no reference code) ----
+ * A per-site network (20 rotation-invariant inputs from the permanent field
+ * and the neighbour distances, 2 hidden layers of 64, tanh) predicts
+ * p - alpha E0 in the site's own axes; the dipole solve then iterates from
+ * that guess to the same tolerance.  Training rows are the solver's own
+ * converged dipoles. */
+/* Allocates the network (seeded weights) and room for capacity_frames
+ * configurations of training rows. */
+int smd_mlp_init(smd_ctx *ctx, int capacity_frames, unsigned int seed);
+/* Appends the current configuration's rows (features and the converged
+ * dipoles of the last force evaluation). */
+int smd_mlp_collect(smd_ctx *ctx);
+/* Adam on the mean-squared error over all collected rows; *loss receives the
+ * final error on one batch.  Marks the network ready for SMD_GUESS_LEARNED. */
+int smd_mlp_train(smd_ctx *ctx, int epochs, int batch, double lr, unsigned int seed, double *loss);
+/* Parameters (weights, then feature mean and 1/std): get and/or set;
+ * *count receives their number. */
+int smd_mlp_params(smd_ctx *ctx, float *get, const float *set, int *count);
+/* Network output (3 per row) for raw feature rows (20 per row). */
+int smd_mlp_eval(smd_ctx *ctx, const float *features, int rows, float *out);
+/* Gradient of the batch loss for the given rows (20 features + 3 targets
+ * each) at the current parameters; replaces the collected training rows. */
+int smd_mlp_gradient(smd_ctx *ctx, const float *rows_data, int rows, float *grad);
+/* Raw features (20 per site) of the current configuration, from the field
+ * of the last evaluation. */
+int smd_mlp_features(smd_ctx *ctx, float *features);
 int smd_set_precision(smd_ctx *ctx, int mode);
 /* Pair-kernel threads per site (1..32, power of two); 0 lets the library pick. */
 int smd_set_tuning(smd_ctx *ctx, int threads_per_site);
@@ -224,7 +251,10 @@ int smd_get_series(smd_ctx *ctx, double *out, int cap, int *count);
 /* Average device time (ms, CUDA events on the context's stream) of each
  * stage of one step, each launched `reps` times on its own:
  * out[0] pair kernel, out[1] reciprocal kernels, out[2] integrate kernel,
- * out[3] a forced pair-list rebuild.  Leaves forces and state unchanged
+ * out[3] a forced pair-list rebuild; for the polarisable model out[4] frames,
+ * out[5] multipole real+self+intra, out[6] multipole reciprocal, out[7]
+ * field + dipole solve, out[8] induced real+self+intra, out[9] induced
+ * reciprocal (out has room for 10).  Leaves forces and state unchanged
  * except for the rebuilt list. */
 int smd_profile_stages(smd_ctx *ctx, int reps, double *out);
 /* smd_run with the device time of the nsteps graph launches (CUDA events on

@@ -54,6 +54,7 @@ class Observables(ctypes.Structure):
 _P = ctypes.c_void_p
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int32)
+_F = ctypes.POINTER(ctypes.c_float)
 
 # name: (restype, argtypes)
 SIGNATURES = {
@@ -95,6 +96,13 @@ SIGNATURES = {
     "smd_solver_stats": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), _D]),
     "smd_get_polarization": (ctypes.c_int, [_P, _D, _D, _D, _D]),
     "smd_set_induced": (ctypes.c_int, [_P, _D]),
+    "smd_mlp_init": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_uint]),
+    "smd_mlp_collect": (ctypes.c_int, [_P]),
+    "smd_mlp_train": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_uint, _D]),
+    "smd_mlp_params": (ctypes.c_int, [_P, _F, _F, ctypes.POINTER(ctypes.c_int)]),
+    "smd_mlp_eval": (ctypes.c_int, [_P, _F, ctypes.c_int, _F]),
+    "smd_mlp_gradient": (ctypes.c_int, [_P, _F, ctypes.c_int, _F]),
+    "smd_mlp_features": (ctypes.c_int, [_P, _F]),
 }
 
 _lib = None
@@ -122,6 +130,10 @@ def dptr(a):
 
 def iptr(a):
     return a.ctypes.data_as(_I) if a is not None else None
+
+
+def fptr(a):
+    return a.ctypes.data_as(_F) if a is not None else None
 
 
 def check(ctx, code):

@@ -121,11 +121,21 @@ void enqueue_polar(Ctx &c, bool mp_short, bool mp_long, bool ind_short, bool ind
     launch_frames(c);
     launch_torques_begin(c);
     if (mp_short) launch_mp_short(c);
-    if (mp_long) launch_mp_long(c);
-    if (c.ind_on && (ind_short || ind_long)) {
+    const bool all = mp_short && mp_long && ind_short && ind_long && c.ind_on;
+    if (all) {
+        // a full evaluation: the permanent structure factors are summed
+        // before the solve, and one reciprocal force pass serves both terms
+        launch_mp_long_sums(c);
         launch_ind_solve(c);
-        if (ind_short) launch_ind_short(c);
-        if (ind_long) launch_ind_long(c);
+        launch_ind_short(c);
+        launch_polar_long_rest(c);
+    } else {
+        if (mp_long) launch_mp_long(c);
+        if (c.ind_on && (ind_short || ind_long)) {
+            launch_ind_solve(c);
+            if (ind_short) launch_ind_short(c);
+            if (ind_long) launch_ind_long(c);
+        }
     }
     launch_torques_end(c);
 }
@@ -461,6 +471,7 @@ int smd_set_multipole(smd_ctx *x, const double *type_mp, const double *polar, do
     const size_t n = c.n;
     CK(dalloc(&c.mu, 3 * n)); CK(dalloc(&c.qd, 6 * n)); CK(dalloc(&c.trq, 3 * n));
     CK(dalloc(&c.e0, 3 * n)); CK(dalloc(&c.pind, 3 * n)); CK(dalloc(&c.cgw, 12 * n));
+    CK(dalloc(&c.frame, 9 * n));
     CK(cudaMemset(c.pind, 0, 3 * n * sizeof(double)));
     CK(cudaMemset(c.e0, 0, 3 * n * sizeof(double)));
     int r = setup_cg(c);
@@ -524,6 +535,131 @@ int smd_set_induced(smd_ctx *x, const double *p) {
         for (int d = 0; d < 3; d++) h[(size_t)d * n + i] = p[3 * i + d];
     CK(cudaMemcpy(c.pind, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
     return SMD_OK;
+}
+
+// ---- dipole-guess network ------------------------------------------------
+int smd_mlp_init(smd_ctx *x, int capacity_frames, unsigned int seed) {
+    if (!x || !x->c.ind_on || capacity_frames <= 0)
+        return fail(x, SMD_ERR_ARG, "smd_mlp_init: set up the induction model first");
+    Ctx &c = x->c;
+    int r = mlp_alloc(c, (long long)capacity_frames * c.n, seed);
+    if (r) return fail(x, r, "smd_mlp_init: allocation failed");
+    c.mlp_ready = 0;
+    c.graph_dirty = 1;
+    return SMD_OK;
+}
+
+int smd_mlp_collect(smd_ctx *x) {
+    if (!x || !x->c.mlp_data) return fail(x, SMD_ERR_ARG, "smd_mlp_collect: call smd_mlp_init first");
+    Ctx &c = x->c;
+    if (c.mlp_rows + c.n > c.mlp_cap) return fail(x, SMD_ERR_ARG, "smd_mlp_collect: training buffer full");
+    launch_mlp_collect(c);
+    c.mlp_rows += c.n;
+    return sync_status(x);
+}
+
+int smd_mlp_train(smd_ctx *x, int epochs, int batch, double lr, unsigned int seed, double *loss) {
+    if (!x || !x->c.mlp_data || x->c.mlp_rows == 0 || epochs <= 0 || batch <= 0 || batch > mlp_max_batch())
+        return fail(x, SMD_ERR_ARG, "smd_mlp_train: no rows collected or bad batch size");
+    Ctx &c = x->c;
+    const long long rows = c.mlp_rows;
+    if (c.mlp_t == 0) launch_mlp_norm(c);
+    std::vector<unsigned int> perm(rows);
+    unsigned int *dperm = nullptr;
+    CK(cudaMalloc(&dperm, rows * sizeof(unsigned int)));
+    unsigned long long s = 0x9E3779B97F4A7C15ull ^ seed;
+    for (int ep = 0; ep < epochs; ep++) {
+        for (long long k = 0; k < rows; k++) perm[k] = (unsigned int)k;
+        for (long long k = rows - 1; k > 0; k--) {  // Fisher-Yates with an xorshift generator
+            s ^= s << 13; s ^= s >> 7; s ^= s << 17;
+            long long j = (long long)(s % (unsigned long long)(k + 1));
+            unsigned int t = perm[k]; perm[k] = perm[j]; perm[j] = t;
+        }
+        CK(cudaMemcpyAsync(dperm, perm.data(), rows * sizeof(unsigned int), cudaMemcpyHostToDevice, c.stream));
+        for (long long r0 = 0; r0 + batch <= rows; r0 += batch) launch_mlp_step(c, dperm, r0, batch, (float)lr, nullptr);
+        CK(cudaStreamSynchronize(c.stream));
+    }
+    if (loss) {  // mean-squared error over (up to) the first max-batch rows of the last order
+        const int b = (int)std::min<long long>(rows, mlp_max_batch());
+        launch_mlp_step(c, dperm, 0, b, 0.f, c.mlp_part + (size_t)64 * mlp_nparam() + 64);
+        std::vector<float> lp(64);
+        const int nb = (b + 255) / 256;
+        CK(cudaMemcpyAsync(lp.data(), c.mlp_part + (size_t)64 * mlp_nparam(), nb * sizeof(float),
+                           cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+        double t = 0;
+        for (int q = 0; q < nb; q++) t += lp[q];
+        *loss = t;
+    }
+    cudaFree(dperm);
+    c.mlp_ready = 1;
+    c.graph_dirty = 1;
+    return sync_status(x);
+}
+
+int smd_mlp_params(smd_ctx *x, float *get, const float *set, int *count) {
+    if (!x || !x->c.mlp_w) return fail(x, SMD_ERR_ARG, "smd_mlp_params: call smd_mlp_init first");
+    Ctx &c = x->c;
+    const int np = mlp_nparam(), nf = mlp_nfeat();
+    if (count) *count = np + 2 * nf;
+    if (get) {
+        CK(cudaMemcpy(get, c.mlp_w, np * sizeof(float), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(get + np, c.mlp_norm, 2 * nf * sizeof(float), cudaMemcpyDeviceToHost));
+    }
+    if (set) {
+        CK(cudaMemcpy(c.mlp_w, set, np * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(c.mlp_norm, set + np, 2 * nf * sizeof(float), cudaMemcpyHostToDevice));
+        c.mlp_ready = 1;
+        c.mlp_t = std::max(c.mlp_t, 1);
+    }
+    return SMD_OK;
+}
+
+int smd_mlp_eval(smd_ctx *x, const float *feat, int rows, float *out) {
+    if (!x || !x->c.mlp_w || !feat || !out || rows <= 0) return fail(x, SMD_ERR_ARG, "smd_mlp_eval: bad arguments");
+    Ctx &c = x->c;
+    float *dx = nullptr, *dy = nullptr;
+    CK(cudaMalloc(&dx, (size_t)rows * mlp_nfeat() * sizeof(float)));
+    CK(cudaMalloc(&dy, (size_t)rows * 3 * sizeof(float)));
+    CK(cudaMemcpy(dx, feat, (size_t)rows * mlp_nfeat() * sizeof(float), cudaMemcpyHostToDevice));
+    launch_mlp_eval(c, rows, dx, dy);
+    CK(cudaMemcpyAsync(out, dy, (size_t)rows * 3 * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    int r = sync_status(x);
+    cudaFree(dx);
+    cudaFree(dy);
+    return r;
+}
+
+int smd_mlp_gradient(smd_ctx *x, const float *rows_data, int rows, float *grad) {
+    if (!x || !x->c.mlp_data || !rows_data || !grad || rows <= 0 || rows > mlp_max_batch() ||
+        rows > x->c.mlp_cap)
+        return fail(x, SMD_ERR_ARG, "smd_mlp_gradient: bad arguments");
+    Ctx &c = x->c;
+    const int w = mlp_nfeat() + 3;
+    CK(cudaMemcpy(c.mlp_data, rows_data, (size_t)rows * w * sizeof(float), cudaMemcpyHostToDevice));
+    c.mlp_rows = rows;
+    std::vector<unsigned int> perm(rows);
+    for (int k = 0; k < rows; k++) perm[k] = k;
+    unsigned int *dperm = nullptr;
+    float *dg = nullptr;
+    CK(cudaMalloc(&dperm, rows * sizeof(unsigned int)));
+    CK(cudaMalloc(&dg, mlp_nparam() * sizeof(float)));
+    CK(cudaMemcpy(dperm, perm.data(), rows * sizeof(unsigned int), cudaMemcpyHostToDevice));
+    launch_mlp_step(c, dperm, 0, rows, 0.f, dg);
+    CK(cudaMemcpyAsync(grad, dg, mlp_nparam() * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    int r = sync_status(x);
+    cudaFree(dperm);
+    cudaFree(dg);
+    c.mlp_rows = 0;
+    return r;
+}
+
+int smd_mlp_features(smd_ctx *x, float *feat) {
+    if (!x || !x->c.mlp_x || !feat) return fail(x, SMD_ERR_ARG, "smd_mlp_features: call smd_mlp_init first");
+    Ctx &c = x->c;
+    launch_mlp_features(c);
+    CK(cudaMemcpyAsync(feat, c.mlp_x, (size_t)c.n * mlp_nfeat() * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    return sync_status(x);
 }
 
 int smd_set_precision(smd_ctx *x, int mode) {
@@ -798,6 +934,28 @@ int smd_profile_stages(smd_ctx *x, int reps, double *out) {
     CK(cudaMemcpyAsync(c.obs, &o_save, sizeof(o_save), cudaMemcpyHostToDevice, c.stream));
     CK(cudaMemcpyAsync(c.scal, sc_save, sizeof(sc_save), cudaMemcpyHostToDevice, c.stream));
     out[3] = timed([&] { launch_nlist(c, true); });
+    for (int q = 4; q < 10; q++) out[q] = 0.0;
+    if (c.mp_on) {
+        out[4] = timed([&] { launch_frames(c); launch_torques_begin(c); });
+        out[5] = timed([&] { launch_mp_short(c); });
+        out[6] = timed([&] { c.ind_on ? launch_mp_long_sums(c) : launch_mp_long(c); });
+        if (c.ind_on) {
+            const int guess = c.cg_guess;
+            if (guess == 0) {
+                out[7] = timed([&] { launch_ind_solve(c); });
+            } else {
+                // a warm start must start from the same dipoles every time
+                std::vector<double> p0(3 * (size_t)c.n);
+                CK(cudaMemcpy(p0.data(), c.pind, p0.size() * sizeof(double), cudaMemcpyDeviceToHost));
+                out[7] = timed([&] {
+                    cudaMemcpyAsync(c.pind, p0.data(), p0.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream);
+                    launch_ind_solve(c);
+                });
+            }
+            out[8] = timed([&] { launch_ind_short(c); });
+            out[9] = timed([&] { launch_polar_long_rest(c); });
+        }
+    }
     // forces for the current positions again, accumulators clear
     CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
     enqueue_forces(c);

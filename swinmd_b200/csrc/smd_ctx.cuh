@@ -100,6 +100,17 @@ struct Ctx {
     int cg_guess = 0;               // 0: alpha E0, 1: previous step, 2: learned (MLP)
     int cg_blocks = 0;
     unsigned int *cg_bar = nullptr; // grid-barrier counter
+    double *frame = nullptr;        // [9][N] site axes u, v, w (lab frame)
+    // per-site network giving the initial induced dipoles (smd_mlp.cu)
+    int mlp_ready = 0;
+    float *mlp_w = nullptr;         // parameters, MLP_NPARAM floats
+    float *mlp_m = nullptr, *mlp_v = nullptr;  // Adam moments
+    float *mlp_part = nullptr;      // per-block gradient partials
+    float *mlp_norm = nullptr;      // feature mean [F] and 1/std [F]
+    float *mlp_x = nullptr;         // [N][F] raw features of the current configuration
+    float *mlp_data = nullptr;      // training rows [cap][F + 3]
+    long long mlp_rows = 0, mlp_cap = 0;
+    int mlp_t = 0;                  // Adam step count
     // buffered 14-7 with virtual H sites
     int buff_on = 0;
     double buff_n = 14, buff_m = 7, buff_delta = 0.07, buff_gamma = 0.12, buff_h = 0.91;
@@ -145,11 +156,24 @@ void launch_mp_long(Ctx &c);
 void launch_ind_solve(Ctx &c);
 void launch_ind_short(Ctx &c);
 void launch_ind_long(Ctx &c);
+void launch_mp_long_sums(Ctx &c);
+void launch_polar_long_rest(Ctx &c);
 void launch_torques_begin(Ctx &c);
 void launch_torques_end(Ctx &c);
 void launch_frames(Ctx &c);
 void launch_buff(Ctx &c);
 int setup_cg(Ctx &c);
+// dipole-guess network (smd_mlp.cu)
+int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed);
+void launch_mlp_guess(Ctx &c);
+void launch_mlp_features(Ctx &c);
+void launch_mlp_collect(Ctx &c);
+void launch_mlp_norm(Ctx &c);
+void launch_mlp_step(Ctx &c, const unsigned int *perm, long long r0, int batch, float lr, float *grad_out);
+void launch_mlp_eval(Ctx &c, int rows, const float *x, float *y);
+int mlp_nparam();
+int mlp_nfeat();
+int mlp_max_batch();
 int setup_recip(Ctx &c);
 
 }  // namespace smd

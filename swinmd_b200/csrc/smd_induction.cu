@@ -516,11 +516,15 @@ void launch_ind_solve(Ctx &c) {
     IndArgs a = ind_args(c);
     const int nb = (int)(((long long)c.n * 8 + 255) / 256);
     k_ind_field<<<nb, 256, 0, c.stream>>>(a);
+    const bool learned = c.cg_guess == SMD_GUESS_LEARNED && c.mlp_ready;
+    if (learned) launch_mlp_guess(c);  // writes the start dipoles into p
     CGArgs g;
     g.ia = a;
     g.r = c.cgw; g.z = c.cgw + 3 * (size_t)c.n; g.v = c.cgw + 6 * (size_t)c.n; g.s = c.cgw + 9 * (size_t)c.n;
     g.part = c.cgs + 8; g.scal = c.cgs; g.bar = c.cg_bar; g.status = c.status;
-    g.nblocks = c.cg_blocks; g.max_iter = c.cg_max_iter; g.guess = c.cg_guess == 0 ? 0 : 1; g.tol = c.cg_tol;
+    g.nblocks = c.cg_blocks; g.max_iter = c.cg_max_iter; g.tol = c.cg_tol;
+    // 0: start from alpha E0; 1: start from the dipoles in p (previous solve or network)
+    g.guess = (c.cg_guess == SMD_GUESS_PREVIOUS || learned) ? 1 : 0;
     cudaMemsetAsync(c.cg_bar, 0, sizeof(unsigned int), c.stream);
     // cooperative launch: the runtime refuses it unless every block can be
     // resident at once, which the grid barrier relies on

@@ -1,0 +1,326 @@
+// Reciprocal-space sums of the polarisable model (Multipole::reciprocal_term,
+// src/forces/Multipole.cpp:951-1245; Induction::reciprocal_term,
+// src/forces/Induction.cpp:1395-1710).
+//
+// Per k (half space, k^2 < kCut^2) and site i, with a = k.r_i:
+//   structure factors  C_qQ + i S_qQ = sum (q_i - k.Q_i.k) e^{ia}
+//                      C_m  + i S_m  = sum (mu_i.k) e^{ia}
+//                      C_p  + i S_p  = sum (p_i.k) e^{ia}      (induced)
+//   permanent energy   c [ |S_qQ|^2 + 2 (S_qQ C_m - C_qQ S_m) + |S_m|^2 ] * ke
+//   induced energy     c [ S_qQ C_p - C_qQ S_p + C_p C_m + S_p S_m ] * ke
+// with c = 4 pi/V exp(-k^2/4a^2)/k^2; forces and torques per site follow
+// from the same sums (terms named after the reference's FqQ, FmiqQ, ...).
+//
+// Kernels: partial structure factors over (k tile x site chunk) blocks with
+// each chunk's site data staged in shared memory; a fixed-order reduction
+// over chunks giving S(k), the energy and the long virial; one per-site
+// pass for forces and torques with the k data staged in shared memory.  In
+// a time step the permanent and induced force terms share one pass (one
+// sine/cosine per site and k).  FP64 path: a = k.r in FP64 as the
+// reference computes it.  FP32 path: a is the exact 32-bit integer phase
+// n.(box fractions) and sine/cosine come from sincospif; sums stay FP64.
+#include "smd_ctx.cuh"
+#include "smd_polar.cuh"
+
+namespace smd {
+
+constexpr double KE = 138.93548501;
+constexpr double SQC_R = 11.78708976;
+constexpr int MK_THREADS = 128;
+constexpr int MK_CHUNKS = 16;
+constexpr int FK_TILE = 256;
+constexpr int F_TPS = 4;
+
+__device__ __forceinline__ void sincos_phase32(int ph, float &s, float &c) {
+    const int hi = ph & ~0xff;
+    const float b = (float)(ph & 0xff) * 1.4629180792671596e-09f;  // pi / 2^31
+    float sh, ch;
+    sincospif((float)hi * 4.656612873077393e-10f, &sh, &ch);
+    s = fmaf(b, ch, sh);
+    c = fmaf(-b, sh, ch);
+}
+
+// site data staged per chunk: phase source + q, mu, Q (perm) or p (induced)
+struct SiteTile {
+    double x[MK_THREADS], y[MK_THREADS], z[MK_THREADS];
+    int ix[MK_THREADS], iy[MK_THREADS], iz[MK_THREADS];
+    double v[10][MK_THREADS];
+};
+
+// MODE 0: permanent sums (4); MODE 1: induced sums (2)
+template <typename R, int MODE>
+__global__ void __launch_bounds__(MK_THREADS) k_rsk_partial(int n, int nk, const double4 *pos4, const int4 *fixq,
+                                                            const int *kn, const double *kvec, const double *tq,
+                                                            const double *mu, const double *qd, const double *pind,
+                                                            double *partial) {
+    __shared__ SiteTile T;
+    const int k = blockIdx.x * MK_THREADS + threadIdx.x;
+    const int ch = blockIdx.y;
+    const int per = (n + MK_CHUNKS - 1) / MK_CHUNKS;
+    const int s0 = ch * per, s1 = min(n, s0 + per);
+    double kx = 0, ky = 0, kz = 0;
+    int nx = 0, ny = 0, nz = 0;
+    if (k < nk) {
+        kx = kvec[k]; ky = kvec[nk + k]; kz = kvec[2 * nk + k];
+        nx = kn[k]; ny = kn[nk + k]; nz = kn[2 * nk + k];
+    }
+    // k.Q.k = Qxx kx^2 + Qyy ky^2 + Qzz kz^2 + 2 (Qxy kx ky + Qxz kx kz + Qyz ky kz)
+    const double kk[6] = {kx * kx, 2 * kx * ky, 2 * kx * kz, ky * ky, 2 * ky * kz, kz * kz};
+    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    for (int base = s0; base < s1; base += MK_THREADS) {
+        const int i = base + threadIdx.x;
+        __syncthreads();
+        if (i < s1) {
+            if (sizeof(R) == 8) {
+                const double4 p = pos4[i];
+                T.x[threadIdx.x] = p.x; T.y[threadIdx.x] = p.y; T.z[threadIdx.x] = p.z;
+            } else {
+                const int4 f = fixq[i];
+                T.ix[threadIdx.x] = f.x; T.iy[threadIdx.x] = f.y; T.iz[threadIdx.x] = f.z;
+            }
+            if (MODE == 0) {
+                T.v[0][threadIdx.x] = tq[(int)pos4[i].w] / SQC_R;
+                for (int d = 0; d < 3; d++) T.v[1 + d][threadIdx.x] = mu[(size_t)d * n + i];
+                for (int d = 0; d < 6; d++) T.v[4 + d][threadIdx.x] = qd[(size_t)d * n + i];
+            } else {
+                for (int d = 0; d < 3; d++) T.v[d][threadIdx.x] = pind[(size_t)d * n + i];
+            }
+        }
+        __syncthreads();
+        const int cnt = min(MK_THREADS, s1 - base);
+        if (k < nk) {
+            for (int q = 0; q < cnt; q++) {
+                double sn, cs;
+                if (sizeof(R) == 8) {
+                    sincos(T.x[q] * kx + T.y[q] * ky + T.z[q] * kz, &sn, &cs);
+                } else {
+                    const int ph = (int)((unsigned)nx * (unsigned)T.ix[q] + (unsigned)ny * (unsigned)T.iy[q] +
+                                         (unsigned)nz * (unsigned)T.iz[q]);
+                    float sf, cf;
+                    sincos_phase32(ph, sf, cf);
+                    sn = sf; cs = cf;
+                }
+                if (MODE == 0) {
+                    const double qk = T.v[0][q] - (T.v[4][q] * kk[0] + T.v[5][q] * kk[1] + T.v[6][q] * kk[2] +
+                                                   T.v[7][q] * kk[3] + T.v[8][q] * kk[4] + T.v[9][q] * kk[5]);
+                    const double mk = T.v[1][q] * kx + T.v[2][q] * ky + T.v[3][q] * kz;
+                    a0 += qk * cs; a1 += qk * sn; a2 += mk * cs; a3 += mk * sn;
+                } else {
+                    const double pk = T.v[0][q] * kx + T.v[1][q] * ky + T.v[2][q] * kz;
+                    a0 += pk * cs; a1 += pk * sn;
+                }
+            }
+        }
+    }
+    if (k < nk) {
+        double *base = partial + (size_t)ch * 6 * nk;
+        if (MODE == 0) {
+            base[k] = a0; base[nk + k] = a1; base[2 * (size_t)nk + k] = a2; base[3 * (size_t)nk + k] = a3;
+        } else {
+            base[4 * (size_t)nk + k] = a0; base[5 * (size_t)nk + k] = a1;
+        }
+    }
+}
+
+// fixed-order chunk sums; energy and long virial (MODE 0 permanent, 1 induced)
+template <int MODE>
+__global__ void k_rsk_reduce(int nk, const double *partial, const double *kcoef, const double *kvec,
+                             double alphaR4, double *sk, long long *acc, int slot_e) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0, vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
+    if (k < nk) {
+        const int q0 = MODE == 0 ? 0 : 4, q1 = MODE == 0 ? 4 : 6;
+        for (int q = q0; q < q1; q++) {
+            double t = 0;
+            for (int ch = 0; ch < MK_CHUNKS; ch++) t += partial[((size_t)ch * 6 + q) * nk + k];
+            sk[(size_t)q * nk + k] = t;
+        }
+        const double CqQ = sk[k], SqQ = sk[nk + k], Cm = sk[2 * (size_t)nk + k], Sm = sk[3 * (size_t)nk + k];
+        const double c = kcoef[k];
+        if (MODE == 0) {
+            e = c * ((CqQ * CqQ + SqQ * SqQ) + 2 * (SqQ * Cm - CqQ * Sm) + (Cm * Cm + Sm * Sm)) * KE;
+        } else {
+            const double Cp = sk[4 * (size_t)nk + k], Sp = sk[5 * (size_t)nk + k];
+            e = c * ((SqQ * Cp - CqQ * Sp) + (Cp * Cm + Sp * Sm)) * KE;
+        }
+        const double kx = kvec[k], ky = kvec[nk + k], kz = kvec[2 * nk + k];
+        const double k2 = kx * kx + ky * ky + kz * kz;
+        const double coeff = 2.0 * (alphaR4 + 1.0 / k2);
+        vxx = e - e * coeff * kx * kx; vyy = e - e * coeff * ky * ky; vzz = e - e * coeff * kz * kz;
+        vxy = -e * coeff * kx * ky; vxz = -e * coeff * kx * kz; vyz = -e * coeff * ky * kz;
+    }
+    if (slot_e < 0) return;  // sums only (no energy or virial from this call)
+    __shared__ double s_r[7][8];
+    double v[7] = {e, vxx, vxy, vxz, vyy, vyz, vzz};
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int q = 0; q < 7; q++) {
+        double t = warp_sum(v[q]);
+        if (lane == 0) s_r[q][w] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < 7) {
+        double t = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += s_r[threadIdx.x][q];
+        const int slots[7][2] = {{slot_e, -1}, {ACC_LVIR + 0, -1}, {ACC_LVIR + 1, ACC_LVIR + 3},
+                                 {ACC_LVIR + 2, ACC_LVIR + 6}, {ACC_LVIR + 4, -1},
+                                 {ACC_LVIR + 5, ACC_LVIR + 7}, {ACC_LVIR + 8, -1}};
+        const long long fx = to_fix(t, ACC_SCALE);
+        atomicAdd((unsigned long long *)&acc[slots[threadIdx.x][0]], (unsigned long long)fx);
+        if (slots[threadIdx.x][1] >= 0)
+            atomicAdd((unsigned long long *)&acc[slots[threadIdx.x][1]], (unsigned long long)fx);
+    }
+}
+
+// Per-site forces and torques; F_TPS threads split the k set, k data staged
+// in shared memory.  PERM / IND select the permanent and induced terms.
+template <typename R, bool PERM, bool IND>
+__global__ void __launch_bounds__(256) k_rforce(int n, int nk, const double4 *pos4, const int4 *fixq,
+                                                const int *kn, const double *kvec, const double *kcoef,
+                                                const double *sk, const double *tq, const double *mu,
+                                                const double *qd, const double *pind, long long *frc,
+                                                long long *trq) {
+    __shared__ double s_k[3][FK_TILE], s_b[FK_TILE], s_S[6][FK_TILE];
+    __shared__ int s_n[3][FK_TILE];
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gt / F_TPS, t = gt % F_TPS;
+    V3 f = v3(0, 0, 0), tau = v3(0, 0, 0);
+    double4 p64 = make_double4(0, 0, 0, 0);
+    int4 pf = make_int4(0, 0, 0, 0);
+    double qi = 0;
+    V3 mi = v3(0, 0, 0), pi_ = v3(0, 0, 0);
+    Q6 Qi = {0, 0, 0, 0, 0, 0};
+    if (i < n) {
+        p64 = pos4[i];
+        if (sizeof(R) == 4) pf = fixq[i];
+        qi = tq[(int)p64.w] / SQC_R;
+        mi = v3(mu[i], mu[n + i], mu[2 * n + i]);
+        Qi = {qd[i], qd[n + i], qd[2 * n + i], qd[3 * n + i], qd[4 * n + i], qd[5 * n + i]};
+        if (IND) pi_ = v3(pind[i], pind[n + i], pind[2 * n + i]);
+    }
+    for (int base = 0; base < nk; base += FK_TILE) {
+        __syncthreads();
+        const int kk = base + threadIdx.x;
+        if (kk < nk) {
+            for (int d = 0; d < 3; d++) {
+                s_k[d][threadIdx.x] = kvec[(size_t)d * nk + kk];
+                s_n[d][threadIdx.x] = kn[(size_t)d * nk + kk];
+            }
+            s_b[threadIdx.x] = 2.0 * kcoef[kk];
+            for (int d = 0; d < 6; d++)
+                s_S[d][threadIdx.x] = (d < 4 || IND) ? sk[(size_t)d * nk + kk] : 0.0;
+        }
+        __syncthreads();
+        const int cnt = min(FK_TILE, nk - base);
+        if (i < n) {
+            for (int q = t; q < cnt; q += F_TPS) {
+                const V3 k = v3(s_k[0][q], s_k[1][q], s_k[2][q]);
+                double sn, cs;
+                if (sizeof(R) == 8) {
+                    sincos(p64.x * k.x + p64.y * k.y + p64.z * k.z, &sn, &cs);
+                } else {
+                    const int ph = (int)((unsigned)s_n[0][q] * (unsigned)pf.x + (unsigned)s_n[1][q] * (unsigned)pf.y +
+                                         (unsigned)s_n[2][q] * (unsigned)pf.z);
+                    float sf, cf;
+                    sincos_phase32(ph, sf, cf);
+                    sn = sf; cs = cf;
+                }
+                const V3 Qk = qv(Qi, k);
+                const double qk = qi - dot(k, Qk);
+                const double c1 = qk * cs, s1 = qk * sn;
+                const double mk = dot(mi, k), mkc = mk * cs, mks = mk * sn;
+                const double b = s_b[q];
+                const double CqQ = s_S[0][q], SqQ = s_S[1][q], Cm = s_S[2][q], Sm = s_S[3][q];
+                const V3 kxm = crs(k, mi), KQ = crs(k, Qk);
+                double val = 0;
+                V3 tq_ = v3(0, 0, 0);
+                if (PERM) {
+                    val += (s1 * CqQ - c1 * SqQ) + (mkc * CqQ + mks * SqQ) - (c1 * Cm + s1 * Sm) + (mks * Cm - mkc * Sm);
+                    tq_ = tq_ + ((SqQ * cs - CqQ * sn) + (Cm * cs + Sm * sn)) * kxm +
+                          (-2.0 * (CqQ * cs + SqQ * sn) + 2.0 * (Sm * cs - Cm * sn)) * KQ;
+                }
+                if (IND) {
+                    const double Cp = s_S[4][q], Sp = s_S[5][q];
+                    const double pk = dot(pi_, k), pkc = pk * cs, pks = pk * sn;
+                    val += (pkc * CqQ + pks * SqQ) - (c1 * Cp + s1 * Sp) + (pks * (Cm + Cp) - pkc * (Sm + Sp)) +
+                           (mks * Cp - mkc * Sp);
+                    tq_ = tq_ + (cs * Cp + sn * Sp) * kxm + (2.0 * (cs * Sp - sn * Cp)) * KQ;
+                }
+                f = f + (b * val) * k;
+                tau = tau + b * tq_;
+            }
+        }
+    }
+    f.x = group_sum<F_TPS>(f.x); f.y = group_sum<F_TPS>(f.y); f.z = group_sum<F_TPS>(f.z);
+    tau.x = group_sum<F_TPS>(tau.x); tau.y = group_sum<F_TPS>(tau.y); tau.z = group_sum<F_TPS>(tau.z);
+    if (i < n && t == 0) {
+        add_fix3(frc, n, i, f, KE);
+        add_fix3(trq, n, i, tau, KE);
+    }
+}
+
+namespace {
+struct RecipBufs {
+    double *partial, *sk;
+};
+RecipBufs bufs(Ctx &c) {
+    double *partial = (double *)c.rc.sk;
+    return {partial, partial + (size_t)6 * c.rc.nk * MK_CHUNKS};
+}
+
+template <int MODE>
+void sums(Ctx &c, int slot_e) {
+    const int nk = c.rc.nk;
+    RecipBufs B = bufs(c);
+    dim3 g1((nk + MK_THREADS - 1) / MK_THREADS, MK_CHUNKS);
+    if (c.precision == SMD_PREC_MIXED)
+        k_rsk_partial<float, MODE><<<g1, MK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,
+                                                                   c.type_q, c.mu, c.qd, c.pind, B.partial);
+    else
+        k_rsk_partial<double, MODE><<<g1, MK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,
+                                                                    c.type_q, c.mu, c.qd, c.pind, B.partial);
+    k_rsk_reduce<MODE><<<(nk + 255) / 256, 256, 0, c.stream>>>(nk, B.partial, c.rc.kcoef, c.rc.kvec,
+                                                              1.0 / (4.0 * c.ew_alpha * c.ew_alpha), B.sk,
+                                                              c.acc, slot_e);
+}
+
+template <bool PERM, bool IND>
+void forces(Ctx &c) {
+    const int nk = c.rc.nk;
+    RecipBufs B = bufs(c);
+    const int nb = (int)(((long long)c.n * F_TPS + 255) / 256);
+    if (c.precision == SMD_PREC_MIXED)
+        k_rforce<float, PERM, IND><<<nb, 256, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec, c.rc.kcoef,
+                                                            B.sk, c.type_q, c.mu, c.qd, c.pind, c.frc, c.trq);
+    else
+        k_rforce<double, PERM, IND><<<nb, 256, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec, c.rc.kcoef,
+                                                             B.sk, c.type_q, c.mu, c.qd, c.pind, c.frc, c.trq);
+}
+}  // namespace
+
+// Multipole::compute_long on its own
+void launch_mp_long(Ctx &c) {
+    if (c.rc.nk == 0) return;
+    sums<0>(c, ACC_E_LONG);
+    forces<true, false>(c);
+}
+
+// Induction::compute_long on its own (permanent sums recomputed for it)
+void launch_ind_long(Ctx &c) {
+    if (c.rc.nk == 0) return;
+    sums<0>(c, -1);
+    sums<1>(c, ACC_E_POL_LONG);
+    forces<false, true>(c);
+}
+
+// within a time step: permanent sums before the dipole solve ...
+void launch_mp_long_sums(Ctx &c) {
+    if (c.rc.nk) sums<0>(c, ACC_E_LONG);
+}
+// ... induced sums after it, then one force pass for both
+void launch_polar_long_rest(Ctx &c) {
+    if (c.rc.nk == 0) return;
+    sums<1>(c, ACC_E_POL_LONG);
+    forces<true, true>(c);
+}
+
+}  // namespace smd

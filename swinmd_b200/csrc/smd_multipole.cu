@@ -40,7 +40,8 @@ __device__ __forceinline__ Q6 ldq(const double *a, int n, int i) {
 // the unit O->H vectors and x from the unit O->H2 vector; then
 // u = x - (x.z) z normalised, v = z x u (Local2Global.cpp:100-150).
 __global__ void k_frames(int nmol, int n, const int *mol_off, const int *mol_atoms,
-                         const double4 *pos4, const double *type_mp, double *mu, double *qd) {
+                         const double4 *pos4, const double *type_mp, double *mu, double *qd,
+                         double *frame) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= nmol) return;
     const int s = mol_off[m];
@@ -65,6 +66,10 @@ __global__ void k_frames(int nmol, int n, const int *mol_off, const int *mol_ato
         const V3 u = (1.0 / len(ss)) * ss;
         const V3 v = crs(w, u);
         const int id = ids[q];
+        if (frame) {  // axes u, v, w per site, for the dipole-guess network
+            const double ax[9] = {u.x, u.y, u.z, v.x, v.y, v.z, w.x, w.y, w.z};
+            for (int d = 0; d < 9; d++) frame[(size_t)d * n + id] = ax[d];
+        }
         const double *tp = type_mp + 9 * (int)pos4[id].w;
         const double dx = tp[0], dy = tp[1], dz = tp[2];
         mu[id] = u.x * dx + v.x * dy + w.x * dz;
@@ -95,7 +100,7 @@ __global__ void k_frames(int nmol, int n, const int *mol_off, const int *mol_ato
 
 void launch_frames(Ctx &c) {
     k_frames<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.n, c.mol_off, c.mol_atoms, c.pos4,
-                                                         c.type_mp, c.mu, c.qd);
+                                                         c.type_mp, c.mu, c.qd, c.frame);
 }
 
 // ---------------------------------------------------------------------------
@@ -290,174 +295,6 @@ __global__ void k_mp_mol(int nmol, int n, const int *mol_off, const int *mol_ato
 }
 
 // ---------------------------------------------------------------------------
-// reciprocal space: structure factors of (q - k.Q.k) and (mu.k)
-// ---------------------------------------------------------------------------
-constexpr int MK_THREADS = 128;
-constexpr int MK_CHUNKS = 16;
-
-// partial[ch][NS][nk]; NS = 4 (qQ cos/sin, m cos/sin) or 6 (+ induced p cos/sin)
-template <int NS>
-__global__ void __launch_bounds__(MK_THREADS) k_mp_sk_partial(int n, int nk, const double4 *pos4,
-                                                              const double *kvec, const double *tq,
-                                                              const double *mu, const double *qd,
-                                                              const double *pind, double *partial) {
-    __shared__ double s_d[MK_THREADS][NS == 6 ? 14 : 11];
-    const int k = blockIdx.x * MK_THREADS + threadIdx.x;
-    const int ch = blockIdx.y;
-    const int per = (n + MK_CHUNKS - 1) / MK_CHUNKS;
-    const int s0 = ch * per, s1 = min(n, s0 + per);
-    V3 kk = v3(0, 0, 0);
-    if (k < nk) kk = v3(kvec[k], kvec[nk + k], kvec[2 * nk + k]);
-    double acc[NS];
-    for (int q = 0; q < NS; q++) acc[q] = 0;
-    for (int base = s0; base < s1; base += MK_THREADS) {
-        const int i = base + threadIdx.x;
-        __syncthreads();
-        if (i < s1) {
-            const double4 p = pos4[i];
-            s_d[threadIdx.x][0] = p.x; s_d[threadIdx.x][1] = p.y; s_d[threadIdx.x][2] = p.z;
-            s_d[threadIdx.x][3] = tq[(int)p.w] / SQRTCOULOMB;
-            s_d[threadIdx.x][4] = mu[i]; s_d[threadIdx.x][5] = mu[n + i]; s_d[threadIdx.x][6] = mu[2 * n + i];
-            // k.Q.k needs the 6 components; store them after the dipole
-            for (int q = 0; q < 6 && 7 + q < (NS == 6 ? 14 : 11); q++) s_d[threadIdx.x][7 + q] = 0;
-        }
-        __syncthreads();
-        const int cnt = min(MK_THREADS, s1 - base);
-        if (k < nk) {
-            for (int q = 0; q < cnt; q++) {
-                const int id = base + q;
-                const double a = s_d[q][0] * kk.x + s_d[q][1] * kk.y + s_d[q][2] * kk.z;
-                double sn, cs;
-                sincos(a, &sn, &cs);
-                const Q6 Qi = ldq(qd, n, id);
-                const double qk = s_d[q][3] - dot(kk, qv(Qi, kk));
-                const double mk = s_d[q][4] * kk.x + s_d[q][5] * kk.y + s_d[q][6] * kk.z;
-                acc[0] += qk * cs; acc[1] += qk * sn;
-                acc[2] += mk * cs; acc[3] += mk * sn;
-                if (NS == 6) {
-                    const double pk = pind[id] * kk.x + pind[n + id] * kk.y + pind[2 * n + id] * kk.z;
-                    acc[4] += pk * cs; acc[5] += pk * sn;
-                }
-            }
-        }
-    }
-    if (k < nk)
-        for (int q = 0; q < NS; q++) partial[((size_t)ch * NS + q) * nk + k] = acc[q];
-}
-
-// Sums over chunks in a fixed order; per-k energy and long virial.
-// mode 0: permanent (UqQ + 2 UmqQ + Umm); mode 1: induction (UmqQ' + Ump)
-template <int NS>
-__global__ void k_mp_sk_reduce(int nk, const double *partial, const double *kcoef, const double *kvec,
-                               double alphaR4, double *sk, long long *acc, int slot_e) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    double e = 0, vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
-    if (k < nk) {
-        double S[NS];
-        for (int q = 0; q < NS; q++) {
-            double t = 0;
-            for (int ch = 0; ch < MK_CHUNKS; ch++) t += partial[((size_t)ch * NS + q) * nk + k];
-            S[q] = t;
-            sk[(size_t)q * nk + k] = t;
-        }
-        const double c = kcoef[k];  // 4 pi/V exp(-k^2/4a^2)/k^2
-        if (NS == 4) {
-            const double UqQ = c * (S[0] * S[0] + S[1] * S[1]);
-            const double UmqQ = c * (S[1] * S[2] - S[0] * S[3]);
-            const double Umm = c * (S[2] * S[2] + S[3] * S[3]);
-            e = (UqQ + 2 * UmqQ + Umm) * COULOMBS;
-        } else {
-            const double UmqQ = c * (S[1] * S[4] - S[0] * S[5]);
-            const double Ump = c * (S[4] * S[2] + S[5] * S[3]);
-            e = (UmqQ + Ump) * COULOMBS;
-        }
-        const double kx = kvec[k], ky = kvec[nk + k], kz = kvec[2 * nk + k];
-        const double k2 = kx * kx + ky * ky + kz * kz;
-        const double coeff = 2.0 * (alphaR4 + 1.0 / k2);
-        vxx = e - e * coeff * kx * kx;
-        vyy = e - e * coeff * ky * ky;
-        vzz = e - e * coeff * kz * kz;
-        vxy = -e * coeff * kx * ky;
-        vxz = -e * coeff * kx * kz;
-        vyz = -e * coeff * ky * kz;
-    }
-    __shared__ double s_r[7][8];
-    double v[7] = {e, vxx, vxy, vxz, vyy, vyz, vzz};
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int q = 0; q < 7; q++) {
-        double t = warp_sum(v[q]);
-        if (lane == 0) s_r[q][w] = t;
-    }
-    __syncthreads();
-    if (threadIdx.x < 7) {
-        double t = 0;
-        for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += s_r[threadIdx.x][q];
-        const int slots[7][2] = {{slot_e, -1}, {ACC_LVIR + 0, -1}, {ACC_LVIR + 1, ACC_LVIR + 3},
-                                 {ACC_LVIR + 2, ACC_LVIR + 6}, {ACC_LVIR + 4, -1},
-                                 {ACC_LVIR + 5, ACC_LVIR + 7}, {ACC_LVIR + 8, -1}};
-        const long long fx = to_fix(t, ACC_SCALE);
-        atomicAdd((unsigned long long *)&acc[slots[threadIdx.x][0]], (unsigned long long)fx);
-        if (slots[threadIdx.x][1] >= 0)
-            atomicAdd((unsigned long long *)&acc[slots[threadIdx.x][1]], (unsigned long long)fx);
-    }
-}
-
-// Per-site reciprocal force and torque; 4 threads split the k set.
-template <int NS>
-__global__ void __launch_bounds__(256) k_mp_recip_force(int n, int nk, const double4 *pos4,
-                                                        const double *kvec, const double *kcoef,
-                                                        const double *sk, const double *tq,
-                                                        const double *mu, const double *qd,
-                                                        const double *pind, long long *frc,
-                                                        long long *trq) {
-    constexpr int TPS = 4;
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = gt / TPS, t = gt % TPS;
-    V3 f = v3(0, 0, 0), tau = v3(0, 0, 0);
-    if (i < n) {
-        const double4 p = pos4[i];
-        const double qi = tq[(int)p.w] / SQRTCOULOMB;
-        const V3 mi = ld3(mu, n, i);
-        const Q6 Qi = ldq(qd, n, i);
-        V3 pi = v3(0, 0, 0);
-        if (NS == 6) pi = ld3(pind, n, i);
-        for (int k = t; k < nk; k += TPS) {
-            const V3 kk = v3(kvec[k], kvec[nk + k], kvec[2 * nk + k]);
-            const double a = p.x * kk.x + p.y * kk.y + p.z * kk.z;
-            double sn, cs;
-            sincos(a, &sn, &cs);
-            const V3 Qk = qv(Qi, kk);
-            const double qk = qi - dot(kk, Qk);
-            const double c1 = qk * cs, s1 = qk * sn;
-            const double mk = dot(mi, kk), mkc = mk * cs, mks = mk * sn;
-            const double b = 2.0 * kcoef[k];
-            const double CqQ = sk[k], SqQ = sk[nk + k], Cm = sk[2 * (size_t)nk + k], Sm = sk[3 * (size_t)nk + k];
-            const V3 kxm = crs(kk, mi), KQ = crs(kk, Qk);
-            double val;
-            if (NS == 4) {
-                val = b * ((s1 * CqQ - c1 * SqQ) + (mkc * CqQ + mks * SqQ) - (c1 * Cm + s1 * Sm) +
-                           (mks * Cm - mkc * Sm));
-                tau = tau + b * ((SqQ * cs - CqQ * sn) * kxm + (Cm * cs + Sm * sn) * kxm -
-                                 2.0 * (CqQ * cs + SqQ * sn) * KQ + 2.0 * (Sm * cs - Cm * sn) * KQ);
-            } else {
-                const double Cp = sk[4 * (size_t)nk + k], Sp = sk[5 * (size_t)nk + k];
-                const double pk = dot(pi, kk), pkc = pk * cs, pks = pk * sn;
-                val = b * ((pkc * CqQ + pks * SqQ) - (c1 * Cp + s1 * Sp) +
-                           (pks * (Cm + Cp) - pkc * (Sm + Sp)) + (mks * Cp - mkc * Sp));
-                tau = tau + b * ((cs * Cp + sn * Sp) * kxm + 2.0 * (cs * Sp - sn * Cp) * KQ);
-            }
-            f = f + val * kk;
-        }
-    }
-    f.x = group_sum<TPS>(f.x); f.y = group_sum<TPS>(f.y); f.z = group_sum<TPS>(f.z);
-    tau.x = group_sum<TPS>(tau.x); tau.y = group_sum<TPS>(tau.y); tau.z = group_sum<TPS>(tau.z);
-    if (i < n && t == 0) {
-        add_fix3(frc, n, i, f, COULOMBS);
-        add_fix3(trq, n, i, tau, COULOMBS);
-    }
-}
-
-// ---------------------------------------------------------------------------
 // torques -> forces on the H O H sites (Multipole::torques2forces)
 // ---------------------------------------------------------------------------
 __global__ void k_torque2force(int nmol, int n, const int *mol_off, const int *mol_atoms,
@@ -533,26 +370,5 @@ void launch_mp_short(Ctx &c) {
                                                          c.excl, c.pos4, c.type_q, c.mu, c.qd, c.box,
                                                          c.ew_alpha, c.acc);
 }
-
-// reciprocal space (Multipole::compute_long); NS = 6 adds the induced dipoles
-template <int NS>
-static void mp_recip(Ctx &c, int slot_e) {
-    const int nk = c.rc.nk;
-    if (nk == 0) return;
-    double *partial = (double *)c.rc.sk;
-    double *sk = partial + (size_t)6 * nk * MK_CHUNKS;
-    dim3 g1((nk + MK_THREADS - 1) / MK_THREADS, MK_CHUNKS);
-    k_mp_sk_partial<NS><<<g1, MK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.rc.kvec, c.type_q, c.mu, c.qd,
-                                                        c.pind, partial);
-    k_mp_sk_reduce<NS><<<(nk + 255) / 256, 256, 0, c.stream>>>(nk, partial, c.rc.kcoef, c.rc.kvec,
-                                                               1.0 / (4.0 * c.ew_alpha * c.ew_alpha), sk,
-                                                               c.acc, slot_e);
-    const int nb = (int)(((long long)c.n * 4 + 255) / 256);
-    k_mp_recip_force<NS><<<nb, 256, 0, c.stream>>>(c.n, nk, c.pos4, c.rc.kvec, c.rc.kcoef, sk, c.type_q,
-                                                  c.mu, c.qd, c.pind, c.frc, c.trq);
-}
-
-void launch_mp_long(Ctx &c) { mp_recip<4>(c, ACC_E_LONG); }
-void launch_ind_long(Ctx &c) { mp_recip<6>(c, ACC_E_POL_LONG); }
 
 }  // namespace smd

@@ -376,6 +376,45 @@ class GpuEnsemble:
         pp = np.ascontiguousarray(p, np.float64).reshape(-1)
         self._chk(self.lib.smd_set_induced(self.ctx, L.dptr(pp)))
 
+    # -- learned initial guess of the induced dipoles ------------------------
+    def mlp_init(self, capacity_frames: int, seed: int = 1):
+        self._chk(self.lib.smd_mlp_init(self.ctx, capacity_frames, seed))
+
+    def mlp_collect(self):
+        self._chk(self.lib.smd_mlp_collect(self.ctx))
+
+    def mlp_train(self, epochs: int, batch: int = 4096, lr: float = 1e-3, seed: int = 1) -> float:
+        loss = ctypes.c_double()
+        self._chk(self.lib.smd_mlp_train(self.ctx, epochs, batch, lr, seed, ctypes.byref(loss)))
+        return loss.value
+
+    def mlp_params(self, set_to: Optional[np.ndarray] = None) -> np.ndarray:
+        cnt = ctypes.c_int()
+        self._chk(self.lib.smd_mlp_params(self.ctx, None, None, ctypes.byref(cnt)))
+        out = np.zeros(cnt.value, np.float32)
+        s = None if set_to is None else np.ascontiguousarray(set_to, np.float32)
+        self._chk(self.lib.smd_mlp_params(self.ctx, L.fptr(out), L.fptr(s), ctypes.byref(cnt)))
+        return out
+
+    def mlp_eval(self, feats: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(feats, np.float32)
+        y = np.zeros((x.shape[0], 3), np.float32)
+        self._chk(self.lib.smd_mlp_eval(self.ctx, L.fptr(x), x.shape[0], L.fptr(y)))
+        return y
+
+    def mlp_gradient(self, rows: np.ndarray) -> np.ndarray:
+        r = np.ascontiguousarray(rows, np.float32)
+        cnt = ctypes.c_int()
+        self._chk(self.lib.smd_mlp_params(self.ctx, None, None, ctypes.byref(cnt)))
+        g = np.zeros(cnt.value - 40, np.float32)
+        self._chk(self.lib.smd_mlp_gradient(self.ctx, L.fptr(r), r.shape[0], L.fptr(g)))
+        return g
+
+    def mlp_features(self) -> np.ndarray:
+        f = np.zeros((self.n, 20), np.float32)
+        self._chk(self.lib.smd_mlp_features(self.ctx, L.fptr(f)))
+        return f
+
 
 # ---------------------------------------------------------------------------
 # Force plugin mirrors (Force::compute / compute_long)
