@@ -305,8 +305,8 @@ def main():
     import ctypes
     kc = ctypes.c_int()
     L.check(ens.ctx, ens.lib.smd_step_kernel_count(ens.ctx, ctypes.byref(kc)))
-    names = ["pair", "recip", "integrate", "list_rebuild", "frames", "mp_real", "mp_recip_sums",
-             "dipole_solve", "ind_real", "recip_induced_sums_and_forces"]
+    names = ["pair", "recip", "integrate", "list_rebuild", "frames", "mp_real", "mp_recip",
+             "dipole_solve", "ind_real", "polar_recip"]
     stage_ms = {k: float(v) for k, v in zip(names, prof)}
     stage_plain = {k: float(v) for k, v in zip(names, prof_plain)}
     peaks = dict(FALLBACK)

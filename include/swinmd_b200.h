@@ -252,10 +252,11 @@ int smd_get_series(smd_ctx *ctx, double *out, int cap, int *count);
  * stage of one step, each launched `reps` times on its own:
  * out[0] pair kernel, out[1] reciprocal kernels, out[2] integrate kernel,
  * out[3] a forced pair-list rebuild; for the polarisable model out[4] frames,
- * out[5] multipole real+self+intra, out[6] multipole reciprocal, out[7]
- * field + dipole solve, out[8] induced real+self+intra, out[9] induced
- * reciprocal (out has room for 10).  Leaves forces and state unchanged
- * except for the rebuilt list. */
+ * out[5] multipole real+self+intra, out[6] multipole reciprocal (models
+ * without induced dipoles), out[7] field + dipole solve, out[8] induced
+ * real+self+intra, out[9] reciprocal structure factors and forces of the
+ * permanent and induced multipoles together (out has room for 10).  Leaves
+ * forces and state unchanged except for the rebuilt list. */
 int smd_profile_stages(smd_ctx *ctx, int reps, double *out);
 /* smd_run with the device time of the nsteps graph launches (CUDA events on
  * the context's stream, synchronized on both sides) returned in *device_ms. */

@@ -123,12 +123,11 @@ void enqueue_polar(Ctx &c, bool mp_short, bool mp_long, bool ind_short, bool ind
     if (mp_short) launch_mp_short(c);
     const bool all = mp_short && mp_long && ind_short && ind_long && c.ind_on;
     if (all) {
-        // a full evaluation: the permanent structure factors are summed
-        // before the solve, and one reciprocal force pass serves both terms
-        launch_mp_long_sums(c);
+        // a full evaluation: after the solve one pass gives all structure
+        // factors and one reciprocal force pass serves both terms
         launch_ind_solve(c);
         launch_ind_short(c);
-        launch_polar_long_rest(c);
+        launch_polar_long(c);
     } else {
         if (mp_long) launch_mp_long(c);
         if (c.ind_on && (ind_short || ind_long)) {
@@ -938,22 +937,27 @@ int smd_profile_stages(smd_ctx *x, int reps, double *out) {
     if (c.mp_on) {
         out[4] = timed([&] { launch_frames(c); launch_torques_begin(c); });
         out[5] = timed([&] { launch_mp_short(c); });
-        out[6] = timed([&] { c.ind_on ? launch_mp_long_sums(c) : launch_mp_long(c); });
+        if (!c.ind_on) out[6] = timed([&] { launch_mp_long(c); });
         if (c.ind_on) {
             const int guess = c.cg_guess;
             if (guess == 0) {
                 out[7] = timed([&] { launch_ind_solve(c); });
             } else {
                 // a warm start must start from the same dipoles every time
-                std::vector<double> p0(3 * (size_t)c.n);
-                CK(cudaMemcpy(p0.data(), c.pind, p0.size() * sizeof(double), cudaMemcpyDeviceToHost));
+                // (a device copy: its time is a few microseconds of the stage)
+                const size_t pb = 3 * (size_t)c.n * sizeof(double);
+                double *p0 = nullptr;
+                CK(cudaMalloc(&p0, pb));
+                CK(cudaMemcpyAsync(p0, c.pind, pb, cudaMemcpyDeviceToDevice, c.stream));
                 out[7] = timed([&] {
-                    cudaMemcpyAsync(c.pind, p0.data(), p0.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream);
+                    cudaMemcpyAsync(c.pind, p0, pb, cudaMemcpyDeviceToDevice, c.stream);
                     launch_ind_solve(c);
                 });
+                CK(cudaStreamSynchronize(c.stream));
+                cudaFree(p0);
             }
             out[8] = timed([&] { launch_ind_short(c); });
-            out[9] = timed([&] { launch_polar_long_rest(c); });
+            out[9] = timed([&] { launch_polar_long(c); });
         }
     }
     // forces for the current positions again, accumulators clear

@@ -156,8 +156,7 @@ void launch_mp_long(Ctx &c);
 void launch_ind_solve(Ctx &c);
 void launch_ind_short(Ctx &c);
 void launch_ind_long(Ctx &c);
-void launch_mp_long_sums(Ctx &c);
-void launch_polar_long_rest(Ctx &c);
+void launch_polar_long(Ctx &c);
 void launch_torques_begin(Ctx &c);
 void launch_torques_end(Ctx &c);
 void launch_frames(Ctx &c);

@@ -11,14 +11,24 @@
 // with c = 4 pi/V exp(-k^2/4a^2)/k^2; forces and torques per site follow
 // from the same sums (terms named after the reference's FqQ, FmiqQ, ...).
 //
+// The reference's permanent and induced force terms together are the force
+// of the site's full multipole set (q, mu + p, Q) in the field of the full
+// structure factor.  With U = C_qQ - S_m - S_p, W = S_qQ + C_m + C_p,
+// A = sin(a) U - cos(a) W and B = cos(a) U + sin(a) W, one k contributes
+//   force   2c k [ (q_i - k.Q_i.k) A + ((mu_i + p_i).k) B ]
+//   torque  2c [ A (mu_i x k) - 2 B (k x Q_i k) ]
+// (permanent terms alone: drop the p terms).
+//
 // Kernels: partial structure factors over (k tile x site chunk) blocks with
 // each chunk's site data staged in shared memory; a fixed-order reduction
-// over chunks giving S(k), the energy and the long virial; one per-site
+// over chunks giving S(k), the energies and the long virial; one per-site
 // pass for forces and torques with the k data staged in shared memory.  In
-// a time step the permanent and induced force terms share one pass (one
-// sine/cosine per site and k).  FP64 path: a = k.r in FP64 as the
-// reference computes it.  FP32 path: a is the exact 32-bit integer phase
-// n.(box fractions) and sine/cosine come from sincospif; sums stay FP64.
+// a time step all six sums come from one pass after the dipole solve and
+// one force pass serves the permanent and induced terms.
+//   FP64 path: a = k.r in FP64 as the reference computes it, FP64 arithmetic.
+//   FP32 path: a is the exact 32-bit integer phase n.(box fractions), sine and
+//   cosine from sincospif; the per-(site, k) arithmetic is FP32 with the
+//   running sums moved into FP64 after every tile of 64-128 terms.
 #include "smd_ctx.cuh"
 #include "smd_polar.cuh"
 
@@ -31,6 +41,8 @@ constexpr int MK_CHUNKS = 16;
 constexpr int FK_TILE = 256;
 constexpr int F_TPS = 4;
 
+// sin and cos of 2 pi ph / 2^32: the top 24 bits go through sincospif
+// exactly, the low 8 bits as a first-order rotation
 __device__ __forceinline__ void sincos_phase32(int ph, float &s, float &c) {
     const int hi = ph & ~0xff;
     const float b = (float)(ph & 0xff) * 1.4629180792671596e-09f;  // pi / 2^31
@@ -40,14 +52,18 @@ __device__ __forceinline__ void sincos_phase32(int ph, float &s, float &c) {
     c = fmaf(-b, sh, ch);
 }
 
-// site data staged per chunk: phase source + q, mu, Q (perm) or p (induced)
+// ---------------------------------------------------------------------------
+// FP64 partial structure factors
+// ---------------------------------------------------------------------------
 struct SiteTile {
     double x[MK_THREADS], y[MK_THREADS], z[MK_THREADS];
     int ix[MK_THREADS], iy[MK_THREADS], iz[MK_THREADS];
-    double v[10][MK_THREADS];
+    double v[13][MK_THREADS];
 };
 
-// MODE 0: permanent sums (4); MODE 1: induced sums (2)
+// MODE 0: permanent sums (slots 0-3); 1: induced sums (4-5); 2: all six.
+// R = float takes the phase from the integer box fractions (used for the
+// induced-only evaluation of the mixed path).
 template <typename R, int MODE>
 __global__ void __launch_bounds__(MK_THREADS) k_rsk_partial(int n, int nk, const double4 *pos4, const int4 *fixq,
                                                             const int *kn, const double *kvec, const double *tq,
@@ -66,7 +82,9 @@ __global__ void __launch_bounds__(MK_THREADS) k_rsk_partial(int n, int nk, const
     }
     // k.Q.k = Qxx kx^2 + Qyy ky^2 + Qzz kz^2 + 2 (Qxy kx ky + Qxz kx kz + Qyz ky kz)
     const double kk[6] = {kx * kx, 2 * kx * ky, 2 * kx * kz, ky * ky, 2 * ky * kz, kz * kz};
-    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    constexpr bool PERM = MODE != 1, IND = MODE != 0;
+    constexpr int PV = MODE == 1 ? 0 : 10;   // induced dipole slots in the tile
+    double a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
     for (int base = s0; base < s1; base += MK_THREADS) {
         const int i = base + threadIdx.x;
         __syncthreads();
@@ -78,13 +96,13 @@ __global__ void __launch_bounds__(MK_THREADS) k_rsk_partial(int n, int nk, const
                 const int4 f = fixq[i];
                 T.ix[threadIdx.x] = f.x; T.iy[threadIdx.x] = f.y; T.iz[threadIdx.x] = f.z;
             }
-            if (MODE == 0) {
+            if (PERM) {
                 T.v[0][threadIdx.x] = tq[(int)pos4[i].w] / SQC_R;
                 for (int d = 0; d < 3; d++) T.v[1 + d][threadIdx.x] = mu[(size_t)d * n + i];
                 for (int d = 0; d < 6; d++) T.v[4 + d][threadIdx.x] = qd[(size_t)d * n + i];
-            } else {
-                for (int d = 0; d < 3; d++) T.v[d][threadIdx.x] = pind[(size_t)d * n + i];
             }
+            if (IND)
+                for (int d = 0; d < 3; d++) T.v[PV + d][threadIdx.x] = pind[(size_t)d * n + i];
         }
         __syncthreads();
         const int cnt = min(MK_THREADS, s1 - base);
@@ -100,36 +118,119 @@ __global__ void __launch_bounds__(MK_THREADS) k_rsk_partial(int n, int nk, const
                     sincos_phase32(ph, sf, cf);
                     sn = sf; cs = cf;
                 }
-                if (MODE == 0) {
+                if (PERM) {
                     const double qk = T.v[0][q] - (T.v[4][q] * kk[0] + T.v[5][q] * kk[1] + T.v[6][q] * kk[2] +
                                                    T.v[7][q] * kk[3] + T.v[8][q] * kk[4] + T.v[9][q] * kk[5]);
                     const double mk = T.v[1][q] * kx + T.v[2][q] * ky + T.v[3][q] * kz;
                     a0 += qk * cs; a1 += qk * sn; a2 += mk * cs; a3 += mk * sn;
-                } else {
-                    const double pk = T.v[0][q] * kx + T.v[1][q] * ky + T.v[2][q] * kz;
-                    a0 += pk * cs; a1 += pk * sn;
+                }
+                if (IND) {
+                    const double pk = T.v[PV][q] * kx + T.v[PV + 1][q] * ky + T.v[PV + 2][q] * kz;
+                    a4 += pk * cs; a5 += pk * sn;
                 }
             }
         }
     }
     if (k < nk) {
         double *base = partial + (size_t)ch * 6 * nk;
-        if (MODE == 0) {
+        if (PERM) {
             base[k] = a0; base[nk + k] = a1; base[2 * (size_t)nk + k] = a2; base[3 * (size_t)nk + k] = a3;
-        } else {
-            base[4 * (size_t)nk + k] = a0; base[5 * (size_t)nk + k] = a1;
+        }
+        if (IND) {
+            base[4 * (size_t)nk + k] = a4; base[5 * (size_t)nk + k] = a5;
         }
     }
 }
 
-// fixed-order chunk sums; energy and long virial (MODE 0 permanent, 1 induced)
+// ---------------------------------------------------------------------------
+// FP32 partial structure factors (mixed path)
+// ---------------------------------------------------------------------------
+template <int MODE>
+__global__ void __launch_bounds__(MK_THREADS) k_rsk_partial_f(int n, int nk, const double4 *pos4, const int4 *fixq,
+                                                              const int *kn, const double *kvec, const double *tq,
+                                                              const double *mu, const double *qd,
+                                                              const double *pind, double *partial) {
+    constexpr bool PERM = MODE != 1, IND = MODE != 0;
+    constexpr int PV = MODE == 1 ? 0 : 10;
+    constexpr int NV = MODE == 0 ? 10 : (MODE == 1 ? 3 : 13);
+    __shared__ int s_i[3][MK_THREADS];
+    __shared__ float s_v[NV][MK_THREADS];
+    const int k = blockIdx.x * MK_THREADS + threadIdx.x;
+    const int ch = blockIdx.y;
+    const int per = (n + MK_CHUNKS - 1) / MK_CHUNKS;
+    const int s0 = ch * per, s1 = min(n, s0 + per);
+    float kx = 0.f, ky = 0.f, kz = 0.f;
+    unsigned nx = 0, ny = 0, nz = 0;
+    if (k < nk) {
+        kx = (float)kvec[k]; ky = (float)kvec[nk + k]; kz = (float)kvec[2 * nk + k];
+        nx = (unsigned)kn[k]; ny = (unsigned)kn[nk + k]; nz = (unsigned)kn[2 * nk + k];
+    }
+    const float kk[6] = {kx * kx, 2.f * kx * ky, 2.f * kx * kz, ky * ky, 2.f * ky * kz, kz * kz};
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int base = s0; base < s1; base += MK_THREADS) {
+        const int i = base + threadIdx.x;
+        __syncthreads();
+        if (i < s1) {
+            const int4 f = fixq[i];
+            s_i[0][threadIdx.x] = f.x; s_i[1][threadIdx.x] = f.y; s_i[2][threadIdx.x] = f.z;
+            if (PERM) {
+                s_v[0][threadIdx.x] = (float)(tq[(int)pos4[i].w] / SQC_R);
+                for (int d = 0; d < 3; d++) s_v[1 + d][threadIdx.x] = (float)mu[(size_t)d * n + i];
+                for (int d = 0; d < 6; d++) s_v[4 + d][threadIdx.x] = (float)qd[(size_t)d * n + i];
+            }
+            if (IND)
+                for (int d = 0; d < 3; d++) s_v[PV + d][threadIdx.x] = (float)pind[(size_t)d * n + i];
+        }
+        __syncthreads();
+        const int cnt = min(MK_THREADS, s1 - base);
+        if (k < nk) {
+            float t0 = 0.f, t1 = 0.f, t2 = 0.f, t3 = 0.f, t4 = 0.f, t5 = 0.f;
+#pragma unroll 4
+            for (int q = 0; q < cnt; q++) {
+                const int ph = (int)(nx * (unsigned)s_i[0][q] + ny * (unsigned)s_i[1][q] + nz * (unsigned)s_i[2][q]);
+                float sn, cs;
+                sincos_phase32(ph, sn, cs);
+                if (PERM) {
+                    float kqk = s_v[4][q] * kk[0];
+                    kqk = fmaf(s_v[5][q], kk[1], kqk);
+                    kqk = fmaf(s_v[6][q], kk[2], kqk);
+                    kqk = fmaf(s_v[7][q], kk[3], kqk);
+                    kqk = fmaf(s_v[8][q], kk[4], kqk);
+                    kqk = fmaf(s_v[9][q], kk[5], kqk);
+                    const float qk = s_v[0][q] - kqk;
+                    const float mk = fmaf(s_v[1][q], kx, fmaf(s_v[2][q], ky, s_v[3][q] * kz));
+                    t0 = fmaf(qk, cs, t0); t1 = fmaf(qk, sn, t1);
+                    t2 = fmaf(mk, cs, t2); t3 = fmaf(mk, sn, t3);
+                }
+                if (IND) {
+                    const float pk = fmaf(s_v[PV][q], kx, fmaf(s_v[PV + 1][q], ky, s_v[PV + 2][q] * kz));
+                    t4 = fmaf(pk, cs, t4); t5 = fmaf(pk, sn, t5);
+                }
+            }
+            acc[0] += t0; acc[1] += t1; acc[2] += t2; acc[3] += t3; acc[4] += t4; acc[5] += t5;
+        }
+    }
+    if (k < nk) {
+        double *base = partial + (size_t)ch * 6 * nk;
+        if (PERM)
+            for (int q = 0; q < 4; q++) base[(size_t)q * nk + k] = acc[q];
+        if (IND)
+            for (int q = 4; q < 6; q++) base[(size_t)q * nk + k] = acc[q];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// fixed-order chunk sums; energies and long virial
+// ---------------------------------------------------------------------------
+// MODE 0 permanent, 1 induced, 2 both (permanent energy to slot_e, induced
+// to slot_e2); slot_e < 0: sums only
 template <int MODE>
 __global__ void k_rsk_reduce(int nk, const double *partial, const double *kcoef, const double *kvec,
-                             double alphaR4, double *sk, long long *acc, int slot_e) {
+                             double alphaR4, double *sk, long long *acc, int slot_e, int slot_e2) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    double e = 0, vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
+    double ep = 0, ei = 0, vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
     if (k < nk) {
-        const int q0 = MODE == 0 ? 0 : 4, q1 = MODE == 0 ? 4 : 6;
+        const int q0 = MODE == 1 ? 4 : 0, q1 = MODE == 0 ? 4 : 6;
         for (int q = q0; q < q1; q++) {
             double t = 0;
             for (int ch = 0; ch < MK_CHUNKS; ch++) t += partial[((size_t)ch * 6 + q) * nk + k];
@@ -137,12 +238,12 @@ __global__ void k_rsk_reduce(int nk, const double *partial, const double *kcoef,
         }
         const double CqQ = sk[k], SqQ = sk[nk + k], Cm = sk[2 * (size_t)nk + k], Sm = sk[3 * (size_t)nk + k];
         const double c = kcoef[k];
-        if (MODE == 0) {
-            e = c * ((CqQ * CqQ + SqQ * SqQ) + 2 * (SqQ * Cm - CqQ * Sm) + (Cm * Cm + Sm * Sm)) * KE;
-        } else {
+        if (MODE != 1) ep = c * ((CqQ * CqQ + SqQ * SqQ) + 2 * (SqQ * Cm - CqQ * Sm) + (Cm * Cm + Sm * Sm)) * KE;
+        if (MODE != 0) {
             const double Cp = sk[4 * (size_t)nk + k], Sp = sk[5 * (size_t)nk + k];
-            e = c * ((SqQ * Cp - CqQ * Sp) + (Cp * Cm + Sp * Sm)) * KE;
+            ei = c * ((SqQ * Cp - CqQ * Sp) + (Cp * Cm + Sp * Sm)) * KE;
         }
+        const double e = ep + ei;
         const double kx = kvec[k], ky = kvec[nk + k], kz = kvec[2 * nk + k];
         const double k2 = kx * kx + ky * ky + kz * kz;
         const double coeff = 2.0 * (alphaR4 + 1.0 / k2);
@@ -150,20 +251,21 @@ __global__ void k_rsk_reduce(int nk, const double *partial, const double *kcoef,
         vxy = -e * coeff * kx * ky; vxz = -e * coeff * kx * kz; vyz = -e * coeff * ky * kz;
     }
     if (slot_e < 0) return;  // sums only (no energy or virial from this call)
-    __shared__ double s_r[7][8];
-    double v[7] = {e, vxx, vxy, vxz, vyy, vyz, vzz};
+    __shared__ double s_r[8][8];
+    double v[8] = {ep + (MODE == 1 ? ei : 0.0), ei, vxx, vxy, vxz, vyy, vyz, vzz};
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int q = 0; q < 7; q++) {
+    for (int q = 0; q < 8; q++) {
         double t = warp_sum(v[q]);
         if (lane == 0) s_r[q][w] = t;
     }
     __syncthreads();
-    if (threadIdx.x < 7) {
+    if (threadIdx.x < 8) {
+        if (threadIdx.x == 1 && MODE != 2) return;
         double t = 0;
         for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += s_r[threadIdx.x][q];
-        const int slots[7][2] = {{slot_e, -1}, {ACC_LVIR + 0, -1}, {ACC_LVIR + 1, ACC_LVIR + 3},
-                                 {ACC_LVIR + 2, ACC_LVIR + 6}, {ACC_LVIR + 4, -1},
-                                 {ACC_LVIR + 5, ACC_LVIR + 7}, {ACC_LVIR + 8, -1}};
+        const int slots[8][2] = {{slot_e, -1}, {slot_e2, -1}, {ACC_LVIR + 0, -1},
+                                 {ACC_LVIR + 1, ACC_LVIR + 3}, {ACC_LVIR + 2, ACC_LVIR + 6},
+                                 {ACC_LVIR + 4, -1}, {ACC_LVIR + 5, ACC_LVIR + 7}, {ACC_LVIR + 8, -1}};
         const long long fx = to_fix(t, ACC_SCALE);
         atomicAdd((unsigned long long *)&acc[slots[threadIdx.x][0]], (unsigned long long)fx);
         if (slots[threadIdx.x][1] >= 0)
@@ -171,8 +273,11 @@ __global__ void k_rsk_reduce(int nk, const double *partial, const double *kcoef,
     }
 }
 
-// Per-site forces and torques; F_TPS threads split the k set, k data staged
-// in shared memory.  PERM / IND select the permanent and induced terms.
+// ---------------------------------------------------------------------------
+// FP64 per-site forces and torques
+// ---------------------------------------------------------------------------
+// F_TPS threads split the k set, k data staged in shared memory.  PERM / IND
+// select the permanent and induced terms.
 template <typename R, bool PERM, bool IND>
 __global__ void __launch_bounds__(256) k_rforce(int n, int nk, const double4 *pos4, const int4 *fixq,
                                                 const int *kn, const double *kvec, const double *kcoef,
@@ -258,6 +363,99 @@ __global__ void __launch_bounds__(256) k_rforce(int n, int nk, const double4 *po
     }
 }
 
+// ---------------------------------------------------------------------------
+// FP32 per-site forces and torques (mixed path): permanent terms, with the
+// induced ones when IND (the combined form in the header)
+// ---------------------------------------------------------------------------
+template <bool IND>
+__global__ void __launch_bounds__(256) k_rforce_f(int n, int nk, const double4 *pos4, const int4 *fixq,
+                                                  const int *kn, const double *kvec, const double *kcoef,
+                                                  const double *sk, const double *tq, const double *mu,
+                                                  const double *qd, const double *pind, long long *frc,
+                                                  long long *trq) {
+    __shared__ float4 s_kb[FK_TILE];   // kx, ky, kz, 2c
+    __shared__ float2 s_uw[FK_TILE];   // U, W
+    __shared__ int4 s_n[FK_TILE];      // integer k
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gt / F_TPS, t = gt % F_TPS;
+    int4 pf = make_int4(0, 0, 0, 0);
+    float qi = 0.f, dx = 0.f, dy = 0.f, dz = 0.f;
+    float Qxx = 0.f, Qxy = 0.f, Qxz = 0.f, Qyy = 0.f, Qyz = 0.f, Qzz = 0.f;
+    if (i < n) {
+        pf = fixq[i];
+        qi = (float)(tq[(int)pos4[i].w] / SQC_R);
+        double d3[3] = {mu[i], mu[n + i], mu[2 * n + i]};
+        if (IND)
+            for (int d = 0; d < 3; d++) d3[d] += pind[(size_t)d * n + i];
+        dx = (float)d3[0]; dy = (float)d3[1]; dz = (float)d3[2];
+        Qxx = (float)qd[i]; Qxy = (float)qd[n + i]; Qxz = (float)qd[2 * n + i];
+        Qyy = (float)qd[3 * n + i]; Qyz = (float)qd[4 * n + i]; Qzz = (float)qd[5 * n + i];
+    }
+    double F[3] = {0, 0, 0}, EA[3] = {0, 0, 0}, GX[3] = {0, 0, 0};
+    for (int base = 0; base < nk; base += FK_TILE) {
+        __syncthreads();
+        const int kk = base + threadIdx.x;
+        if (kk < nk) {
+            const double CqQ = sk[kk], SqQ = sk[nk + kk], Cm = sk[2 * (size_t)nk + kk], Sm = sk[3 * (size_t)nk + kk];
+            double U = CqQ - Sm, W = SqQ + Cm;
+            if (IND) {
+                U -= sk[5 * (size_t)nk + kk];
+                W += sk[4 * (size_t)nk + kk];
+            }
+            s_kb[threadIdx.x] = make_float4((float)kvec[kk], (float)kvec[nk + kk], (float)kvec[2 * (size_t)nk + kk],
+                                            (float)(2.0 * kcoef[kk]));
+            s_uw[threadIdx.x] = make_float2((float)U, (float)W);
+            s_n[threadIdx.x] = make_int4(kn[kk], kn[nk + kk], kn[2 * (size_t)nk + kk], 0);
+        }
+        __syncthreads();
+        const int cnt = min(FK_TILE, nk - base);
+        if (i < n) {
+            float f0 = 0.f, f1 = 0.f, f2 = 0.f, e0 = 0.f, e1 = 0.f, e2 = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
+#pragma unroll 2
+            for (int q = t; q < cnt; q += F_TPS) {
+                const float4 kb = s_kb[q];
+                const float2 uw = s_uw[q];
+                const int4 nn = s_n[q];
+                const int ph = (int)((unsigned)nn.x * (unsigned)pf.x + (unsigned)nn.y * (unsigned)pf.y +
+                                     (unsigned)nn.z * (unsigned)pf.z);
+                float sn, cs;
+                sincos_phase32(ph, sn, cs);
+                const float A = fmaf(sn, uw.x, -cs * uw.y);
+                const float B = fmaf(cs, uw.x, sn * uw.y);
+                const float qkx = fmaf(Qxx, kb.x, fmaf(Qxy, kb.y, Qxz * kb.z));
+                const float qky = fmaf(Qxy, kb.x, fmaf(Qyy, kb.y, Qyz * kb.z));
+                const float qkz = fmaf(Qxz, kb.x, fmaf(Qyz, kb.y, Qzz * kb.z));
+                const float qk = qi - fmaf(kb.x, qkx, fmaf(kb.y, qky, kb.z * qkz));
+                const float mk = fmaf(dx, kb.x, fmaf(dy, kb.y, dz * kb.z));
+                const float bA = kb.w * A, bB = kb.w * B;
+                const float al = fmaf(qk, bA, mk * bB);
+                f0 = fmaf(al, kb.x, f0); f1 = fmaf(al, kb.y, f1); f2 = fmaf(al, kb.z, f2);
+                e0 = fmaf(bA, kb.x, e0); e1 = fmaf(bA, kb.y, e1); e2 = fmaf(bA, kb.z, e2);
+                // k x (Q k)
+                g0 = fmaf(bB, fmaf(kb.y, qkz, -kb.z * qky), g0);
+                g1 = fmaf(bB, fmaf(kb.z, qkx, -kb.x * qkz), g1);
+                g2 = fmaf(bB, fmaf(kb.x, qky, -kb.y * qkx), g2);
+            }
+            F[0] += f0; F[1] += f1; F[2] += f2;
+            EA[0] += e0; EA[1] += e1; EA[2] += e2;
+            GX[0] += g0; GX[1] += g1; GX[2] += g2;
+        }
+    }
+    for (int d = 0; d < 3; d++) {
+        F[d] = group_sum<F_TPS>(F[d]);
+        EA[d] = group_sum<F_TPS>(EA[d]);
+        GX[d] = group_sum<F_TPS>(GX[d]);
+    }
+    if (i < n && t == 0) {
+        // torque on the permanent multipoles: mu x EA - 2 GX
+        const V3 m = v3(mu[i], mu[n + i], mu[2 * n + i]);
+        const V3 ea = v3(EA[0], EA[1], EA[2]);
+        const V3 tau = crs(m, ea) - 2.0 * v3(GX[0], GX[1], GX[2]);
+        add_fix3(frc, n, i, v3(F[0], F[1], F[2]), KE);
+        add_fix3(trq, n, i, tau, KE);
+    }
+}
+
 namespace {
 struct RecipBufs {
     double *partial, *sk;
@@ -268,19 +466,19 @@ RecipBufs bufs(Ctx &c) {
 }
 
 template <int MODE>
-void sums(Ctx &c, int slot_e) {
+void sums(Ctx &c, int slot_e, int slot_e2 = -1) {
     const int nk = c.rc.nk;
     RecipBufs B = bufs(c);
     dim3 g1((nk + MK_THREADS - 1) / MK_THREADS, MK_CHUNKS);
     if (c.precision == SMD_PREC_MIXED)
-        k_rsk_partial<float, MODE><<<g1, MK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,
-                                                                   c.type_q, c.mu, c.qd, c.pind, B.partial);
+        k_rsk_partial_f<MODE><<<g1, MK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,
+                                                               c.type_q, c.mu, c.qd, c.pind, B.partial);
     else
         k_rsk_partial<double, MODE><<<g1, MK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,
                                                                     c.type_q, c.mu, c.qd, c.pind, B.partial);
     k_rsk_reduce<MODE><<<(nk + 255) / 256, 256, 0, c.stream>>>(nk, B.partial, c.rc.kcoef, c.rc.kvec,
                                                               1.0 / (4.0 * c.ew_alpha * c.ew_alpha), B.sk,
-                                                              c.acc, slot_e);
+                                                              c.acc, slot_e, slot_e2);
 }
 
 template <bool PERM, bool IND>
@@ -288,12 +486,18 @@ void forces(Ctx &c) {
     const int nk = c.rc.nk;
     RecipBufs B = bufs(c);
     const int nb = (int)(((long long)c.n * F_TPS + 255) / 256);
-    if (c.precision == SMD_PREC_MIXED)
-        k_rforce<float, PERM, IND><<<nb, 256, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec, c.rc.kcoef,
-                                                            B.sk, c.type_q, c.mu, c.qd, c.pind, c.frc, c.trq);
-    else
+    if (c.precision == SMD_PREC_MIXED) {
+        if (PERM)
+            k_rforce_f<IND><<<nb, 256, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec, c.rc.kcoef,
+                                                      B.sk, c.type_q, c.mu, c.qd, c.pind, c.frc, c.trq);
+        else
+            k_rforce<float, PERM, IND><<<nb, 256, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,
+                                                                c.rc.kcoef, B.sk, c.type_q, c.mu, c.qd, c.pind,
+                                                                c.frc, c.trq);
+    } else {
         k_rforce<double, PERM, IND><<<nb, 256, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec, c.rc.kcoef,
                                                              B.sk, c.type_q, c.mu, c.qd, c.pind, c.frc, c.trq);
+    }
 }
 }  // namespace
 
@@ -312,14 +516,11 @@ void launch_ind_long(Ctx &c) {
     forces<false, true>(c);
 }
 
-// within a time step: permanent sums before the dipole solve ...
-void launch_mp_long_sums(Ctx &c) {
-    if (c.rc.nk) sums<0>(c, ACC_E_LONG);
-}
-// ... induced sums after it, then one force pass for both
-void launch_polar_long_rest(Ctx &c) {
+// Both reciprocal terms of a time step, after the dipole solve: one pass for
+// all six structure factors, one force pass
+void launch_polar_long(Ctx &c) {
     if (c.rc.nk == 0) return;
-    sums<1>(c, ACC_E_POL_LONG);
+    sums<2>(c, ACC_E_LONG, ACC_E_POL_LONG);
     forces<true, true>(c);
 }
 

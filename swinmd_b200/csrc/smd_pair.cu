@@ -46,6 +46,8 @@ struct PairArgs {
     double alpha, alpha2, alpha2pi, ew_rc2;
     // buffered 14-7 (BuffvdWForce): exponents, buffers, taper
     double bn, bm, bdelta, bgamma, bc[6], bsw2;
+    float bswf, bwinv;  // taper start and 1/(cutoff - start), FP32 path
+    int buff_int;       // n - m and m are small positive integers
     long long *frc;
     long long *acc;
 };
@@ -203,14 +205,114 @@ __device__ __forceinline__ void vdw_pair_f(float r2f, float dr2, float &e, float
     }
 }
 
+// FP32 value with its first-order relative error: true value ~ v (1 + d).
+// Every rounding of the buffered 14-7 chain is recovered exactly (FMA
+// product/division remainders, two-sum) and carried in d, so the n-m and m
+// fold powers do not amplify the roundings of r, rho + delta and the two
+// quotients; what is left is a few final roundings per pair.
+struct FE {
+    float v, d;
+};
+__device__ __forceinline__ float fe_rel(float err, float v) { return v != 0.f ? __fdividef(err, v) : 0.f; }
+__device__ __forceinline__ FE fe_mul(FE a, FE b) {
+    const float v = a.v * b.v;
+    return {v, a.d + b.d + fe_rel(fmaf(a.v, b.v, -v), v)};
+}
+__device__ __forceinline__ FE fe_div(FE a, FE b) {
+    const float v = __fdiv_rn(a.v, b.v);
+    const float rem = fmaf(-v, b.v, a.v);   // exact: a - v b
+    return {v, a.d - b.d + fe_rel(rem, a.v)};
+}
+__device__ __forceinline__ FE fe_add(FE a, FE b) {
+    const float s = a.v + b.v;
+    const float bb = s - a.v;
+    const float err = (a.v - (s - bb)) + (b.v - bb);
+    return {s, fe_rel(err + a.v * a.d + b.v * b.d, s)};
+}
+__device__ __forceinline__ FE fe_pow(FE x, int k) {
+    FE r = {1.f, 0.f};
+    bool first = true;
+    while (k > 0) {
+        if (k & 1) {
+            r = first ? x : fe_mul(r, x);
+            first = false;
+        }
+        k >>= 1;
+        if (k) x = fe_mul(x, x);
+    }
+    return r;
+}
+__device__ __forceinline__ FE fe_of(double x) {
+    const float v = (float)x;
+    return {v, v != 0.f ? (float)((x - (double)v) / (double)v) : 0.f};
+}
+__device__ __forceinline__ float fe_val(FE a) { return fmaf(a.v, a.d, a.v); }
+
+struct BuffF {
+    FE delta, gamma, c1, c2;
+    int nm, m;
+};
+
+// FP32 buffered 14-7 between virtual sites for integer exponents (the same
+// formula as vdw_pair<VDW_BUFF>).  tp = (1/sigma, its relative rounding,
+// eps, its relative rounding).  The taper is evaluated in its equivalent
+// well-conditioned form S = (1-t)^3 (1 + 3t + 6t^2), t = (r - rs)/(rc - rs),
+// which the reference's monomial coefficients c0..c5 expand.
+__device__ __forceinline__ void buff_pair_f(float r2f, float dr2, float &e, float &fs, float4 tp,
+                                            const BuffF &b, const PairArgs &a, bool same) {
+    e = 0.f;
+    fs = 0.f;
+    if (same || !(r2f <= (float)a.vdw_rc2) || tp.z == 0.f) return;
+    const float r = sqrtf(r2f);
+    const float dr = 0.5f * (fmaf(-r, r, r2f) / r2f + dr2);   // r_exact = r (1 + dr)
+    const FE IS = {tp.x, tp.y}, EPS = {tp.z, tp.w};
+    const FE rho = fe_mul(FE{r, dr}, IS);
+    const FE sd = fe_add(rho, b.delta);
+    const FE P1n = fe_pow(fe_div(b.c1, sd), b.nm);
+    const FE rm1 = fe_pow(rho, b.m - 1);
+    const FE dm = fe_add(fe_mul(rm1, rho), b.gamma);
+    const FE P2 = fe_div(b.c2, dm);
+    const FE EP = fe_mul(EPS, P1n);
+    const FE E = fe_mul(EP, fe_add(P2, FE{-2.f, 0.f}));
+    const FE t1 = fe_div(fe_mul(fe_mul(E, FE{(float)b.nm, 0.f}), IS), sd);
+    const FE t2 = fe_div(fe_mul(fe_mul(fe_mul(EP, P2), FE{(float)b.m, 0.f}), fe_mul(rm1, IS)), dm);
+    float en = fe_val(E);
+    float tmpf = -(fe_val(t1) + fe_val(t2));
+    if (a.switch_on && r2f > (float)a.bsw2) {
+        const float t = fminf(1.f, fmaxf(0.f, (r - a.bswf) * a.bwinv));
+        const float o = 1.f - t;
+        const float sv = o * o * o * fmaf(6.f * t, t, fmaf(3.f, t, 1.f));
+        const float dsv = -30.f * t * t * o * o * a.bwinv;
+        tmpf = tmpf * sv + en * dsv;
+        en *= sv;
+    }
+    e = en;
+    fs = -tmpf / r * (1.f - dr);
+}
+
 template <typename R, int VDW, bool EWALD, int TPP>
 __global__ void __launch_bounds__(PAIR_BLOCK) k_pair(PairArgs a) {
     __shared__ R s_par[MAX_TYPES * MAX_TYPES * 4];
     __shared__ R s_q[MAX_TYPES];
     __shared__ double s_red[PAIR_BLOCK / 32][11];
+    constexpr bool BUFF_F = sizeof(R) == 4 && VDW == VDW_BUFF;
+    __shared__ float4 s_bf[BUFF_F ? MAX_TYPES * MAX_TYPES : 1];
     const int nt2 = a.ntypes * a.ntypes;
     for (int k = threadIdx.x; k < nt2 * 4; k += blockDim.x) s_par[k] = R(a.par[k]);
     for (int k = threadIdx.x; k < a.ntypes; k += blockDim.x) s_q[k] = R(a.type_q[k]);
+    BuffF bf{};
+    if (BUFF_F) {
+        for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
+            const FE is = fe_of(1.0 / a.par[k * 4 + 0]), ep = fe_of(a.par[k * 4 + 1]);
+            s_bf[k] = make_float4(is.v, is.d, ep.v, ep.d);
+        }
+        bf.delta = fe_of(a.bdelta);
+        bf.gamma = fe_of(a.bgamma);
+        bf.c1 = fe_of(1.0 + a.bdelta);
+        bf.c2 = fe_of(1.0 + a.bgamma);
+        bf.nm = (int)(a.bn - a.bm);
+        bf.m = (int)a.bm;
+    }
     __syncthreads();
 
     const int gt = blockIdx.x * blockDim.x + threadIdx.x;
@@ -271,6 +373,8 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_pair(PairArgs a) {
             if (sizeof(R) == 4 && VDW == VDW_LJ)
                 lj_pair_f((float)r2, r2c, *(float *)&e, *(float *)&fs,
                           (const float *)&s_par[(ti * a.ntypes + tj) * 4], a, same);
+            else if (BUFF_F && a.buff_int)
+                buff_pair_f((float)r2, r2c, *(float *)&e, *(float *)&fs, s_bf[ti * a.ntypes + tj], bf, a, same);
             else if (sizeof(R) == 4 && (VDW == VDW_MIE || VDW == VDW_BMH))
                 vdw_pair_f<VDW>((float)r2, r2c, *(float *)&e, *(float *)&fs,
                                 (const float *)&s_par[(ti * a.ntypes + tj) * 4], a, same);
@@ -449,6 +553,13 @@ void launch_pair(Ctx &c) {
     a.bn = c.buff_n; a.bm = c.buff_m; a.bdelta = c.buff_delta; a.bgamma = c.buff_gamma;
     for (int q = 0; q < 6; q++) a.bc[q] = c.buff_c[q];
     a.bsw2 = c.buff_sw * c.buff_sw;
+    a.bswf = (float)c.buff_sw;
+    a.bwinv = (float)(1.0 / (sqrt(c.vdw_rc2) - c.buff_sw));
+    {
+        const double nm = c.buff_n - c.buff_m;
+        a.buff_int = nm == floor(nm) && c.buff_m == floor(c.buff_m) && nm >= 1 && nm <= 64 && c.buff_m >= 1 &&
+                     c.buff_m <= 64;
+    }
     const bool buff = c.vdw == VDW_BUFF;
     if (buff) {
         // the pair term acts between the virtual sites; their forces are
