@@ -99,6 +99,7 @@ int alloc_list(smd_ctx *x) {
     }
     c.list_valid = 0;
     c.graph_dirty = 1;
+    if (ensure_ind_rows(c)) return fail(x, SMD_ERR_CUDA, "dipole-solve tensor rows: allocation failed");
     return SMD_OK;
 }
 
@@ -206,7 +207,7 @@ void smd_destroy(smd_ctx *x) {
                     c.series, c.pl.nbr, c.pl.nnbr, c.pl.cell_of, c.pl.cell_slot,
                     c.pl.cell_count, c.pl.cell_start, c.pl.cell_atoms, c.rc.kn, c.rc.kcoef,
                     c.rc.sk, c.rc.kvec, c.clen2, c.type_mp, c.type_polar, c.mu, c.qd, c.trq, c.e0,
-                    c.pind, c.cgw, c.cgs, c.cg_bar, c.vpos4, c.vfixq, c.fv};
+                    c.pind, c.cgw, c.cgs, c.cg_bar, c.vpos4, c.vfixq, c.fv, c.ind_rj, c.ind_rc, c.ind_cnt};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -317,6 +318,7 @@ int smd_set_exclusions(smd_ctx *x, const int32_t *offsets, const int32_t *partne
     if (tot) CK(cudaMemcpy(c.excl, partners, tot * sizeof(int), cudaMemcpyHostToDevice));
     c.list_valid = 0;
     c.graph_dirty = 1;
+    if (ensure_ind_rows(c)) return fail(x, SMD_ERR_CUDA, "dipole-solve tensor rows: allocation failed");
     return SMD_OK;
 }
 
@@ -469,15 +471,16 @@ int smd_set_multipole(smd_ctx *x, const double *type_mp, const double *polar, do
     CK(cudaMemcpy(c.type_polar, polar, c.ntypes * sizeof(double), cudaMemcpyHostToDevice));
     const size_t n = c.n;
     CK(dalloc(&c.mu, 3 * n)); CK(dalloc(&c.qd, 6 * n)); CK(dalloc(&c.trq, 3 * n));
-    CK(dalloc(&c.e0, 3 * n)); CK(dalloc(&c.pind, 3 * n)); CK(dalloc(&c.cgw, 12 * n));
+    CK(dalloc(&c.e0, 3 * n)); CK(dalloc(&c.pind, 3 * n)); CK(dalloc(&c.cgw, 20 * n));
     CK(dalloc(&c.frame, 9 * n));
     CK(cudaMemset(c.pind, 0, 3 * n * sizeof(double)));
     CK(cudaMemset(c.e0, 0, 3 * n * sizeof(double)));
     int r = setup_cg(c);
     if (r) return fail(x, r, "smd_set_multipole: solver set-up failed");
-    CK(dalloc(&c.cgs, 8 + 4 * (size_t)c.cg_blocks));
-    CK(cudaMemset(c.cgs, 0, (8 + 4 * (size_t)c.cg_blocks) * sizeof(double)));
+    CK(dalloc(&c.cgs, 8 + 8 * (size_t)c.cg_blocks));
+    CK(cudaMemset(c.cgs, 0, (8 + 8 * (size_t)c.cg_blocks) * sizeof(double)));
     CK(dalloc(&c.cg_bar, 1));
+    if (ensure_ind_rows(c)) return fail(x, SMD_ERR_CUDA, "smd_set_multipole: tensor rows: allocation failed");
     r = setup_recip(c);
     if (r) return fail(x, r, "smd_set_multipole: reciprocal set-up failed");
     c.graph_dirty = 1;

@@ -93,13 +93,17 @@ struct Ctx {
     long long *trq = nullptr;       // [3][N] torques, fixed point
     double *e0 = nullptr;           // [3][N] permanent field at the sites
     double *pind = nullptr;         // [3][N] induced dipoles
-    double *cgw = nullptr;          // CG work vectors: r, z, v, s  [4][3][N]
-    double *cgs = nullptr;          // CG scalars / partials
+    double *cgw = nullptr;          // CG work: r, z, v [3][N] each, alpha [N], two gather copies [N][4]
+    double *cgs = nullptr;          // CG scalars [8] and partials [2][blocks][4]
     int cg_max_iter = 500;
     double cg_tol = 2.0819e-8;      // RMS dipole change tolerance (e nm); 1e-6 D
     int cg_guess = 0;               // 0: alpha E0, 1: previous step, 2: learned (MLP)
     int cg_blocks = 0;
     unsigned int *cg_bar = nullptr; // grid-barrier counter
+    int *ind_rj = nullptr;          // damped-tensor rows of the solve: partners [N][cap]
+    void *ind_rc = nullptr;         // coefficients [N][cap] (float4 or double4)
+    int *ind_cnt = nullptr;         // row lengths [N]
+    int ind_cap = 0;
     double *frame = nullptr;        // [9][N] site axes u, v, w (lab frame)
     // per-site network giving the initial induced dipoles (smd_mlp.cu)
     int mlp_ready = 0;
@@ -162,6 +166,7 @@ void launch_torques_end(Ctx &c);
 void launch_frames(Ctx &c);
 void launch_buff(Ctx &c);
 int setup_cg(Ctx &c);
+int ensure_ind_rows(Ctx &c);
 // dipole-guess network (smd_mlp.cu)
 int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed);
 void launch_mlp_guess(Ctx &c);

@@ -21,6 +21,8 @@
 //                 correction energy (:1760-2150; energy only under
 //                 constraints)
 // The reciprocal term is mp_recip<6> in smd_multipole.cu.
+#include <algorithm>
+#include <type_traits>
 #include "smd_ctx.cuh"
 #include "smd_polar.cuh"
 
@@ -57,9 +59,11 @@ struct IndArgs {
 // ---------------------------------------------------------------------------
 // permanent field
 // ---------------------------------------------------------------------------
-// field at i from site j, r = r_i - r_j (Induction.cpp:293-425)
+// field at i from site j, r = r_i - r_j (Induction.cpp:293-425); also
+// returns the damped dipole-tensor coefficients of the pair,
+// T = c5 r r^T - c3 I with c3 = l3/r^3, c5 = 3 l5/r^5
 __device__ __forceinline__ V3 perm_field(V3 r, double r2, double qj, V3 mj, const Q6 &Qj, double pi_,
-                                         double pj_, double a) {
+                                         double pj_, double a, double &c3, double &c5) {
     const double rr = sqrt(r2);
     const double r_1 = 1.0 / rr, r_3 = r_1 * r_1 * r_1, r_5 = r_3 * r_1 * r_1, r_7 = r_5 * r_1 * r_1;
     const double u3 = r2 * rr / sqrt(pi_ * pj_);
@@ -68,69 +72,84 @@ __device__ __forceinline__ V3 perm_field(V3 r, double r2, double qj, V3 mj, cons
     const double l7 = 1.0 - (1.0 + a * u3 + 3.0 * a * a * u3 * u3 / 5.0) * e;
     const V3 Qjr = qv(Qj, r);
     const double QjRij = dot(r, Qjr), QjI = qtr(Qj);
+    c3 = l3 * r_3;
+    c5 = 3.0 * l5 * r_5;
     return (qj * l3 * r_3) * r + (3.0 * l5 * r_5 * dot(r, mj)) * r - (l3 * r_3) * mj +
            (15.0 * l7 * r_7 * QjRij) * r - (6.0 * l5 * r_5) * Qjr - (3.0 * l5 * r_5 * QjI) * r;
 }
 
-__global__ void k_ind_field(IndArgs a) {
+// Rows of the damped tensor the dipole solve applies: for site i, slot s
+// (s < cnt[i]) holds the partner j and (sqrt(c5) r, c3), so that
+// T_ij v = (r'.v) r' - c3 v.  TS is the storage type: double in the FP64
+// path, float in the mixed path.  Rows are site-major, so the lanes of one
+// site read consecutive slots.
+struct TRows {
+    int *j;       // [N][cap]
+    void *c;      // [N][cap] of TS4
+    int *cnt;     // [N]
+    int cap;
+};
+
+template <typename TS>
+__device__ __forceinline__ void put_row(const TRows &R, int i, int s, int j, V3 r, double c3, double c5,
+                                        unsigned int *status) {
+    if (s >= R.cap) {
+        atomicOr(status, ST_LIST_OVERFLOW);
+        return;
+    }
+    const double sc = sqrt(c5);
+    const size_t at = (size_t)i * R.cap + s;
+    R.j[at] = j;
+    using TS4 = typename std::conditional<sizeof(TS) == 4, float4, double4>::type;
+    ((TS4 *)R.c)[at] = TS4{(TS)(sc * r.x), (TS)(sc * r.y), (TS)(sc * r.z), (TS)c3};
+}
+
+// Permanent field and tensor rows.  The pairs are those of the reference's
+// A matrix within cutoffInd: Verlet-list neighbours (compacted in list order
+// with a ballot per pass of the site's lanes) and then the molecule's
+// excluded sites, which enter A but not the field.
+template <typename TS>
+__global__ void __launch_bounds__(256) k_ind_field(IndArgs a, TRows R, unsigned int *status) {
     const int gt = blockIdx.x * blockDim.x + threadIdx.x;
     constexpr int TPP = 8;
     const int i = gt / TPP, t = gt % TPP;
+    const int lane = threadIdx.x & 31, gbase = lane & ~(TPP - 1);
     V3 E = v3(0, 0, 0);
-    if (i < a.n) {
-        const double4 pi = a.pos4[i];
-        const double poli = fmax(1e-8, a.polar[(int)pi.w]);
-        const int cnt = a.nnbr[i];
-        for (int k = t; k < cnt; k += TPP) {
-            const int j = a.nbr[(size_t)k * a.n + i] & 0x7fffffff;
+    const bool own = i < a.n;
+    double4 pi = make_double4(0, 0, 0, 0);
+    double poli = 1;
+    int cnt = 0;
+    if (own) {
+        pi = a.pos4[i];
+        poli = fmax(1e-8, a.polar[(int)pi.w]);
+        cnt = a.nnbr[i];
+    }
+    const int wmax = __reduce_max_sync(0xffffffffu, cnt);
+    int base = 0;
+    for (int k0 = 0; k0 < wmax; k0 += TPP) {
+        const int k = k0 + t;
+        bool valid = false;
+        int j = 0;
+        V3 r = v3(0, 0, 0);
+        double c3 = 0, c5 = 0;
+        if (k < cnt) {
+            j = a.nbr[(size_t)k * a.n + i] & 0x7fffffff;
             const double4 pj = a.pos4[j];
-            const V3 r = mind(pi, pj, a.box);
+            r = mind(pi, pj, a.box);
             const double rr = sqrt(dot(r, r)), r2 = rr * rr;
-            if (!(r2 <= a.cut2)) continue;
-            E = E + perm_field(r, r2, a.tq[(int)pj.w] / SQC, ld3i(a.mu, a.n, j), ldqi(a.qd, a.n, j), poli,
-                               fmax(1e-8, a.polar[(int)pj.w]), a.a);
+            if (r2 <= a.cut2) {
+                valid = true;
+                E = E + perm_field(r, r2, a.tq[(int)pj.w] / SQC, ld3i(a.mu, a.n, j), ldqi(a.qd, a.n, j), poli,
+                                   fmax(1e-8, a.polar[(int)pj.w]), a.a, c3, c5);
+            }
         }
+        const unsigned grp = (__ballot_sync(0xffffffffu, valid) >> gbase) & ((1u << TPP) - 1);
+        if (valid) put_row<TS>(R, i, base + __popc(grp & ((1u << t) - 1)), j, r, c3, c5, status);
+        base += __popc(grp);
     }
     E.x = group_sum<TPP>(E.x); E.y = group_sum<TPP>(E.y); E.z = group_sum<TPP>(E.z);
-    if (i < a.n && t == 0) {
+    if (own && t == 0) {
         a.e0[i] = E.x; a.e0[a.n + i] = E.y; a.e0[2 * a.n + i] = E.z;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// matrix-free A v and the PCG solve
-// ---------------------------------------------------------------------------
-// (A v)_i = v_i / a_i - sum_j T_ij v_j, T_ij = l5 3 r r^T / r^5 - l3 / r^3
-// over Verlet-list neighbours and the molecule's other sites within cutoffInd
-__device__ __forceinline__ V3 tmul(V3 r, double r2, V3 v, double pi_, double pj_, double a) {
-    const double rr = sqrt(r2);
-    const double r_1 = 1.0 / rr, r_3 = r_1 * r_1 * r_1, r_5 = r_3 * r_1 * r_1;
-    const double u3 = r2 * rr / sqrt(pi_ * pj_);
-    const double e = exp(-a * u3);
-    const double l3 = 1.0 - e, l5 = 1.0 - (1.0 + a * u3) * e;
-    return (l5 * 3.0 * r_5 * dot(r, v)) * r - (l3 * r_3) * v;
-}
-
-// vectors written by other blocks of the persistent solver are read past L1
-__device__ __forceinline__ V3 ld3cg(const double *a, int n, int i) {
-    return v3(__ldcg(&a[i]), __ldcg(&a[n + i]), __ldcg(&a[2 * n + i]));
-}
-
-__device__ V3 apply_A(const IndArgs &a, int i, const double *v, int t, int tpp) {
-    const double4 pi = a.pos4[i];
-    const double poli = fmax(1e-8, a.polar[(int)pi.w]);
-    V3 acc = v3(0, 0, 0);
-    const int cnt = a.nnbr[i];
-    for (int k = t; k < cnt; k += tpp) {
-        const int j = a.nbr[(size_t)k * a.n + i] & 0x7fffffff;
-        const double4 pj = a.pos4[j];
-        const V3 r = mind(pi, pj, a.box);
-        const double rr = sqrt(dot(r, r)), r2 = rr * rr;
-        if (!(r2 <= a.cut2)) continue;
-        acc = acc - tmul(r, r2, ld3cg(v, a.n, j), poli, fmax(1e-8, a.polar[(int)pj.w]), a.a);
-    }
-    if (t == 0) {
-        // the molecule's excluded sites (not in the Verlet list, but in A)
         const int m = a.mol[i];
         for (int q = a.mol_off[m]; q < a.mol_off[m + 1]; q++) {
             const int j = a.mol_atoms[q];
@@ -139,25 +158,39 @@ __device__ V3 apply_A(const IndArgs &a, int i, const double *v, int t, int tpp) 
             const V3 r = mind(pi, pj, a.box);
             const double rr = sqrt(dot(r, r)), r2 = rr * rr;
             if (!(r2 <= a.cut2)) continue;
-            acc = acc - tmul(r, r2, ld3cg(v, a.n, j), poli, fmax(1e-8, a.polar[(int)pj.w]), a.a);
+            const double ipp = 1.0 / sqrt(poli * fmax(1e-8, a.polar[(int)pj.w]));
+            const double u3 = r2 * rr * ipp, e = exp(-a.a * u3);
+            const double r_3 = 1.0 / (r2 * rr);
+            put_row<TS>(R, i, base++, j, r, (1.0 - e) * r_3, 3.0 * (1.0 - (1.0 + a.a * u3) * e) * r_3 / r2, status);
         }
-        acc = acc + (1.0 / poli) * ld3cg(v, a.n, i);
+        R.cnt[i] = base < R.cap ? base : R.cap;
     }
-    return acc;
 }
 
+// ---------------------------------------------------------------------------
+// matrix-free A v and the PCG solve
+// ---------------------------------------------------------------------------
+// (A v)_i = v_i / a_i - sum_j T_ij v_j over the site's tensor row (the
+// Verlet-list neighbours and the molecule's other sites within cutoffInd)
+
 // Grid barrier with a bounded spin: every block of the (co-resident)
-// cooperative launch arrives once per phase; a block that waits longer than
-// the cap raises ST_CG_ITER and returns false, and the caller stops.
+// cooperative launch arrives once per phase (release add), then polls the
+// counter with acquire loads; a block that waits longer than the cap raises
+// ST_CG_ITER and returns false, and the caller stops.
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned int *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ bool grid_barrier(unsigned int *bar, unsigned int target, unsigned int *status) {
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
-        atomicAdd(bar, 1u);
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" : : "l"(bar) : "memory");
         unsigned int spins = 0;
-        while (atomicAdd(bar, 0u) < target) {
-            __nanosleep(64);
-            if (++spins > (1u << 24)) {  // ~1 s
+        while (ld_acquire_u32(bar) < target) {
+            __nanosleep(32);
+            if (++spins > (1u << 25)) {  // ~1 s
                 atomicOr(status, ST_CG_ITER);
                 break;
             }
@@ -170,23 +203,34 @@ __device__ bool grid_barrier(unsigned int *bar, unsigned int target, unsigned in
 
 struct CGArgs {
     IndArgs ia;
-    double *r, *z, *v, *s;   // [3][N] each
-    double *part;            // per block partials [nblocks][4]
-    double *scal;            // [0] iterations, [1] final rms change, [2] initial guess mode
-    unsigned int *bar, *status;
+    TRows rows;
+    double *r, *z, *v, *al;  // [3][N] residual, A v, direction; [N] polarisabilities
+    void *g0, *g1;           // per-site packed copies (float4 / double4) of the start dipoles and of v
+    double *part;            // partials [2][nblocks][4]
+    double *scal;            // [0] iterations, [1] final rms change
+    unsigned *bar, *status;
     int nblocks, max_iter, guess;
     double tol;
 };
 
-// fixed-order block sums, every block computes the same totals
-__device__ void grid_sum(const double *part, int nblocks, int nq, double *out, double *s_tmp) {
-    if (threadIdx.x < nq) {
-        double t = 0;
-        for (int b = 0; b < nblocks; b++) t += __ldcg(&part[b * 4 + threadIdx.x]);
-        s_tmp[threadIdx.x] = t;
+// fixed-order block sums, every block computes the same totals: each thread
+// loads a strided share of the block partials (all loads in flight at once),
+// then a fixed shuffle tree and a fixed pass over the warps
+__device__ void grid_sum(const double *part, int nblocks, int nq, double *out, double (*s_w)[4]) {
+    double v[4] = {0, 0, 0, 0};
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+        for (int q = 0; q < nq; q++) v[q] += __ldcg(&part[b * 4 + q]);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int q = 0; q < nq; q++) {
+        const double t = warp_sum(v[q]);
+        if (lane == 0) s_w[w][q] = t;
     }
     __syncthreads();
-    for (int q = 0; q < nq; q++) out[q] = s_tmp[q];
+    for (int q = 0; q < nq; q++) {
+        double t = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += s_w[k][q];
+        out[q] = t;
+    }
     __syncthreads();
 }
 
@@ -207,96 +251,166 @@ __device__ void block_partials(double *vals, int nq, double *part, double (*s_w)
 constexpr int CG_THREADS = 256;
 constexpr int CG_TPP = 8;
 
-__global__ void __launch_bounds__(CG_THREADS) k_ind_cg(CGArgs c) {
+__device__ __forceinline__ double4 ldcg4(const double4 *p) {
+    const double2 a = __ldcg((const double2 *)p), b = __ldcg((const double2 *)p + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ float4 ldcg4(const float4 *p) { return __ldcg(p); }
+
+// (A v)_i from the site's row: CG_TPP lanes take consecutive slots; the
+// row entries are read in batches of CG_UNROLL per lane before the gathers
+// of v, so each lane keeps several loads in flight.  GR is the arithmetic
+// type of the products (the row's storage type), summed per lane in GR.
+template <typename G4, typename GR>
+__device__ V3 amul(const CGArgs &c, int i, int t, const G4 *g) {
+    constexpr int CG_UNROLL = sizeof(GR) == 4 ? 4 : 2;
+    const TRows &R = c.rows;
+    const int cnt = R.cnt[i];
+    const int *rj = R.j + (size_t)i * R.cap;
+    const G4 *rc = (const G4 *)R.c + (size_t)i * R.cap;
+    GR ax = 0, ay = 0, az = 0;
+    for (int s0 = t; s0 < cnt; s0 += CG_UNROLL * CG_TPP) {
+        int jj[CG_UNROLL];
+        G4 cc[CG_UNROLL];
+#pragma unroll
+        for (int u = 0; u < CG_UNROLL; u++) {
+            const int s = s0 + u * CG_TPP;
+            jj[u] = s < cnt ? rj[s] : -1;
+            if (s < cnt) cc[u] = rc[s];
+        }
+        G4 vj[CG_UNROLL];
+#pragma unroll
+        for (int u = 0; u < CG_UNROLL; u++)
+            if (jj[u] >= 0) vj[u] = ldcg4(&g[jj[u]]);
+#pragma unroll
+        for (int u = 0; u < CG_UNROLL; u++)
+            if (jj[u] >= 0) {
+                const GR rv = cc[u].x * vj[u].x + cc[u].y * vj[u].y + cc[u].z * vj[u].z;
+                ax += cc[u].w * vj[u].x - rv * cc[u].x;
+                ay += cc[u].w * vj[u].y - rv * cc[u].y;
+                az += cc[u].w * vj[u].z - rv * cc[u].z;
+            }
+    }
+    V3 acc = v3(ax, ay, az);
+    if (t == 0) {
+        const G4 vi = ldcg4(&g[i]);
+        acc = acc + (1.0 / __ldcg(&c.al[i])) * v3(vi.x, vi.y, vi.z);
+    }
+    return acc;
+}
+
+// Jacobi-preconditioned CG (M^-1 = diag(a_i)) as one persistent cooperative
+// kernel, three grid barriers per iteration:
+//   A  z = A v (TPP lanes per site), v.z          | barrier, alpha = rs / v.z
+//   B  p += alpha v, r -= alpha z, rs' = r.a r,   | barrier, stop on the RMS
+//      |alpha v|^2                                |  change of p, beta
+//   C  v = a r + beta v, packed copy of v         | barrier
+// The two reductions use separate partial buffers, so no extra barrier
+// guards their reuse.  Vectors written in one phase and read by other
+// blocks in the next are read past L1.
+template <bool F32>
+__global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
+    using G4 = typename std::conditional<F32, float4, double4>::type;
+    using GR = typename std::conditional<F32, float, double>::type;
     __shared__ double s_w[CG_THREADS / 32][4];
-    __shared__ double s_tmp[4];
     const IndArgs &a = c.ia;
     const int n = a.n;
-    const int sites_per_pass = (c.nblocks * CG_THREADS) / CG_TPP;
-    const int gslot = (blockIdx.x * CG_THREADS + threadIdx.x) / CG_TPP, t = threadIdx.x % CG_TPP;
+    G4 *g0 = (G4 *)c.g0, *g1 = (G4 *)c.g1;
+    double *part0 = c.part, *part1 = c.part + 4 * c.nblocks;
+    const int nthreads = c.nblocks * CG_THREADS;
+    const int gtid = blockIdx.x * CG_THREADS + threadIdx.x;
+    const int sites_per_pass = nthreads / CG_TPP;
+    const int gslot = gtid / CG_TPP, t = threadIdx.x % CG_TPP;
     // every lane runs the same number of passes, so the group shuffles in
     // the matrix-vector products always see full warps
     const int passes = (n + sites_per_pass - 1) / sites_per_pass;
     unsigned int phase = 0;
     double tot[4];
     // p0: alpha E0 (guess 0) or the dipoles already in p (previous step / learned)
-    double vals[4] = {0, 0, 0, 0};
-    for (int i = gslot; i < n; i += sites_per_pass) {
-        if (c.guess == 0 && t == 0) {
-            const double pol = fmax(1e-8, a.polar[(int)a.pos4[i].w]);
-            for (int d = 0; d < 3; d++) a.p[d * n + i] = pol * a.e0[d * n + i];
+    for (int i = gtid; i < n; i += nthreads) {
+        const double al = fmax(1e-8, a.polar[(int)a.pos4[i].w]);
+        c.al[i] = al;
+        double p3[3];
+        for (int d = 0; d < 3; d++) {
+            p3[d] = c.guess == 0 ? al * a.e0[d * n + i] : a.p[d * n + i];
+            if (c.guess == 0) a.p[d * n + i] = p3[d];
         }
+        g0[i] = G4{(GR)p3[0], (GR)p3[1], (GR)p3[2], (GR)0};
     }
     if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
-    // r = E0 - A p ; s = M^-1 r ; v = s ; rs = r.s
+    // r = E0 - A p ; v = M^-1 r ; rs = r.M^-1 r
+    double vals[4] = {0, 0, 0, 0};
     for (int ps = 0; ps < passes; ps++) {
         const int i = gslot + ps * sites_per_pass;
-        V3 Ap = i < n ? apply_A(a, i, a.p, t, CG_TPP) : v3(0, 0, 0);
+        V3 Ap = i < n ? amul<G4, GR>(c, i, t, g0) : v3(0, 0, 0);
         Ap.x = group_sum<CG_TPP>(Ap.x); Ap.y = group_sum<CG_TPP>(Ap.y); Ap.z = group_sum<CG_TPP>(Ap.z);
         if (i < n && t == 0) {
-            const double pol = fmax(1e-8, a.polar[(int)a.pos4[i].w]);
+            const double al = __ldcg(&c.al[i]);
             const double rr[3] = {a.e0[i] - Ap.x, a.e0[n + i] - Ap.y, a.e0[2 * n + i] - Ap.z};
             for (int d = 0; d < 3; d++) {
                 c.r[d * n + i] = rr[d];
-                c.s[d * n + i] = pol * rr[d];
-                c.v[d * n + i] = pol * rr[d];
-                vals[0] += rr[d] * pol * rr[d];
+                c.v[d * n + i] = al * rr[d];
+                vals[0] += rr[d] * al * rr[d];
             }
+            g1[i] = G4{(GR)(al * rr[0]), (GR)(al * rr[1]), (GR)(al * rr[2]), (GR)0};
         }
     }
-    block_partials(vals, 1, c.part, s_w);
+    block_partials(vals, 1, part0, s_w);
     if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
-    grid_sum(c.part, c.nblocks, 1, tot, s_tmp);
+    grid_sum(part0, c.nblocks, 1, tot, s_w);
     double rs = tot[0];
     int it = 0;
     double rms = 0;
     for (; it < c.max_iter; it++) {
         if (!(rs > 0)) break;
-        // z = A v ; vz = v.z
+        // A: z = A v ; v.z
         vals[0] = 0;
         for (int ps = 0; ps < passes; ps++) {
             const int i = gslot + ps * sites_per_pass;
-            V3 Av = i < n ? apply_A(a, i, c.v, t, CG_TPP) : v3(0, 0, 0);
+            V3 Av = i < n ? amul<G4, GR>(c, i, t, g1) : v3(0, 0, 0);
             Av.x = group_sum<CG_TPP>(Av.x); Av.y = group_sum<CG_TPP>(Av.y); Av.z = group_sum<CG_TPP>(Av.z);
             if (i < n && t == 0) {
                 c.z[i] = Av.x; c.z[n + i] = Av.y; c.z[2 * n + i] = Av.z;
-                vals[0] += c.v[i] * Av.x + c.v[n + i] * Av.y + c.v[2 * n + i] * Av.z;
+                vals[0] += __ldcg(&c.v[i]) * Av.x + __ldcg(&c.v[n + i]) * Av.y + __ldcg(&c.v[2 * n + i]) * Av.z;
             }
         }
-        // the previous barrier reused the partials: wait before overwriting
+        block_partials(vals, 1, part1, s_w);
         if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
-        block_partials(vals, 1, c.part, s_w);
-        if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
-        grid_sum(c.part, c.nblocks, 1, tot, s_tmp);
+        grid_sum(part1, c.nblocks, 1, tot, s_w);
         const double alpha_cg = rs / tot[0];
-        // p += alpha v ; r -= alpha z ; s = M^-1 r ; rs' = r.s ; dp2 = |alpha v|^2
+        // B: p += alpha v ; r -= alpha z ; rs' = r.M^-1 r ; dp2 = |alpha v|^2
         vals[0] = 0; vals[1] = 0;
-        for (int i = gslot; i < n; i += sites_per_pass) {
-            if (t == 0) {
-                const double pol = fmax(1e-8, a.polar[(int)a.pos4[i].w]);
-                for (int d = 0; d < 3; d++) {
-                    const int idx = d * n + i;
-                    const double dp = alpha_cg * c.v[idx];
-                    a.p[idx] += dp;
-                    c.r[idx] -= alpha_cg * c.z[idx];
-                    c.s[idx] = pol * c.r[idx];
-                    vals[0] += c.r[idx] * c.s[idx];
-                    vals[1] += dp * dp;
-                }
+        for (int i = gtid; i < n; i += nthreads) {
+            const double al = __ldcg(&c.al[i]);
+            for (int d = 0; d < 3; d++) {
+                const int idx = d * n + i;
+                const double dp = alpha_cg * __ldcg(&c.v[idx]);
+                a.p[idx] = __ldcg(&a.p[idx]) + dp;
+                const double r = __ldcg(&c.r[idx]) - alpha_cg * __ldcg(&c.z[idx]);
+                c.r[idx] = r;
+                vals[0] += r * al * r;
+                vals[1] += dp * dp;
             }
         }
+        block_partials(vals, 2, part0, s_w);
         if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
-        block_partials(vals, 2, c.part, s_w);
-        if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
-        grid_sum(c.part, c.nblocks, 2, tot, s_tmp);
+        grid_sum(part0, c.nblocks, 2, tot, s_w);
         const double rs_new = tot[0];
         rms = sqrt(tot[1] / (3.0 * n));
         if (rms < c.tol) { it++; break; }
         const double beta = rs_new / rs;
         rs = rs_new;
-        for (int i = gslot; i < n; i += sites_per_pass)
-            if (t == 0)
-                for (int d = 0; d < 3; d++) c.v[d * n + i] = c.s[d * n + i] + beta * c.v[d * n + i];
+        // C: v = M^-1 r + beta v
+        for (int i = gtid; i < n; i += nthreads) {
+            const double al = __ldcg(&c.al[i]);
+            double w[3];
+            for (int d = 0; d < 3; d++) {
+                const int idx = d * n + i;
+                w[d] = al * __ldcg(&c.r[idx]) + beta * __ldcg(&c.v[idx]);
+                c.v[idx] = w[d];
+            }
+            g1[i] = G4{(GR)w[0], (GR)w[1], (GR)w[2], (GR)0};
+        }
         if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -341,20 +455,21 @@ __device__ __forceinline__ void ind_pair(double qi, V3 mi, const Q6 &Qi, V3 pi_,
     const double a2 = alpha * alpha, a2pi = 2.0 * alpha / SQRT_PI_I, ex = exp(-a2 * r2);
     double B[6];
     B[0] = erfc(alpha * rr) / rr;
-    B[1] = (-B[0] - a2pi * ex) / r2;
-    B[2] = (-3 * B[1] + 2 * a2pi * a2 * ex) / r2;
-    B[3] = (-5 * B[2] - 4 * a2pi * a2 * a2 * ex) / r2;
-    B[4] = (-7 * B[3] + 8 * a2pi * a2 * a2 * a2 * ex) / r2;
+    const double ir2 = 1.0 / r2;
+    B[1] = (-B[0] - a2pi * ex) * ir2;
+    B[2] = (-3 * B[1] + 2 * a2pi * a2 * ex) * ir2;
+    B[3] = (-5 * B[2] - 4 * a2pi * a2 * a2 * ex) * ir2;
+    B[4] = (-7 * B[3] + 8 * a2pi * a2 * a2 * a2 * ex) * ir2;
     const double e = exp(-a * u3), au3 = a * u3, a2u6 = au3 * au3, a3u9 = a2u6 * au3;
     const double l3 = 1.0 - e;
-    const double gl3 = 3.0 * au3 * e / r2;
-    const double gl5 = 3.0 * a2u6 * e / r2;
-    const double gl7 = (-3.0 * a2u6 + 9.0 * a3u9) * e / (5.0 * r2);
+    const double gl3 = 3.0 * au3 * e * ir2;
+    const double gl5 = 3.0 * a2u6 * e * ir2;
+    const double gl7 = (-3.0 * a2u6 + 9.0 * a3u9) * e * (0.2 * ir2);
     const double B1d = B[1] * l3;
     const double B2d = B[2] * l3 + B[1] * gl3;
-    const double B3d = B[3] * l3 + B[2] * 2.0 * gl3 + B[1] * (gl3 - 3.0 * gl5) / r2;
-    const double B4d = B[4] * l3 + B[3] * 3.0 * gl3 + B[2] * (3.0 * gl3 - 9.0 * gl5) / r2 +
-                       B[1] * (-gl3 - 6.0 * gl5 + 15.0 * gl7) / (r2 * r2);
+    const double B3d = B[3] * l3 + B[2] * 2.0 * gl3 + B[1] * (gl3 - 3.0 * gl5) * ir2;
+    const double B4d = B[4] * l3 + B[3] * 3.0 * gl3 + B[2] * (3.0 * gl3 - 9.0 * gl5) * ir2 +
+                       B[1] * (-gl3 - 6.0 * gl5 + 15.0 * gl7) * (ir2 * ir2);
     o.e = 0.5 * ((G1i + G1j) * B1d + (G2i + G2j) * B2d + (G3i + G3j) * B3d) * scale;
     const double G1ip = -dot(pi_, pj_), G2ip = -dot(pi_, r) * pjr;
     const V3 gG2ip = (-pjr) * pi_, gG2jp = (-pirji) * pj_;
@@ -375,7 +490,7 @@ struct IndRealArgs {
     long long *frc, *trq, *acc;
 };
 
-__global__ void __launch_bounds__(256) k_ind_real(IndRealArgs A) {
+__global__ void __launch_bounds__(64) k_ind_real(IndRealArgs A) {
     const IndArgs &a = A.ia;
     constexpr int TPP = 8;
     const int gt = blockIdx.x * blockDim.x + threadIdx.x;
@@ -500,9 +615,11 @@ static IndArgs ind_args(Ctx &c) {
 }
 
 int setup_cg(Ctx &c) {
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ind_cg, CG_THREADS, 0) != cudaSuccess)
+    int per_sm = 0, per_sm32 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ind_cg<false>, CG_THREADS, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, k_ind_cg<true>, CG_THREADS, 0) != cudaSuccess)
         return SMD_ERR_CUDA;
+    per_sm = per_sm < per_sm32 ? per_sm : per_sm32;
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, c.device) != cudaSuccess) return SMD_ERR_CUDA;
     int want = (c.n * CG_TPP + CG_THREADS - 1) / CG_THREADS;
@@ -512,15 +629,45 @@ int setup_cg(Ctx &c) {
     return 0;
 }
 
+// tensor rows: one slot per Verlet-list entry plus the molecule's sites
+int ensure_ind_rows(Ctx &c) {
+    if (!c.mp_on || !c.ind_on || c.n == 0) return 0;
+    int maxmol = 1;
+    for (size_t m = 0; m + 1 < c.h_mol_off.size(); m++)
+        maxmol = std::max(maxmol, c.h_mol_off[m + 1] - c.h_mol_off[m]);
+    const int cap = ((c.pl.max_nbr + maxmol + 3) / 4) * 4;
+    if (cap == c.ind_cap && c.ind_rj) return 0;
+    cudaFree(c.ind_rj); cudaFree(c.ind_rc); cudaFree(c.ind_cnt);
+    c.ind_rj = nullptr; c.ind_rc = nullptr; c.ind_cnt = nullptr;
+    c.ind_cap = 0;
+    const size_t slots = (size_t)c.n * cap;
+    if (cudaMalloc(&c.ind_rj, slots * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&c.ind_rc, slots * sizeof(double4)) != cudaSuccess ||
+        cudaMalloc(&c.ind_cnt, (size_t)c.n * sizeof(int)) != cudaSuccess)
+        return SMD_ERR_CUDA;
+    c.ind_cap = cap;
+    c.graph_dirty = 1;
+    return 0;
+}
+
 void launch_ind_solve(Ctx &c) {
     IndArgs a = ind_args(c);
+    const bool f32 = c.precision == SMD_PREC_MIXED;
+    TRows R;
+    R.j = c.ind_rj; R.c = c.ind_rc; R.cnt = c.ind_cnt; R.cap = c.ind_cap;
     const int nb = (int)(((long long)c.n * 8 + 255) / 256);
-    k_ind_field<<<nb, 256, 0, c.stream>>>(a);
+    if (f32)
+        k_ind_field<float><<<nb, 256, 0, c.stream>>>(a, R, c.status);
+    else
+        k_ind_field<double><<<nb, 256, 0, c.stream>>>(a, R, c.status);
     const bool learned = c.cg_guess == SMD_GUESS_LEARNED && c.mlp_ready;
     if (learned) launch_mlp_guess(c);  // writes the start dipoles into p
     CGArgs g;
     g.ia = a;
-    g.r = c.cgw; g.z = c.cgw + 3 * (size_t)c.n; g.v = c.cgw + 6 * (size_t)c.n; g.s = c.cgw + 9 * (size_t)c.n;
+    g.rows = R;
+    const size_t n = c.n;
+    g.r = c.cgw; g.z = c.cgw + 3 * n; g.v = c.cgw + 6 * n; g.al = c.cgw + 9 * n;
+    g.g0 = c.cgw + 12 * n; g.g1 = c.cgw + 16 * n;
     g.part = c.cgs + 8; g.scal = c.cgs; g.bar = c.cg_bar; g.status = c.status;
     g.nblocks = c.cg_blocks; g.max_iter = c.cg_max_iter; g.tol = c.cg_tol;
     // 0: start from alpha E0; 1: start from the dipoles in p (previous solve or network)
@@ -537,15 +684,20 @@ void launch_ind_solve(Ctx &c) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_ind_cg, g);
+    if (f32)
+        cudaLaunchKernelEx(&cfg, k_ind_cg<true>, g);
+    else
+        cudaLaunchKernelEx(&cfg, k_ind_cg<false>, g);
 }
 
 void launch_ind_short(Ctx &c) {
     IndRealArgs A;
     A.ia = ind_args(c);
     A.frc = c.frc; A.trq = c.trq; A.acc = c.acc;
-    const int nb = (int)(((long long)c.n * 8 + 255) / 256);
-    k_ind_real<<<nb, 256, 0, c.stream>>>(A);
+    // 64-thread blocks: at this kernel's register count the SM holds more
+    // warps in small blocks than in one 256-thread block
+    const int nb = (int)(((long long)c.n * 8 + 63) / 64);
+    k_ind_real<<<nb, 64, 0, c.stream>>>(A);
     k_ind_mol<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(A.ia, c.trq, c.acc);
 }
 

@@ -43,11 +43,37 @@ __device__ __forceinline__ V3 in_axes(const double *frame, int n, int i, V3 e) {
     return v3(dot(axis(frame, n, i, 0), e), dot(axis(frame, n, i, 1), e), dot(axis(frame, n, i, 2), e));
 }
 
+// MLP_FTPP lanes per site split the neighbour row; the radial densities are
+// combined by shuffles in a fixed order
+constexpr int MLP_FTPP = 8;
 __global__ void k_mlp_features(int n, const int *nbr, const int *nnbr, const int *mol, const int *mol_off,
                                const int *mol_atoms, const double4 *pos4, Box box, double rc,
                                const double *frame, const double *e0, float *x) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gt / MLP_FTPP, t = gt % MLP_FTPP;
+    float g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double4 pi = make_double4(0, 0, 0, 0);
+    if (i < n) {
+        pi = pos4[i];
+        const int cnt = nnbr[i];
+        const float rcf = (float)rc, irc = 1.f / (float)rc;
+        for (int k = t; k < cnt; k += MLP_FTPP) {
+            const int j = nbr[(size_t)k * n + i] & 0x7fffffff;
+            const double4 pj = pos4[j];
+            const double dx = pbc1(pj.x - pi.x, box.L[0], box.half[0]);
+            const double dy = pbc1(pj.y - pi.y, box.L[1], box.half[1]);
+            const double dz = pbc1(pj.z - pi.z, box.L[2], box.half[2]);
+            const float r = sqrtf((float)(dx * dx + dy * dy + dz * dz));
+            if (r >= rcf) continue;
+            const float fc = 0.5f * (cospif(r * irc) + 1.f);
+            for (int b = 0; b < 8; b++) {
+                const float d = r - (0.22f + 0.09f * b);
+                g[b] += expf(-d * d * 200.f) * fc;   // 1 / (2 * 0.05^2)
+            }
+        }
+    }
+    for (int b = 0; b < 8; b++) g[b] = group_sum<MLP_FTPP>(g[b]);
+    if (i >= n || t != 0) return;
     float f[MF];
     const V3 E = v3(e0[i], e0[n + i], e0[2 * n + i]);
     const V3 El = in_axes(frame, n, i, E);
@@ -62,27 +88,10 @@ __global__ void k_mlp_features(int n, const int *nbr, const int *nnbr, const int
         f[q++] = (float)Ej.x; f[q++] = (float)Ej.y; f[q++] = (float)Ej.z;
     }
     for (; q < 10; q++) f[q] = 0.f;
-    float g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    const double4 pi = pos4[i];
-    const int cnt = nnbr[i];
-    for (int k = 0; k < cnt; k++) {
-        const int j = nbr[(size_t)k * n + i] & 0x7fffffff;
-        const double4 pj = pos4[j];
-        const double dx = pbc1(pj.x - pi.x, box.L[0], box.half[0]);
-        const double dy = pbc1(pj.y - pi.y, box.L[1], box.half[1]);
-        const double dz = pbc1(pj.z - pi.z, box.L[2], box.half[2]);
-        const float r = (float)sqrt(dx * dx + dy * dy + dz * dz);
-        if (r >= (float)rc) continue;
-        const float fc = 0.5f * (cospif(r / (float)rc) + 1.f);
-        for (int b = 0; b < 8; b++) {
-            const float d = r - (0.22f + 0.09f * b);
-            g[b] += expf(-d * d * 200.f) * fc;   // 1 / (2 * 0.05^2)
-        }
-    }
     for (int b = 0; b < 8; b++) f[10 + b] = g[b];
-    const int t = (int)pi.w;
-    f[18] = t == 0 ? 1.f : 0.f;
-    f[19] = t == 0 ? 0.f : 1.f;
+    const int ty = (int)pi.w;
+    f[18] = ty == 0 ? 1.f : 0.f;
+    f[19] = ty == 0 ? 0.f : 1.f;
     for (int k = 0; k < MF; k++) x[(size_t)i * MF + k] = f[k];
 }
 
@@ -243,7 +252,7 @@ __global__ void k_mlp_adam(int nblocks, const float *part, float *W, float *m, f
 // host side
 // ---------------------------------------------------------------------------
 void launch_mlp_features(Ctx &c) {
-    k_mlp_features<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.pl.nbr, c.pl.nnbr, c.mol, c.mol_off,
+    k_mlp_features<<<(int)(((long long)c.n * MLP_FTPP + 127) / 128), 128, 0, c.stream>>>(c.n, c.pl.nbr, c.pl.nnbr, c.mol, c.mol_off,
                                                             c.mol_atoms, c.pos4, c.box, c.cutoff, c.frame,
                                                             c.e0, c.mlp_x);
 }

@@ -41,6 +41,14 @@ constexpr int MK_CHUNKS = 16;
 constexpr int FK_TILE = 256;
 constexpr int F_TPS = 4;
 
+// several blocks (k ranges) add into one site: integer atomics keep the sum
+// independent of their order
+__device__ __forceinline__ void add_fix3_atomic(long long *arr, int n, int i, V3 v, double s) {
+    atomicAdd((unsigned long long *)&arr[i], (unsigned long long)to_fix(s * v.x, FRC_SCALE));
+    atomicAdd((unsigned long long *)&arr[n + i], (unsigned long long)to_fix(s * v.y, FRC_SCALE));
+    atomicAdd((unsigned long long *)&arr[2 * n + i], (unsigned long long)to_fix(s * v.z, FRC_SCALE));
+}
+
 // sin and cos of 2 pi ph / 2^32: the top 24 bits go through sincospif
 // exactly, the low 8 bits as a first-order rotation
 __device__ __forceinline__ void sincos_phase32(int ph, float &s, float &c) {
@@ -72,7 +80,7 @@ __global__ void __launch_bounds__(MK_THREADS) k_rsk_partial(int n, int nk, const
     __shared__ SiteTile T;
     const int k = blockIdx.x * MK_THREADS + threadIdx.x;
     const int ch = blockIdx.y;
-    const int per = (n + MK_CHUNKS - 1) / MK_CHUNKS;
+    const int per = (n + gridDim.y - 1) / gridDim.y;
     const int s0 = ch * per, s1 = min(n, s0 + per);
     double kx = 0, ky = 0, kz = 0;
     int nx = 0, ny = 0, nz = 0;
@@ -157,7 +165,7 @@ __global__ void __launch_bounds__(MK_THREADS) k_rsk_partial_f(int n, int nk, con
     __shared__ float s_v[NV][MK_THREADS];
     const int k = blockIdx.x * MK_THREADS + threadIdx.x;
     const int ch = blockIdx.y;
-    const int per = (n + MK_CHUNKS - 1) / MK_CHUNKS;
+    const int per = (n + gridDim.y - 1) / gridDim.y;
     const int s0 = ch * per, s1 = min(n, s0 + per);
     float kx = 0.f, ky = 0.f, kz = 0.f;
     unsigned nx = 0, ny = 0, nz = 0;
@@ -225,7 +233,7 @@ __global__ void __launch_bounds__(MK_THREADS) k_rsk_partial_f(int n, int nk, con
 // MODE 0 permanent, 1 induced, 2 both (permanent energy to slot_e, induced
 // to slot_e2); slot_e < 0: sums only
 template <int MODE>
-__global__ void k_rsk_reduce(int nk, const double *partial, const double *kcoef, const double *kvec,
+__global__ void k_rsk_reduce(int nk, int nch, const double *partial, const double *kcoef, const double *kvec,
                              double alphaR4, double *sk, long long *acc, int slot_e, int slot_e2) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     double ep = 0, ei = 0, vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
@@ -233,7 +241,7 @@ __global__ void k_rsk_reduce(int nk, const double *partial, const double *kcoef,
         const int q0 = MODE == 1 ? 4 : 0, q1 = MODE == 0 ? 4 : 6;
         for (int q = q0; q < q1; q++) {
             double t = 0;
-            for (int ch = 0; ch < MK_CHUNKS; ch++) t += partial[((size_t)ch * 6 + q) * nk + k];
+            for (int ch = 0; ch < nch; ch++) t += partial[((size_t)ch * 6 + q) * nk + k];
             sk[(size_t)q * nk + k] = t;
         }
         const double CqQ = sk[k], SqQ = sk[nk + k], Cm = sk[2 * (size_t)nk + k], Sm = sk[3 * (size_t)nk + k];
@@ -302,10 +310,12 @@ __global__ void __launch_bounds__(256) k_rforce(int n, int nk, const double4 *po
         Qi = {qd[i], qd[n + i], qd[2 * n + i], qd[3 * n + i], qd[4 * n + i], qd[5 * n + i]};
         if (IND) pi_ = v3(pind[i], pind[n + i], pind[2 * n + i]);
     }
-    for (int base = 0; base < nk; base += FK_TILE) {
+    const int kper = (((nk + gridDim.y - 1) / gridDim.y + FK_TILE - 1) / FK_TILE) * FK_TILE;
+    const int kb0 = blockIdx.y * kper, kb1 = min(nk, kb0 + kper);
+    for (int base = kb0; base < kb1; base += FK_TILE) {
         __syncthreads();
         const int kk = base + threadIdx.x;
-        if (kk < nk) {
+        if (kk < kb1) {
             for (int d = 0; d < 3; d++) {
                 s_k[d][threadIdx.x] = kvec[(size_t)d * nk + kk];
                 s_n[d][threadIdx.x] = kn[(size_t)d * nk + kk];
@@ -315,7 +325,7 @@ __global__ void __launch_bounds__(256) k_rforce(int n, int nk, const double4 *po
                 s_S[d][threadIdx.x] = (d < 4 || IND) ? sk[(size_t)d * nk + kk] : 0.0;
         }
         __syncthreads();
-        const int cnt = min(FK_TILE, nk - base);
+        const int cnt = min(FK_TILE, kb1 - base);
         if (i < n) {
             for (int q = t; q < cnt; q += F_TPS) {
                 const V3 k = v3(s_k[0][q], s_k[1][q], s_k[2][q]);
@@ -358,8 +368,8 @@ __global__ void __launch_bounds__(256) k_rforce(int n, int nk, const double4 *po
     f.x = group_sum<F_TPS>(f.x); f.y = group_sum<F_TPS>(f.y); f.z = group_sum<F_TPS>(f.z);
     tau.x = group_sum<F_TPS>(tau.x); tau.y = group_sum<F_TPS>(tau.y); tau.z = group_sum<F_TPS>(tau.z);
     if (i < n && t == 0) {
-        add_fix3(frc, n, i, f, KE);
-        add_fix3(trq, n, i, tau, KE);
+        add_fix3_atomic(frc, n, i, f, KE);
+        add_fix3_atomic(trq, n, i, tau, KE);
     }
 }
 
@@ -392,10 +402,12 @@ __global__ void __launch_bounds__(256) k_rforce_f(int n, int nk, const double4 *
         Qyy = (float)qd[3 * n + i]; Qyz = (float)qd[4 * n + i]; Qzz = (float)qd[5 * n + i];
     }
     double F[3] = {0, 0, 0}, EA[3] = {0, 0, 0}, GX[3] = {0, 0, 0};
-    for (int base = 0; base < nk; base += FK_TILE) {
+    const int kper = (((nk + gridDim.y - 1) / gridDim.y + FK_TILE - 1) / FK_TILE) * FK_TILE;
+    const int kb0 = blockIdx.y * kper, kb1 = min(nk, kb0 + kper);
+    for (int base = kb0; base < kb1; base += FK_TILE) {
         __syncthreads();
         const int kk = base + threadIdx.x;
-        if (kk < nk) {
+        if (kk < kb1) {
             const double CqQ = sk[kk], SqQ = sk[nk + kk], Cm = sk[2 * (size_t)nk + kk], Sm = sk[3 * (size_t)nk + kk];
             double U = CqQ - Sm, W = SqQ + Cm;
             if (IND) {
@@ -408,7 +420,7 @@ __global__ void __launch_bounds__(256) k_rforce_f(int n, int nk, const double4 *
             s_n[threadIdx.x] = make_int4(kn[kk], kn[nk + kk], kn[2 * (size_t)nk + kk], 0);
         }
         __syncthreads();
-        const int cnt = min(FK_TILE, nk - base);
+        const int cnt = min(FK_TILE, kb1 - base);
         if (i < n) {
             float f0 = 0.f, f1 = 0.f, f2 = 0.f, e0 = 0.f, e1 = 0.f, e2 = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
 #pragma unroll 2
@@ -451,8 +463,8 @@ __global__ void __launch_bounds__(256) k_rforce_f(int n, int nk, const double4 *
         const V3 m = v3(mu[i], mu[n + i], mu[2 * n + i]);
         const V3 ea = v3(EA[0], EA[1], EA[2]);
         const V3 tau = crs(m, ea) - 2.0 * v3(GX[0], GX[1], GX[2]);
-        add_fix3(frc, n, i, v3(F[0], F[1], F[2]), KE);
-        add_fix3(trq, n, i, tau, KE);
+        add_fix3_atomic(frc, n, i, v3(F[0], F[1], F[2]), KE);
+        add_fix3_atomic(trq, n, i, tau, KE);
     }
 }
 
@@ -465,20 +477,65 @@ RecipBufs bufs(Ctx &c) {
     return {partial, partial + (size_t)6 * c.rc.nk * MK_CHUNKS};
 }
 
+// resident blocks per SM of each kernel, looked up once per kernel
+int blocks_per_sm(const void *kernel, int threads) {
+    static const void *keys[32];
+    static int vals[32], count = 0;
+    for (int q = 0; q < count; q++)
+        if (keys[q] == kernel) return vals[q];
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    if (count < 32) {
+        keys[count] = kernel;
+        vals[count++] = per_sm;
+    }
+    return per_sm;
+}
+int sm_count() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 1;
+    }
+    return sms;
+}
+
+// site chunks of the partial sums: enough blocks for one full wave of the
+// device (at most MK_CHUNKS, the partial buffer's size)
+int chunks_for(const void *kernel, int kblocks) {
+    const int ch = sm_count() * blocks_per_sm(kernel, MK_THREADS) / (kblocks > 0 ? kblocks : 1);
+    return ch < 1 ? 1 : (ch > MK_CHUNKS ? MK_CHUNKS : ch);
+}
+
 template <int MODE>
 void sums(Ctx &c, int slot_e, int slot_e2 = -1) {
     const int nk = c.rc.nk;
     RecipBufs B = bufs(c);
-    dim3 g1((nk + MK_THREADS - 1) / MK_THREADS, MK_CHUNKS);
-    if (c.precision == SMD_PREC_MIXED)
-        k_rsk_partial_f<MODE><<<g1, MK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,
-                                                               c.type_q, c.mu, c.qd, c.pind, B.partial);
-    else
-        k_rsk_partial<double, MODE><<<g1, MK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,
-                                                                    c.type_q, c.mu, c.qd, c.pind, B.partial);
-    k_rsk_reduce<MODE><<<(nk + 255) / 256, 256, 0, c.stream>>>(nk, B.partial, c.rc.kcoef, c.rc.kvec,
+    const int kb = (nk + MK_THREADS - 1) / MK_THREADS;
+    int nch;
+    if (c.precision == SMD_PREC_MIXED) {
+        nch = chunks_for((const void *)k_rsk_partial_f<MODE>, kb);
+        k_rsk_partial_f<MODE><<<dim3(kb, nch), MK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn,
+                                                                          c.rc.kvec, c.type_q, c.mu, c.qd, c.pind,
+                                                                          B.partial);
+    } else {
+        nch = chunks_for((const void *)k_rsk_partial<double, MODE>, kb);
+        k_rsk_partial<double, MODE><<<dim3(kb, nch), MK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn,
+                                                                               c.rc.kvec, c.type_q, c.mu, c.qd,
+                                                                               c.pind, B.partial);
+    }
+    k_rsk_reduce<MODE><<<(nk + 255) / 256, 256, 0, c.stream>>>(nk, nch, B.partial, c.rc.kcoef, c.rc.kvec,
                                                               1.0 / (4.0 * c.ew_alpha * c.ew_alpha), B.sk,
                                                               c.acc, slot_e, slot_e2);
+}
+
+// k ranges of the force pass: site blocks x k ranges fill about one wave
+int ksplit_for(const void *kernel, int sblocks, int nk) {
+    const int ks = sm_count() * blocks_per_sm(kernel, 256) / (sblocks > 0 ? sblocks : 1);
+    const int tiles = (nk + FK_TILE - 1) / FK_TILE;
+    return ks < 1 ? 1 : (ks > tiles ? tiles : ks);
 }
 
 template <bool PERM, bool IND>
@@ -487,16 +544,22 @@ void forces(Ctx &c) {
     RecipBufs B = bufs(c);
     const int nb = (int)(((long long)c.n * F_TPS + 255) / 256);
     if (c.precision == SMD_PREC_MIXED) {
-        if (PERM)
-            k_rforce_f<IND><<<nb, 256, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec, c.rc.kcoef,
-                                                      B.sk, c.type_q, c.mu, c.qd, c.pind, c.frc, c.trq);
-        else
-            k_rforce<float, PERM, IND><<<nb, 256, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,
+        if (PERM) {
+            const int ks = ksplit_for((const void *)k_rforce_f<IND>, nb, nk);
+            k_rforce_f<IND><<<dim3(nb, ks), 256, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,
                                                                 c.rc.kcoef, B.sk, c.type_q, c.mu, c.qd, c.pind,
                                                                 c.frc, c.trq);
+        } else {
+            const int ks = ksplit_for((const void *)k_rforce<float, PERM, IND>, nb, nk);
+            k_rforce<float, PERM, IND><<<dim3(nb, ks), 256, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn,
+                                                                          c.rc.kvec, c.rc.kcoef, B.sk, c.type_q,
+                                                                          c.mu, c.qd, c.pind, c.frc, c.trq);
+        }
     } else {
-        k_rforce<double, PERM, IND><<<nb, 256, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec, c.rc.kcoef,
-                                                             B.sk, c.type_q, c.mu, c.qd, c.pind, c.frc, c.trq);
+        const int ks = ksplit_for((const void *)k_rforce<double, PERM, IND>, nb, nk);
+        k_rforce<double, PERM, IND><<<dim3(nb, ks), 256, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn,
+                                                                       c.rc.kvec, c.rc.kcoef, B.sk, c.type_q, c.mu,
+                                                                       c.qd, c.pind, c.frc, c.trq);
     }
 }
 }  // namespace

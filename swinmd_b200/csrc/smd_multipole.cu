@@ -149,13 +149,13 @@ __device__ __forceinline__ void mp_torque_i(double qj, V3 mi, const Q6 &Qi, V3 m
 // B_n of erfc(a r)/r (Multipole.cpp:632-637); D_n of erf(a r)/r (:1495-1500)
 __device__ __forceinline__ void bn_erfc(double r2, double alpha, double B[6]) {
     const double a2 = alpha * alpha, a2pi = 2.0 * alpha / SQRT_PI_D;
-    const double r = sqrt(r2), ex = exp(-a2 * r2);
+    const double r = sqrt(r2), ex = exp(-a2 * r2), ir2 = 1.0 / r2;
     B[0] = erfc(alpha * r) / r;
-    B[1] = (-B[0] - a2pi * ex) / r2;
-    B[2] = (-3 * B[1] + 2 * a2pi * a2 * ex) / r2;
-    B[3] = (-5 * B[2] - 4 * a2pi * a2 * a2 * ex) / r2;
-    B[4] = (-7 * B[3] + 8 * a2pi * a2 * a2 * a2 * ex) / r2;
-    B[5] = (-9 * B[4] - 16 * a2pi * a2 * a2 * a2 * a2 * ex) / r2;
+    B[1] = (-B[0] - a2pi * ex) * ir2;
+    B[2] = (-3 * B[1] + 2 * a2pi * a2 * ex) * ir2;
+    B[3] = (-5 * B[2] - 4 * a2pi * a2 * a2 * ex) * ir2;
+    B[4] = (-7 * B[3] + 8 * a2pi * a2 * a2 * a2 * ex) * ir2;
+    B[5] = (-9 * B[4] - 16 * a2pi * a2 * a2 * a2 * a2 * ex) * ir2;
 }
 __device__ __forceinline__ void dn_erf(double r2, double alpha, double D[6]) {
     const double a2 = alpha * alpha, a2pi = 2.0 * alpha / SQRT_PI_D;
@@ -182,7 +182,7 @@ struct MPArgs {
 };
 
 template <int TPP>
-__global__ void __launch_bounds__(256) k_mp_real(MPArgs a) {
+__global__ void __launch_bounds__(128, 3) k_mp_real(MPArgs a) {
     const int gt = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = gt / TPP, t = gt % TPP;
     V3 f = v3(0, 0, 0), tau = v3(0, 0, 0);
@@ -364,8 +364,10 @@ void launch_mp_short(Ctx &c) {
     a.tq = c.type_q; a.box = c.box; a.alpha = c.ew_alpha; a.rc2 = c.mp_rc2;
     a.frc = c.frc; a.trq = c.trq; a.acc = c.acc;
     const int tpp = 8;
-    const int nb = (int)(((long long)c.n * tpp + 255) / 256);
-    k_mp_real<tpp><<<nb, 256, 0, c.stream>>>(a);
+    // 128-thread blocks: at this kernel's register count the SM holds more
+    // warps in small blocks than in one 256-thread block
+    const int nb = (int)(((long long)c.n * tpp + 127) / 128);
+    k_mp_real<tpp><<<nb, 128, 0, c.stream>>>(a);
     k_mp_mol<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.n, c.mol_off, c.mol_atoms, c.excl_off,
                                                          c.excl, c.pos4, c.type_q, c.mu, c.qd, c.box,
                                                          c.ew_alpha, c.acc);
