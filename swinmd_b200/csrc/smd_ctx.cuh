@@ -40,6 +40,7 @@ struct Recip {               // Ewald reciprocal space (k half-space, k^2 < kcut
     double *kcoef = nullptr; // [nk] 4 pi/V * exp(-k^2/4a^2)/k^2
     long long *sk = nullptr; // [2][nk] structure factor, fixed point (SK_SCALE)
     double *kvec = nullptr;  // [3][nk] k in 1/nm
+    int nmax = 0;            // largest |n| of any component
 };
 
 struct Ctx {
@@ -179,5 +180,6 @@ int mlp_nparam();
 int mlp_nfeat();
 int mlp_max_batch();
 int setup_recip(Ctx &c);
+int mp_recip_prepare(Ctx &c);
 
 }  // namespace smd

@@ -468,6 +468,229 @@ __global__ void __launch_bounds__(256) k_rforce_f(int n, int nk, const double4 *
     }
 }
 
+// ---------------------------------------------------------------------------
+// FP32 passes with per-site phase tables (mixed path, |n| < TAB_MAX)
+// ---------------------------------------------------------------------------
+// For a site with box fractions (fx, fy, fz) the table holds
+// e^{2 pi i m f / 2^32} for m = 0 .. nt-1 on each axis, every entry from the
+// exact integer phase m f mod 2^32 through sincos_phase32; the phase factor
+// of k = (nx, ny, nz) is X[nx] Y[|ny|] Z[|nz|] with the conjugate taken for
+// negative components (nx >= 0 in the half space).  Per (site, k) this is two
+// complex products instead of one sine/cosine evaluation.
+constexpr int TAB_MAX = 32;
+constexpr int TF_SITES = 64;    // sites per block of the force pass (F_TPS lanes each)
+constexpr int TS_THREADS = 256; // k per block of the sums pass
+constexpr int TS_SITES = 128;   // sites per tile of the sums pass
+
+__device__ __forceinline__ void table_entry(int m, unsigned f, float2 &out) {
+    float sn, cs;
+    sincos_phase32((int)((unsigned)m * f), sn, cs);
+    out = make_float2(cs, sn);
+}
+
+// offsets of k's three entries in a site table, sign bits of ny and nz
+__device__ __forceinline__ int4 table_offsets(int nx, int ny, int nz, int nt) {
+    return make_int4(nx, nt + (ny < 0 ? -ny : ny), 2 * nt + (nz < 0 ? -nz : nz), (ny < 0 ? 1 : 0) | (nz < 0 ? 2 : 0));
+}
+
+__device__ __forceinline__ void table_phase(const float2 *tab, int4 o, float &sn, float &cs) {
+    const float2 X = tab[o.x], Y = tab[o.y], Z = tab[o.z];
+    const float yi = (o.w & 1) ? -Y.y : Y.y, zi = (o.w & 2) ? -Z.y : Z.y;
+    const float xr = fmaf(X.x, Y.x, -X.y * yi), xi = fmaf(X.x, yi, X.y * Y.x);
+    cs = fmaf(xr, Z.x, -xi * zi);
+    sn = fmaf(xr, zi, xi * Z.x);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(TS_THREADS) k_rsk_partial_t(int n, int nk, int nt, const double4 *pos4,
+                                                              const int4 *fixq, const int *kn, const double *kvec,
+                                                              const double *tq, const double *mu, const double *qd,
+                                                              const double *pind, double *partial) {
+    constexpr bool PERM = MODE != 1, IND = MODE != 0;
+    constexpr int PV = MODE == 1 ? 0 : 10;
+    constexpr int NV = MODE == 0 ? 10 : (MODE == 1 ? 3 : 13);
+    extern __shared__ float4 s_dyn4[];
+    float2 *s_tab = (float2 *)s_dyn4;                          // [TS_SITES][3 nt]
+    float *s_v = (float *)(s_tab + (size_t)TS_SITES * 3 * nt); // [NV][TS_SITES]
+    const int k = blockIdx.x * TS_THREADS + threadIdx.x;
+    const int ch = blockIdx.y;
+    const int per = (n + gridDim.y - 1) / gridDim.y;
+    const int s0 = ch * per, s1 = min(n, s0 + per);
+    float kx = 0.f, ky = 0.f, kz = 0.f;
+    int4 o = make_int4(0, 0, 0, 0);
+    if (k < nk) {
+        kx = (float)kvec[k]; ky = (float)kvec[nk + k]; kz = (float)kvec[2 * nk + k];
+        o = table_offsets(kn[k], kn[nk + k], kn[2 * nk + k], nt);
+    }
+    const float kk[6] = {kx * kx, 2.f * kx * ky, 2.f * kx * kz, ky * ky, 2.f * ky * kz, kz * kz};
+    const int row = 3 * nt;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int base = s0; base < s1; base += TS_SITES) {
+        const int cnt = min(TS_SITES, s1 - base);
+        __syncthreads();
+        for (int e = threadIdx.x; e < cnt * row; e += TS_THREADS) {
+            const int sl = e / row, r = e - sl * row, ax = r / nt, m = r - ax * nt;
+            const int4 f = fixq[base + sl];
+            table_entry(m, (unsigned)(ax == 0 ? f.x : (ax == 1 ? f.y : f.z)), s_tab[e]);
+        }
+        if (threadIdx.x < cnt) {
+            const int i = base + threadIdx.x;
+            if (PERM) {
+                s_v[threadIdx.x] = (float)(tq[(int)pos4[i].w] / SQC_R);
+                for (int d = 0; d < 3; d++) s_v[(1 + d) * TS_SITES + threadIdx.x] = (float)mu[(size_t)d * n + i];
+                for (int d = 0; d < 6; d++) s_v[(4 + d) * TS_SITES + threadIdx.x] = (float)qd[(size_t)d * n + i];
+            }
+            if (IND)
+                for (int d = 0; d < 3; d++) s_v[(PV + d) * TS_SITES + threadIdx.x] = (float)pind[(size_t)d * n + i];
+        }
+        __syncthreads();
+        if (k < nk) {
+            float t0 = 0.f, t1 = 0.f, t2 = 0.f, t3 = 0.f, t4 = 0.f, t5 = 0.f;
+#pragma unroll 4
+            for (int q = 0; q < cnt; q++) {
+                float sn, cs;
+                table_phase(s_tab + q * row, o, sn, cs);
+                if (PERM) {
+                    const float *v = s_v + q;
+                    float kqk = v[4 * TS_SITES] * kk[0];
+                    kqk = fmaf(v[5 * TS_SITES], kk[1], kqk);
+                    kqk = fmaf(v[6 * TS_SITES], kk[2], kqk);
+                    kqk = fmaf(v[7 * TS_SITES], kk[3], kqk);
+                    kqk = fmaf(v[8 * TS_SITES], kk[4], kqk);
+                    kqk = fmaf(v[9 * TS_SITES], kk[5], kqk);
+                    const float qk = v[0] - kqk;
+                    const float mk = fmaf(v[TS_SITES], kx, fmaf(v[2 * TS_SITES], ky, v[3 * TS_SITES] * kz));
+                    t0 = fmaf(qk, cs, t0); t1 = fmaf(qk, sn, t1);
+                    t2 = fmaf(mk, cs, t2); t3 = fmaf(mk, sn, t3);
+                }
+                if (IND) {
+                    const float *v = s_v + PV * TS_SITES + q;
+                    const float pk = fmaf(v[0], kx, fmaf(v[TS_SITES], ky, v[2 * TS_SITES] * kz));
+                    t4 = fmaf(pk, cs, t4); t5 = fmaf(pk, sn, t5);
+                }
+            }
+            acc[0] += t0; acc[1] += t1; acc[2] += t2; acc[3] += t3; acc[4] += t4; acc[5] += t5;
+        }
+    }
+    if (k < nk) {
+        double *pb = partial + (size_t)ch * 6 * nk;
+        if (PERM)
+            for (int q = 0; q < 4; q++) pb[(size_t)q * nk + k] = acc[q];
+        if (IND)
+            for (int q = 4; q < 6; q++) pb[(size_t)q * nk + k] = acc[q];
+    }
+}
+
+template <bool IND>
+__global__ void __launch_bounds__(256) k_rforce_t(int n, int nk, int nt, const double4 *pos4, const int4 *fixq,
+                                                  const int *kn, const double *kvec, const double *kcoef,
+                                                  const double *sk, const double *tq, const double *mu,
+                                                  const double *qd, const double *pind, long long *frc,
+                                                  long long *trq) {
+    extern __shared__ float4 s_dyn4[];
+    float4 *s_kb = s_dyn4;                          // [FK_TILE] kx, ky, kz, 2c
+    int4 *s_o = (int4 *)(s_kb + FK_TILE);           // [FK_TILE] table offsets
+    float2 *s_uw = (float2 *)(s_o + FK_TILE);       // [FK_TILE] U, W
+    float2 *s_tab = s_uw + FK_TILE;                 // [TF_SITES][3 nt]
+    const int ls = threadIdx.x / F_TPS, t = threadIdx.x % F_TPS;
+    const int i = blockIdx.x * TF_SITES + ls;
+    const int row = 3 * nt;
+    float2 *tab = s_tab + ls * row;
+    float qi = 0.f, dx = 0.f, dy = 0.f, dz = 0.f;
+    float Qxx = 0.f, Qxy = 0.f, Qxz = 0.f, Qyy = 0.f, Qyz = 0.f, Qzz = 0.f;
+    if (i < n) {
+        const int4 pf = fixq[i];
+        for (int e = t; e < row; e += F_TPS) {
+            const int ax = e / nt, m = e - ax * nt;
+            table_entry(m, (unsigned)(ax == 0 ? pf.x : (ax == 1 ? pf.y : pf.z)), tab[e]);
+        }
+        qi = (float)(tq[(int)pos4[i].w] / SQC_R);
+        double d3[3] = {mu[i], mu[n + i], mu[2 * n + i]};
+        if (IND)
+            for (int d = 0; d < 3; d++) d3[d] += pind[(size_t)d * n + i];
+        dx = (float)d3[0]; dy = (float)d3[1]; dz = (float)d3[2];
+        Qxx = (float)qd[i]; Qxy = (float)qd[n + i]; Qxz = (float)qd[2 * n + i];
+        Qyy = (float)qd[3 * n + i]; Qyz = (float)qd[4 * n + i]; Qzz = (float)qd[5 * n + i];
+    }
+    double F[3] = {0, 0, 0}, EA[3] = {0, 0, 0}, GX[3] = {0, 0, 0};
+    const int kper = (((nk + gridDim.y - 1) / gridDim.y + FK_TILE - 1) / FK_TILE) * FK_TILE;
+    const int kb0 = blockIdx.y * kper, kb1 = min(nk, kb0 + kper);
+    for (int base = kb0; base < kb1; base += FK_TILE) {
+        __syncthreads();
+        const int kk = base + threadIdx.x;
+        if (kk < kb1) {
+            const double CqQ = sk[kk], SqQ = sk[nk + kk], Cm = sk[2 * (size_t)nk + kk], Sm = sk[3 * (size_t)nk + kk];
+            double U = CqQ - Sm, W = SqQ + Cm;
+            if (IND) {
+                U -= sk[5 * (size_t)nk + kk];
+                W += sk[4 * (size_t)nk + kk];
+            }
+            s_kb[threadIdx.x] = make_float4((float)kvec[kk], (float)kvec[nk + kk], (float)kvec[2 * (size_t)nk + kk],
+                                            (float)(2.0 * kcoef[kk]));
+            s_uw[threadIdx.x] = make_float2((float)U, (float)W);
+            s_o[threadIdx.x] = table_offsets(kn[kk], kn[nk + kk], kn[2 * (size_t)nk + kk], nt);
+        }
+        __syncthreads();
+        const int cnt = min(FK_TILE, kb1 - base);
+        if (i < n) {
+            float f0 = 0.f, f1 = 0.f, f2 = 0.f, e0 = 0.f, e1 = 0.f, e2 = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
+#pragma unroll 2
+            for (int q = t; q < cnt; q += F_TPS) {
+                const float4 kb = s_kb[q];
+                const float2 uw = s_uw[q];
+                float sn, cs;
+                table_phase(tab, s_o[q], sn, cs);
+                const float A = fmaf(sn, uw.x, -cs * uw.y);
+                const float B = fmaf(cs, uw.x, sn * uw.y);
+                const float qkx = fmaf(Qxx, kb.x, fmaf(Qxy, kb.y, Qxz * kb.z));
+                const float qky = fmaf(Qxy, kb.x, fmaf(Qyy, kb.y, Qyz * kb.z));
+                const float qkz = fmaf(Qxz, kb.x, fmaf(Qyz, kb.y, Qzz * kb.z));
+                const float qk = qi - fmaf(kb.x, qkx, fmaf(kb.y, qky, kb.z * qkz));
+                const float mk = fmaf(dx, kb.x, fmaf(dy, kb.y, dz * kb.z));
+                const float bA = kb.w * A, bB = kb.w * B;
+                const float al = fmaf(qk, bA, mk * bB);
+                f0 = fmaf(al, kb.x, f0); f1 = fmaf(al, kb.y, f1); f2 = fmaf(al, kb.z, f2);
+                e0 = fmaf(bA, kb.x, e0); e1 = fmaf(bA, kb.y, e1); e2 = fmaf(bA, kb.z, e2);
+                g0 = fmaf(bB, fmaf(kb.y, qkz, -kb.z * qky), g0);
+                g1 = fmaf(bB, fmaf(kb.z, qkx, -kb.x * qkz), g1);
+                g2 = fmaf(bB, fmaf(kb.x, qky, -kb.y * qkx), g2);
+            }
+            F[0] += f0; F[1] += f1; F[2] += f2;
+            EA[0] += e0; EA[1] += e1; EA[2] += e2;
+            GX[0] += g0; GX[1] += g1; GX[2] += g2;
+        }
+    }
+    for (int d = 0; d < 3; d++) {
+        F[d] = group_sum<F_TPS>(F[d]);
+        EA[d] = group_sum<F_TPS>(EA[d]);
+        GX[d] = group_sum<F_TPS>(GX[d]);
+    }
+    if (i < n && t == 0) {
+        const V3 m = v3(mu[i], mu[n + i], mu[2 * n + i]);
+        const V3 tau = crs(m, v3(EA[0], EA[1], EA[2])) - 2.0 * v3(GX[0], GX[1], GX[2]);
+        add_fix3_atomic(frc, n, i, v3(F[0], F[1], F[2]), KE);
+        add_fix3_atomic(trq, n, i, tau, KE);
+    }
+}
+
+size_t tsum_smem(int nt, int nv) { return (size_t)TS_SITES * 3 * nt * sizeof(float2) + (size_t)nv * TS_SITES * sizeof(float); }
+size_t tforce_smem(int nt) {
+    return (size_t)FK_TILE * (sizeof(float4) + sizeof(int4) + sizeof(float2)) + (size_t)TF_SITES * 3 * nt * sizeof(float2);
+}
+
+// dynamic shared memory of the table kernels (set once, outside any capture)
+int mp_recip_prepare(Ctx &c) {
+    const int nt = c.rc.nmax + 1;
+    if (nt > TAB_MAX) return 0;
+    cudaError_t e = cudaSuccess;
+    e = e ? e : cudaFuncSetAttribute(k_rsk_partial_t<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(nt, 10));
+    e = e ? e : cudaFuncSetAttribute(k_rsk_partial_t<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(nt, 3));
+    e = e ? e : cudaFuncSetAttribute(k_rsk_partial_t<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(nt, 13));
+    e = e ? e : cudaFuncSetAttribute(k_rforce_t<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tforce_smem(nt));
+    e = e ? e : cudaFuncSetAttribute(k_rforce_t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tforce_smem(nt));
+    return e == cudaSuccess ? 0 : SMD_ERR_CUDA;
+}
+
 namespace {
 struct RecipBufs {
     double *partial, *sk;
@@ -478,16 +701,18 @@ RecipBufs bufs(Ctx &c) {
 }
 
 // resident blocks per SM of each kernel, looked up once per kernel
-int blocks_per_sm(const void *kernel, int threads) {
+int blocks_per_sm(const void *kernel, int threads, size_t smem = 0) {
     static const void *keys[32];
+    static size_t smems[32];
     static int vals[32], count = 0;
     for (int q = 0; q < count; q++)
-        if (keys[q] == kernel) return vals[q];
+        if (keys[q] == kernel && smems[q] == smem) return vals[q];
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     if (count < 32) {
         keys[count] = kernel;
+        smems[count] = smem;
         vals[count++] = per_sm;
     }
     return per_sm;
@@ -515,7 +740,16 @@ void sums(Ctx &c, int slot_e, int slot_e2 = -1) {
     RecipBufs B = bufs(c);
     const int kb = (nk + MK_THREADS - 1) / MK_THREADS;
     int nch;
-    if (c.precision == SMD_PREC_MIXED) {
+    const int nt = c.rc.nmax + 1;
+    if (c.precision == SMD_PREC_MIXED && nt <= TAB_MAX) {
+        const int kbt = (nk + TS_THREADS - 1) / TS_THREADS;
+        const size_t sm = tsum_smem(nt, MODE == 0 ? 10 : (MODE == 1 ? 3 : 13));
+        int ch = sm_count() * blocks_per_sm((const void *)k_rsk_partial_t<MODE>, TS_THREADS, sm) / kbt;
+        nch = ch < 1 ? 1 : (ch > MK_CHUNKS ? MK_CHUNKS : ch);
+        k_rsk_partial_t<MODE><<<dim3(kbt, nch), TS_THREADS, sm, c.stream>>>(c.n, nk, nt, c.pos4, c.fixq, c.rc.kn,
+                                                                           c.rc.kvec, c.type_q, c.mu, c.qd, c.pind,
+                                                                           B.partial);
+    } else if (c.precision == SMD_PREC_MIXED) {
         nch = chunks_for((const void *)k_rsk_partial_f<MODE>, kb);
         k_rsk_partial_f<MODE><<<dim3(kb, nch), MK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn,
                                                                           c.rc.kvec, c.type_q, c.mu, c.qd, c.pind,
@@ -543,7 +777,18 @@ void forces(Ctx &c) {
     const int nk = c.rc.nk;
     RecipBufs B = bufs(c);
     const int nb = (int)(((long long)c.n * F_TPS + 255) / 256);
-    if (c.precision == SMD_PREC_MIXED) {
+    const int nt = c.rc.nmax + 1;
+    if (c.precision == SMD_PREC_MIXED && PERM && nt <= TAB_MAX) {
+        const int nbt = (c.n + TF_SITES - 1) / TF_SITES;
+        const size_t sm = tforce_smem(nt);
+        const int per = blocks_per_sm((const void *)k_rforce_t<IND>, 256, sm);
+        int ks = sm_count() * per / nbt;
+        const int tiles = (nk + FK_TILE - 1) / FK_TILE;
+        ks = ks < 1 ? 1 : (ks > tiles ? tiles : ks);
+        k_rforce_t<IND><<<dim3(nbt, ks), 256, sm, c.stream>>>(c.n, nk, nt, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,
+                                                              c.rc.kcoef, B.sk, c.type_q, c.mu, c.qd, c.pind,
+                                                              c.frc, c.trq);
+    } else if (c.precision == SMD_PREC_MIXED) {
         if (PERM) {
             const int ks = ksplit_for((const void *)k_rforce_f<IND>, nb, nk);
             k_rforce_f<IND><<<dim3(nb, ks), 256, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,

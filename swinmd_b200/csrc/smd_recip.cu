@@ -16,6 +16,8 @@
 // argument in [-pi, pi) with no reduction error.
 #include <cmath>
 #include <vector>
+#include <algorithm>
+#include <cstdlib>
 #include "smd_ctx.cuh"
 
 namespace smd {
@@ -242,6 +244,9 @@ int setup_recip(Ctx &c) {
     }
     const int nk = (int)nxs.size();
     c.rc.nk = nk;
+    c.rc.nmax = 0;
+    for (int k = 0; k < nk; k++)
+        c.rc.nmax = std::max(c.rc.nmax, std::max(std::abs(nxs[k]), std::max(std::abs(nys[k]), std::abs(nzs[k]))));
     std::vector<int> kn(3 * (size_t)nk);
     std::vector<double> kv(3 * (size_t)nk);
     for (int k = 0; k < nk; k++) {
@@ -262,7 +267,7 @@ int setup_recip(Ctx &c) {
         cudaMemcpy(c.rc.kcoef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice);
     }
     c.graph_dirty = 1;
-    return 0;
+    return c.mp_on ? mp_recip_prepare(c) : 0;
 }
 
 void launch_recip(Ctx &c) {
