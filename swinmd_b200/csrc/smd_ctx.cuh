@@ -41,6 +41,10 @@ struct Recip {               // Ewald reciprocal space (k half-space, k^2 < kcut
     long long *sk = nullptr; // [2][nk] structure factor, fixed point (SK_SCALE)
     double *kvec = nullptr;  // [3][nk] k in 1/nm
     int nmax = 0;            // largest |n| of any component
+    // FP32 force pass of the polarisable model: per k (nx, ny, nz, offset in
+    // its column) and (kx, ky, kz, 2c)
+    int4 *kpack = nullptr;
+    float4 *kb4 = nullptr;
 };
 
 struct Ctx {

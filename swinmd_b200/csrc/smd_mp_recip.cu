@@ -29,6 +29,7 @@
 //   FP32 path: a is the exact 32-bit integer phase n.(box fractions), sine and
 //   cosine from sincospif; the per-(site, k) arithmetic is FP32 with the
 //   running sums moved into FP64 after every tile of 64-128 terms.
+#include <vector>
 #include "smd_ctx.cuh"
 #include "smd_polar.cuh"
 
@@ -469,23 +470,33 @@ __global__ void __launch_bounds__(256) k_rforce_f(int n, int nk, const double4 *
 }
 
 // ---------------------------------------------------------------------------
-// FP32 passes with per-site phase tables (mixed path, |n| < TAB_MAX)
+// FP32 passes of the mixed path
 // ---------------------------------------------------------------------------
-// For a site with box fractions (fx, fy, fz) the table holds
-// e^{2 pi i m f / 2^32} for m = 0 .. nt-1 on each axis, every entry from the
-// exact integer phase m f mod 2^32 through sincos_phase32; the phase factor
-// of k = (nx, ny, nz) is X[nx] Y[|ny|] Z[|nz|] with the conjugate taken for
-// negative components (nx >= 0 in the half space).  Per (site, k) this is two
-// complex products instead of one sine/cosine evaluation.
-constexpr int TAB_MAX = 32;
-constexpr int TF_SITES = 64;    // sites per block of the force pass (F_TPS lanes each)
-constexpr int TS_THREADS = 256; // k per block of the sums pass
-constexpr int TS_SITES = 128;   // sites per tile of the sums pass
+// The k list is stored column by column: nx, then ny, then nz ascending by
+// one within a column.  Every phase factor below comes from exact integer
+// phases (sincos_phase32) with at most two complex products after them.
+//
+// Sums pass (one thread per k, site tiles in shared memory): each site of a
+// tile gets a table e^{2 pi i m f / 2^32}, m = 0 .. nt-1, per axis; the phase
+// factor of k = (nx, ny, nz) is X[nx] Y[|ny|] Z[|nz|], conjugated for
+// negative components (nx >= 0 in the half space).
+//
+// Force pass (one thread per site walking the k list): the factor of the
+// first k of a column comes from its exact phase, the others in the column
+// are that times the site's table entry e^{2 pi i m fz / 2^32}, m the offset
+// in the column.  All lanes read the same k record (shared-memory broadcast);
+// each lane's table row is at an odd stride, so the table reads of a warp
+// fall in distinct banks.
+constexpr int TAB_MAX = 32;     // |n| < TAB_MAX
+constexpr int TS_THREADS = 256; // k per block, sums pass
+constexpr int TS_SITES = 128;   // sites per tile, sums pass
+constexpr int CF_THREADS = 128; // sites per block, force pass
+constexpr int CF_KTILE = 256;
 
-__device__ __forceinline__ void table_entry(int m, unsigned f, float2 &out) {
+__device__ __forceinline__ float2 table_entry(int m, unsigned f) {
     float sn, cs;
     sincos_phase32((int)((unsigned)m * f), sn, cs);
-    out = make_float2(cs, sn);
+    return make_float2(cs, sn);
 }
 
 // offsets of k's three entries in a site table, sign bits of ny and nz
@@ -501,17 +512,16 @@ __device__ __forceinline__ void table_phase(const float2 *tab, int4 o, float &sn
     sn = fmaf(xr, zi, xi * Z.x);
 }
 
+// site data of a tile: (q, mu), (Qxx, Qxy, Qxz, Qyy), (Qyz, Qzz, px, py), (pz)
 template <int MODE>
-__global__ void __launch_bounds__(TS_THREADS) k_rsk_partial_t(int n, int nk, int nt, const double4 *pos4,
-                                                              const int4 *fixq, const int *kn, const double *kvec,
-                                                              const double *tq, const double *mu, const double *qd,
-                                                              const double *pind, double *partial) {
+__global__ void __launch_bounds__(TS_THREADS) k_rsk_tab(int n, int nk, int nt, const double4 *pos4,
+                                                        const int4 *fixq, const int *kn, const double *kvec,
+                                                        const double *tq, const double *mu, const double *qd,
+                                                        const double *pind, double *partial) {
     constexpr bool PERM = MODE != 1, IND = MODE != 0;
-    constexpr int PV = MODE == 1 ? 0 : 10;
-    constexpr int NV = MODE == 0 ? 10 : (MODE == 1 ? 3 : 13);
     extern __shared__ float4 s_dyn4[];
-    float2 *s_tab = (float2 *)s_dyn4;                          // [TS_SITES][3 nt]
-    float *s_v = (float *)(s_tab + (size_t)TS_SITES * 3 * nt); // [NV][TS_SITES]
+    float4 *s_v = s_dyn4;                                  // [TS_SITES][4]
+    float2 *s_tab = (float2 *)(s_v + 4 * TS_SITES);        // [TS_SITES][3 nt]
     const int k = blockIdx.x * TS_THREADS + threadIdx.x;
     const int ch = blockIdx.y;
     const int per = (n + gridDim.y - 1) / gridDim.y;
@@ -522,7 +532,7 @@ __global__ void __launch_bounds__(TS_THREADS) k_rsk_partial_t(int n, int nk, int
         kx = (float)kvec[k]; ky = (float)kvec[nk + k]; kz = (float)kvec[2 * nk + k];
         o = table_offsets(kn[k], kn[nk + k], kn[2 * nk + k], nt);
     }
-    const float kk[6] = {kx * kx, 2.f * kx * ky, 2.f * kx * kz, ky * ky, 2.f * ky * kz, kz * kz};
+    const float k0 = kx * kx, k1 = 2.f * kx * ky, k2 = 2.f * kx * kz, k3 = ky * ky, k4 = 2.f * ky * kz, k5 = kz * kz;
     const int row = 3 * nt;
     double acc[6] = {0, 0, 0, 0, 0, 0};
     for (int base = s0; base < s1; base += TS_SITES) {
@@ -531,17 +541,20 @@ __global__ void __launch_bounds__(TS_THREADS) k_rsk_partial_t(int n, int nk, int
         for (int e = threadIdx.x; e < cnt * row; e += TS_THREADS) {
             const int sl = e / row, r = e - sl * row, ax = r / nt, m = r - ax * nt;
             const int4 f = fixq[base + sl];
-            table_entry(m, (unsigned)(ax == 0 ? f.x : (ax == 1 ? f.y : f.z)), s_tab[e]);
+            s_tab[e] = table_entry(m, (unsigned)(ax == 0 ? f.x : (ax == 1 ? f.y : f.z)));
         }
         if (threadIdx.x < cnt) {
             const int i = base + threadIdx.x;
+            float v[16] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             if (PERM) {
-                s_v[threadIdx.x] = (float)(tq[(int)pos4[i].w] / SQC_R);
-                for (int d = 0; d < 3; d++) s_v[(1 + d) * TS_SITES + threadIdx.x] = (float)mu[(size_t)d * n + i];
-                for (int d = 0; d < 6; d++) s_v[(4 + d) * TS_SITES + threadIdx.x] = (float)qd[(size_t)d * n + i];
+                v[0] = (float)(tq[(int)pos4[i].w] / SQC_R);
+                for (int d = 0; d < 3; d++) v[1 + d] = (float)mu[(size_t)d * n + i];
+                for (int d = 0; d < 6; d++) v[4 + d] = (float)qd[(size_t)d * n + i];
             }
             if (IND)
-                for (int d = 0; d < 3; d++) s_v[(PV + d) * TS_SITES + threadIdx.x] = (float)pind[(size_t)d * n + i];
+                for (int d = 0; d < 3; d++) v[10 + d] = (float)pind[(size_t)d * n + i];
+            for (int w = 0; w < 4; w++)
+                s_v[threadIdx.x * 4 + w] = make_float4(v[4 * w], v[4 * w + 1], v[4 * w + 2], v[4 * w + 3]);
         }
         __syncthreads();
         if (k < nk) {
@@ -551,21 +564,21 @@ __global__ void __launch_bounds__(TS_THREADS) k_rsk_partial_t(int n, int nk, int
                 float sn, cs;
                 table_phase(s_tab + q * row, o, sn, cs);
                 if (PERM) {
-                    const float *v = s_v + q;
-                    float kqk = v[4 * TS_SITES] * kk[0];
-                    kqk = fmaf(v[5 * TS_SITES], kk[1], kqk);
-                    kqk = fmaf(v[6 * TS_SITES], kk[2], kqk);
-                    kqk = fmaf(v[7 * TS_SITES], kk[3], kqk);
-                    kqk = fmaf(v[8 * TS_SITES], kk[4], kqk);
-                    kqk = fmaf(v[9 * TS_SITES], kk[5], kqk);
-                    const float qk = v[0] - kqk;
-                    const float mk = fmaf(v[TS_SITES], kx, fmaf(v[2 * TS_SITES], ky, v[3 * TS_SITES] * kz));
+                    const float4 a = s_v[q * 4], b = s_v[q * 4 + 1], c = s_v[q * 4 + 2];
+                    float kqk = b.x * k0;
+                    kqk = fmaf(b.y, k1, kqk);
+                    kqk = fmaf(b.z, k2, kqk);
+                    kqk = fmaf(b.w, k3, kqk);
+                    kqk = fmaf(c.x, k4, kqk);
+                    kqk = fmaf(c.y, k5, kqk);
+                    const float qk = a.x - kqk;
+                    const float mk = fmaf(a.y, kx, fmaf(a.z, ky, a.w * kz));
                     t0 = fmaf(qk, cs, t0); t1 = fmaf(qk, sn, t1);
                     t2 = fmaf(mk, cs, t2); t3 = fmaf(mk, sn, t3);
                 }
                 if (IND) {
-                    const float *v = s_v + PV * TS_SITES + q;
-                    const float pk = fmaf(v[0], kx, fmaf(v[TS_SITES], ky, v[2 * TS_SITES] * kz));
+                    const float4 c = s_v[q * 4 + 2], d = s_v[q * 4 + 3];
+                    const float pk = fmaf(c.z, kx, fmaf(c.w, ky, d.x * kz));
                     t4 = fmaf(pk, cs, t4); t5 = fmaf(pk, sn, t5);
                 }
             }
@@ -581,29 +594,25 @@ __global__ void __launch_bounds__(TS_THREADS) k_rsk_partial_t(int n, int nk, int
     }
 }
 
+// kpack[k] = (nx, ny, nz, m) with m the offset of k in its column
 template <bool IND>
-__global__ void __launch_bounds__(256) k_rforce_t(int n, int nk, int nt, const double4 *pos4, const int4 *fixq,
-                                                  const int *kn, const double *kvec, const double *kcoef,
-                                                  const double *sk, const double *tq, const double *mu,
-                                                  const double *qd, const double *pind, long long *frc,
-                                                  long long *trq) {
+__global__ void __launch_bounds__(CF_THREADS) k_rforce_col(int n, int nk, int zs, const double4 *pos4,
+                                                           const int4 *fixq, const int4 *kpack, const float4 *kb4,
+                                                           const double *sk, const double *tq, const double *mu,
+                                                           const double *qd, const double *pind, long long *frc,
+                                                           long long *trq) {
     extern __shared__ float4 s_dyn4[];
-    float4 *s_kb = s_dyn4;                          // [FK_TILE] kx, ky, kz, 2c
-    int4 *s_o = (int4 *)(s_kb + FK_TILE);           // [FK_TILE] table offsets
-    float2 *s_uw = (float2 *)(s_o + FK_TILE);       // [FK_TILE] U, W
-    float2 *s_tab = s_uw + FK_TILE;                 // [TF_SITES][3 nt]
-    const int ls = threadIdx.x / F_TPS, t = threadIdx.x % F_TPS;
-    const int i = blockIdx.x * TF_SITES + ls;
-    const int row = 3 * nt;
-    float2 *tab = s_tab + ls * row;
+    int4 *s_kp = (int4 *)s_dyn4;                    // [CF_KTILE]
+    float4 *s_kb = (float4 *)(s_kp + CF_KTILE);     // [CF_KTILE]
+    float2 *s_uw = (float2 *)(s_kb + CF_KTILE);     // [CF_KTILE]
+    float2 *s_z = s_uw + CF_KTILE;                  // [CF_THREADS][zs]
+    const int i = blockIdx.x * CF_THREADS + threadIdx.x;
+    const bool own = i < n;
+    int4 pf = make_int4(0, 0, 0, 0);
     float qi = 0.f, dx = 0.f, dy = 0.f, dz = 0.f;
     float Qxx = 0.f, Qxy = 0.f, Qxz = 0.f, Qyy = 0.f, Qyz = 0.f, Qzz = 0.f;
-    if (i < n) {
-        const int4 pf = fixq[i];
-        for (int e = t; e < row; e += F_TPS) {
-            const int ax = e / nt, m = e - ax * nt;
-            table_entry(m, (unsigned)(ax == 0 ? pf.x : (ax == 1 ? pf.y : pf.z)), tab[e]);
-        }
+    if (own) {
+        pf = fixq[i];
         qi = (float)(tq[(int)pos4[i].w] / SQC_R);
         double d3[3] = {mu[i], mu[n + i], mu[2 * n + i]};
         if (IND)
@@ -612,34 +621,42 @@ __global__ void __launch_bounds__(256) k_rforce_t(int n, int nk, int nt, const d
         Qxx = (float)qd[i]; Qxy = (float)qd[n + i]; Qxz = (float)qd[2 * n + i];
         Qyy = (float)qd[3 * n + i]; Qyz = (float)qd[4 * n + i]; Qzz = (float)qd[5 * n + i];
     }
+    float2 *zt = s_z + threadIdx.x * zs;
+    for (int m = 0; m < zs; m++) zt[m] = table_entry(m, (unsigned)pf.z);
     double F[3] = {0, 0, 0}, EA[3] = {0, 0, 0}, GX[3] = {0, 0, 0};
-    const int kper = (((nk + gridDim.y - 1) / gridDim.y + FK_TILE - 1) / FK_TILE) * FK_TILE;
+    const int kper = (((nk + gridDim.y - 1) / gridDim.y + CF_KTILE - 1) / CF_KTILE) * CF_KTILE;
     const int kb0 = blockIdx.y * kper, kb1 = min(nk, kb0 + kper);
-    for (int base = kb0; base < kb1; base += FK_TILE) {
+    float c0 = 1.f, s0 = 0.f;   // factor of the current column's first k
+    for (int base = kb0; base < kb1; base += CF_KTILE) {
+        const int cnt = min(CF_KTILE, kb1 - base);
         __syncthreads();
-        const int kk = base + threadIdx.x;
-        if (kk < kb1) {
-            const double CqQ = sk[kk], SqQ = sk[nk + kk], Cm = sk[2 * (size_t)nk + kk], Sm = sk[3 * (size_t)nk + kk];
+        for (int e = threadIdx.x; e < cnt; e += CF_THREADS) {
+            const int k = base + e;
+            s_kp[e] = kpack[k];
+            s_kb[e] = kb4[k];
+            const double CqQ = sk[k], SqQ = sk[nk + k], Cm = sk[2 * (size_t)nk + k], Sm = sk[3 * (size_t)nk + k];
             double U = CqQ - Sm, W = SqQ + Cm;
             if (IND) {
-                U -= sk[5 * (size_t)nk + kk];
-                W += sk[4 * (size_t)nk + kk];
+                U -= sk[5 * (size_t)nk + k];
+                W += sk[4 * (size_t)nk + k];
             }
-            s_kb[threadIdx.x] = make_float4((float)kvec[kk], (float)kvec[nk + kk], (float)kvec[2 * (size_t)nk + kk],
-                                            (float)(2.0 * kcoef[kk]));
-            s_uw[threadIdx.x] = make_float2((float)U, (float)W);
-            s_o[threadIdx.x] = table_offsets(kn[kk], kn[nk + kk], kn[2 * (size_t)nk + kk], nt);
+            s_uw[e] = make_float2((float)U, (float)W);
         }
         __syncthreads();
-        const int cnt = min(FK_TILE, kb1 - base);
-        if (i < n) {
+        for (int t0 = 0; t0 < cnt; t0 += 64) {
             float f0 = 0.f, f1 = 0.f, f2 = 0.f, e0 = 0.f, e1 = 0.f, e2 = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
-#pragma unroll 2
-            for (int q = t; q < cnt; q += F_TPS) {
-                const float4 kb = s_kb[q];
-                const float2 uw = s_uw[q];
-                float sn, cs;
-                table_phase(tab, s_o[q], sn, cs);
+            const int t1 = min(cnt, t0 + 64);
+            for (int t = t0; t < t1; t++) {
+                const int4 kp = s_kp[t];
+                if (kp.w == 0 || base + t == kb0) {
+                    const int ph = (int)((unsigned)kp.x * (unsigned)pf.x + (unsigned)kp.y * (unsigned)pf.y +
+                                         (unsigned)(kp.z - kp.w) * (unsigned)pf.z);
+                    sincos_phase32(ph, s0, c0);
+                }
+                const float2 z = zt[kp.w];
+                const float cs = fmaf(c0, z.x, -s0 * z.y), sn = fmaf(c0, z.y, s0 * z.x);
+                const float4 kb = s_kb[t];
+                const float2 uw = s_uw[t];
                 const float A = fmaf(sn, uw.x, -cs * uw.y);
                 const float B = fmaf(cs, uw.x, sn * uw.y);
                 const float qkx = fmaf(Qxx, kb.x, fmaf(Qxy, kb.y, Qxz * kb.z));
@@ -660,12 +677,7 @@ __global__ void __launch_bounds__(256) k_rforce_t(int n, int nk, int nt, const d
             GX[0] += g0; GX[1] += g1; GX[2] += g2;
         }
     }
-    for (int d = 0; d < 3; d++) {
-        F[d] = group_sum<F_TPS>(F[d]);
-        EA[d] = group_sum<F_TPS>(EA[d]);
-        GX[d] = group_sum<F_TPS>(GX[d]);
-    }
-    if (i < n && t == 0) {
+    if (own) {
         const V3 m = v3(mu[i], mu[n + i], mu[2 * n + i]);
         const V3 tau = crs(m, v3(EA[0], EA[1], EA[2])) - 2.0 * v3(GX[0], GX[1], GX[2]);
         add_fix3_atomic(frc, n, i, v3(F[0], F[1], F[2]), KE);
@@ -673,21 +685,47 @@ __global__ void __launch_bounds__(256) k_rforce_t(int n, int nk, int nt, const d
     }
 }
 
-size_t tsum_smem(int nt, int nv) { return (size_t)TS_SITES * 3 * nt * sizeof(float2) + (size_t)nv * TS_SITES * sizeof(float); }
-size_t tforce_smem(int nt) {
-    return (size_t)FK_TILE * (sizeof(float4) + sizeof(int4) + sizeof(float2)) + (size_t)TF_SITES * 3 * nt * sizeof(float2);
+size_t tsum_smem(int nt) { return (size_t)TS_SITES * (4 * sizeof(float4) + 3 * nt * sizeof(float2)); }
+int zrow(int nmax) { return (2 * nmax + 1) | 1; }
+size_t tforce_smem(int zs) {
+    return (size_t)CF_KTILE * (sizeof(int4) + sizeof(float4) + sizeof(float2)) + (size_t)CF_THREADS * zs * sizeof(float2);
 }
 
-// dynamic shared memory of the table kernels (set once, outside any capture)
+// per-k records of the force pass and the kernels' dynamic shared memory
+// (once per k set, outside any capture)
 int mp_recip_prepare(Ctx &c) {
-    const int nt = c.rc.nmax + 1;
-    if (nt > TAB_MAX) return 0;
+    const int nk = c.rc.nk;
+    cudaFree(c.rc.kpack); cudaFree(c.rc.kb4);
+    c.rc.kpack = nullptr; c.rc.kb4 = nullptr;
+    if (nk == 0 || c.n == 0 || c.rc.nmax + 1 > TAB_MAX) return 0;
+    std::vector<int> kn(3 * (size_t)nk);
+    std::vector<double> kv(3 * (size_t)nk), kc(nk);
+    if (cudaMemcpy(kn.data(), c.rc.kn, kn.size() * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(kv.data(), c.rc.kvec, kv.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(kc.data(), c.rc.kcoef, kc.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return SMD_ERR_CUDA;
+    std::vector<int4> kp(nk);
+    std::vector<float4> kb(nk);
+    int col = 0;
+    for (int k = 0; k < nk; k++) {
+        const int nx = kn[k], ny = kn[nk + k], nz = kn[2 * nk + k];
+        const bool start = k == 0 || nx != kn[k - 1] || ny != kn[nk + k - 1] || nz != kn[2 * nk + k - 1] + 1;
+        if (start) col = k;
+        kp[k] = make_int4(nx, ny, nz, k - col);
+        kb[k] = make_float4((float)kv[k], (float)kv[nk + k], (float)kv[2 * nk + k], (float)(2.0 * kc[k]));
+    }
+    if (cudaMalloc(&c.rc.kpack, nk * sizeof(int4)) != cudaSuccess ||
+        cudaMalloc(&c.rc.kb4, nk * sizeof(float4)) != cudaSuccess)
+        return SMD_ERR_CUDA;
+    cudaMemcpy(c.rc.kpack, kp.data(), nk * sizeof(int4), cudaMemcpyHostToDevice);
+    cudaMemcpy(c.rc.kb4, kb.data(), nk * sizeof(float4), cudaMemcpyHostToDevice);
+    const int nt = c.rc.nmax + 1, zs = zrow(c.rc.nmax);
     cudaError_t e = cudaSuccess;
-    e = e ? e : cudaFuncSetAttribute(k_rsk_partial_t<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(nt, 10));
-    e = e ? e : cudaFuncSetAttribute(k_rsk_partial_t<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(nt, 3));
-    e = e ? e : cudaFuncSetAttribute(k_rsk_partial_t<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(nt, 13));
-    e = e ? e : cudaFuncSetAttribute(k_rforce_t<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tforce_smem(nt));
-    e = e ? e : cudaFuncSetAttribute(k_rforce_t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tforce_smem(nt));
+    if (!e) e = cudaFuncSetAttribute(k_rsk_tab<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(nt));
+    if (!e) e = cudaFuncSetAttribute(k_rsk_tab<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(nt));
+    if (!e) e = cudaFuncSetAttribute(k_rsk_tab<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(nt));
+    if (!e) e = cudaFuncSetAttribute(k_rforce_col<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tforce_smem(zs));
+    if (!e) e = cudaFuncSetAttribute(k_rforce_col<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tforce_smem(zs));
     return e == cudaSuccess ? 0 : SMD_ERR_CUDA;
 }
 
@@ -740,15 +778,14 @@ void sums(Ctx &c, int slot_e, int slot_e2 = -1) {
     RecipBufs B = bufs(c);
     const int kb = (nk + MK_THREADS - 1) / MK_THREADS;
     int nch;
-    const int nt = c.rc.nmax + 1;
-    if (c.precision == SMD_PREC_MIXED && nt <= TAB_MAX) {
+    if (c.precision == SMD_PREC_MIXED && c.rc.kpack) {
+        const int nt = c.rc.nmax + 1;
         const int kbt = (nk + TS_THREADS - 1) / TS_THREADS;
-        const size_t sm = tsum_smem(nt, MODE == 0 ? 10 : (MODE == 1 ? 3 : 13));
-        int ch = sm_count() * blocks_per_sm((const void *)k_rsk_partial_t<MODE>, TS_THREADS, sm) / kbt;
+        const size_t sm = tsum_smem(nt);
+        int ch = sm_count() * blocks_per_sm((const void *)k_rsk_tab<MODE>, TS_THREADS, sm) / kbt;
         nch = ch < 1 ? 1 : (ch > MK_CHUNKS ? MK_CHUNKS : ch);
-        k_rsk_partial_t<MODE><<<dim3(kbt, nch), TS_THREADS, sm, c.stream>>>(c.n, nk, nt, c.pos4, c.fixq, c.rc.kn,
-                                                                           c.rc.kvec, c.type_q, c.mu, c.qd, c.pind,
-                                                                           B.partial);
+        k_rsk_tab<MODE><<<dim3(kbt, nch), TS_THREADS, sm, c.stream>>>(c.n, nk, nt, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,
+                                                                     c.type_q, c.mu, c.qd, c.pind, B.partial);
     } else if (c.precision == SMD_PREC_MIXED) {
         nch = chunks_for((const void *)k_rsk_partial_f<MODE>, kb);
         k_rsk_partial_f<MODE><<<dim3(kb, nch), MK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn,
@@ -777,17 +814,16 @@ void forces(Ctx &c) {
     const int nk = c.rc.nk;
     RecipBufs B = bufs(c);
     const int nb = (int)(((long long)c.n * F_TPS + 255) / 256);
-    const int nt = c.rc.nmax + 1;
-    if (c.precision == SMD_PREC_MIXED && PERM && nt <= TAB_MAX) {
-        const int nbt = (c.n + TF_SITES - 1) / TF_SITES;
-        const size_t sm = tforce_smem(nt);
-        const int per = blocks_per_sm((const void *)k_rforce_t<IND>, 256, sm);
-        int ks = sm_count() * per / nbt;
-        const int tiles = (nk + FK_TILE - 1) / FK_TILE;
+    if (c.precision == SMD_PREC_MIXED && PERM && c.rc.kpack) {
+        const int nbs = (c.n + CF_THREADS - 1) / CF_THREADS;
+        const int tiles = (nk + CF_KTILE - 1) / CF_KTILE;
+        const int zs = zrow(c.rc.nmax);
+        const size_t sm = tforce_smem(zs);
+        int ks = sm_count() * blocks_per_sm((const void *)k_rforce_col<IND>, CF_THREADS, sm) / nbs;
         ks = ks < 1 ? 1 : (ks > tiles ? tiles : ks);
-        k_rforce_t<IND><<<dim3(nbt, ks), 256, sm, c.stream>>>(c.n, nk, nt, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,
-                                                              c.rc.kcoef, B.sk, c.type_q, c.mu, c.qd, c.pind,
-                                                              c.frc, c.trq);
+        k_rforce_col<IND><<<dim3(nbs, ks), CF_THREADS, sm, c.stream>>>(c.n, nk, zs, c.pos4, c.fixq, c.rc.kpack,
+                                                                      c.rc.kb4, B.sk, c.type_q, c.mu, c.qd, c.pind,
+                                                                      c.frc, c.trq);
     } else if (c.precision == SMD_PREC_MIXED) {
         if (PERM) {
             const int ks = ksplit_for((const void *)k_rforce_f<IND>, nb, nk);
