@@ -79,8 +79,12 @@ enum {
     SMD_GUESS_LEARNED = 2   /* p0 from the per-site network (smd_mlp_*) */
 };
 
-/* thermostat kinds */
-enum { SMD_THERMO_NONE = 0, SMD_THERMO_NOSE_HOOVER = 1 };
+/* thermostat kinds: SMD_THERMO_NOSE_HOOVER is the leap-frog integrator of
+ * LFIntegrator; SMD_THERMO_NH_CHAIN selects the velocity-Verlet integrator
+ * with the 4-link MTK chain of NHIntegrator::chain
+ * (src/integrators/NHIntegrator.cpp:1814-1912) at constant volume, which
+ * also carries SLLOD shear (strain_rate != 0, with Lees-Edwards images) */
+enum { SMD_THERMO_NONE = 0, SMD_THERMO_NOSE_HOOVER = 1, SMD_THERMO_NH_CHAIN = 2 };
 
 /* Leap-frog integrator settings: the config.txt fields that
  * LFIntegrator / Integrator read (src/Integrator.cpp:14-99). */
@@ -96,7 +100,8 @@ typedef struct {
     int shake_max_iter;    /* SHAKE maxCount */
     int atom_ndf;          /* degrees of freedom (Integrator.cpp:22-27) */
     int mol_ndf;
-    double strain_rate;    /* SLLOD planar Couette rate (1/ps); 0: equilibrium */
+    double strain_rate;    /* SLLOD planar Couette rate du_x/dy (1/ps); 0: equilibrium.
+                              Needs SMD_THERMO_NH_CHAIN and short-range terms only */
 } smd_integrator_params;
 
 /* Per-step observables the reference keeps in Ensemble/Integrator members. */
@@ -116,6 +121,7 @@ typedef struct {
     int64_t pairs_in_cutoff; /* unordered pairs inside the short-range cutoff */
     uint32_t status;
     uint32_t pad;
+    double shear_offset;     /* Lees-Edwards offset of the images one box up (nm) */
 } smd_observables;
 
 /* ---- lifetime -------------------------------------------------------- */

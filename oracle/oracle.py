@@ -33,6 +33,14 @@ def lib():
                                   ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                   ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                   ctypes.c_int, _D, _D, _D]
+        _lib.or_lj_nhc_md.restype = ctypes.c_int
+        _lib.or_lj_nhc_md.argtypes = [ctypes.c_int, _D, _D, _D, _I, _D, ctypes.c_int, _D, _D,
+                                      ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                      _D, _D, _D, _D, _D]
+        _lib.or_lj_le_forces.restype = ctypes.c_double
+        _lib.or_lj_le_forces.argtypes = [ctypes.c_int, _D, _I, _D, ctypes.c_double, ctypes.c_int, _D, _D,
+                                         ctypes.c_double, ctypes.c_int, _D, _D]
         _lib.or_ewald_real.restype = ctypes.c_double
         _lib.or_ewald_real.argtypes = [ctypes.c_int, _D, _D, _D, ctypes.c_double, ctypes.c_double,
                                        _I, ctypes.c_int64, _D, _D]
@@ -106,6 +114,39 @@ def lj_md(system, pos, vel, box, nsteps, e_lrc=0.0, v_lrc=0.0):
     assert r == 0, r
     return {"pos": pos.reshape(-1, 3), "vel": vel.reshape(-1, 3), "vtminus": vtm.reshape(-1, 3),
             "epot": ep, "temp": tt, "zeta": zz}
+
+
+def lj_nhc_md(system, pos, vel, box, nsteps, strain_rate=0.0, ndf=None):
+    """Nose-Hoover chain velocity-Verlet MD (optionally SLLOD + Lees-Edwards)
+    of a Lennard-Jones system; see or_lj_nhc_md in smd_oracle.c."""
+    c = system.config
+    s2, e4 = system.lj_table()
+    L = np.array(box if np.ndim(box) else [box] * 3, np.float64)
+    pos = np.array(pos, np.float64).reshape(-1).copy()
+    vel = np.array(vel, np.float64).reshape(-1).copy()
+    out = [np.zeros(nsteps) for _ in range(5)]
+    ndf = 3 * system.n_atoms - 3 if ndf is None else ndf
+    r = lib().or_lj_nhc_md(system.n_atoms, pos.ctypes.data_as(_D), vel.ctypes.data_as(_D),
+                           d(system.masses()), i32(system.atom_type), d(L), len(system.atom_types), d(s2),
+                           d(e4), c.cutoff, int(c.switch_on), c.timestep, c.temperature, c.coupl_const,
+                           strain_rate, ndf, nsteps, *[o.ctypes.data_as(_D) for o in out])
+    assert r == 0, r
+    return {"pos": pos.reshape(-1, 3), "vel": vel.reshape(-1, 3), "epot": out[0], "temp": out[1],
+            "vnh0": out[2], "pxy": out[3], "delta": out[4]}
+
+
+def lj_le_forces(system, pos, box, delta):
+    """LJ forces and energy with Lees-Edwards images at offset delta."""
+    c = system.config
+    s2, e4 = system.lj_table()
+    L = np.array(box if np.ndim(box) else [box] * 3, np.float64)
+    pos = np.ascontiguousarray(pos, np.float64).reshape(-1)
+    f = np.zeros(3 * system.n_atoms)
+    w = np.zeros(9)
+    e = lib().or_lj_le_forces(system.n_atoms, pos.ctypes.data_as(_D), i32(system.atom_type), d(L), delta,
+                              len(system.atom_types), d(s2), d(e4), c.cutoff, int(c.switch_on),
+                              f.ctypes.data_as(_D), w.ctypes.data_as(_D))
+    return f.reshape(-1, 3), e
 
 
 def ewald(system, pos, box, pairs):

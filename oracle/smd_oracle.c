@@ -465,3 +465,176 @@ int or_water_md(int nmol, double *pos, double *vel, const double *mass, const in
     free(pairs); free(f); free(f2); free(vtm); free(disp); free(P);
     return 0;
 }
+
+/* ------------------------------------------------------------------------
+ * Nose-Hoover chain (NVT) velocity-Verlet MD of a Lennard-Jones system,
+ * optionally under SLLOD planar Couette shear with Lees-Edwards images.
+ *
+ * The chain restates NHIntegrator::chain (src/integrators/NHIntegrator.cpp:
+ * 1814-1912): 4 links, nc = 5 multiple steps, 3 Suzuki-Yoshida weights,
+ * Q_0 = Nf kT tau^2, Q_k = kT tau^2 (:113-119).  The reference's integrator
+ * couples a barostat in every step (vlog, glog, box rescaling); this NVT
+ * restatement drops that degree of freedom (vlog = 0, Nf kT in the first
+ * link's force).  Step order as NHIntegrator::run (:380-408, :628-644):
+ * chain half step, half kick, drift, forces, half kick, chain half step.
+ *
+ * SLLOD (no reference code; Evans and Morriss, "Statistical Mechanics of
+ * Nonequilibrium Liquids", ch. 6): peculiar velocities v, flow u = (g y,0,0);
+ *   dr/dt = v + g y e_x,   dv/dt = F/m - g v_y e_x - zeta v.
+ * The streaming and the -g v_y e_x term are each integrated exactly over
+ * their sub-steps: around every half kick v_x -= g (dt/2) v_y; the drift is
+ * x += dt v_x + g dt (y + dt v_y / 2), y += dt v_y, z += dt v_z.
+ * Lees-Edwards: the image one box up is shifted by delta = g Ly t (mod Lx)
+ * in x; minimum image takes y first (shifting x by -/+ delta per crossing),
+ * then x and z.  All pairs within rc are found by a direct O(N^2) search.
+ * Outputs per step: potential energy after the step's forces, atomic
+ * temperature 2 KE / (Nf kB), first chain velocity, pressure tensor xy
+ * component (sum m v_x v_y + W_xy)/V with W_ab = -sum r_a f_b, and delta.
+ * Parity unpinned: the reference has neither a constant-volume chain
+ * integrator nor SLLOD, so nothing of the reference's own output checks this
+ * function.
+ * ---------------------------------------------------------------------- */
+static void pbc_le(double *d, const double *L, double delta) {
+    double hy = L[1] / 2.0, hx = L[0] / 2.0, hz = L[2] / 2.0;
+    while (d[1] >= hy) { d[1] -= L[1]; d[0] -= delta; }
+    while (d[1] < -hy) { d[1] += L[1]; d[0] += delta; }
+    while (d[0] >= hx) d[0] -= L[0];
+    while (d[0] < -hx) d[0] += L[0];
+    while (d[2] >= hz) d[2] -= L[2];
+    while (d[2] < -hz) d[2] += L[2];
+}
+
+static double lj_le_forces(int n, const double *pos, const int32_t *type, const double *L, double delta,
+                           int nt, const double *sig2, const double *eps4, double rc, int shift,
+                           double *f, double *w) {
+    double rc2 = rc * rc, rcut_2 = 1.0 / rc2, energy = 0.0;
+    memset(f, 0, sizeof(double) * 3 * n);
+    memset(w, 0, sizeof(double) * 9);
+    for (int i = 0; i < n; i++)
+        for (int j = i + 1; j < n; j++) {
+            double d[3] = {pos[3 * j] - pos[3 * i], pos[3 * j + 1] - pos[3 * i + 1],
+                           pos[3 * j + 2] - pos[3 * i + 2]};
+            pbc_le(d, L, delta);
+            double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            double rij2 = r * r;
+            if (rij2 > rc2) continue;
+            int t = type[i] * nt + type[j];
+            double r_1 = 1.0 / r, rij_2 = r_1 * r_1;
+            double sr2 = sig2[t] * rij_2, sr6 = sr2 * sr2 * sr2, sr12 = sr6 * sr6;
+            double e = eps4[t] * (sr12 - sr6);
+            double fs = (sr12 + sr12 - sr6) * 6 * eps4[t] * rij_2;
+            if (shift) {
+                double c2 = sig2[t] * rcut_2, c6 = c2 * c2 * c2;
+                e -= eps4[t] * (c6 * c6 - c6);
+            }
+            energy += e;
+            double fij[3] = {-fs * d[0], -fs * d[1], -fs * d[2]};
+            for (int k = 0; k < 3; k++) { f[3 * i + k] += fij[k]; f[3 * j + k] -= fij[k]; }
+            vir_add(w, fij, d);
+        }
+    return energy;
+}
+
+static double nhc_half(double *vnh, const double *qnh, double ekin, double kT, double nf, double dt) {
+    const double w0 = 1.0 / (2.0 - pow(2.0, 1.0 / 3.0));
+    const double wj[3] = {w0, 1.0 - 2.0 * w0, w0};
+    const int nc = 5;
+    double scale = 1.0, gnh[4];
+    for (int i = 0; i < nc; i++)
+        for (int j = 0; j < 3; j++) {
+            double dts = wj[j] * dt / nc, dts2 = 0.5 * dts, dts4 = 0.25 * dts, dts8 = 0.125 * dts, ex;
+            gnh[3] = (qnh[2] * vnh[2] * vnh[2] - kT) / qnh[3];
+            vnh[3] += gnh[3] * dts4;
+            gnh[2] = (qnh[1] * vnh[1] * vnh[1] - kT) / qnh[2];
+            ex = exp(-vnh[3] * dts8);
+            vnh[2] = ex * (vnh[2] * ex + gnh[2] * dts4);
+            gnh[1] = (qnh[0] * vnh[0] * vnh[0] - kT) / qnh[1];
+            ex = exp(-vnh[2] * dts8);
+            vnh[1] = ex * (vnh[1] * ex + gnh[1] * dts4);
+            gnh[0] = (2.0 * ekin - nf * kT) / qnh[0];
+            ex = exp(-vnh[1] * dts8);
+            vnh[0] = ex * (vnh[0] * ex + gnh[0] * dts4);
+            ex = exp(-vnh[0] * dts2);
+            scale *= ex;
+            ekin = ekin * ex * ex;
+            gnh[0] = (2.0 * ekin - nf * kT) / qnh[0];
+            ex = exp(-vnh[1] * dts8);
+            vnh[0] = ex * (vnh[0] * ex + gnh[0] * dts4);
+            gnh[1] = (qnh[0] * vnh[0] * vnh[0] - kT) / qnh[1];
+            ex = exp(-vnh[2] * dts8);
+            vnh[1] = ex * (vnh[1] * ex + gnh[1] * dts4);
+            gnh[2] = (qnh[1] * vnh[1] * vnh[1] - kT) / qnh[2];
+            ex = exp(-vnh[3] * dts8);
+            vnh[2] = ex * (vnh[2] * ex + gnh[2] * dts4);
+            gnh[3] = (qnh[2] * vnh[2] * vnh[2] - kT) / qnh[3];
+            vnh[3] += gnh[3] * dts4;
+        }
+    return scale;
+}
+
+int or_lj_nhc_md(int n, double *pos, double *vel, const double *mass, const int32_t *type, const double *L,
+                 int nt, const double *sig2, const double *eps4, double rc, int shift, double dt, double T,
+                 double tau, double gamma, int ndf, int nsteps, double *out_epot, double *out_temp,
+                 double *out_vnh0, double *out_pxy, double *out_delta) {
+    double *f = (double *)malloc(sizeof(double) * 3 * n);
+    double w[9];
+    const double kT = OR_KB * T, nf = (double)ndf, vol = L[0] * L[1] * L[2];
+    double qnh[4], vnh[4] = {0, 0, 0, 0};
+    for (int k = 0; k < 4; k++) qnh[k] = kT * tau * tau;
+    qnh[0] *= nf;
+    double delta = 0.0;
+    lj_le_forces(n, pos, type, L, delta, nt, sig2, eps4, rc, shift, f, w);
+    for (int s = 0; s < nsteps; s++) {
+        double ekin = 0;
+        for (int i = 0; i < n; i++)
+            ekin += 0.5 * mass[i] * (vel[3 * i] * vel[3 * i] + vel[3 * i + 1] * vel[3 * i + 1] + vel[3 * i + 2] * vel[3 * i + 2]);
+        double sc = nhc_half(vnh, qnh, ekin, kT, nf, dt);
+        delta = fmod(delta + gamma * L[1] * dt, L[0]);
+        if (delta < 0) delta += L[0];
+        for (int i = 0; i < n; i++) {
+            double *v = &vel[3 * i], *r = &pos[3 * i], mr = 1.0 / mass[i];
+            for (int k = 0; k < 3; k++) v[k] *= sc;
+            v[0] -= gamma * 0.5 * dt * v[1];
+            for (int k = 0; k < 3; k++) v[k] += 0.5 * dt * mr * f[3 * i + k];
+            r[0] += dt * v[0] + gamma * dt * (r[1] + 0.5 * dt * v[1]);
+            r[1] += dt * v[1];
+            r[2] += dt * v[2];
+            /* Lees-Edwards wrap (y first), then x and z */
+            if (r[1] >= L[1] / 2.0) { r[1] -= L[1]; r[0] -= delta; }
+            else if (r[1] < -L[1] / 2.0) { r[1] += L[1]; r[0] += delta; }
+            while (r[0] >= L[0] / 2.0) r[0] -= L[0];
+            while (r[0] < -L[0] / 2.0) r[0] += L[0];
+            while (r[2] >= L[2] / 2.0) r[2] -= L[2];
+            while (r[2] < -L[2] / 2.0) r[2] += L[2];
+        }
+        out_epot[s] = lj_le_forces(n, pos, type, L, delta, nt, sig2, eps4, rc, shift, f, w);
+        ekin = 0;
+        double kxy = 0;
+        for (int i = 0; i < n; i++) {
+            double *v = &vel[3 * i], mr = 1.0 / mass[i];
+            for (int k = 0; k < 3; k++) v[k] += 0.5 * dt * mr * f[3 * i + k];
+            v[0] -= gamma * 0.5 * dt * v[1];
+            ekin += 0.5 * mass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        }
+        sc = nhc_half(vnh, qnh, ekin, kT, nf, dt);
+        ekin = 0;
+        for (int i = 0; i < n; i++) {
+            double *v = &vel[3 * i];
+            for (int k = 0; k < 3; k++) v[k] *= sc;
+            ekin += 0.5 * mass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            kxy += mass[i] * v[0] * v[1];
+        }
+        out_temp[s] = 2.0 * ekin / (nf * OR_KB);
+        out_vnh0[s] = vnh[0];
+        out_pxy[s] = (kxy + w[1]) / vol;
+        out_delta[s] = delta;
+    }
+    free(f);
+    return 0;
+}
+
+/* Lees-Edwards LJ forces of a configuration at offset delta (all pairs). */
+double or_lj_le_forces(int n, const double *pos, const int32_t *type, const double *L, double delta, int nt,
+                       const double *sig2, const double *eps4, double rc, int shift, double *f, double *w) {
+    return lj_le_forces(n, pos, type, L, delta, nt, sig2, eps4, rc, shift, f, w);
+}

@@ -22,7 +22,7 @@ E_VDW, E_REAL, E_LONG, E_CORRECT, E_MOLCORRECT, E_SURF = 0, 1, 2, 3, 4, 5
 E_POL_REAL, E_POL_LONG, E_POL_SELF, E_POL_INTRA, E_COUNT = 6, 7, 8, 9, 12
 VDW_NONE, VDW_LJ, VDW_MIE, VDW_BMH, VDW_BUFF = 0, 1, 2, 3, 4
 GUESS_DIRECT, GUESS_PREVIOUS, GUESS_LEARNED = 0, 1, 2
-THERMO_NONE, THERMO_NOSE_HOOVER = 0, 1
+THERMO_NONE, THERMO_NOSE_HOOVER, THERMO_NH_CHAIN = 0, 1, 2
 
 
 class SmdError(RuntimeError):
@@ -48,7 +48,8 @@ class Observables(ctypes.Structure):
                 ("zeta", ctypes.c_double), ("virial", ctypes.c_double * 9),
                 ("atom_pressure", ctypes.c_double * 9), ("mol_pressure", ctypes.c_double * 9),
                 ("volume", ctypes.c_double), ("pairs_in_cutoff", ctypes.c_int64),
-                ("status", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+                ("status", ctypes.c_uint32), ("pad", ctypes.c_uint32),
+                ("shear_offset", ctypes.c_double)]
 
 
 _P = ctypes.c_void_p

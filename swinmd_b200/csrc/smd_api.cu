@@ -153,6 +153,17 @@ void enqueue_forces(Ctx &c) {
 // (or smd_integrator_start / smd_upload_positions) has already written the
 // box fractions the pair kernel reads.
 void enqueue_step(Ctx &c) {
+    if (c.ip.thermostat == SMD_THERMO_NH_CHAIN) {
+        // velocity Verlet: chain, kick and drift first, then the list test,
+        // forces at t + dt, the second kick and chain
+        launch_nhc_first(c);
+        launch_nlist(c, false);
+        c.fixq_from_integrate = 1;
+        enqueue_forces(c);
+        c.fixq_from_integrate = 0;
+        launch_nhc_second(c);
+        return;
+    }
     launch_nlist(c, false);
     c.fixq_from_integrate = 1;
     enqueue_forces(c);
@@ -180,14 +191,14 @@ int smd_create(int device, smd_ctx **out) {
         delete x;
         return SMD_ERR_CUDA;
     }
-    if (dalloc(&c.acc, ACC_COUNT) != cudaSuccess || dalloc(&c.scal, 8) != cudaSuccess ||
+    if (dalloc(&c.acc, ACC_COUNT) != cudaSuccess || dalloc(&c.scal, SC_NSCAL) != cudaSuccess ||
         dalloc(&c.ticket, 1) != cudaSuccess || dalloc(&c.status, 1) != cudaSuccess ||
         dalloc(&c.flags, 4) != cudaSuccess || dalloc(&c.obs, 1) != cudaSuccess) {
         delete x;
         return SMD_ERR_CUDA;
     }
     cudaMemset(c.acc, 0, ACC_COUNT * sizeof(long long));
-    cudaMemset(c.scal, 0, 8 * sizeof(double));
+    cudaMemset(c.scal, 0, SC_NSCAL * sizeof(double));
     cudaMemset(c.ticket, 0, sizeof(unsigned));
     cudaMemset(c.status, 0, sizeof(unsigned));
     cudaMemset(c.flags, 0, 4 * sizeof(int));
@@ -834,8 +845,21 @@ int smd_set_integrator(smd_ctx *x, const smd_integrator_params *p) {
         return fail(x, SMD_ERR_ARG, "smd_set_integrator: SHAKE tolerance and maxCount must be > 0");
     if (p->long_steps > 1)
         return fail(x, SMD_ERR_ARG, "smd_set_integrator: long_steps > 1 not supported");
+    if (p->thermostat < SMD_THERMO_NONE || p->thermostat > SMD_THERMO_NH_CHAIN)
+        return fail(x, SMD_ERR_ARG, "smd_set_integrator: unknown thermostat");
+    if (p->thermostat == SMD_THERMO_NH_CHAIN && (p->constraint != 0 || !(p->coupl_const > 0)))
+        return fail(x, SMD_ERR_ARG, "smd_set_integrator: the chain integrator needs tau > 0 and no constraints");
+    if (p->strain_rate != 0.0) {
+        if (p->thermostat != SMD_THERMO_NH_CHAIN)
+            return fail(x, SMD_ERR_ARG, "smd_set_integrator: SLLOD shear runs with the chain integrator");
+        if (x->c.ewald_on || x->c.mp_on || x->c.vdw == VDW_BUFF)
+            return fail(x, SMD_ERR_ARG,
+                        "smd_set_integrator: SLLOD shear supports the LJ / Mie / BMH pair terms only");
+    }
     Ctx &c = x->c;
     c.ip = *p;
+    // the sheared cell search moves a 4-cell x window across the y boundary
+    if (p->strain_rate != 0.0 && c.grid.use_cells && c.grid.n[0] < 4) c.grid.use_cells = 0;
     if (c.ip.atom_ndf <= 0) c.ip.atom_ndf = 3 * c.n - 3;
     if (c.ip.mol_ndf <= 0) c.ip.mol_ndf = 3 * c.nmol - 3;
     c.integrator_ready = 1;
@@ -869,8 +893,16 @@ int smd_integrator_start(smd_ctx *x) {
     launch_nlist(c, true);
     c.list_valid = 1;
     CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
-    enqueue_forces(c);
-    launch_start_velocities(c);
+    if (c.ip.thermostat == SMD_THERMO_NH_CHAIN) {
+        launch_nhc_start(c);   // delta = 0 before the first list and forces
+        launch_nlist(c, true);
+        CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
+        enqueue_forces(c);
+        CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
+    } else {
+        enqueue_forces(c);
+        launch_start_velocities(c);
+    }
     c.steps_done = 0;
     return sync_status(x);
 }

@@ -63,6 +63,18 @@ enum StatusBits {
     ST_SHAKE_GEOM = 64       // SHAKE geometric failure (reference LFIntegrator.cpp:1758)
 };
 
+// integrator scalars shared by several files (ctx->scal): 0-7 belong to the
+// leap-frog integrator (smd_integrate.cu)
+enum ScalShared {
+    SC_VNH = 8,      // 4: chain thermostat velocities
+    SC_EKIN = 12,    // kinetic energy of the current velocities (chain input)
+    SC_SCALE = 13,   // last chain velocity scale
+    SC_LE = 14,      // Lees-Edwards offset delta (nm), in [0, Lx)
+    SC_LE_B = 15,    // delta at the last pair-list build
+    SC_DRMAX = 16,   // displacement^2 limit of the current step's list test
+    SC_NSCAL = 32
+};
+
 struct Box {
     double L[3];      // edges (nm)
     double half[3];   // L/2
@@ -78,6 +90,35 @@ __device__ __forceinline__ double pbc1(double d, double L, double h) {
     for (int k = 0; k < 8 && d >= h; k++) d -= L;
     for (int k = 0; k < 8 && d < -h; k++) d += L;
     return d;
+}
+
+// Lees-Edwards minimum image (sliding images under planar Couette shear):
+// the image one box up in y sits delta further in x, so y is reduced first,
+// moving x by -/+ delta per crossing, then x and z as pbc1.
+__device__ __forceinline__ void min_image_le(double &dx, double &dy, double &dz, const Box &b, double delta) {
+    for (int k = 0; k < 8 && dy >= b.half[1]; k++) { dy -= b.L[1]; dx -= delta; }
+    for (int k = 0; k < 8 && dy < -b.half[1]; k++) { dy += b.L[1]; dx += delta; }
+    dx = pbc1(dx, b.L[0], b.half[0]);
+    dz = pbc1(dz, b.L[2], b.half[2]);
+}
+
+// The same on 32-bit box fractions: the y difference's wrap count w (from
+// the 64-bit difference) takes w Lees-Edwards offsets (as a fraction of Lx,
+// modulo 2^32) off the x difference.  frac32 measures y from 0, the box
+// from -Ly/2: flipping the top bit measures both from the box edge, so the
+// 64-bit difference is the true y difference in units of Ly / 2^32.
+__device__ __forceinline__ int le_dx_frac(int fxi, int fyi, int fxj, int fyj, unsigned dfrac) {
+    const long long dy64 = (long long)((unsigned)fyj ^ 0x80000000u) - (long long)((unsigned)fyi ^ 0x80000000u);
+    const int iy = (int)(unsigned)(dy64 & 0xffffffffLL);
+    const long long w = (dy64 - iy) >> 32;
+    return (int)((unsigned)fxj - (unsigned)fxi - (unsigned)(w * (long long)dfrac));
+}
+
+// Lees-Edwards offset as a fraction of the box edge, modulo 2^32
+__device__ __forceinline__ unsigned le_frac(double delta, double invL) {
+    double f = delta * invL;
+    f -= floor(f);
+    return (unsigned)(__double2ll_rn(f * 4294967296.0) & 0xffffffffLL);
 }
 
 // Box fraction of a coordinate as an unsigned 32-bit fixed-point number;

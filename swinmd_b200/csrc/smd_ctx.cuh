@@ -157,6 +157,9 @@ void launch_pair(Ctx &c);
 void launch_recip(Ctx &c);
 void launch_integrate(Ctx &c);
 void launch_start_velocities(Ctx &c);
+void launch_nhc_first(Ctx &c);
+void launch_nhc_second(Ctx &c);
+void launch_nhc_start(Ctx &c);
 void launch_finalize_forces(Ctx &c, double *f_out_dev);
 void launch_intra(Ctx &c);
 // polarisable model: term groups (each maps its own torques to forces)

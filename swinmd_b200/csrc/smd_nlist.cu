@@ -126,14 +126,17 @@ struct BuildArgs {
     int *nbr, *nnbr;
     unsigned int *status;
     const int *flags;
+    const double *le;   // Lees-Edwards offset on the device, or null
 };
 
 // r^2 of the reference's pair test, without contraction into FMA
 // (x86-64 -O2 builds of the reference use separate multiply and add).
 __device__ __forceinline__ double ref_r2(const double4 &a, const double4 &b, const Box &bx,
-                                         bool pbc) {
+                                         bool pbc, bool le, double delta) {
     double dx = __dsub_rn(b.x, a.x), dy = __dsub_rn(b.y, a.y), dz = __dsub_rn(b.z, a.z);
-    if (pbc) {
+    if (le) {
+        min_image_le(dx, dy, dz, bx, delta);
+    } else if (pbc) {
         dx = pbc1(dx, bx.L[0], bx.half[0]);
         dy = pbc1(dy, bx.L[1], bx.half[1]);
         dz = pbc1(dz, bx.L[2], bx.half[2]);
@@ -151,6 +154,8 @@ __global__ void k_build(BuildArgs a) {
     const double4 pi = a.pos4[i];
     const int mi = a.mol[i];
     const int e0 = a.excl_off[i], e1 = a.excl_off[i + 1];
+    const bool le = a.le != nullptr;
+    const double delta = le ? *a.le : 0.0;
     int count = 0;
     auto consider = [&](int j, bool pbc, bool valid) {
         bool take = valid && j != i;
@@ -158,7 +163,7 @@ __global__ void k_build(BuildArgs a) {
             for (int e = e0; e < e1; e++)
                 if (a.excl[e] == j) { take = false; break; }
         }
-        if (take) take = ref_r2(pi, a.pos4[j], a.box, pbc) < a.rl2;
+        if (take) take = ref_r2(pi, a.pos4[j], a.box, pbc, le && pbc, delta) < a.rl2;
         unsigned m = __ballot_sync(0xffffffffu, take);
         if (take) {
             int slot = count + __popc(m & ((1u << lane) - 1));
@@ -173,9 +178,19 @@ __global__ void k_build(BuildArgs a) {
         for (int dz = -1; dz <= 1; dz++) {
             int z = cz + dz; z = z < 0 ? z + a.g.n[2] : (z >= a.g.n[2] ? z - a.g.n[2] : z);
             for (int dy = -1; dy <= 1; dy++) {
-                int y = cy + dy; y = y < 0 ? y + a.g.n[1] : (y >= a.g.n[1] ? y - a.g.n[1] : y);
-                for (int dx = -1; dx <= 1; dx++) {
-                    int x = cx + dx; x = x < 0 ? x + a.g.n[0] : (x >= a.g.n[0] ? x - a.g.n[0] : x);
+                int y = cy + dy;
+                // under shear, the images across the y boundary sit delta
+                // further in x: the x window moves by delta and widens by a cell
+                const int wy = y < 0 ? -1 : (y >= a.g.n[1] ? 1 : 0);
+                y = y < 0 ? y + a.g.n[1] : (y >= a.g.n[1] ? y - a.g.n[1] : y);
+                int sh = 0, dx1 = 1;
+                if (le && wy != 0) {
+                    sh = (int)floor((wy < 0 ? delta : -delta) * a.g.rlen[0]);
+                    dx1 = 2;
+                }
+                for (int dx = -1; dx <= dx1; dx++) {
+                    int x = (cx + sh + dx) % a.g.n[0];
+                    x = x < 0 ? x + a.g.n[0] : x;
                     int nc = (z * a.g.n[1] + y) * a.g.n[0] + x;
                     // same-cell pairs are tested without minimum image, as the
                     // reference does (CellManager.cpp:246-262)
@@ -203,10 +218,12 @@ __global__ void k_build(BuildArgs a) {
     }
 }
 
-__global__ void k_list_done(int *flags) {
+__global__ void k_list_done(int *flags, double *scal_le) {
     if (flags[0]) {
         flags[1] += 1;
         flags[0] = 0;
+        // the Lees-Edwards offset this list was built for
+        if (scal_le) scal_le[SC_LE_B - SC_LE] = scal_le[0];
     }
 }
 
@@ -236,9 +253,10 @@ void launch_nlist(Ctx &c, bool force_rebuild) {
     a.excl_off = c.excl_off; a.excl = c.excl; a.cell_of = c.pl.cell_of;
     a.cell_start = c.pl.cell_start; a.cell_atoms = c.pl.cell_atoms; a.g = c.grid; a.box = c.box;
     a.rl2 = c.pl.rl2; a.nbr = c.pl.nbr; a.nnbr = c.pl.nnbr; a.status = c.status; a.flags = c.flags;
+    a.le = c.ip.strain_rate != 0.0 && c.integrator_ready ? c.scal + SC_LE : nullptr;
     int nbw = (c.n * 32 + T - 1) / T;
     k_build<<<nbw, T, 0, c.stream>>>(a);
-    k_list_done<<<1, 1, 0, c.stream>>>(c.flags);
+    k_list_done<<<1, 1, 0, c.stream>>>(c.flags, a.le ? c.scal + SC_LE : nullptr);
 }
 
 }  // namespace smd

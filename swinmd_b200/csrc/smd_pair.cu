@@ -48,6 +48,7 @@ struct PairArgs {
     double bn, bm, bdelta, bgamma, bc[6], bsw2;
     float bswf, bwinv;  // taper start and 1/(cutoff - start), FP32 path
     int buff_int;       // n - m and m are small positive integers
+    const double *le;   // Lees-Edwards offset on the device (planar shear), or null
     long long *frc;
     long long *acc;
 };
@@ -318,6 +319,8 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_pair(PairArgs a) {
     const int gt = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = gt / TPP;
     const int t = gt % TPP;
+    const double le_d = a.le ? *a.le : 0.0;
+    const unsigned le_f = a.le ? le_frac(le_d, a.box.inv[0]) : 0u;
     double fx = 0, fy = 0, fz = 0;
     R evdw = 0, ereal = 0;
     int npair = 0;
@@ -344,14 +347,21 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_pair(PairArgs a) {
             int tj;
             if (sizeof(R) == 8) {
                 const double4 pj = a.pos4[j];
-                dx = pbc1(pj.x - pi64.x, a.box.L[0], a.box.half[0]);
-                dy = pbc1(pj.y - pi64.y, a.box.L[1], a.box.half[1]);
-                dz = pbc1(pj.z - pi64.z, a.box.L[2], a.box.half[2]);
+                if (a.le) {
+                    double ex = pj.x - pi64.x, ey = pj.y - pi64.y, ez = pj.z - pi64.z;
+                    min_image_le(ex, ey, ez, a.box, le_d);
+                    dx = ex; dy = ey; dz = ez;
+                } else {
+                    dx = pbc1(pj.x - pi64.x, a.box.L[0], a.box.half[0]);
+                    dy = pbc1(pj.y - pi64.y, a.box.L[1], a.box.half[1]);
+                    dz = pbc1(pj.z - pi64.z, a.box.L[2], a.box.half[2]);
+                }
                 r2 = dx * dx + dy * dy + dz * dz;
                 tj = (int)pj.w;
             } else {
                 const int4 pj = a.fixq[j];
-                const int ix = pj.x - pif.x, iy = pj.y - pif.y, iz = pj.z - pif.z;
+                const int ix = a.le ? le_dx_frac(pif.x, pif.y, pj.x, pj.y, le_f) : pj.x - pif.x;
+                const int iy = pj.y - pif.y, iz = pj.z - pif.z;
                 dx = R(ix) * R(a.dscale[0]);
                 dy = R(iy) * R(a.dscale[1]);
                 dz = R(iz) * R(a.dscale[2]);
@@ -550,6 +560,7 @@ void launch_pair(Ctx &c) {
     a.alpha2pi = 2.0 * c.ew_alpha / 1.7724538509055160273;
     a.ew_rc2 = c.ew_rc2;
     a.frc = c.frc; a.acc = c.acc;
+    a.le = c.ip.strain_rate != 0.0 && c.integrator_ready ? c.scal + SC_LE : nullptr;
     a.bn = c.buff_n; a.bm = c.buff_m; a.bdelta = c.buff_delta; a.bgamma = c.buff_gamma;
     for (int q = 0; q < 6; q++) a.bc[q] = c.buff_c[q];
     a.bsw2 = c.buff_sw * c.buff_sw;

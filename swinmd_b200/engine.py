@@ -473,6 +473,8 @@ class LFIntegrator:
     """``LFIntegrator`` (src/integrators/LFIntegrator.cpp): ``start()`` is
     LFIntegrator::start (F(0), vtMinus), ``run(n)`` advances n steps."""
 
+    thermostat_kind = None   # set by subclasses; None: from the configuration
+
     def __init__(self, ensemble: GpuEnsemble, series_capacity: int = 0):
         self.ens = ensemble
         s, c = ensemble.system, ensemble.system.config
@@ -481,6 +483,8 @@ class LFIntegrator:
         p.temperature = c.temperature
         p.coupl_const = c.coupl_const
         p.thermostat = L.THERMO_NOSE_HOOVER if c.thermostat == "NoseHoover" else L.THERMO_NONE
+        if self.thermostat_kind is not None:
+            p.thermostat = self.thermostat_kind
         p.atom_thermo = int(c.atom_thermo)
         p.constraint = int(c.constraint)
         p.long_steps = int(c.long_steps)
@@ -519,6 +523,16 @@ class LFIntegrator:
         L.check(self.ens.ctx, self.ens.lib.smd_get_series(self.ens.ctx, L.dptr(out),
                                                           self.series_capacity, ctypes.byref(cnt)))
         return out[:5 * cnt.value].reshape(-1, 5)
+
+
+class NHIntegrator(LFIntegrator):
+    """Velocity-Verlet integrator with the 4-link Nose-Hoover chain of
+    ``NHIntegrator::chain`` (src/integrators/NHIntegrator.cpp:1814-1912) at
+    constant volume, and SLLOD planar Couette shear with Lees-Edwards images
+    when the configuration asks for it (testMode 2, ``rate``).  ``start()``
+    computes F(0) and the chain's starting kinetic energy."""
+
+    thermostat_kind = L.THERMO_NH_CHAIN
 
 
 class BuffvdWForce(GpuForce):
