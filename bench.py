@@ -145,6 +145,8 @@ def cpu_reference(s, steps, timeout=1800):
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
+    if args.workload == "replicas64":
+        return run_reference_replicas(args, world)
     s, desc = workload(args.workload)
     steps = max(1, min(args.steps, 2 if args.workload == "polwater4096" else 2000))
     sps = cpu_reference(s, steps, timeout=3600)
@@ -161,6 +163,168 @@ def run_reference_arm(args, rank, world):
                                    "LFIntegrator::start; SwinMD's own LFIntegrator::run, one "
                                    "process, one core (the image has no MPI)"},
         "e2e": {"value": v, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def run_reference_replicas(args, world):
+    """The reference on the replica workload: one SwinMD process per host core
+    (the reference is single-threaded and runs replicas as separate runs),
+    each a bounded number of steps of one replica at zero shear (it has no
+    SLLOD); the aggregate is the sum of the concurrent processes' ns/day."""
+    import refdump
+    from concurrent.futures import ThreadPoolExecutor
+    from swinmd_b200 import systems
+    if not os.path.exists(refdump.REF_DUMP):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_dump is not built"}))
+        return
+    reps = systems.replica_set(count=64, seed=1)
+    cores = max(1, min(64, os.cpu_count() or 1))
+    steps = max(1, min(args.steps, 50))
+
+    def one(s):
+        s.config.rate = 0.0
+        s.config.test_mode = 0
+        with tempfile.TemporaryDirectory() as d:
+            systems.write_reference_case(s, d)
+            r = refdump.run_ref(d, "run", steps, out="run.txt", timeout=1800)
+        return float(r["run_seconds"][0]) / steps
+
+    with ThreadPoolExecutor(cores) as ex:
+        sps = list(ex.map(one, reps[:cores]))
+    dt = reps[0].config.timestep
+    v = sum(ns_per_day(x, dt) for x in sps)
+    print(json.dumps({
+        "metric": "aggregate ns/day of 64 batched LJ replicas (uneven sizes, per-replica shear and "
+                  "Nose-Hoover chain)",
+        "value": v, "unit": "ns/day", "impl": "reference", "n_gpus": world, "steps": steps, "warmup": 0,
+        "ms_per_step": float(np.mean(sps)) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": {"workload": "replicas64"},
+        "cpu_baseline": {"value": v, "unit": "ns/day", "cores": cores, "kind": "reference",
+                         "sample": f"{cores} concurrent SwinMD processes (one per core), {steps} steps "
+                                   "each of the first replicas at zero shear, LFIntegrator::run"},
+        "e2e": {"value": v, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def run_replicas(args, rank, world, local):
+    """64 independent LJ replicas (sizes log-uniform 500-8000 atoms, strain
+    rates uniform 0-0.2 reduced, own Nose-Hoover chains) in one graph per
+    step; aggregate ns/day over all replicas and ranks."""
+    import torch
+    from swinmd_b200 import engine, systems
+    torch.cuda.set_device(local)
+    reps = systems.replica_set(count=64, seed=1 + rank)
+    ens, integ = [], []
+    for s in reps:
+        e = engine.GpuEnsemble(s, precision="mixed", device=local)
+        nh = engine.NHIntegrator(e)
+        nh.start()
+        ens.append(e)
+        integ.append(nh)
+    batch = engine.ReplicaBatch(ens)
+    tpp = batch.autotune(reps=10)
+    batch.run(args.warmup)
+    l2 = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    total, done = 0.0, 0
+    while done < args.steps:
+        k = min(args.chunk, args.steps - done)
+        l2.add_(1.0)
+        torch.cuda.synchronize()
+        total += batch.run(k)
+        done += k
+    clocks = clk.stop()
+    t = torch.tensor([total], dtype=torch.float64)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t[0]) / args.steps
+    dt = reps[0].config.timestep
+    value = ns_per_day(ms * 1e-3, dt) * len(reps) * world
+    # per-replica force error of the mixed path against FP64
+    errs = []
+    for e in ens:
+        f32, _, _ = e.compute_forces()
+        e.set_precision("fp64")
+        f64, _, _ = e.compute_forces()
+        e.set_precision("mixed")
+        errs.append(float(np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum())))
+    # end to end: host buffers in and out around every block of steps
+    every = args.e2e_every
+    hb = []
+    for e in ens:
+        st = e.state()
+        p = torch.empty(st["pos"].size, dtype=torch.float64).pin_memory().numpy()
+        v = torch.empty(st["vel"].size, dtype=torch.float64).pin_memory().numpy()
+        p[:] = st["pos"].reshape(-1)
+        v[:] = st["vel"].reshape(-1)
+        hb.append((p, v))
+    e2e_steps = max(every, (min(args.steps, 100) // every) * every)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps // every):
+        for e, (p, v) in zip(ens, hb):
+            e.upload_positions(p)
+            e.upload_velocities(v)
+        batch.run(every)
+        for e, (p, v) in zip(ens, hb):
+            st = e.state()
+            p[:] = st["pos"].reshape(-1)
+            v[:] = st["vel"].reshape(-1)
+    torch.cuda.synchronize()
+    te = torch.tensor([(time.perf_counter() - t0) * 1e3], dtype=torch.float64)
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e = ns_per_day(float(te[0]) / e2e_steps * 1e-3, dt) * len(reps) * world
+    import ctypes
+    launches = 0
+    for e in ens:
+        kc = ctypes.c_int()
+        L_ = __import__("swinmd_b200._lib", fromlist=["_lib"])
+        L_.check(e.ctx, e.lib.smd_step_kernel_count(e.ctx, ctypes.byref(kc)))
+        launches += kc.value
+    natoms = sum(s.n_atoms for s in reps)
+    pairs = sum(int(integ[r].observables().pairs_in_cutoff) for r in range(len(reps)))
+    # FP32 rate of the whole step over the LJ pair work (23 flop per pair in
+    # each direction of the full list): a lower bound for the pair kernel
+    achieved = pairs * 2 * 23 / (ms * 1e-3) / 1e12
+    peak = 148 * 128 * 2 * 1.965e9 / 1e12
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        sample = systems.lj_fluid(ncell=8, seed=5, n_steps=50)
+        sample.config.long_correct = True
+        sps = cpu_reference(sample, 50)
+        if sps:
+            cpu = {"value": ns_per_day(sps, dt), "unit": "ns/day", "cores": 1, "kind": "reference",
+                   "sample": "50 steps of one 2048-atom replica at zero shear with SwinMD's own "
+                             "LFIntegrator::run (the reference has no SLLOD), one process, one core; "
+                             "64 such processes on 64 cores would give 64x this"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "aggregate ns/day of 64 batched LJ replicas (uneven sizes, per-replica shear and "
+                      "Nose-Hoover chain)",
+            "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 pair math on exact fractions, f64 integrator",
+            "data": "synthetic (seeded FCC lattices, Maxwell-Boltzmann velocities)",
+            "config": {"workload": f"replicas64: 64 LJ fluids, {natoms} atoms in total, sizes log-uniform "
+                                   "500-8000 atoms (FCC 4 ncell^3), rho*=0.8442, T*=0.722, rc=2.5 sigma, "
+                                   "strain rates uniform 0-0.2 (SLLOD, Lees-Edwards), NH chain tau*=0.5, "
+                                   "dt*=0.005; one CUDA graph per step over all replicas",
+                       "replicas": len(reps) * world, "l2": "256 MB buffer written before every chunk",
+                       "parallelism": "replicas only"},
+            "autotuned_threads_per_site": [int(x) for x in tpp],
+            "force_rms_rel_err_vs_fp64": {"max": max(errs), "median": float(np.median(errs))},
+            "e2e": {"value": e2e, "unit": "ns/day", "h2d_bytes_per_step": natoms * 6 * 8 / every,
+                    "d2h_bytes_per_step": natoms * 9 * 8 / every},
+            "gpu_launches": launches * args.steps,
+            "roofline": {"bound": "fp32", "kernel": "k_pair (LJ) over the whole step", "achieved": achieved,
+                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "peak_source": "nominal FP32 SIMT rate at the measured max SM clock"},
+            "clocks": clocks, "cpu_baseline": cpu}))
+    batch.close()
 
 
 def timed_steps(lf, l2, steps, chunk):
@@ -204,6 +368,11 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        if dist:
+            dist.destroy_process_group()
+        return
+    if args.workload == "replicas64":
+        run_replicas(args, rank, world, local)
         if dist:
             dist.destroy_process_group()
         return

@@ -271,6 +271,28 @@ int smd_run_timed(smd_ctx *ctx, int nsteps, double *device_ms);
  * step's CUDA graph). */
 int smd_step_kernel_count(smd_ctx *ctx, int *count);
 
+/* ---- batched replicas ---------------------------------------------------- */
+/* Many independent systems (replicas of uneven size, each with its own
+ * seed, strain rate and thermostat chain) advanced together: one CUDA graph
+ * per step whose branches are the replicas' steps, each on its replica's
+ * stream, so one launch runs them all concurrently on the device.  The
+ * reference runs such replicas as separate processes (one Simulation per
+ * run, src/NEMDMain.cpp); there is no reference interface for the batch
+ * itself.  The contexts must be on one device with their integrators set
+ * and started; they stay owned by the caller and must outlive the batch,
+ * and must not be reconfigured while it exists. */
+typedef struct smd_batch smd_batch;
+int smd_batch_create(smd_ctx *const *ctxs, int count, smd_batch **out);
+void smd_batch_destroy(smd_batch *batch);
+const char *smd_batch_last_error(const smd_batch *batch);
+/* Autotuner: for each replica, times its pair kernel `reps` times at every
+ * threads-per-site shape (1, 2, ..., 32), keeps the fastest (tpp_out[r], may
+ * be null) and recomputes the replica's forces. */
+int smd_batch_autotune(smd_batch *batch, int reps, int32_t *tpp_out);
+/* nsteps steps of every replica; *device_ms (may be null) gets the device
+ * time of the graph launches (CUDA events on the batch stream). */
+int smd_batch_run(smd_batch *batch, int nsteps, double *device_ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -60,6 +60,11 @@ _F = ctypes.POINTER(ctypes.c_float)
 # name: (restype, argtypes)
 SIGNATURES = {
     "smd_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P)]),
+    "smd_batch_create": (ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int, ctypes.POINTER(_P)]),
+    "smd_batch_destroy": (None, [_P]),
+    "smd_batch_last_error": (ctypes.c_char_p, [_P]),
+    "smd_batch_autotune": (ctypes.c_int, [_P, ctypes.c_int, _I]),
+    "smd_batch_run": (ctypes.c_int, [_P, ctypes.c_int, _D]),
     "smd_destroy": (None, [_P]),
     "smd_last_error": (ctypes.c_char_p, [_P]),
     "smd_set_topology": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _I, _I, _D, _D]),

@@ -1097,4 +1097,171 @@ int smd_get_series(smd_ctx *x, double *out, int cap, int *count) {
     return SMD_OK;
 }
 
+
+/* ---- batched replicas --------------------------------------------------- */
+}  // extern "C"
+
+struct smd_batch {
+    int device = 0;
+    std::vector<smd_ctx *> reps;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    int dirty = 1;
+    std::string err;
+};
+
+namespace {
+int bfail(smd_batch *b, int code, const std::string &msg) {
+    if (b) b->err = msg;
+    return code;
+}
+#define BCK(call)                                                                              \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return bfail(b, SMD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// every replica's step as one branch of one graph: fork from the batch
+// stream, each replica's kernels on its own stream, join back
+int batch_build(smd_batch *b) {
+    if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+    cudaGraph_t g;
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    cudaEventRecord(b->fork, b->stream);
+    for (size_t r = 0; r < b->reps.size(); r++) {
+        Ctx &c = b->reps[r]->c;
+        cudaStreamWaitEvent(c.stream, b->fork, 0);
+        enqueue_step(c);
+        cudaEventRecord(b->join[r], c.stream);
+        cudaStreamWaitEvent(b->stream, b->join[r], 0);
+    }
+    BCK(cudaStreamEndCapture(b->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    BCK(e);
+    b->dirty = 0;
+    return SMD_OK;
+}
+
+int batch_status(smd_batch *b) {
+    BCK(cudaStreamSynchronize(b->stream));
+    for (size_t r = 0; r < b->reps.size(); r++) {
+        const int rc = sync_status(b->reps[r]);
+        if (rc) return bfail(b, rc, "replica " + std::to_string(r) + ": " + b->reps[r]->c.err);
+    }
+    return SMD_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int smd_batch_create(smd_ctx *const *ctxs, int count, smd_batch **out) {
+    if (!out || !ctxs || count <= 0) return SMD_ERR_ARG;
+    *out = nullptr;
+    smd_batch *b = new (std::nothrow) smd_batch();
+    if (!b) return SMD_ERR_ARG;
+    b->device = ctxs[0] ? ctxs[0]->c.device : 0;
+    for (int r = 0; r < count; r++) {
+        if (!ctxs[r] || !ctxs[r]->c.integrator_ready || ctxs[r]->c.device != b->device) {
+            delete b;
+            return SMD_ERR_ARG;
+        }
+        b->reps.push_back(ctxs[r]);
+    }
+    if (cudaSetDevice(b->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) {
+        delete b;
+        return SMD_ERR_CUDA;
+    }
+    b->join.assign(count, nullptr);
+    for (int r = 0; r < count; r++)
+        if (cudaEventCreateWithFlags(&b->join[r], cudaEventDisableTiming) != cudaSuccess) {
+            smd_batch_destroy(b);
+            return SMD_ERR_CUDA;
+        }
+    *out = b;
+    return SMD_OK;
+}
+
+void smd_batch_destroy(smd_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (cudaEvent_t e : b->join)
+        if (e) cudaEventDestroy(e);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+const char *smd_batch_last_error(const smd_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+int smd_batch_autotune(smd_batch *b, int reps, int32_t *tpp_out) {
+    if (!b || reps <= 0) return SMD_ERR_ARG;
+    BCK(cudaSetDevice(b->device));
+    cudaEvent_t e0, e1;
+    BCK(cudaEventCreate(&e0));
+    BCK(cudaEventCreate(&e1));
+    const int cand[6] = {1, 2, 4, 8, 16, 32};
+    for (size_t r = 0; r < b->reps.size(); r++) {
+        Ctx &c = b->reps[r]->c;
+        float best = 1e30f;
+        int best_t = c.tpp;
+        for (int q = 0; q < 6; q++) {
+            c.tpp = cand[q];
+            launch_pair(c);   // warm
+            cudaEventRecord(e0, c.stream);
+            for (int k = 0; k < reps; k++) launch_pair(c);
+            cudaEventRecord(e1, c.stream);
+            BCK(cudaEventSynchronize(e1));
+            float ms = 0;
+            BCK(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best) { best = ms; best_t = cand[q]; }
+        }
+        c.tpp = best_t;
+        c.graph_dirty = 1;
+        if (tpp_out) tpp_out[r] = best_t;
+        // the step expects the full forces of the current positions
+        BCK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
+        enqueue_forces(c);
+        BCK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->dirty = 1;
+    return batch_status(b);
+}
+
+int smd_batch_run(smd_batch *b, int nsteps, double *device_ms) {
+    if (!b || nsteps < 0) return SMD_ERR_ARG;
+    BCK(cudaSetDevice(b->device));
+    if (b->dirty || !b->graph) {
+        const int r = batch_build(b);
+        if (r) return r;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (device_ms) {
+        BCK(cudaEventCreate(&e0));
+        BCK(cudaEventCreate(&e1));
+        BCK(cudaStreamSynchronize(b->stream));
+        BCK(cudaEventRecord(e0, b->stream));
+    }
+    for (int s = 0; s < nsteps; s++) BCK(cudaGraphLaunch(b->graph, b->stream));
+    if (device_ms) {
+        BCK(cudaEventRecord(e1, b->stream));
+        BCK(cudaEventSynchronize(e1));
+        float ms = 0;
+        BCK(cudaEventElapsedTime(&ms, e0, e1));
+        *device_ms = ms;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    for (smd_ctx *x : b->reps) x->c.steps_done += nsteps;
+    return batch_status(b);
+}
+
 }  // extern "C"

@@ -563,3 +563,45 @@ class Induction(GpuForce):
         f, e, w = self.ens.compute_forces(L.TERM_IND_LONG)
         self.long_force, self.long_energy, self.long_virial = f, float(e[L.E_POL_LONG]), w
         return f
+
+
+class ReplicaBatch:
+    """Independent replicas (``GpuEnsemble`` objects with their integrators
+    started) advanced by one CUDA graph per step (``smd_batch_*``)."""
+
+    def __init__(self, ensembles):
+        self.lib = L.load()
+        self.ensembles = list(ensembles)
+        arr = (ctypes.c_void_p * len(self.ensembles))(*[e.ctx for e in self.ensembles])
+        b = ctypes.c_void_p()
+        code = self.lib.smd_batch_create(arr, len(self.ensembles), ctypes.byref(b))
+        if code != L.SMD_OK:
+            raise L.SmdError(code, "smd_batch_create failed")
+        self.b = b
+
+    def _chk(self, code):
+        if code != L.SMD_OK:
+            raise L.SmdError(code, (self.lib.smd_batch_last_error(self.b) or b"").decode())
+
+    def autotune(self, reps: int = 20) -> np.ndarray:
+        """Threads per site chosen for each replica's pair kernel."""
+        out = np.zeros(len(self.ensembles), np.int32)
+        self._chk(self.lib.smd_batch_autotune(self.b, int(reps), L.iptr(out)))
+        return out
+
+    def run(self, nsteps: int) -> float:
+        """Advances every replica by nsteps; returns the device time (ms)."""
+        ms = ctypes.c_double()
+        self._chk(self.lib.smd_batch_run(self.b, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if self.b:
+            self.lib.smd_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

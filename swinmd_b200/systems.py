@@ -510,3 +510,21 @@ def constraint_lengths(s: System) -> np.ndarray:
     out[:, 1] = l2 * l2
     out[:, 2] = l3 * l3
     return out
+
+
+def replica_set(count: int = 64, n_min: int = 500, n_max: int = 8000, rate_max_star: float = 0.2,
+                seed: int = 1, n_steps: int = 5000) -> list:
+    """Independent Lennard-Jones fluids for batched runs: sizes log-uniform
+    in [n_min, n_max] atoms (rounded to the nearest FCC 4 ncell^3, ncell >= 5),
+    strain rates uniform in [0, rate_max_star] (reduced units), one seed each."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for r in range(count):
+        n = math.exp(rng.uniform(math.log(n_min), math.log(n_max)))
+        ncell = max(5, int(round((n / 4.0) ** (1.0 / 3.0))))
+        rate = float(rng.uniform(0.0, rate_max_star))
+        s = lj_fluid(ncell=ncell, seed=seed * 1000 + r, jitter_star=0.02, n_steps=n_steps,
+                     strain_rate_star=rate)
+        s.config.long_correct = False
+        out.append(s)
+    return out
