@@ -187,16 +187,19 @@ int smd_get_polarization(smd_ctx *ctx, double *mu, double *quad, double *e0, dou
 int smd_set_induced(smd_ctx *ctx, const double *p);
 
 /* ---- learned initial guess of the induced dipoles (no reference code) ----
- * A per-site network (20 rotation-invariant inputs from the permanent field
- * and the neighbour distances, 2 hidden layers of 64, tanh) predicts
- * p - alpha E0 in the site's own axes; the dipole solve then iterates from
- * that guess to the same tolerance.  Training rows are the solver's own
- * converged dipoles. */
+ * The guess is the previous step's converged dipoles moved by the linear
+ * response alpha (E0(t) - E0(t-1)) to the change of the permanent field
+ * (each time step stores its dipoles and field; smd_integrator_start clears
+ * the store), plus a correction from a per-site network (20 rotation-
+ * invariant inputs in the site's own axes: the permanent fields at the
+ * molecule's sites, the field change, the previous dipoles and their last
+ * change; 2 hidden layers of 64, tanh).  The dipole solve then iterates from that guess to
+ * the same tolerance.  Training rows are the solver's own converged dipoles. */
 /* Allocates the network (seeded weights) and room for capacity_frames
  * configurations of training rows. */
 int smd_mlp_init(smd_ctx *ctx, int capacity_frames, unsigned int seed);
 /* Appends the current configuration's rows (features and the converged
- * dipoles of the last force evaluation). */
+ * dipoles of the last force evaluation); needs two stored time steps. */
 int smd_mlp_collect(smd_ctx *ctx);
 /* Adam on the mean-squared error over all collected rows; *loss receives the
  * final error on one batch.  Marks the network ready for SMD_GUESS_LEARNED. */

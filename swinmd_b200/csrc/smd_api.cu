@@ -159,14 +159,18 @@ void enqueue_step(Ctx &c) {
         launch_nhc_first(c);
         launch_nlist(c, false);
         c.fixq_from_integrate = 1;
+        c.in_step = 1;
         enqueue_forces(c);
+        c.in_step = 0;
         c.fixq_from_integrate = 0;
         launch_nhc_second(c);
         return;
     }
     launch_nlist(c, false);
     c.fixq_from_integrate = 1;
+    c.in_step = 1;
     enqueue_forces(c);
+    c.in_step = 0;
     c.fixq_from_integrate = 0;
     launch_integrate(c);
 }
@@ -219,7 +223,7 @@ void smd_destroy(smd_ctx *x) {
                     c.pl.cell_count, c.pl.cell_start, c.pl.cell_atoms, c.rc.kn, c.rc.kcoef,
                     c.rc.sk, c.rc.kvec, c.clen2, c.type_mp, c.type_polar, c.mu, c.qd, c.trq, c.e0,
                     c.pind, c.cgw, c.cgs, c.cg_bar, c.vpos4, c.vfixq, c.fv, c.ind_rj, c.ind_rc, c.ind_cnt,
-                    c.rc.kpack, c.rc.kb4};
+                    c.rc.kpack, c.rc.kb4, c.phist};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -492,6 +496,10 @@ int smd_set_multipole(smd_ctx *x, const double *type_mp, const double *polar, do
     CK(dalloc(&c.cgs, 8 + 8 * (size_t)c.cg_blocks));
     CK(cudaMemset(c.cgs, 0, (8 + 8 * (size_t)c.cg_blocks) * sizeof(double)));
     CK(dalloc(&c.cg_bar, 1));
+    if (c.ind_on) {
+        CK(dalloc(&c.phist, 24 * n));
+        CK(cudaMemset(c.flags + 2, 0, sizeof(int)));
+    }
     if (ensure_ind_rows(c)) return fail(x, SMD_ERR_CUDA, "smd_set_multipole: tensor rows: allocation failed");
     r = setup_recip(c);
     if (r) return fail(x, r, "smd_set_multipole: reciprocal set-up failed");
@@ -567,6 +575,9 @@ int smd_mlp_collect(smd_ctx *x) {
     if (!x || !x->c.mlp_data) return fail(x, SMD_ERR_ARG, "smd_mlp_collect: call smd_mlp_init first");
     Ctx &c = x->c;
     if (c.mlp_rows + c.n > c.mlp_cap) return fail(x, SMD_ERR_ARG, "smd_mlp_collect: training buffer full");
+    int cnt = 0;
+    CK(cudaMemcpy(&cnt, c.flags + 2, sizeof(int), cudaMemcpyDeviceToHost));
+    if (cnt < 2) return fail(x, SMD_ERR_ARG, "smd_mlp_collect: the guess needs 2 stored time steps first");
     launch_mlp_collect(c);
     c.mlp_rows += c.n;
     return sync_status(x);
@@ -890,6 +901,9 @@ int smd_integrator_start(smd_ctx *x) {
     CK(cudaMemsetAsync(c.status, 0, sizeof(unsigned), c.stream));
     CK(cudaMemsetAsync(c.obs, 0, sizeof(smd_observables), c.stream));
     CK(cudaMemsetAsync(c.ticket, 0, sizeof(unsigned), c.stream));
+    // the dipole history of the guess starts afresh (uploads keep it: the
+    // solve converges to its tolerance from any start)
+    CK(cudaMemsetAsync(c.flags + 2, 0, sizeof(int), c.stream));
     launch_nlist(c, true);
     c.list_valid = 1;
     CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));

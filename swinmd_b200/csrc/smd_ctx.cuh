@@ -109,6 +109,8 @@ struct Ctx {
     void *ind_rc = nullptr;         // coefficients [N][cap] (float4 or double4)
     int *ind_cnt = nullptr;         // row lengths [N]
     int ind_cap = 0;
+    double *phist = nullptr;        // last 4 steps' converged dipoles and fields [4][6][N] (ring, count in flags[2])
+    int in_step = 0;                // enqueueing the step graph: the solve stores its dipoles
     double *frame = nullptr;        // [9][N] site axes u, v, w (lab frame)
     // per-site network giving the initial induced dipoles (smd_mlp.cu)
     int mlp_ready = 0;

@@ -604,6 +604,17 @@ __global__ void k_ind_mol(IndArgs a, long long *trq, long long *acc) {
     }
 }
 
+// ring of the last 4 steps' converged dipoles and permanent fields;
+// flags[2] counts the stored steps
+__global__ void k_hist_push(int n, const double *p, const double *e0, double *ph, const int *flags) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double *h = ph + (size_t)(flags[2] & 3) * 6 * n;
+    h[i] = p[i]; h[n + i] = p[n + i]; h[2 * n + i] = p[2 * n + i];
+    h[3 * n + i] = e0[i]; h[4 * n + i] = e0[n + i]; h[5 * n + i] = e0[2 * n + i];
+}
+__global__ void k_hist_advance(int *flags) { flags[2] += 1; }
+
 static IndArgs ind_args(Ctx &c) {
     IndArgs a;
     a.n = c.n; a.nmol = c.nmol; a.nbr = c.pl.nbr; a.nnbr = c.pl.nnbr; a.mol = c.mol;
@@ -688,6 +699,11 @@ void launch_ind_solve(Ctx &c) {
         cudaLaunchKernelEx(&cfg, k_ind_cg<true>, g);
     else
         cudaLaunchKernelEx(&cfg, k_ind_cg<false>, g);
+    // a time step stores its converged dipoles for the next steps' guess
+    if (c.in_step && c.phist) {
+        k_hist_push<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.pind, c.e0, c.phist, c.flags);
+        k_hist_advance<<<1, 1, 0, c.stream>>>(c.flags);
+    }
 }
 
 void launch_ind_short(Ctx &c) {

@@ -1,19 +1,23 @@
 // Per-site network giving the initial guess of the induced dipoles.
 //
 // The induced dipoles are solved to the same tolerance from whatever start
-// the solver is given; this network only supplies a better start than the
-// first-order guess p0 = alpha E0, so the solve needs fewer iterations.
+// the solver is given; this guess only brings the start closer, so the solve
+// needs fewer iterations.  The guess is the previous step's converged
+// dipoles moved by the linear response to the change of the permanent field,
+// pl = p(t-1) + alpha (E0(t) - E0(t-1)), plus a correction the network
+// predicts (the mutual induction the first-order response leaves out).
+// Each time step stores its converged dipoles and permanent field.
 //
-// Inputs (F = 20 per site, all invariant under rotation of the system):
-//   0-2   permanent field E0 at the site in the site's own axes (u, v, w)
-//   3     |E0|
-//   4-9   E0 at the molecule's two other sites, in this site's axes
-//   10-17 radial densities of the neighbours within the cutoff:
-//         sum_j exp(-(r - R_k)^2 / 2s^2) fc(r), R_k = 0.22 + 0.09 k nm,
-//         s = 0.05 nm, fc = (cos(pi r/rc) + 1)/2
-//   18-19 site type (H, O) one-hot
-// Output (3): 1000 (p - alpha E0) in the site axes; the guess is
-//   p0 = alpha E0 + (u, v, w) y / 1000.
+// Inputs (F = 20 per site, in the site's own axes u, v, w, so invariant under
+// rotation of the system):
+//   0-2   permanent field E0(t) at the site
+//   3     |E0(t)|
+//   4-6   E0(t) - E0(t-1)
+//   7-12  E0(t) at the molecule's two other sites
+//   13-15 p(t-1)
+//   16-18 p(t-1) - p(t-2)
+//   19    site type (O = 1, H = 0)
+// Output (3): 1e5 (p - pl) in the site axes.
 // Network: F -> 64 -> 64 -> 3, tanh hidden activations, FP32 weights.
 // Training (on rows the solver itself produced): mean-squared error, Adam,
 // forward and backward on the GPU with one thread per row; weight gradients
@@ -29,7 +33,7 @@ namespace smd {
 constexpr int MF = 20, MH = 64, MO = 3;
 constexpr int OW1 = 0, OB1 = OW1 + MH * MF, OW2 = OB1 + MH, OB2 = OW2 + MH * MH, OW3 = OB2 + MH,
               OB3 = OW3 + MO * MH, MLP_NPARAM = OB3 + MO;
-constexpr float TARGET_SCALE = 1000.0f;
+constexpr float TARGET_SCALE = 1.0e5f;
 constexpr int MLP_THREADS = 256;
 constexpr int MLP_MAX_BLOCKS = 64;
 
@@ -43,68 +47,68 @@ __device__ __forceinline__ V3 in_axes(const double *frame, int n, int i, V3 e) {
     return v3(dot(axis(frame, n, i, 0), e), dot(axis(frame, n, i, 1), e), dot(axis(frame, n, i, 2), e));
 }
 
-// MLP_FTPP lanes per site split the neighbour row; the radial densities are
-// combined by shuffles in a fixed order
-constexpr int MLP_FTPP = 8;
-__global__ void k_mlp_features(int n, const int *nbr, const int *nnbr, const int *mol, const int *mol_off,
-                               const int *mol_atoms, const double4 *pos4, Box box, double rc,
-                               const double *frame, const double *e0, float *x) {
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = gt / MLP_FTPP, t = gt % MLP_FTPP;
-    float g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    double4 pi = make_double4(0, 0, 0, 0);
-    if (i < n) {
-        pi = pos4[i];
-        const int cnt = nnbr[i];
-        const float rcf = (float)rc, irc = 1.f / (float)rc;
-        for (int k = t; k < cnt; k += MLP_FTPP) {
-            const int j = nbr[(size_t)k * n + i] & 0x7fffffff;
-            const double4 pj = pos4[j];
-            const double dx = pbc1(pj.x - pi.x, box.L[0], box.half[0]);
-            const double dy = pbc1(pj.y - pi.y, box.L[1], box.half[1]);
-            const double dz = pbc1(pj.z - pi.z, box.L[2], box.half[2]);
-            const float r = sqrtf((float)(dx * dx + dy * dy + dz * dz));
-            if (r >= rcf) continue;
-            const float fc = 0.5f * (cospif(r * irc) + 1.f);
-            for (int b = 0; b < 8; b++) {
-                const float d = r - (0.22f + 0.09f * b);
-                g[b] += expf(-d * d * 200.f) * fc;   // 1 / (2 * 0.05^2)
-            }
-        }
-    }
-    for (int b = 0; b < 8; b++) g[b] = group_sum<MLP_FTPP>(g[b]);
-    if (i >= n || t != 0) return;
+// stored step k = 1, 2 (most recent first): dipole and permanent field of
+// site i; the ring holds [4][6][N] (p x y z, E0 x y z), flags[2] counts steps
+__device__ __forceinline__ V3 hist_p(const double *ph, int n, int cnt, int k, int i) {
+    const double *h = ph + (size_t)((cnt - k) & 3) * 6 * n;
+    return v3(h[i], h[n + i], h[2 * n + i]);
+}
+__device__ __forceinline__ V3 hist_e(const double *ph, int n, int cnt, int k, int i) {
+    const double *h = ph + (size_t)((cnt - k) & 3) * 6 * n + 3 * (size_t)n;
+    return v3(h[i], h[n + i], h[2 * n + i]);
+}
+
+// first-order guess: the previous dipoles moved by the linear response to
+// the change of the permanent field (alpha E0 when nothing is stored)
+__device__ __forceinline__ V3 linear_guess(const double *ph, int n, int cnt, int i, V3 E, double alpha) {
+    if (cnt < 1) return alpha * E;
+    return hist_p(ph, n, cnt, 1, i) + alpha * (E - hist_e(ph, n, cnt, 1, i));
+}
+
+__global__ void k_mlp_features(int n, const int *mol, const int *mol_off, const int *mol_atoms,
+                               const double4 *pos4, const double *frame, const double *e0, const double *ph,
+                               const int *flags, float *x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int cnt = flags[2];
     float f[MF];
     const V3 E = v3(e0[i], e0[n + i], e0[2 * n + i]);
     const V3 El = in_axes(frame, n, i, E);
     f[0] = (float)El.x; f[1] = (float)El.y; f[2] = (float)El.z;
     f[3] = (float)len(E);
-    int q = 4;
+    for (int q = 4; q < 19; q++) f[q] = 0.f;
+    if (cnt >= 2) {
+        const V3 dE = in_axes(frame, n, i, E - hist_e(ph, n, cnt, 1, i));
+        const V3 p1 = hist_p(ph, n, cnt, 1, i);
+        const V3 pl = in_axes(frame, n, i, p1), dp = in_axes(frame, n, i, p1 - hist_p(ph, n, cnt, 2, i));
+        f[4] = (float)dE.x; f[5] = (float)dE.y; f[6] = (float)dE.z;
+        f[13] = (float)pl.x; f[14] = (float)pl.y; f[15] = (float)pl.z;
+        f[16] = (float)dp.x; f[17] = (float)dp.y; f[18] = (float)dp.z;
+    }
+    int q = 7;
     const int m = mol[i];
-    for (int k = mol_off[m]; k < mol_off[m + 1] && q < 10; k++) {
+    for (int k = mol_off[m]; k < mol_off[m + 1] && q < 13; k++) {
         const int j = mol_atoms[k];
         if (j == i) continue;
         const V3 Ej = in_axes(frame, n, i, v3(e0[j], e0[n + j], e0[2 * n + j]));
         f[q++] = (float)Ej.x; f[q++] = (float)Ej.y; f[q++] = (float)Ej.z;
     }
-    for (; q < 10; q++) f[q] = 0.f;
-    for (int b = 0; b < 8; b++) f[10 + b] = g[b];
-    const int ty = (int)pi.w;
-    f[18] = ty == 0 ? 1.f : 0.f;
-    f[19] = ty == 0 ? 0.f : 1.f;
+    f[19] = (int)pos4[i].w == 0 ? 0.f : 1.f;
     for (int k = 0; k < MF; k++) x[(size_t)i * MF + k] = f[k];
 }
 
-// appends (features, target) rows of the current configuration
-__global__ void k_mlp_collect(int n, const float *x, const double *frame, const double *e0, const double *p,
-                              const double4 *pos4, const double *polar, float *data, long long row0) {
+// appends (features, target) rows of the current configuration: the target
+// is what the network should add to the first-order guess (needs 2 stored steps)
+__global__ void k_mlp_collect(int n, const float *x, const double *frame, const double *p, const double *e0,
+                              const double4 *pos4, const double *polar, const double *ph, const int *flags,
+                              float *data, long long row0) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float *row = data + (size_t)(row0 + i) * (MF + MO);
     for (int k = 0; k < MF; k++) row[k] = x[(size_t)i * MF + k];
     const double a = fmax(1e-8, polar[(int)pos4[i].w]);
-    const V3 d = v3(p[i] - a * e0[i], p[n + i] - a * e0[n + i], p[2 * n + i] - a * e0[2 * n + i]);
-    const V3 dl = in_axes(frame, n, i, d);
+    const V3 pl = linear_guess(ph, n, flags[2], i, v3(e0[i], e0[n + i], e0[2 * n + i]), a);
+    const V3 dl = in_axes(frame, n, i, v3(p[i], p[n + i], p[2 * n + i]) - pl);
     row[MF] = (float)dl.x * TARGET_SCALE;
     row[MF + 1] = (float)dl.y * TARGET_SCALE;
     row[MF + 2] = (float)dl.z * TARGET_SCALE;
@@ -151,22 +155,62 @@ __device__ __forceinline__ void mlp_forward(const float *W, const float *xn, flo
     }
 }
 
-__global__ void k_mlp_infer(int n, const float *x, const float *norm, const float *Wg, const double *frame,
-                            const double *e0, const double4 *pos4, const double *polar, double *p) {
-    __shared__ float W[MLP_NPARAM];
-    for (int k = threadIdx.x; k < MLP_NPARAM; k += blockDim.x) W[k] = Wg[k];
+// Inference with MLP_ITPP threads per site: each computes MH / MLP_ITPP
+// hidden units of each layer; the hidden activations go through shared
+// memory (rows padded to avoid bank conflicts), the three outputs are summed
+// over the site's threads by shuffles.
+constexpr int MLP_ITPP = 4;
+constexpr int MLP_IBLOCK = 128;
+constexpr int MLP_ISITES = MLP_IBLOCK / MLP_ITPP;
+constexpr int HP = MH + 1;   // padded row of hidden activations / of W2
+__global__ void __launch_bounds__(MLP_IBLOCK) k_mlp_infer(int n, const float *x, const float *norm, const float *Wg,
+                                                          const double *frame, const double *e0,
+                                                          const double4 *pos4, const double *polar,
+                                                          const double *ph, const int *flags, double *p) {
+    __shared__ float sW1[MH * MF], sB1[MH], sW2[MH * HP], sB2[MH], sW3[MO * MH], sB3[MO];
+    __shared__ float sX[MLP_ISITES][MF], sH1[MLP_ISITES][HP];
+    for (int k = threadIdx.x; k < MH * MF; k += blockDim.x) sW1[k] = Wg[OW1 + k];
+    for (int k = threadIdx.x; k < MH * MH; k += blockDim.x) sW2[(k / MH) * HP + k % MH] = Wg[OW2 + k];
+    for (int k = threadIdx.x; k < MO * MH; k += blockDim.x) sW3[k] = Wg[OW3 + k];
+    for (int k = threadIdx.x; k < MH; k += blockDim.x) { sB1[k] = Wg[OB1 + k]; sB2[k] = Wg[OB2 + k]; }
+    if (threadIdx.x < MO) sB3[threadIdx.x] = Wg[OB3 + threadIdx.x];
+    const int ls = threadIdx.x / MLP_ITPP, t = threadIdx.x % MLP_ITPP;
+    const int i = blockIdx.x * MLP_ISITES + ls;
+    const bool own = i < n;
+    const int cnt = flags[2];
+    for (int f = t; f < MF; f += MLP_ITPP)
+        sX[ls][f] = own ? (x[(size_t)i * MF + f] - norm[f]) * norm[MF + f] : 0.f;
     __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    float xn[MF], h1[MH], y[MO];
-    for (int f = 0; f < MF; f++) xn[f] = (x[(size_t)i * MF + f] - norm[f]) * norm[MF + f];
-    mlp_forward(W, xn, h1, y);
+    for (int j = t; j < MH; j += MLP_ITPP) {
+        float z = sB1[j];
+#pragma unroll
+        for (int f = 0; f < MF; f++) z = fmaf(sW1[j * MF + f], sX[ls][f], z);
+        sH1[ls][j] = tanhf(z);
+    }
+    __syncthreads();
+    float y0 = 0.f, y1 = 0.f, y2 = 0.f;
+    for (int j = t; j < MH; j += MLP_ITPP) {
+        float z = sB2[j];
+#pragma unroll 16
+        for (int k = 0; k < MH; k++) z = fmaf(sW2[j * HP + k], sH1[ls][k], z);
+        const float h2 = tanhf(z);
+        y0 = fmaf(sW3[j], h2, y0);
+        y1 = fmaf(sW3[MH + j], h2, y1);
+        y2 = fmaf(sW3[2 * MH + j], h2, y2);
+    }
+    y0 = group_sum<MLP_ITPP>(y0) + sB3[0];
+    y1 = group_sum<MLP_ITPP>(y1) + sB3[1];
+    y2 = group_sum<MLP_ITPP>(y2) + sB3[2];
+    if (!own || t != 0) return;
     const double a = fmax(1e-8, polar[(int)pos4[i].w]);
-    const V3 u = axis(frame, n, i, 0), v = axis(frame, n, i, 1), w = axis(frame, n, i, 2);
-    const V3 d = (y[0] / TARGET_SCALE) * u + (y[1] / TARGET_SCALE) * v + (y[2] / TARGET_SCALE) * w;
-    p[i] = a * e0[i] + d.x;
-    p[n + i] = a * e0[n + i] + d.y;
-    p[2 * n + i] = a * e0[2 * n + i] + d.z;
+    V3 g = linear_guess(ph, n, cnt, i, v3(e0[i], e0[n + i], e0[2 * n + i]), a);
+    if (cnt >= 2) {
+        const V3 u = axis(frame, n, i, 0), v = axis(frame, n, i, 1), w = axis(frame, n, i, 2);
+        g = g + (y0 / TARGET_SCALE) * u + (y1 / TARGET_SCALE) * v + (y2 / TARGET_SCALE) * w;
+    }
+    p[i] = g.x;
+    p[n + i] = g.y;
+    p[2 * n + i] = g.z;
 }
 
 // gradient of the batch loss (1/(3B)) sum (y - t)^2 ; rows idx[r0 .. r0+B)
@@ -252,15 +296,14 @@ __global__ void k_mlp_adam(int nblocks, const float *part, float *W, float *m, f
 // host side
 // ---------------------------------------------------------------------------
 void launch_mlp_features(Ctx &c) {
-    k_mlp_features<<<(int)(((long long)c.n * MLP_FTPP + 127) / 128), 128, 0, c.stream>>>(c.n, c.pl.nbr, c.pl.nnbr, c.mol, c.mol_off,
-                                                            c.mol_atoms, c.pos4, c.box, c.cutoff, c.frame,
-                                                            c.e0, c.mlp_x);
+    k_mlp_features<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.mol, c.mol_off, c.mol_atoms, c.pos4, c.frame,
+                                                            c.e0, c.phist, c.flags, c.mlp_x);
 }
 
 void launch_mlp_guess(Ctx &c) {
     launch_mlp_features(c);
-    k_mlp_infer<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.mlp_x, c.mlp_norm, c.mlp_w, c.frame, c.e0,
-                                                         c.pos4, c.type_polar, c.pind);
+    k_mlp_infer<<<(c.n + MLP_ISITES - 1) / MLP_ISITES, MLP_IBLOCK, 0, c.stream>>>(
+        c.n, c.mlp_x, c.mlp_norm, c.mlp_w, c.frame, c.e0, c.pos4, c.type_polar, c.phist, c.flags, c.pind);
 }
 
 int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed) {
@@ -300,8 +343,9 @@ int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed) {
 
 void launch_mlp_collect(Ctx &c) {
     launch_mlp_features(c);
-    k_mlp_collect<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.mlp_x, c.frame, c.e0, c.pind, c.pos4,
-                                                           c.type_polar, c.mlp_data, c.mlp_rows);
+    k_mlp_collect<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.mlp_x, c.frame, c.pind, c.e0, c.pos4,
+                                                           c.type_polar, c.phist, c.flags, c.mlp_data,
+                                                           c.mlp_rows);
 }
 
 void launch_mlp_norm(Ctx &c) {

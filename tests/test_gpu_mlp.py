@@ -44,6 +44,7 @@ def test_learned_guess_cuts_iterations():
     ens.set_solver(tol=2.0819e-8, max_iter=500, guess=L.GUESS_DIRECT)
     lf = engine.LFIntegrator(ens)
     lf.start()
+    lf.run(2)                      # the guess starts from the last two solves
     ens.mlp_init(capacity_frames=40, seed=3)
     for _ in range(40):            # training frames from the solver itself
         lf.run(2)
