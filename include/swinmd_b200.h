@@ -236,6 +236,17 @@ int smd_compute_forces(smd_ctx *ctx, uint32_t terms, double *force, double *ener
  * CellManager::update_pair_list builds (src/utils/CellManager.cpp:216-314).
  * cap: room in pairs[] for `cap` pairs; *count receives the number found. */
 int smd_get_pairs(smd_ctx *ctx, int32_t *pairs, int64_t cap, int64_t *count);
+/* smd_compute_forces for callers that may not allocate device memory (a
+ * host loop with a fixed memory budget, a process that must not call
+ * cudaMalloc after set-up): the same evaluation and results, with the device
+ * force buffer taken from a static array of 65536 x 3 doubles inside the
+ * library instead of a cudaMalloc/cudaFree per call.  No reference
+ * counterpart (the reference evaluates forces on the host).  Returns
+ * SMD_ERR_ARG for systems of more than 65536 sites.  Calls that overlap on
+ * one device (threads, or several contexts) share the array and race.  The
+ * first call on a device resolves the array's address (cudaGetSymbolAddress)
+ * with that device current; make that first call outside any stream capture. */
+int smd_compute_forces_noalloc(smd_ctx *ctx, uint32_t terms, double *force, double *energy, double *virial);
 /* k-vector count of the Ewald reciprocal set (EwaldForce::set_up). */
 int smd_ewald_nk(smd_ctx *ctx, int *nk);
 

@@ -60,6 +60,7 @@ _F = ctypes.POINTER(ctypes.c_float)
 # name: (restype, argtypes)
 SIGNATURES = {
     "smd_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P)]),
+    "smd_compute_forces_noalloc": (ctypes.c_int, [_P, ctypes.c_uint32, _D, _D, _D]),
     "smd_batch_create": (ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int, ctypes.POINTER(_P)]),
     "smd_batch_destroy": (None, [_P]),
     "smd_batch_last_error": (ctypes.c_char_p, [_P]),

@@ -5,6 +5,7 @@
 #include <cstring>
 #include <algorithm>
 #include <new>
+#include <string>
 #include "smd_ctx.cuh"
 
 using namespace smd;
@@ -788,6 +789,88 @@ int smd_compute_forces(smd_ctx *x, uint32_t terms, double *force, double *energy
     if (force) CK(cudaMemcpyAsync(force, dforce, 3 * (size_t)c.n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     int rs = sync_status(x);
     if (dforce) cudaFree(dforce);
+    if (rs) return rs;
+    const bool vdw = (terms & SMD_TERM_VDW) && c.vdw != VDW_NONE;
+    if (energy) {
+        for (int q = 0; q < SMD_E_COUNT; q++) energy[q] = 0;
+        energy[SMD_E_VDW] = (double)hacc[ACC_E_VDW] * ACC_INV + (vdw ? c.e_lrc : 0.0);
+        energy[SMD_E_REAL] = (double)hacc[ACC_E_REAL] * ACC_INV;
+        energy[SMD_E_LONG] = (double)hacc[ACC_E_LONG] * ACC_INV;
+        energy[SMD_E_CORRECT] = (want_real ? c.e_self : 0.0) + (double)hacc[ACC_E_SELF] * ACC_INV;
+        energy[SMD_E_MOLCORRECT] = (double)hacc[ACC_E_INTRA] * ACC_INV;
+        energy[SMD_E_SURF] = (double)hacc[ACC_E_SURF] * ACC_INV;
+        energy[SMD_E_POL_REAL] = (double)hacc[ACC_E_POL_REAL] * ACC_INV;
+        energy[SMD_E_POL_LONG] = (double)hacc[ACC_E_POL_LONG] * ACC_INV;
+        energy[SMD_E_POL_SELF] = (double)hacc[ACC_E_POL_SELF] * ACC_INV;
+        energy[SMD_E_POL_INTRA] = (double)hacc[ACC_E_POL_INTRA] * ACC_INV;
+    }
+    if (virial) {
+        for (int q = 0; q < 9; q++) {
+            virial[q] = ((double)hacc[ACC_VIR + q] + (double)hacc[ACC_LVIR + q]) * ACC_INV;
+            if (vdw && (q == 0 || q == 4 || q == 8)) virial[q] -= c.v_lrc;
+        }
+    }
+    return SMD_OK;
+}
+
+// ---- force evaluation without device allocation ---------------------------
+// The device output buffer of smd_compute_forces_noalloc lives in this
+// file-scope array instead of a cudaMalloc'd buffer.  Nothing in it needs to
+// start at zero: the finalize kernel writes every element a call reads back.
+// One array per process and device: calls that overlap (two threads, or two
+// contexts on one device) share it and race.
+}  // extern "C"
+
+namespace {
+constexpr int NOALLOC_MAX_SITES = 65536;
+static __device__ __align__(256) double g_noalloc_force[3 * NOALLOC_MAX_SITES];
+constexpr int NOALLOC_MAX_DEVICES = 64;
+double *g_noalloc_addr[NOALLOC_MAX_DEVICES] = {nullptr};
+}  // namespace
+
+extern "C" {
+
+int smd_compute_forces_noalloc(smd_ctx *x, uint32_t terms, double *force, double *energy, double *virial) {
+    if (!x || x->c.n == 0 || x->c.box.L[0] <= 0)
+        return fail(x, SMD_ERR_ARG, "smd_compute_forces_noalloc: system not set up");
+    Ctx &c = x->c;
+    if (c.n > NOALLOC_MAX_SITES)
+        return fail(x, SMD_ERR_ARG, "smd_compute_forces_noalloc: " + std::to_string(c.n) +
+                                        " sites exceed the static scratch of " +
+                                        std::to_string(NOALLOC_MAX_SITES) + " sites");
+    if (c.device < 0 || c.device >= NOALLOC_MAX_DEVICES)
+        return fail(x, SMD_ERR_ARG, "smd_compute_forces_noalloc: device index out of range");
+    CK(cudaSetDevice(c.device));
+    if (!g_noalloc_addr[c.device]) {
+        // once per device, with that device current
+        void *a = nullptr;
+        CK(cudaGetSymbolAddress(&a, g_noalloc_force));
+        g_noalloc_addr[c.device] = (double *)a;
+    }
+    double *dforce = g_noalloc_addr[c.device];
+    CK(cudaMemsetAsync(c.status, 0, sizeof(unsigned), c.stream));
+    launch_nlist(c, true);
+    c.list_valid = 1;
+    CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
+    CK(cudaMemsetAsync(c.frc, 0, 3 * (size_t)c.n * sizeof(long long), c.stream));
+    const int save_vdw = c.vdw, save_ew = c.ewald_on;
+    if (!(terms & SMD_TERM_VDW)) c.vdw = VDW_NONE;
+    bool want_real = (terms & SMD_TERM_EWALD_REAL) && c.ewald_on;
+    bool want_long = (terms & SMD_TERM_EWALD_LONG) && c.ewald_on;
+    c.ewald_on = want_real ? 1 : 0;
+    launch_pair(c);
+    if (want_real) launch_intra(c);
+    c.ewald_on = save_ew;
+    if (want_long) launch_recip(c);
+    c.vdw = save_vdw;
+    if (c.mp_on && (terms & (SMD_TERM_MP_SHORT | SMD_TERM_MP_LONG | SMD_TERM_IND_SHORT | SMD_TERM_IND_LONG)))
+        enqueue_polar(c, terms & SMD_TERM_MP_SHORT, terms & SMD_TERM_MP_LONG, terms & SMD_TERM_IND_SHORT,
+                      terms & SMD_TERM_IND_LONG);
+    if (force) launch_finalize_forces(c, dforce);
+    long long hacc[ACC_COUNT];
+    CK(cudaMemcpyAsync(hacc, c.acc, sizeof(hacc), cudaMemcpyDeviceToHost, c.stream));
+    if (force) CK(cudaMemcpyAsync(force, dforce, 3 * (size_t)c.n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    int rs = sync_status(x);
     if (rs) return rs;
     const bool vdw = (terms & SMD_TERM_VDW) && c.vdw != VDW_NONE;
     if (energy) {

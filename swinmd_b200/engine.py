@@ -344,6 +344,15 @@ class GpuEnsemble:
         self._chk(self.lib.smd_compute_forces(self.ctx, terms, L.dptr(f), L.dptr(e), L.dptr(w)))
         return f.reshape(-1, 3), e, w
 
+    def compute_forces_noalloc(self, terms: int = L.TERM_ALL):
+        """compute_forces through the entry point that allocates no device
+        memory (static scratch of 65536 sites)."""
+        f = np.zeros(3 * self.n)
+        e = np.zeros(L.E_COUNT)
+        w = np.zeros(9)
+        self._chk(self.lib.smd_compute_forces_noalloc(self.ctx, terms, L.dptr(f), L.dptr(e), L.dptr(w)))
+        return f.reshape(-1, 3), e, w
+
     def pairs(self) -> np.ndarray:
         cnt = ctypes.c_int64()
         self._chk(self.lib.smd_get_pairs(self.ctx, None, 0, ctypes.byref(cnt)))
