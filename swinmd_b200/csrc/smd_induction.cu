@@ -485,9 +485,81 @@ __device__ __forceinline__ void ind_pair(double qi, V3 mi, const Q6 &Qi, V3 pi_,
     o.tau = scale * (B1d * Gt1 + B2d * Gt2 + B3d * Gt3);
 }
 
+// Mixed path: the same terms with the angular algebra (G, their gradients
+// and the torque coefficients) in FP32 and the radial Ewald / Thole factors,
+// the energy and the force assembly in FP64.
+struct IndAlgF {
+    float G1i, G2i, G3i, G1j, G2j, G3j, G1ip, G2ip;
+    F3 gG1i, gG2i, gG3i, gG1j, gG2j, gG3j, gG2ip, gG2jp, Gt1, Gt2, Gt3;
+};
+
+__device__ __forceinline__ void ind_algebra_f(float qi, F3 mi, const Q6F &Qi, F3 pi_, float qj, F3 mj,
+                                              const Q6F &Qj, F3 pj_, F3 r, IndAlgF &A) {
+    const F3 rji = -r;
+    const float QiI = qtr(Qi), QjI = qtr(Qj);
+    const F3 Qir = qv(Qi, r), Qjrji = qv(Qj, rji);
+    const float QiRij = dot(r, Qir), QjRji = dot(r, qv(Qj, r));
+    const float pjr = dot(pj_, r), pirji = dot(pi_, rji);
+    A.G1i = -qi * pjr - dot(mi, pj_);
+    A.G2i = -dot(mi, r) * pjr - 2.f * dot(pj_, Qir) - pjr * QiI;
+    A.G3i = -pjr * QiRij;
+    A.G1j = -qj * pirji - dot(mj, pi_);
+    A.G2j = -dot(mj, rji) * pirji - 2.f * dot(pi_, Qjrji) - pirji * QjI;
+    A.G3j = -pirji * QjRji;
+    A.gG1i = (-qi) * pj_;
+    A.gG2i = (-pjr) * mi - dot(mi, r) * pj_ - 2.f * qv(Qi, pj_) - QiI * pj_;
+    A.gG3i = (-QiRij) * pj_ - (2.f * pjr) * Qir;
+    A.gG1j = (-qj) * pi_;
+    A.gG2j = (-pirji) * mj - dot(mj, rji) * pi_ - 2.f * qv(Qj, pi_) - QjI * pi_;
+    A.gG3j = (-QjRji) * pi_ - (2.f * pirji) * Qjrji;
+    A.G1ip = -dot(pi_, pj_);
+    A.G2ip = -dot(pi_, r) * pjr;
+    A.gG2ip = (-pjr) * pi_;
+    A.gG2jp = (-pirji) * pj_;
+    A.Gt1 = crs(mi, pj_);
+    A.Gt2 = pjr * crs(mi, r) + 2.f * crs(Qir, pj_) + 2.f * crs(qv(Qi, pj_), r);
+    A.Gt3 = (2.f * pjr) * crs(Qir, r);
+}
+
+__device__ __forceinline__ void ind_pair_mixed(const IndAlgF &A, V3 r, double r2, double poli, double polj,
+                                               double a, double alpha, double scale, IndPairOut &o) {
+    const double rr = sqrt(r2);
+    const double u3 = rr * rr * rr / sqrt(poli * polj);
+    const double a2 = alpha * alpha, a2pi = 2.0 * alpha / SQRT_PI_I, ex = exp(-a2 * r2);
+    double B[5];
+    B[0] = erfc(alpha * rr) / rr;
+    const double ir2 = 1.0 / r2;
+    B[1] = (-B[0] - a2pi * ex) * ir2;
+    B[2] = (-3 * B[1] + 2 * a2pi * a2 * ex) * ir2;
+    B[3] = (-5 * B[2] - 4 * a2pi * a2 * a2 * ex) * ir2;
+    B[4] = (-7 * B[3] + 8 * a2pi * a2 * a2 * a2 * ex) * ir2;
+    const double e = exp(-a * u3), au3 = a * u3, a2u6 = au3 * au3, a3u9 = a2u6 * au3;
+    const double l3 = 1.0 - e;
+    const double gl3 = 3.0 * au3 * e * ir2;
+    const double gl5 = 3.0 * a2u6 * e * ir2;
+    const double gl7 = (-3.0 * a2u6 + 9.0 * a3u9) * e * (0.2 * ir2);
+    const double B1d = B[1] * l3;
+    const double B2d = B[2] * l3 + B[1] * gl3;
+    const double B3d = B[3] * l3 + B[2] * 2.0 * gl3 + B[1] * (gl3 - 3.0 * gl5) * ir2;
+    const double B4d = B[4] * l3 + B[3] * 3.0 * gl3 + B[2] * (3.0 * gl3 - 9.0 * gl5) * ir2 +
+                       B[1] * (-gl3 - 6.0 * gl5 + 15.0 * gl7) * (ir2 * ir2);
+    o.e = 0.5 * (((double)A.G1i + A.G1j) * B1d + ((double)A.G2i + A.G2j) * B2d + ((double)A.G3i + A.G3j) * B3d) *
+          scale;
+    const V3 fi = -(scale * (B1d * to_v3(A.gG1i) + B2d * to_v3(A.gG2i) + B3d * to_v3(A.gG3i)) +
+                    B2d * to_v3(A.gG2ip)) -
+                  (scale * (A.G1i * B2d + A.G2i * B3d + A.G3i * B4d) + A.G1ip * B2d + A.G2ip * B3d) * r;
+    const V3 fj = -(scale * (B1d * to_v3(A.gG1j) + B2d * to_v3(A.gG2j) + B3d * to_v3(A.gG3j)) +
+                    B2d * to_v3(A.gG2jp)) -
+                  (scale * (A.G1j * B2d + A.G2j * B3d + A.G3j * B4d)) * (-r);
+    o.fij = fi - fj;
+    o.tau = scale * (B1d * to_v3(A.Gt1) + B2d * to_v3(A.Gt2) + B3d * to_v3(A.Gt3));
+}
+
 struct IndRealArgs {
     IndArgs ia;
     long long *frc, *trq, *acc;
+    const int4 *fixq;      // mixed path: box fractions
+    double dscale[3];      // L / 2^32 per axis
 };
 
 __global__ void __launch_bounds__(64) k_ind_real(IndRealArgs A) {
@@ -549,6 +621,82 @@ __global__ void __launch_bounds__(64) k_ind_real(IndRealArgs A) {
         for (int q = 0; q < (int)(blockDim.x >> 5); q++) s += s_r[q][threadIdx.x];
         const int slot = threadIdx.x == 0 ? ACC_E_POL_REAL : ACC_VIR + threadIdx.x - 1;
         if (s != 0.0) atomicAdd((unsigned long long *)&A.acc[slot], (unsigned long long)to_fix(s, ACC_SCALE));
+    }
+}
+
+// Mixed-path induced real space: displacements from the box fractions (the
+// exact integer difference, r^2 from the 64-bit integer sum), FP32 algebra,
+// FP64 radial factors and accumulation (cubic boxes)
+__global__ void __launch_bounds__(64) k_ind_real_f(IndRealArgs A) {
+    const IndArgs &a = A.ia;
+    constexpr int TPP = 8;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gt / TPP, t = gt % TPP;
+    V3 f = v3(0, 0, 0), tau = v3(0, 0, 0);
+    double en = 0, w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (i < a.n) {
+        const int4 fi = A.fixq[i];
+        const float qi = (float)(a.tq[fi.w] / SQC);
+        const double poli = a.polar[fi.w];
+        const F3 mi = f3((float)a.mu[i], (float)a.mu[a.n + i], (float)a.mu[2 * a.n + i]);
+        const F3 pii = f3((float)a.p[i], (float)a.p[a.n + i], (float)a.p[2 * a.n + i]);
+        const Q6F Qi = {(float)a.qd[i], (float)a.qd[a.n + i], (float)a.qd[2 * a.n + i],
+                        (float)a.qd[3 * a.n + i], (float)a.qd[4 * a.n + i], (float)a.qd[5 * a.n + i]};
+        const double s2u = A.dscale[0] * A.dscale[0];
+        auto pair = [&](int j, double scale) {
+            const int4 fj = A.fixq[j];
+            const int ix = fi.x - fj.x, iy = fi.y - fj.y, iz = fi.z - fj.z;   // r = r_i - r_j
+            const unsigned long long s2 = (unsigned long long)((long long)ix * ix) +
+                                          (unsigned long long)((long long)iy * iy) +
+                                          (unsigned long long)((long long)iz * iz);
+            const double r2 = (double)s2 * s2u;
+            if (!(r2 < a.rc2)) return;
+            const V3 r = v3(ix * A.dscale[0], iy * A.dscale[1], iz * A.dscale[2]);
+            const F3 rf = f3((float)r.x, (float)r.y, (float)r.z);
+            const Q6F Qj = {(float)a.qd[j], (float)a.qd[a.n + j], (float)a.qd[2 * a.n + j],
+                            (float)a.qd[3 * a.n + j], (float)a.qd[4 * a.n + j], (float)a.qd[5 * a.n + j]};
+            IndAlgF al;
+            ind_algebra_f(qi, mi, Qi, pii, (float)(a.tq[fj.w] / SQC),
+                          f3((float)a.mu[j], (float)a.mu[a.n + j], (float)a.mu[2 * a.n + j]), Qj,
+                          f3((float)a.p[j], (float)a.p[a.n + j], (float)a.p[2 * a.n + j]), rf, al);
+            IndPairOut o;
+            ind_pair_mixed(al, r, r2, poli, a.polar[fj.w], a.a, a.alpha, scale, o);
+            en += o.e;
+            f = f + o.fij;
+            tau = tau + o.tau;
+            const double fr[3] = {o.fij.x, o.fij.y, o.fij.z}, rr[3] = {r.x, r.y, r.z};
+            for (int p = 0; p < 3; p++)
+                for (int q = 0; q < 3; q++) w[3 * p + q] -= 0.5 * fr[q] * rr[p];
+        };
+        const int cnt = a.nnbr[i];
+        for (int k = t; k < cnt; k += TPP) pair(a.nbr[(size_t)k * a.n + i] & 0x7fffffff, 1.0);
+        if (t == 0) {
+            const int m = a.mol[i];
+            for (int q = a.mol_off[m]; q < a.mol_off[m + 1]; q++) {
+                const int j = a.mol_atoms[q];
+                if (j != i && is_excluded(i, j, a.excl_off, a.excl)) pair(j, 0.0);
+            }
+        }
+    }
+    f.x = group_sum<TPP>(f.x); f.y = group_sum<TPP>(f.y); f.z = group_sum<TPP>(f.z);
+    tau.x = group_sum<TPP>(tau.x); tau.y = group_sum<TPP>(tau.y); tau.z = group_sum<TPP>(tau.z);
+    if (i < a.n && t == 0) {
+        add_fix3(A.frc, a.n, i, f, COU);
+        add_fix3(A.trq, a.n, i, tau, COU);
+    }
+    __shared__ double s_r[8][10];
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    double vals[10] = {0.5 * en * COU, w[0], w[1], w[2], w[3], w[4], w[5], w[6], w[7], w[8]};
+    for (int q = 0; q < 10; q++) {
+        double sv = warp_sum(vals[q]);
+        if (lane == 0) s_r[wp][q] = sv;
+    }
+    __syncthreads();
+    if (threadIdx.x < 10) {
+        double sv = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) sv += s_r[q][threadIdx.x];
+        const int slot = threadIdx.x == 0 ? ACC_E_POL_REAL : ACC_VIR + threadIdx.x - 1;
+        if (sv != 0.0) atomicAdd((unsigned long long *)&A.acc[slot], (unsigned long long)to_fix(sv, ACC_SCALE));
     }
 }
 
@@ -713,7 +861,15 @@ void launch_ind_short(Ctx &c) {
     // 64-thread blocks: at this kernel's register count the SM holds more
     // warps in small blocks than in one 256-thread block
     const int nb = (int)(((long long)c.n * 8 + 63) / 64);
-    k_ind_real<<<nb, 64, 0, c.stream>>>(A);
+    const bool cubic = c.box.L[0] == c.box.L[1] && c.box.L[1] == c.box.L[2];
+    if (c.precision == SMD_PREC_MIXED && cubic) {
+        if (!c.fixq_from_integrate) launch_fixq(c);
+        A.fixq = c.fixq;
+        for (int d = 0; d < 3; d++) A.dscale[d] = c.box.L[d] / 4294967296.0;
+        k_ind_real_f<<<nb, 64, 0, c.stream>>>(A);
+    } else {
+        k_ind_real<<<nb, 64, 0, c.stream>>>(A);
+    }
     k_ind_mol<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(A.ia, c.trq, c.acc);
 }
 

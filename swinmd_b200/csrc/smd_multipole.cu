@@ -17,7 +17,9 @@
 //                 and dipole structure factors (:951-1245)
 //   k_torque2force  torques mapped onto the H-O-H sites
 //                 (Multipole::torques2forces, :1946-2134)
-// All sums are FP64; forces and torques accumulate in 64-bit fixed point.
+// The FP64 path computes in FP64; the mixed path (k_mp_real_f) keeps the
+// radial factors and the charge-charge term in FP64 and the multipole
+// algebra in FP32.  Forces and torques accumulate in 64-bit fixed point.
 #include "smd_ctx.cuh"
 #include "smd_polar.cuh"
 
@@ -106,44 +108,48 @@ void launch_frames(Ctx &c) {
 // ---------------------------------------------------------------------------
 // pair invariants of the multipole-multipole interaction (r = r_i - r_j)
 // ---------------------------------------------------------------------------
+template <class R, class V>
 struct MPPair {
-    double G[5];
-    V3 gG[5];   // gradients of G1..G4 (gG[0] unused)
+    R G[5];
+    V gG[5];   // gradients of G1..G4 (gG[0] unused)
 };
 
-__device__ __forceinline__ void mp_invariants(double qi, V3 mi, const Q6 &Qi, double qj, V3 mj,
-                                              const Q6 &Qj, V3 r, MPPair &P) {
-    const double QiI = qtr(Qi), QjI = qtr(Qj);
-    const V3 Qir = qv(Qi, r), Qjr = qv(Qj, r);
-    const double QiRij = dot(r, Qir), QjRij = dot(r, Qjr);
-    const double mir = dot(mi, r), mjr = dot(mj, r);
+// The invariants and torque coefficients are written once for the FP64 path
+// (V3, Q6, double) and the mixed path's FP32 algebra (F3, Q6F, float).
+template <class R, class V, class Q>
+__device__ __forceinline__ void mp_invariants(R qi, V mi, const Q &Qi, R qj, V mj, const Q &Qj, V r,
+                                              MPPair<R, V> &P) {
+    const R QiI = qtr(Qi), QjI = qtr(Qj);
+    const V Qir = qv(Qi, r), Qjr = qv(Qj, r);
+    const R QiRij = dot(r, Qir), QjRij = dot(r, Qjr);
+    const R mir = dot(mi, r), mjr = dot(mj, r);
     P.G[0] = qi * qj;
     P.G[1] = qj * mir - qi * mjr - dot(mi, mj) + qj * QiI + qi * QjI;
-    P.G[2] = qj * QiRij + qi * QjRij - mir * mjr - mjr * QiI + mir * QjI - 2 * dot(mj, Qir) +
-             2 * dot(mi, Qjr) + QiI * QjI + 2 * qdd(Qi, Qj);
-    P.G[3] = mir * QjRij - mjr * QiRij + QiI * QjRij + QjI * QiRij + 4 * dot(Qir, Qjr);
+    P.G[2] = qj * QiRij + qi * QjRij - mir * mjr - mjr * QiI + mir * QjI - R(2) * dot(mj, Qir) +
+             R(2) * dot(mi, Qjr) + QiI * QjI + R(2) * qdd(Qi, Qj);
+    P.G[3] = mir * QjRij - mjr * QiRij + QiI * QjRij + QjI * QiRij + R(4) * dot(Qir, Qjr);
     P.G[4] = QiRij * QjRij;
     P.gG[1] = qj * mi - qi * mj;
-    P.gG[2] = (2 * qj) * Qir - mjr * mi - mir * mj - 2.0 * qv(Qi, mj) - QiI * mj + (2 * qi) * Qjr +
-              2.0 * qv(Qj, mi) + QjI * mi;
-    P.gG[3] = (-QiRij) * mj - (2 * mjr) * Qir + QjRij * mi + (2 * mir) * Qjr + (2 * QiI) * Qjr +
-              (2 * QjI) * Qir + 4.0 * qv(Qi, Qjr) + 4.0 * qv(Qj, Qir);
-    P.gG[4] = (2 * QjRij) * Qir + (2 * QiRij) * Qjr;
+    P.gG[2] = (R(2) * qj) * Qir - mjr * mi - mir * mj - R(2) * qv(Qi, mj) - QiI * mj + (R(2) * qi) * Qjr +
+              R(2) * qv(Qj, mi) + QjI * mi;
+    P.gG[3] = (-QiRij) * mj - (R(2) * mjr) * Qir + QjRij * mi + (R(2) * mir) * Qjr + (R(2) * QiI) * Qjr +
+              (R(2) * QjI) * Qir + R(4) * qv(Qi, Qjr) + R(4) * qv(Qj, Qir);
+    P.gG[4] = (R(2) * QjRij) * Qir + (R(2) * QiRij) * Qjr;
 }
 
 // torque coefficients on site i (Multipole.cpp real_term, Gt1i..Gt4i)
-__device__ __forceinline__ void mp_torque_i(double qj, V3 mi, const Q6 &Qi, V3 mj, const Q6 &Qj,
-                                            V3 r, V3 Gt[5]) {
-    const V3 Qir = qv(Qi, r), Qjr = qv(Qj, r);
-    const double QjI = qtr(Qj), QjRij = dot(r, Qjr), mjr = dot(mj, r);
-    const V3 rxmi = crs(r, mi);
-    const V3 RxQi = crs(r, Qir);
+template <class R, class V, class Q>
+__device__ __forceinline__ void mp_torque_i(R qj, V mi, const Q &Qi, V mj, const Q &Qj, V r, V Gt[5]) {
+    const V Qir = qv(Qi, r), Qjr = qv(Qj, r);
+    const R QjI = qtr(Qj), QjRij = dot(r, Qjr), mjr = dot(mj, r);
+    const V rxmi = crs(r, mi);
+    const V RxQi = crs(r, Qir);
     Gt[1] = qj * rxmi - crs(mj, mi);
-    Gt[2] = (-mjr) * rxmi + 2.0 * crs(Qjr, mi) + QjI * rxmi + (2 * qj) * RxQi -
-            2.0 * crs(mj, Qir) - 2.0 * crs(r, qv(Qi, mj)) + 4.0 * qcross(Qj, Qi);
-    Gt[3] = QjRij * rxmi - (2 * mjr) * RxQi + (2 * QjI) * RxQi + 4.0 * crs(r, qv(Qi, Qjr)) +
-            4.0 * crs(Qjr, Qir);
-    Gt[4] = (2 * QjRij) * RxQi;
+    Gt[2] = (-mjr) * rxmi + R(2) * crs(Qjr, mi) + QjI * rxmi + (R(2) * qj) * RxQi -
+            R(2) * crs(mj, Qir) - R(2) * crs(r, qv(Qi, mj)) + R(4) * qcross(Qj, Qi);
+    Gt[3] = QjRij * rxmi - (R(2) * mjr) * RxQi + (R(2) * QjI) * RxQi + R(4) * crs(r, qv(Qi, Qjr)) +
+            R(4) * crs(Qjr, Qir);
+    Gt[4] = (R(2) * QjRij) * RxQi;
 }
 
 // B_n of erfc(a r)/r (Multipole.cpp:632-637); D_n of erf(a r)/r (:1495-1500)
@@ -179,6 +185,8 @@ struct MPArgs {
     Box box;
     double alpha, rc2;
     long long *frc, *trq, *acc;
+    const int4 *fixq;      // mixed path: box fractions
+    double dscale[3];      // L / 2^32 per axis
 };
 
 template <int TPP>
@@ -204,7 +212,7 @@ __global__ void __launch_bounds__(128, 3) k_mp_real(MPArgs a) {
             const double qj = a.tq[(int)pj.w] / SQRTCOULOMB;
             const V3 mj = ld3(a.mu, a.n, j);
             const Q6 Qj = ldq(a.qd, a.n, j);
-            MPPair P;
+            MPPair<double, V3> P;
             mp_invariants(qi, mi, Qi, qj, mj, Qj, r, P);
             double B[6];
             bn_erfc(r2, a.alpha, B);
@@ -243,6 +251,82 @@ __global__ void __launch_bounds__(128, 3) k_mp_real(MPArgs a) {
     }
 }
 
+// Mixed path: displacement from the box fractions (exact integer difference,
+// r^2 from the 64-bit integer sum), the multipole invariants, their
+// gradients and the torque coefficients in FP32; the B_n, the charge-charge
+// term q_i q_j B_n, the energy and the force assembly in FP64 (cubic boxes).
+template <int TPP>
+__global__ void __launch_bounds__(128, 3) k_mp_real_f(MPArgs a) {
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gt / TPP, t = gt % TPP;
+    V3 f = v3(0, 0, 0), tau = v3(0, 0, 0);
+    double en = 0, w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (i < a.n) {
+        const int4 fi = a.fixq[i];
+        const double qi_d = a.tq[fi.w] / SQRTCOULOMB;
+        const float qi = (float)qi_d;
+        const F3 mi = f3((float)a.mu[i], (float)a.mu[a.n + i], (float)a.mu[2 * a.n + i]);
+        const Q6F Qi = {(float)a.qd[i], (float)a.qd[a.n + i], (float)a.qd[2 * a.n + i],
+                        (float)a.qd[3 * a.n + i], (float)a.qd[4 * a.n + i], (float)a.qd[5 * a.n + i]};
+        const double s2u = a.dscale[0] * a.dscale[0];
+        const int cnt = a.nnbr[i];
+        for (int k = t; k < cnt; k += TPP) {
+            const int j = a.nbr[(size_t)k * a.n + i] & 0x7fffffff;
+            const int4 fj = a.fixq[j];
+            const int ix = fi.x - fj.x, iy = fi.y - fj.y, iz = fi.z - fj.z;   // r = r_i - r_j
+            const unsigned long long s2 = (unsigned long long)((long long)ix * ix) +
+                                          (unsigned long long)((long long)iy * iy) +
+                                          (unsigned long long)((long long)iz * iz);
+            const double r2 = (double)s2 * s2u;
+            if (!(r2 < a.rc2)) continue;
+            const V3 r = v3(ix * a.dscale[0], iy * a.dscale[1], iz * a.dscale[2]);
+            const F3 rf = f3((float)r.x, (float)r.y, (float)r.z);
+            const double qj_d = a.tq[fj.w] / SQRTCOULOMB;
+            const float qj = (float)qj_d;
+            const F3 mj = f3((float)a.mu[j], (float)a.mu[a.n + j], (float)a.mu[2 * a.n + j]);
+            const Q6F Qj = {(float)a.qd[j], (float)a.qd[a.n + j], (float)a.qd[2 * a.n + j],
+                            (float)a.qd[3 * a.n + j], (float)a.qd[4 * a.n + j], (float)a.qd[5 * a.n + j]};
+            MPPair<float, F3> P;
+            mp_invariants(qi, mi, Qi, qj, mj, Qj, rf, P);
+            double B[6];
+            bn_erfc(r2, a.alpha, B);
+            const double G0 = qi_d * qj_d;
+            en += G0 * B[0] + P.G[1] * B[1] + P.G[2] * B[2] + P.G[3] * B[3] + P.G[4] * B[4];
+            const double radial = G0 * B[1] + P.G[1] * B[2] + P.G[2] * B[3] + P.G[3] * B[4] + P.G[4] * B[5];
+            const V3 fij = -(B[1] * to_v3(P.gG[1]) + B[2] * to_v3(P.gG[2]) + B[3] * to_v3(P.gG[3]) +
+                             B[4] * to_v3(P.gG[4])) -
+                           radial * r;
+            f = f + fij;
+            const double fr[3] = {fij.x, fij.y, fij.z}, rr[3] = {r.x, r.y, r.z};
+            for (int p = 0; p < 3; p++)
+                for (int q = 0; q < 3; q++) w[3 * p + q] -= 0.5 * fr[q] * rr[p];
+            F3 Gt[5];
+            mp_torque_i(qj, mi, Qi, mj, Qj, rf, Gt);
+            tau = tau + (B[1] * to_v3(Gt[1]) + B[2] * to_v3(Gt[2]) + B[3] * to_v3(Gt[3]) + B[4] * to_v3(Gt[4]));
+        }
+    }
+    f.x = group_sum<TPP>(f.x); f.y = group_sum<TPP>(f.y); f.z = group_sum<TPP>(f.z);
+    tau.x = group_sum<TPP>(tau.x); tau.y = group_sum<TPP>(tau.y); tau.z = group_sum<TPP>(tau.z);
+    if (i < a.n && t == 0) {
+        add_fix3(a.frc, a.n, i, f, COULOMBS);
+        add_fix3(a.trq, a.n, i, tau, COULOMBS);
+    }
+    __shared__ double s_r[8][10];
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    double vals[10] = {0.5 * en * COULOMBS, w[0], w[1], w[2], w[3], w[4], w[5], w[6], w[7], w[8]};
+    for (int q = 0; q < 10; q++) {
+        double sv = warp_sum(vals[q]);
+        if (lane == 0) s_r[wp][q] = sv;
+    }
+    __syncthreads();
+    if (threadIdx.x < 10) {
+        double sv = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) sv += s_r[q][threadIdx.x];
+        const int slot = threadIdx.x == 0 ? ACC_E_REAL : ACC_VIR + threadIdx.x - 1;
+        if (sv != 0.0) atomicAdd((unsigned long long *)&a.acc[slot], (unsigned long long)to_fix(sv, ACC_SCALE));
+    }
+}
+
 // ---------------------------------------------------------------------------
 // self energy and intramolecular correction (energy only: rigid molecules)
 // ---------------------------------------------------------------------------
@@ -274,7 +358,7 @@ __global__ void k_mp_mol(int nmol, int n, const int *mol_off, const int *mol_ato
                 V3 r = v3(pbc1(pi.x - pj.x, box.L[0], box.half[0]), pbc1(pi.y - pj.y, box.L[1], box.half[1]),
                           pbc1(pi.z - pj.z, box.L[2], box.half[2]));
                 const double r2 = dot(r, r);
-                MPPair P;
+                MPPair<double, V3> P;
                 mp_invariants(qi, mi, Qi, tq[(int)pj.w] / SQRTCOULOMB, ld3(mu, n, j), ldq(qd, n, j), r, P);
                 double D[6];
                 dn_erf(r2, alpha, D);
@@ -367,7 +451,15 @@ void launch_mp_short(Ctx &c) {
     // 128-thread blocks: at this kernel's register count the SM holds more
     // warps in small blocks than in one 256-thread block
     const int nb = (int)(((long long)c.n * tpp + 127) / 128);
-    k_mp_real<tpp><<<nb, 128, 0, c.stream>>>(a);
+    const bool cubic = c.box.L[0] == c.box.L[1] && c.box.L[1] == c.box.L[2];
+    if (c.precision == SMD_PREC_MIXED && cubic) {
+        if (!c.fixq_from_integrate) launch_fixq(c);
+        a.fixq = c.fixq;
+        for (int d = 0; d < 3; d++) a.dscale[d] = c.box.L[d] / 4294967296.0;
+        k_mp_real_f<tpp><<<nb, 128, 0, c.stream>>>(a);
+    } else {
+        k_mp_real<tpp><<<nb, 128, 0, c.stream>>>(a);
+    }
     k_mp_mol<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.n, c.mol_off, c.mol_atoms, c.excl_off,
                                                          c.excl, c.pos4, c.type_q, c.mu, c.qd, c.box,
                                                          c.ew_alpha, c.acc);

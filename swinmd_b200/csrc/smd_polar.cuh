@@ -37,6 +37,37 @@ __device__ __forceinline__ V3 qcross(const Q6 &a, const Q6 &b) {
     return crs(a0, b0) + crs(a1, b1) + crs(a2, b2);
 }
 
+// FP32 counterparts for the mixed-precision pair algebra
+struct F3 {
+    float x, y, z;
+};
+__device__ __forceinline__ F3 f3(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ F3 operator+(F3 a, F3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ F3 operator-(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ F3 operator-(F3 a) { return {-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ F3 operator*(float s, F3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ float dot(F3 a, F3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
+__device__ __forceinline__ F3 crs(F3 a, F3 b) {
+    return {a.y * b.z - b.y * a.z, b.x * a.z - a.x * b.z, a.x * b.y - b.x * a.y};
+}
+struct Q6F {
+    float xx, xy, xz, yy, yz, zz;
+};
+__device__ __forceinline__ F3 qv(const Q6F &q, F3 r) {
+    return {fmaf(q.xx, r.x, fmaf(q.xy, r.y, q.xz * r.z)), fmaf(q.xy, r.x, fmaf(q.yy, r.y, q.yz * r.z)),
+            fmaf(q.xz, r.x, fmaf(q.yz, r.y, q.zz * r.z))};
+}
+__device__ __forceinline__ float qtr(const Q6F &q) { return q.xx + q.yy + q.zz; }
+__device__ __forceinline__ float qdd(const Q6F &a, const Q6F &b) {
+    return a.xx * b.xx + a.yy * b.yy + a.zz * b.zz + 2.f * (a.xy * b.xy + a.xz * b.xz + a.yz * b.yz);
+}
+__device__ __forceinline__ F3 qcross(const Q6F &a, const Q6F &b) {
+    F3 a0 = f3(a.xx, a.xy, a.xz), a1 = f3(a.xy, a.yy, a.yz), a2 = f3(a.xz, a.yz, a.zz);
+    F3 b0 = f3(b.xx, b.xy, b.xz), b1 = f3(b.xy, b.yy, b.yz), b2 = f3(b.xz, b.yz, b.zz);
+    return crs(a0, b0) + crs(a1, b1) + crs(a2, b2);
+}
+__device__ __forceinline__ V3 to_v3(F3 a) { return v3(a.x, a.y, a.z); }
+
 __device__ __forceinline__ void add_fix3(long long *arr, int n, int i, V3 v, double s) {
     arr[i] += to_fix(s * v.x, FRC_SCALE);
     arr[n + i] += to_fix(s * v.y, FRC_SCALE);
