@@ -485,14 +485,16 @@ def main():
     if os.path.exists(PEAKS):
         peaks.update(json.load(open(PEAKS)))
         peak_src = "measured"
-    # dominant stage of the fast arm: the reciprocal sums and forces of the
-    # permanent and induced multipoles (FP32 SIMT work, a few MB of traffic):
-    # 35 flop per (site, k) in the sums pass and 65 in the force pass, a phase
-    # counted as 1; the peak is the nominal FP32 rate of 148 SMs x 128 lanes
-    # at the measured maximum SM clock
+    # the reciprocal sums and forces of the permanent and induced multipoles
+    # (FP32 SIMT work, a few MB of traffic), counted as the FP32 operations
+    # of the column formulation (an FMA is 2): 33 per (site, k) in the sums
+    # pass (27 per k plus the run's shared 22 over 3.7 k) and 26 in the force
+    # pass (24 per k plus the column fold, 42 over 24 k); the peak
+    # is the nominal FP32 rate of 148 SMs x 128 lanes at the measured maximum
+    # SM clock
     dom = max(stage_ms, key=stage_ms.get)
     nk = ens.ewald_nk() if polar else 0
-    flops = float(nk) * n * (35 + 65)
+    flops = float(nk) * n * (33 + 26)
     sm_mhz = peaks.get("sm_max_mhz", 1965.0)
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
     rstage = "polar_recip" if polar else "pair"
@@ -532,8 +534,9 @@ def main():
                "kernels_per_step": kc.value,
                "stage_ms_fast": stage_ms, "stage_ms_plain": stage_plain,
                "list_updates": int(o_end.list_updates),
-               "roofline": {"bound": "fp32", "kernel": "k_rsk_tab<2> + k_rforce_col<1> (reciprocal sums "
-                                                      "and forces of the permanent + induced multipoles)",
+               "roofline": {"bound": "fp32", "kernel": "k_rsk_seg<2,4> + k_rforce_grp<1> (reciprocal "
+                                                      "sums and forces of the permanent + induced "
+                                                      "multipoles)",
                             "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                             "frac": achieved / fp32_peak if achieved else None,
                             "alg_flops_per_step": flops, "k_vectors": nk,

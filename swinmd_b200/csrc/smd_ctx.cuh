@@ -41,10 +41,16 @@ struct Recip {               // Ewald reciprocal space (k half-space, k^2 < kcut
     long long *sk = nullptr; // [2][nk] structure factor, fixed point (SK_SCALE)
     double *kvec = nullptr;  // [3][nk] k in 1/nm
     int nmax = 0;            // largest |n| of any component
-    // FP32 force pass of the polarisable model: per k (nx, ny, nz, offset in
-    // its column) and (kx, ky, kz, 2c)
-    int4 *kpack = nullptr;
-    float4 *kb4 = nullptr;
+    // FP32 passes of the polarisable model (built once per k set; the k list
+    // is ordered column by column, nz ascending by one within a column)
+    int nseg = 0, ncol = 0, ngrp = 0, row = 0, tab_n = 0;
+    int4 *kseg = nullptr;    // sums pass: runs of <= 4 k of one column (first k, count, nx | ny << 16, first nz)
+    int4 *kcol = nullptr;    // force pass: columns (first k, length, nx | ny << 16, first nz)
+    int4 *kgrp = nullptr;    // force pass: groups of whole columns (first column, columns, first k, k count)
+    float4 *kzr = nullptr;   // per k (kz, kz^2, 2c, 0)
+    float2 *kcxy = nullptr;  // per column (kx, ky)
+    float2 *stab = nullptr;  // per site phase tables [n][row]: e^{2 pi i m f / 2^32}, m < nmax + 1, per axis
+    float4 *ssv = nullptr;   // per site values [n][4]: q, mu, Q (6), p
 };
 
 struct Ctx {

@@ -473,25 +473,39 @@ __global__ void __launch_bounds__(256) k_rforce_f(int n, int nk, const double4 *
 // FP32 passes of the mixed path
 // ---------------------------------------------------------------------------
 // The k list is stored column by column: nx, then ny, then nz ascending by
-// one within a column.  Every phase factor below comes from exact integer
-// phases (sincos_phase32) with at most two complex products after them.
+// one within a column.  The box is orthorhombic, so kx and ky are fixed
+// within a column and every k-dependent weight is a polynomial in kz:
+//   q - k.Q.k = a + kz (b + c kz),  a = q - Qxx kx^2 - 2 Qxy kx ky - Qyy ky^2,
+//                                  b = -2 (Qxz kx + Qyz ky),  c = -Qzz
+//   mu.k      = d + e kz,           d = mux kx + muy ky,  e = muz
+// Every phase factor comes from exact integer phases (sincos_phase32) with
+// at most two complex products after them.
 //
-// Sums pass (one thread per k, site tiles in shared memory): each site of a
-// tile gets a table e^{2 pi i m f / 2^32}, m = 0 .. nt-1, per axis; the phase
-// factor of k = (nx, ny, nz) is X[nx] Y[|ny|] Z[|nz|], conjugated for
-// negative components (nx >= 0 in the half space).
+// Site tables (one pass per evaluation): per site and axis the factors
+// e^{2 pi i m f / 2^32}, m = 0 .. nmax, and the site's q, mu, Q, p in FP32.
 //
-// Force pass (one thread per site walking the k list): the factor of the
-// first k of a column comes from its exact phase, the others in the column
-// are that times the site's table entry e^{2 pi i m fz / 2^32}, m the offset
-// in the column.  All lanes read the same k record (shared-memory broadcast);
-// each lane's table row is at an odd stride, so the table reads of a warp
-// fall in distinct banks.
+// Sums pass: one thread per run of up to TS_SEG k of one column, sites
+// staged in shared memory tile by tile.  Per site a run shares X[nx] Y[|ny|]
+// and the column parts a, b, d of the weights; per k it takes Z[|nz|]
+// (conjugated for negative components) and two FMAs per weight.
+//
+// Force pass: one thread per site walking whole columns.  The factor of a
+// column's first k comes from its exact phase, the others are that times the
+// site's e^{2 pi i m fz / 2^32}, m the offset in the column.  With U', W' the
+// combined structure factors times 2c, A = sin U' - cos W' and
+// B = cos U' + sin W', a column accumulates only sum A kz^j (j = 0..3) and
+// sum B kz^j (j = 0..2); at its end these fold into the moments
+//   M1_a = sum A k_a,  M2_ab = sum B k_a k_b,  M3_abc = sum A k_a k_b k_c
+// (FP64 across column groups), which give at the end
+//   force   F_a = q M1_a - Q_bc M3_abc + (mu + p)_b M2_ab
+//   torque  mu x M1 - 2 g,  g_a = eps_abc (Q M2)_cb.
 constexpr int TAB_MAX = 32;     // |n| < TAB_MAX
-constexpr int TS_THREADS = 256; // k per block, sums pass
-constexpr int TS_SITES = 128;   // sites per tile, sums pass
+constexpr int TS_THREADS = 128; // runs per block, sums pass
+constexpr int TS_SITES = 64;    // sites per tile, sums pass
+constexpr int TS_SEG = 4;       // k per run, sums pass
 constexpr int CF_THREADS = 128; // sites per block, force pass
-constexpr int CF_KTILE = 256;
+constexpr int CF_KGROUP = 256;  // k per column group at most, force pass
+constexpr int CF_CGROUP = 64;   // columns per group at most
 
 __device__ __forceinline__ float2 table_entry(int m, unsigned f) {
     float sn, cs;
@@ -499,204 +513,303 @@ __device__ __forceinline__ float2 table_entry(int m, unsigned f) {
     return make_float2(cs, sn);
 }
 
-// offsets of k's three entries in a site table, sign bits of ny and nz
-__device__ __forceinline__ int4 table_offsets(int nx, int ny, int nz, int nt) {
-    return make_int4(nx, nt + (ny < 0 ? -ny : ny), 2 * nt + (nz < 0 ? -nz : nz), (ny < 0 ? 1 : 0) | (nz < 0 ? 2 : 0));
+// site tables [n][row]: X[0..nt), Y[0..nt), Z[0..nt), zero padding to an
+// even row; site values [n][4]: (q, mux, muy, muz), (Qxx, Qxy, Qxz, Qyy),
+// (Qyz, Qzz, px, py), (pz, 0, 0, 0)
+__global__ void k_site_tab(int n, int nt, int row, int with_p, const double4 *pos4, const int4 *fixq,
+                           const double *tq, const double *mu, const double *qd, const double *pind,
+                           float2 *stab, float4 *ssv) {
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long ntab = (long long)n * row;
+    if (e < ntab) {
+        const int i = (int)(e / row), r = (int)(e - (long long)i * row);
+        const int ax = r / nt, m = r - ax * nt;
+        float2 v = make_float2(0.f, 0.f);
+        if (ax < 3) {
+            const int4 f = fixq[i];
+            v = table_entry(m, (unsigned)(ax == 0 ? f.x : (ax == 1 ? f.y : f.z)));
+        }
+        stab[e] = v;
+    } else if (e < ntab + n) {
+        const int i = (int)(e - ntab);
+        const size_t N = (size_t)n;
+        float p[3] = {0.f, 0.f, 0.f};
+        if (with_p)
+            for (int d = 0; d < 3; d++) p[d] = (float)pind[d * N + i];
+        ssv[4 * (size_t)i] = make_float4((float)(tq[(int)pos4[i].w] / SQC_R), (float)mu[i], (float)mu[N + i],
+                                         (float)mu[2 * N + i]);
+        ssv[4 * (size_t)i + 1] = make_float4((float)qd[i], (float)qd[N + i], (float)qd[2 * N + i], (float)qd[3 * N + i]);
+        ssv[4 * (size_t)i + 2] = make_float4((float)qd[4 * N + i], (float)qd[5 * N + i], p[0], p[1]);
+        ssv[4 * (size_t)i + 3] = make_float4(p[2], 0.f, 0.f, 0.f);
+    }
 }
 
-__device__ __forceinline__ void table_phase(const float2 *tab, int4 o, float &sn, float &cs) {
-    const float2 X = tab[o.x], Y = tab[o.y], Z = tab[o.z];
-    const float yi = (o.w & 1) ? -Y.y : Y.y, zi = (o.w & 2) ? -Z.y : Z.y;
-    const float xr = fmaf(X.x, Y.x, -X.y * yi), xi = fmaf(X.x, yi, X.y * Y.x);
-    cs = fmaf(xr, Z.x, -xi * zi);
-    sn = fmaf(xr, zi, xi * Z.x);
-}
-
-// site data of a tile: (q, mu), (Qxx, Qxy, Qxz, Qyy), (Qyz, Qzz, px, py), (pz)
-template <int MODE>
-__global__ void __launch_bounds__(TS_THREADS) k_rsk_tab(int n, int nk, int nt, const double4 *pos4,
-                                                        const int4 *fixq, const int *kn, const double *kvec,
-                                                        const double *tq, const double *mu, const double *qd,
-                                                        const double *pind, double *partial) {
+// MODE 0: permanent sums (slots 0-3); 1: induced sums (4-5); 2: all six.
+// kseg[s] = (first k, count, nx | ny << 16, first nz)
+template <int MODE, int SEG>
+__global__ void __launch_bounds__(TS_THREADS) k_rsk_seg(int n, int nk, int nseg, int nt, int row,
+                                                        const int4 *kseg, const double *kvec,
+                                                        const float2 *stab, const float4 *ssv, double *partial) {
     constexpr bool PERM = MODE != 1, IND = MODE != 0;
     extern __shared__ float4 s_dyn4[];
-    float4 *s_v = s_dyn4;                                  // [TS_SITES][4]
-    float2 *s_tab = (float2 *)(s_v + 4 * TS_SITES);        // [TS_SITES][3 nt]
-    const int k = blockIdx.x * TS_THREADS + threadIdx.x;
+    float4 *s_v = s_dyn4;                              // [TS_SITES][4]
+    float2 *s_tab = (float2 *)(s_v + 4 * TS_SITES);    // [TS_SITES][row]
+    const int sid = blockIdx.x * TS_THREADS + threadIdx.x;
+    const bool own = sid < nseg;
     const int ch = blockIdx.y;
     const int per = (n + gridDim.y - 1) / gridDim.y;
     const int s0 = ch * per, s1 = min(n, s0 + per);
-    float kx = 0.f, ky = 0.f, kz = 0.f;
-    int4 o = make_int4(0, 0, 0, 0);
-    if (k < nk) {
-        kx = (float)kvec[k]; ky = (float)kvec[nk + k]; kz = (float)kvec[2 * nk + k];
-        o = table_offsets(kn[k], kn[nk + k], kn[2 * nk + k], nt);
+    const int4 sg = own ? kseg[sid] : make_int4(0, 0, 0, 0);
+    const int nx = (short)(sg.z & 0xffff), ny = sg.z >> 16;
+    float kx = 0.f, ky = 0.f;
+    if (own) {
+        kx = (float)kvec[sg.x];
+        ky = (float)kvec[nk + sg.x];
     }
-    const float k0 = kx * kx, k1 = 2.f * kx * ky, k2 = 2.f * kx * kz, k3 = ky * ky, k4 = 2.f * ky * kz, k5 = kz * kz;
-    const int row = 3 * nt;
-    double acc[6] = {0, 0, 0, 0, 0, 0};
+    float kz[SEG], zsg[SEG];
+    int oz[SEG];
+#pragma unroll
+    for (int j = 0; j < SEG; j++) {
+        const bool v = j < sg.y;
+        const int nz = sg.w + j;
+        kz[j] = v ? (float)kvec[2 * (size_t)nk + sg.x + j] : 0.f;
+        oz[j] = 2 * nt + (v ? (nz < 0 ? -nz : nz) : 0);
+        zsg[j] = nz < 0 ? -1.f : 1.f;
+    }
+    const int ox = nx, oy = nt + (ny < 0 ? -ny : ny);
+    const float ysg = ny < 0 ? -1.f : 1.f;
+    const float kxx = kx * kx, kxy2 = 2.f * kx * ky, kyy = ky * ky, kx2 = 2.f * kx, ky2 = 2.f * ky;
+    double acc[SEG][6];
+#pragma unroll
+    for (int j = 0; j < SEG; j++)
+#pragma unroll
+        for (int q = 0; q < 6; q++) acc[j][q] = 0.0;
     for (int base = s0; base < s1; base += TS_SITES) {
         const int cnt = min(TS_SITES, s1 - base);
         __syncthreads();
-        for (int e = threadIdx.x; e < cnt * row; e += TS_THREADS) {
-            const int sl = e / row, r = e - sl * row, ax = r / nt, m = r - ax * nt;
-            const int4 f = fixq[base + sl];
-            s_tab[e] = table_entry(m, (unsigned)(ax == 0 ? f.x : (ax == 1 ? f.y : f.z)));
-        }
-        if (threadIdx.x < cnt) {
-            const int i = base + threadIdx.x;
-            float v[16] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            if (PERM) {
-                v[0] = (float)(tq[(int)pos4[i].w] / SQC_R);
-                for (int d = 0; d < 3; d++) v[1 + d] = (float)mu[(size_t)d * n + i];
-                for (int d = 0; d < 6; d++) v[4 + d] = (float)qd[(size_t)d * n + i];
-            }
-            if (IND)
-                for (int d = 0; d < 3; d++) v[10 + d] = (float)pind[(size_t)d * n + i];
-            for (int w = 0; w < 4; w++)
-                s_v[threadIdx.x * 4 + w] = make_float4(v[4 * w], v[4 * w + 1], v[4 * w + 2], v[4 * w + 3]);
+        {
+            // row is even, so every site's row starts on a 16-byte boundary
+            // and a tile is a whole number of float4s
+            const float4 *src = (const float4 *)(stab + (size_t)base * row);
+            float4 *dst = (float4 *)s_tab;
+            const int nv = cnt * row / 2;
+            for (int e = threadIdx.x; e < nv; e += TS_THREADS) dst[e] = src[e];
+            const float4 *sv = ssv + (size_t)base * 4;
+            for (int e = threadIdx.x; e < cnt * 4; e += TS_THREADS) s_v[e] = sv[e];
         }
         __syncthreads();
-        if (k < nk) {
-            float t0 = 0.f, t1 = 0.f, t2 = 0.f, t3 = 0.f, t4 = 0.f, t5 = 0.f;
-#pragma unroll 4
-            for (int q = 0; q < cnt; q++) {
-                float sn, cs;
-                table_phase(s_tab + q * row, o, sn, cs);
+        float t[SEG][6];
+#pragma unroll
+        for (int j = 0; j < SEG; j++)
+#pragma unroll
+            for (int q = 0; q < 6; q++) t[j][q] = 0.f;
+        const float2 *tp = s_tab;
+        for (int q = 0; q < cnt; q++, tp += row) {
+            const float2 X = tp[ox], Y = tp[oy];
+            const float yi = Y.y * ysg;
+            const float xr = fmaf(X.x, Y.x, -X.y * yi), xi = fmaf(X.x, yi, X.y * Y.x);
+            float a = 0.f, b = 0.f, c = 0.f, d = 0.f, e = 0.f, pd = 0.f, pe = 0.f;
+            if (PERM) {
+                const float4 v0 = s_v[q * 4], v1 = s_v[q * 4 + 1], v2 = s_v[q * 4 + 2];
+                a = v0.x - fmaf(v1.x, kxx, fmaf(v1.y, kxy2, v1.w * kyy));
+                b = -fmaf(v1.z, kx2, v2.x * ky2);
+                c = -v2.y;
+                d = fmaf(v0.y, kx, v0.z * ky);
+                e = v0.w;
+            }
+            if (IND) {
+                const float4 v2 = s_v[q * 4 + 2], v3 = s_v[q * 4 + 3];
+                pd = fmaf(v2.z, kx, v2.w * ky);
+                pe = v3.x;
+            }
+#pragma unroll
+            for (int j = 0; j < SEG; j++) {
+                const float2 Z = tp[oz[j]];
+                const float zi = Z.y * zsg[j];
+                const float cs = fmaf(xr, Z.x, -xi * zi), sn = fmaf(xr, zi, xi * Z.x);
                 if (PERM) {
-                    const float4 a = s_v[q * 4], b = s_v[q * 4 + 1], c = s_v[q * 4 + 2];
-                    float kqk = b.x * k0;
-                    kqk = fmaf(b.y, k1, kqk);
-                    kqk = fmaf(b.z, k2, kqk);
-                    kqk = fmaf(b.w, k3, kqk);
-                    kqk = fmaf(c.x, k4, kqk);
-                    kqk = fmaf(c.y, k5, kqk);
-                    const float qk = a.x - kqk;
-                    const float mk = fmaf(a.y, kx, fmaf(a.z, ky, a.w * kz));
-                    t0 = fmaf(qk, cs, t0); t1 = fmaf(qk, sn, t1);
-                    t2 = fmaf(mk, cs, t2); t3 = fmaf(mk, sn, t3);
+                    const float w = fmaf(kz[j], fmaf(c, kz[j], b), a);
+                    const float m = fmaf(e, kz[j], d);
+                    t[j][0] = fmaf(w, cs, t[j][0]); t[j][1] = fmaf(w, sn, t[j][1]);
+                    t[j][2] = fmaf(m, cs, t[j][2]); t[j][3] = fmaf(m, sn, t[j][3]);
                 }
                 if (IND) {
-                    const float4 c = s_v[q * 4 + 2], d = s_v[q * 4 + 3];
-                    const float pk = fmaf(c.z, kx, fmaf(c.w, ky, d.x * kz));
-                    t4 = fmaf(pk, cs, t4); t5 = fmaf(pk, sn, t5);
+                    const float p = fmaf(pe, kz[j], pd);
+                    t[j][4] = fmaf(p, cs, t[j][4]); t[j][5] = fmaf(p, sn, t[j][5]);
                 }
             }
-            acc[0] += t0; acc[1] += t1; acc[2] += t2; acc[3] += t3; acc[4] += t4; acc[5] += t5;
         }
+#pragma unroll
+        for (int j = 0; j < SEG; j++)
+#pragma unroll
+            for (int q = 0; q < 6; q++) acc[j][q] += t[j][q];
     }
-    if (k < nk) {
+    if (own) {
         double *pb = partial + (size_t)ch * 6 * nk;
-        if (PERM)
-            for (int q = 0; q < 4; q++) pb[(size_t)q * nk + k] = acc[q];
-        if (IND)
-            for (int q = 4; q < 6; q++) pb[(size_t)q * nk + k] = acc[q];
+#pragma unroll
+        for (int j = 0; j < SEG; j++) {
+            if (j >= sg.y) break;
+            const size_t k = (size_t)sg.x + j;
+            if (PERM)
+                for (int q = 0; q < 4; q++) pb[(size_t)q * nk + k] = acc[j][q];
+            if (IND)
+                for (int q = 4; q < 6; q++) pb[(size_t)q * nk + k] = acc[j][q];
+        }
     }
 }
 
-// kpack[k] = (nx, ny, nz, m) with m the offset of k in its column
+// index of the symmetric pair (a, b) in xx xy xz yy yz zz and of the
+// symmetric triple (a, b, c) in xxx xxy xxz xyy xyz xzz yyy yyz yzz zzz
+__device__ __forceinline__ int sym2(int a, int b) {
+    const int lo = a < b ? a : b, hi = a < b ? b : a;
+    return lo == 0 ? hi : (lo == 1 ? 2 + hi : 5);
+}
+__device__ __forceinline__ int sym3(int a, int b, int c) {
+    int x = a, y = b, z = c, t;
+    if (x > y) { t = x; x = y; y = t; }
+    if (y > z) { t = y; y = z; z = t; }
+    if (x > y) { t = x; x = y; y = t; }
+    return x == 0 ? sym2(y, z) : (x == 1 ? 5 + sym2(y, z) - 2 : 9);
+}
+
+// kgrp[g] = (first column, columns, first k, k count); kcol[c] = (first k,
+// length, nx | ny << 16, first nz); kzr[k] = (kz, kz^2, 2c, 0)
 template <bool IND>
-__global__ void __launch_bounds__(CF_THREADS) k_rforce_col(int n, int nk, int zs, const double4 *pos4,
-                                                           const int4 *fixq, const int4 *kpack, const float4 *kb4,
-                                                           const double *sk, const double *tq, const double *mu,
-                                                           const double *qd, const double *pind, long long *frc,
-                                                           long long *trq) {
+__global__ void __launch_bounds__(CF_THREADS) k_rforce_grp(int n, int nk, int zs, int ngrp, const double4 *pos4,
+                                                           const int4 *fixq, const int4 *kgrp, const int4 *kcol,
+                                                           const float2 *kcxy, const float4 *kzr, const double *sk,
+                                                           const double *tq, const double *mu, const double *qd,
+                                                           const double *pind, long long *frc, long long *trq) {
     extern __shared__ float4 s_dyn4[];
-    int4 *s_kp = (int4 *)s_dyn4;                    // [CF_KTILE]
-    float4 *s_kb = (float4 *)(s_kp + CF_KTILE);     // [CF_KTILE]
-    float2 *s_uw = (float2 *)(s_kb + CF_KTILE);     // [CF_KTILE]
-    float2 *s_z = s_uw + CF_KTILE;                  // [CF_THREADS][zs]
+    float4 *s_k = s_dyn4;                           // [CF_KGROUP] (U', W', kz, kz^2)
+    int4 *s_col = (int4 *)(s_k + CF_KGROUP);        // [CF_CGROUP]
+    float2 *s_cxy = (float2 *)(s_col + CF_CGROUP);  // [CF_CGROUP]
+    float2 *s_z = s_cxy + CF_CGROUP;                // [CF_THREADS][zs]
     const int i = blockIdx.x * CF_THREADS + threadIdx.x;
     const bool own = i < n;
-    int4 pf = make_int4(0, 0, 0, 0);
-    float qi = 0.f, dx = 0.f, dy = 0.f, dz = 0.f;
-    float Qxx = 0.f, Qxy = 0.f, Qxz = 0.f, Qyy = 0.f, Qyz = 0.f, Qzz = 0.f;
-    if (own) {
-        pf = fixq[i];
-        qi = (float)(tq[(int)pos4[i].w] / SQC_R);
-        double d3[3] = {mu[i], mu[n + i], mu[2 * n + i]};
-        if (IND)
-            for (int d = 0; d < 3; d++) d3[d] += pind[(size_t)d * n + i];
-        dx = (float)d3[0]; dy = (float)d3[1]; dz = (float)d3[2];
-        Qxx = (float)qd[i]; Qxy = (float)qd[n + i]; Qxz = (float)qd[2 * n + i];
-        Qyy = (float)qd[3 * n + i]; Qyz = (float)qd[4 * n + i]; Qzz = (float)qd[5 * n + i];
-    }
+    const int4 pf = own ? fixq[i] : make_int4(0, 0, 0, 0);
     float2 *zt = s_z + threadIdx.x * zs;
     for (int m = 0; m < zs; m++) zt[m] = table_entry(m, (unsigned)pf.z);
-    double F[3] = {0, 0, 0}, EA[3] = {0, 0, 0}, GX[3] = {0, 0, 0};
-    const int kper = (((nk + gridDim.y - 1) / gridDim.y + CF_KTILE - 1) / CF_KTILE) * CF_KTILE;
-    const int kb0 = blockIdx.y * kper, kb1 = min(nk, kb0 + kper);
-    float c0 = 1.f, s0 = 0.f;   // factor of the current column's first k
-    for (int base = kb0; base < kb1; base += CF_KTILE) {
-        const int cnt = min(CF_KTILE, kb1 - base);
+    double D1[3] = {0, 0, 0}, D2[6] = {0, 0, 0, 0, 0, 0}, D3[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const int gper = (ngrp + gridDim.y - 1) / gridDim.y;
+    const int g0 = blockIdx.y * gper, g1 = min(ngrp, g0 + gper);
+    for (int g = g0; g < g1; g++) {
+        const int4 gr = kgrp[g];
         __syncthreads();
-        for (int e = threadIdx.x; e < cnt; e += CF_THREADS) {
-            const int k = base + e;
-            s_kp[e] = kpack[k];
-            s_kb[e] = kb4[k];
-            const double CqQ = sk[k], SqQ = sk[nk + k], Cm = sk[2 * (size_t)nk + k], Sm = sk[3 * (size_t)nk + k];
-            double U = CqQ - Sm, W = SqQ + Cm;
+        for (int e = threadIdx.x; e < gr.w; e += CF_THREADS) {
+            const size_t k = (size_t)gr.z + e;
+            const float4 r = kzr[k];
+            double U = sk[k] - sk[3 * (size_t)nk + k], W = sk[nk + k] + sk[2 * (size_t)nk + k];
             if (IND) {
                 U -= sk[5 * (size_t)nk + k];
                 W += sk[4 * (size_t)nk + k];
             }
-            s_uw[e] = make_float2((float)U, (float)W);
+            s_k[e] = make_float4((float)(r.z * U), (float)(r.z * W), r.x, r.y);
+        }
+        for (int e = threadIdx.x; e < gr.y; e += CF_THREADS) {
+            int4 cc = kcol[gr.x + e];
+            cc.x -= gr.z;
+            s_col[e] = cc;
+            s_cxy[e] = kcxy[gr.x + e];
         }
         __syncthreads();
-        for (int t0 = 0; t0 < cnt; t0 += 64) {
-            float f0 = 0.f, f1 = 0.f, f2 = 0.f, e0 = 0.f, e1 = 0.f, e2 = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
-            const int t1 = min(cnt, t0 + 64);
-            for (int t = t0; t < t1; t++) {
-                const int4 kp = s_kp[t];
-                if (kp.w == 0 || base + t == kb0) {
-                    const int ph = (int)((unsigned)kp.x * (unsigned)pf.x + (unsigned)kp.y * (unsigned)pf.y +
-                                         (unsigned)(kp.z - kp.w) * (unsigned)pf.z);
-                    sincos_phase32(ph, s0, c0);
-                }
-                const float2 z = zt[kp.w];
+        float M1[3] = {0.f, 0.f, 0.f}, M2[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float M3[10] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        for (int cix = 0; cix < gr.y; cix++) {
+            const int4 cc = s_col[cix];
+            const int nx = (short)(cc.z & 0xffff), ny = cc.z >> 16;
+            float s0, c0;
+            sincos_phase32((int)((unsigned)nx * (unsigned)pf.x + (unsigned)ny * (unsigned)pf.y +
+                                 (unsigned)cc.w * (unsigned)pf.z), s0, c0);
+            float P0 = 0.f, P1 = 0.f, P2 = 0.f, P3 = 0.f, R0 = 0.f, R1 = 0.f, R2 = 0.f;
+            const float4 *kr = s_k + cc.x;
+            for (int m = 0; m < cc.y; m++) {
+                const float4 r = kr[m];
+                const float2 z = zt[m];
                 const float cs = fmaf(c0, z.x, -s0 * z.y), sn = fmaf(c0, z.y, s0 * z.x);
-                const float4 kb = s_kb[t];
-                const float2 uw = s_uw[t];
-                const float A = fmaf(sn, uw.x, -cs * uw.y);
-                const float B = fmaf(cs, uw.x, sn * uw.y);
-                const float qkx = fmaf(Qxx, kb.x, fmaf(Qxy, kb.y, Qxz * kb.z));
-                const float qky = fmaf(Qxy, kb.x, fmaf(Qyy, kb.y, Qyz * kb.z));
-                const float qkz = fmaf(Qxz, kb.x, fmaf(Qyz, kb.y, Qzz * kb.z));
-                const float qk = qi - fmaf(kb.x, qkx, fmaf(kb.y, qky, kb.z * qkz));
-                const float mk = fmaf(dx, kb.x, fmaf(dy, kb.y, dz * kb.z));
-                const float bA = kb.w * A, bB = kb.w * B;
-                const float al = fmaf(qk, bA, mk * bB);
-                f0 = fmaf(al, kb.x, f0); f1 = fmaf(al, kb.y, f1); f2 = fmaf(al, kb.z, f2);
-                e0 = fmaf(bA, kb.x, e0); e1 = fmaf(bA, kb.y, e1); e2 = fmaf(bA, kb.z, e2);
-                g0 = fmaf(bB, fmaf(kb.y, qkz, -kb.z * qky), g0);
-                g1 = fmaf(bB, fmaf(kb.z, qkx, -kb.x * qkz), g1);
-                g2 = fmaf(bB, fmaf(kb.x, qky, -kb.y * qkx), g2);
+                const float A = fmaf(sn, r.x, -cs * r.y), B = fmaf(cs, r.x, sn * r.y);
+                const float Akz = A * r.z;
+                P0 += A; P1 += Akz; P2 = fmaf(A, r.w, P2); P3 = fmaf(Akz, r.w, P3);
+                R0 += B; R1 = fmaf(B, r.z, R1); R2 = fmaf(B, r.w, R2);
             }
-            F[0] += f0; F[1] += f1; F[2] += f2;
-            EA[0] += e0; EA[1] += e1; EA[2] += e2;
-            GX[0] += g0; GX[1] += g1; GX[2] += g2;
+            const float2 kk = s_cxy[cix];
+            const float kx = kk.x, ky = kk.y, kxx = kx * kx, kxy = kx * ky, kyy = ky * ky;
+            M1[0] = fmaf(kx, P0, M1[0]); M1[1] = fmaf(ky, P0, M1[1]); M1[2] += P1;
+            M2[0] = fmaf(kxx, R0, M2[0]); M2[1] = fmaf(kxy, R0, M2[1]); M2[2] = fmaf(kx, R1, M2[2]);
+            M2[3] = fmaf(kyy, R0, M2[3]); M2[4] = fmaf(ky, R1, M2[4]); M2[5] += R2;
+            M3[0] = fmaf(kxx * kx, P0, M3[0]); M3[1] = fmaf(kxx * ky, P0, M3[1]); M3[2] = fmaf(kxx, P1, M3[2]);
+            M3[3] = fmaf(kx * kyy, P0, M3[3]); M3[4] = fmaf(kxy, P1, M3[4]); M3[5] = fmaf(kx, P2, M3[5]);
+            M3[6] = fmaf(kyy * ky, P0, M3[6]); M3[7] = fmaf(kyy, P1, M3[7]); M3[8] = fmaf(ky, P2, M3[8]);
+            M3[9] += P3;
         }
+#pragma unroll
+        for (int q = 0; q < 3; q++) D1[q] += M1[q];
+#pragma unroll
+        for (int q = 0; q < 6; q++) D2[q] += M2[q];
+#pragma unroll
+        for (int q = 0; q < 10; q++) D3[q] += M3[q];
     }
     if (own) {
-        const V3 m = v3(mu[i], mu[n + i], mu[2 * n + i]);
-        const V3 tau = crs(m, v3(EA[0], EA[1], EA[2])) - 2.0 * v3(GX[0], GX[1], GX[2]);
+        const size_t N = (size_t)n;
+        const double q = tq[(int)pos4[i].w] / SQC_R;
+        double m[3], d[3], Q[3][3];
+        for (int a = 0; a < 3; a++) {
+            m[a] = mu[a * N + i];
+            d[a] = m[a] + (IND ? pind[a * N + i] : 0.0);
+        }
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) Q[a][b] = qd[sym2(a, b) * N + i];
+        double F[3], G[3], QM[3][3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            double f = q * D1[a];
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                f += d[b] * D2[sym2(a, b)];
+#pragma unroll
+                for (int c = 0; c < 3; c++) f -= Q[b][c] * D3[sym3(a, b, c)];
+            }
+            F[a] = f;
+        }
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                double t = 0;
+#pragma unroll
+                for (int c = 0; c < 3; c++) t += Q[a][c] * D2[sym2(c, b)];
+                QM[a][b] = t;
+            }
+        G[0] = QM[2][1] - QM[1][2];
+        G[1] = QM[0][2] - QM[2][0];
+        G[2] = QM[1][0] - QM[0][1];
+        const V3 tau = crs(v3(m[0], m[1], m[2]), v3(D1[0], D1[1], D1[2])) - 2.0 * v3(G[0], G[1], G[2]);
         add_fix3_atomic(frc, n, i, v3(F[0], F[1], F[2]), KE);
         add_fix3_atomic(trq, n, i, tau, KE);
     }
 }
 
-size_t tsum_smem(int nt) { return (size_t)TS_SITES * (4 * sizeof(float4) + 3 * nt * sizeof(float2)); }
+int tab_row(int nt) { return (3 * nt + 1) & ~1; }
+size_t tsum_smem(int row) { return (size_t)TS_SITES * (4 * sizeof(float4) + row * sizeof(float2)); }
 int zrow(int nmax) { return (2 * nmax + 1) | 1; }
 size_t tforce_smem(int zs) {
-    return (size_t)CF_KTILE * (sizeof(int4) + sizeof(float4) + sizeof(float2)) + (size_t)CF_THREADS * zs * sizeof(float2);
+    return (size_t)CF_KGROUP * sizeof(float4) + (size_t)CF_CGROUP * (sizeof(int4) + sizeof(float2)) +
+           (size_t)CF_THREADS * zs * sizeof(float2);
 }
 
-// per-k records of the force pass and the kernels' dynamic shared memory
-// (once per k set, outside any capture)
+// column, run and group records of the FP32 passes, the site-table buffers
+// and the kernels' dynamic shared memory (once per k set, outside any
+// capture).  Leaves the FP32 column passes off (rc.kseg null) when the k
+// list is not column ordered with fixed (kx, ky) per column or |n| is too
+// large for the tables.
 int mp_recip_prepare(Ctx &c) {
     const int nk = c.rc.nk;
-    cudaFree(c.rc.kpack); cudaFree(c.rc.kb4);
-    c.rc.kpack = nullptr; c.rc.kb4 = nullptr;
+    void *old[] = {c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab, c.rc.ssv};
+    for (void *p : old)
+        if (p) cudaFree(p);
+    c.rc.kseg = nullptr; c.rc.kcol = nullptr; c.rc.kgrp = nullptr; c.rc.kzr = nullptr;
+    c.rc.kcxy = nullptr; c.rc.stab = nullptr; c.rc.ssv = nullptr;
+    c.rc.nseg = c.rc.ncol = c.rc.ngrp = c.rc.row = 0;
     if (nk == 0 || c.n == 0 || c.rc.nmax + 1 > TAB_MAX) return 0;
     std::vector<int> kn(3 * (size_t)nk);
     std::vector<double> kv(3 * (size_t)nk), kc(nk);
@@ -704,28 +817,54 @@ int mp_recip_prepare(Ctx &c) {
         cudaMemcpy(kv.data(), c.rc.kvec, kv.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess ||
         cudaMemcpy(kc.data(), c.rc.kcoef, kc.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
         return SMD_ERR_CUDA;
-    std::vector<int4> kp(nk);
-    std::vector<float4> kb(nk);
-    int col = 0;
+    std::vector<int4> col, seg, grp;
+    std::vector<float2> cxy;
+    std::vector<float4> kzr(nk);
     for (int k = 0; k < nk; k++) {
         const int nx = kn[k], ny = kn[nk + k], nz = kn[2 * nk + k];
         const bool start = k == 0 || nx != kn[k - 1] || ny != kn[nk + k - 1] || nz != kn[2 * nk + k - 1] + 1;
-        if (start) col = k;
-        kp[k] = make_int4(nx, ny, nz, k - col);
-        kb[k] = make_float4((float)kv[k], (float)kv[nk + k], (float)kv[2 * nk + k], (float)(2.0 * kc[k]));
+        if (start) {
+            col.push_back(make_int4(k, 0, (int)(((unsigned)nx & 0xffffu) | ((unsigned)ny << 16)), nz));
+            cxy.push_back(make_float2((float)kv[k], (float)kv[nk + k]));
+        } else if (kv[k] != kv[k - 1] || kv[nk + k] != kv[nk + k - 1]) {
+            return 0;  // (kx, ky) varies within a column: not an orthorhombic k set
+        }
+        col.back().y++;
+        const double kz = kv[2 * (size_t)nk + k];
+        kzr[k] = make_float4((float)kz, (float)(kz * kz), (float)(2.0 * kc[k]), 0.f);
     }
-    if (cudaMalloc(&c.rc.kpack, nk * sizeof(int4)) != cudaSuccess ||
-        cudaMalloc(&c.rc.kb4, nk * sizeof(float4)) != cudaSuccess)
+    for (const int4 &cl : col)
+        for (int j = 0; j < cl.y; j += TS_SEG)
+            seg.push_back(make_int4(cl.x + j, std::min(TS_SEG, cl.y - j), cl.z, cl.w + j));
+    for (int q = 0; q < (int)col.size(); q++) {
+        const int len = col[q].y;
+        if (grp.empty() || grp.back().w + len > CF_KGROUP || grp.back().y >= CF_CGROUP)
+            grp.push_back(make_int4(q, 0, col[q].x, 0));
+        grp.back().y++;
+        grp.back().w += len;
+    }
+    const int nt = c.rc.nmax + 1, row = tab_row(nt), zs = zrow(c.rc.nmax);
+    auto put = [](auto **p, const auto &v) -> bool {
+        using T = typename std::remove_reference<decltype(v)>::type::value_type;
+        if (cudaMalloc((void **)p, v.size() * sizeof(T)) != cudaSuccess) return false;
+        return cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) == cudaSuccess;
+    };
+    if (!put(&c.rc.kseg, seg) || !put(&c.rc.kcol, col) || !put(&c.rc.kgrp, grp) || !put(&c.rc.kzr, kzr) ||
+        !put(&c.rc.kcxy, cxy) ||
+        cudaMalloc((void **)&c.rc.stab, (size_t)c.n * row * sizeof(float2)) != cudaSuccess ||
+        cudaMalloc((void **)&c.rc.ssv, (size_t)c.n * 4 * sizeof(float4)) != cudaSuccess)
         return SMD_ERR_CUDA;
-    cudaMemcpy(c.rc.kpack, kp.data(), nk * sizeof(int4), cudaMemcpyHostToDevice);
-    cudaMemcpy(c.rc.kb4, kb.data(), nk * sizeof(float4), cudaMemcpyHostToDevice);
-    const int nt = c.rc.nmax + 1, zs = zrow(c.rc.nmax);
+    c.rc.nseg = (int)seg.size();
+    c.rc.ncol = (int)col.size();
+    c.rc.ngrp = (int)grp.size();
+    c.rc.row = row;
+    c.rc.tab_n = c.n;
     cudaError_t e = cudaSuccess;
-    if (!e) e = cudaFuncSetAttribute(k_rsk_tab<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(nt));
-    if (!e) e = cudaFuncSetAttribute(k_rsk_tab<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(nt));
-    if (!e) e = cudaFuncSetAttribute(k_rsk_tab<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(nt));
-    if (!e) e = cudaFuncSetAttribute(k_rforce_col<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tforce_smem(zs));
-    if (!e) e = cudaFuncSetAttribute(k_rforce_col<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tforce_smem(zs));
+    if (!e) e = cudaFuncSetAttribute(k_rsk_seg<0, TS_SEG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(row));
+    if (!e) e = cudaFuncSetAttribute(k_rsk_seg<1, TS_SEG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(row));
+    if (!e) e = cudaFuncSetAttribute(k_rsk_seg<2, TS_SEG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(row));
+    if (!e) e = cudaFuncSetAttribute(k_rforce_grp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tforce_smem(zs));
+    if (!e) e = cudaFuncSetAttribute(k_rforce_grp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tforce_smem(zs));
     return e == cudaSuccess ? 0 : SMD_ERR_CUDA;
 }
 
@@ -778,14 +917,19 @@ void sums(Ctx &c, int slot_e, int slot_e2 = -1) {
     RecipBufs B = bufs(c);
     const int kb = (nk + MK_THREADS - 1) / MK_THREADS;
     int nch;
-    if (c.precision == SMD_PREC_MIXED && c.rc.kpack) {
-        const int nt = c.rc.nmax + 1;
-        const int kbt = (nk + TS_THREADS - 1) / TS_THREADS;
-        const size_t sm = tsum_smem(nt);
-        int ch = sm_count() * blocks_per_sm((const void *)k_rsk_tab<MODE>, TS_THREADS, sm) / kbt;
+    if (c.precision == SMD_PREC_MIXED && c.rc.kseg && c.rc.tab_n == c.n) {
+        const int nt = c.rc.nmax + 1, row = c.rc.row;
+        const long long ntab = (long long)c.n * (row + 1);
+        k_site_tab<<<(unsigned)((ntab + 255) / 256), 256, 0, c.stream>>>(c.n, nt, row, MODE != 0, c.pos4, c.fixq,
+                                                                          c.type_q, c.mu, c.qd, c.pind, c.rc.stab,
+                                                                          c.rc.ssv);
+        const int kbt = (c.rc.nseg + TS_THREADS - 1) / TS_THREADS;
+        const size_t sm = tsum_smem(row);
+        int ch = sm_count() * blocks_per_sm((const void *)k_rsk_seg<MODE, TS_SEG>, TS_THREADS, sm) / kbt;
         nch = ch < 1 ? 1 : (ch > MK_CHUNKS ? MK_CHUNKS : ch);
-        k_rsk_tab<MODE><<<dim3(kbt, nch), TS_THREADS, sm, c.stream>>>(c.n, nk, nt, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,
-                                                                     c.type_q, c.mu, c.qd, c.pind, B.partial);
+        k_rsk_seg<MODE, TS_SEG><<<dim3(kbt, nch), TS_THREADS, sm, c.stream>>>(c.n, nk, c.rc.nseg, nt, row, c.rc.kseg,
+                                                                             c.rc.kvec, c.rc.stab, c.rc.ssv,
+                                                                             B.partial);
     } else if (c.precision == SMD_PREC_MIXED) {
         nch = chunks_for((const void *)k_rsk_partial_f<MODE>, kb);
         k_rsk_partial_f<MODE><<<dim3(kb, nch), MK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn,
@@ -814,16 +958,16 @@ void forces(Ctx &c) {
     const int nk = c.rc.nk;
     RecipBufs B = bufs(c);
     const int nb = (int)(((long long)c.n * F_TPS + 255) / 256);
-    if (c.precision == SMD_PREC_MIXED && PERM && c.rc.kpack) {
+    if (c.precision == SMD_PREC_MIXED && PERM && c.rc.kseg && c.rc.tab_n == c.n) {
         const int nbs = (c.n + CF_THREADS - 1) / CF_THREADS;
-        const int tiles = (nk + CF_KTILE - 1) / CF_KTILE;
+        const int ng = c.rc.ngrp;
         const int zs = zrow(c.rc.nmax);
         const size_t sm = tforce_smem(zs);
-        int ks = sm_count() * blocks_per_sm((const void *)k_rforce_col<IND>, CF_THREADS, sm) / nbs;
-        ks = ks < 1 ? 1 : (ks > tiles ? tiles : ks);
-        k_rforce_col<IND><<<dim3(nbs, ks), CF_THREADS, sm, c.stream>>>(c.n, nk, zs, c.pos4, c.fixq, c.rc.kpack,
-                                                                      c.rc.kb4, B.sk, c.type_q, c.mu, c.qd, c.pind,
-                                                                      c.frc, c.trq);
+        int ks = sm_count() * blocks_per_sm((const void *)k_rforce_grp<IND>, CF_THREADS, sm) / nbs;
+        ks = ks < 1 ? 1 : (ks > ng ? ng : ks);
+        k_rforce_grp<IND><<<dim3(nbs, ks), CF_THREADS, sm, c.stream>>>(c.n, nk, zs, ng, c.pos4, c.fixq, c.rc.kgrp,
+                                                                      c.rc.kcol, c.rc.kcxy, c.rc.kzr, B.sk,
+                                                                      c.type_q, c.mu, c.qd, c.pind, c.frc, c.trq);
     } else if (c.precision == SMD_PREC_MIXED) {
         if (PERM) {
             const int ks = ksplit_for((const void *)k_rforce_f<IND>, nb, nk);

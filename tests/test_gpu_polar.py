@@ -90,6 +90,29 @@ def test_induction(ens):
     assert err < 1e-8
 
 
+@pytest.mark.parametrize("term,fkey,ekey,eidx", [
+    (L.TERM_VDW, "f_buff_force", "f_buff_energy", (L.E_VDW, 0)),
+    (L.TERM_MP_SHORT, "f_mp_short_force", "f_mp_short_energy", (L.E_REAL, 1)),
+    (L.TERM_MP_LONG, "f_mp_long_force", "f_mp_long_energy", (L.E_LONG, 2)),
+    (L.TERM_IND_SHORT, "f_ind_short_force", "f_ind_short_energy", (L.E_POL_REAL, 6)),
+    (L.TERM_IND_LONG, "f_ind_long_force", "f_ind_long_energy", (L.E_POL_LONG, 7)),
+])
+def test_mixed_terms_against_reference(term, fkey, ekey, eidx):
+    # the mixed path (FP32 pair and multipole algebra on exact-fraction
+    # displacements, FP32 reciprocal phases, FP32 dipole solve rows) against
+    # the reference's FP64 results: RMS relative force error below 1e-6
+    g = golden("polwater216")
+    e = engine.GpuEnsemble(_pw(), precision="mixed")
+    e.set_solver(tol=1e-13, max_iter=1000)
+    f, en, _ = e.compute_forces(term)
+    err = rms_rel(f, g[fkey].reshape(-1, 3))
+    ref = g[ekey][eidx[1]]
+    print(fkey, err, en[eidx[0]], ref)
+    assert err < 1e-6
+    assert abs(en[eidx[0]] - ref) < 1e-6 * abs(ref)
+    e.close()
+
+
 def test_polar_trajectory():
     g = golden("polwater216")
     e = engine.GpuEnsemble(_pw())
