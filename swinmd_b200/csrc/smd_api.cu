@@ -121,6 +121,7 @@ int sync_status(smd_ctx *x) {
 // mapped onto the sites at the end (the mapping is linear in the torques).
 void enqueue_polar(Ctx &c, bool mp_short, bool mp_long, bool ind_short, bool ind_long) {
     launch_frames(c);
+    launch_pack_sites(c);
     launch_torques_begin(c);
     if (mp_short) launch_mp_short(c);
     const bool all = mp_short && mp_long && ind_short && ind_long && c.ind_on;
@@ -224,7 +225,7 @@ void smd_destroy(smd_ctx *x) {
                     c.pl.cell_count, c.pl.cell_start, c.pl.cell_atoms, c.rc.kn, c.rc.kcoef,
                     c.rc.sk, c.rc.kvec, c.clen2, c.type_mp, c.type_polar, c.mu, c.qd, c.trq, c.e0,
                     c.pind, c.cgw, c.cgs, c.cg_bar, c.vpos4, c.vfixq, c.fv, c.ind_rj, c.ind_rc, c.ind_cnt,
-                    c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab, c.rc.ssv, c.phist};
+                    c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab, c.srec, c.phist};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -491,6 +492,8 @@ int smd_set_multipole(smd_ctx *x, const double *type_mp, const double *polar, do
     CK(dalloc(&c.e0, 3 * n)); CK(dalloc(&c.pind, 3 * n)); CK(dalloc(&c.cgw, 20 * n));
     CK(dalloc(&c.frame, 9 * n));
     CK(cudaMemset(c.pind, 0, 3 * n * sizeof(double)));
+    CK(dalloc(&c.srec, 4 * n));
+    CK(cudaMemset(c.srec, 0, 4 * n * sizeof(float4)));
     CK(cudaMemset(c.e0, 0, 3 * n * sizeof(double)));
     int r = setup_cg(c);
     if (r) return fail(x, r, "smd_set_multipole: solver set-up failed");
@@ -1068,7 +1071,7 @@ int smd_profile_stages(smd_ctx *x, int reps, double *out) {
     out[3] = timed([&] { launch_nlist(c, true); });
     for (int q = 4; q < 10; q++) out[q] = 0.0;
     if (c.mp_on) {
-        out[4] = timed([&] { launch_frames(c); launch_torques_begin(c); });
+        out[4] = timed([&] { launch_frames(c); launch_pack_sites(c); launch_torques_begin(c); });
         out[5] = timed([&] { launch_mp_short(c); });
         if (!c.ind_on) out[6] = timed([&] { launch_mp_long(c); });
         if (c.ind_on) {

@@ -50,7 +50,6 @@ struct Recip {               // Ewald reciprocal space (k half-space, k^2 < kcut
     float4 *kzr = nullptr;   // per k (kz, kz^2, 2c, 0)
     float2 *kcxy = nullptr;  // per column (kx, ky)
     float2 *stab = nullptr;  // per site phase tables [n][row]: e^{2 pi i m f / 2^32}, m < nmax + 1, per axis
-    float4 *ssv = nullptr;   // per site values [n][4]: q, mu, Q (6), p
 };
 
 struct Ctx {
@@ -104,6 +103,7 @@ struct Ctx {
     long long *trq = nullptr;       // [3][N] torques, fixed point
     double *e0 = nullptr;           // [3][N] permanent field at the sites
     double *pind = nullptr;         // [3][N] induced dipoles
+    float4 *srec = nullptr;         // [N][4] mixed path, FP32: (q, mu), (Qxx, Qxy, Qxz, Qyy), (Qyz, Qzz, px, py), (pz, 0, 0, 0)
     double *cgw = nullptr;          // CG work: r, z, v [3][N] each, alpha [N], two gather copies [N][4]
     double *cgs = nullptr;          // CG scalars [8] and partials [2][blocks][4]
     int cg_max_iter = 500;
@@ -180,6 +180,7 @@ void launch_polar_long(Ctx &c);
 void launch_torques_begin(Ctx &c);
 void launch_torques_end(Ctx &c);
 void launch_frames(Ctx &c);
+void launch_pack_sites(Ctx &c);
 void launch_buff(Ctx &c);
 int setup_cg(Ctx &c);
 int ensure_ind_rows(Ctx &c);

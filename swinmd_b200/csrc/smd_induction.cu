@@ -167,6 +167,110 @@ __global__ void __launch_bounds__(256) k_ind_field(IndArgs a, TRows R, unsigned 
     }
 }
 
+// Mixed path: displacements from the box fractions (exact integer
+// difference, r^2 from the 64-bit integer sum), the partner's multipoles
+// from its FP32 site record.  The Thole-damped radial factors c3 = l3/r^3,
+// c5 = 3 l5/r^5, c7 = 15 l7/r^7 and the charge term q_j c3 r are FP64; the
+// dipole and quadrupole field
+//   c5 (r.mu_j) r - c3 mu_j + c7 (r.Q_j.r) r - 2 c5 Q_j r - c5 tr(Q_j) r
+// is FP32 algebra on FP32 copies of the factors, summed in FP64.  The rows
+// and the molecule's excluded sites are as in k_ind_field<float>.
+struct FieldMixArgs {
+    const int4 *fixq;
+    const float4 *srec;
+    double dscale[3];
+    int ntypes;
+};
+
+__global__ void __launch_bounds__(256) k_ind_field_f(IndArgs a, FieldMixArgs m, TRows R, unsigned int *status) {
+    __shared__ double s_ipp[64];   // 1 / sqrt(a_i a_j) per type pair (ntypes <= 8)
+    for (int q = threadIdx.x; q < m.ntypes * m.ntypes; q += blockDim.x)
+        s_ipp[q] = 1.0 / sqrt(fmax(1e-8, a.polar[q / m.ntypes]) * fmax(1e-8, a.polar[q % m.ntypes]));
+    __syncthreads();
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    constexpr int TPP = 8;
+    const int i = gt / TPP, t = gt % TPP;
+    const int lane = threadIdx.x & 31, gbase = lane & ~(TPP - 1);
+    V3 E = v3(0, 0, 0);
+    const bool own = i < a.n;
+    int4 fi = make_int4(0, 0, 0, 0);
+    int cnt = 0;
+    if (own) {
+        fi = m.fixq[i];
+        cnt = a.nnbr[i];
+    }
+    const double s2u = m.dscale[0] * m.dscale[0];
+    const int wmax = __reduce_max_sync(0xffffffffu, cnt);
+    int base = 0;
+    for (int k0 = 0; k0 < wmax; k0 += TPP) {
+        const int k = k0 + t;
+        bool valid = false;
+        int j = 0;
+        F3 rf = f3(0.f, 0.f, 0.f);
+        float c3f = 0.f, c5f = 0.f;
+        if (k < cnt) {
+            j = a.nbr[(size_t)k * a.n + i] & 0x7fffffff;
+            const int4 fj = m.fixq[j];
+            const int ix = fi.x - fj.x, iy = fi.y - fj.y, iz = fi.z - fj.z;   // r = r_i - r_j
+            const unsigned long long s2 = (unsigned long long)((long long)ix * ix) +
+                                          (unsigned long long)((long long)iy * iy) +
+                                          (unsigned long long)((long long)iz * iz);
+            const double r2 = (double)s2 * s2u;
+            if (r2 <= a.cut2) {
+                valid = true;
+                const V3 r = v3(ix * m.dscale[0], iy * m.dscale[1], iz * m.dscale[2]);
+                rf = f3((float)r.x, (float)r.y, (float)r.z);
+                const double rr = sqrt(r2), r_1 = 1.0 / rr, r_2 = r_1 * r_1, r_3 = r_1 * r_2;
+                const double au3 = a.a * r2 * rr * s_ipp[fi.w * m.ntypes + fj.w];
+                const double e = exp(-au3);
+                const double l3 = 1.0 - e, l5 = 1.0 - (1.0 + au3) * e;
+                const double l7 = 1.0 - (1.0 + au3 + 0.6 * au3 * au3) * e;
+                const double c3 = l3 * r_3, c5 = 3.0 * l5 * r_3 * r_2, c7 = 15.0 * l7 * r_3 * r_2 * r_2;
+                c3f = (float)c3;
+                c5f = (float)c5;
+                const float4 *rj = m.srec + 4 * (size_t)j;
+                const float4 j0 = __ldg(rj), j1 = __ldg(rj + 1), j2 = __ldg(rj + 2);
+                const F3 mj = f3(j0.y, j0.z, j0.w);
+                const Q6F Qj = {j1.x, j1.y, j1.z, j1.w, j2.x, j2.y};
+                const F3 Qjr = qv(Qj, rf);
+                const float sc = c5f * (dot(rf, mj) - qtr(Qj)) + (float)c7 * dot(rf, Qjr);
+                const F3 em = sc * rf - c3f * mj - (2.f * c5f) * Qjr;
+                E = E + (a.tq[fj.w] / SQC * c3) * r + to_v3(em);
+            }
+        }
+        const unsigned grp = (__ballot_sync(0xffffffffu, valid) >> gbase) & ((1u << TPP) - 1);
+        if (valid && base + __popc(grp & ((1u << t) - 1)) < R.cap) {
+            const size_t at = (size_t)i * R.cap + base + __popc(grp & ((1u << t) - 1));
+            const float sc = sqrtf(c5f);
+            R.j[at] = j;
+            ((float4 *)R.c)[at] = make_float4(sc * rf.x, sc * rf.y, sc * rf.z, c3f);
+        } else if (valid) {
+            atomicOr(status, ST_LIST_OVERFLOW);
+        }
+        base += __popc(grp);
+    }
+    E.x = group_sum<TPP>(E.x); E.y = group_sum<TPP>(E.y); E.z = group_sum<TPP>(E.z);
+    if (own && t == 0) {
+        a.e0[i] = E.x; a.e0[a.n + i] = E.y; a.e0[2 * a.n + i] = E.z;
+        const double4 pi = a.pos4[i];
+        const double poli = fmax(1e-8, a.polar[(int)pi.w]);
+        const int mo = a.mol[i];
+        for (int q = a.mol_off[mo]; q < a.mol_off[mo + 1]; q++) {
+            const int j = a.mol_atoms[q];
+            if (j == i || !is_excluded(i, j, a.excl_off, a.excl)) continue;
+            const double4 pj = a.pos4[j];
+            const V3 r = mind(pi, pj, a.box);
+            const double rr = sqrt(dot(r, r)), r2 = rr * rr;
+            if (!(r2 <= a.cut2)) continue;
+            const double ipp = 1.0 / sqrt(poli * fmax(1e-8, a.polar[(int)pj.w]));
+            const double u3 = r2 * rr * ipp, e = exp(-a.a * u3);
+            const double r_3 = 1.0 / (r2 * rr);
+            put_row<float>(R, i, base++, j, r, (1.0 - e) * r_3, 3.0 * (1.0 - (1.0 + a.a * u3) * e) * r_3 / r2, status);
+        }
+        R.cnt[i] = base < R.cap ? base : R.cap;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // matrix-free A v and the PCG solve
 // ---------------------------------------------------------------------------
@@ -559,6 +663,7 @@ struct IndRealArgs {
     IndArgs ia;
     long long *frc, *trq, *acc;
     const int4 *fixq;      // mixed path: box fractions
+    const float4 *srec;    // mixed path: FP32 site records (q, mu, Q, p)
     double dscale[3];      // L / 2^32 per axis
 };
 
@@ -636,12 +741,13 @@ __global__ void __launch_bounds__(64) k_ind_real_f(IndRealArgs A) {
     double en = 0, w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     if (i < a.n) {
         const int4 fi = A.fixq[i];
-        const float qi = (float)(a.tq[fi.w] / SQC);
         const double poli = a.polar[fi.w];
-        const F3 mi = f3((float)a.mu[i], (float)a.mu[a.n + i], (float)a.mu[2 * a.n + i]);
-        const F3 pii = f3((float)a.p[i], (float)a.p[a.n + i], (float)a.p[2 * a.n + i]);
-        const Q6F Qi = {(float)a.qd[i], (float)a.qd[a.n + i], (float)a.qd[2 * a.n + i],
-                        (float)a.qd[3 * a.n + i], (float)a.qd[4 * a.n + i], (float)a.qd[5 * a.n + i]};
+        const float4 *ri = A.srec + 4 * (size_t)i;
+        const float4 i0 = ri[0], i1 = ri[1], i2 = ri[2], i3 = ri[3];
+        const float qi = i0.x;
+        const F3 mi = f3(i0.y, i0.z, i0.w);
+        const F3 pii = f3(i2.z, i2.w, i3.x);
+        const Q6F Qi = {i1.x, i1.y, i1.z, i1.w, i2.x, i2.y};
         const double s2u = A.dscale[0] * A.dscale[0];
         auto pair = [&](int j, double scale) {
             const int4 fj = A.fixq[j];
@@ -653,12 +759,11 @@ __global__ void __launch_bounds__(64) k_ind_real_f(IndRealArgs A) {
             if (!(r2 < a.rc2)) return;
             const V3 r = v3(ix * A.dscale[0], iy * A.dscale[1], iz * A.dscale[2]);
             const F3 rf = f3((float)r.x, (float)r.y, (float)r.z);
-            const Q6F Qj = {(float)a.qd[j], (float)a.qd[a.n + j], (float)a.qd[2 * a.n + j],
-                            (float)a.qd[3 * a.n + j], (float)a.qd[4 * a.n + j], (float)a.qd[5 * a.n + j]};
+            const float4 *rj = A.srec + 4 * (size_t)j;
+            const float4 j0 = __ldg(rj), j1 = __ldg(rj + 1), j2 = __ldg(rj + 2), j3 = __ldg(rj + 3);
+            const Q6F Qj = {j1.x, j1.y, j1.z, j1.w, j2.x, j2.y};
             IndAlgF al;
-            ind_algebra_f(qi, mi, Qi, pii, (float)(a.tq[fj.w] / SQC),
-                          f3((float)a.mu[j], (float)a.mu[a.n + j], (float)a.mu[2 * a.n + j]), Qj,
-                          f3((float)a.p[j], (float)a.p[a.n + j], (float)a.p[2 * a.n + j]), rf, al);
+            ind_algebra_f(qi, mi, Qi, pii, j0.x, f3(j0.y, j0.z, j0.w), Qj, f3(j2.z, j2.w, j3.x), rf, al);
             IndPairOut o;
             ind_pair_mixed(al, r, r2, poli, a.polar[fj.w], a.a, a.alpha, scale, o);
             en += o.e;
@@ -815,7 +920,14 @@ void launch_ind_solve(Ctx &c) {
     TRows R;
     R.j = c.ind_rj; R.c = c.ind_rc; R.cnt = c.ind_cnt; R.cap = c.ind_cap;
     const int nb = (int)(((long long)c.n * 8 + 255) / 256);
-    if (f32)
+    const bool cubic = c.box.L[0] == c.box.L[1] && c.box.L[1] == c.box.L[2];
+    if (f32 && cubic && c.srec && c.ntypes <= 8) {
+        if (!c.fixq_from_integrate) launch_fixq(c);
+        FieldMixArgs m;
+        m.fixq = c.fixq; m.srec = c.srec; m.ntypes = c.ntypes;
+        for (int d = 0; d < 3; d++) m.dscale[d] = c.box.L[d] / 4294967296.0;
+        k_ind_field_f<<<nb, 256, 0, c.stream>>>(a, m, R, c.status);
+    } else if (f32)
         k_ind_field<float><<<nb, 256, 0, c.stream>>>(a, R, c.status);
     else
         k_ind_field<double><<<nb, 256, 0, c.stream>>>(a, R, c.status);
@@ -847,6 +959,7 @@ void launch_ind_solve(Ctx &c) {
         cudaLaunchKernelEx(&cfg, k_ind_cg<true>, g);
     else
         cudaLaunchKernelEx(&cfg, k_ind_cg<false>, g);
+    launch_pack_sites(c);   // the mixed path's site records get the new dipoles
     // a time step stores its converged dipoles for the next steps' guess
     if (c.in_step && c.phist) {
         k_hist_push<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.pind, c.e0, c.phist, c.flags);
@@ -865,6 +978,7 @@ void launch_ind_short(Ctx &c) {
     if (c.precision == SMD_PREC_MIXED && cubic) {
         if (!c.fixq_from_integrate) launch_fixq(c);
         A.fixq = c.fixq;
+        A.srec = c.srec;
         for (int d = 0; d < 3; d++) A.dscale[d] = c.box.L[d] / 4294967296.0;
         k_ind_real_f<<<nb, 64, 0, c.stream>>>(A);
     } else {

@@ -482,7 +482,8 @@ __global__ void __launch_bounds__(256) k_rforce_f(int n, int nk, const double4 *
 // at most two complex products after them.
 //
 // Site tables (one pass per evaluation): per site and axis the factors
-// e^{2 pi i m f / 2^32}, m = 0 .. nmax, and the site's q, mu, Q, p in FP32.
+// e^{2 pi i m f / 2^32}, m = 0 .. nmax; the site's q, mu, Q, p in FP32 come
+// from the mixed path's site records.
 //
 // Sums pass: one thread per run of up to TS_SEG k of one column, sites
 // staged in shared memory tile by tile.  Per site a run shares X[nx] Y[|ny|]
@@ -514,34 +515,18 @@ __device__ __forceinline__ float2 table_entry(int m, unsigned f) {
 }
 
 // site tables [n][row]: X[0..nt), Y[0..nt), Z[0..nt), zero padding to an
-// even row; site values [n][4]: (q, mux, muy, muz), (Qxx, Qxy, Qxz, Qyy),
-// (Qyz, Qzz, px, py), (pz, 0, 0, 0)
-__global__ void k_site_tab(int n, int nt, int row, int with_p, const double4 *pos4, const int4 *fixq,
-                           const double *tq, const double *mu, const double *qd, const double *pind,
-                           float2 *stab, float4 *ssv) {
+// even row
+__global__ void k_site_tab(int n, int nt, int row, const int4 *fixq, float2 *stab) {
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long ntab = (long long)n * row;
-    if (e < ntab) {
-        const int i = (int)(e / row), r = (int)(e - (long long)i * row);
-        const int ax = r / nt, m = r - ax * nt;
-        float2 v = make_float2(0.f, 0.f);
-        if (ax < 3) {
-            const int4 f = fixq[i];
-            v = table_entry(m, (unsigned)(ax == 0 ? f.x : (ax == 1 ? f.y : f.z)));
-        }
-        stab[e] = v;
-    } else if (e < ntab + n) {
-        const int i = (int)(e - ntab);
-        const size_t N = (size_t)n;
-        float p[3] = {0.f, 0.f, 0.f};
-        if (with_p)
-            for (int d = 0; d < 3; d++) p[d] = (float)pind[d * N + i];
-        ssv[4 * (size_t)i] = make_float4((float)(tq[(int)pos4[i].w] / SQC_R), (float)mu[i], (float)mu[N + i],
-                                         (float)mu[2 * N + i]);
-        ssv[4 * (size_t)i + 1] = make_float4((float)qd[i], (float)qd[N + i], (float)qd[2 * N + i], (float)qd[3 * N + i]);
-        ssv[4 * (size_t)i + 2] = make_float4((float)qd[4 * N + i], (float)qd[5 * N + i], p[0], p[1]);
-        ssv[4 * (size_t)i + 3] = make_float4(p[2], 0.f, 0.f, 0.f);
+    if (e >= (long long)n * row) return;
+    const int i = (int)(e / row), r = (int)(e - (long long)i * row);
+    const int ax = r / nt, m = r - ax * nt;
+    float2 v = make_float2(0.f, 0.f);
+    if (ax < 3) {
+        const int4 f = fixq[i];
+        v = table_entry(m, (unsigned)(ax == 0 ? f.x : (ax == 1 ? f.y : f.z)));
     }
+    stab[e] = v;
 }
 
 // MODE 0: permanent sums (slots 0-3); 1: induced sums (4-5); 2: all six.
@@ -804,13 +789,13 @@ size_t tforce_smem(int zs) {
 // large for the tables.
 int mp_recip_prepare(Ctx &c) {
     const int nk = c.rc.nk;
-    void *old[] = {c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab, c.rc.ssv};
+    void *old[] = {c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab};
     for (void *p : old)
         if (p) cudaFree(p);
     c.rc.kseg = nullptr; c.rc.kcol = nullptr; c.rc.kgrp = nullptr; c.rc.kzr = nullptr;
-    c.rc.kcxy = nullptr; c.rc.stab = nullptr; c.rc.ssv = nullptr;
+    c.rc.kcxy = nullptr; c.rc.stab = nullptr;
     c.rc.nseg = c.rc.ncol = c.rc.ngrp = c.rc.row = 0;
-    if (nk == 0 || c.n == 0 || c.rc.nmax + 1 > TAB_MAX) return 0;
+    if (nk == 0 || c.n == 0 || c.rc.nmax + 1 > TAB_MAX || !c.srec) return 0;
     std::vector<int> kn(3 * (size_t)nk);
     std::vector<double> kv(3 * (size_t)nk), kc(nk);
     if (cudaMemcpy(kn.data(), c.rc.kn, kn.size() * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
@@ -851,8 +836,7 @@ int mp_recip_prepare(Ctx &c) {
     };
     if (!put(&c.rc.kseg, seg) || !put(&c.rc.kcol, col) || !put(&c.rc.kgrp, grp) || !put(&c.rc.kzr, kzr) ||
         !put(&c.rc.kcxy, cxy) ||
-        cudaMalloc((void **)&c.rc.stab, (size_t)c.n * row * sizeof(float2)) != cudaSuccess ||
-        cudaMalloc((void **)&c.rc.ssv, (size_t)c.n * 4 * sizeof(float4)) != cudaSuccess)
+        cudaMalloc((void **)&c.rc.stab, (size_t)c.n * row * sizeof(float2)) != cudaSuccess)
         return SMD_ERR_CUDA;
     c.rc.nseg = (int)seg.size();
     c.rc.ncol = (int)col.size();
@@ -919,16 +903,14 @@ void sums(Ctx &c, int slot_e, int slot_e2 = -1) {
     int nch;
     if (c.precision == SMD_PREC_MIXED && c.rc.kseg && c.rc.tab_n == c.n) {
         const int nt = c.rc.nmax + 1, row = c.rc.row;
-        const long long ntab = (long long)c.n * (row + 1);
-        k_site_tab<<<(unsigned)((ntab + 255) / 256), 256, 0, c.stream>>>(c.n, nt, row, MODE != 0, c.pos4, c.fixq,
-                                                                          c.type_q, c.mu, c.qd, c.pind, c.rc.stab,
-                                                                          c.rc.ssv);
+        const long long ntab = (long long)c.n * row;
+        k_site_tab<<<(unsigned)((ntab + 255) / 256), 256, 0, c.stream>>>(c.n, nt, row, c.fixq, c.rc.stab);
         const int kbt = (c.rc.nseg + TS_THREADS - 1) / TS_THREADS;
         const size_t sm = tsum_smem(row);
         int ch = sm_count() * blocks_per_sm((const void *)k_rsk_seg<MODE, TS_SEG>, TS_THREADS, sm) / kbt;
         nch = ch < 1 ? 1 : (ch > MK_CHUNKS ? MK_CHUNKS : ch);
         k_rsk_seg<MODE, TS_SEG><<<dim3(kbt, nch), TS_THREADS, sm, c.stream>>>(c.n, nk, c.rc.nseg, nt, row, c.rc.kseg,
-                                                                             c.rc.kvec, c.rc.stab, c.rc.ssv,
+                                                                             c.rc.kvec, c.rc.stab, c.srec,
                                                                              B.partial);
     } else if (c.precision == SMD_PREC_MIXED) {
         nch = chunks_for((const void *)k_rsk_partial_f<MODE>, kb);

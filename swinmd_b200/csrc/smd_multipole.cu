@@ -105,6 +105,28 @@ void launch_frames(Ctx &c) {
                                                          c.type_mp, c.mu, c.qd, c.frame);
 }
 
+// FP32 site records of the mixed path, one 64-byte row per site, so that a
+// pair kernel gathers a partner's charge and multipoles with four vector
+// loads: (q, mu), (Qxx, Qxy, Qxz, Qyy), (Qyz, Qzz, px, py), (pz, 0, 0, 0)
+__global__ void k_pack_sites(int n, const double4 *pos4, const double *tq, const double *mu, const double *qd,
+                             const double *pind, float4 *srec) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t N = (size_t)n;
+    float4 *o = srec + 4 * (size_t)i;
+    o[0] = make_float4((float)(tq[(int)pos4[i].w] / SQRTCOULOMB), (float)mu[i], (float)mu[N + i],
+                       (float)mu[2 * N + i]);
+    o[1] = make_float4((float)qd[i], (float)qd[N + i], (float)qd[2 * N + i], (float)qd[3 * N + i]);
+    o[2] = make_float4((float)qd[4 * N + i], (float)qd[5 * N + i], (float)pind[i], (float)pind[N + i]);
+    o[3] = make_float4((float)pind[2 * N + i], 0.f, 0.f, 0.f);
+}
+
+// after the frames (permanent multipoles) and after the dipole solve (p)
+void launch_pack_sites(Ctx &c) {
+    if (c.precision != SMD_PREC_MIXED || !c.srec) return;
+    k_pack_sites<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.pos4, c.type_q, c.mu, c.qd, c.pind, c.srec);
+}
+
 // ---------------------------------------------------------------------------
 // pair invariants of the multipole-multipole interaction (r = r_i - r_j)
 // ---------------------------------------------------------------------------
@@ -186,6 +208,7 @@ struct MPArgs {
     double alpha, rc2;
     long long *frc, *trq, *acc;
     const int4 *fixq;      // mixed path: box fractions
+    const float4 *srec;    // mixed path: FP32 site records (q, mu, Q, p)
     double dscale[3];      // L / 2^32 per axis
 };
 
@@ -264,10 +287,10 @@ __global__ void __launch_bounds__(128, 3) k_mp_real_f(MPArgs a) {
     if (i < a.n) {
         const int4 fi = a.fixq[i];
         const double qi_d = a.tq[fi.w] / SQRTCOULOMB;
-        const float qi = (float)qi_d;
-        const F3 mi = f3((float)a.mu[i], (float)a.mu[a.n + i], (float)a.mu[2 * a.n + i]);
-        const Q6F Qi = {(float)a.qd[i], (float)a.qd[a.n + i], (float)a.qd[2 * a.n + i],
-                        (float)a.qd[3 * a.n + i], (float)a.qd[4 * a.n + i], (float)a.qd[5 * a.n + i]};
+        const float4 i0 = a.srec[4 * (size_t)i], i1 = a.srec[4 * (size_t)i + 1], i2 = a.srec[4 * (size_t)i + 2];
+        const float qi = i0.x;
+        const F3 mi = f3(i0.y, i0.z, i0.w);
+        const Q6F Qi = {i1.x, i1.y, i1.z, i1.w, i2.x, i2.y};
         const double s2u = a.dscale[0] * a.dscale[0];
         const int cnt = a.nnbr[i];
         for (int k = t; k < cnt; k += TPP) {
@@ -282,10 +305,11 @@ __global__ void __launch_bounds__(128, 3) k_mp_real_f(MPArgs a) {
             const V3 r = v3(ix * a.dscale[0], iy * a.dscale[1], iz * a.dscale[2]);
             const F3 rf = f3((float)r.x, (float)r.y, (float)r.z);
             const double qj_d = a.tq[fj.w] / SQRTCOULOMB;
-            const float qj = (float)qj_d;
-            const F3 mj = f3((float)a.mu[j], (float)a.mu[a.n + j], (float)a.mu[2 * a.n + j]);
-            const Q6F Qj = {(float)a.qd[j], (float)a.qd[a.n + j], (float)a.qd[2 * a.n + j],
-                            (float)a.qd[3 * a.n + j], (float)a.qd[4 * a.n + j], (float)a.qd[5 * a.n + j]};
+            const float4 j0 = __ldg(&a.srec[4 * (size_t)j]), j1 = __ldg(&a.srec[4 * (size_t)j + 1]);
+            const float4 j2 = __ldg(&a.srec[4 * (size_t)j + 2]);
+            const float qj = j0.x;
+            const F3 mj = f3(j0.y, j0.z, j0.w);
+            const Q6F Qj = {j1.x, j1.y, j1.z, j1.w, j2.x, j2.y};
             MPPair<float, F3> P;
             mp_invariants(qi, mi, Qi, qj, mj, Qj, rf, P);
             double B[6];
@@ -455,6 +479,7 @@ void launch_mp_short(Ctx &c) {
     if (c.precision == SMD_PREC_MIXED && cubic) {
         if (!c.fixq_from_integrate) launch_fixq(c);
         a.fixq = c.fixq;
+        a.srec = c.srec;
         for (int d = 0; d < 3; d++) a.dscale[d] = c.box.L[d] / 4294967296.0;
         k_mp_real_f<tpp><<<nb, 128, 0, c.stream>>>(a);
     } else {

@@ -159,11 +159,13 @@ __global__ void k_build(BuildArgs a) {
     int count = 0;
     auto consider = [&](int j, bool pbc, bool valid) {
         bool take = valid && j != i;
+        // the distance test first: only the few candidates inside the list
+        // radius read the exclusion list
+        if (take) take = ref_r2(pi, a.pos4[j], a.box, pbc, le && pbc, delta) < a.rl2;
         if (take) {
             for (int e = e0; e < e1; e++)
                 if (a.excl[e] == j) { take = false; break; }
         }
-        if (take) take = ref_r2(pi, a.pos4[j], a.box, pbc, le && pbc, delta) < a.rl2;
         unsigned m = __ballot_sync(0xffffffffu, take);
         if (take) {
             int slot = count + __popc(m & ((1u << lane) - 1));
