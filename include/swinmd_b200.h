@@ -274,7 +274,9 @@ int smd_get_series(smd_ctx *ctx, double *out, int cap, int *count);
  * out[3] a forced pair-list rebuild; for the polarisable model out[4] frames,
  * out[5] multipole real+self+intra, out[6] multipole reciprocal (models
  * without induced dipoles), out[7] field + dipole solve, out[8] induced
- * real+self+intra, out[9] reciprocal structure factors and forces of the
+ * real+self+intra (in the mixed precision mode the multipole and induced
+ * real space are one fused pass after the solve: out[8] then holds both and
+ * out[5] is 0), out[9] reciprocal structure factors and forces of the
  * permanent and induced multipoles together (out has room for 10).  Leaves
  * forces and state unchanged except for the rebuilt list. */
 int smd_profile_stages(smd_ctx *ctx, int reps, double *out);

@@ -123,8 +123,17 @@ void enqueue_polar(Ctx &c, bool mp_short, bool mp_long, bool ind_short, bool ind
     launch_frames(c);
     launch_pack_sites(c);
     launch_torques_begin(c);
-    if (mp_short) launch_mp_short(c);
     const bool all = mp_short && mp_long && ind_short && ind_long && c.ind_on;
+    if (all && polar_short_fused(c)) {
+        // mixed path: the multipole real space does not feed the solve, so
+        // it runs after it, fused with the induced real space
+        launch_ind_solve(c);
+        launch_polar_short(c);
+        launch_polar_long(c);
+        launch_torques_end(c);
+        return;
+    }
+    if (mp_short) launch_mp_short(c);
     if (all) {
         // a full evaluation: after the solve one pass gives all structure
         // factors and one reciprocal force pass serves both terms
@@ -489,7 +498,7 @@ int smd_set_multipole(smd_ctx *x, const double *type_mp, const double *polar, do
     CK(cudaMemcpy(c.type_polar, polar, c.ntypes * sizeof(double), cudaMemcpyHostToDevice));
     const size_t n = c.n;
     CK(dalloc(&c.mu, 3 * n)); CK(dalloc(&c.qd, 6 * n)); CK(dalloc(&c.trq, 3 * n));
-    CK(dalloc(&c.e0, 3 * n)); CK(dalloc(&c.pind, 3 * n)); CK(dalloc(&c.cgw, 20 * n));
+    CK(dalloc(&c.e0, 3 * n)); CK(dalloc(&c.pind, 3 * n)); CK(dalloc(&c.cgw, 26 * n));
     CK(dalloc(&c.frame, 9 * n));
     CK(cudaMemset(c.pind, 0, 3 * n * sizeof(double)));
     CK(dalloc(&c.srec, 4 * n));
@@ -497,8 +506,8 @@ int smd_set_multipole(smd_ctx *x, const double *type_mp, const double *polar, do
     CK(cudaMemset(c.e0, 0, 3 * n * sizeof(double)));
     int r = setup_cg(c);
     if (r) return fail(x, r, "smd_set_multipole: solver set-up failed");
-    CK(dalloc(&c.cgs, 8 + 8 * (size_t)c.cg_blocks));
-    CK(cudaMemset(c.cgs, 0, (8 + 8 * (size_t)c.cg_blocks) * sizeof(double)));
+    CK(dalloc(&c.cgs, 8 + 16 * (size_t)c.cg_blocks));
+    CK(cudaMemset(c.cgs, 0, (8 + 16 * (size_t)c.cg_blocks) * sizeof(double)));
     CK(dalloc(&c.cg_bar, 1));
     if (c.ind_on) {
         CK(dalloc(&c.phist, 24 * n));
@@ -1072,7 +1081,8 @@ int smd_profile_stages(smd_ctx *x, int reps, double *out) {
     for (int q = 4; q < 10; q++) out[q] = 0.0;
     if (c.mp_on) {
         out[4] = timed([&] { launch_frames(c); launch_pack_sites(c); launch_torques_begin(c); });
-        out[5] = timed([&] { launch_mp_short(c); });
+        const bool fused = polar_short_fused(c);
+        if (!fused) out[5] = timed([&] { launch_mp_short(c); });
         if (!c.ind_on) out[6] = timed([&] { launch_mp_long(c); });
         if (c.ind_on) {
             const int guess = c.cg_guess;
@@ -1092,7 +1102,8 @@ int smd_profile_stages(smd_ctx *x, int reps, double *out) {
                 CK(cudaStreamSynchronize(c.stream));
                 cudaFree(p0);
             }
-            out[8] = timed([&] { launch_ind_short(c); });
+            // with the fused pass the multipole real space is part of this stage
+            out[8] = timed([&] { if (fused) launch_polar_short(c); else launch_ind_short(c); });
             out[9] = timed([&] { launch_polar_long(c); });
         }
     }

@@ -104,8 +104,8 @@ struct Ctx {
     double *e0 = nullptr;           // [3][N] permanent field at the sites
     double *pind = nullptr;         // [3][N] induced dipoles
     float4 *srec = nullptr;         // [N][4] mixed path, FP32: (q, mu), (Qxx, Qxy, Qxz, Qyy), (Qyz, Qzz, px, py), (pz, 0, 0, 0)
-    double *cgw = nullptr;          // CG work: r, z, v [3][N] each, alpha [N], two gather copies [N][4]
-    double *cgs = nullptr;          // CG scalars [8] and partials [2][blocks][4]
+    double *cgw = nullptr;          // CG work: r, w, p [3][N] each, alpha [N], two gather copies [N][4], s, u [3][N]
+    double *cgs = nullptr;          // CG scalars [8] and partials [4][blocks][4]
     int cg_max_iter = 500;
     double cg_tol = 2.0819e-8;      // RMS dipole change tolerance (e nm); 1e-6 D
     int cg_guess = 0;               // 0: alpha E0, 1: previous step, 2: learned (MLP)
@@ -175,6 +175,9 @@ void launch_mp_short(Ctx &c);
 void launch_mp_long(Ctx &c);
 void launch_ind_solve(Ctx &c);
 void launch_ind_short(Ctx &c);
+void launch_mp_mol(Ctx &c);
+bool polar_short_fused(const Ctx &c);
+void launch_polar_short(Ctx &c);
 void launch_ind_long(Ctx &c);
 void launch_polar_long(Ctx &c);
 void launch_torques_begin(Ctx &c);

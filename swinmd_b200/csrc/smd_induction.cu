@@ -308,9 +308,10 @@ __device__ bool grid_barrier(unsigned int *bar, unsigned int target, unsigned in
 struct CGArgs {
     IndArgs ia;
     TRows rows;
-    double *r, *z, *v, *al;  // [3][N] residual, A v, direction; [N] polarisabilities
+    double *r, *z, *v, *al;  // [3][N] residual, w = A u, direction p; [N] polarisabilities
+    double *s, *u;           // [3][N] s = A p, u = M^-1 r
     void *g0, *g1;           // per-site packed copies (float4 / double4) of the start dipoles and of v
-    double *part;            // partials [2][nblocks][4]
+    double *part;            // partials [4][nblocks][4]
     double *scal;            // [0] iterations, [1] final rms change
     unsigned *bar, *status;
     int nblocks, max_iter, guess;
@@ -365,6 +366,8 @@ __device__ __forceinline__ float4 ldcg4(const float4 *p) { return __ldcg(p); }
 // row entries are read in batches of CG_UNROLL per lane before the gathers
 // of v, so each lane keeps several loads in flight.  GR is the arithmetic
 // type of the products (the row's storage type), summed per lane in GR.
+// The packed vector is rewritten every iteration, so it is gathered past L1
+// (tried through L1, relying on the barrier's acquire: slower).
 template <typename G4, typename GR>
 __device__ V3 amul(const CGArgs &c, int i, int t, const G4 *g) {
     constexpr int CG_UNROLL = sizeof(GR) == 4 ? 4 : 2;
@@ -404,14 +407,21 @@ __device__ V3 amul(const CGArgs &c, int i, int t, const G4 *g) {
 }
 
 // Jacobi-preconditioned CG (M^-1 = diag(a_i)) as one persistent cooperative
-// kernel, three grid barriers per iteration:
-//   A  z = A v (TPP lanes per site), v.z          | barrier, alpha = rs / v.z
-//   B  p += alpha v, r -= alpha z, rs' = r.a r,   | barrier, stop on the RMS
-//      |alpha v|^2                                |  change of p, beta
-//   C  v = a r + beta v, packed copy of v         | barrier
-// The two reductions use separate partial buffers, so no extra barrier
-// guards their reuse.  Vectors written in one phase and read by other
-// blocks in the next are read past L1.
+// kernel in the single-reduction form of Chronopoulos and Gear (1989): with
+// u = M^-1 r and w = A u kept alongside, the direction p = u + beta p and
+// s = A p = w + beta s follow by recurrence, and both inner products of an
+// iteration, gamma = r.u and delta = w.u, come from one pass each side of
+// the matrix-vector product.  Two grid barriers per iteration:
+//   U  p = u + beta p, s = w + beta s, x += alpha p, r -= alpha s,
+//      u = M^-1 r (and its packed copy); r.u, |alpha p|^2   | barrier, stop
+//                                                           |  on the RMS
+//                                                           |  change of x
+//   W  w = A u (TPP lanes per site); w.u                    | barrier
+//   beta = gamma'/gamma, alpha = gamma' / (delta' - beta gamma'/alpha)
+// (alpha and beta are those of standard PCG in exact arithmetic).  The
+// partial sums of U and W alternate between two buffers each by iteration
+// parity, so no barrier is needed to guard their reuse.  Vectors written in
+// one phase and read by other blocks in the next are read past L1.
 template <bool F32>
 __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
     using G4 = typename std::conditional<F32, float4, double4>::type;
@@ -420,7 +430,8 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
     const IndArgs &a = c.ia;
     const int n = a.n;
     G4 *g0 = (G4 *)c.g0, *g1 = (G4 *)c.g1;
-    double *part0 = c.part, *part1 = c.part + 4 * c.nblocks;
+    double *const pu0 = c.part, *const pu1 = c.part + 4 * c.nblocks;
+    double *const pw0 = c.part + 8 * c.nblocks, *const pw1 = c.part + 12 * c.nblocks;
     const int nthreads = c.nblocks * CG_THREADS;
     const int gtid = blockIdx.x * CG_THREADS + threadIdx.x;
     const int sites_per_pass = nthreads / CG_TPP;
@@ -430,7 +441,7 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
     const int passes = (n + sites_per_pass - 1) / sites_per_pass;
     unsigned int phase = 0;
     double tot[4];
-    // p0: alpha E0 (guess 0) or the dipoles already in p (previous step / learned)
+    // x0: alpha E0 (guess 0) or the dipoles already in p (previous step / learned)
     for (int i = gtid; i < n; i += nthreads) {
         const double al = fmax(1e-8, a.polar[(int)a.pos4[i].w]);
         c.al[i] = al;
@@ -442,7 +453,7 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
         g0[i] = G4{(GR)p3[0], (GR)p3[1], (GR)p3[2], (GR)0};
     }
     if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
-    // r = E0 - A p ; v = M^-1 r ; rs = r.M^-1 r
+    // r = E0 - A x ; u = M^-1 r ; gamma = r.u
     double vals[4] = {0, 0, 0, 0};
     for (int ps = 0; ps < passes; ps++) {
         const int i = gslot + ps * sites_per_pass;
@@ -453,69 +464,84 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
             const double rr[3] = {a.e0[i] - Ap.x, a.e0[n + i] - Ap.y, a.e0[2 * n + i] - Ap.z};
             for (int d = 0; d < 3; d++) {
                 c.r[d * n + i] = rr[d];
-                c.v[d * n + i] = al * rr[d];
+                c.u[d * n + i] = al * rr[d];
                 vals[0] += rr[d] * al * rr[d];
             }
             g1[i] = G4{(GR)(al * rr[0]), (GR)(al * rr[1]), (GR)(al * rr[2]), (GR)0};
         }
     }
-    block_partials(vals, 1, part0, s_w);
+    block_partials(vals, 1, pu1, s_w);
     if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
-    grid_sum(part0, c.nblocks, 1, tot, s_w);
-    double rs = tot[0];
+    // w = A u ; delta = w.u
+    vals[0] = 0;
+    for (int ps = 0; ps < passes; ps++) {
+        const int i = gslot + ps * sites_per_pass;
+        V3 Au = i < n ? amul<G4, GR>(c, i, t, g1) : v3(0, 0, 0);
+        Au.x = group_sum<CG_TPP>(Au.x); Au.y = group_sum<CG_TPP>(Au.y); Au.z = group_sum<CG_TPP>(Au.z);
+        if (i < n && t == 0) {
+            c.z[i] = Au.x; c.z[n + i] = Au.y; c.z[2 * n + i] = Au.z;
+            vals[0] += __ldcg(&c.u[i]) * Au.x + __ldcg(&c.u[n + i]) * Au.y + __ldcg(&c.u[2 * n + i]) * Au.z;
+        }
+    }
+    block_partials(vals, 1, pw1, s_w);
+    if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
+    grid_sum(pu1, c.nblocks, 1, tot, s_w);
+    double gamma = tot[0];
+    grid_sum(pw1, c.nblocks, 1, tot, s_w);
+    double alpha_cg = gamma / tot[0], beta = 0.0;
     int it = 0;
     double rms = 0;
     for (; it < c.max_iter; it++) {
-        if (!(rs > 0)) break;
-        // A: z = A v ; v.z
-        vals[0] = 0;
-        for (int ps = 0; ps < passes; ps++) {
-            const int i = gslot + ps * sites_per_pass;
-            V3 Av = i < n ? amul<G4, GR>(c, i, t, g1) : v3(0, 0, 0);
-            Av.x = group_sum<CG_TPP>(Av.x); Av.y = group_sum<CG_TPP>(Av.y); Av.z = group_sum<CG_TPP>(Av.z);
-            if (i < n && t == 0) {
-                c.z[i] = Av.x; c.z[n + i] = Av.y; c.z[2 * n + i] = Av.z;
-                vals[0] += __ldcg(&c.v[i]) * Av.x + __ldcg(&c.v[n + i]) * Av.y + __ldcg(&c.v[2 * n + i]) * Av.z;
-            }
-        }
-        block_partials(vals, 1, part1, s_w);
-        if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
-        grid_sum(part1, c.nblocks, 1, tot, s_w);
-        const double alpha_cg = rs / tot[0];
-        // B: p += alpha v ; r -= alpha z ; rs' = r.M^-1 r ; dp2 = |alpha v|^2
+        if (!(gamma > 0) || !(alpha_cg > 0)) break;
+        // U: p = u + beta p ; s = w + beta s ; x += alpha p ; r -= alpha s ;
+        //    u = M^-1 r ; gamma' = r.u ; |alpha p|^2
         vals[0] = 0; vals[1] = 0;
         for (int i = gtid; i < n; i += nthreads) {
             const double al = __ldcg(&c.al[i]);
+            double w3[3];
             for (int d = 0; d < 3; d++) {
                 const int idx = d * n + i;
-                const double dp = alpha_cg * __ldcg(&c.v[idx]);
+                const double pd = __ldcg(&c.u[idx]) + (it ? beta * __ldcg(&c.v[idx]) : 0.0);
+                const double sd = __ldcg(&c.z[idx]) + (it ? beta * __ldcg(&c.s[idx]) : 0.0);
+                c.v[idx] = pd;
+                c.s[idx] = sd;
+                const double dp = alpha_cg * pd;
                 a.p[idx] = __ldcg(&a.p[idx]) + dp;
-                const double r = __ldcg(&c.r[idx]) - alpha_cg * __ldcg(&c.z[idx]);
+                const double r = __ldcg(&c.r[idx]) - alpha_cg * sd;
                 c.r[idx] = r;
-                vals[0] += r * al * r;
+                w3[d] = al * r;
+                c.u[idx] = w3[d];
+                vals[0] += r * w3[d];
                 vals[1] += dp * dp;
             }
+            g1[i] = G4{(GR)w3[0], (GR)w3[1], (GR)w3[2], (GR)0};
         }
-        block_partials(vals, 2, part0, s_w);
+        double *const pu = (it & 1) ? pu1 : pu0;
+        block_partials(vals, 2, pu, s_w);
         if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
-        grid_sum(part0, c.nblocks, 2, tot, s_w);
-        const double rs_new = tot[0];
+        grid_sum(pu, c.nblocks, 2, tot, s_w);
+        const double gamma_new = tot[0];
         rms = sqrt(tot[1] / (3.0 * n));
         if (rms < c.tol) { it++; break; }
-        const double beta = rs_new / rs;
-        rs = rs_new;
-        // C: v = M^-1 r + beta v
-        for (int i = gtid; i < n; i += nthreads) {
-            const double al = __ldcg(&c.al[i]);
-            double w[3];
-            for (int d = 0; d < 3; d++) {
-                const int idx = d * n + i;
-                w[d] = al * __ldcg(&c.r[idx]) + beta * __ldcg(&c.v[idx]);
-                c.v[idx] = w[d];
+        // W: w = A u ; delta' = w.u
+        vals[0] = 0;
+        for (int ps = 0; ps < passes; ps++) {
+            const int i = gslot + ps * sites_per_pass;
+            V3 Au = i < n ? amul<G4, GR>(c, i, t, g1) : v3(0, 0, 0);
+            Au.x = group_sum<CG_TPP>(Au.x); Au.y = group_sum<CG_TPP>(Au.y); Au.z = group_sum<CG_TPP>(Au.z);
+            if (i < n && t == 0) {
+                c.z[i] = Au.x; c.z[n + i] = Au.y; c.z[2 * n + i] = Au.z;
+                vals[0] += __ldcg(&c.u[i]) * Au.x + __ldcg(&c.u[n + i]) * Au.y + __ldcg(&c.u[2 * n + i]) * Au.z;
             }
-            g1[i] = G4{(GR)w[0], (GR)w[1], (GR)w[2], (GR)0};
         }
+        double *const pw = (it & 1) ? pw1 : pw0;
+        block_partials(vals, 1, pw, s_w);
         if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
+        grid_sum(pw, c.nblocks, 1, tot, s_w);
+        const double delta = tot[0];
+        beta = gamma_new / gamma;
+        alpha_cg = gamma_new / (delta - beta * gamma_new / alpha_cg);
+        gamma = gamma_new;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         c.scal[0] = it;
@@ -625,18 +651,12 @@ __device__ __forceinline__ void ind_algebra_f(float qi, F3 mi, const Q6F &Qi, F3
     A.Gt3 = (2.f * pjr) * crs(Qir, r);
 }
 
-__device__ __forceinline__ void ind_pair_mixed(const IndAlgF &A, V3 r, double r2, double poli, double polj,
-                                               double a, double alpha, double scale, IndPairOut &o) {
+// the radial part given the Ewald B_0..B_4 of the pair (bn_erfc)
+__device__ __forceinline__ void ind_pair_mixed_b(const IndAlgF &A, V3 r, double r2, const double *B, double poli,
+                                                 double polj, double a, double scale, IndPairOut &o) {
     const double rr = sqrt(r2);
     const double u3 = rr * rr * rr / sqrt(poli * polj);
-    const double a2 = alpha * alpha, a2pi = 2.0 * alpha / SQRT_PI_I, ex = exp(-a2 * r2);
-    double B[5];
-    B[0] = erfc(alpha * rr) / rr;
     const double ir2 = 1.0 / r2;
-    B[1] = (-B[0] - a2pi * ex) * ir2;
-    B[2] = (-3 * B[1] + 2 * a2pi * a2 * ex) * ir2;
-    B[3] = (-5 * B[2] - 4 * a2pi * a2 * a2 * ex) * ir2;
-    B[4] = (-7 * B[3] + 8 * a2pi * a2 * a2 * a2 * ex) * ir2;
     const double e = exp(-a * u3), au3 = a * u3, a2u6 = au3 * au3, a3u9 = a2u6 * au3;
     const double l3 = 1.0 - e;
     const double gl3 = 3.0 * au3 * e * ir2;
@@ -657,6 +677,13 @@ __device__ __forceinline__ void ind_pair_mixed(const IndAlgF &A, V3 r, double r2
                   (scale * (A.G1j * B2d + A.G2j * B3d + A.G3j * B4d)) * (-r);
     o.fij = fi - fj;
     o.tau = scale * (B1d * to_v3(A.Gt1) + B2d * to_v3(A.Gt2) + B3d * to_v3(A.Gt3));
+}
+
+__device__ __forceinline__ void ind_pair_mixed(const IndAlgF &A, V3 r, double r2, double poli, double polj,
+                                               double a, double alpha, double scale, IndPairOut &o) {
+    double B[6];
+    bn_erfc(r2, alpha, B);
+    ind_pair_mixed_b(A, r, r2, B, poli, polj, a, scale, o);
 }
 
 struct IndRealArgs {
@@ -805,6 +832,106 @@ __global__ void __launch_bounds__(64) k_ind_real_f(IndRealArgs A) {
     }
 }
 
+// Mixed path, one pass for both real-space polarisable terms after the
+// dipole solve: the multipole real-space term of k_mp_real_f and the induced
+// term of k_ind_real_f share the pair loop, the partner's site record and
+// the Ewald B_n of the pair.  Energies go to their own slots; forces,
+// torques and virial are summed.
+__global__ void __launch_bounds__(64) k_polar_real_f(IndRealArgs A) {
+    const IndArgs &a = A.ia;
+    constexpr int TPP = 8;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gt / TPP, t = gt % TPP;
+    V3 f = v3(0, 0, 0), tau = v3(0, 0, 0);
+    double emp = 0, eind = 0, w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (i < a.n) {
+        const int4 fi = A.fixq[i];
+        const double poli = a.polar[fi.w];
+        const double qi_d = a.tq[fi.w] / SQC;
+        const float4 *ri = A.srec + 4 * (size_t)i;
+        const float4 i0 = ri[0], i1 = ri[1], i2 = ri[2], i3 = ri[3];
+        const float qi = i0.x;
+        const F3 mi = f3(i0.y, i0.z, i0.w);
+        const F3 pii = f3(i2.z, i2.w, i3.x);
+        const Q6F Qi = {i1.x, i1.y, i1.z, i1.w, i2.x, i2.y};
+        const double s2u = A.dscale[0] * A.dscale[0];
+        // listed: a Verlet-list neighbour (both terms); otherwise one of the
+        // molecule's excluded sites (induced term with its permanent part
+        // scaled by 0)
+        auto pair = [&](int j, bool listed) {
+            const int4 fj = A.fixq[j];
+            const int ix = fi.x - fj.x, iy = fi.y - fj.y, iz = fi.z - fj.z;   // r = r_i - r_j
+            const unsigned long long s2 = (unsigned long long)((long long)ix * ix) +
+                                          (unsigned long long)((long long)iy * iy) +
+                                          (unsigned long long)((long long)iz * iz);
+            const double r2 = (double)s2 * s2u;
+            if (!(r2 < a.rc2)) return;
+            const V3 r = v3(ix * A.dscale[0], iy * A.dscale[1], iz * A.dscale[2]);
+            const F3 rf = f3((float)r.x, (float)r.y, (float)r.z);
+            const float4 *rj = A.srec + 4 * (size_t)j;
+            const float4 j0 = __ldg(rj), j1 = __ldg(rj + 1), j2 = __ldg(rj + 2), j3 = __ldg(rj + 3);
+            const F3 mj = f3(j0.y, j0.z, j0.w);
+            const Q6F Qj = {j1.x, j1.y, j1.z, j1.w, j2.x, j2.y};
+            double B[6];
+            bn_erfc(r2, a.alpha, B);
+            V3 fij = v3(0, 0, 0), ti = v3(0, 0, 0);
+            if (listed) {
+                MPPair<float, F3> P;
+                mp_invariants(qi, mi, Qi, j0.x, mj, Qj, rf, P);
+                const double G0 = qi_d * (a.tq[fj.w] / SQC);
+                emp += G0 * B[0] + P.G[1] * B[1] + P.G[2] * B[2] + P.G[3] * B[3] + P.G[4] * B[4];
+                const double radial = G0 * B[1] + P.G[1] * B[2] + P.G[2] * B[3] + P.G[3] * B[4] + P.G[4] * B[5];
+                fij = -(B[1] * to_v3(P.gG[1]) + B[2] * to_v3(P.gG[2]) + B[3] * to_v3(P.gG[3]) +
+                        B[4] * to_v3(P.gG[4])) -
+                      radial * r;
+                F3 Gt[5];
+                mp_torque_i(j0.x, mi, Qi, mj, Qj, rf, Gt);
+                ti = B[1] * to_v3(Gt[1]) + B[2] * to_v3(Gt[2]) + B[3] * to_v3(Gt[3]) + B[4] * to_v3(Gt[4]);
+            }
+            IndAlgF al;
+            ind_algebra_f(qi, mi, Qi, pii, j0.x, mj, Qj, f3(j2.z, j2.w, j3.x), rf, al);
+            IndPairOut o;
+            ind_pair_mixed_b(al, r, r2, B, poli, a.polar[fj.w], a.a, listed ? 1.0 : 0.0, o);
+            eind += o.e;
+            fij = fij + o.fij;
+            f = f + fij;
+            tau = tau + ti + o.tau;
+            const double fr[3] = {fij.x, fij.y, fij.z}, rr[3] = {r.x, r.y, r.z};
+            for (int p = 0; p < 3; p++)
+                for (int q = 0; q < 3; q++) w[3 * p + q] -= 0.5 * fr[q] * rr[p];
+        };
+        const int cnt = a.nnbr[i];
+        for (int k = t; k < cnt; k += TPP) pair(a.nbr[(size_t)k * a.n + i] & 0x7fffffff, true);
+        if (t == 0) {
+            const int m = a.mol[i];
+            for (int q = a.mol_off[m]; q < a.mol_off[m + 1]; q++) {
+                const int j = a.mol_atoms[q];
+                if (j != i && is_excluded(i, j, a.excl_off, a.excl)) pair(j, false);
+            }
+        }
+    }
+    f.x = group_sum<TPP>(f.x); f.y = group_sum<TPP>(f.y); f.z = group_sum<TPP>(f.z);
+    tau.x = group_sum<TPP>(tau.x); tau.y = group_sum<TPP>(tau.y); tau.z = group_sum<TPP>(tau.z);
+    if (i < a.n && t == 0) {
+        add_fix3(A.frc, a.n, i, f, COU);
+        add_fix3(A.trq, a.n, i, tau, COU);
+    }
+    __shared__ double s_r[2][11];
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    double vals[11] = {0.5 * emp * COU, 0.5 * eind * COU, w[0], w[1], w[2], w[3], w[4], w[5], w[6], w[7], w[8]};
+    for (int q = 0; q < 11; q++) {
+        double sv = warp_sum(vals[q]);
+        if (lane == 0) s_r[wp][q] = sv;
+    }
+    __syncthreads();
+    if (threadIdx.x < 11) {
+        double sv = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) sv += s_r[q][threadIdx.x];
+        const int slot = threadIdx.x == 0 ? ACC_E_REAL : (threadIdx.x == 1 ? ACC_E_POL_REAL : ACC_VIR + threadIdx.x - 2);
+        if (sv != 0.0) atomicAdd((unsigned long long *)&A.acc[slot], (unsigned long long)to_fix(sv, ACC_SCALE));
+    }
+}
+
 // self energy + torque, intramolecular correction energy
 __global__ void k_ind_mol(IndArgs a, long long *trq, long long *acc) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -939,6 +1066,7 @@ void launch_ind_solve(Ctx &c) {
     const size_t n = c.n;
     g.r = c.cgw; g.z = c.cgw + 3 * n; g.v = c.cgw + 6 * n; g.al = c.cgw + 9 * n;
     g.g0 = c.cgw + 12 * n; g.g1 = c.cgw + 16 * n;
+    g.s = c.cgw + 20 * n; g.u = c.cgw + 23 * n;
     g.part = c.cgs + 8; g.scal = c.cgs; g.bar = c.cg_bar; g.status = c.status;
     g.nblocks = c.cg_blocks; g.max_iter = c.cg_max_iter; g.tol = c.cg_tol;
     // 0: start from alpha E0; 1: start from the dipoles in p (previous solve or network)
@@ -984,6 +1112,32 @@ void launch_ind_short(Ctx &c) {
     } else {
         k_ind_real<<<nb, 64, 0, c.stream>>>(A);
     }
+    k_ind_mol<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(A.ia, c.trq, c.acc);
+}
+
+bool polar_short_fused(const Ctx &c) {
+    const bool cubic = c.box.L[0] == c.box.L[1] && c.box.L[1] == c.box.L[2];
+    return c.precision == SMD_PREC_MIXED && cubic && c.srec && c.ind_on;
+}
+
+// Both real-space polarisable terms after the dipole solve: one fused pass
+// in the mixed path, the two separate passes otherwise
+void launch_polar_short(Ctx &c) {
+    if (!polar_short_fused(c)) {
+        launch_mp_short(c);
+        launch_ind_short(c);
+        return;
+    }
+    IndRealArgs A;
+    A.ia = ind_args(c);
+    A.frc = c.frc; A.trq = c.trq; A.acc = c.acc;
+    if (!c.fixq_from_integrate) launch_fixq(c);
+    A.fixq = c.fixq;
+    A.srec = c.srec;
+    for (int d = 0; d < 3; d++) A.dscale[d] = c.box.L[d] / 4294967296.0;
+    const int nb = (int)(((long long)c.n * 8 + 63) / 64);
+    k_polar_real_f<<<nb, 64, 0, c.stream>>>(A);
+    launch_mp_mol(c);
     k_ind_mol<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(A.ia, c.trq, c.acc);
 }
 

@@ -128,75 +128,6 @@ void launch_pack_sites(Ctx &c) {
 }
 
 // ---------------------------------------------------------------------------
-// pair invariants of the multipole-multipole interaction (r = r_i - r_j)
-// ---------------------------------------------------------------------------
-template <class R, class V>
-struct MPPair {
-    R G[5];
-    V gG[5];   // gradients of G1..G4 (gG[0] unused)
-};
-
-// The invariants and torque coefficients are written once for the FP64 path
-// (V3, Q6, double) and the mixed path's FP32 algebra (F3, Q6F, float).
-template <class R, class V, class Q>
-__device__ __forceinline__ void mp_invariants(R qi, V mi, const Q &Qi, R qj, V mj, const Q &Qj, V r,
-                                              MPPair<R, V> &P) {
-    const R QiI = qtr(Qi), QjI = qtr(Qj);
-    const V Qir = qv(Qi, r), Qjr = qv(Qj, r);
-    const R QiRij = dot(r, Qir), QjRij = dot(r, Qjr);
-    const R mir = dot(mi, r), mjr = dot(mj, r);
-    P.G[0] = qi * qj;
-    P.G[1] = qj * mir - qi * mjr - dot(mi, mj) + qj * QiI + qi * QjI;
-    P.G[2] = qj * QiRij + qi * QjRij - mir * mjr - mjr * QiI + mir * QjI - R(2) * dot(mj, Qir) +
-             R(2) * dot(mi, Qjr) + QiI * QjI + R(2) * qdd(Qi, Qj);
-    P.G[3] = mir * QjRij - mjr * QiRij + QiI * QjRij + QjI * QiRij + R(4) * dot(Qir, Qjr);
-    P.G[4] = QiRij * QjRij;
-    P.gG[1] = qj * mi - qi * mj;
-    P.gG[2] = (R(2) * qj) * Qir - mjr * mi - mir * mj - R(2) * qv(Qi, mj) - QiI * mj + (R(2) * qi) * Qjr +
-              R(2) * qv(Qj, mi) + QjI * mi;
-    P.gG[3] = (-QiRij) * mj - (R(2) * mjr) * Qir + QjRij * mi + (R(2) * mir) * Qjr + (R(2) * QiI) * Qjr +
-              (R(2) * QjI) * Qir + R(4) * qv(Qi, Qjr) + R(4) * qv(Qj, Qir);
-    P.gG[4] = (R(2) * QjRij) * Qir + (R(2) * QiRij) * Qjr;
-}
-
-// torque coefficients on site i (Multipole.cpp real_term, Gt1i..Gt4i)
-template <class R, class V, class Q>
-__device__ __forceinline__ void mp_torque_i(R qj, V mi, const Q &Qi, V mj, const Q &Qj, V r, V Gt[5]) {
-    const V Qir = qv(Qi, r), Qjr = qv(Qj, r);
-    const R QjI = qtr(Qj), QjRij = dot(r, Qjr), mjr = dot(mj, r);
-    const V rxmi = crs(r, mi);
-    const V RxQi = crs(r, Qir);
-    Gt[1] = qj * rxmi - crs(mj, mi);
-    Gt[2] = (-mjr) * rxmi + R(2) * crs(Qjr, mi) + QjI * rxmi + (R(2) * qj) * RxQi -
-            R(2) * crs(mj, Qir) - R(2) * crs(r, qv(Qi, mj)) + R(4) * qcross(Qj, Qi);
-    Gt[3] = QjRij * rxmi - (R(2) * mjr) * RxQi + (R(2) * QjI) * RxQi + R(4) * crs(r, qv(Qi, Qjr)) +
-            R(4) * crs(Qjr, Qir);
-    Gt[4] = (R(2) * QjRij) * RxQi;
-}
-
-// B_n of erfc(a r)/r (Multipole.cpp:632-637); D_n of erf(a r)/r (:1495-1500)
-__device__ __forceinline__ void bn_erfc(double r2, double alpha, double B[6]) {
-    const double a2 = alpha * alpha, a2pi = 2.0 * alpha / SQRT_PI_D;
-    const double r = sqrt(r2), ex = exp(-a2 * r2), ir2 = 1.0 / r2;
-    B[0] = erfc(alpha * r) / r;
-    B[1] = (-B[0] - a2pi * ex) * ir2;
-    B[2] = (-3 * B[1] + 2 * a2pi * a2 * ex) * ir2;
-    B[3] = (-5 * B[2] - 4 * a2pi * a2 * a2 * ex) * ir2;
-    B[4] = (-7 * B[3] + 8 * a2pi * a2 * a2 * a2 * ex) * ir2;
-    B[5] = (-9 * B[4] - 16 * a2pi * a2 * a2 * a2 * a2 * ex) * ir2;
-}
-__device__ __forceinline__ void dn_erf(double r2, double alpha, double D[6]) {
-    const double a2 = alpha * alpha, a2pi = 2.0 * alpha / SQRT_PI_D;
-    const double r = sqrt(r2), ex = exp(-a2 * r2);
-    D[0] = erf(alpha * r) / r;
-    D[1] = (-D[0] + a2pi * ex) / r2;
-    D[2] = (-3 * D[1] - 2 * a2pi * a2 * ex) / r2;
-    D[3] = (-5 * D[2] + 4 * a2pi * a2 * a2 * ex) / r2;
-    D[4] = (-7 * D[3] - 8 * a2pi * a2 * a2 * a2 * ex) / r2;
-    D[5] = (-9 * D[4] + 16 * a2pi * a2 * a2 * a2 * a2 * ex) / r2;
-}
-
-// ---------------------------------------------------------------------------
 // real space
 // ---------------------------------------------------------------------------
 struct MPArgs {
@@ -485,6 +416,11 @@ void launch_mp_short(Ctx &c) {
     } else {
         k_mp_real<tpp><<<nb, 128, 0, c.stream>>>(a);
     }
+    launch_mp_mol(c);
+}
+
+// self energy and intramolecular correction of the multipoles
+void launch_mp_mol(Ctx &c) {
     k_mp_mol<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.n, c.mol_off, c.mol_atoms, c.excl_off,
                                                          c.excl, c.pos4, c.type_q, c.mu, c.qd, c.box,
                                                          c.ew_alpha, c.acc);

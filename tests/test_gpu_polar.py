@@ -113,6 +113,37 @@ def test_mixed_terms_against_reference(term, fkey, ekey, eidx):
     e.close()
 
 
+def test_mixed_full_evaluation():
+    # a full mixed evaluation runs the multipole and the induced real space
+    # as one fused pass after the dipole solve: it equals the sum of the
+    # single-term evaluations (separate passes) and the reference's total
+    g = golden("polwater216")
+    e = engine.GpuEnsemble(_pw(), precision="mixed")
+    e.set_solver(tol=1e-13, max_iter=1000)
+    f_all, en_all, w_all = e.compute_forces()
+    f_sum = np.zeros_like(f_all)
+    en = {}
+    for term in (L.TERM_VDW, L.TERM_MP_SHORT, L.TERM_MP_LONG, L.TERM_IND_SHORT, L.TERM_IND_LONG):
+        f, en[term], _ = e.compute_forces(term)
+        f_sum += f
+    # the fused pass does the same pair arithmetic as the two separate ones
+    for slot, term in ((L.E_REAL, L.TERM_MP_SHORT), (L.E_POL_REAL, L.TERM_IND_SHORT)):
+        assert abs(en_all[slot] - en[term][slot]) < 1e-10 * abs(en[term][slot])
+    # a full evaluation takes the reciprocal terms from one combined pass
+    # (six structure factors, one force pass), the single-term calls from
+    # separate FP32 passes: the totals agree to FP32 rounding
+    print("full vs terms", rms_rel(f_all, f_sum))
+    assert rms_rel(f_all, f_sum) < 3e-7
+    ref = sum(g[k].reshape(-1, 3) for k in ("f_buff_force", "f_mp_short_force", "f_mp_long_force",
+                                            "f_ind_short_force", "f_ind_long_force"))
+    err = rms_rel(f_all, ref)
+    print("mixed total vs reference", err)
+    assert err < 1e-6
+    assert abs(en_all[L.E_REAL] - g["f_mp_short_energy"][1]) < 1e-6 * abs(g["f_mp_short_energy"][1])
+    assert abs(en_all[L.E_POL_REAL] - g["f_ind_short_energy"][6]) < 1e-6 * abs(g["f_ind_short_energy"][6])
+    e.close()
+
+
 def test_polar_trajectory():
     g = golden("polwater216")
     e = engine.GpuEnsemble(_pw())
