@@ -87,6 +87,7 @@ struct TRows {
     int *j;       // [N][cap]
     void *c;      // [N][cap] of TS4
     int *cnt;     // [N]
+    int *lcnt;    // [N] slots taken by Verlet-list partners (the molecule's sites follow)
     int cap;
 };
 
@@ -150,6 +151,7 @@ __global__ void __launch_bounds__(256) k_ind_field(IndArgs a, TRows R, unsigned 
     E.x = group_sum<TPP>(E.x); E.y = group_sum<TPP>(E.y); E.z = group_sum<TPP>(E.z);
     if (own && t == 0) {
         a.e0[i] = E.x; a.e0[a.n + i] = E.y; a.e0[2 * a.n + i] = E.z;
+        R.lcnt[i] = base < R.cap ? base : R.cap;
         const int m = a.mol[i];
         for (int q = a.mol_off[m]; q < a.mol_off[m + 1]; q++) {
             const int j = a.mol_atoms[q];
@@ -252,6 +254,7 @@ __global__ void __launch_bounds__(256) k_ind_field_f(IndArgs a, FieldMixArgs m, 
     E.x = group_sum<TPP>(E.x); E.y = group_sum<TPP>(E.y); E.z = group_sum<TPP>(E.z);
     if (own && t == 0) {
         a.e0[i] = E.x; a.e0[a.n + i] = E.y; a.e0[2 * a.n + i] = E.z;
+        R.lcnt[i] = base < R.cap ? base : R.cap;
         const double4 pi = a.pos4[i];
         const double poli = fmax(1e-8, a.polar[(int)pi.w]);
         const int mo = a.mol[i];
@@ -692,6 +695,8 @@ struct IndRealArgs {
     const int4 *fixq;      // mixed path: box fractions
     const float4 *srec;    // mixed path: FP32 site records (q, mu, Q, p)
     double dscale[3];      // L / 2^32 per axis
+    const int *rj, *rcnt, *rlcnt;   // the solve's tensor rows (partners within cutoffInd)
+    int rcap;
 };
 
 __global__ void __launch_bounds__(64) k_ind_real(IndRealArgs A) {
@@ -836,7 +841,12 @@ __global__ void __launch_bounds__(64) k_ind_real_f(IndRealArgs A) {
 // dipole solve: the multipole real-space term of k_mp_real_f and the induced
 // term of k_ind_real_f share the pair loop, the partner's site record and
 // the Ewald B_n of the pair.  Energies go to their own slots; forces,
-// torques and virial are summed.
+// torques and virial are summed.  ROWS: the partners come from the solve's
+// tensor rows (the Verlet-list partners within cutoffInd, compacted, then the
+// molecule's excluded sites), which hold every pair inside the real-space
+// cutoff when cutoffInd is at least that cutoff, so that no lane idles on a
+// list entry beyond it.
+template <bool ROWS>
 __global__ void __launch_bounds__(64) k_polar_real_f(IndRealArgs A) {
     const IndArgs &a = A.ia;
     constexpr int TPP = 8;
@@ -900,13 +910,20 @@ __global__ void __launch_bounds__(64) k_polar_real_f(IndRealArgs A) {
             for (int p = 0; p < 3; p++)
                 for (int q = 0; q < 3; q++) w[3 * p + q] -= 0.5 * fr[q] * rr[p];
         };
-        const int cnt = a.nnbr[i];
-        for (int k = t; k < cnt; k += TPP) pair(a.nbr[(size_t)k * a.n + i] & 0x7fffffff, true);
-        if (t == 0) {
-            const int m = a.mol[i];
-            for (int q = a.mol_off[m]; q < a.mol_off[m + 1]; q++) {
-                const int j = a.mol_atoms[q];
-                if (j != i && is_excluded(i, j, a.excl_off, a.excl)) pair(j, false);
+        if (ROWS) {
+            const int *rj = A.rj + (size_t)i * A.rcap;
+            const int lc = A.rlcnt[i], cnt = A.rcnt[i];
+            for (int k = t; k < lc; k += TPP) pair(rj[k], true);
+            for (int k = lc + t; k < cnt; k += TPP) pair(rj[k], false);
+        } else {
+            const int cnt = a.nnbr[i];
+            for (int k = t; k < cnt; k += TPP) pair(a.nbr[(size_t)k * a.n + i] & 0x7fffffff, true);
+            if (t == 0) {
+                const int m = a.mol[i];
+                for (int q = a.mol_off[m]; q < a.mol_off[m + 1]; q++) {
+                    const int j = a.mol_atoms[q];
+                    if (j != i && is_excluded(i, j, a.excl_off, a.excl)) pair(j, false);
+                }
             }
         }
     }
@@ -1034,7 +1051,7 @@ int ensure_ind_rows(Ctx &c) {
     const size_t slots = (size_t)c.n * cap;
     if (cudaMalloc(&c.ind_rj, slots * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&c.ind_rc, slots * sizeof(double4)) != cudaSuccess ||
-        cudaMalloc(&c.ind_cnt, (size_t)c.n * sizeof(int)) != cudaSuccess)
+        cudaMalloc(&c.ind_cnt, 2 * (size_t)c.n * sizeof(int)) != cudaSuccess)
         return SMD_ERR_CUDA;
     c.ind_cap = cap;
     c.graph_dirty = 1;
@@ -1045,7 +1062,7 @@ void launch_ind_solve(Ctx &c) {
     IndArgs a = ind_args(c);
     const bool f32 = c.precision == SMD_PREC_MIXED;
     TRows R;
-    R.j = c.ind_rj; R.c = c.ind_rc; R.cnt = c.ind_cnt; R.cap = c.ind_cap;
+    R.j = c.ind_rj; R.c = c.ind_rc; R.cnt = c.ind_cnt; R.lcnt = c.ind_cnt + c.n; R.cap = c.ind_cap;
     const int nb = (int)(((long long)c.n * 8 + 255) / 256);
     const bool cubic = c.box.L[0] == c.box.L[1] && c.box.L[1] == c.box.L[2];
     if (f32 && cubic && c.srec && c.ntypes <= 8) {
@@ -1135,8 +1152,14 @@ void launch_polar_short(Ctx &c) {
     A.fixq = c.fixq;
     A.srec = c.srec;
     for (int d = 0; d < 3; d++) A.dscale[d] = c.box.L[d] / 4294967296.0;
+    A.rj = c.ind_rj; A.rcnt = c.ind_cnt; A.rlcnt = c.ind_cnt + c.n; A.rcap = c.ind_cap;
     const int nb = (int)(((long long)c.n * 8 + 63) / 64);
-    k_polar_real_f<<<nb, 64, 0, c.stream>>>(A);
+    // the rows hold every pair inside the real-space cutoff when cutoffInd
+    // reaches it; the pair test r^2 < rc^2 stays in the kernel
+    if (c.ind_cut2 >= c.mp_rc2)
+        k_polar_real_f<true><<<nb, 64, 0, c.stream>>>(A);
+    else
+        k_polar_real_f<false><<<nb, 64, 0, c.stream>>>(A);
     launch_mp_mol(c);
     k_ind_mol<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(A.ia, c.trq, c.acc);
 }
