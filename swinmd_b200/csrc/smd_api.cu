@@ -295,7 +295,7 @@ int smd_set_topology(smd_ctx *x, int n, int ntypes, const int32_t *atom_type,
     CK(dalloc(&c.frc, 3 * (size_t)n));
     CK(dalloc(&c.pl.nnbr, n)); CK(dalloc(&c.pl.cell_of, n)); CK(dalloc(&c.pl.cell_slot, n));
     CK(dalloc(&c.pl.cell_atoms, n));
-    int nb = (nmol + 127) / 128;
+    int nb = (nmol + 31) / 32;   // the integrate kernels' smallest blocks
     CK(dalloc(&c.partials, (size_t)nb * 40));  // per block: NPART (35) partial sums
     CK(cudaMemcpy(c.type, atom_type, n * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.mol, mol_id, n * sizeof(int), cudaMemcpyHostToDevice));

@@ -82,6 +82,122 @@ __device__ __forceinline__ void pbc3(double &x, double &y, double &z, const Box 
 
 constexpr int MAX_MOL_SITES = 8;
 
+// SHAKE step of one molecule (LFIntegrator::shake, NVT branch) and its
+// contributions to the observables.  NS > 0 fixes the number of sites at
+// compile time, so that every loop over sites and bonds unrolls and the
+// per-site arrays stay in registers (three-site water); NS = 0 takes the
+// count at run time (up to MAX_MOL_SITES sites, arrays in local memory).
+template <int NS>
+__device__ __forceinline__ void shake_mol(const IntArgs &a, int m, int s, int e, int ns_rt, double fnh,
+                                          bool apply_vom, double vomx, double vomy, double vomz,
+                                          double (&part)[NPART], bool &rebuild, bool &bad, bool &shake_fail,
+                                          bool &shake_geom, double &cx, double &cy, double &cz, double &px,
+                                          double &py, double &pz, double &M) {
+    constexpr int CAP = NS ? NS : MAX_MOL_SITES;
+    const int ns = NS ? NS : ns_rt;
+    // molecular momentum of the previous step (Molecule::momenta)
+    double Px = 0, Py = 0, Pz = 0;
+    for (int k = s; k < e; k++) {
+        const double4 v = a.vel4[a.mol_atoms[k]];
+        const double mass = 1.0 / v.w;
+        Px += v.x * mass; Py += v.y * mass; Pz += v.z * mass;
+    }
+    double ro[CAP][3], rn[CAP][3], mr[CAP];
+    double4 vmv[CAP];
+    for (int q = 0; q < ns; q++) {
+        const int at = a.mol_atoms[s + q];
+        double4 vm = a.vtm4[at];
+        if (apply_vom) { vm.x -= vomx; vm.y -= vomy; vm.z -= vomz; }
+        vmv[q] = vm;
+        mr[q] = 1.0 / vm.w;
+        const double3 f = fetch_force(a.frc, a.n, at);
+        const double4 p = a.pos4[at];
+        double vpx, vpy, vpz;
+        if (a.thermostat == SMD_THERMO_NOSE_HOOVER) {
+            vpx = vm.x + a.dt * mr[q] * (f.x - fnh * Px / ns);
+            vpy = vm.y + a.dt * mr[q] * (f.y - fnh * Py / ns);
+            vpz = vm.z + a.dt * mr[q] * (f.z - fnh * Pz / ns);
+        } else {
+            vpx = vm.x + a.dt * mr[q] * f.x;
+            vpy = vm.y + a.dt * mr[q] * f.y;
+            vpz = vm.z + a.dt * mr[q] * f.z;
+        }
+        ro[q][0] = p.x; ro[q][1] = p.y; ro[q][2] = p.z;
+        rn[q][0] = p.x + a.dt * vpx; rn[q][1] = p.y + a.dt * vpy; rn[q][2] = p.z + a.dt * vpz;
+    }
+    const int nb = (ns == 3) ? 3 : ns - 1;
+    const double tol2 = 2 * a.shake_tol;
+    const double *bl = a.clen2 + (size_t)m * 3;
+    // the old bond vectors stay fixed during the iteration: their
+    // minimum images once, and the SHAKE virial sum_k f_k n_k (x) o
+    // as (sum_k f_k n_k) (x) o per bond at the end
+    double ob[CAP][3], sfn[CAP][3];
+    for (int i = 0; i < nb; i++) {
+        const int nx = i + 1 == ns ? 0 : i + 1;
+        double ox = ro[i][0] - ro[nx][0], oy = ro[i][1] - ro[nx][1], oz = ro[i][2] - ro[nx][2];
+        pbc3(ox, oy, oz, a.box);
+        ob[i][0] = ox; ob[i][1] = oy; ob[i][2] = oz;
+        sfn[i][0] = 0; sfn[i][1] = 0; sfn[i][2] = 0;
+    }
+    int count = 0;
+    bool done = false;
+    while (!done && count < a.shake_max) {
+        done = true;
+        for (int i = 0; i < nb; i++) {
+            int nx = i + 1;
+            if (nx == ns) nx = 0;
+            double nx_ = rn[i][0] - rn[nx][0], ny_ = rn[i][1] - rn[nx][1], nz_ = rn[i][2] - rn[nx][2];
+            pbc3(nx_, ny_, nz_, a.box);
+            const double r2 = nx_ * nx_ + ny_ * ny_ + nz_ * nz_;
+            const double blen = bl[i < 3 ? i : 2];
+            const double diff = blen - r2;
+            if (fabs(diff) > blen * tol2) {
+                const double ox = ob[i][0], oy = ob[i][1], oz = ob[i][2];
+                const double rr = ox * nx_ + oy * ny_ + oz * nz_;
+                if (rr < blen * a.shake_tol) { shake_geom = true; done = true; count = a.shake_max; break; }
+                const double factor = diff / (2 * rr * (mr[i] + mr[nx]));
+                sfn[i][0] += factor * nx_; sfn[i][1] += factor * ny_; sfn[i][2] += factor * nz_;
+                rn[i][0] += factor * ox * mr[i]; rn[i][1] += factor * oy * mr[i]; rn[i][2] += factor * oz * mr[i];
+                rn[nx][0] -= factor * ox * mr[nx]; rn[nx][1] -= factor * oy * mr[nx]; rn[nx][2] -= factor * oz * mr[nx];
+                done = false;
+            }
+        }
+        count++;
+    }
+    if (!done) shake_fail = true;
+    for (int i = 0; i < nb; i++)
+        for (int p = 0; p < 3; p++)
+            for (int q = 0; q < 3; q++) part[P_SV + 3 * p + q] += sfn[i][p] * ob[i][q];
+    for (int q = 0; q < ns; q++) {
+        const int at = a.mol_atoms[s + q];
+        double4 p = a.pos4[at];
+        const double drx = rn[q][0] - p.x, dry = rn[q][1] - p.y, drz = rn[q][2] - p.z;
+        p.x += drx; p.y += dry; p.z += drz;
+        double4 d = a.disp4[at];
+        d.x += drx; d.y += dry; d.z += drz;
+        if (d.x * d.x + d.y * d.y + d.z * d.z > a.drmax) rebuild = true;
+        double4 vm = vmv[q];
+        const double vpx = drx / a.dt, vpy = dry / a.dt, vpz = drz / a.dt;
+        double4 v = a.vel4[at];
+        v.x = (vpx + vm.x) * 0.5; v.y = (vpy + vm.y) * 0.5; v.z = (vpz + vm.z) * 0.5;
+        vm.x = vpx; vm.y = vpy; vm.z = vpz;
+        a.vel4[at] = v;
+        a.vtm4[at] = vm;
+        a.disp4[at] = d;
+        a.pos4[at] = p;
+        if (!isfinite(p.x + p.y + p.z)) bad = true;
+        const double mass = vm.w;
+        const double mx = v.x * mass, my = v.y * mass, mz = v.z * mass;
+        px += mx; py += my; pz += mz;
+        cx += mass * p.x; cy += mass * p.y; cz += mass * p.z;
+        M += mass;
+        part[P_KEA] += (v.x * v.x + v.y * v.y + v.z * v.z) * mass;
+        part[P_AP + 0] += mx * mx / mass; part[P_AP + 1] += mx * my / mass; part[P_AP + 2] += mx * mz / mass;
+        part[P_AP + 3] += my * my / mass; part[P_AP + 4] += my * mz / mass; part[P_AP + 5] += mz * mz / mass;
+        part[P_VM + 0] += vm.x * mass; part[P_VM + 1] += vm.y * mass; part[P_VM + 2] += vm.z * mass;
+    }
+}
+
 template <bool SHAKE>
 __global__ void __launch_bounds__(INT_BLOCK) k_integrate(IntArgs a) {
     __shared__ double s_part[INT_BLOCK / 32][NPART];
@@ -99,99 +215,12 @@ __global__ void __launch_bounds__(INT_BLOCK) k_integrate(IntArgs a) {
         const int s = a.mol_off[m], e = a.mol_off[m + 1];
         const int ns = e - s;
         double cx = 0, cy = 0, cz = 0, px = 0, py = 0, pz = 0, M = 0;
-        if (SHAKE && ns > 1 && ns <= MAX_MOL_SITES) {
-            // molecular momentum of the previous step (Molecule::momenta)
-            double Px = 0, Py = 0, Pz = 0;
-            for (int k = s; k < e; k++) {
-                const double4 v = a.vel4[a.mol_atoms[k]];
-                const double mass = 1.0 / v.w;
-                Px += v.x * mass; Py += v.y * mass; Pz += v.z * mass;
-            }
-            double ro[MAX_MOL_SITES][3], rn[MAX_MOL_SITES][3], mr[MAX_MOL_SITES];
-            double4 vmv[MAX_MOL_SITES];
-            for (int q = 0; q < ns; q++) {
-                const int at = a.mol_atoms[s + q];
-                double4 vm = a.vtm4[at];
-                if (apply_vom) { vm.x -= vomx; vm.y -= vomy; vm.z -= vomz; }
-                vmv[q] = vm;
-                mr[q] = 1.0 / vm.w;
-                const double3 f = fetch_force(a.frc, a.n, at);
-                const double4 p = a.pos4[at];
-                double vpx, vpy, vpz;
-                if (a.thermostat == SMD_THERMO_NOSE_HOOVER) {
-                    vpx = vm.x + a.dt * mr[q] * (f.x - fnh * Px / ns);
-                    vpy = vm.y + a.dt * mr[q] * (f.y - fnh * Py / ns);
-                    vpz = vm.z + a.dt * mr[q] * (f.z - fnh * Pz / ns);
-                } else {
-                    vpx = vm.x + a.dt * mr[q] * f.x;
-                    vpy = vm.y + a.dt * mr[q] * f.y;
-                    vpz = vm.z + a.dt * mr[q] * f.z;
-                }
-                ro[q][0] = p.x; ro[q][1] = p.y; ro[q][2] = p.z;
-                rn[q][0] = p.x + a.dt * vpx; rn[q][1] = p.y + a.dt * vpy; rn[q][2] = p.z + a.dt * vpz;
-            }
-            const int nb = (ns == 3) ? 3 : ns - 1;
-            const double tol2 = 2 * a.shake_tol;
-            const double *bl = a.clen2 + (size_t)m * 3;
-            int count = 0;
-            bool done = false;
-            while (!done && count < a.shake_max) {
-                done = true;
-                for (int i = 0; i < nb; i++) {
-                    int nx = i + 1;
-                    if (nx == ns) nx = 0;
-                    double nx_ = rn[i][0] - rn[nx][0], ny_ = rn[i][1] - rn[nx][1], nz_ = rn[i][2] - rn[nx][2];
-                    pbc3(nx_, ny_, nz_, a.box);
-                    const double r2 = nx_ * nx_ + ny_ * ny_ + nz_ * nz_;
-                    const double blen = bl[i < 3 ? i : 2];
-                    const double diff = blen - r2;
-                    if (fabs(diff) > blen * tol2) {
-                        double ox = ro[i][0] - ro[nx][0], oy = ro[i][1] - ro[nx][1], oz = ro[i][2] - ro[nx][2];
-                        pbc3(ox, oy, oz, a.box);
-                        const double rr = ox * nx_ + oy * ny_ + oz * nz_;
-                        if (rr < blen * a.shake_tol) { shake_geom = true; done = true; count = a.shake_max; break; }
-                        const double factor = diff / (2 * rr * (mr[i] + mr[nx]));
-                        part[P_SV + 0] += factor * nx_ * ox; part[P_SV + 1] += factor * nx_ * oy;
-                        part[P_SV + 2] += factor * nx_ * oz; part[P_SV + 3] += factor * ny_ * ox;
-                        part[P_SV + 4] += factor * ny_ * oy; part[P_SV + 5] += factor * ny_ * oz;
-                        part[P_SV + 6] += factor * nz_ * ox; part[P_SV + 7] += factor * nz_ * oy;
-                        part[P_SV + 8] += factor * nz_ * oz;
-                        rn[i][0] += factor * ox * mr[i]; rn[i][1] += factor * oy * mr[i]; rn[i][2] += factor * oz * mr[i];
-                        rn[nx][0] -= factor * ox * mr[nx]; rn[nx][1] -= factor * oy * mr[nx]; rn[nx][2] -= factor * oz * mr[nx];
-                        done = false;
-                    }
-                }
-                count++;
-            }
-            if (!done) shake_fail = true;
-            for (int q = 0; q < ns; q++) {
-                const int at = a.mol_atoms[s + q];
-                double4 p = a.pos4[at];
-                const double drx = rn[q][0] - p.x, dry = rn[q][1] - p.y, drz = rn[q][2] - p.z;
-                p.x += drx; p.y += dry; p.z += drz;
-                double4 d = a.disp4[at];
-                d.x += drx; d.y += dry; d.z += drz;
-                if (d.x * d.x + d.y * d.y + d.z * d.z > a.drmax) rebuild = true;
-                double4 vm = vmv[q];
-                const double vpx = drx / a.dt, vpy = dry / a.dt, vpz = drz / a.dt;
-                double4 v = a.vel4[at];
-                v.x = (vpx + vm.x) * 0.5; v.y = (vpy + vm.y) * 0.5; v.z = (vpz + vm.z) * 0.5;
-                vm.x = vpx; vm.y = vpy; vm.z = vpz;
-                a.vel4[at] = v;
-                a.vtm4[at] = vm;
-                a.disp4[at] = d;
-                a.pos4[at] = p;
-                if (!isfinite(p.x + p.y + p.z)) bad = true;
-                const double mass = vm.w;
-                const double mx = v.x * mass, my = v.y * mass, mz = v.z * mass;
-                px += mx; py += my; pz += mz;
-                cx += mass * p.x; cy += mass * p.y; cz += mass * p.z;
-                M += mass;
-                part[P_KEA] += (v.x * v.x + v.y * v.y + v.z * v.z) * mass;
-                part[P_AP + 0] += mx * mx / mass; part[P_AP + 1] += mx * my / mass; part[P_AP + 2] += mx * mz / mass;
-                part[P_AP + 3] += my * my / mass; part[P_AP + 4] += my * mz / mass; part[P_AP + 5] += mz * mz / mass;
-                part[P_VM + 0] += vm.x * mass; part[P_VM + 1] += vm.y * mass; part[P_VM + 2] += vm.z * mass;
-            }
+        if (SHAKE && ns == 3) {
+            shake_mol<3>(a, m, s, e, ns, fnh, apply_vom, vomx, vomy, vomz, part, rebuild, bad, shake_fail,
+                         shake_geom, cx, cy, cz, px, py, pz, M);
+        } else if (SHAKE && ns > 1 && ns <= MAX_MOL_SITES) {
+            shake_mol<0>(a, m, s, e, ns, fnh, apply_vom, vomx, vomy, vomz, part, rebuild, bad, shake_fail,
+                         shake_geom, cx, cy, cz, px, py, pz, M);
         } else {
             for (int k = s; k < e; k++) {
                 const int at = a.mol_atoms[k];
