@@ -459,6 +459,134 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_pair(PairArgs a) {
     }
 }
 
+// x^k for a small positive integer k: a fixed product chain when K is a
+// compile-time constant, binary powering otherwise
+template <int K>
+__device__ __forceinline__ double ipow_d(double x, int k) {
+    if (K == 7) {
+        const double x2 = x * x, x4 = x2 * x2;
+        return x4 * x2 * x;
+    }
+    if (K == 6) {
+        const double x2 = x * x;
+        return x2 * x2 * x2;
+    }
+    double r = 1.0;
+    for (int q = 0; q < 7 && k > 0; q++) {
+        if (k & 1) r *= x;
+        k >>= 1;
+        if (k) x *= x;
+    }
+    return r;
+}
+
+// Mixed path, buffered 14-7 with small integer exponents (NM = n - m and M,
+// 0 = taken at run time): r^2 exact from the box fractions, the pair
+// arithmetic in FP64 with the powers as products and the taper in its
+// well-conditioned form S = (1-t)^3 (1 + 3t + 6t^2).  Every pair quantity
+// carries FP64 rounding only, at a lower cost on B200 than the FP32 path's
+// error-tracking arithmetic (buff_pair_f).  Same list walk, accumulation
+// and outputs as k_pair.
+template <int TPP, int NM, int M>
+__global__ void __launch_bounds__(PAIR_BLOCK) k_buff_d(PairArgs a) {
+    __shared__ double s_is[MAX_TYPES * MAX_TYPES], s_ep[MAX_TYPES * MAX_TYPES];
+    __shared__ double s_red[PAIR_BLOCK / 32][11];
+    const int nt2 = a.ntypes * a.ntypes;
+    for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
+        s_is[k] = 1.0 / a.par[k * 4 + 0];
+        s_ep[k] = a.par[k * 4 + 1];
+    }
+    __syncthreads();
+    const int nm = NM ? NM : (int)(a.bn - a.bm), mm = M ? M : (int)a.bm;
+    const double c1 = 1.0 + a.bdelta, c2 = 1.0 + a.bgamma;
+    const double rs = sqrt(a.bsw2), winv = 1.0 / (sqrt(a.vdw_rc2) - rs);
+    const double ds0 = (double)a.box.L[0] / 4294967296.0, ds1 = (double)a.box.L[1] / 4294967296.0,
+                 ds2 = (double)a.box.L[2] / 4294967296.0;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gt / TPP;
+    const int t = gt % TPP;
+    double fx = 0, fy = 0, fz = 0, evdw = 0;
+    double vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
+    int npair = 0;
+    if (i < a.n) {
+        const int cnt = a.nnbr[i];
+        const int4 pif = a.fixq[i];
+        const int ti = pif.w;
+        for (int k = t; k < cnt; k += TPP) {
+            const int raw = a.nbr[(size_t)k * a.n + i];
+            const int j = raw & 0x7fffffff;
+            const int4 pj = a.fixq[j];
+            const int ix = pj.x - pif.x, iy = pj.y - pif.y, iz = pj.z - pif.z;   // r_j - r_i
+            const unsigned long long s2 = (unsigned long long)((long long)ix * ix) +
+                                          (unsigned long long)((long long)iy * iy) +
+                                          (unsigned long long)((long long)iz * iz);
+            const double r2 = (double)s2 * a.r2scale;
+            if (!(r2 <= a.vdw_rc2)) continue;
+            npair++;
+            const double ep = s_ep[ti * a.ntypes + pj.w];
+            if (raw < 0 || ep == 0.0) continue;   // same molecule, or no well
+            const double is = s_is[ti * a.ntypes + pj.w];
+            const double r = sqrt(r2), ir = 1.0 / r;
+            const double rho = r * is;
+            const double t1 = 1.0 / (rho + a.bdelta);
+            const double p1n = ipow_d<NM>(c1 * t1, nm);
+            const double rm1 = ipow_d<(M > 1 ? M - 1 : 0)>(rho, mm - 1);
+            const double t2 = 1.0 / (rm1 * rho + a.bgamma);
+            const double p2 = c2 * t2;
+            double en = ep * p1n * (p2 - 2.0);
+            double tmpf = -(en * nm * is * t1 + ep * p1n * p2 * mm * rm1 * is * t2);
+            if (a.switch_on && r2 > a.bsw2) {
+                const double tt = fmin(1.0, fmax(0.0, (r - rs) * winv));
+                const double o = 1.0 - tt;
+                const double sv = o * o * o * (1.0 + tt * (3.0 + 6.0 * tt));
+                const double dsv = -30.0 * tt * tt * o * o * winv;
+                tmpf = tmpf * sv + en * dsv;
+                en *= sv;
+            }
+            const double fs = -tmpf * ir;
+            const double dx = ix * ds0, dy = iy * ds1, dz = iz * ds2;
+            const double fijx = -fs * dx, fijy = -fs * dy, fijz = -fs * dz;
+            fx += fijx; fy += fijy; fz += fijz;
+            evdw += en;
+            vxx += fijx * dx; vxy += fijy * dx; vxz += fijz * dx;
+            vyy += fijy * dy; vyz += fijz * dy; vzz += fijz * dz;
+        }
+    }
+    fx = group_sum<TPP>(fx);
+    fy = group_sum<TPP>(fy);
+    fz = group_sum<TPP>(fz);
+    if (i < a.n && t == 0) {
+        a.frc[i] = to_fix(fx, FRC_SCALE);
+        a.frc[a.n + i] = to_fix(fy, FRC_SCALE);
+        a.frc[2 * a.n + i] = to_fix(fz, FRC_SCALE);
+    }
+    double v[8] = {evdw, 0.0, vxx, vxy, vxz, vyy, vyz, vzz};
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    {
+        int np = warp_sum(npair);
+        if (lane == 0 && np) atomicAdd((unsigned long long *)&a.acc[ACC_NPAIR], (unsigned long long)np);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        double sv = warp_sum(v[q]);
+        if (lane == 0) s_red[w][q] = sv;
+    }
+    __syncthreads();
+    if (threadIdx.x < 8 && threadIdx.x != 1) {
+        double sv = 0;
+        for (int q = 0; q < PAIR_BLOCK / 32; q++) sv += s_red[q][threadIdx.x];
+        sv *= 0.5;  // each pair appears twice in the full list
+        const int slots[8] = {ACC_E_VDW, 0, ACC_VIR + 0, ACC_VIR + 1, ACC_VIR + 2, ACC_VIR + 4, ACC_VIR + 5, ACC_VIR + 8};
+        if (threadIdx.x >= 2) sv = -sv;   // Ensemble::virial sign
+        const long long fxv = to_fix(sv, ACC_SCALE);
+        if (sv != 0.0) atomicAdd((unsigned long long *)&a.acc[slots[threadIdx.x]], (unsigned long long)fxv);
+        // the virial of central pair forces is symmetric
+        if (threadIdx.x == 3) atomicAdd((unsigned long long *)&a.acc[ACC_VIR + 3], (unsigned long long)fxv);
+        if (threadIdx.x == 4) atomicAdd((unsigned long long *)&a.acc[ACC_VIR + 6], (unsigned long long)fxv);
+        if (threadIdx.x == 6) atomicAdd((unsigned long long *)&a.acc[ACC_VIR + 7], (unsigned long long)fxv);
+    }
+}
+
 template <typename R, int VDW, bool EWALD>
 static void dispatch_tpp(Ctx &c, const PairArgs &a) {
     int tpp = c.tpp;
@@ -581,7 +709,14 @@ void launch_pair(Ctx &c) {
         a.fixq = c.vfixq;
         a.frc = c.fv;
     }
-    if (c.precision == SMD_PREC_MIXED) {
+    if (c.precision == SMD_PREC_MIXED && buff && a.buff_int && a.cubic && !c.ewald_on && !a.le) {
+        if (!c.fixq_from_integrate) launch_fixq(c);
+        const int nb = (int)(((long long)c.n * 8 + PAIR_BLOCK - 1) / PAIR_BLOCK);
+        if (c.buff_n - c.buff_m == 7 && c.buff_m == 7)
+            k_buff_d<8, 7, 7><<<nb, PAIR_BLOCK, 0, c.stream>>>(a);
+        else
+            k_buff_d<8, 0, 0><<<nb, PAIR_BLOCK, 0, c.stream>>>(a);
+    } else if (c.precision == SMD_PREC_MIXED) {
         if (!c.fixq_from_integrate) launch_fixq(c);
         if (c.ewald_on) dispatch_vdw<float, true>(c, a);
         else dispatch_vdw<float, false>(c, a);
