@@ -373,7 +373,7 @@ __device__ __forceinline__ float4 ldcg4(const float4 *p) { return __ldcg(p); }
 // (tried through L1, relying on the barrier's acquire: slower).
 template <typename G4, typename GR>
 __device__ V3 amul(const CGArgs &c, int i, int t, const G4 *g) {
-    constexpr int CG_UNROLL = sizeof(GR) == 4 ? 4 : 2;
+    constexpr int CG_UNROLL = sizeof(GR) == 4 ? 6 : 2;
     const TRows &R = c.rows;
     const int cnt = R.cnt[i];
     const int *rj = R.j + (size_t)i * R.cap;
