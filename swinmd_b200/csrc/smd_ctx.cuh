@@ -174,6 +174,8 @@ void launch_intra(Ctx &c);
 void launch_mp_short(Ctx &c);
 void launch_mp_long(Ctx &c);
 void launch_ind_solve(Ctx &c);
+void launch_ind_field(Ctx &c);
+void launch_ind_cg(Ctx &c);
 void launch_ind_short(Ctx &c);
 void launch_mp_mol(Ctx &c);
 bool polar_short_fused(const Ctx &c);

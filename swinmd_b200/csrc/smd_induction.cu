@@ -930,8 +930,8 @@ __global__ void __launch_bounds__(64) k_polar_real_f(IndRealArgs A) {
     f.x = group_sum<TPP>(f.x); f.y = group_sum<TPP>(f.y); f.z = group_sum<TPP>(f.z);
     tau.x = group_sum<TPP>(tau.x); tau.y = group_sum<TPP>(tau.y); tau.z = group_sum<TPP>(tau.z);
     if (i < a.n && t == 0) {
-        add_fix3(A.frc, a.n, i, f, COU);
-        add_fix3(A.trq, a.n, i, tau, COU);
+        add_fix3_at(A.frc, a.n, i, f, COU);
+        add_fix3_at(A.trq, a.n, i, tau, COU);
     }
     __shared__ double s_r[2][11];
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
@@ -961,7 +961,7 @@ __global__ void k_ind_mol(IndArgs a, long long *trq, long long *acc) {
             const double4 pi = a.pos4[i];
             const V3 mi = ld3i(a.mu, a.n, i), pii = ld3i(a.p, a.n, i);
             eself += -dot(mi, pii) * a2pi * a2 / 3 * COU;
-            add_fix3(trq, a.n, i, crs(mi, pii), COU * (2.0 / 3.0) * a2pi * a2);
+            add_fix3_at(trq, a.n, i, crs(mi, pii), COU * (2.0 / 3.0) * a2pi * a2);
             const double qi = a.tq[(int)pi.w] / SQC;
             const Q6 Qi = ldqi(a.qd, a.n, i);
             for (int q = p + 1; q < e; q++) {
@@ -1058,7 +1058,8 @@ int ensure_ind_rows(Ctx &c) {
     return 0;
 }
 
-void launch_ind_solve(Ctx &c) {
+// permanent field and tensor rows, then the learned start dipoles
+void launch_ind_field(Ctx &c) {
     IndArgs a = ind_args(c);
     const bool f32 = c.precision == SMD_PREC_MIXED;
     TRows R;
@@ -1077,6 +1078,16 @@ void launch_ind_solve(Ctx &c) {
         k_ind_field<double><<<nb, 256, 0, c.stream>>>(a, R, c.status);
     const bool learned = c.cg_guess == SMD_GUESS_LEARNED && c.mlp_ready;
     if (learned) launch_mlp_guess(c);  // writes the start dipoles into p
+}
+
+// the PCG solve from the start dipoles, then the site records' new dipoles
+// and the step's dipole history
+void launch_ind_cg(Ctx &c) {
+    IndArgs a = ind_args(c);
+    const bool f32 = c.precision == SMD_PREC_MIXED;
+    TRows R;
+    R.j = c.ind_rj; R.c = c.ind_rc; R.cnt = c.ind_cnt; R.lcnt = c.ind_cnt + c.n; R.cap = c.ind_cap;
+    const bool learned = c.cg_guess == SMD_GUESS_LEARNED && c.mlp_ready;
     CGArgs g;
     g.ia = a;
     g.rows = R;
@@ -1110,6 +1121,11 @@ void launch_ind_solve(Ctx &c) {
         k_hist_push<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.pind, c.e0, c.phist, c.flags);
         k_hist_advance<<<1, 1, 0, c.stream>>>(c.flags);
     }
+}
+
+void launch_ind_solve(Ctx &c) {
+    launch_ind_field(c);
+    launch_ind_cg(c);
 }
 
 void launch_ind_short(Ctx &c) {

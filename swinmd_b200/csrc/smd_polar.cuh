@@ -73,6 +73,13 @@ __device__ __forceinline__ void add_fix3(long long *arr, int n, int i, V3 v, dou
     arr[n + i] += to_fix(s * v.y, FRC_SCALE);
     arr[2 * n + i] += to_fix(s * v.z, FRC_SCALE);
 }
+// the same through integer atomics, for sites that several threads or
+// kernels add to: the sum does not depend on the order
+__device__ __forceinline__ void add_fix3_at(long long *arr, int n, int i, V3 v, double s) {
+    atomicAdd((unsigned long long *)&arr[i], (unsigned long long)to_fix(s * v.x, FRC_SCALE));
+    atomicAdd((unsigned long long *)&arr[n + i], (unsigned long long)to_fix(s * v.y, FRC_SCALE));
+    atomicAdd((unsigned long long *)&arr[2 * n + i], (unsigned long long)to_fix(s * v.z, FRC_SCALE));
+}
 
 constexpr double SQRT_PI_POLAR = 1.7724538509055160273;
 

@@ -144,6 +144,33 @@ def test_mixed_full_evaluation():
     e.close()
 
 
+def _mixed_run(steps):
+    e = engine.GpuEnsemble(_pw(), precision="mixed")
+    e.set_solver(tol=1e-10, max_iter=1000)
+    lf = engine.LFIntegrator(e, series_capacity=16)
+    lf.start()
+    lf.run(steps)
+    ser, st = lf.series(), e.state()
+    e.close()
+    return ser, st
+
+
+def test_mixed_step():
+    # the mixed step (FP64 buffered 14-7, fused real space after the solve,
+    # column reciprocal passes): integer atomics make every sum independent
+    # of thread order, so two runs are bitwise equal, and the energies follow
+    # the reference's trajectory
+    g = golden("polwater216")
+    ser1, st1 = _mixed_run(10)
+    ser2, st2 = _mixed_run(10)
+    assert np.array_equal(st1["pos"], st2["pos"])
+    assert np.array_equal(st1["vel"], st2["vel"])
+    assert np.array_equal(ser1, ser2)
+    print(ser1[:, 0], g["r_step_epot"])
+    assert np.allclose(ser1[:, 0], g["r_step_epot"], rtol=2e-6)
+    assert np.allclose(ser1[:, 2], g["r_step_atomtemp"], rtol=2e-6)
+
+
 def test_polar_trajectory():
     g = golden("polwater216")
     e = engine.GpuEnsemble(_pw())
