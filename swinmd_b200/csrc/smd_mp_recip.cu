@@ -502,10 +502,10 @@ __global__ void __launch_bounds__(256) k_rforce_f(int n, int nk, const double4 *
 //   torque  mu x M1 - 2 g,  g_a = eps_abc (Q M2)_cb.
 constexpr int TAB_MAX = 32;     // |n| < TAB_MAX
 constexpr int TS_THREADS = 128; // runs per block, sums pass
-constexpr int TS_SITES = 64;    // sites per tile, sums pass
+constexpr int TS_SITES = 128;   // sites per tile, sums pass
 constexpr int TS_SEG = 4;       // k per run, sums pass
-constexpr int CF_THREADS = 128; // sites per block, force pass
-constexpr int CF_KGROUP = 256;  // k per column group at most, force pass
+constexpr int CF_THREADS = 256; // sites per block, force pass
+constexpr int CF_KGROUP = 128;  // k per column group at most, force pass
 constexpr int CF_CGROUP = 64;   // columns per group at most
 
 __device__ __forceinline__ float2 table_entry(int m, unsigned f) {
