@@ -177,6 +177,16 @@ int smd_set_multipole(smd_ctx *ctx, const double *type_mp, const double *polar, 
                       double kcut, double real_cut, int induction, double ind_cut, double thole_a);
 /* Dipole solver: RMS change tolerance (e nm), iteration cap, initial guess. */
 int smd_set_solver(smd_ctx *ctx, double tol, int max_iter, int guess);
+/* Preconditioner of the dipole solve.  No counterpart in the reference, which
+ * runs unpreconditioned CG on its dense matrix (src/forces/Induction.cpp:
+ * 2401-2467); the converged dipoles are the same, the iteration count is not.
+ * SMD_PRECOND_SITE: diag(alpha_i).  SMD_PRECOND_MOLECULE (default): the
+ * inverse of each molecule's own block of A (its sites' 1/alpha and their
+ * Thole-damped mutual couplings), which also starts the solve from that
+ * block solution under SMD_GUESS_DIRECT. */
+#define SMD_PRECOND_SITE 0
+#define SMD_PRECOND_MOLECULE 1
+int smd_set_preconditioner(smd_ctx *ctx, int kind);
 /* Solver statistics of the last solve: iterations and final RMS change. */
 int smd_solver_stats(smd_ctx *ctx, int *iterations, double *rms_change);
 /* Lab-frame dipoles, quadrupoles, permanent field and induced dipoles of the

@@ -22,6 +22,7 @@ E_VDW, E_REAL, E_LONG, E_CORRECT, E_MOLCORRECT, E_SURF = 0, 1, 2, 3, 4, 5
 E_POL_REAL, E_POL_LONG, E_POL_SELF, E_POL_INTRA, E_COUNT = 6, 7, 8, 9, 12
 VDW_NONE, VDW_LJ, VDW_MIE, VDW_BMH, VDW_BUFF = 0, 1, 2, 3, 4
 GUESS_DIRECT, GUESS_PREVIOUS, GUESS_LEARNED = 0, 1, 2
+PRECOND_SITE, PRECOND_MOLECULE = 0, 1
 THERMO_NONE, THERMO_NOSE_HOOVER, THERMO_NH_CHAIN = 0, 1, 2
 
 
@@ -100,6 +101,7 @@ SIGNATURES = {
                                          ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_double]),
     "smd_set_solver": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
+    "smd_set_preconditioner": (ctypes.c_int, [_P, ctypes.c_int]),
     "smd_solver_stats": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), _D]),
     "smd_get_polarization": (ctypes.c_int, [_P, _D, _D, _D, _D]),
     "smd_set_induced": (ctypes.c_int, [_P, _D]),

@@ -234,7 +234,7 @@ void smd_destroy(smd_ctx *x) {
                     c.pl.cell_count, c.pl.cell_start, c.pl.cell_atoms, c.rc.kn, c.rc.kcoef,
                     c.rc.sk, c.rc.kvec, c.clen2, c.type_mp, c.type_polar, c.mu, c.qd, c.trq, c.e0,
                     c.pind, c.cgw, c.cgs, c.cg_bar, c.vpos4, c.vfixq, c.fv, c.ind_rj, c.ind_rc, c.ind_cnt,
-                    c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab, c.srec, c.phist};
+                    c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab, c.srec, c.phist, c.cg_blk};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -500,6 +500,7 @@ int smd_set_multipole(smd_ctx *x, const double *type_mp, const double *polar, do
     CK(dalloc(&c.mu, 3 * n)); CK(dalloc(&c.qd, 6 * n)); CK(dalloc(&c.trq, 3 * n));
     CK(dalloc(&c.e0, 3 * n)); CK(dalloc(&c.pind, 3 * n)); CK(dalloc(&c.cgw, 26 * n));
     CK(dalloc(&c.frame, 9 * n));
+    CK(dalloc(&c.cg_blk, 81 * (size_t)c.nmol));
     CK(cudaMemset(c.pind, 0, 3 * n * sizeof(double)));
     CK(dalloc(&c.srec, 4 * n));
     CK(cudaMemset(c.srec, 0, 4 * n * sizeof(float4)));
@@ -526,6 +527,14 @@ int smd_set_solver(smd_ctx *x, double tol, int max_iter, int guess) {
     x->c.cg_tol = tol;
     x->c.cg_max_iter = max_iter;
     x->c.cg_guess = guess;
+    x->c.graph_dirty = 1;
+    return SMD_OK;
+}
+
+int smd_set_preconditioner(smd_ctx *x, int kind) {
+    if (!x || (kind != SMD_PRECOND_SITE && kind != SMD_PRECOND_MOLECULE))
+        return fail(x, SMD_ERR_ARG, "smd_set_preconditioner: kind must be SMD_PRECOND_SITE or SMD_PRECOND_MOLECULE");
+    x->c.cg_precond = kind;
     x->c.graph_dirty = 1;
     return SMD_OK;
 }

@@ -110,6 +110,8 @@ struct Ctx {
     double cg_tol = 2.0819e-8;      // RMS dipole change tolerance (e nm); 1e-6 D
     int cg_guess = 0;               // 0: alpha E0, 1: previous step, 2: learned (MLP)
     int cg_blocks = 0;
+    int cg_precond = SMD_PRECOND_MOLECULE;  // dipole-solve preconditioner
+    double *cg_blk = nullptr;       // [nmol][81] inverse molecule blocks of A
     unsigned int *cg_bar = nullptr; // grid-barrier counter
     int *ind_rj = nullptr;          // damped-tensor rows of the solve: partners [N][cap]
     void *ind_rc = nullptr;         // coefficients [N][cap] (float4 or double4)

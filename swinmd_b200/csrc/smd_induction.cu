@@ -319,6 +319,7 @@ struct CGArgs {
     unsigned *bar, *status;
     int nblocks, max_iter, guess;
     double tol;
+    const double *blk;       // [nmol][81] inverse molecule blocks of A (molecule preconditioner)
 };
 
 // fixed-order block sums, every block computes the same totals: each thread
@@ -409,8 +410,121 @@ __device__ V3 amul(const CGArgs &c, int i, int t, const G4 *g) {
     return acc;
 }
 
-// Jacobi-preconditioned CG (M^-1 = diag(a_i)) as one persistent cooperative
-// kernel in the single-reduction form of Chronopoulos and Gear (1989): with
+// Molecule-block preconditioner: for every molecule (at most 3 sites) the
+// block of A = diag(1/a_i) - T over its own sites, with T_ij from the
+// excluded-site entries of the tensor rows (T v = (r'.v) r' - c3 v), is
+// inverted in FP64.  It captures the strong Thole-damped coupling inside a
+// water molecule that the diagonal preconditioner leaves out.  81 threads
+// per molecule (entry (r, c) of its 9 x 9 block; unused sites padded with
+// the identity), three molecules per block, and an in-place Gauss-Jordan
+// sweep over the nine pivots (no pivoting: the block is positive definite).
+// A block with a non-positive pivot falls back to diag(a_i).  The inverses
+// are stored entry-major over molecules (entry e of molecule m at
+// e * nmol + m), so that the solve's loads of one entry coalesce.
+constexpr int MB_MOLS = 3;
+template <typename TS>
+__global__ void __launch_bounds__(81 * MB_MOLS) k_mol_blocks(int nmol, const int *mol_off, const int *mol_atoms,
+                                                             TRows R, const double *polar, const double4 *pos4,
+                                                             double *blk) {
+    using TS4 = typename std::conditional<sizeof(TS) == 4, float4, double4>::type;
+    __shared__ double s_a[MB_MOLS][81];
+    __shared__ int s_bad[MB_MOLS];
+    const int lm = threadIdx.x / 81, e = threadIdx.x - 81 * lm, r = e / 9, cc = e - 9 * r;
+    const int m = blockIdx.x * MB_MOLS + lm;
+    const bool act = m < nmol;
+    int ns = 0;
+    double val = r == cc ? 1.0 : 0.0, al_r = 1.0;
+    if (act) {
+        const int s0 = mol_off[m];
+        ns = min(3, mol_off[m + 1] - s0);
+        const int q = r / 3, qq = cc / 3, x = r - 3 * q, y = cc - 3 * qq;
+        if (q < ns) al_r = fmax(1e-8, polar[(int)pos4[mol_atoms[s0 + q]].w]);
+        if (q < ns && qq < ns) {
+            if (q == qq) {
+                val = x == y ? 1.0 / al_r : 0.0;
+            } else {
+                const int i = mol_atoms[s0 + q], j = mol_atoms[s0 + qq];
+                const int c1 = min(R.cnt[i], R.cap);
+                val = 0.0;
+                for (int k = R.lcnt[i]; k < c1; k++)
+                    if (R.j[(size_t)i * R.cap + k] == j) {
+                        const TS4 t = ((const TS4 *)R.c)[(size_t)i * R.cap + k];
+                        const double v[3] = {(double)t.x, (double)t.y, (double)t.z};
+                        val = -(v[x] * v[y] - (x == y ? (double)t.w : 0.0));
+                    }
+            }
+        }
+    }
+    s_a[lm][e] = val;
+    if (e == 0) s_bad[lm] = 0;
+    __syncthreads();
+    for (int k = 0; k < 9; k++) {
+        const double p = s_a[lm][k * 9 + k], rk = s_a[lm][r * 9 + k], kc = s_a[lm][k * 9 + cc];
+        const double own = s_a[lm][e];
+        __syncthreads();
+        if (!(p > 0.0)) {
+            if (e == 0) s_bad[lm] = 1;
+        } else {
+            double v;
+            if (r == k && cc == k) v = 1.0 / p;
+            else if (r == k) v = kc / p;
+            else if (cc == k) v = -rk / p;
+            else v = own - rk * kc / p;
+            s_a[lm][e] = v;
+        }
+        __syncthreads();
+    }
+    if (act) {
+        const int nd = 3 * ns;
+        double out = s_a[lm][e];
+        if (s_bad[lm]) out = (r == cc && r < nd) ? al_r : 0.0;
+        if (r >= nd || cc >= nd) out = 0.0;
+        blk[(size_t)e * nmol + m] = out;
+    }
+}
+
+// u = B_m^-1 v for every molecule, nine threads per molecule (thread e of a
+// molecule owns component e = 3 q + d, site q, axis d) in tiles of
+// CG_THREADS / 9 molecules per block; the components meet in shared memory.
+// in(m, e, i, idx) gives (and may update) component e of v, out(...) takes
+// u's component; the packed copy pk of u (one G4 per site) is written here.
+// Block-uniform loop: every thread of the block reaches each barrier.
+template <typename G4, typename GR, class FIn, class FOut>
+__device__ __forceinline__ void mol_tiles(const IndArgs &a, const double *blk, G4 *pk, double *s_v, double *s_u,
+                                          FIn &&in, FOut &&out) {
+    constexpr int TM = CG_THREADS / 9;
+    const int n = a.n, nmol = a.nmol;
+    const int ml = threadIdx.x / 9, e = threadIdx.x - 9 * ml, q = e / 3, d = e - 3 * q;
+    for (int m0 = blockIdx.x * TM; m0 < nmol; m0 += gridDim.x * TM) {
+        const int m = m0 + ml;
+        int ns = 0, i = -1;
+        if (ml < TM && m < nmol) {
+            const int s0 = a.mol_off[m];
+            ns = min(3, a.mol_off[m + 1] - s0);
+            if (q < ns) i = a.mol_atoms[s0 + q];
+        }
+        double v = 0.0;
+        if (i >= 0) v = in(m, e, i, d * n + i);
+        if (ml < TM) s_v[threadIdx.x] = v;
+        __syncthreads();
+        double u = 0.0;
+        if (i >= 0) {
+            for (int col = 0; col < 3 * ns; col++) u += __ldcg(&blk[(size_t)(e * 9 + col) * nmol + m]) * s_v[9 * ml + col];
+            out(m, e, i, d * n + i, v, u);
+        }
+        if (ml < TM) s_u[threadIdx.x] = u;
+        __syncthreads();
+        if (i >= 0 && d == 0)
+            pk[i] = G4{(GR)s_u[threadIdx.x], (GR)s_u[threadIdx.x + 1], (GR)s_u[threadIdx.x + 2], (GR)0};
+        __syncthreads();
+    }
+}
+
+// Preconditioned CG as one persistent cooperative kernel, M^-1 = diag(a_i)
+// (BJ false) or the inverse molecule blocks of k_mol_blocks (BJ true: the
+// start x0 = M^-1 E0 and u = M^-1 r are formed per molecule, which costs one
+// more grid barrier before the first product), in the single-reduction form
+// of Chronopoulos and Gear (1989): with
 // u = M^-1 r and w = A u kept alongside, the direction p = u + beta p and
 // s = A p = w + beta s follow by recurrence, and both inner products of an
 // iteration, gamma = r.u and delta = w.u, come from one pass each side of
@@ -425,11 +539,12 @@ __device__ V3 amul(const CGArgs &c, int i, int t, const G4 *g) {
 // partial sums of U and W alternate between two buffers each by iteration
 // parity, so no barrier is needed to guard their reuse.  Vectors written in
 // one phase and read by other blocks in the next are read past L1.
-template <bool F32>
+template <bool F32, bool BJ>
 __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
     using G4 = typename std::conditional<F32, float4, double4>::type;
     using GR = typename std::conditional<F32, float, double>::type;
     __shared__ double s_w[CG_THREADS / 32][4];
+    __shared__ double s_bv[BJ ? CG_THREADS : 1], s_bu[BJ ? CG_THREADS : 1];
     const IndArgs &a = c.ia;
     const int n = a.n;
     G4 *g0 = (G4 *)c.g0, *g1 = (G4 *)c.g1;
@@ -444,16 +559,27 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
     const int passes = (n + sites_per_pass - 1) / sites_per_pass;
     unsigned int phase = 0;
     double tot[4];
-    // x0: alpha E0 (guess 0) or the dipoles already in p (previous step / learned)
-    for (int i = gtid; i < n; i += nthreads) {
-        const double al = fmax(1e-8, a.polar[(int)a.pos4[i].w]);
-        c.al[i] = al;
-        double p3[3];
-        for (int d = 0; d < 3; d++) {
-            p3[d] = c.guess == 0 ? al * a.e0[d * n + i] : a.p[d * n + i];
-            if (c.guess == 0) a.p[d * n + i] = p3[d];
+    // x0: M^-1 E0 (guess 0) or the dipoles already in p (previous step / learned)
+    if (BJ) {
+        for (int i = gtid; i < n; i += nthreads) c.al[i] = fmax(1e-8, a.polar[(int)a.pos4[i].w]);
+        if (c.guess == 0) {
+            mol_tiles<G4, GR>(a, c.blk, g0, s_bv, s_bu, [&](int, int, int, int idx) { return a.e0[idx]; },
+                              [&](int, int, int, int idx, double, double u) { a.p[idx] = u; });
+        } else {
+            for (int i = gtid; i < n; i += nthreads)
+                g0[i] = G4{(GR)a.p[i], (GR)a.p[n + i], (GR)a.p[2 * n + i], (GR)0};
         }
-        g0[i] = G4{(GR)p3[0], (GR)p3[1], (GR)p3[2], (GR)0};
+    } else {
+        for (int i = gtid; i < n; i += nthreads) {
+            const double al = fmax(1e-8, a.polar[(int)a.pos4[i].w]);
+            c.al[i] = al;
+            double p3[3];
+            for (int d = 0; d < 3; d++) {
+                p3[d] = c.guess == 0 ? al * a.e0[d * n + i] : a.p[d * n + i];
+                if (c.guess == 0) a.p[d * n + i] = p3[d];
+            }
+            g0[i] = G4{(GR)p3[0], (GR)p3[1], (GR)p3[2], (GR)0};
+        }
     }
     if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
     // r = E0 - A x ; u = M^-1 r ; gamma = r.u
@@ -465,13 +591,24 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
         if (i < n && t == 0) {
             const double al = __ldcg(&c.al[i]);
             const double rr[3] = {a.e0[i] - Ap.x, a.e0[n + i] - Ap.y, a.e0[2 * n + i] - Ap.z};
-            for (int d = 0; d < 3; d++) {
-                c.r[d * n + i] = rr[d];
-                c.u[d * n + i] = al * rr[d];
-                vals[0] += rr[d] * al * rr[d];
+            for (int d = 0; d < 3; d++) c.r[d * n + i] = rr[d];
+            if (!BJ) {
+                for (int d = 0; d < 3; d++) {
+                    c.u[d * n + i] = al * rr[d];
+                    vals[0] += rr[d] * al * rr[d];
+                }
+                g1[i] = G4{(GR)(al * rr[0]), (GR)(al * rr[1]), (GR)(al * rr[2]), (GR)0};
             }
-            g1[i] = G4{(GR)(al * rr[0]), (GR)(al * rr[1]), (GR)(al * rr[2]), (GR)0};
         }
+    }
+    if (BJ) {
+        // u = B^-1 r per molecule, once every site's residual is in place
+        if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
+        mol_tiles<G4, GR>(a, c.blk, g1, s_bv, s_bu, [&](int, int, int, int idx) { return __ldcg(&c.r[idx]); },
+                          [&](int, int, int, int idx, double r, double u) {
+                              c.u[idx] = u;
+                              vals[0] += r * u;
+                          });
     }
     block_partials(vals, 1, pu1, s_w);
     if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
@@ -499,25 +636,45 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
         // U: p = u + beta p ; s = w + beta s ; x += alpha p ; r -= alpha s ;
         //    u = M^-1 r ; gamma' = r.u ; |alpha p|^2
         vals[0] = 0; vals[1] = 0;
-        for (int i = gtid; i < n; i += nthreads) {
-            const double al = __ldcg(&c.al[i]);
-            double w3[3];
-            for (int d = 0; d < 3; d++) {
-                const int idx = d * n + i;
-                const double pd = __ldcg(&c.u[idx]) + (it ? beta * __ldcg(&c.v[idx]) : 0.0);
-                const double sd = __ldcg(&c.z[idx]) + (it ? beta * __ldcg(&c.s[idx]) : 0.0);
-                c.v[idx] = pd;
-                c.s[idx] = sd;
-                const double dp = alpha_cg * pd;
-                a.p[idx] = __ldcg(&a.p[idx]) + dp;
-                const double r = __ldcg(&c.r[idx]) - alpha_cg * sd;
-                c.r[idx] = r;
-                w3[d] = al * r;
-                c.u[idx] = w3[d];
-                vals[0] += r * w3[d];
-                vals[1] += dp * dp;
+        if (BJ) {
+            mol_tiles<G4, GR>(a, c.blk, g1, s_bv, s_bu,
+                              [&](int, int, int, int idx) {
+                                  const double pd = __ldcg(&c.u[idx]) + (it ? beta * __ldcg(&c.v[idx]) : 0.0);
+                                  const double sd = __ldcg(&c.z[idx]) + (it ? beta * __ldcg(&c.s[idx]) : 0.0);
+                                  c.v[idx] = pd;
+                                  c.s[idx] = sd;
+                                  const double dp = alpha_cg * pd;
+                                  a.p[idx] = __ldcg(&a.p[idx]) + dp;
+                                  const double r = __ldcg(&c.r[idx]) - alpha_cg * sd;
+                                  c.r[idx] = r;
+                                  vals[1] += dp * dp;
+                                  return r;
+                              },
+                              [&](int, int, int, int idx, double r, double u) {
+                                  c.u[idx] = u;
+                                  vals[0] += r * u;
+                              });
+        } else {
+            for (int i = gtid; i < n; i += nthreads) {
+                const double al = __ldcg(&c.al[i]);
+                double w3[3];
+                for (int d = 0; d < 3; d++) {
+                    const int idx = d * n + i;
+                    const double pd = __ldcg(&c.u[idx]) + (it ? beta * __ldcg(&c.v[idx]) : 0.0);
+                    const double sd = __ldcg(&c.z[idx]) + (it ? beta * __ldcg(&c.s[idx]) : 0.0);
+                    c.v[idx] = pd;
+                    c.s[idx] = sd;
+                    const double dp = alpha_cg * pd;
+                    a.p[idx] = __ldcg(&a.p[idx]) + dp;
+                    const double r = __ldcg(&c.r[idx]) - alpha_cg * sd;
+                    c.r[idx] = r;
+                    w3[d] = al * r;
+                    c.u[idx] = w3[d];
+                    vals[0] += r * w3[d];
+                    vals[1] += dp * dp;
+                }
+                g1[i] = G4{(GR)w3[0], (GR)w3[1], (GR)w3[2], (GR)0};
             }
-            g1[i] = G4{(GR)w3[0], (GR)w3[1], (GR)w3[2], (GR)0};
         }
         double *const pu = (it & 1) ? pu1 : pu0;
         block_partials(vals, 2, pu, s_w);
@@ -847,7 +1004,7 @@ __global__ void __launch_bounds__(64) k_ind_real_f(IndRealArgs A) {
 // cutoff when cutoffInd is at least that cutoff, so that no lane idles on a
 // list entry beyond it.
 template <bool ROWS>
-__global__ void __launch_bounds__(64) k_polar_real_f(IndRealArgs A) {
+__global__ void __launch_bounds__(128) k_polar_real_f(IndRealArgs A) {
     const IndArgs &a = A.ia;
     constexpr int TPP = 8;
     const int gt = blockIdx.x * blockDim.x + threadIdx.x;
@@ -933,7 +1090,7 @@ __global__ void __launch_bounds__(64) k_polar_real_f(IndRealArgs A) {
         add_fix3_at(A.frc, a.n, i, f, COU);
         add_fix3_at(A.trq, a.n, i, tau, COU);
     }
-    __shared__ double s_r[2][11];
+    __shared__ double s_r[4][11];
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     double vals[11] = {0.5 * emp * COU, 0.5 * eind * COU, w[0], w[1], w[2], w[3], w[4], w[5], w[6], w[7], w[8]};
     for (int q = 0; q < 11; q++) {
@@ -1023,11 +1180,15 @@ static IndArgs ind_args(Ctx &c) {
 }
 
 int setup_cg(Ctx &c) {
-    int per_sm = 0, per_sm32 = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ind_cg<false>, CG_THREADS, 0) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, k_ind_cg<true>, CG_THREADS, 0) != cudaSuccess)
-        return SMD_ERR_CUDA;
-    per_sm = per_sm < per_sm32 ? per_sm : per_sm32;
+    // the grid must be co-resident for every variant of the solve kernel
+    const void *kernels[4] = {(const void *)k_ind_cg<false, false>, (const void *)k_ind_cg<true, false>,
+                              (const void *)k_ind_cg<false, true>, (const void *)k_ind_cg<true, true>};
+    int per_sm = 1 << 30;
+    for (const void *k : kernels) {
+        int v = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k, CG_THREADS, 0) != cudaSuccess) return SMD_ERR_CUDA;
+        per_sm = v < per_sm ? v : per_sm;
+    }
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, c.device) != cudaSuccess) return SMD_ERR_CUDA;
     int want = (c.n * CG_TPP + CG_THREADS - 1) / CG_THREADS;
@@ -1099,6 +1260,17 @@ void launch_ind_cg(Ctx &c) {
     g.nblocks = c.cg_blocks; g.max_iter = c.cg_max_iter; g.tol = c.cg_tol;
     // 0: start from alpha E0; 1: start from the dipoles in p (previous solve or network)
     g.guess = (c.cg_guess == SMD_GUESS_PREVIOUS || learned) ? 1 : 0;
+    const bool bj = c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk;
+    g.blk = c.cg_blk;
+    if (bj) {
+        const int nb = (c.nmol + MB_MOLS - 1) / MB_MOLS;
+        if (f32)
+            k_mol_blocks<float><<<nb, 81 * MB_MOLS, 0, c.stream>>>(c.nmol, c.mol_off, c.mol_atoms, R, c.type_polar,
+                                                                   c.pos4, c.cg_blk);
+        else
+            k_mol_blocks<double><<<nb, 81 * MB_MOLS, 0, c.stream>>>(c.nmol, c.mol_off, c.mol_atoms, R, c.type_polar,
+                                                                    c.pos4, c.cg_blk);
+    }
     cudaMemsetAsync(c.cg_bar, 0, sizeof(unsigned int), c.stream);
     // cooperative launch: the runtime refuses it unless every block can be
     // resident at once, which the grid barrier relies on
@@ -1111,10 +1283,14 @@ void launch_ind_cg(Ctx &c) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (f32)
-        cudaLaunchKernelEx(&cfg, k_ind_cg<true>, g);
+    if (f32 && bj)
+        cudaLaunchKernelEx(&cfg, k_ind_cg<true, true>, g);
+    else if (f32)
+        cudaLaunchKernelEx(&cfg, k_ind_cg<true, false>, g);
+    else if (bj)
+        cudaLaunchKernelEx(&cfg, k_ind_cg<false, true>, g);
     else
-        cudaLaunchKernelEx(&cfg, k_ind_cg<false>, g);
+        cudaLaunchKernelEx(&cfg, k_ind_cg<false, false>, g);
     launch_pack_sites(c);   // the mixed path's site records get the new dipoles
     // a time step stores its converged dipoles for the next steps' guess
     if (c.in_step && c.phist) {
@@ -1169,13 +1345,13 @@ void launch_polar_short(Ctx &c) {
     A.srec = c.srec;
     for (int d = 0; d < 3; d++) A.dscale[d] = c.box.L[d] / 4294967296.0;
     A.rj = c.ind_rj; A.rcnt = c.ind_cnt; A.rlcnt = c.ind_cnt + c.n; A.rcap = c.ind_cap;
-    const int nb = (int)(((long long)c.n * 8 + 63) / 64);
+    const int nb = (int)(((long long)c.n * 8 + 127) / 128);
     // the rows hold every pair inside the real-space cutoff when cutoffInd
     // reaches it; the pair test r^2 < rc^2 stays in the kernel
     if (c.ind_cut2 >= c.mp_rc2)
-        k_polar_real_f<true><<<nb, 64, 0, c.stream>>>(A);
+        k_polar_real_f<true><<<nb, 128, 0, c.stream>>>(A);
     else
-        k_polar_real_f<false><<<nb, 64, 0, c.stream>>>(A);
+        k_polar_real_f<false><<<nb, 128, 0, c.stream>>>(A);
     launch_mp_mol(c);
     k_ind_mol<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(A.ia, c.trq, c.acc);
 }

@@ -365,8 +365,13 @@ class GpuEnsemble:
         self._chk(self.lib.smd_ewald_nk(self.ctx, ctypes.byref(nk)))
         return nk.value
 
-    def set_solver(self, tol: float = 2.0819e-8, max_iter: int = 500, guess: int = L.GUESS_DIRECT):
+    def set_solver(self, tol: float = 2.0819e-8, max_iter: int = 500, guess: int = L.GUESS_DIRECT,
+                   precond: int = None):
+        """Dipole solve settings; precond (L.PRECOND_SITE / L.PRECOND_MOLECULE,
+        default molecule blocks) is left unchanged when None."""
         self._chk(self.lib.smd_set_solver(self.ctx, tol, max_iter, guess))
+        if precond is not None:
+            self._chk(self.lib.smd_set_preconditioner(self.ctx, precond))
 
     def solver_stats(self):
         it = ctypes.c_int()

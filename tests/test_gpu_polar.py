@@ -90,6 +90,30 @@ def test_induction(ens):
     assert err < 1e-8
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_preconditioners(precision):
+    # the diagonal and the molecule-block preconditioner converge to the same
+    # dipoles (the reference's, in FP64); the blocks take fewer iterations at
+    # both the tight and the working tolerance
+    g = golden("polwater216")
+    its = {}
+    for pc in (L.PRECOND_SITE, L.PRECOND_MOLECULE):
+        e = engine.GpuEnsemble(_pw(), precision=precision)
+        for tol in (1e-13, 2.0819e-8):
+            e.set_solver(tol=tol, max_iter=1000, precond=pc)
+            e.compute_forces(L.TERM_IND_SHORT)
+            its[pc, tol] = e.solver_stats()[0]
+            if tol == 1e-13:
+                p = e.polarization()["p"].reshape(-1)
+                err = rms_rel(p, g["f_ind_P"])
+                print(precision, pc, "p err", err)
+                assert err < (1e-9 if precision == "fp64" else 1e-6)
+        e.close()
+    print(its)
+    for tol in (1e-13, 2.0819e-8):
+        assert its[L.PRECOND_MOLECULE, tol] < its[L.PRECOND_SITE, tol]
+
+
 @pytest.mark.parametrize("term,fkey,ekey,eidx", [
     (L.TERM_VDW, "f_buff_force", "f_buff_energy", (L.E_VDW, 0)),
     (L.TERM_MP_SHORT, "f_mp_short_force", "f_mp_short_energy", (L.E_REAL, 1)),
