@@ -428,36 +428,44 @@ __global__ void __launch_bounds__(81 * MB_MOLS) k_mol_blocks(int nmol, const int
                                                              double *blk) {
     using TS4 = typename std::conditional<sizeof(TS) == 4, float4, double4>::type;
     __shared__ double s_a[MB_MOLS][81];
-    __shared__ int s_bad[MB_MOLS];
+    __shared__ double s_al[MB_MOLS][3];
+    __shared__ int s_bad[MB_MOLS], s_ns[MB_MOLS];
     const int lm = threadIdx.x / 81, e = threadIdx.x - 81 * lm, r = e / 9, cc = e - 9 * r;
     const int m = blockIdx.x * MB_MOLS + lm;
     const bool act = m < nmol;
-    int ns = 0;
-    double val = r == cc ? 1.0 : 0.0, al_r = 1.0;
-    if (act) {
-        const int s0 = mol_off[m];
-        ns = min(3, mol_off[m + 1] - s0);
-        const int q = r / 3, qq = cc / 3, x = r - 3 * q, y = cc - 3 * qq;
-        if (q < ns) al_r = fmax(1e-8, polar[(int)pos4[mol_atoms[s0 + q]].w]);
+    s_a[lm][e] = r == cc ? 1.0 : 0.0;   // identity padding for absent sites
+    __syncthreads();
+    // nine threads per molecule assemble the 3 x 3 site-pair blocks (q, qq)
+    if (act && e < 9) {
+        const int q = e / 3, qq = e - 3 * q;
+        const int s0 = mol_off[m], ns = min(3, mol_off[m + 1] - s0);
+        if (e == 0) { s_ns[lm] = ns; s_bad[lm] = 0; }
         if (q < ns && qq < ns) {
+            const int i = mol_atoms[s0 + q];
+            const double al = fmax(1e-8, polar[(int)pos4[i].w]);
+            double *blk3 = &s_a[lm][27 * q + 3 * qq];   // rows 3q.., columns 3qq..
             if (q == qq) {
-                val = x == y ? 1.0 / al_r : 0.0;
+                s_al[lm][q] = al;
+                for (int x = 0; x < 3; x++)
+                    for (int y = 0; y < 3; y++) blk3[9 * x + y] = x == y ? 1.0 / al : 0.0;
             } else {
-                const int i = mol_atoms[s0 + q], j = mol_atoms[s0 + qq];
+                const int j = mol_atoms[s0 + qq];
                 const int c1 = min(R.cnt[i], R.cap);
-                val = 0.0;
+                for (int x = 0; x < 3; x++)
+                    for (int y = 0; y < 3; y++) blk3[9 * x + y] = 0.0;
                 for (int k = R.lcnt[i]; k < c1; k++)
                     if (R.j[(size_t)i * R.cap + k] == j) {
                         const TS4 t = ((const TS4 *)R.c)[(size_t)i * R.cap + k];
                         const double v[3] = {(double)t.x, (double)t.y, (double)t.z};
-                        val = -(v[x] * v[y] - (x == y ? (double)t.w : 0.0));
+                        for (int x = 0; x < 3; x++)
+                            for (int y = 0; y < 3; y++) blk3[9 * x + y] = -(v[x] * v[y] - (x == y ? (double)t.w : 0.0));
                     }
             }
         }
     }
-    s_a[lm][e] = val;
-    if (e == 0) s_bad[lm] = 0;
     __syncthreads();
+    const int ns = act ? s_ns[lm] : 0;
+    const double al_r = act && r / 3 < ns ? s_al[lm][r / 3] : 1.0;
     for (int k = 0; k < 9; k++) {
         const double p = s_a[lm][k * 9 + k], rk = s_a[lm][r * 9 + k], kc = s_a[lm][k * 9 + cc];
         const double own = s_a[lm][e];

@@ -146,11 +146,7 @@ __device__ __forceinline__ double ref_r2(const double4 &a, const double4 &b, con
 
 // One warp per site i; candidates are tested 32 at a time and appended in
 // candidate order (ballot + popc), so the row order is deterministic.
-__global__ void k_build(BuildArgs a) {
-    if (!a.flags[0]) return;
-    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
-    if (i >= a.n) return;
+__device__ void build_site(const BuildArgs &a, int i, int lane) {
     const double4 pi = a.pos4[i];
     const int mi = a.mol[i];
     const int e0 = a.excl_off[i], e1 = a.excl_off[i + 1];
@@ -220,6 +216,116 @@ __global__ void k_build(BuildArgs a) {
     }
 }
 
+__global__ void k_build(BuildArgs a) {
+    if (!a.flags[0]) return;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= a.n) return;
+    build_site(a, i, threadIdx.x & 31);
+}
+
+// The same rows, with the candidates staged in shared memory: a block takes
+// BS_SITES sites that are consecutive in cell order (one warp each).  When
+// they all lie in one cell they share its 27-cell stencil: the stencil's
+// candidates, in build_site's order (cells dz, dy, dx; sites in cell order),
+// are staged BS_STAGE at a time with their positions, molecules and a
+// same-cell flag, and every warp tests them from shared memory.  Blocks
+// whose sites straddle a cell boundary take build_site.  Not for
+// Lees-Edwards (sheared) boxes.
+constexpr int BS_SITES = 16, BS_STAGE = 1024;
+__global__ void __launch_bounds__(BS_SITES * 32) k_build_staged(BuildArgs a) {
+    if (!a.flags[0]) return;
+    __shared__ double s_x[BS_STAGE], s_y[BS_STAGE], s_z[BS_STAGE];
+    __shared__ int s_j[BS_STAGE], s_m[BS_STAGE];
+    __shared__ int s_cell[BS_SITES], s_cs[27], s_off[28], s_nc[27];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int slot = blockIdx.x * BS_SITES + w;
+    const bool has = slot < a.n;
+    const int i = has ? a.cell_atoms[slot] : -1;
+    if (lane == 0) s_cell[w] = has ? a.cell_of[i] : -1;
+    __syncthreads();
+    const int c = s_cell[0];
+    bool same = true;
+    for (int q = 1; q < BS_SITES; q++)
+        if (s_cell[q] != c && s_cell[q] != -1) same = false;
+    if (!same) {   // block-uniform: no barrier follows on this branch
+        if (has) build_site(a, i, lane);
+        return;
+    }
+    // the stencil's cells in build_site's order, their ranges and offsets
+    if (threadIdx.x < 27) {
+        const int t = threadIdx.x, dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+        const int cx = c % a.g.n[0], cy = (c / a.g.n[0]) % a.g.n[1], cz = c / (a.g.n[0] * a.g.n[1]);
+        int z = cz + dz; z = z < 0 ? z + a.g.n[2] : (z >= a.g.n[2] ? z - a.g.n[2] : z);
+        int y = cy + dy; y = y < 0 ? y + a.g.n[1] : (y >= a.g.n[1] ? y - a.g.n[1] : y);
+        int x = (cx + dx) % a.g.n[0];
+        x = x < 0 ? x + a.g.n[0] : x;
+        const int nc = (z * a.g.n[1] + y) * a.g.n[0] + x;
+        s_nc[t] = nc;
+        s_cs[t] = a.cell_start[nc];
+        s_off[t + 1] = a.cell_start[nc + 1] - a.cell_start[nc];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_off[0] = 0;
+        for (int t = 0; t < 27; t++) s_off[t + 1] += s_off[t];
+    }
+    __syncthreads();
+    const int total = s_off[27];
+    double4 pi = make_double4(0, 0, 0, 0);
+    int mi = 0, e0 = 0, e1 = 0, count = 0;
+    if (has) {
+        pi = a.pos4[i];
+        mi = a.mol[i];
+        e0 = a.excl_off[i];
+        e1 = a.excl_off[i + 1];
+    }
+    for (int base = 0; base < total; base += BS_STAGE) {
+        const int cnt = min(BS_STAGE, total - base);
+        __syncthreads();
+        for (int f = threadIdx.x; f < cnt; f += BS_SITES * 32) {
+            const int g = base + f;
+            int t = 0;
+            while (s_off[t + 1] <= g) t++;
+            const int j = a.cell_atoms[s_cs[t] + g - s_off[t]];
+            const double4 pj = a.pos4[j];
+            s_x[f] = pj.x; s_y[f] = pj.y; s_z[f] = pj.z;
+            s_j[f] = j;
+            // same-cell pairs without minimum image, as build_site (flag in bit 31)
+            s_m[f] = a.mol[j] | (s_nc[t] == c ? (int)0x80000000 : 0);
+        }
+        __syncthreads();
+        if (!has) continue;
+        for (int k = 0; k < cnt; k += 32) {
+            const int kk = k + lane;
+            const bool valid = kk < cnt;
+            const int j = valid ? s_j[kk] : -1;
+            const int mj = valid ? s_m[kk] : 0;
+            bool take = valid && j != i;
+            if (take) {
+                const double4 pj = make_double4(s_x[kk], s_y[kk], s_z[kk], 0.0);
+                take = ref_r2(pi, pj, a.box, mj >= 0, false, 0.0) < a.rl2;
+            }
+            if (take)
+                for (int q = e0; q < e1; q++)
+                    if (a.excl[q] == j) { take = false; break; }
+            const unsigned m = __ballot_sync(0xffffffffu, take);
+            if (take) {
+                const int at = count + __popc(m & ((1u << lane) - 1));
+                if (at < a.max_nbr)
+                    a.nbr[(size_t)at * a.n + i] = j | ((mj & 0x7fffffff) == mi ? (int)0x80000000 : 0);
+            }
+            count += __popc(m);
+        }
+    }
+    if (has && lane == 0) {
+        if (count > a.max_nbr) {
+            atomicOr(a.status, ST_LIST_OVERFLOW);
+            count = a.max_nbr;
+        }
+        a.nnbr[i] = count;
+    }
+}
+
 __global__ void k_list_done(int *flags, double *scal_le) {
     if (flags[0]) {
         flags[1] += 1;
@@ -256,8 +362,12 @@ void launch_nlist(Ctx &c, bool force_rebuild) {
     a.cell_start = c.pl.cell_start; a.cell_atoms = c.pl.cell_atoms; a.g = c.grid; a.box = c.box;
     a.rl2 = c.pl.rl2; a.nbr = c.pl.nbr; a.nnbr = c.pl.nnbr; a.status = c.status; a.flags = c.flags;
     a.le = c.ip.strain_rate != 0.0 && c.integrator_ready ? c.scal + SC_LE : nullptr;
-    int nbw = (c.n * 32 + T - 1) / T;
-    k_build<<<nbw, T, 0, c.stream>>>(a);
+    if (c.grid.use_cells && !a.le) {
+        k_build_staged<<<(c.n + BS_SITES - 1) / BS_SITES, BS_SITES * 32, 0, c.stream>>>(a);
+    } else {
+        int nbw = (c.n * 32 + T - 1) / T;
+        k_build<<<nbw, T, 0, c.stream>>>(a);
+    }
     k_list_done<<<1, 1, 0, c.stream>>>(c.flags, a.le ? c.scal + SC_LE : nullptr);
 }
 
