@@ -524,7 +524,7 @@ def main():
                "config": dict(desc, l2="256 MB buffer written before every chunk of "
                               f"{args.chunk} steps", replicas=world, parallelism="replicas only"),
                "plain": {"value": plain_value, "ms_per_step": plain_ms, "solver_iterations": plain_it,
-                         "dtype": "f64", "guess": "alpha E0"},
+                         "dtype": "f64", "guess": "M^-1 E0 (molecule blocks)"},
                "fast": {"value": value, "ms_per_step": fast_ms, "solver_iterations": fast_it,
                         "guess": "learned" if polar else "n/a",
                         "force_rms_rel_err_vs_fp64": force_err},
