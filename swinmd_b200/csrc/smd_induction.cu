@@ -819,12 +819,11 @@ __device__ __forceinline__ void ind_algebra_f(float qi, F3 mi, const Q6F &Qi, F3
     A.Gt3 = (2.f * pjr) * crs(Qir, r);
 }
 
-// the radial part given the Ewald B_0..B_4 of the pair (bn_erfc)
-__device__ __forceinline__ void ind_pair_mixed_b(const IndAlgF &A, V3 r, double r2, const double *B, double poli,
-                                                 double polj, double a, double scale, IndPairOut &o) {
-    const double rr = sqrt(r2);
-    const double u3 = rr * rr * rr / sqrt(poli * polj);
-    const double ir2 = 1.0 / r2;
+// the radial part given the Ewald B_0..B_4 of the pair (bn_erfc), |r|,
+// 1/r^2 and ipp = 1/sqrt(a_i a_j)
+__device__ __forceinline__ void ind_pair_mixed_b(const IndAlgF &A, V3 r, double rr, double ir2, const double *B,
+                                                 double ipp, double a, double scale, IndPairOut &o) {
+    const double u3 = rr * rr * rr * ipp;
     const double e = exp(-a * u3), au3 = a * u3, a2u6 = au3 * au3, a3u9 = a2u6 * au3;
     const double l3 = 1.0 - e;
     const double gl3 = 3.0 * au3 * e * ir2;
@@ -851,7 +850,7 @@ __device__ __forceinline__ void ind_pair_mixed(const IndAlgF &A, V3 r, double r2
                                                double a, double alpha, double scale, IndPairOut &o) {
     double B[6];
     bn_erfc(r2, alpha, B);
-    ind_pair_mixed_b(A, r, r2, B, poli, polj, a, scale, o);
+    ind_pair_mixed_b(A, r, sqrt(r2), 1.0 / r2, B, 1.0 / sqrt(poli * polj), a, scale, o);
 }
 
 struct IndRealArgs {
@@ -862,6 +861,7 @@ struct IndRealArgs {
     double dscale[3];      // L / 2^32 per axis
     const int *rj, *rcnt, *rlcnt;   // the solve's tensor rows (partners within cutoffInd)
     int rcap;
+    int ntypes;
 };
 
 __global__ void __launch_bounds__(64) k_ind_real(IndRealArgs A) {
@@ -1014,6 +1014,10 @@ __global__ void __launch_bounds__(64) k_ind_real_f(IndRealArgs A) {
 template <bool ROWS>
 __global__ void __launch_bounds__(128) k_polar_real_f(IndRealArgs A) {
     const IndArgs &a = A.ia;
+    __shared__ double s_ipp[64];   // 1 / sqrt(a_i a_j) per type pair (at most 8 types)
+    for (int q = threadIdx.x; q < A.ntypes * A.ntypes; q += blockDim.x)
+        s_ipp[q] = 1.0 / sqrt(a.polar[q / A.ntypes] * a.polar[q % A.ntypes]);
+    __syncthreads();
     constexpr int TPP = 8;
     const int gt = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = gt / TPP, t = gt % TPP;
@@ -1021,7 +1025,6 @@ __global__ void __launch_bounds__(128) k_polar_real_f(IndRealArgs A) {
     double emp = 0, eind = 0, w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     if (i < a.n) {
         const int4 fi = A.fixq[i];
-        const double poli = a.polar[fi.w];
         const double qi_d = a.tq[fi.w] / SQC;
         const float4 *ri = A.srec + 4 * (size_t)i;
         const float4 i0 = ri[0], i1 = ri[1], i2 = ri[2], i3 = ri[3];
@@ -1047,8 +1050,8 @@ __global__ void __launch_bounds__(128) k_polar_real_f(IndRealArgs A) {
             const float4 j0 = __ldg(rj), j1 = __ldg(rj + 1), j2 = __ldg(rj + 2), j3 = __ldg(rj + 3);
             const F3 mj = f3(j0.y, j0.z, j0.w);
             const Q6F Qj = {j1.x, j1.y, j1.z, j1.w, j2.x, j2.y};
-            double B[6];
-            bn_erfc(r2, a.alpha, B);
+            double B[6], rr, ir2;
+            bn_erfc_r(r2, a.alpha, B, rr, ir2);
             V3 fij = v3(0, 0, 0), ti = v3(0, 0, 0);
             if (listed) {
                 MPPair<float, F3> P;
@@ -1066,14 +1069,14 @@ __global__ void __launch_bounds__(128) k_polar_real_f(IndRealArgs A) {
             IndAlgF al;
             ind_algebra_f(qi, mi, Qi, pii, j0.x, mj, Qj, f3(j2.z, j2.w, j3.x), rf, al);
             IndPairOut o;
-            ind_pair_mixed_b(al, r, r2, B, poli, a.polar[fj.w], a.a, listed ? 1.0 : 0.0, o);
+            ind_pair_mixed_b(al, r, rr, ir2, B, s_ipp[fi.w * A.ntypes + fj.w], a.a, listed ? 1.0 : 0.0, o);
             eind += o.e;
             fij = fij + o.fij;
             f = f + fij;
             tau = tau + ti + o.tau;
-            const double fr[3] = {fij.x, fij.y, fij.z}, rr[3] = {r.x, r.y, r.z};
+            const double fr[3] = {fij.x, fij.y, fij.z}, rv[3] = {r.x, r.y, r.z};
             for (int p = 0; p < 3; p++)
-                for (int q = 0; q < 3; q++) w[3 * p + q] -= 0.5 * fr[q] * rr[p];
+                for (int q = 0; q < 3; q++) w[3 * p + q] -= 0.5 * fr[q] * rv[p];
         };
         if (ROWS) {
             const int *rj = A.rj + (size_t)i * A.rcap;
@@ -1353,6 +1356,7 @@ void launch_polar_short(Ctx &c) {
     A.srec = c.srec;
     for (int d = 0; d < 3; d++) A.dscale[d] = c.box.L[d] / 4294967296.0;
     A.rj = c.ind_rj; A.rcnt = c.ind_cnt; A.rlcnt = c.ind_cnt + c.n; A.rcap = c.ind_cap;
+    A.ntypes = c.ntypes;
     const int nb = (int)(((long long)c.n * 8 + 127) / 128);
     // the rows hold every pair inside the real-space cutoff when cutoffInd
     // reaches it; the pair test r^2 < rc^2 stays in the kernel
