@@ -526,12 +526,13 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_buff_d(PairArgs a) {
             const double ep = s_ep[ti * a.ntypes + pj.w];
             if (raw < 0 || ep == 0.0) continue;   // same molecule, or no well
             const double is = s_is[ti * a.ntypes + pj.w];
-            const double r = sqrt(r2), ir = 1.0 / r;
+            const double ir = rsqrt(r2), r = r2 * ir;
             const double rho = r * is;
-            const double t1 = 1.0 / (rho + a.bdelta);
-            const double p1n = ipow_d<NM>(c1 * t1, nm);
             const double rm1 = ipow_d<(M > 1 ? M - 1 : 0)>(rho, mm - 1);
-            const double t2 = 1.0 / (rm1 * rho + a.bgamma);
+            // both quotients from one division
+            const double sd = rho + a.bdelta, dm = rm1 * rho + a.bgamma, inv = 1.0 / (sd * dm);
+            const double t1 = dm * inv, t2 = sd * inv;
+            const double p1n = ipow_d<NM>(c1 * t1, nm);
             const double p2 = c2 * t2;
             double en = ep * p1n * (p2 - 2.0);
             double tmpf = -(en * nm * is * t1 + ep * p1n * p2 * mm * rm1 * is * t2);
