@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(256) k_ind_field_f(IndArgs a, FieldMixArgs m, 
                 valid = true;
                 const V3 r = v3(ix * m.dscale[0], iy * m.dscale[1], iz * m.dscale[2]);
                 rf = f3((float)r.x, (float)r.y, (float)r.z);
-                const double rr = sqrt(r2), r_1 = 1.0 / rr, r_2 = r_1 * r_1, r_3 = r_1 * r_2;
+                const double r_1 = rsqrt(r2), rr = r2 * r_1, r_2 = r_1 * r_1, r_3 = r_1 * r_2;
                 const double au3 = a.a * r2 * rr * s_ipp[fi.w * m.ntypes + fj.w];
                 const double e = exp(-au3);
                 const double l3 = 1.0 - e, l5 = 1.0 - (1.0 + au3) * e;

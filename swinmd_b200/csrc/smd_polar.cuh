@@ -141,14 +141,15 @@ __device__ __forceinline__ void bn_erfc(double r2, double alpha, double B[6]) {
     B[4] = (-7 * B[3] + 8 * a2pi * a2 * a2 * a2 * ex) * ir2;
     B[5] = (-9 * B[4] - 16 * a2pi * a2 * a2 * a2 * a2 * ex) * ir2;
 }
-// the same B_n for a pass that also needs r and 1/r^2 (one division: 1/r
-// is r / r^2)
+// the same B_n for a pass that also needs r and 1/r^2, from one reciprocal
+// square root
 __device__ __forceinline__ void bn_erfc_r(double r2, double alpha, double B[6], double &r, double &ir2) {
     const double a2 = alpha * alpha, a2pi = 2.0 * alpha / SQRT_PI_POLAR;
-    r = sqrt(r2);
-    ir2 = 1.0 / r2;
+    const double ir = rsqrt(r2);
+    r = r2 * ir;
+    ir2 = ir * ir;
     const double ex = exp(-a2 * r2);
-    B[0] = erfc(alpha * r) * (r * ir2);
+    B[0] = erfc(alpha * r) * ir;
     B[1] = (-B[0] - a2pi * ex) * ir2;
     B[2] = (-3 * B[1] + 2 * a2pi * a2 * ex) * ir2;
     B[3] = (-5 * B[2] - 4 * a2pi * a2 * a2 * ex) * ir2;
