@@ -290,6 +290,7 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned int *p) {
     return v;
 }
 __device__ bool grid_barrier(unsigned int *bar, unsigned int target, unsigned int *status) {
+    __shared__ int s_ok;   // thread 0's verdict: every thread of the block takes the same branch
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
@@ -303,9 +304,10 @@ __device__ bool grid_barrier(unsigned int *bar, unsigned int target, unsigned in
             }
         }
         __threadfence();
+        s_ok = (*(volatile unsigned int *)status & ST_CG_ITER) == 0;
     }
     __syncthreads();
-    return (*(volatile unsigned int *)status & ST_CG_ITER) == 0;
+    return s_ok != 0;
 }
 
 struct CGArgs {
