@@ -194,6 +194,7 @@ int ensure_ind_rows(Ctx &c);
 // dipole-guess network (smd_mlp.cu)
 int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed);
 void launch_mlp_guess(Ctx &c);
+void launch_blk_response(Ctx &c, double *out);
 void launch_mlp_features(Ctx &c);
 void launch_mlp_collect(Ctx &c);
 void launch_mlp_norm(Ctx &c);

@@ -1250,8 +1250,59 @@ void launch_ind_field(Ctx &c) {
         k_ind_field<float><<<nb, 256, 0, c.stream>>>(a, R, c.status);
     else
         k_ind_field<double><<<nb, 256, 0, c.stream>>>(a, R, c.status);
+    // the preconditioner's inverse molecule blocks (they need this step's tensor rows)
+    if (c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk) {
+        const int nbm = (c.nmol + MB_MOLS - 1) / MB_MOLS;
+        if (f32)
+            k_mol_blocks<float><<<nbm, 81 * MB_MOLS, 0, c.stream>>>(c.nmol, c.mol_off, c.mol_atoms, R, c.type_polar,
+                                                                    c.pos4, c.cg_blk);
+        else
+            k_mol_blocks<double><<<nbm, 81 * MB_MOLS, 0, c.stream>>>(c.nmol, c.mol_off, c.mol_atoms, R,
+                                                                     c.type_polar, c.pos4, c.cg_blk);
+    }
     const bool learned = c.cg_guess == SMD_GUESS_LEARNED && c.mlp_ready;
     if (learned) launch_mlp_guess(c);  // writes the start dipoles into p
+}
+
+// Response of each molecule's own block to the change of the permanent field
+// since the last stored step, out = M_m^-1 (E0(t) - E0(t-1)) (M_m^-1 E0(t)
+// when no step is stored), nine threads per molecule; with the site
+// preconditioner the block is diag(alpha).  It is the first-order part of
+// the learned guess.
+constexpr int RESP_MOLS = 32;
+__global__ void __launch_bounds__(9 * RESP_MOLS) k_blk_response(int n, int nmol, const int *mol_off,
+                                                               const int *mol_atoms, const double *blk,
+                                                               const double *polar, const double4 *pos4,
+                                                               const double *e0, const double *ph,
+                                                               const int *flags, double *out) {
+    __shared__ double s_v[9 * RESP_MOLS];
+    const int ml = threadIdx.x / 9, e = threadIdx.x - 9 * ml, q = e / 3, d = e - 3 * q;
+    const int m = blockIdx.x * RESP_MOLS + ml;
+    const int cnt = flags[2];
+    const double *eprev = cnt >= 1 ? ph + (size_t)((cnt - 1) & 3) * 6 * n + 3 * (size_t)n : nullptr;
+    int ns = 0, i = -1;
+    if (m < nmol) {
+        const int s0 = mol_off[m];
+        ns = min(3, mol_off[m + 1] - s0);
+        if (q < ns) i = mol_atoms[s0 + q];
+    }
+    const size_t idx = (size_t)d * n + i;
+    s_v[threadIdx.x] = i >= 0 ? e0[idx] - (eprev ? eprev[idx] : 0.0) : 0.0;
+    __syncthreads();
+    if (i < 0) return;
+    double u = 0.0;
+    if (blk) {
+        for (int col = 0; col < 3 * ns; col++) u += blk[(size_t)(e * 9 + col) * nmol + m] * s_v[9 * ml + col];
+    } else {
+        u = fmax(1e-8, polar[(int)pos4[i].w]) * s_v[threadIdx.x];
+    }
+    out[idx] = u;
+}
+
+void launch_blk_response(Ctx &c, double *out) {
+    const double *blk = c.cg_precond == SMD_PRECOND_MOLECULE ? c.cg_blk : nullptr;
+    k_blk_response<<<(c.nmol + RESP_MOLS - 1) / RESP_MOLS, 9 * RESP_MOLS, 0, c.stream>>>(
+        c.n, c.nmol, c.mol_off, c.mol_atoms, blk, c.type_polar, c.pos4, c.e0, c.phist, c.flags, out);
 }
 
 // the PCG solve from the start dipoles, then the site records' new dipoles
@@ -1273,17 +1324,8 @@ void launch_ind_cg(Ctx &c) {
     g.nblocks = c.cg_blocks; g.max_iter = c.cg_max_iter; g.tol = c.cg_tol;
     // 0: start from alpha E0; 1: start from the dipoles in p (previous solve or network)
     g.guess = (c.cg_guess == SMD_GUESS_PREVIOUS || learned) ? 1 : 0;
-    const bool bj = c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk;
+    const bool bj = c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk;   // blocks built by launch_ind_field
     g.blk = c.cg_blk;
-    if (bj) {
-        const int nb = (c.nmol + MB_MOLS - 1) / MB_MOLS;
-        if (f32)
-            k_mol_blocks<float><<<nb, 81 * MB_MOLS, 0, c.stream>>>(c.nmol, c.mol_off, c.mol_atoms, R, c.type_polar,
-                                                                   c.pos4, c.cg_blk);
-        else
-            k_mol_blocks<double><<<nb, 81 * MB_MOLS, 0, c.stream>>>(c.nmol, c.mol_off, c.mol_atoms, R, c.type_polar,
-                                                                    c.pos4, c.cg_blk);
-    }
     cudaMemsetAsync(c.cg_bar, 0, sizeof(unsigned int), c.stream);
     // cooperative launch: the runtime refuses it unless every block can be
     // resident at once, which the grid barrier relies on

@@ -26,6 +26,7 @@
 // Integrator::computePressure (src/Integrator.cpp:205-270, SHAKE virial added
 // to the atomic tensor as at LFIntegrator.cpp:805-814) and clears the force
 // accumulators for the next step.
+#include <type_traits>
 #include "smd_ctx.cuh"
 
 namespace smd {
@@ -141,29 +142,47 @@ __device__ __forceinline__ void shake_mol(const IntArgs &a, int m, int s, int e,
     }
     int count = 0;
     bool done = false;
-    while (!done && count < a.shake_max) {
-        done = true;
-        for (int i = 0; i < nb; i++) {
-            int nx = i + 1;
-            if (nx == ns) nx = 0;
-            double nx_ = rn[i][0] - rn[nx][0], ny_ = rn[i][1] - rn[nx][1], nz_ = rn[i][2] - rn[nx][2];
-            pbc3(nx_, ny_, nz_, a.box);
-            const double r2 = nx_ * nx_ + ny_ * ny_ + nz_ * nz_;
-            const double blen = bl[i < 3 ? i : 2];
-            const double diff = blen - r2;
-            if (fabs(diff) > blen * tol2) {
-                const double ox = ob[i][0], oy = ob[i][1], oz = ob[i][2];
-                const double rr = ox * nx_ + oy * ny_ + oz * nz_;
-                if (rr < blen * a.shake_tol) { shake_geom = true; done = true; count = a.shake_max; break; }
-                const double factor = diff / (2 * rr * (mr[i] + mr[nx]));
-                sfn[i][0] += factor * nx_; sfn[i][1] += factor * ny_; sfn[i][2] += factor * nz_;
-                rn[i][0] += factor * ox * mr[i]; rn[i][1] += factor * oy * mr[i]; rn[i][2] += factor * oz * mr[i];
-                rn[nx][0] -= factor * ox * mr[nx]; rn[nx][1] -= factor * oy * mr[nx]; rn[nx][2] -= factor * oz * mr[nx];
-                done = false;
+    // the cyclic sweeps; PBC selects the minimum image of the new bond vectors
+    auto sweeps = [&](auto pbc) {
+        while (!done && count < a.shake_max) {
+            done = true;
+            for (int i = 0; i < nb; i++) {
+                int nx = i + 1;
+                if (nx == ns) nx = 0;
+                double nx_ = rn[i][0] - rn[nx][0], ny_ = rn[i][1] - rn[nx][1], nz_ = rn[i][2] - rn[nx][2];
+                if (decltype(pbc)::value) pbc3(nx_, ny_, nz_, a.box);
+                const double r2 = nx_ * nx_ + ny_ * ny_ + nz_ * nz_;
+                const double blen = bl[i < 3 ? i : 2];
+                const double diff = blen - r2;
+                if (fabs(diff) > blen * tol2) {
+                    const double ox = ob[i][0], oy = ob[i][1], oz = ob[i][2];
+                    const double rr = ox * nx_ + oy * ny_ + oz * nz_;
+                    if (rr < blen * a.shake_tol) { shake_geom = true; done = true; count = a.shake_max; break; }
+                    const double factor = diff / (2 * rr * (mr[i] + mr[nx]));
+                    sfn[i][0] += factor * nx_; sfn[i][1] += factor * ny_; sfn[i][2] += factor * nz_;
+                    rn[i][0] += factor * ox * mr[i]; rn[i][1] += factor * oy * mr[i]; rn[i][2] += factor * oz * mr[i];
+                    rn[nx][0] -= factor * ox * mr[nx]; rn[nx][1] -= factor * oy * mr[nx];
+                    rn[nx][2] -= factor * oz * mr[nx];
+                    done = false;
+                }
             }
+            count++;
         }
-        count++;
+    };
+    // The minimum image leaves a bond vector unchanged while each component is
+    // below half the box.  When every bond starts below a quarter of the box
+    // the corrections (a small fraction of a bond length) cannot carry one
+    // across half the box, so the sweeps skip the image test and give the
+    // same numbers; a molecule split across the boundary takes the test.
+    bool whole = true;
+    for (int i = 0; i < nb; i++) {
+        const int nx = i + 1 == ns ? 0 : i + 1;
+        for (int d = 0; d < 3; d++) whole = whole && fabs(rn[i][d] - rn[nx][d]) < 0.5 * a.box.half[d];
     }
+    if (whole)
+        sweeps(std::integral_constant<bool, false>());
+    else
+        sweeps(std::integral_constant<bool, true>());
     if (!done) shake_fail = true;
     for (int i = 0; i < nb; i++)
         for (int p = 0; p < 3; p++)
@@ -335,25 +354,24 @@ __global__ void __launch_bounds__(INT_BLOCK) k_integrate(IntArgs a) {
     __threadfence();
 
     // ---- last block: totals in a fixed order ---------------------------
-    // each thread sums a fixed strided subset of blocks for every slot, then
-    // a fixed tree over the threads (same order on every run)
-    __shared__ double s_acc[INT_BLOCK][NPART + 1];
+    // warp w sums slots w, w + 4, ...: each lane a fixed strided subset of
+    // the blocks, then the warp's butterfly (same order on every run)
     __shared__ double tot[NPART];
-    for (int q = 0; q < NPART; q++) {
+    for (int q = w; q < NPART; q += INT_BLOCK / 32) {
         double v = 0;
-        for (int b = threadIdx.x; b < a.nblocks; b += INT_BLOCK)
-            v += __ldcg(&a.partials[(size_t)b * NPART + q]);
-        s_acc[threadIdx.x][q] = v;
+        for (int b = lane; b < a.nblocks; b += 32) v += __ldcg(&a.partials[(size_t)b * NPART + q]);
+        v = warp_sum(v);
+        if (lane == 0) tot[q] = v;
     }
-    __syncthreads();
-    for (int o = INT_BLOCK / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o)
-            for (int q = 0; q < NPART; q++) s_acc[threadIdx.x][q] += s_acc[threadIdx.x + o][q];
-        __syncthreads();
-    }
-    if (threadIdx.x < NPART) tot[threadIdx.x] = s_acc[0][threadIdx.x];
     __syncthreads();
     if (threadIdx.x == 0) {
+        // every accumulator into registers before the first store through o
+        long long acc[ACC_COUNT];
+#pragma unroll
+        for (int q = 0; q < ACC_COUNT; q++) acc[q] = __ldcg(&a.acc[q]);
+        const double fnhmi = a.scal[SC_FNHMI];
+        const int list_updates = a.flags[1];
+        const unsigned int status = *a.status;
         smd_observables &o = *a.obs;
         const double keA = tot[P_KEA], keM = tot[P_KEM];
         // Nose-Hoover zeta update (LFIntegrator.cpp:688-722)
@@ -362,7 +380,6 @@ __global__ void __launch_bounds__(INT_BLOCK) k_integrate(IntArgs a) {
             const double qq = ndf * KB * a.temperature * a.tau * a.tau;
             const double invqq = 1.0 / qq;
             const double ke = a.atom_thermo ? keA : keM;
-            const double fnhmi = a.scal[SC_FNHMI];
             const double fnhpl = fnhmi + a.dt * invqq * (ke - ndf * KB * a.temperature);
             a.scal[SC_FNH] = 0.5 * (fnhpl + fnhmi);
             a.scal[SC_FNHMI] = fnhpl;
@@ -374,26 +391,29 @@ __global__ void __launch_bounds__(INT_BLOCK) k_integrate(IntArgs a) {
         o.ke_mol = 0.5 * keM;
         o.t_atom = keA / (a.atom_ndf * KB);
         o.t_mol = keM / (a.mol_ndf * KB);
-        const long long *acc = a.acc;
-        o.energy[SMD_E_VDW] = (double)__ldcg(&acc[ACC_E_VDW]) * ACC_INV + a.e_lrc;
-        o.energy[SMD_E_REAL] = (double)__ldcg(&acc[ACC_E_REAL]) * ACC_INV;
-        o.energy[SMD_E_LONG] = (double)__ldcg(&acc[ACC_E_LONG]) * ACC_INV;
-        o.energy[SMD_E_CORRECT] = a.e_self + (double)__ldcg(&acc[ACC_E_SELF]) * ACC_INV;
-        o.energy[SMD_E_MOLCORRECT] = (double)__ldcg(&acc[ACC_E_INTRA]) * ACC_INV;
-        o.energy[SMD_E_SURF] = (double)__ldcg(&acc[ACC_E_SURF]) * ACC_INV;
-        o.energy[SMD_E_POL_REAL] = (double)__ldcg(&acc[ACC_E_POL_REAL]) * ACC_INV;
-        o.energy[SMD_E_POL_LONG] = (double)__ldcg(&acc[ACC_E_POL_LONG]) * ACC_INV;
-        o.energy[SMD_E_POL_SELF] = (double)__ldcg(&acc[ACC_E_POL_SELF]) * ACC_INV;
-        o.energy[SMD_E_POL_INTRA] = (double)__ldcg(&acc[ACC_E_POL_INTRA]) * ACC_INV;
+        double en[10];
+        en[SMD_E_VDW] = (double)acc[ACC_E_VDW] * ACC_INV + a.e_lrc;
+        en[SMD_E_REAL] = (double)acc[ACC_E_REAL] * ACC_INV;
+        en[SMD_E_LONG] = (double)acc[ACC_E_LONG] * ACC_INV;
+        en[SMD_E_CORRECT] = a.e_self + (double)acc[ACC_E_SELF] * ACC_INV;
+        en[SMD_E_MOLCORRECT] = (double)acc[ACC_E_INTRA] * ACC_INV;
+        en[SMD_E_SURF] = (double)acc[ACC_E_SURF] * ACC_INV;
+        en[SMD_E_POL_REAL] = (double)acc[ACC_E_POL_REAL] * ACC_INV;
+        en[SMD_E_POL_LONG] = (double)acc[ACC_E_POL_LONG] * ACC_INV;
+        en[SMD_E_POL_SELF] = (double)acc[ACC_E_POL_SELF] * ACC_INV;
+        en[SMD_E_POL_INTRA] = (double)acc[ACC_E_POL_INTRA] * ACC_INV;
         double ep = 0;
-        for (int q = 0; q < 10; q++) ep += o.energy[q];
+        for (int q = 0; q < 10; q++) {
+            o.energy[q] = en[q];
+            ep += en[q];
+        }
         o.e_potential = ep;
         // virial and pressure tensors (Integrator::computePressure; SHAKE
         // virial added afterwards to the atomic tensor, LFIntegrator.cpp:805-814)
         const int sym[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
         const double idt2 = 1.0 / (a.dt * a.dt);
         for (int q = 0; q < 9; q++) {
-            double vir = ((double)__ldcg(&acc[ACC_VIR + q]) + (double)__ldcg(&acc[ACC_LVIR + q])) * ACC_INV;
+            double vir = ((double)acc[ACC_VIR + q] + (double)acc[ACC_LVIR + q]) * ACC_INV;
             if (q == 0 || q == 4 || q == 8) vir -= a.v_lrc;
             o.mol_pressure[q] = (tot[P_MP + sym[q]] + vir - tot[P_MC + q]) / a.volume;
             o.atom_pressure[q] = (tot[P_AP + sym[q]] + vir) / a.volume;
@@ -411,9 +431,9 @@ __global__ void __launch_bounds__(INT_BLOCK) k_integrate(IntArgs a) {
         a.scal[SC_VOM] = vx; a.scal[SC_VOM + 1] = vy; a.scal[SC_VOM + 2] = vz;
         a.scal[SC_APPLY] = (fabs(vx) > 1e-11 || fabs(vy) > 1e-11 || fabs(vz) > 1e-11) ? 1.0 : 0.0;
         o.step += 1;
-        o.list_updates = a.flags[1];
-        o.pairs_in_cutoff = __ldcg(&acc[ACC_NPAIR]) / 2;
-        o.status = *a.status;
+        o.list_updates = list_updates;
+        o.pairs_in_cutoff = acc[ACC_NPAIR] / 2;
+        o.status = status;
         if (a.series_cap > 0) {
             long long slot = (o.step - 1) % a.series_cap;
             double *r = a.series + slot * 5;

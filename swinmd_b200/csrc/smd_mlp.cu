@@ -58,11 +58,13 @@ __device__ __forceinline__ V3 hist_e(const double *ph, int n, int cnt, int k, in
     return v3(h[i], h[n + i], h[2 * n + i]);
 }
 
-// first-order guess: the previous dipoles moved by the linear response to
-// the change of the permanent field (alpha E0 when nothing is stored)
-__device__ __forceinline__ V3 linear_guess(const double *ph, int n, int cnt, int i, V3 E, double alpha) {
-    if (cnt < 1) return alpha * E;
-    return hist_p(ph, n, cnt, 1, i) + alpha * (E - hist_e(ph, n, cnt, 1, i));
+// first-order guess: the previous dipoles moved by dl, the response of the
+// molecule's block to the change of the permanent field (k_blk_response;
+// dl = M^-1 E0 when nothing is stored)
+__device__ __forceinline__ V3 linear_guess(const double *ph, int n, int cnt, int i, const double *dl) {
+    const V3 r = v3(dl[i], dl[n + i], dl[2 * n + i]);
+    if (cnt < 1) return r;
+    return hist_p(ph, n, cnt, 1, i) + r;
 }
 
 __global__ void k_mlp_features(int n, const int *mol, const int *mol_off, const int *mol_atoms,
@@ -99,19 +101,17 @@ __global__ void k_mlp_features(int n, const int *mol, const int *mol_off, const 
 
 // appends (features, target) rows of the current configuration: the target
 // is what the network should add to the first-order guess (needs 2 stored steps)
-__global__ void k_mlp_collect(int n, const float *x, const double *frame, const double *p, const double *e0,
-                              const double4 *pos4, const double *polar, const double *ph, const int *flags,
-                              float *data, long long row0) {
+__global__ void k_mlp_collect(int n, const float *x, const double *frame, const double *p, const double *dl,
+                              const double *ph, const int *flags, float *data, long long row0) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float *row = data + (size_t)(row0 + i) * (MF + MO);
     for (int k = 0; k < MF; k++) row[k] = x[(size_t)i * MF + k];
-    const double a = fmax(1e-8, polar[(int)pos4[i].w]);
-    const V3 pl = linear_guess(ph, n, flags[2], i, v3(e0[i], e0[n + i], e0[2 * n + i]), a);
-    const V3 dl = in_axes(frame, n, i, v3(p[i], p[n + i], p[2 * n + i]) - pl);
-    row[MF] = (float)dl.x * TARGET_SCALE;
-    row[MF + 1] = (float)dl.y * TARGET_SCALE;
-    row[MF + 2] = (float)dl.z * TARGET_SCALE;
+    const V3 pl = linear_guess(ph, n, flags[2], i, dl);
+    const V3 dt = in_axes(frame, n, i, v3(p[i], p[n + i], p[2 * n + i]) - pl);
+    row[MF] = (float)dt.x * TARGET_SCALE;
+    row[MF + 1] = (float)dt.y * TARGET_SCALE;
+    row[MF + 2] = (float)dt.z * TARGET_SCALE;
 }
 
 // feature mean and 1/std over the collected rows (one block, fixed order)
@@ -164,8 +164,7 @@ constexpr int MLP_IBLOCK = 128;
 constexpr int MLP_ISITES = MLP_IBLOCK / MLP_ITPP;
 constexpr int HP = MH + 1;   // padded row of hidden activations / of W2
 __global__ void __launch_bounds__(MLP_IBLOCK) k_mlp_infer(int n, const float *x, const float *norm, const float *Wg,
-                                                          const double *frame, const double *e0,
-                                                          const double4 *pos4, const double *polar,
+                                                          const double *frame, const double *dl,
                                                           const double *ph, const int *flags, double *p) {
     __shared__ float sW1[MH * MF], sB1[MH], sW2[MH * HP], sB2[MH], sW3[MO * MH], sB3[MO];
     __shared__ float sX[MLP_ISITES][MF], sH1[MLP_ISITES][HP];
@@ -202,8 +201,7 @@ __global__ void __launch_bounds__(MLP_IBLOCK) k_mlp_infer(int n, const float *x,
     y1 = group_sum<MLP_ITPP>(y1) + sB3[1];
     y2 = group_sum<MLP_ITPP>(y2) + sB3[2];
     if (!own || t != 0) return;
-    const double a = fmax(1e-8, polar[(int)pos4[i].w]);
-    V3 g = linear_guess(ph, n, cnt, i, v3(e0[i], e0[n + i], e0[2 * n + i]), a);
+    V3 g = linear_guess(ph, n, cnt, i, dl);
     if (cnt >= 2) {
         const V3 u = axis(frame, n, i, 0), v = axis(frame, n, i, 1), w = axis(frame, n, i, 2);
         g = g + (y0 / TARGET_SCALE) * u + (y1 / TARGET_SCALE) * v + (y2 / TARGET_SCALE) * w;
@@ -300,10 +298,16 @@ void launch_mlp_features(Ctx &c) {
                                                             c.e0, c.phist, c.flags, c.mlp_x);
 }
 
+// the first-order response goes to the solver's s slot of its work area,
+// which the solve writes before it first reads it
+static double *response_scratch(Ctx &c) { return c.cgw + 20 * (size_t)c.n; }
+
 void launch_mlp_guess(Ctx &c) {
     launch_mlp_features(c);
+    double *dl = response_scratch(c);
+    launch_blk_response(c, dl);
     k_mlp_infer<<<(c.n + MLP_ISITES - 1) / MLP_ISITES, MLP_IBLOCK, 0, c.stream>>>(
-        c.n, c.mlp_x, c.mlp_norm, c.mlp_w, c.frame, c.e0, c.pos4, c.type_polar, c.phist, c.flags, c.pind);
+        c.n, c.mlp_x, c.mlp_norm, c.mlp_w, c.frame, dl, c.phist, c.flags, c.pind);
 }
 
 int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed) {
@@ -343,9 +347,10 @@ int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed) {
 
 void launch_mlp_collect(Ctx &c) {
     launch_mlp_features(c);
-    k_mlp_collect<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.mlp_x, c.frame, c.pind, c.e0, c.pos4,
-                                                           c.type_polar, c.phist, c.flags, c.mlp_data,
-                                                           c.mlp_rows);
+    double *dl = response_scratch(c);
+    launch_blk_response(c, dl);   // the blocks of the solve that produced p
+    k_mlp_collect<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.mlp_x, c.frame, c.pind, dl, c.phist, c.flags,
+                                                           c.mlp_data, c.mlp_rows);
 }
 
 void launch_mlp_norm(Ctx &c) {
