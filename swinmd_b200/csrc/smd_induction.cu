@@ -1173,14 +1173,29 @@ __global__ void k_ind_mol(IndArgs a, long long *trq, long long *acc) {
 
 // ring of the last 4 steps' converged dipoles and permanent fields;
 // flags[2] counts the stored steps
-__global__ void k_hist_push(int n, const double *p, const double *e0, double *ph, const int *flags) {
+// Stores the step's dipoles and permanent field in ring slot flags[2] & 3.
+// The last block to finish (ticket flags[3]) advances the step count
+// flags[2] and clears the ticket: every block has read the count before it
+// takes its ticket.
+__global__ void k_hist_push(int n, const double *p, const double *e0, double *ph, int *flags) {
+    __shared__ bool s_last;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double *h = ph + (size_t)(flags[2] & 3) * 6 * n;
-    h[i] = p[i]; h[n + i] = p[n + i]; h[2 * n + i] = p[2 * n + i];
-    h[3 * n + i] = e0[i]; h[4 * n + i] = e0[n + i]; h[5 * n + i] = e0[2 * n + i];
+    if (i < n) {
+        double *h = ph + (size_t)(flags[2] & 3) * 6 * n;
+        h[i] = p[i]; h[n + i] = p[n + i]; h[2 * n + i] = p[2 * n + i];
+        h[3 * n + i] = e0[i]; h[4 * n + i] = e0[n + i]; h[5 * n + i] = e0[2 * n + i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&flags[3], 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        flags[2] += 1;
+        flags[3] = 0;
+    }
 }
-__global__ void k_hist_advance(int *flags) { flags[2] += 1; }
 
 static IndArgs ind_args(Ctx &c) {
     IndArgs a;
@@ -1350,7 +1365,6 @@ void launch_ind_cg(Ctx &c) {
     // a time step stores its converged dipoles for the next steps' guess
     if (c.in_step && c.phist) {
         k_hist_push<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.pind, c.e0, c.phist, c.flags);
-        k_hist_advance<<<1, 1, 0, c.stream>>>(c.flags);
     }
 }
 

@@ -67,13 +67,10 @@ __device__ __forceinline__ V3 linear_guess(const double *ph, int n, int cnt, int
     return hist_p(ph, n, cnt, 1, i) + r;
 }
 
-__global__ void k_mlp_features(int n, const int *mol, const int *mol_off, const int *mol_atoms,
-                               const double4 *pos4, const double *frame, const double *e0, const double *ph,
-                               const int *flags, float *x) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int cnt = flags[2];
-    float f[MF];
+// the F inputs of site i (one thread)
+__device__ __forceinline__ void site_features(int i, int n, int cnt, const int *mol, const int *mol_off,
+                                              const int *mol_atoms, const double4 *pos4, const double *frame,
+                                              const double *e0, const double *ph, float (&f)[MF]) {
     const V3 E = v3(e0[i], e0[n + i], e0[2 * n + i]);
     const V3 El = in_axes(frame, n, i, E);
     f[0] = (float)El.x; f[1] = (float)El.y; f[2] = (float)El.z;
@@ -96,6 +93,15 @@ __global__ void k_mlp_features(int n, const int *mol, const int *mol_off, const 
         f[q++] = (float)Ej.x; f[q++] = (float)Ej.y; f[q++] = (float)Ej.z;
     }
     f[19] = (int)pos4[i].w == 0 ? 0.f : 1.f;
+}
+
+__global__ void k_mlp_features(int n, const int *mol, const int *mol_off, const int *mol_atoms,
+                               const double4 *pos4, const double *frame, const double *e0, const double *ph,
+                               const int *flags, float *x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float f[MF];
+    site_features(i, n, flags[2], mol, mol_off, mol_atoms, pos4, frame, e0, ph, f);
     for (int k = 0; k < MF; k++) x[(size_t)i * MF + k] = f[k];
 }
 
@@ -155,44 +161,66 @@ __device__ __forceinline__ void mlp_forward(const float *W, const float *xn, flo
     }
 }
 
-// Inference with MLP_ITPP threads per site: each computes MH / MLP_ITPP
-// hidden units of each layer; the hidden activations go through shared
-// memory (rows padded to avoid bank conflicts), the three outputs are summed
+// Inference with MLP_ITPP threads per site, features computed in the same
+// kernel (one thread per site, while the block stages the weights).  Each
+// thread computes MH / MLP_ITPP hidden units of each layer; weights and
+// activations sit in shared memory in rows padded to a multiple of four
+// floats, read as float4 with four partial sums per unit (the two operands
+// of four multiply-adds in two 16-byte loads); the three outputs are summed
 // over the site's threads by shuffles.
 constexpr int MLP_ITPP = 4;
 constexpr int MLP_IBLOCK = 128;
 constexpr int MLP_ISITES = MLP_IBLOCK / MLP_ITPP;
-constexpr int HP = MH + 1;   // padded row of hidden activations / of W2
-__global__ void __launch_bounds__(MLP_IBLOCK) k_mlp_infer(int n, const float *x, const float *norm, const float *Wg,
+constexpr int HP = MH + 4;   // padded row of hidden activations / of W2
+static_assert(MF % 4 == 0 && MH % 4 == 0 && OW2 % 4 == 0, "float4 rows");
+__device__ __forceinline__ float dot4(const float4 *w, const float4 *h, int cnt4, float z) {
+    float z1 = 0.f, z2 = 0.f, z3 = 0.f;
+#pragma unroll
+    for (int k = 0; k < cnt4; k++) {
+        const float4 a = w[k], b = h[k];
+        z = fmaf(a.x, b.x, z); z1 = fmaf(a.y, b.y, z1); z2 = fmaf(a.z, b.z, z2); z3 = fmaf(a.w, b.w, z3);
+    }
+    return (z + z1) + (z2 + z3);
+}
+__global__ void __launch_bounds__(MLP_IBLOCK) k_mlp_infer(int n, const int *mol, const int *mol_off,
+                                                          const int *mol_atoms, const double4 *pos4,
+                                                          const double *e0, const float *norm, const float *Wg,
                                                           const double *frame, const double *dl,
                                                           const double *ph, const int *flags, double *p) {
-    __shared__ float sW1[MH * MF], sB1[MH], sW2[MH * HP], sB2[MH], sW3[MO * MH], sB3[MO];
-    __shared__ float sX[MLP_ISITES][MF], sH1[MLP_ISITES][HP];
-    for (int k = threadIdx.x; k < MH * MF; k += blockDim.x) sW1[k] = Wg[OW1 + k];
-    for (int k = threadIdx.x; k < MH * MH; k += blockDim.x) sW2[(k / MH) * HP + k % MH] = Wg[OW2 + k];
+    __shared__ __align__(16) float sW1[MH * MF];
+    __shared__ __align__(16) float sW2[MH * HP];
+    __shared__ __align__(16) float sX[MLP_ISITES][MF];
+    __shared__ __align__(16) float sH1[MLP_ISITES][HP];
+    __shared__ float sB1[MH], sB2[MH], sW3[MO * MH], sB3[MO];
+    const int cnt = flags[2];
+    {
+        const float4 *g1 = (const float4 *)(Wg + OW1), *g2 = (const float4 *)(Wg + OW2);
+        for (int k = threadIdx.x; k < MH * MF / 4; k += blockDim.x) ((float4 *)sW1)[k] = g1[k];
+        for (int k = threadIdx.x; k < MH * MH / 4; k += blockDim.x) {
+            const int j = k / (MH / 4), c4 = k - j * (MH / 4);
+            *(float4 *)&sW2[j * HP + 4 * c4] = g2[k];
+        }
+    }
     for (int k = threadIdx.x; k < MO * MH; k += blockDim.x) sW3[k] = Wg[OW3 + k];
     for (int k = threadIdx.x; k < MH; k += blockDim.x) { sB1[k] = Wg[OB1 + k]; sB2[k] = Wg[OB2 + k]; }
     if (threadIdx.x < MO) sB3[threadIdx.x] = Wg[OB3 + threadIdx.x];
+    if (threadIdx.x < MLP_ISITES) {
+        const int is = blockIdx.x * MLP_ISITES + threadIdx.x;
+        float f[MF];
+        if (is < n) site_features(is, n, cnt, mol, mol_off, mol_atoms, pos4, frame, e0, ph, f);
+#pragma unroll
+        for (int k = 0; k < MF; k++) sX[threadIdx.x][k] = is < n ? (f[k] - norm[k]) * norm[MF + k] : 0.f;
+    }
     const int ls = threadIdx.x / MLP_ITPP, t = threadIdx.x % MLP_ITPP;
     const int i = blockIdx.x * MLP_ISITES + ls;
     const bool own = i < n;
-    const int cnt = flags[2];
-    for (int f = t; f < MF; f += MLP_ITPP)
-        sX[ls][f] = own ? (x[(size_t)i * MF + f] - norm[f]) * norm[MF + f] : 0.f;
     __syncthreads();
-    for (int j = t; j < MH; j += MLP_ITPP) {
-        float z = sB1[j];
-#pragma unroll
-        for (int f = 0; f < MF; f++) z = fmaf(sW1[j * MF + f], sX[ls][f], z);
-        sH1[ls][j] = tanhf(z);
-    }
+    for (int j = t; j < MH; j += MLP_ITPP)
+        sH1[ls][j] = tanhf(dot4((const float4 *)&sW1[j * MF], (const float4 *)sX[ls], MF / 4, sB1[j]));
     __syncthreads();
     float y0 = 0.f, y1 = 0.f, y2 = 0.f;
     for (int j = t; j < MH; j += MLP_ITPP) {
-        float z = sB2[j];
-#pragma unroll 16
-        for (int k = 0; k < MH; k++) z = fmaf(sW2[j * HP + k], sH1[ls][k], z);
-        const float h2 = tanhf(z);
+        const float h2 = tanhf(dot4((const float4 *)&sW2[j * HP], (const float4 *)sH1[ls], MH / 4, sB2[j]));
         y0 = fmaf(sW3[j], h2, y0);
         y1 = fmaf(sW3[MH + j], h2, y1);
         y2 = fmaf(sW3[2 * MH + j], h2, y2);
@@ -303,11 +331,11 @@ void launch_mlp_features(Ctx &c) {
 static double *response_scratch(Ctx &c) { return c.cgw + 20 * (size_t)c.n; }
 
 void launch_mlp_guess(Ctx &c) {
-    launch_mlp_features(c);
     double *dl = response_scratch(c);
     launch_blk_response(c, dl);
     k_mlp_infer<<<(c.n + MLP_ISITES - 1) / MLP_ISITES, MLP_IBLOCK, 0, c.stream>>>(
-        c.n, c.mlp_x, c.mlp_norm, c.mlp_w, c.frame, dl, c.phist, c.flags, c.pind);
+        c.n, c.mol, c.mol_off, c.mol_atoms, c.pos4, c.e0, c.mlp_norm, c.mlp_w, c.frame, dl, c.phist, c.flags,
+        c.pind);
 }
 
 int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed) {
