@@ -416,80 +416,98 @@ __device__ V3 amul(const CGArgs &c, int i, int t, const G4 *g) {
 // block of A = diag(1/a_i) - T over its own sites, with T_ij from the
 // excluded-site entries of the tensor rows (T v = (r'.v) r' - c3 v), is
 // inverted in FP64.  It captures the strong Thole-damped coupling inside a
-// water molecule that the diagonal preconditioner leaves out.  81 threads
-// per molecule (entry (r, c) of its 9 x 9 block; unused sites padded with
-// the identity), three molecules per block, and an in-place Gauss-Jordan
-// sweep over the nine pivots (no pivoting: the block is positive definite).
-// A block with a non-positive pivot falls back to diag(a_i).  The inverses
-// are stored entry-major over molecules (entry e of molecule m at
-// e * nmol + m), so that the solve's loads of one entry coalesce.
-constexpr int MB_MOLS = 3;
+// water molecule that the diagonal preconditioner leaves out.  Nine threads
+// per molecule, each holding one row of its 9 x 9 block in registers
+// (unused sites padded with the identity), MB_MOLS molecules per block, and
+// an in-place Gauss-Jordan sweep over the nine pivots (no pivoting: the
+// block is positive definite): the pivot row, scaled by the reciprocal of
+// the pivot, goes through shared memory to the other eight rows.  A block
+// with a non-positive pivot falls back to diag(a_i).  The inverses are
+// stored entry-major over molecules (entry e of molecule m at e * nmol + m),
+// so that the solve's loads of one entry coalesce.
+constexpr int MB_MOLS = 32;
 template <typename TS>
-__global__ void __launch_bounds__(81 * MB_MOLS) k_mol_blocks(int nmol, const int *mol_off, const int *mol_atoms,
-                                                             TRows R, const double *polar, const double4 *pos4,
-                                                             double *blk) {
+__global__ void __launch_bounds__(9 * MB_MOLS) k_mol_blocks(int nmol, const int *mol_off, const int *mol_atoms,
+                                                            TRows R, const double *polar, const double4 *pos4,
+                                                            double *blk) {
     using TS4 = typename std::conditional<sizeof(TS) == 4, float4, double4>::type;
-    __shared__ double s_a[MB_MOLS][81];
-    __shared__ double s_al[MB_MOLS][3];
-    __shared__ int s_bad[MB_MOLS], s_ns[MB_MOLS];
-    const int lm = threadIdx.x / 81, e = threadIdx.x - 81 * lm, r = e / 9, cc = e - 9 * r;
+    __shared__ double s_piv[MB_MOLS][9];
+    __shared__ int s_bad[MB_MOLS];
+    const int lm = threadIdx.x / 9, r = threadIdx.x - 9 * lm, q = r / 3, x = r - 3 * q;
     const int m = blockIdx.x * MB_MOLS + lm;
     const bool act = m < nmol;
-    s_a[lm][e] = r == cc ? 1.0 : 0.0;   // identity padding for absent sites
-    __syncthreads();
-    // nine threads per molecule assemble the 3 x 3 site-pair blocks (q, qq)
-    if (act && e < 9) {
-        const int q = e / 3, qq = e - 3 * q;
-        const int s0 = mol_off[m], ns = min(3, mol_off[m + 1] - s0);
-        if (e == 0) { s_ns[lm] = ns; s_bad[lm] = 0; }
-        if (q < ns && qq < ns) {
-            const int i = mol_atoms[s0 + q];
-            const double al = fmax(1e-8, polar[(int)pos4[i].w]);
-            double *blk3 = &s_a[lm][27 * q + 3 * qq];   // rows 3q.., columns 3qq..
-            if (q == qq) {
-                s_al[lm][q] = al;
-                for (int x = 0; x < 3; x++)
-                    for (int y = 0; y < 3; y++) blk3[9 * x + y] = x == y ? 1.0 / al : 0.0;
-            } else {
-                const int j = mol_atoms[s0 + qq];
-                const int c1 = min(R.cnt[i], R.cap);
-                for (int x = 0; x < 3; x++)
-                    for (int y = 0; y < 3; y++) blk3[9 * x + y] = 0.0;
-                for (int k = R.lcnt[i]; k < c1; k++)
-                    if (R.j[(size_t)i * R.cap + k] == j) {
-                        const TS4 t = ((const TS4 *)R.c)[(size_t)i * R.cap + k];
-                        const double v[3] = {(double)t.x, (double)t.y, (double)t.z};
-                        for (int x = 0; x < 3; x++)
-                            for (int y = 0; y < 3; y++) blk3[9 * x + y] = -(v[x] * v[y] - (x == y ? (double)t.w : 0.0));
-                    }
-            }
+    if (r == 0) s_bad[lm] = 0;
+    // row r = 3 q + x: site q, axis x; columns 3 qq + y
+    // (all indices into row[] are compile-time, so that it stays in registers)
+    double row[9];
+    int ns = 0;
+    double al = 1.0, diag = 1.0;
+    int js[3] = {-1, -1, -1};
+    int i = -1;
+    if (act) {
+        const int s0 = mol_off[m];
+        ns = min(3, mol_off[m + 1] - s0);
+#pragma unroll
+        for (int qq = 0; qq < 3; qq++)
+            if (qq < ns) js[qq] = mol_atoms[s0 + qq];
+        if (q < ns) {
+            i = q == 0 ? js[0] : (q == 1 ? js[1] : js[2]);
+            al = fmax(1e-8, polar[(int)pos4[i].w]);
+            diag = 1.0 / al;
         }
     }
-    __syncthreads();
-    const int ns = act ? s_ns[lm] : 0;
-    const double al_r = act && r / 3 < ns ? s_al[lm][r / 3] : 1.0;
+#pragma unroll
+    for (int c = 0; c < 9; c++) row[c] = c == r ? diag : 0.0;
+    if (i >= 0) {
+        const int c1 = min(R.cnt[i], R.cap);
+        for (int k = R.lcnt[i]; k < c1; k++) {
+            const int j = R.j[(size_t)i * R.cap + k];
+#pragma unroll
+            for (int qq = 0; qq < 3; qq++)
+                if (qq != q && j == js[qq]) {
+                    const TS4 t = ((const TS4 *)R.c)[(size_t)i * R.cap + k];
+                    const double v0 = (double)t.x, v1 = (double)t.y, v2 = (double)t.z, w = (double)t.w;
+                    const double vx = x == 0 ? v0 : (x == 1 ? v1 : v2);
+                    row[3 * qq] = -(vx * v0 - (x == 0 ? w : 0.0));
+                    row[3 * qq + 1] = -(vx * v1 - (x == 1 ? w : 0.0));
+                    row[3 * qq + 2] = -(vx * v2 - (x == 2 ? w : 0.0));
+                }
+        }
+    }
+#pragma unroll
     for (int k = 0; k < 9; k++) {
-        const double p = s_a[lm][k * 9 + k], rk = s_a[lm][r * 9 + k], kc = s_a[lm][k * 9 + cc];
-        const double own = s_a[lm][e];
-        __syncthreads();
-        if (!(p > 0.0)) {
-            if (e == 0) s_bad[lm] = 1;
-        } else {
-            double v;
-            if (r == k && cc == k) v = 1.0 / p;
-            else if (r == k) v = kc / p;
-            else if (cc == k) v = -rk / p;
-            else v = own - rk * kc / p;
-            s_a[lm][e] = v;
+        __syncthreads();   // the previous pivot row has been read by every row
+        if (r == k) {
+            const double p = row[k];
+            if (!(p > 0.0)) {
+                s_bad[lm] = 1;
+            } else {
+                const double ip = 1.0 / p;
+#pragma unroll
+                for (int c = 0; c < 9; c++) row[c] = c == k ? ip : row[c] * ip;
+            }
+#pragma unroll
+            for (int c = 0; c < 9; c++) s_piv[lm][c] = row[c];
         }
         __syncthreads();
+        if (r != k) {
+            const double f = row[k];
+            const double ip = s_piv[lm][k];
+#pragma unroll
+            for (int c = 0; c < 9; c++) row[c] = c == k ? -f * ip : fma(-f, s_piv[lm][c], row[c]);
+        }
     }
+    __syncthreads();
     if (act) {
         const int nd = 3 * ns;
-        double out = s_a[lm][e];
-        if (s_bad[lm]) out = (r == cc && r < nd) ? al_r : 0.0;
-        if (r >= nd || cc >= nd) out = 0.0;
-        blk[(size_t)e * nmol + m] = out;
+        const bool bad = s_bad[lm] != 0;
+#pragma unroll
+        for (int c = 0; c < 9; c++) {
+            double out = row[c];
+            if (bad) out = (r == c && r < nd) ? al : 0.0;
+            if (r >= nd || c >= nd) out = 0.0;
+            blk[(size_t)(r * 9 + c) * nmol + m] = out;
+        }
     }
 }
 
@@ -1269,11 +1287,11 @@ void launch_ind_field(Ctx &c) {
     if (c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk) {
         const int nbm = (c.nmol + MB_MOLS - 1) / MB_MOLS;
         if (f32)
-            k_mol_blocks<float><<<nbm, 81 * MB_MOLS, 0, c.stream>>>(c.nmol, c.mol_off, c.mol_atoms, R, c.type_polar,
-                                                                    c.pos4, c.cg_blk);
+            k_mol_blocks<float><<<nbm, 9 * MB_MOLS, 0, c.stream>>>(c.nmol, c.mol_off, c.mol_atoms, R, c.type_polar,
+                                                                   c.pos4, c.cg_blk);
         else
-            k_mol_blocks<double><<<nbm, 81 * MB_MOLS, 0, c.stream>>>(c.nmol, c.mol_off, c.mol_atoms, R,
-                                                                     c.type_polar, c.pos4, c.cg_blk);
+            k_mol_blocks<double><<<nbm, 9 * MB_MOLS, 0, c.stream>>>(c.nmol, c.mol_off, c.mol_atoms, R, c.type_polar,
+                                                                    c.pos4, c.cg_blk);
     }
     const bool learned = c.cg_guess == SMD_GUESS_LEARNED && c.mlp_ready;
     if (learned) launch_mlp_guess(c);  // writes the start dipoles into p
