@@ -370,31 +370,22 @@ __device__ __forceinline__ float4 ldcg4(const float4 *p) { return __ldcg(p); }
 
 // (A v)_i from the site's row: CG_TPP lanes take consecutive slots; the
 // row entries are read in batches of CG_UNROLL per lane before the gathers
-// of v, so each lane keeps several loads in flight.  GR is the arithmetic
-// type of the products (the row's storage type), summed per lane in GR.
-// The packed vector is rewritten every iteration, so it is gathered past L1
-// (tried through L1, relying on the barrier's acquire: slower).
+// of v, so each lane keeps several loads in flight.  In FP32 the next
+// batch's row loads are issued before the current batch's products, so the
+// row reads of one batch overlap the gathers of the previous one (in FP64
+// the extra registers spill).  GR is the arithmetic type of the products
+// (the row's storage type), summed per lane in GR.  The packed vector is
+// rewritten every iteration, so it is gathered past L1 (tried through L1,
+// relying on the barrier's acquire: slower).
 template <typename G4, typename GR>
 __device__ V3 amul(const CGArgs &c, int i, int t, const G4 *g) {
-    constexpr int CG_UNROLL = sizeof(GR) == 4 ? 6 : 2;
+    constexpr int CG_UNROLL = sizeof(GR) == 4 ? 3 : 2;
     const TRows &R = c.rows;
     const int cnt = R.cnt[i];
     const int *rj = R.j + (size_t)i * R.cap;
     const G4 *rc = (const G4 *)R.c + (size_t)i * R.cap;
     GR ax = 0, ay = 0, az = 0;
-    for (int s0 = t; s0 < cnt; s0 += CG_UNROLL * CG_TPP) {
-        int jj[CG_UNROLL];
-        G4 cc[CG_UNROLL];
-#pragma unroll
-        for (int u = 0; u < CG_UNROLL; u++) {
-            const int s = s0 + u * CG_TPP;
-            jj[u] = s < cnt ? rj[s] : -1;
-            if (s < cnt) cc[u] = rc[s];
-        }
-        G4 vj[CG_UNROLL];
-#pragma unroll
-        for (int u = 0; u < CG_UNROLL; u++)
-            if (jj[u] >= 0) vj[u] = ldcg4(&g[jj[u]]);
+    auto products = [&](const int (&jj)[CG_UNROLL], const G4 (&cc)[CG_UNROLL], const G4 (&vj)[CG_UNROLL]) {
 #pragma unroll
         for (int u = 0; u < CG_UNROLL; u++)
             if (jj[u] >= 0) {
@@ -403,6 +394,45 @@ __device__ V3 amul(const CGArgs &c, int i, int t, const G4 *g) {
                 ay += cc[u].w * vj[u].y - rv * cc[u].y;
                 az += cc[u].w * vj[u].z - rv * cc[u].z;
             }
+    };
+    auto rows = [&](int s0, int (&jj)[CG_UNROLL], G4 (&cc)[CG_UNROLL]) {
+#pragma unroll
+        for (int u = 0; u < CG_UNROLL; u++) {
+            const int s = s0 + u * CG_TPP;
+            jj[u] = s < cnt ? rj[s] : -1;
+            if (s < cnt) cc[u] = rc[s];
+        }
+    };
+    auto gathers = [&](const int (&jj)[CG_UNROLL], G4 (&vj)[CG_UNROLL]) {
+#pragma unroll
+        for (int u = 0; u < CG_UNROLL; u++)
+            if (jj[u] >= 0) vj[u] = ldcg4(&g[jj[u]]);
+    };
+    if constexpr (sizeof(GR) == 4) {
+        int jj[CG_UNROLL];
+        G4 cc[CG_UNROLL];
+        rows(t, jj, cc);
+        for (int s0 = t; s0 < cnt; s0 += CG_UNROLL * CG_TPP) {
+            G4 vj[CG_UNROLL];
+            gathers(jj, vj);
+            int jn[CG_UNROLL];
+            G4 cn[CG_UNROLL];
+            rows(s0 + CG_UNROLL * CG_TPP, jn, cn);
+            products(jj, cc, vj);
+#pragma unroll
+            for (int u = 0; u < CG_UNROLL; u++) {
+                jj[u] = jn[u];
+                cc[u] = cn[u];
+            }
+        }
+    } else {
+        for (int s0 = t; s0 < cnt; s0 += CG_UNROLL * CG_TPP) {
+            int jj[CG_UNROLL];
+            G4 cc[CG_UNROLL], vj[CG_UNROLL];
+            rows(s0, jj, cc);
+            gathers(jj, vj);
+            products(jj, cc, vj);
+        }
     }
     V3 acc = v3(ax, ay, az);
     if (t == 0) {
