@@ -120,9 +120,7 @@ int sync_status(smd_ctx *x) {
 // induced dipoles (solved once per step) short and long; all torques are
 // mapped onto the sites at the end (the mapping is linear in the torques).
 void enqueue_polar(Ctx &c, bool mp_short, bool mp_long, bool ind_short, bool ind_long) {
-    launch_frames(c);
-    launch_pack_sites(c);
-    launch_torques_begin(c);
+    launch_frames(c);   // also the site records and cleared torques
     const bool all = mp_short && mp_long && ind_short && ind_long && c.ind_on;
     if (all && polar_short_fused(c)) {
         // mixed path: the multipole real space does not feed the solve, so
@@ -1089,7 +1087,7 @@ int smd_profile_stages(smd_ctx *x, int reps, double *out) {
     out[3] = timed([&] { launch_nlist(c, true); });
     for (int q = 4; q < 10; q++) out[q] = 0.0;
     if (c.mp_on) {
-        out[4] = timed([&] { launch_frames(c); launch_pack_sites(c); launch_torques_begin(c); });
+        out[4] = timed([&] { launch_frames(c); });
         const bool fused = polar_short_fused(c);
         if (!fused) out[5] = timed([&] { launch_mp_short(c); });
         if (!c.ind_on) out[6] = timed([&] { launch_mp_long(c); });

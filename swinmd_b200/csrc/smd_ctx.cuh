@@ -184,10 +184,8 @@ bool polar_short_fused(const Ctx &c);
 void launch_polar_short(Ctx &c);
 void launch_ind_long(Ctx &c);
 void launch_polar_long(Ctx &c);
-void launch_torques_begin(Ctx &c);
 void launch_torques_end(Ctx &c);
 void launch_frames(Ctx &c);
-void launch_pack_sites(Ctx &c);
 void launch_buff(Ctx &c);
 int setup_cg(Ctx &c);
 int ensure_ind_rows(Ctx &c);

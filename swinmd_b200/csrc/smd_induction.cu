@@ -322,6 +322,7 @@ struct CGArgs {
     int nblocks, max_iter, guess;
     double tol;
     const double *blk;       // [nmol][81] inverse molecule blocks of A (molecule preconditioner)
+    float *srec;             // mixed path: site records (16 floats per site, p at 10..12), kept current
 };
 
 // fixed-order block sums, every block computes the same totals: each thread
@@ -617,15 +618,24 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
     const int passes = (n + sites_per_pass - 1) / sites_per_pass;
     unsigned int phase = 0;
     double tot[4];
+    // every write of a dipole component also goes to the site records, so
+    // that they hold the solution when the solve ends
+    auto put_p = [&](int i, int d, double v) {
+        a.p[d * n + i] = v;
+        if (c.srec) c.srec[16 * (size_t)i + 10 + d] = (float)v;
+    };
     // x0: M^-1 E0 (guess 0) or the dipoles already in p (previous step / learned)
     if (BJ) {
         for (int i = gtid; i < n; i += nthreads) c.al[i] = fmax(1e-8, a.polar[(int)a.pos4[i].w]);
         if (c.guess == 0) {
             mol_tiles<G4, GR>(a, c.blk, g0, s_bv, s_bu, [&](int, int, int, int idx) { return a.e0[idx]; },
-                              [&](int, int, int, int idx, double, double u) { a.p[idx] = u; });
+                              [&](int, int e, int i, int, double, double u) { put_p(i, e % 3, u); });
         } else {
-            for (int i = gtid; i < n; i += nthreads)
-                g0[i] = G4{(GR)a.p[i], (GR)a.p[n + i], (GR)a.p[2 * n + i], (GR)0};
+            for (int i = gtid; i < n; i += nthreads) {
+                const double p0 = a.p[i], p1 = a.p[n + i], p2 = a.p[2 * n + i];
+                g0[i] = G4{(GR)p0, (GR)p1, (GR)p2, (GR)0};
+                put_p(i, 0, p0); put_p(i, 1, p1); put_p(i, 2, p2);
+            }
         }
     } else {
         for (int i = gtid; i < n; i += nthreads) {
@@ -634,7 +644,7 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
             double p3[3];
             for (int d = 0; d < 3; d++) {
                 p3[d] = c.guess == 0 ? al * a.e0[d * n + i] : a.p[d * n + i];
-                if (c.guess == 0) a.p[d * n + i] = p3[d];
+                put_p(i, d, p3[d]);
             }
             g0[i] = G4{(GR)p3[0], (GR)p3[1], (GR)p3[2], (GR)0};
         }
@@ -696,13 +706,13 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
         vals[0] = 0; vals[1] = 0;
         if (BJ) {
             mol_tiles<G4, GR>(a, c.blk, g1, s_bv, s_bu,
-                              [&](int, int, int, int idx) {
+                              [&](int, int e, int i, int idx) {
                                   const double pd = __ldcg(&c.u[idx]) + (it ? beta * __ldcg(&c.v[idx]) : 0.0);
                                   const double sd = __ldcg(&c.z[idx]) + (it ? beta * __ldcg(&c.s[idx]) : 0.0);
                                   c.v[idx] = pd;
                                   c.s[idx] = sd;
                                   const double dp = alpha_cg * pd;
-                                  a.p[idx] = __ldcg(&a.p[idx]) + dp;
+                                  put_p(i, e % 3, __ldcg(&a.p[idx]) + dp);
                                   const double r = __ldcg(&c.r[idx]) - alpha_cg * sd;
                                   c.r[idx] = r;
                                   vals[1] += dp * dp;
@@ -723,7 +733,7 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
                     c.v[idx] = pd;
                     c.s[idx] = sd;
                     const double dp = alpha_cg * pd;
-                    a.p[idx] = __ldcg(&a.p[idx]) + dp;
+                    put_p(i, d, __ldcg(&a.p[idx]) + dp);
                     const double r = __ldcg(&c.r[idx]) - alpha_cg * sd;
                     c.r[idx] = r;
                     w3[d] = al * r;
@@ -1219,6 +1229,79 @@ __global__ void k_ind_mol(IndArgs a, long long *trq, long long *acc) {
     }
 }
 
+// Self and intramolecular corrections of both the multipole and the induced
+// terms after the fused real-space pass, three threads per molecule: thread
+// t takes the self terms of the molecule's sites t, t + 3, ... and its
+// site pairs (p < q, in row order) t, t + 3, ...  The terms are those of
+// k_mp_mol (Multipole self and intramolecular energies) and k_ind_mol
+// (induced self energy and torque, induced intramolecular energy); spread
+// over three threads, one molecule's chain of FP64 work is a third as long.
+constexpr int PM_TPM = 3;
+__global__ void __launch_bounds__(96) k_polar_mol(IndArgs a, long long *trq, long long *acc) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = g / PM_TPM, t = g - PM_TPM * m;
+    double e_mps = 0, e_mpi = 0, e_ps = 0, e_pi = 0;
+    if (m < a.nmol) {
+        const double a2 = a.alpha * a.alpha, a2pi = 2.0 * a.alpha / SQRT_PI_I;
+        const int s = a.mol_off[m], ns = a.mol_off[m + 1] - s;
+        for (int p = t; p < ns; p += PM_TPM) {
+            const int i = a.mol_atoms[s + p];
+            const double4 pi = a.pos4[i];
+            const double qi = a.tq[(int)pi.w] / SQC;
+            const V3 mi = ld3i(a.mu, a.n, i), pii = ld3i(a.p, a.n, i);
+            const Q6 Qi = ldqi(a.qd, a.n, i);
+            const double QiI = qtr(Qi), QiQi = qdd(Qi, Qi);
+            const double selfterm = qi * qi * a2pi + (dot(mi, mi) - 2 * qi * QiI) * 2 * a2pi * a2 / 3 +
+                                    (QiI * QiI + 2 * QiQi) * 4 * a2pi * a2 * a2 / 5;
+            e_mps += -0.5 * selfterm * COU;
+            e_ps += -dot(mi, pii) * a2pi * a2 / 3 * COU;
+            add_fix3_at(trq, a.n, i, crs(mi, pii), COU * (2.0 / 3.0) * a2pi * a2);
+        }
+        const int npair = ns * (ns - 1) / 2;
+        for (int k = t; k < npair; k += PM_TPM) {
+            int p = 0, rem = k;
+            while (rem >= ns - 1 - p) { rem -= ns - 1 - p; p++; }
+            const int q = p + 1 + rem;
+            const int i = a.mol_atoms[s + p], j = a.mol_atoms[s + q];
+            if (!is_excluded(i, j, a.excl_off, a.excl)) continue;
+            const double4 pi = a.pos4[i], pj = a.pos4[j];
+            const V3 r = mind(pi, pj, a.box);
+            const double r2 = dot(r, r);
+            const double qi = a.tq[(int)pi.w] / SQC, qj = a.tq[(int)pj.w] / SQC;
+            const V3 mi = ld3i(a.mu, a.n, i), mj = ld3i(a.mu, a.n, j);
+            const V3 pii = ld3i(a.p, a.n, i), pjj = ld3i(a.p, a.n, j);
+            const Q6 Qi = ldqi(a.qd, a.n, i), Qj = ldqi(a.qd, a.n, j);
+            double D[6];
+            dn_erf(r2, a.alpha, D);
+            // multipole: G . D of the permanent pair
+            MPPair<double, V3> P;
+            mp_invariants(qi, mi, Qi, qj, mj, Qj, r, P);
+            e_mpi += -(P.G[0] * D[0] + P.G[1] * D[1] + P.G[2] * D[2] + P.G[3] * D[3] + P.G[4] * D[4]) * COU;
+            // induced: the induced-permanent invariants of the pair
+            const V3 rji = -r;
+            const double pjr = dot(pjj, r), pirji = dot(pii, rji);
+            const double G1i = -qi * pjr - dot(mi, pjj);
+            const double G2i = -dot(mi, r) * pjr - 2.0 * dot(pjj, qv(Qi, r)) - pjr * qtr(Qi);
+            const double G3i = -pjr * dot(r, qv(Qi, r));
+            const double G1j = -qj * pirji - dot(mj, pii);
+            const double G2j = -dot(mj, rji) * pirji - 2.0 * dot(pii, qv(Qj, rji)) - pirji * qtr(Qj);
+            const double G3j = -pirji * dot(r, qv(Qj, r));
+            e_pi += -0.5 * ((G1i + G1j) * D[1] + (G2i + G2j) * D[2] + (G3i + G3j) * D[3]) * COU;
+        }
+    }
+    __shared__ double s_r[4][3];
+    const double v[4] = {warp_sum(e_mps), warp_sum(e_mpi), warp_sum(e_ps), warp_sum(e_pi)};
+    if ((threadIdx.x & 31) == 0)
+        for (int q = 0; q < 4; q++) s_r[q][threadIdx.x >> 5] = v[q];
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double tot = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += s_r[threadIdx.x][w];
+        const int slot[4] = {ACC_E_SELF, ACC_E_INTRA, ACC_E_POL_SELF, ACC_E_POL_INTRA};
+        atomicAdd((unsigned long long *)&acc[slot[threadIdx.x]], (unsigned long long)to_fix(tot, ACC_SCALE));
+    }
+}
+
 // ring of the last 4 steps' converged dipoles and permanent fields;
 // flags[2] counts the stored steps
 // Stores the step's dipoles and permanent field in ring slot flags[2] & 3.
@@ -1389,6 +1472,8 @@ void launch_ind_cg(Ctx &c) {
     g.guess = (c.cg_guess == SMD_GUESS_PREVIOUS || learned) ? 1 : 0;
     const bool bj = c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk;   // blocks built by launch_ind_field
     g.blk = c.cg_blk;
+    // the mixed path's site records take the dipoles inside the solve
+    g.srec = f32 && c.srec ? (float *)c.srec : nullptr;
     cudaMemsetAsync(c.cg_bar, 0, sizeof(unsigned int), c.stream);
     // cooperative launch: the runtime refuses it unless every block can be
     // resident at once, which the grid barrier relies on
@@ -1409,7 +1494,6 @@ void launch_ind_cg(Ctx &c) {
         cudaLaunchKernelEx(&cfg, k_ind_cg<false, true>, g);
     else
         cudaLaunchKernelEx(&cfg, k_ind_cg<false, false>, g);
-    launch_pack_sites(c);   // the mixed path's site records get the new dipoles
     // a time step stores its converged dipoles for the next steps' guess
     if (c.in_step && c.phist) {
         k_hist_push<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.pind, c.e0, c.phist, c.flags);
@@ -1470,8 +1554,7 @@ void launch_polar_short(Ctx &c) {
         k_polar_real_f<true><<<nb, 128, 0, c.stream>>>(A);
     else
         k_polar_real_f<false><<<nb, 128, 0, c.stream>>>(A);
-    launch_mp_mol(c);
-    k_ind_mol<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(A.ia, c.trq, c.acc);
+    k_polar_mol<<<(c.nmol * PM_TPM + 95) / 96, 96, 0, c.stream>>>(A.ia, c.trq, c.acc);
 }
 
 }  // namespace smd

@@ -232,25 +232,40 @@ __global__ void __launch_bounds__(MK_THREADS) k_rsk_partial_f(int n, int nk, con
 // fixed-order chunk sums; energies and long virial
 // ---------------------------------------------------------------------------
 // MODE 0 permanent, 1 induced, 2 both (permanent energy to slot_e, induced
-// to slot_e2); slot_e < 0: sums only
+// to slot_e2); slot_e < 0: sums only.  A block takes RR_K k with one thread
+// per (structure factor, k); its first warp forms the energies and virial.
+constexpr int RR_K = 32;
 template <int MODE>
-__global__ void k_rsk_reduce(int nk, int nch, const double *partial, const double *kcoef, const double *kvec,
-                             double alphaR4, double *sk, long long *acc, int slot_e, int slot_e2) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(6 * RR_K) k_rsk_reduce(int nk, int nch, const double *partial,
+                                                         const double *kcoef, const double *kvec, double alphaR4,
+                                                         double *sk, long long *acc, int slot_e, int slot_e2) {
+    __shared__ double s_s[6][RR_K];
+    const int q0 = MODE == 1 ? 4 : 0, q1 = MODE == 0 ? 4 : 6;
+    const int kl = threadIdx.x % RR_K, q = threadIdx.x / RR_K;
+    const int k = blockIdx.x * RR_K + kl;
+    // one thread per (structure factor, k): the chunk partials in a fixed order
+    if (k < nk && q >= q0 && q < q1) {
+        double t = 0;
+        for (int ch = 0; ch < nch; ch++) t += partial[((size_t)ch * 6 + q) * nk + k];
+        sk[(size_t)q * nk + k] = t;
+        s_s[q][kl] = t;
+    }
+    if (slot_e < 0) return;  // sums only (no energy or virial from this call)
+    __syncthreads();
+    if (threadIdx.x >= RR_K) return;
+    // the first warp: energy and virial of its k, then the block totals
     double ep = 0, ei = 0, vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
     if (k < nk) {
-        const int q0 = MODE == 1 ? 4 : 0, q1 = MODE == 0 ? 4 : 6;
-        for (int q = q0; q < q1; q++) {
-            double t = 0;
-            for (int ch = 0; ch < nch; ch++) t += partial[((size_t)ch * 6 + q) * nk + k];
-            sk[(size_t)q * nk + k] = t;
-        }
-        const double CqQ = sk[k], SqQ = sk[nk + k], Cm = sk[2 * (size_t)nk + k], Sm = sk[3 * (size_t)nk + k];
+        const double CqQ = MODE != 1 ? s_s[0][kl] : 0.0, SqQ = MODE != 1 ? s_s[1][kl] : 0.0;
+        const double Cm = MODE != 1 ? s_s[2][kl] : 0.0, Sm = MODE != 1 ? s_s[3][kl] : 0.0;
         const double c = kcoef[k];
         if (MODE != 1) ep = c * ((CqQ * CqQ + SqQ * SqQ) + 2 * (SqQ * Cm - CqQ * Sm) + (Cm * Cm + Sm * Sm)) * KE;
         if (MODE != 0) {
-            const double Cp = sk[4 * (size_t)nk + k], Sp = sk[5 * (size_t)nk + k];
-            ei = c * ((SqQ * Cp - CqQ * Sp) + (Cp * Cm + Sp * Sm)) * KE;
+            // the induced energy needs the permanent sums too: read them back
+            const double Cq = MODE == 1 ? sk[k] : CqQ, Sq = MODE == 1 ? sk[nk + k] : SqQ;
+            const double C2 = MODE == 1 ? sk[2 * (size_t)nk + k] : Cm, S2 = MODE == 1 ? sk[3 * (size_t)nk + k] : Sm;
+            const double Cp = s_s[4][kl], Sp = s_s[5][kl];
+            ei = c * ((Sq * Cp - Cq * Sp) + (Cp * C2 + Sp * S2)) * KE;
         }
         const double e = ep + ei;
         const double kx = kvec[k], ky = kvec[nk + k], kz = kvec[2 * nk + k];
@@ -259,26 +274,22 @@ __global__ void k_rsk_reduce(int nk, int nch, const double *partial, const doubl
         vxx = e - e * coeff * kx * kx; vyy = e - e * coeff * ky * ky; vzz = e - e * coeff * kz * kz;
         vxy = -e * coeff * kx * ky; vxz = -e * coeff * kx * kz; vyz = -e * coeff * ky * kz;
     }
-    if (slot_e < 0) return;  // sums only (no energy or virial from this call)
-    __shared__ double s_r[8][8];
     double v[8] = {ep + (MODE == 1 ? ei : 0.0), ei, vxx, vxy, vxz, vyy, vyz, vzz};
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int q = 0; q < 8; q++) {
-        double t = warp_sum(v[q]);
-        if (lane == 0) s_r[q][w] = t;
-    }
-    __syncthreads();
-    if (threadIdx.x < 8) {
-        if (threadIdx.x == 1 && MODE != 2) return;
-        double t = 0;
-        for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += s_r[threadIdx.x][q];
+#pragma unroll
+    for (int r = 0; r < 8; r++) v[r] = warp_sum(v[r]);
+    const int lane = threadIdx.x;
+    if (lane < 8) {
+        if (lane == 1 && MODE != 2) return;
+        double t = v[0];
+#pragma unroll
+        for (int r = 1; r < 8; r++)
+            if (lane == r) t = v[r];
         const int slots[8][2] = {{slot_e, -1}, {slot_e2, -1}, {ACC_LVIR + 0, -1},
                                  {ACC_LVIR + 1, ACC_LVIR + 3}, {ACC_LVIR + 2, ACC_LVIR + 6},
                                  {ACC_LVIR + 4, -1}, {ACC_LVIR + 5, ACC_LVIR + 7}, {ACC_LVIR + 8, -1}};
         const long long fx = to_fix(t, ACC_SCALE);
-        atomicAdd((unsigned long long *)&acc[slots[threadIdx.x][0]], (unsigned long long)fx);
-        if (slots[threadIdx.x][1] >= 0)
-            atomicAdd((unsigned long long *)&acc[slots[threadIdx.x][1]], (unsigned long long)fx);
+        atomicAdd((unsigned long long *)&acc[slots[lane][0]], (unsigned long long)fx);
+        if (slots[lane][1] >= 0) atomicAdd((unsigned long long *)&acc[slots[lane][1]], (unsigned long long)fx);
     }
 }
 
@@ -923,7 +934,7 @@ void sums(Ctx &c, int slot_e, int slot_e2 = -1) {
                                                                                c.rc.kvec, c.type_q, c.mu, c.qd,
                                                                                c.pind, B.partial);
     }
-    k_rsk_reduce<MODE><<<(nk + 255) / 256, 256, 0, c.stream>>>(nk, nch, B.partial, c.rc.kcoef, c.rc.kvec,
+    k_rsk_reduce<MODE><<<(nk + RR_K - 1) / RR_K, 6 * RR_K, 0, c.stream>>>(nk, nch, B.partial, c.rc.kcoef, c.rc.kvec,
                                                               1.0 / (4.0 * c.ew_alpha * c.ew_alpha), B.sk,
                                                               c.acc, slot_e, slot_e2);
 }

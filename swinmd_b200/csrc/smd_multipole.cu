@@ -41,9 +41,14 @@ __device__ __forceinline__ Q6 ldq(const double *a, int n, int i) {
 // from the lab x axis (lab y when |z.x| > 0.866); O takes z along the sum of
 // the unit O->H vectors and x from the unit O->H2 vector; then
 // u = x - (x.z) z normalised, v = z x u (Local2Global.cpp:100-150).
+// The same thread then writes the sites' FP32 records of the mixed path
+// (srec, when given) and clears their torque accumulators.  A record is one
+// 64-byte row per site, so that a pair kernel gathers a partner's charge and
+// multipoles with four vector loads: (q, mu), (Qxx, Qxy, Qxz, Qyy),
+// (Qyz, Qzz, px, py), (pz, 0, 0, 0); the dipole solve rewrites p.
 __global__ void k_frames(int nmol, int n, const int *mol_off, const int *mol_atoms,
                          const double4 *pos4, const double *type_mp, double *mu, double *qd,
-                         double *frame) {
+                         double *frame, const double *tq, const double *pind, float4 *srec, long long *trq) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= nmol) return;
     const int s = mol_off[m];
@@ -97,34 +102,27 @@ __global__ void k_frames(int nmol, int n, const int *mol_off, const int *mol_ato
         qd[3 * n + id] = G[1][1];
         qd[4 * n + id] = G[1][2];
         qd[5 * n + id] = G[2][2];
+        if (srec) {
+            float4 *o = srec + 4 * (size_t)id;
+            o[0] = make_float4((float)(tq[(int)pos4[id].w] / SQRTCOULOMB), (float)mu[id], (float)mu[n + id],
+                               (float)mu[2 * n + id]);
+            o[1] = make_float4((float)G[0][0], (float)G[0][1], (float)G[0][2], (float)G[1][1]);
+            o[2] = make_float4((float)G[1][2], (float)G[2][2], (float)pind[id], (float)pind[n + id]);
+            o[3] = make_float4((float)pind[2 * n + id], 0.f, 0.f, 0.f);
+        }
+        trq[id] = 0;
+        trq[n + id] = 0;
+        trq[2 * n + id] = 0;
     }
 }
 
+// local frames, lab-frame multipoles, the mixed path's site records and
+// cleared torques in one launch (every multipole molecule is an H O H triple)
 void launch_frames(Ctx &c) {
+    float4 *srec = c.precision == SMD_PREC_MIXED ? c.srec : nullptr;
     k_frames<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.n, c.mol_off, c.mol_atoms, c.pos4,
-                                                         c.type_mp, c.mu, c.qd, c.frame);
-}
-
-// FP32 site records of the mixed path, one 64-byte row per site, so that a
-// pair kernel gathers a partner's charge and multipoles with four vector
-// loads: (q, mu), (Qxx, Qxy, Qxz, Qyy), (Qyz, Qzz, px, py), (pz, 0, 0, 0)
-__global__ void k_pack_sites(int n, const double4 *pos4, const double *tq, const double *mu, const double *qd,
-                             const double *pind, float4 *srec) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const size_t N = (size_t)n;
-    float4 *o = srec + 4 * (size_t)i;
-    o[0] = make_float4((float)(tq[(int)pos4[i].w] / SQRTCOULOMB), (float)mu[i], (float)mu[N + i],
-                       (float)mu[2 * N + i]);
-    o[1] = make_float4((float)qd[i], (float)qd[N + i], (float)qd[2 * N + i], (float)qd[3 * N + i]);
-    o[2] = make_float4((float)qd[4 * N + i], (float)qd[5 * N + i], (float)pind[i], (float)pind[N + i]);
-    o[3] = make_float4((float)pind[2 * N + i], 0.f, 0.f, 0.f);
-}
-
-// after the frames (permanent multipoles) and after the dipole solve (p)
-void launch_pack_sites(Ctx &c) {
-    if (c.precision != SMD_PREC_MIXED || !c.srec) return;
-    k_pack_sites<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.pos4, c.type_q, c.mu, c.qd, c.pind, c.srec);
+                                                         c.type_mp, c.mu, c.qd, c.frame, c.type_q, c.pind, srec,
+                                                         c.trq);
 }
 
 // ---------------------------------------------------------------------------
@@ -385,10 +383,6 @@ __global__ void k_torque2force(int nmol, int n, const int *mol_off, const int *m
     add_fix3(frc, n, h1, fh1, 1.0);
     add_fix3(frc, n, o, fo, 1.0);
     add_fix3(frc, n, h2, fh2, 1.0);
-}
-
-void launch_torques_begin(Ctx &c) {
-    cudaMemsetAsync(c.trq, 0, 3 * (size_t)c.n * sizeof(long long), c.stream);
 }
 
 void launch_torques_end(Ctx &c) {
