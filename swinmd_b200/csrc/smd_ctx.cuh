@@ -193,6 +193,9 @@ int ensure_ind_rows(Ctx &c);
 int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed);
 void launch_mlp_guess(Ctx &c);
 void launch_blk_response(Ctx &c, double *out);
+// first-order part of the learned guess: the solver's s slot of its work
+// area, which the solve writes before it first reads it
+inline double *guess_response(Ctx &c) { return c.cgw + 20 * (size_t)c.n; }
 void launch_mlp_features(Ctx &c);
 void launch_mlp_collect(Ctx &c);
 void launch_mlp_norm(Ctx &c);

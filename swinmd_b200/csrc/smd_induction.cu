@@ -457,10 +457,15 @@ __device__ V3 amul(const CGArgs &c, int i, int t, const G4 *g) {
 // stored entry-major over molecules (entry e of molecule m at e * nmol + m),
 // so that the solve's loads of one entry coalesce.
 constexpr int MB_MOLS = 32;
+// With dl given, the same threads also form the blocks' response to the
+// change of the permanent field since the last stored step,
+// dl = M_m^-1 (E0(t) - E0(t-1)) (M_m^-1 E0 when none is stored), the first-order
+// part of the learned guess (as k_blk_response does from the stored blocks).
 template <typename TS>
-__global__ void __launch_bounds__(9 * MB_MOLS) k_mol_blocks(int nmol, const int *mol_off, const int *mol_atoms,
+__global__ void __launch_bounds__(9 * MB_MOLS) k_mol_blocks(int n, int nmol, const int *mol_off, const int *mol_atoms,
                                                             TRows R, const double *polar, const double4 *pos4,
-                                                            double *blk) {
+                                                            double *blk, const double *e0, const double *ph,
+                                                            const int *flags, double *dl) {
     using TS4 = typename std::conditional<sizeof(TS) == 4, float4, double4>::type;
     __shared__ double s_piv[MB_MOLS][9];
     __shared__ int s_bad[MB_MOLS];
@@ -529,15 +534,32 @@ __global__ void __launch_bounds__(9 * MB_MOLS) k_mol_blocks(int nmol, const int 
         }
     }
     __syncthreads();
-    if (act) {
-        const int nd = 3 * ns;
-        const bool bad = s_bad[lm] != 0;
+    const int nd = 3 * ns;
+    const bool bad = act && s_bad[lm] != 0;
 #pragma unroll
-        for (int c = 0; c < 9; c++) {
-            double out = row[c];
-            if (bad) out = (r == c && r < nd) ? al : 0.0;
-            if (r >= nd || c >= nd) out = 0.0;
-            blk[(size_t)(r * 9 + c) * nmol + m] = out;
+    for (int c = 0; c < 9; c++) {
+        if (bad) row[c] = (r == c && r < nd) ? al : 0.0;
+        if (r >= nd || c >= nd) row[c] = 0.0;
+    }
+    if (act) {
+#pragma unroll
+        for (int c = 0; c < 9; c++) blk[(size_t)(r * 9 + c) * nmol + m] = row[c];
+    }
+    if (dl) {
+        __shared__ double s_de[MB_MOLS][9];
+        const int cnt = flags[2];
+        double de = 0.0;
+        if (i >= 0) {
+            const size_t idx = (size_t)x * n + i;
+            de = e0[idx] - (cnt >= 1 ? ph[(size_t)((cnt - 1) & 3) * 6 * n + 3 * (size_t)n + idx] : 0.0);
+        }
+        s_de[lm][r] = de;
+        __syncthreads();
+        if (i >= 0) {
+            double u = 0.0;
+#pragma unroll
+            for (int c = 0; c < 9; c++) u += row[c] * s_de[lm][c];
+            dl[(size_t)x * n + i] = u;
         }
     }
 }
@@ -1397,16 +1419,20 @@ void launch_ind_field(Ctx &c) {
     else
         k_ind_field<double><<<nb, 256, 0, c.stream>>>(a, R, c.status);
     // the preconditioner's inverse molecule blocks (they need this step's tensor rows)
+    const bool learned = c.cg_guess == SMD_GUESS_LEARNED && c.mlp_ready;
     if (c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk) {
+        // with the learned guess, also its first-order part
+        double *dl = learned ? guess_response(c) : nullptr;
         const int nbm = (c.nmol + MB_MOLS - 1) / MB_MOLS;
         if (f32)
-            k_mol_blocks<float><<<nbm, 9 * MB_MOLS, 0, c.stream>>>(c.nmol, c.mol_off, c.mol_atoms, R, c.type_polar,
-                                                                   c.pos4, c.cg_blk);
+            k_mol_blocks<float><<<nbm, 9 * MB_MOLS, 0, c.stream>>>(c.n, c.nmol, c.mol_off, c.mol_atoms, R,
+                                                                   c.type_polar, c.pos4, c.cg_blk, c.e0, c.phist,
+                                                                   c.flags, dl);
         else
-            k_mol_blocks<double><<<nbm, 9 * MB_MOLS, 0, c.stream>>>(c.nmol, c.mol_off, c.mol_atoms, R, c.type_polar,
-                                                                    c.pos4, c.cg_blk);
+            k_mol_blocks<double><<<nbm, 9 * MB_MOLS, 0, c.stream>>>(c.n, c.nmol, c.mol_off, c.mol_atoms, R,
+                                                                    c.type_polar, c.pos4, c.cg_blk, c.e0, c.phist,
+                                                                    c.flags, dl);
     }
-    const bool learned = c.cg_guess == SMD_GUESS_LEARNED && c.mlp_ready;
     if (learned) launch_mlp_guess(c);  // writes the start dipoles into p
 }
 

@@ -326,13 +326,10 @@ void launch_mlp_features(Ctx &c) {
                                                             c.e0, c.phist, c.flags, c.mlp_x);
 }
 
-// the first-order response goes to the solver's s slot of its work area,
-// which the solve writes before it first reads it
-static double *response_scratch(Ctx &c) { return c.cgw + 20 * (size_t)c.n; }
-
 void launch_mlp_guess(Ctx &c) {
-    double *dl = response_scratch(c);
-    launch_blk_response(c, dl);
+    double *dl = guess_response(c);
+    // with the molecule blocks the block kernel has just formed it
+    if (!(c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk)) launch_blk_response(c, dl);
     k_mlp_infer<<<(c.n + MLP_ISITES - 1) / MLP_ISITES, MLP_IBLOCK, 0, c.stream>>>(
         c.n, c.mol, c.mol_off, c.mol_atoms, c.pos4, c.e0, c.mlp_norm, c.mlp_w, c.frame, dl, c.phist, c.flags,
         c.pind);
@@ -375,7 +372,7 @@ int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed) {
 
 void launch_mlp_collect(Ctx &c) {
     launch_mlp_features(c);
-    double *dl = response_scratch(c);
+    double *dl = guess_response(c);
     launch_blk_response(c, dl);   // the blocks of the solve that produced p
     k_mlp_collect<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.mlp_x, c.frame, c.pind, dl, c.phist, c.flags,
                                                            c.mlp_data, c.mlp_rows);

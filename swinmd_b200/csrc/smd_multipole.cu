@@ -41,38 +41,43 @@ __device__ __forceinline__ Q6 ldq(const double *a, int n, int i) {
 // from the lab x axis (lab y when |z.x| > 0.866); O takes z along the sum of
 // the unit O->H vectors and x from the unit O->H2 vector; then
 // u = x - (x.z) z normalised, v = z x u (Local2Global.cpp:100-150).
-// The same thread then writes the sites' FP32 records of the mixed path
-// (srec, when given) and clears their torque accumulators.  A record is one
+// One thread per site (thread q of a molecule takes site q), which then
+// writes the site's FP32 record of the mixed path (srec, when given) and
+// clears its torque accumulators.  A record is one
 // 64-byte row per site, so that a pair kernel gathers a partner's charge and
 // multipoles with four vector loads: (q, mu), (Qxx, Qxy, Qxz, Qyy),
 // (Qyz, Qzz, px, py), (pz, 0, 0, 0); the dipole solve rewrites p.
 __global__ void k_frames(int nmol, int n, const int *mol_off, const int *mol_atoms,
                          const double4 *pos4, const double *type_mp, double *mu, double *qd,
                          double *frame, const double *tq, const double *pind, float4 *srec, long long *trq) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = g / 3, q = g - 3 * m;
     if (m >= nmol) return;
     const int s = mol_off[m];
     if (mol_off[m + 1] - s != 3) return;
     const int ih1 = mol_atoms[s], io = mol_atoms[s + 1], ih2 = mol_atoms[s + 2];
     const double4 a = pos4[ih1], b = pos4[io], c = pos4[ih2];
     const V3 rh1 = v3(a.x, a.y, a.z), ro = v3(b.x, b.y, b.z), rh2 = v3(c.x, c.y, c.z);
-    V3 p1[3], p2[3];
-    p1[0] = ro - rh1;
-    p2[0] = fabs(p1[0].x / len(p1[0])) > 0.8660 ? v3(0, 1, 0) : v3(1, 0, 0);
-    V3 t1 = rh1 - ro, t2 = rh2 - ro;
-    t1 = (1.0 / len(t1)) * t1;
-    t2 = (1.0 / len(t2)) * t2;
-    p1[1] = t1 + t2;
-    p2[1] = t2;
-    p1[2] = ro - rh2;
-    p2[2] = fabs(p1[2].x / len(p1[2])) > 0.8660 ? v3(0, 1, 0) : v3(1, 0, 0);
-    const int ids[3] = {ih1, io, ih2};
-    for (int q = 0; q < 3; q++) {
-        const V3 w = (1.0 / len(p1[q])) * p1[q];
-        const V3 ss = p2[q] - dot(p2[q], w) * w;
+    V3 p1, p2;
+    if (q == 0) {
+        p1 = ro - rh1;
+        p2 = fabs(p1.x / len(p1)) > 0.8660 ? v3(0, 1, 0) : v3(1, 0, 0);
+    } else if (q == 1) {
+        V3 t1 = rh1 - ro, t2 = rh2 - ro;
+        t1 = (1.0 / len(t1)) * t1;
+        t2 = (1.0 / len(t2)) * t2;
+        p1 = t1 + t2;
+        p2 = t2;
+    } else {
+        p1 = ro - rh2;
+        p2 = fabs(p1.x / len(p1)) > 0.8660 ? v3(0, 1, 0) : v3(1, 0, 0);
+    }
+    {
+        const V3 w = (1.0 / len(p1)) * p1;
+        const V3 ss = p2 - dot(p2, w) * w;
         const V3 u = (1.0 / len(ss)) * ss;
         const V3 v = crs(w, u);
-        const int id = ids[q];
+        const int id = q == 0 ? ih1 : (q == 1 ? io : ih2);
         if (frame) {  // axes u, v, w per site, for the dipole-guess network
             const double ax[9] = {u.x, u.y, u.z, v.x, v.y, v.z, w.x, w.y, w.z};
             for (int d = 0; d < 9; d++) frame[(size_t)d * n + id] = ax[d];
@@ -120,7 +125,7 @@ __global__ void k_frames(int nmol, int n, const int *mol_off, const int *mol_ato
 // cleared torques in one launch (every multipole molecule is an H O H triple)
 void launch_frames(Ctx &c) {
     float4 *srec = c.precision == SMD_PREC_MIXED ? c.srec : nullptr;
-    k_frames<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.n, c.mol_off, c.mol_atoms, c.pos4,
+    k_frames<<<(3 * c.nmol + 95) / 96, 96, 0, c.stream>>>(c.nmol, c.n, c.mol_off, c.mol_atoms, c.pos4,
                                                          c.type_mp, c.mu, c.qd, c.frame, c.type_q, c.pind, srec,
                                                          c.trq);
 }
@@ -334,9 +339,13 @@ __global__ void k_mp_mol(int nmol, int n, const int *mol_off, const int *mol_ato
 // ---------------------------------------------------------------------------
 // torques -> forces on the H O H sites (Multipole::torques2forces)
 // ---------------------------------------------------------------------------
+// One thread per site: thread q of a molecule maps site q's torque and adds
+// the forces on the molecule's sites atomically (integer adds, so the sum
+// does not depend on their order).
 __global__ void k_torque2force(int nmol, int n, const int *mol_off, const int *mol_atoms,
                                const double4 *pos4, const long long *trq, long long *frc) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = g / 3, q = g - 3 * m;
     if (m >= nmol) return;
     const int s = mol_off[m];
     if (mol_off[m + 1] - s != 3) return;
@@ -362,8 +371,8 @@ __global__ void k_torque2force(int nmol, int n, const int *mol_off, const int *m
         fh = fh - dUdu;
         fo = fo + dUdu;
     };
-    hsite(rh1, tq(h1), fh1);
-    {   // O site: u = O - H1, v = O - H2, half weight on the w rotation
+    if (q == 0) hsite(rh1, tq(h1), fh1);
+    if (q == 1) {   // O site: u = O - H1, v = O - H2, half weight on the w rotation
         const V3 tau = tq(o);
         V3 u = ro - rh1, v = ro - rh2;
         V3 w = crs(u, v);
@@ -379,14 +388,14 @@ __global__ void k_torque2force(int nmol, int n, const int *mol_off, const int *m
         fh1 = fh1 + dUdu;
         fh2 = fh2 + dUdv;
     }
-    hsite(rh2, tq(h2), fh2);
-    add_fix3(frc, n, h1, fh1, 1.0);
-    add_fix3(frc, n, o, fo, 1.0);
-    add_fix3(frc, n, h2, fh2, 1.0);
+    if (q == 2) hsite(rh2, tq(h2), fh2);
+    if (q != 2) add_fix3_at(frc, n, h1, fh1, 1.0);
+    add_fix3_at(frc, n, o, fo, 1.0);
+    if (q != 0) add_fix3_at(frc, n, h2, fh2, 1.0);
 }
 
 void launch_torques_end(Ctx &c) {
-    k_torque2force<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.n, c.mol_off, c.mol_atoms,
+    k_torque2force<<<(3 * c.nmol + 95) / 96, 96, 0, c.stream>>>(c.nmol, c.n, c.mol_off, c.mol_atoms,
                                                                 c.pos4, c.trq, c.frc);
 }
 
