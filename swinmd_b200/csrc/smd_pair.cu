@@ -626,47 +626,52 @@ __global__ void k_fixq(int n, const double4 *pos4, int4 *fixq, Box b) {
 // Virtual sites of the buffered 14-7 term (BuffvdWForce::VirtualPositions,
 // src/forces/BuffvdWForce.cpp:358-385): a type-0 (H) site moves to
 // f r_H + (1 - f) r_O, with O the molecule's second site; others stay.
-__global__ void k_virtual(int nmol, const int *mol_off, const int *mol_atoms, const double4 *pos4,
+__global__ void k_virtual(int n, const int *mol, const int *mol_off, const int *mol_atoms, const double4 *pos4,
                           double f, Box b, double4 *vpos4, int4 *vfixq) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= nmol) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int m = mol[i];
     const int s = mol_off[m], e = mol_off[m + 1];
-    const double4 po = pos4[mol_atoms[s + (e - s > 1 ? 1 : 0)]];
-    for (int k = s; k < e; k++) {
-        const int i = mol_atoms[k];
-        double4 p = pos4[i];
-        if ((int)p.w == 0 && e - s > 1) {
-            p.x = f * p.x + (1.0 - f) * po.x;
-            p.y = f * p.y + (1.0 - f) * po.y;
-            p.z = f * p.z + (1.0 - f) * po.z;
-        }
-        vpos4[i] = p;
-        vfixq[i] = make_int4(frac32(p.x, b.inv[0]), frac32(p.y, b.inv[1]), frac32(p.z, b.inv[2]), (int)p.w);
+    double4 p = pos4[i];
+    if ((int)p.w == 0 && e - s > 1) {
+        const double4 po = pos4[mol_atoms[s + 1]];
+        p.x = f * p.x + (1.0 - f) * po.x;
+        p.y = f * p.y + (1.0 - f) * po.y;
+        p.z = f * p.z + (1.0 - f) * po.z;
     }
+    vpos4[i] = p;
+    vfixq[i] = make_int4(frac32(p.x, b.inv[0]), frac32(p.y, b.inv[1]), frac32(p.z, b.inv[2]), (int)p.w);
 }
 
 // Force on a virtual H site: f on H, (1 - f) on the molecule's O
-// (BuffvdWForce.cpp:257-274).  Writes the molecule's forces (first term).
-__global__ void k_buff_distribute(int nmol, int n, const int *mol_off, const int *mol_atoms,
+// (BuffvdWForce.cpp:257-274).  Writes the sites' forces (first term), one
+// thread per site: the O site also gathers the (1 - f) shares of its
+// molecule's H sites, in site order.
+__global__ void k_buff_distribute(int n, const int *mol, const int *mol_off, const int *mol_atoms,
                                   const double4 *pos4, double f, const long long *fv, long long *frc) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= nmol) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int m = mol[i];
     const int s = mol_off[m], e = mol_off[m + 1];
-    const int o = mol_atoms[s + (e - s > 1 ? 1 : 0)];
-    double acc[3] = {0, 0, 0};
-    for (int k = s; k < e; k++) {
-        const int i = mol_atoms[k];
-        if ((int)pos4[i].w == 0 && e - s > 1) {
-            for (int d = 0; d < 3; d++) {
-                const double v = (double)fv[d * n + i] * FRC_INV;
-                frc[d * n + i] = to_fix(f * v, FRC_SCALE);
-                acc[d] += (1.0 - f) * v;
-            }
-        } else {
-            for (int d = 0; d < 3; d++) frc[d * n + i] = fv[d * n + i];
-        }
+    const bool multi = e - s > 1;
+    const int o = mol_atoms[s + (multi ? 1 : 0)];
+    long long out[3];
+    if ((int)pos4[i].w == 0 && multi) {
+        for (int d = 0; d < 3; d++) out[d] = to_fix(f * ((double)fv[d * n + i] * FRC_INV), FRC_SCALE);
+    } else {
+        for (int d = 0; d < 3; d++) out[d] = fv[d * n + i];
     }
-    for (int d = 0; d < 3; d++) frc[d * n + o] += to_fix(acc[d], FRC_SCALE);
+    if (i == o) {
+        double acc[3] = {0, 0, 0};
+        if (multi)
+            for (int k = s; k < e; k++) {
+                const int j = mol_atoms[k];
+                if ((int)pos4[j].w == 0)
+                    for (int d = 0; d < 3; d++) acc[d] += (1.0 - f) * ((double)fv[d * n + j] * FRC_INV);
+            }
+        for (int d = 0; d < 3; d++) out[d] += to_fix(acc[d], FRC_SCALE);
+    }
+    for (int d = 0; d < 3; d++) frc[d * n + i] = out[d];
 }
 
 void launch_fixq(Ctx &c) {
@@ -704,8 +709,8 @@ void launch_pair(Ctx &c) {
     if (buff) {
         // the pair term acts between the virtual sites; their forces are
         // handed to the real sites afterwards
-        k_virtual<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.mol_off, c.mol_atoms, c.pos4,
-                                                               c.buff_h, c.box, c.vpos4, c.vfixq);
+        k_virtual<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.mol, c.mol_off, c.mol_atoms, c.pos4, c.buff_h,
+                                                            c.box, c.vpos4, c.vfixq);
         a.pos4 = c.vpos4;
         a.fixq = c.vfixq;
         a.frc = c.fv;
@@ -726,8 +731,8 @@ void launch_pair(Ctx &c) {
         else dispatch_vdw<double, false>(c, a);
     }
     if (buff)
-        k_buff_distribute<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.n, c.mol_off, c.mol_atoms,
-                                                                       c.pos4, c.buff_h, c.fv, c.frc);
+        k_buff_distribute<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.mol, c.mol_off, c.mol_atoms, c.pos4,
+                                                                    c.buff_h, c.fv, c.frc);
 }
 
 }  // namespace smd
