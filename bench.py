@@ -547,7 +547,14 @@ def main():
                             "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                             "frac": achieved / fp32_peak if achieved else None,
                             "alg_flops_per_step": flops, "k_vectors": nk,
-                            "traffic": None,
+                            # DRAM bytes of one launch of each pass on this workload, from one ncu
+                            # capture (dram__bytes_read.sum + dram__bytes_write.sum: 6.45 + 0 MB
+                            # and 3.17 + 0 MB); the passes read their tables from L2 and shared
+                            # memory, so they are not bound by HBM
+                            "traffic": (6.45e6 + 3.17e6) if polar else None,
+                            "traffic_unit": "bytes per step (both passes)",
+                            "traffic_source": "ncu --set full capture of the polwater4096 step "
+                                              "(profiles/polwater4096_top_kernels.md)",
                             "peak_source": "nominal FP32 SIMT rate at sm_max_mhz of MEASURED_PEAKS.json "
                                            f"({peak_src}); the file's HBM copy and bf16 GEMM rates do not "
                                            "bound these kernels",
