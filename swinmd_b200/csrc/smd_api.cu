@@ -99,6 +99,7 @@ int alloc_list(smd_ctx *x) {
         c.pl.cell_cap = ncell;
     }
     c.list_valid = 0;
+    c.list_built = 0;
     c.graph_dirty = 1;
     if (ensure_ind_rows(c)) return fail(x, SMD_ERR_CUDA, "dipole-solve tensor rows: allocation failed");
     return SMD_OK;
@@ -232,7 +233,8 @@ void smd_destroy(smd_ctx *x) {
                     c.pl.cell_count, c.pl.cell_start, c.pl.cell_atoms, c.rc.kn, c.rc.kcoef,
                     c.rc.sk, c.rc.kvec, c.clen2, c.type_mp, c.type_polar, c.mu, c.qd, c.trq, c.e0,
                     c.pind, c.cgw, c.cgs, c.cg_bar, c.vpos4, c.vfixq, c.fv, c.ind_rj, c.ind_rc, c.ind_cnt,
-                    c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab, c.srec, c.phist, c.cg_blk};
+                    c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab, c.srec, c.phist, c.cg_blk,
+                    c.upload4};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -321,6 +323,7 @@ int smd_set_topology(smd_ctx *x, int n, int ntypes, const int32_t *atom_type,
     CK(dalloc(&c.pair_par, (size_t)ntypes * ntypes * 4));
     CK(cudaMemset(c.pair_par, 0, (size_t)ntypes * ntypes * 4 * sizeof(double)));
     c.list_valid = 0;
+    c.list_built = 0;
     c.graph_dirty = 1;
     return alloc_list(x);
 }
@@ -342,6 +345,7 @@ int smd_set_exclusions(smd_ctx *x, const int32_t *offsets, const int32_t *partne
     CK(cudaMemcpy(c.excl_off, offsets, (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
     if (tot) CK(cudaMemcpy(c.excl, partners, tot * sizeof(int), cudaMemcpyHostToDevice));
     c.list_valid = 0;
+    c.list_built = 0;
     c.graph_dirty = 1;
     if (ensure_ind_rows(c)) return fail(x, SMD_ERR_CUDA, "dipole-solve tensor rows: allocation failed");
     return SMD_OK;
@@ -732,13 +736,22 @@ int smd_upload_positions(smd_ctx *x, const double *pos) {
     std::vector<double4> p(c.n);
     for (int i = 0; i < c.n; i++)
         p[i] = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], (double)c.h_type[i]);
-    CK(cudaMemcpyAsync(c.pos4, p.data(), c.n * sizeof(double4), cudaMemcpyHostToDevice, c.stream));
-    CK(cudaMemsetAsync(c.disp4, 0, c.n * sizeof(double4), c.stream));
-    int one = 1;  // the next step rebuilds the pair list from these positions
-    CK(cudaMemcpyAsync(c.flags, &one, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+    if (c.list_built && c.ip.strain_rate == 0.0) {
+        // the list stays valid while every site has moved less than half the
+        // skin since the last rebuild: the upload adds each site's minimum-image
+        // displacement and raises the rebuild flag past that, as a step does
+        if (!c.upload4) CK(dalloc(&c.upload4, c.n));
+        CK(cudaMemcpyAsync(c.upload4, p.data(), c.n * sizeof(double4), cudaMemcpyHostToDevice, c.stream));
+        launch_upload_positions(c);
+    } else {
+        CK(cudaMemcpyAsync(c.pos4, p.data(), c.n * sizeof(double4), cudaMemcpyHostToDevice, c.stream));
+        CK(cudaMemsetAsync(c.disp4, 0, c.n * sizeof(double4), c.stream));
+        int one = 1;  // the next step rebuilds the pair list from these positions
+        CK(cudaMemcpyAsync(c.flags, &one, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+    }
     launch_fixq(c);
     CK(cudaStreamSynchronize(c.stream));
-    c.list_valid = 0;
+    c.list_valid = 0;   // smd_get_pairs builds a fresh list from these positions
     return SMD_OK;
 }
 

@@ -155,6 +155,8 @@ struct Ctx {
     int nb_blocks = 0;              // blocks of the integrate kernel
     long long steps_done = 0;
     int list_valid = 0;
+    int list_built = 0;      // a pair list exists for the current set-up (its sites may have moved within the skin)
+    double4 *upload4 = nullptr;  // staging of uploaded positions
     // CUDA graph of one step
     cudaGraphExec_t step_graph = nullptr;
     int graph_dirty = 1;
@@ -162,6 +164,7 @@ struct Ctx {
 
 // launchers (each enqueues on ctx.stream)
 void launch_fixq(Ctx &c);
+void launch_upload_positions(Ctx &c);
 void launch_nlist(Ctx &c, bool force_rebuild);
 void launch_pair(Ctx &c);
 void launch_recip(Ctx &c);

@@ -447,6 +447,28 @@ __global__ void __launch_bounds__(INT_BLOCK) k_integrate(IntArgs a) {
     if (threadIdx.x < ACC_COUNT) a.acc[threadIdx.x] = 0;
 }
 
+// Uploaded positions (staged in upload4, type in w) replace pos4; each
+// site's minimum-image displacement adds to its displacement since the last
+// list rebuild, and the rebuild flag is raised past half the skin.
+__global__ void k_upload_positions(int n, const double4 *np, double4 *pos4, double4 *disp4, Box b, double drmax,
+                                   int *flags) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 o = pos4[i], p = np[i];
+    double4 d = disp4[i];
+    d.x += pbc1(p.x - o.x, b.L[0], b.half[0]);
+    d.y += pbc1(p.y - o.y, b.L[1], b.half[1]);
+    d.z += pbc1(p.z - o.z, b.L[2], b.half[2]);
+    disp4[i] = d;
+    pos4[i] = p;
+    if (d.x * d.x + d.y * d.y + d.z * d.z > drmax) atomicOr(&flags[0], 1);
+}
+
+void launch_upload_positions(Ctx &c) {
+    k_upload_positions<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.upload4, c.pos4, c.disp4, c.box,
+                                                               c.pl.drmax, c.flags);
+}
+
 void launch_integrate(Ctx &c) {
     IntArgs a;
     a.n = c.n; a.nmol = c.nmol;

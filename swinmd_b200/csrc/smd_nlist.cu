@@ -339,6 +339,7 @@ void launch_nlist(Ctx &c, bool force_rebuild) {
     if (force_rebuild) {
         int one = 1;
         cudaMemcpyAsync(c.flags, &one, sizeof(int), cudaMemcpyHostToDevice, c.stream);
+        c.list_built = 1;
     }
     const int T = 256;
     int nb = (c.n + T - 1) / T;

@@ -73,3 +73,23 @@ def test_leapfrog_nose_hoover_trajectory():
     assert o.step == 20
     p_ref = g["r_step_atompressure"].reshape(-1, 9)[-1]
     assert np.allclose(np.array(o.atom_pressure), p_ref, rtol=1e-8, atol=1e-6)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_upload_within_skin_keeps_the_list(precision):
+    """Uploading positions that moved less than half the skin since the last
+    rebuild keeps the pair list (the displacement test decides, as in a step):
+    a run interrupted by a download and upload of the same positions matches
+    an uninterrupted one bit for bit, with no extra rebuild."""
+    runs = []
+    for upload in (False, True):
+        ens = engine.GpuEnsemble(_sys(), precision=precision)
+        lf = engine.LFIntegrator(ens)
+        lf.start()
+        lf.run(10)
+        if upload:
+            ens.upload_positions(ens.state()["pos"])
+        lf.run(10)
+        runs.append((ens.state()["pos"].copy(), lf.observables().list_updates))
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert runs[0][1] == runs[1][1]
