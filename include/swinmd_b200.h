@@ -230,6 +230,10 @@ int smd_set_precision(smd_ctx *ctx, int mode);
 int smd_set_tuning(smd_ctx *ctx, int threads_per_site);
 
 /* ---- state ------------------------------------------------------------ */
+/* Positions pos[3 n].  Once a pair list exists (and without shear), the list
+ * is kept while every site stays within half the skin of where it was at the
+ * last rebuild, minimum image, the same test a step makes; otherwise the next
+ * step rebuilds it. */
 int smd_upload_positions(smd_ctx *ctx, const double *pos);
 /* vel: Atom::velocity; vtminus may be NULL (then set by smd_integrator_start) */
 int smd_upload_velocities(smd_ctx *ctx, const double *vel, const double *vtminus);
