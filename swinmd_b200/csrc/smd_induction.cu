@@ -290,7 +290,7 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned int *p) {
     return v;
 }
 __device__ bool grid_barrier(unsigned int *bar, unsigned int target, unsigned int *status) {
-    __shared__ int s_ok;   // thread 0's verdict: every thread of the block takes the same branch
+    __shared__ int s_ok;   // thread 0's outcome: every thread of the block takes the same branch
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
