@@ -514,7 +514,7 @@ int smd_set_multipole(smd_ctx *x, const double *type_mp, const double *polar, do
     CK(dalloc(&c.cg_bar, 1));
     if (c.ind_on) {
         CK(dalloc(&c.phist, 24 * n));
-        CK(cudaMemset(c.flags + 2, 0, sizeof(int)));
+        CK(cudaMemset(c.flags + 2, 0, 2 * sizeof(int)));
     }
     if (ensure_ind_rows(c)) return fail(x, SMD_ERR_CUDA, "smd_set_multipole: tensor rows: allocation failed");
     r = setup_recip(c);
@@ -1018,7 +1018,7 @@ int smd_integrator_start(smd_ctx *x) {
     CK(cudaMemsetAsync(c.ticket, 0, sizeof(unsigned), c.stream));
     // the dipole history of the guess starts afresh (uploads keep it: the
     // solve converges to its tolerance from any start)
-    CK(cudaMemsetAsync(c.flags + 2, 0, sizeof(int), c.stream));
+    CK(cudaMemsetAsync(c.flags + 2, 0, 2 * sizeof(int), c.stream));   // step count and the push's ticket
     launch_nlist(c, true);
     c.list_valid = 1;
     CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
