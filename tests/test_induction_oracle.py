@@ -1,0 +1,83 @@
+"""The dense restatement of the reference's induced-dipole system against
+the reference's own converged dipoles (golden fixture polwater216: the
+reference's permanent field E0 in, its dipoles out), and the molecule-block
+preconditioner of the CUDA solve restated on that matrix (CPU only)."""
+import numpy as np
+
+from conftest import golden
+import induction_oracle
+from swinmd_b200 import systems
+
+TOL = 2.0819e-8   # 1e-6 D in e nm: RMS change of the dipoles at which the solve stops
+
+
+def _case():
+    g = golden("polwater216")
+    s = systems.polarizable_water(nmol=216, cutoff=0.9, switch=0.8, alpha=3.5, kmax=7, seed=3, n_steps=10)
+    polar = np.array([s.atom_types[t].polar for t in g["atom_type"]])
+    return g, s, polar
+
+
+def rms_rel(a, b):
+    return float(np.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2)))
+
+
+def test_dense_solve_matches_reference_dipoles():
+    g, s, polar = _case()
+    p = induction_oracle.solve_dipoles(g["pos"], polar, g["box"], s.config.a_damping, s.config.cutoff_ind,
+                                       g["f_ind_E0"])
+    err = rms_rel(p.reshape(-1), g["f_ind_P"])
+    print("rms rel error vs reference dipoles", err)
+    assert err < 1e-10
+
+
+def pcg(A, b, apply_m, x0, tol, max_iter=200):
+    """Preconditioned CG stopping when the RMS step of x drops below tol
+    (the CUDA solve's test); returns x and the iteration count."""
+    x = x0.copy()
+    r = b - A @ x
+    z = apply_m(r)
+    p = z.copy()
+    rz = r @ z
+    for it in range(1, max_iter + 1):
+        Ap = A @ p
+        alpha = rz / (p @ Ap)
+        x += alpha * p
+        if np.sqrt(np.mean((alpha * p) ** 2)) < tol:
+            return x, it
+        r -= alpha * Ap
+        z = apply_m(r)
+        rz_new = r @ z
+        p = z + (rz_new / rz) * p
+        rz = rz_new
+    return x, max_iter
+
+
+def test_molecule_blocks_cut_iterations():
+    g, s, polar = _case()
+    A = induction_oracle.induction_matrix(g["pos"], polar, g["box"], s.config.a_damping, s.config.cutoff_ind)
+    b = np.asarray(g["f_ind_E0"], np.float64)
+    exact = np.linalg.solve(A, b)
+    al = np.repeat(np.maximum(induction_oracle.POLMIN, polar), 3)
+    # each molecule's own block of A (its sites' 1/alpha and mutual couplings), inverted
+    mol = np.asarray(g["mol_id"])
+    blocks = []
+    for m in np.unique(mol):
+        idx = np.concatenate([np.arange(3 * i, 3 * i + 3) for i in np.flatnonzero(mol == m)])
+        blocks.append((idx, np.linalg.inv(A[np.ix_(idx, idx)])))
+
+    def m_site(r):
+        return al * r
+
+    def m_mol(r):
+        out = np.empty_like(r)
+        for idx, inv in blocks:
+            out[idx] = inv @ r[idx]
+        return out
+
+    x_site, it_site = pcg(A, b, m_site, m_site(b), TOL)
+    x_mol, it_mol = pcg(A, b, m_mol, m_mol(b), TOL)
+    print("iterations: site", it_site, "molecule blocks", it_mol)
+    for x in (x_site, x_mol):
+        assert np.sqrt(np.mean((x - exact) ** 2)) < 10 * TOL
+    assert it_mol < it_site
