@@ -1,5 +1,6 @@
-"""Dense restatement of the reference's induced-dipole system (test
-infrastructure: only tests/ use it, as the checker).
+"""Restatement of the reference's induced-dipole system: the permanent
+field and the dense matrix (test infrastructure: only tests/ use it, as the
+checker).
 
 Induction::compute builds A p = E0 over all 3N dipole components
 (src/forces/Induction.cpp):
@@ -61,6 +62,69 @@ def induction_matrix(pos, polar, box, a, cutoff, damp=True):
             A[3 * i:3 * i + 3, 3 * jj:3 * jj + 3] = -T[k]
             A[3 * jj:3 * jj + 3, 3 * i:3 * i + 3] = -T[k]
     return A
+
+
+def quad_matrix(q6):
+    """3 x 3 quadrupoles from the six components xx xy xz yy yz zz (N x 6)."""
+    q6 = np.asarray(q6, np.float64).reshape(-1, 6)
+    Q = np.empty((len(q6), 3, 3))
+    for (r, c), k in {(0, 0): 0, (0, 1): 1, (0, 2): 2, (1, 1): 3, (1, 2): 4, (2, 2): 5}.items():
+        Q[:, r, c] = q6[:, k]
+        Q[:, c, r] = q6[:, k]
+    return Q
+
+
+def permanent_field(pos, q, dip, quad, polar, box, a, cutoff, mol_id):
+    """E0 (N x 3): the Thole-damped field of the other molecules' charges,
+    dipoles and quadrupoles (lab frame) at every site, pairs within
+    cutoffInd, sites of one molecule excluded from each other
+    (Induction.cpp:371-431, the b_i / b_j terms):
+        b_i = q_j l3 r / r^3 + 3 l5 r (r.mu_j) / r^5 - l3 mu_j / r^3
+              + 15 l7 (r.Q_j.r) r / r^7 - 6 l5 Q_j r / r^5 - 3 l5 tr(Q_j) r / r^5
+    with r = r_i - r_j, b_j the same with i, j swapped (r -> -r) and
+    l7 = 1 - (1 + a u^3 + 3 (a u^3)^2 / 5) e."""
+    pos = np.asarray(pos, np.float64)
+    box = np.asarray(box, np.float64)
+    q = np.asarray(q, np.float64)
+    mu = np.asarray(dip, np.float64).reshape(-1, 3)
+    Q = quad_matrix(quad)
+    mol = np.asarray(mol_id)
+    n = len(pos)
+    al = np.maximum(POLMIN, np.asarray(polar, np.float64))
+    E = np.zeros((n, 3))
+    trQ = np.trace(Q, axis1=1, axis2=2)
+    for i in range(n - 1):
+        j = np.arange(i + 1, n)
+        r = min_image(pos[i] - pos[j], box)
+        r2 = np.einsum("ij,ij->i", r, r)
+        keep = (r2 <= cutoff * cutoff) & (mol[j] != mol[i])
+        j, r, r2 = j[keep], r[keep], r2[keep]
+        if len(j) == 0:
+            continue
+        rr = np.sqrt(r2)
+        r_3 = 1.0 / (r2 * rr)
+        r_5 = r_3 / r2
+        r_7 = r_5 / r2
+        au3 = a * r2 * rr / np.sqrt(al[i] * al[j])
+        e = np.exp(-au3)
+        l3 = 1.0 - e
+        l5 = 1.0 - (1.0 + au3) * e
+        l7 = 1.0 - (1.0 + au3 + 0.6 * au3 * au3) * e
+        Qj_r = np.einsum("kab,kb->ka", Q[j], r)
+        Qi_r = Q[i] @ r.T
+        rQjr = np.einsum("ka,ka->k", r, Qj_r)
+        rQir = np.einsum("ka,ak->k", r, Qi_r)
+        r_muj = np.einsum("ka,ka->k", r, mu[j])
+        r_mui = r @ mu[i]
+        bi = ((q[j] * l3 * r_3)[:, None] * r + (3.0 * l5 * r_5 * r_muj)[:, None] * r
+              - (l3 * r_3)[:, None] * mu[j] + (15.0 * l7 * r_7 * rQjr)[:, None] * r
+              - (6.0 * l5 * r_5)[:, None] * Qj_r - (3.0 * l5 * r_5 * trQ[j])[:, None] * r)
+        bj = (-(q[i] * l3 * r_3)[:, None] * r + (3.0 * l5 * r_5 * r_mui)[:, None] * r
+              - (l3 * r_3)[:, None] * mu[i] - (15.0 * l7 * r_7 * rQir)[:, None] * r
+              + (6.0 * l5 * r_5)[:, None] * Qi_r.T + (3.0 * l5 * r_5 * trQ[i])[:, None] * r)
+        E[i] += bi.sum(axis=0)
+        np.add.at(E, j, bj)
+    return E
 
 
 def solve_dipoles(pos, polar, box, a, cutoff, e0, damp=True):

@@ -1,7 +1,8 @@
-"""The dense restatement of the reference's induced-dipole system against
-the reference's own converged dipoles (golden fixture polwater216: the
-reference's permanent field E0 in, its dipoles out), and the molecule-block
-preconditioner of the CUDA solve restated on that matrix (CPU only)."""
+"""The restatement of the reference's induced-dipole system against the
+reference's own results (golden fixture polwater216): its permanent field
+from the reference's lab-frame multipoles, and its converged dipoles; and the
+molecule-block preconditioner of the CUDA solve restated on that matrix (CPU
+only)."""
 import numpy as np
 
 from conftest import golden
@@ -29,6 +30,20 @@ def test_dense_solve_matches_reference_dipoles():
     err = rms_rel(p.reshape(-1), g["f_ind_P"])
     print("rms rel error vs reference dipoles", err)
     assert err < 1e-10
+
+
+def test_permanent_field_matches_reference():
+    """E0 from the fixture's positions and the reference's own lab-frame
+    multipoles, then the dipoles from that field."""
+    g, s, polar = _case()
+    q = np.array([s.atom_types[t].charge for t in g["atom_type"]])
+    e0 = induction_oracle.permanent_field(g["pos"], q, g["f_mp_dip"], g["f_mp_quad"], polar, g["box"],
+                                          s.config.a_damping, s.config.cutoff_ind, g["mol_id"])
+    err = rms_rel(e0.reshape(-1), g["f_ind_E0"])
+    print("rms rel error vs reference E0", err)
+    assert err < 1e-12
+    p = induction_oracle.solve_dipoles(g["pos"], polar, g["box"], s.config.a_damping, s.config.cutoff_ind, e0)
+    assert rms_rel(p.reshape(-1), g["f_ind_P"]) < 1e-10
 
 
 def pcg(A, b, apply_m, x0, tol, max_iter=200):
