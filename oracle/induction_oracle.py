@@ -1,6 +1,6 @@
-"""Restatement of the reference's induced-dipole system: the permanent
-field and the dense matrix (test infrastructure: only tests/ use it, as the
-checker).
+"""Restatement of the reference's induced-dipole system: lab-frame
+multipoles, the permanent field and the dense matrix (test infrastructure:
+only tests/ use it, as the checker).
 
 Induction::compute builds A p = E0 over all 3N dipole components
 (src/forces/Induction.cpp):
@@ -62,6 +62,45 @@ def induction_matrix(pos, polar, box, a, cutoff, damp=True):
             A[3 * i:3 * i + 3, 3 * jj:3 * jj + 3] = -T[k]
             A[3 * jj:3 * jj + 3, 3 * i:3 * i + 3] = -T[k]
     return A
+
+
+def lab_multipoles(pos, mol_id, dip_local, quad_local):
+    """Lab-frame dipoles (N x 3) and quadrupoles (N x 6, xx xy xz yy yz zz)
+    of H O H molecules (sites in that order within each molecule), from
+    each site's local-frame values (Local2Global::FrameofReference,
+    src/utils/Local2Global.cpp): an H site takes w along O - H and the lab x
+    axis (lab y when |w.x| > 0.866) as its second vector; O takes w along
+    the sum of the unit O->H vectors and the unit O->H2 vector; then
+    u = s - (s.w) w normalised, v = w x u, mu = [u v w] mu_local and
+    Q = [u v w] Q_local [u v w]^T / 3.  Positions are used as given (whole
+    molecules), as the reference does."""
+    pos = np.asarray(pos, np.float64)
+    mol = np.asarray(mol_id)
+    dl = np.asarray(dip_local, np.float64).reshape(-1, 3)
+    QL = quad_matrix(quad_local)
+    n = len(pos)
+    mu = np.zeros((n, 3))
+    Q6 = np.zeros((n, 6))
+
+    def unit(v):
+        return v / np.linalg.norm(v)
+
+    for m in np.unique(mol):
+        h1, o, h2 = np.flatnonzero(mol == m)
+        p1 = [pos[o] - pos[h1], unit(pos[h1] - pos[o]) + unit(pos[h2] - pos[o]), pos[o] - pos[h2]]
+        ex, ey = np.array([1.0, 0.0, 0.0]), np.array([0.0, 1.0, 0.0])
+        p2 = [ey if abs(p1[0][0] / np.linalg.norm(p1[0])) > 0.8660 else ex, unit(pos[h2] - pos[o]),
+              ey if abs(p1[2][0] / np.linalg.norm(p1[2])) > 0.8660 else ex]
+        for k, i in enumerate((h1, o, h2)):
+            w = unit(p1[k])
+            ss = p2[k] - (p2[k] @ w) * w
+            u = unit(ss)
+            v = np.cross(w, u)
+            R = np.stack([u, v, w], axis=1)
+            mu[i] = R @ dl[i]
+            G = R @ QL[i] @ R.T / 3.0
+            Q6[i] = [G[0, 0], G[0, 1], G[0, 2], G[1, 1], G[1, 2], G[2, 2]]
+    return mu, Q6
 
 
 def quad_matrix(q6):
