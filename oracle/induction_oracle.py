@@ -1,6 +1,7 @@
-"""Restatement of the reference's induced-dipole system: lab-frame
-multipoles, the permanent field and the dense matrix (test infrastructure:
-only tests/ use it, as the checker).
+"""Restatement of the reference's polarisable multipole model: lab-frame
+multipoles, the multipole Ewald real-space energy, and the induced-dipole
+system (permanent field and dense matrix).  Test infrastructure: only
+tests/ use it, as the checker.
 
 Induction::compute builds A p = E0 over all 3N dipole components
 (src/forces/Induction.cpp):
@@ -164,6 +165,68 @@ def permanent_field(pos, q, dip, quad, polar, box, a, cutoff, mol_id):
         E[i] += bi.sum(axis=0)
         np.add.at(E, j, bj)
     return E
+
+
+COULOMBS = 138.93548501   # 1 / (4 pi eps0) in kJ mol^-1 nm e^-2 (src/NEMD_defs.h:104)
+
+
+def multipole_real_energy(pos, q, dip, quad, box, alpha, cutoff, mol_id):
+    """Ewald real-space energy of charges, dipoles and quadrupoles
+    (Multipole::compute, src/forces/Multipole.cpp:540-653): for every pair of
+    sites of different molecules within the real-space cutoff,
+    COULOMBS * sum_n G_n B_n with r = r_i - r_j,
+        B_0 = erfc(alpha r) / r,
+        B_n = ((2n - 1) B_{n-1} + (2 alpha^2)^n e^{-alpha^2 r^2} / (alpha sqrt(pi))) / r^2
+              (with the reference's signs: B1 = (-B0 - c e)/r^2, B2 = (-3 B1 + 2 c a^2 e)/r^2, ...)
+        G_0 = q_i q_j
+        G_1 = q_j mu_i.r - q_i mu_j.r - mu_i.mu_j + q_j tr Q_i + q_i tr Q_j
+        G_2 = q_j r.Q_i.r + q_i r.Q_j.r - (mu_i.r)(mu_j.r) - (mu_j.r) tr Q_i + (mu_i.r) tr Q_j
+              - 2 mu_j.Q_i r + 2 mu_i.Q_j r + tr Q_i tr Q_j + 2 Q_i:Q_j
+        G_3 = (mu_i.r) r.Q_j.r - (mu_j.r) r.Q_i.r + tr Q_i r.Q_j.r + tr Q_j r.Q_i.r
+              + 4 (Q_i r).(Q_j r)
+        G_4 = (r.Q_i.r)(r.Q_j.r)."""
+    from scipy.special import erfc
+    pos = np.asarray(pos, np.float64)
+    box = np.asarray(box, np.float64)
+    q = np.asarray(q, np.float64)
+    mu = np.asarray(dip, np.float64).reshape(-1, 3)
+    Q = quad_matrix(quad)
+    trQ = np.trace(Q, axis1=1, axis2=2)
+    mol = np.asarray(mol_id)
+    n = len(pos)
+    a2 = alpha * alpha
+    c = 2.0 * alpha / np.sqrt(np.pi)
+    energy = 0.0
+    for i in range(n - 1):
+        j = np.arange(i + 1, n)
+        r = min_image(pos[i] - pos[j], box)
+        r2 = np.einsum("ij,ij->i", r, r)
+        keep = (r2 < cutoff * cutoff) & (mol[j] != mol[i])
+        j, r, r2 = j[keep], r[keep], r2[keep]
+        if len(j) == 0:
+            continue
+        rr = np.sqrt(r2)
+        ex = np.exp(-a2 * r2)
+        B0 = erfc(alpha * rr) / rr
+        B1 = (-B0 - c * ex) / r2
+        B2 = (-3 * B1 + 2 * c * a2 * ex) / r2
+        B3 = (-5 * B2 - 4 * c * a2 * a2 * ex) / r2
+        B4 = (-7 * B3 + 8 * c * a2 * a2 * a2 * ex) / r2
+        Qi_r = (Q[i] @ r.T).T
+        Qj_r = np.einsum("kab,kb->ka", Q[j], r)
+        rQir = np.einsum("ka,ka->k", r, Qi_r)
+        rQjr = np.einsum("ka,ka->k", r, Qj_r)
+        mir = r @ mu[i]
+        mjr = np.einsum("ka,ka->k", r, mu[j])
+        G0 = q[i] * q[j]
+        G1 = q[j] * mir - q[i] * mjr - mu[j] @ mu[i] + q[j] * trQ[i] + q[i] * trQ[j]
+        G2 = (q[j] * rQir + q[i] * rQjr - mir * mjr - mjr * trQ[i] + mir * trQ[j]
+              - 2 * np.einsum("ka,ka->k", mu[j], Qi_r) + 2 * (Qj_r @ mu[i]) + trQ[i] * trQ[j]
+              + 2 * np.einsum("ab,kab->k", Q[i], Q[j]))
+        G3 = mir * rQjr - mjr * rQir + trQ[i] * rQjr + trQ[j] * rQir + 4 * np.einsum("ka,ka->k", Qi_r, Qj_r)
+        G4 = rQir * rQjr
+        energy += float(np.sum(G0 * B0 + G1 * B1 + G2 * B2 + G3 * B3 + G4 * B4))
+    return energy * COULOMBS
 
 
 def solve_dipoles(pos, polar, box, a, cutoff, e0, damp=True):
