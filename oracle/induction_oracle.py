@@ -229,6 +229,41 @@ def multipole_real_energy(pos, q, dip, quad, box, alpha, cutoff, mol_id):
     return energy * COULOMBS
 
 
+def multipole_recip_energy(pos, q, dip, quad, box, alpha, kcut):
+    """Ewald reciprocal energy of charges, dipoles and quadrupoles
+    (Multipole::reciprocal_term, src/forces/Multipole.cpp:245-293 for the k
+    half-space, :1054-1131 for the sums):
+        k = 2 pi (nx / Lx, ny / Ly, nz / Lz), nx >= 0, k^2 < kcut^2, one of each +-k pair,
+        C = sum_i (q_i - k.Q_i.k) cos(k.r_i),  S = sum_i (q_i - k.Q_i.k) sin(k.r_i),
+        M_c = sum_i (mu_i.k) cos(k.r_i),       M_s = sum_i (mu_i.k) sin(k.r_i),
+        E = COULOMBS (4 pi / V) sum_k e^{-k^2 / (4 alpha^2)} / k^2
+            (C^2 + S^2 + 2 (S M_c - C M_s) + M_c^2 + M_s^2)."""
+    pos = np.asarray(pos, np.float64)
+    box = np.asarray(box, np.float64)
+    q = np.asarray(q, np.float64)
+    mu = np.asarray(dip, np.float64).reshape(-1, 3)
+    Q = quad_matrix(quad)
+    nmax = [int(kcut * L / (2 * np.pi)) for L in box]
+    v = 2 * np.pi / box
+    ks = []
+    for nx in range(0, nmax[0] + 1):
+        for ny in range(0 if nx == 0 else -nmax[1], nmax[1] + 1):
+            for nz in range(1 if nx == 0 and ny == 0 else -nmax[2], nmax[2] + 1):
+                k = np.array([nx, ny, nz]) * v
+                if k @ k < kcut * kcut:
+                    ks.append(k)
+    ks = np.array(ks)
+    k2 = np.einsum("ka,ka->k", ks, ks)
+    ph = pos @ ks.T                                    # N x K
+    w = q[:, None] - np.einsum("ka,iab,kb->ik", ks, Q, ks)
+    m = mu @ ks.T
+    cs, sn = np.cos(ph), np.sin(ph)
+    C, S = (w * cs).sum(0), (w * sn).sum(0)
+    Mc, Ms = (m * cs).sum(0), (m * sn).sum(0)
+    coef = 4 * np.pi / np.prod(box) * np.exp(-k2 / (4 * alpha * alpha)) / k2
+    return float(np.sum(coef * (C * C + S * S + 2 * (S * Mc - C * Ms) + Mc * Mc + Ms * Ms))) * COULOMBS
+
+
 def solve_dipoles(pos, polar, box, a, cutoff, e0, damp=True):
     """Induced dipoles p (N x 3) with A p = E0 (e0: N x 3 or 3N, site-major)."""
     A = induction_matrix(pos, polar, box, a, cutoff, damp)

@@ -76,6 +76,18 @@ def test_multipole_real_energy_matches_reference():
     assert abs(e - ref) < 1e-12 * abs(ref)
 
 
+def test_multipole_recip_energy_matches_reference():
+    """Ewald reciprocal energy of the permanent multipoles over the
+    reference's k half-space against its longEnergy."""
+    g, s, polar = _case()
+    q = np.array([s.atom_types[k].charge for k in g["atom_type"]])
+    e = induction_oracle.multipole_recip_energy(g["pos"], q, g["f_mp_dip"], g["f_mp_quad"], g["box"],
+                                                s.config.alpha, s.config.k_cutoff)
+    ref = g["f_mp_long_energy"][2]
+    print("reciprocal energy", e, ref)
+    assert abs(e - ref) < 1e-12 * abs(ref)
+
+
 def pcg(A, b, apply_m, x0, tol, max_iter=200):
     """Preconditioned CG stopping when the RMS step of x drops below tol
     (the CUDA solve's test); returns x and the iteration count."""
