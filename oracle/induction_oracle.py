@@ -212,19 +212,7 @@ def multipole_real_energy(pos, q, dip, quad, box, alpha, cutoff, mol_id):
         B2 = (-3 * B1 + 2 * c * a2 * ex) / r2
         B3 = (-5 * B2 - 4 * c * a2 * a2 * ex) / r2
         B4 = (-7 * B3 + 8 * c * a2 * a2 * a2 * ex) / r2
-        Qi_r = (Q[i] @ r.T).T
-        Qj_r = np.einsum("kab,kb->ka", Q[j], r)
-        rQir = np.einsum("ka,ka->k", r, Qi_r)
-        rQjr = np.einsum("ka,ka->k", r, Qj_r)
-        mir = r @ mu[i]
-        mjr = np.einsum("ka,ka->k", r, mu[j])
-        G0 = q[i] * q[j]
-        G1 = q[j] * mir - q[i] * mjr - mu[j] @ mu[i] + q[j] * trQ[i] + q[i] * trQ[j]
-        G2 = (q[j] * rQir + q[i] * rQjr - mir * mjr - mjr * trQ[i] + mir * trQ[j]
-              - 2 * np.einsum("ka,ka->k", mu[j], Qi_r) + 2 * (Qj_r @ mu[i]) + trQ[i] * trQ[j]
-              + 2 * np.einsum("ab,kab->k", Q[i], Q[j]))
-        G3 = mir * rQjr - mjr * rQir + trQ[i] * rQjr + trQ[j] * rQir + 4 * np.einsum("ka,ka->k", Qi_r, Qj_r)
-        G4 = rQir * rQjr
+        G0, G1, G2, G3, G4 = _pair_invariants(q, mu, Q, trQ, i, j, r)
         energy += float(np.sum(G0 * B0 + G1 * B1 + G2 * B2 + G3 * B3 + G4 * B4))
     return energy * COULOMBS
 
@@ -262,6 +250,69 @@ def multipole_recip_energy(pos, q, dip, quad, box, alpha, kcut):
     Mc, Ms = (m * cs).sum(0), (m * sn).sum(0)
     coef = 4 * np.pi / np.prod(box) * np.exp(-k2 / (4 * alpha * alpha)) / k2
     return float(np.sum(coef * (C * C + S * S + 2 * (S * Mc - C * Ms) + Mc * Mc + Ms * Ms))) * COULOMBS
+
+
+def _pair_invariants(q, mu, Q, trQ, i, j, r):
+    """G_0..G_4 of site i with sites j (arrays), r = r_i - r_j (the same
+    invariants as in multipole_real_energy)."""
+    Qi_r = (Q[i] @ r.T).T
+    Qj_r = np.einsum("kab,kb->ka", Q[j], r)
+    rQir = np.einsum("ka,ka->k", r, Qi_r)
+    rQjr = np.einsum("ka,ka->k", r, Qj_r)
+    mir = r @ mu[i]
+    mjr = np.einsum("ka,ka->k", r, mu[j])
+    G0 = q[i] * q[j]
+    G1 = q[j] * mir - q[i] * mjr - mu[j] @ mu[i] + q[j] * trQ[i] + q[i] * trQ[j]
+    G2 = (q[j] * rQir + q[i] * rQjr - mir * mjr - mjr * trQ[i] + mir * trQ[j]
+          - 2 * np.einsum("ka,ka->k", mu[j], Qi_r) + 2 * (Qj_r @ mu[i]) + trQ[i] * trQ[j]
+          + 2 * np.einsum("ab,kab->k", Q[i], Q[j]))
+    G3 = mir * rQjr - mjr * rQir + trQ[i] * rQjr + trQ[j] * rQir + 4 * np.einsum("ka,ka->k", Qi_r, Qj_r)
+    G4 = rQir * rQjr
+    return G0, G1, G2, G3, G4
+
+
+def multipole_correct_energies(pos, q, dip, quad, box, alpha, mol_id):
+    """The reference's correctEnergy and molCorrectEnergy of the multipoles
+    (Multipole::self_correct, src/forces/Multipole.cpp:338-386, the net
+    charge term at :104, and the intramolecular correction set at :1689):
+        self = -1/2 COULOMBS sum_i [q^2 c + (mu.mu - 2 q tr Q) 2 c alpha^2 / 3
+                                    + ((tr Q)^2 + 2 Q:Q) 4 c alpha^4 / 5],  c = 2 alpha / sqrt(pi)
+        charged = -pi (sum q)^2 / (2 V alpha^2)
+        intra = -COULOMBS sum over site pairs of one molecule of sum_n G_n D_n
+    with D_0 = erf(alpha r) / r and the upward recursion of the B_n with the
+    signs of erf (D_1 = (-D_0 + c e^{-alpha^2 r^2}) / r^2, ...)."""
+    from scipy.special import erf
+    pos = np.asarray(pos, np.float64)
+    box = np.asarray(box, np.float64)
+    q = np.asarray(q, np.float64)
+    mu = np.asarray(dip, np.float64).reshape(-1, 3)
+    Q = quad_matrix(quad)
+    trQ = np.trace(Q, axis1=1, axis2=2)
+    QQ = np.einsum("iab,iab->i", Q, Q)
+    a2 = alpha * alpha
+    c = 2.0 * alpha / np.sqrt(np.pi)
+    selfterm = (q * q * c + (np.einsum("ia,ia->i", mu, mu) - 2 * q * trQ) * 2 * c * a2 / 3
+                + (trQ * trQ + 2 * QQ) * 4 * c * a2 * a2 / 5)
+    e_self = float(np.sum(-0.5 * selfterm * COULOMBS))
+    e_charged = -np.pi * q.sum() ** 2 / (2.0 * np.prod(box) * a2)
+    mol = np.asarray(mol_id)
+    intra = 0.0
+    for m in np.unique(mol):
+        sites = np.flatnonzero(mol == m)
+        for k, i in enumerate(sites[:-1]):
+            j = sites[k + 1:]
+            r = min_image(pos[i] - pos[j], box)
+            r2 = np.einsum("ka,ka->k", r, r)
+            rr = np.sqrt(r2)
+            ex = np.exp(-a2 * r2)
+            D0 = erf(alpha * rr) / rr
+            D1 = (-D0 + c * ex) / r2
+            D2 = (-3 * D1 - 2 * c * a2 * ex) / r2
+            D3 = (-5 * D2 + 4 * c * a2 * a2 * ex) / r2
+            D4 = (-7 * D3 - 8 * c * a2 * a2 * a2 * ex) / r2
+            G0, G1, G2, G3, G4 = _pair_invariants(q, mu, Q, trQ, i, j, r)
+            intra += float(np.sum(G0 * D0 + G1 * D1 + G2 * D2 + G3 * D3 + G4 * D4))
+    return e_self + e_charged, -intra * COULOMBS
 
 
 def solve_dipoles(pos, polar, box, a, cutoff, e0, damp=True):

@@ -88,6 +88,18 @@ def test_multipole_recip_energy_matches_reference():
     assert abs(e - ref) < 1e-12 * abs(ref)
 
 
+def test_multipole_correct_energies_match_reference():
+    """Self (+ net charge) and intramolecular corrections of the multipoles
+    against the reference's correctEnergy and molCorrectEnergy."""
+    g, s, polar = _case()
+    q = np.array([s.atom_types[k].charge for k in g["atom_type"]])
+    e_corr, e_intra = induction_oracle.multipole_correct_energies(g["pos"], q, g["f_mp_dip"], g["f_mp_quad"],
+                                                                  g["box"], s.config.alpha, g["mol_id"])
+    ref = g["f_mp_short_energy"]
+    assert abs(e_corr - ref[3]) < 1e-12 * abs(ref[3])
+    assert abs(e_intra - ref[4]) < 1e-12 * abs(ref[4])
+
+
 def pcg(A, b, apply_m, x0, tol, max_iter=200):
     """Preconditioned CG stopping when the RMS step of x drops below tol
     (the CUDA solve's test); returns x and the iteration count."""
