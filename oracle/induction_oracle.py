@@ -315,6 +315,53 @@ def multipole_correct_energies(pos, q, dip, quad, box, alpha, mol_id):
     return e_self + e_charged, -intra * COULOMBS
 
 
+def induced_correct_energies(pos, q, dip, quad, p, box, alpha, mol_id):
+    """The reference's correctPolEnergy and molCorrectPolEnergy: the induced
+    dipoles' Ewald self term -COULOMBS sum_i (mu_i.p_i) c alpha^2 / 3 and the
+    intramolecular correction -1/2 COULOMBS sum over site pairs of one
+    molecule of (G1_i + G1_j) D_1 + (G2_i + G2_j) D_2 + (G3_i + G3_j) D_3,
+    with the permanent-induced invariants (r = r_i - r_j)
+        G1_i = -q_i p_j.r - mu_i.p_j
+        G2_i = -(mu_i.r)(p_j.r) - 2 p_j.Q_i r - (p_j.r) tr Q_i
+        G3_i = -(p_j.r)(r.Q_i.r)
+    and G*_j the same with i, j swapped (r -> -r), D_n as in
+    multipole_correct_energies."""
+    from scipy.special import erf
+    pos = np.asarray(pos, np.float64)
+    box = np.asarray(box, np.float64)
+    q = np.asarray(q, np.float64)
+    mu = np.asarray(dip, np.float64).reshape(-1, 3)
+    pp = np.asarray(p, np.float64).reshape(-1, 3)
+    Q = quad_matrix(quad)
+    trQ = np.trace(Q, axis1=1, axis2=2)
+    a2 = alpha * alpha
+    c = 2.0 * alpha / np.sqrt(np.pi)
+    e_self = float(np.sum(-np.einsum("ia,ia->i", mu, pp) * c * a2 / 3 * COULOMBS))
+    mol = np.asarray(mol_id)
+    intra = 0.0
+    for m in np.unique(mol):
+        sites = np.flatnonzero(mol == m)
+        for k, i in enumerate(sites[:-1]):
+            for j in sites[k + 1:]:
+                r = min_image(pos[i] - pos[j], box)
+                r2 = r @ r
+                rr = np.sqrt(r2)
+                ex = np.exp(-a2 * r2)
+                D0 = erf(alpha * rr) / rr
+                D1 = (-D0 + c * ex) / r2
+                D2 = (-3 * D1 - 2 * c * a2 * ex) / r2
+                D3 = (-5 * D2 + 4 * c * a2 * a2 * ex) / r2
+                pjr, pir = pp[j] @ r, pp[i] @ (-r)
+                G1i = -q[i] * pjr - mu[i] @ pp[j]
+                G2i = -(mu[i] @ r) * pjr - 2.0 * (pp[j] @ (Q[i] @ r)) - pjr * trQ[i]
+                G3i = -pjr * (r @ Q[i] @ r)
+                G1j = -q[j] * pir - mu[j] @ pp[i]
+                G2j = -(mu[j] @ (-r)) * pir - 2.0 * (pp[i] @ (Q[j] @ (-r))) - pir * trQ[j]
+                G3j = -pir * (r @ Q[j] @ r)
+                intra += (G1i + G1j) * D1 + (G2i + G2j) * D2 + (G3i + G3j) * D3
+    return e_self, -0.5 * intra * COULOMBS
+
+
 def solve_dipoles(pos, polar, box, a, cutoff, e0, damp=True):
     """Induced dipoles p (N x 3) with A p = E0 (e0: N x 3 or 3N, site-major)."""
     A = induction_matrix(pos, polar, box, a, cutoff, damp)

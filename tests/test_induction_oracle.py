@@ -100,6 +100,19 @@ def test_multipole_correct_energies_match_reference():
     assert abs(e_intra - ref[4]) < 1e-12 * abs(ref[4])
 
 
+def test_induced_correct_energies_match_reference():
+    """Induced dipoles' self and intramolecular corrections (from the
+    reference's converged dipoles) against its correctPolEnergy and
+    molCorrectPolEnergy."""
+    g, s, polar = _case()
+    q = np.array([s.atom_types[k].charge for k in g["atom_type"]])
+    e_self, e_intra = induction_oracle.induced_correct_energies(g["pos"], q, g["f_mp_dip"], g["f_mp_quad"],
+                                                                g["f_ind_P"], g["box"], s.config.alpha, g["mol_id"])
+    ref = g["f_ind_short_energy"]
+    assert abs(e_self - ref[8]) < 1e-12 * abs(ref[8])
+    assert abs(e_intra - ref[9]) < 1e-12 * abs(ref[9])
+
+
 def pcg(A, b, apply_m, x0, tol, max_iter=200):
     """Preconditioned CG stopping when the RMS step of x drops below tol
     (the CUDA solve's test); returns x and the iteration count."""
