@@ -362,6 +362,67 @@ def induced_correct_energies(pos, q, dip, quad, p, box, alpha, mol_id):
     return e_self, -0.5 * intra * COULOMBS
 
 
+def induced_real_energy(pos, q, dip, quad, p, polar, box, alpha, a, cutoff, mol_id):
+    """The reference's realPolEnergy (Induction.cpp:985-1075, Thole damping
+    applied to the Ewald B_n, not the AMOEBA form): for every pair of sites
+    of different molecules within the real-space cutoff
+        1/2 COULOMBS [(G1_i + G1_j) B1d + (G2_i + G2_j) B2d + (G3_i + G3_j) B3d]
+    with the invariants of induced_correct_energies, u^3 = r^3 / sqrt(a_i a_j),
+    e = exp(-a u^3), l3 = 1 - e, g3 = 3 a u^3 e / r^2, g5 = 3 (a u^3)^2 e / r^2,
+        B1d = B1 l3,  B2d = B2 l3 + B1 g3,  B3d = B3 l3 + 2 B2 g3 + B1 (g3 - 3 g5) / r^2
+    and the erfc-based B_n of multipole_real_energy."""
+    from scipy.special import erfc
+    pos = np.asarray(pos, np.float64)
+    box = np.asarray(box, np.float64)
+    q = np.asarray(q, np.float64)
+    mu = np.asarray(dip, np.float64).reshape(-1, 3)
+    pp = np.asarray(p, np.float64).reshape(-1, 3)
+    al = np.asarray(polar, np.float64)
+    Q = quad_matrix(quad)
+    trQ = np.trace(Q, axis1=1, axis2=2)
+    mol = np.asarray(mol_id)
+    n = len(pos)
+    a2 = alpha * alpha
+    c = 2.0 * alpha / np.sqrt(np.pi)
+    energy = 0.0
+    for i in range(n - 1):
+        j = np.arange(i + 1, n)
+        r = min_image(pos[i] - pos[j], box)
+        r2 = np.einsum("ij,ij->i", r, r)
+        keep = (r2 < cutoff * cutoff) & (mol[j] != mol[i])
+        j, r, r2 = j[keep], r[keep], r2[keep]
+        if len(j) == 0:
+            continue
+        rr = np.sqrt(r2)
+        ex = np.exp(-a2 * r2)
+        B0 = erfc(alpha * rr) / rr
+        B1 = (-B0 - c * ex) / r2
+        B2 = (-3 * B1 + 2 * c * a2 * ex) / r2
+        B3 = (-5 * B2 - 4 * c * a2 * a2 * ex) / r2
+        au3 = a * r2 * rr / np.sqrt(al[i] * al[j])
+        e = np.exp(-au3)
+        l3 = 1.0 - e
+        g3 = 3.0 * au3 * e / r2
+        g5 = 3.0 * au3 * au3 * e / r2
+        B1d = B1 * l3
+        B2d = B2 * l3 + B1 * g3
+        B3d = B3 * l3 + 2.0 * B2 * g3 + B1 * (g3 - 3.0 * g5) / r2
+        Qi_r = (Q[i] @ r.T).T
+        Qj_r = np.einsum("kab,kb->ka", Q[j], r)
+        rQir = np.einsum("ka,ka->k", r, Qi_r)
+        rQjr = np.einsum("ka,ka->k", r, Qj_r)
+        pjr = np.einsum("ka,ka->k", pp[j], r)
+        pir = -(r @ pp[i])
+        G1i = -q[i] * pjr - pp[j] @ mu[i]
+        G2i = -(r @ mu[i]) * pjr - 2.0 * np.einsum("ka,ka->k", pp[j], Qi_r) - pjr * trQ[i]
+        G3i = -pjr * rQir
+        G1j = -q[j] * pir - mu[j] @ pp[i]
+        G2j = -(-np.einsum("ka,ka->k", mu[j], r)) * pir + 2.0 * (Qj_r @ pp[i]) - pir * trQ[j]
+        G3j = -pir * rQjr
+        energy += float(np.sum((G1i + G1j) * B1d + (G2i + G2j) * B2d + (G3i + G3j) * B3d))
+    return 0.5 * energy * COULOMBS
+
+
 def solve_dipoles(pos, polar, box, a, cutoff, e0, damp=True):
     """Induced dipoles p (N x 3) with A p = E0 (e0: N x 3 or 3N, site-major)."""
     A = induction_matrix(pos, polar, box, a, cutoff, damp)

@@ -113,6 +113,18 @@ def test_induced_correct_energies_match_reference():
     assert abs(e_intra - ref[9]) < 1e-12 * abs(ref[9])
 
 
+def test_induced_real_energy_matches_reference():
+    """Thole-damped Ewald real-space energy of the induced dipoles (from the
+    reference's converged dipoles) against its realPolEnergy."""
+    g, s, polar = _case()
+    q = np.array([s.atom_types[k].charge for k in g["atom_type"]])
+    e = induction_oracle.induced_real_energy(g["pos"], q, g["f_mp_dip"], g["f_mp_quad"], g["f_ind_P"], polar,
+                                             g["box"], s.config.alpha, s.config.a_damping, s.config.cutoff_ew,
+                                             g["mol_id"])
+    ref = g["f_ind_short_energy"][6]
+    assert abs(e - ref) < 1e-12 * abs(ref)
+
+
 def pcg(A, b, apply_m, x0, tol, max_iter=200):
     """Preconditioned CG stopping when the RMS step of x drops below tol
     (the CUDA solve's test); returns x and the iteration count."""
