@@ -231,6 +231,14 @@ def multipole_recip_energy(pos, q, dip, quad, box, alpha, kcut):
     q = np.asarray(q, np.float64)
     mu = np.asarray(dip, np.float64).reshape(-1, 3)
     Q = quad_matrix(quad)
+    C, S, Mc, Ms, Pc, Ps, coef = _recip_sums(pos, q, mu, Q, None, box, alpha, kcut)
+    return float(np.sum(coef * (C * C + S * S + 2 * (S * Mc - C * Ms) + Mc * Mc + Ms * Ms))) * COULOMBS
+
+
+def _recip_sums(pos, q, mu, Q, p, box, alpha, kcut):
+    """Structure sums over the reference's k half-space (see
+    multipole_recip_energy) and the coefficients 4 pi / V e^{-k^2/(4 alpha^2)} / k^2;
+    Pc, Ps are those of the dipoles p (None: zeros)."""
     nmax = [int(kcut * L / (2 * np.pi)) for L in box]
     v = 2 * np.pi / box
     ks = []
@@ -248,8 +256,26 @@ def multipole_recip_energy(pos, q, dip, quad, box, alpha, kcut):
     cs, sn = np.cos(ph), np.sin(ph)
     C, S = (w * cs).sum(0), (w * sn).sum(0)
     Mc, Ms = (m * cs).sum(0), (m * sn).sum(0)
+    if p is None:
+        Pc = Ps = np.zeros_like(C)
+    else:
+        pk = np.asarray(p, np.float64).reshape(-1, 3) @ ks.T
+        Pc, Ps = (pk * cs).sum(0), (pk * sn).sum(0)
     coef = 4 * np.pi / np.prod(box) * np.exp(-k2 / (4 * alpha * alpha)) / k2
-    return float(np.sum(coef * (C * C + S * S + 2 * (S * Mc - C * Ms) + Mc * Mc + Ms * Ms))) * COULOMBS
+    return C, S, Mc, Ms, Pc, Ps, coef
+
+
+def induced_recip_energy(pos, q, dip, quad, p, box, alpha, kcut):
+    """The reference's longPolEnergy: the reciprocal energy between the
+    induced dipoles and the permanent multipoles,
+        COULOMBS sum_k coef_k [(S P_c - C P_s) + (P_c M_c + P_s M_s)]
+    with the sums of multipole_recip_energy and P_c, P_s those of p.k."""
+    pos = np.asarray(pos, np.float64)
+    box = np.asarray(box, np.float64)
+    C, S, Mc, Ms, Pc, Ps, coef = _recip_sums(pos, np.asarray(q, np.float64),
+                                             np.asarray(dip, np.float64).reshape(-1, 3), quad_matrix(quad), p,
+                                             box, alpha, kcut)
+    return float(np.sum(coef * ((S * Pc - C * Ps) + (Pc * Mc + Ps * Ms)))) * COULOMBS
 
 
 def _pair_invariants(q, mu, Q, trQ, i, j, r):

@@ -125,6 +125,17 @@ def test_induced_real_energy_matches_reference():
     assert abs(e - ref) < 1e-12 * abs(ref)
 
 
+def test_induced_recip_energy_matches_reference():
+    """Reciprocal energy between the induced dipoles (the reference's
+    converged ones) and the permanent multipoles against its longPolEnergy."""
+    g, s, polar = _case()
+    q = np.array([s.atom_types[k].charge for k in g["atom_type"]])
+    e = induction_oracle.induced_recip_energy(g["pos"], q, g["f_mp_dip"], g["f_mp_quad"], g["f_ind_P"],
+                                              g["box"], s.config.alpha, s.config.k_cutoff)
+    ref = g["f_ind_long_energy"][7]
+    assert abs(e - ref) < 1e-12 * abs(ref)
+
+
 def pcg(A, b, apply_m, x0, tol, max_iter=200):
     """Preconditioned CG stopping when the RMS step of x drops below tol
     (the CUDA solve's test); returns x and the iteration count."""
