@@ -7,7 +7,7 @@ Default workload: rigid polarisable multipole water, 4096 molecules (12,288
 sites), the configuration the headline metric is quoted on.  Two arms are
 timed on the same system:
   plain   FP64 pair/reciprocal/dipole arithmetic, dipole solve started from
-          the first-order guess alpha E0;
+          the molecule-block solution M^-1 E0;
   fast    the learned initial guess (per-site network trained beforehand, on
           the GPU, on dipoles the solver itself converged) + the mixed path.
 Both solve the dipoles to the same tolerance (RMS change 1e-6 D).  `value`
@@ -24,8 +24,8 @@ bracketed by barriers and the slowest rank's time is used.
 
 The reference arm (--impl reference) times the reference's own C++ build
 (oracle/_ref/ref_dump: LFIntegrator::start, then LFIntegrator::run) on the
-same workload, single-threaded (the build has no MPI), bounded to at most
-two MD steps because one step of this size takes about two minutes.
+same workload, single-threaded (the build has no MPI), bounded to one MD
+step because one step of this size takes more than a minute.
 """
 import argparse
 import json

@@ -32,7 +32,9 @@ enum {
     SMD_ERR_SHAKE = 5,        /* SHAKE did not converge (LFIntegrator.cpp:1798-1812) */
     SMD_ERR_NAN = 6,          /* non-finite force or position */
     SMD_ERR_CG = 7,           /* dipole solve did not converge */
-    SMD_ERR_NO_DEVICE = 8     /* no CUDA device / extension unusable */
+    SMD_ERR_NO_DEVICE = 8,    /* no CUDA device / extension unusable */
+    SMD_ERR_TIMEOUT = 9       /* a bounded device-side wait ran out (the dipole
+                                 solve's grid barrier; see smd_set_wait_limit) */
 };
 
 /* arithmetic of the pair, reciprocal and dipole-field kernels */
@@ -50,7 +52,8 @@ enum {
     SMD_TERM_MP_SHORT = 8,   /* Multipole::compute(): self + real + intramolecular */
     SMD_TERM_MP_LONG = 16,   /* Multipole::compute_long() */
     SMD_TERM_IND_SHORT = 32, /* Induction::compute(): dipole solve, self, real, intra */
-    SMD_TERM_IND_LONG = 64,  /* Induction::compute_long() (solves the dipoles too) */
+    SMD_TERM_IND_LONG = 64,  /* Induction::compute_long() (solves the dipoles if no
+                                earlier call did for these positions) */
     SMD_TERM_ALL = 0xffff
 };
 
@@ -187,6 +190,16 @@ int smd_set_solver(smd_ctx *ctx, double tol, int max_iter, int guess);
 #define SMD_PRECOND_SITE 0
 #define SMD_PRECOND_MOLECULE 1
 int smd_set_preconditioner(smd_ctx *ctx, int kind);
+/* Limit (seconds, default 1) of every bounded device-side wait: the dipole
+ * solve's grid barrier.  A wait that runs out makes the solve leave, sets
+ * SMD_ERR_TIMEOUT and keeps the context usable.  No reference counterpart
+ * (the reference has no device waits). */
+int smd_set_wait_limit(smd_ctx *ctx, double seconds);
+/* Failure-path test hook, no reference counterpart: block `block` of the
+ * following dipole solves returns before its first grid-barrier arrival, so
+ * the other blocks' waits run out after the wait limit and the evaluation
+ * returns SMD_ERR_TIMEOUT.  -1 (the default) turns it off. */
+int smd_test_skip_arrival(smd_ctx *ctx, int block);
 /* Solver statistics of the last solve: iterations and final RMS change. */
 int smd_solver_stats(smd_ctx *ctx, int *iterations, double *rms_change);
 /* Lab-frame dipoles, quadrupoles, permanent field and induced dipoles of the
@@ -233,17 +246,24 @@ int smd_set_tuning(smd_ctx *ctx, int threads_per_site);
 /* Positions pos[3 n].  Once a pair list exists (and without shear), the list
  * is kept while every site stays within half the skin of where it was at the
  * last rebuild, minimum image, the same test a step makes; otherwise the next
- * step rebuilds it. */
+ * step rebuilds it.  A non-finite coordinate returns SMD_ERR_NAN and leaves
+ * the state unchanged (the reference would carry it into every force). */
 int smd_upload_positions(smd_ctx *ctx, const double *pos);
 /* vel: Atom::velocity; vtminus may be NULL (then set by smd_integrator_start) */
 int smd_upload_velocities(smd_ctx *ctx, const double *vel, const double *vtminus);
 int smd_download_state(smd_ctx *ctx, double *pos, double *vel, double *vtminus);
 
 /* ---- forces (Force::compute / compute_long, src/Force.h:59) ----------
- * Rebuilds the pair list from the current positions, evaluates the selected
- * terms and returns: force[3n] (the terms' contribution to Atom::force),
- * energy[SMD_E_COUNT] (NULL allowed), virial[9] (contribution to
- * Ensemble::virial + longVirial, i.e. +sum r_ij f_ij; NULL allowed). */
+ * Evaluates the selected terms at the current positions and returns:
+ * force[3n] (the terms' contribution to Atom::force), energy[SMD_E_COUNT]
+ * (NULL allowed), virial[9] (contribution to Ensemble::virial + longVirial,
+ * i.e. +sum r_ij f_ij; NULL allowed).  As in the reference's step, the pair
+ * list is rebuilt only once a site has moved half the skin since the last
+ * build (src/integrators/LFIntegrator.cpp:307-341), and the induced dipoles
+ * are solved once per configuration: SMD_TERM_IND_LONG after
+ * SMD_TERM_IND_SHORT on the same positions uses the dipoles that call solved,
+ * as Induction::compute_long uses those of Induction::compute.  The device
+ * output buffer is allocated on the first call and kept with the context. */
 int smd_compute_forces(smd_ctx *ctx, uint32_t terms, double *force, double *energy,
                        double *virial);
 /* Unordered pairs of the current Verlet list as (i < j) int32 pairs, the set
@@ -254,12 +274,15 @@ int smd_get_pairs(smd_ctx *ctx, int32_t *pairs, int64_t cap, int64_t *count);
  * host loop with a fixed memory budget, a process that must not call
  * cudaMalloc after set-up): the same evaluation and results, with the device
  * force buffer taken from a static array of 65536 x 3 doubles inside the
- * library instead of a cudaMalloc/cudaFree per call.  No reference
- * counterpart (the reference evaluates forces on the host).  Returns
- * SMD_ERR_ARG for systems of more than 65536 sites.  Calls that overlap on
- * one device (threads, or several contexts) share the array and race.  The
- * first call on a device resolves the array's address (cudaGetSymbolAddress)
- * with that device current; make that first call outside any stream capture. */
+ * library instead of the context's own buffer (which smd_compute_forces
+ * allocates on its first call).  No reference counterpart (the reference
+ * evaluates forces on the host).  Returns SMD_ERR_ARG for systems of more
+ * than 65536 sites.  Calls that overlap on one device (threads, or several
+ * contexts) share the array and race.  The first call on a device resolves
+ * the array's address (cudaGetSymbolAddress) with that device current, under
+ * a lock; make that first call outside any stream capture.  The address is
+ * forgotten when the device's last context is destroyed: after a device
+ * reset, destroy that device's contexts before creating new ones. */
 int smd_compute_forces_noalloc(smd_ctx *ctx, uint32_t terms, double *force, double *energy, double *virial);
 /* k-vector count of the Ewald reciprocal set (EwaldForce::set_up). */
 int smd_ewald_nk(smd_ctx *ctx, int *nk);

@@ -14,7 +14,10 @@ LIB_PATH = os.path.join(HERE, "libswinmd_b200.so")
 
 SMD_OK = 0
 ERRORS = {1: "SMD_ERR_ARG", 2: "SMD_ERR_CUDA", 3: "SMD_ERR_LIST_OVERFLOW", 4: "SMD_ERR_NH_ITER",
-          5: "SMD_ERR_SHAKE", 6: "SMD_ERR_NAN", 7: "SMD_ERR_CG", 8: "SMD_ERR_NO_DEVICE"}
+          5: "SMD_ERR_SHAKE", 6: "SMD_ERR_NAN", 7: "SMD_ERR_CG", 8: "SMD_ERR_NO_DEVICE",
+          9: "SMD_ERR_TIMEOUT"}
+SMD_ERR_ARG, SMD_ERR_CUDA, SMD_ERR_LIST_OVERFLOW, SMD_ERR_NH_ITER = 1, 2, 3, 4
+SMD_ERR_SHAKE, SMD_ERR_NAN, SMD_ERR_CG, SMD_ERR_NO_DEVICE, SMD_ERR_TIMEOUT = 5, 6, 7, 8, 9
 PREC_FP64, PREC_MIXED = 0, 1
 TERM_VDW, TERM_EWALD_REAL, TERM_EWALD_LONG, TERM_ALL = 1, 2, 4, 0xFFFF
 TERM_MP_SHORT, TERM_MP_LONG, TERM_IND_SHORT, TERM_IND_LONG = 8, 16, 32, 64
@@ -103,6 +106,8 @@ SIGNATURES = {
     "smd_set_solver": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
     "smd_set_preconditioner": (ctypes.c_int, [_P, ctypes.c_int]),
     "smd_solver_stats": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), _D]),
+    "smd_set_wait_limit": (ctypes.c_int, [_P, ctypes.c_double]),
+    "smd_test_skip_arrival": (ctypes.c_int, [_P, ctypes.c_int]),
     "smd_get_polarization": (ctypes.c_int, [_P, _D, _D, _D, _D]),
     "smd_set_induced": (ctypes.c_int, [_P, _D]),
     "smd_mlp_init": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_uint]),

@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <mutex>
 #include <new>
 #include <string>
 #include "smd_ctx.cuh"
@@ -13,6 +14,24 @@ using namespace smd;
 struct smd_ctx {
     Ctx c;
 };
+
+// ---- scratch of the force evaluation without device allocation ------------
+// The device output buffer of smd_compute_forces_noalloc lives in this
+// file-scope array instead of the context's buffer.  Nothing in it needs to
+// start at zero: the finalize kernel writes every element a call reads back.
+// One array per process and device: calls that overlap (two threads, or two
+// contexts on one device) share it and race.
+namespace {
+constexpr int NOALLOC_MAX_SITES = 65536;
+static __device__ __align__(256) double g_noalloc_force[3 * NOALLOC_MAX_SITES];
+constexpr int NOALLOC_MAX_DEVICES = 64;
+// the array's device address per device, resolved once with that device
+// current; cleared when the last context of the device is destroyed, so a
+// device reset followed by new contexts resolves it again
+std::mutex g_noalloc_mu;
+double *g_noalloc_addr[NOALLOC_MAX_DEVICES] = {nullptr};
+int g_live_ctx[NOALLOC_MAX_DEVICES] = {0};
+}  // namespace
 
 namespace {
 
@@ -41,6 +60,7 @@ int status_to_code(unsigned st) {
     if (st & ST_NAN) return SMD_ERR_NAN;
     if (st & (ST_SHAKE_ITER | ST_SHAKE_GEOM)) return SMD_ERR_SHAKE;
     if (st & ST_NH_ITER) return SMD_ERR_NH_ITER;
+    if (st & ST_WAIT_TIMEOUT) return SMD_ERR_TIMEOUT;
     if (st & ST_CG_ITER) return SMD_ERR_CG;
     return SMD_OK;
 }
@@ -51,6 +71,8 @@ const char *status_text(unsigned st) {
     if (st & ST_SHAKE_GEOM) return "SHAKE geometric failure";
     if (st & ST_SHAKE_ITER) return "SHAKE did not converge within maxCount";
     if (st & ST_NH_ITER) return "NH iteration Error";
+    if (st & ST_WAIT_TIMEOUT)
+        return "dipole solve: a grid-barrier wait ran out (solve blocks not all resident, or one never arrived)";
     if (st & ST_CG_ITER) return "dipole solve did not converge";
     return "";
 }
@@ -101,6 +123,7 @@ int alloc_list(smd_ctx *x) {
     c.list_valid = 0;
     c.list_built = 0;
     c.graph_dirty = 1;
+    touch(c);
     if (ensure_ind_rows(c)) return fail(x, SMD_ERR_CUDA, "dipole-solve tensor rows: allocation failed");
     return SMD_OK;
 }
@@ -120,13 +143,17 @@ int sync_status(smd_ctx *x) {
 // terms (LFIntegrator.cpp:440-458): multipoles short and long, then the
 // induced dipoles (solved once per step) short and long; all torques are
 // mapped onto the sites at the end (the mapping is linear in the torques).
-void enqueue_polar(Ctx &c, bool mp_short, bool mp_long, bool ind_short, bool ind_long) {
-    launch_frames(c);   // also the site records and cleared torques
+// solved: the induced dipoles (and the solve's tensor rows) already belong
+// to the current configuration, as after an earlier smd_compute_forces on
+// it; the reference's Induction::compute_long likewise uses the dipoles its
+// compute() solved (src/forces/Induction.cpp:567-590).
+void enqueue_polar(Ctx &c, bool mp_short, bool mp_long, bool ind_short, bool ind_long, bool solved = false) {
+    launch_frames(c);   // also the site records (with the current dipoles) and cleared torques
     const bool all = mp_short && mp_long && ind_short && ind_long && c.ind_on;
     if (all && polar_short_fused(c)) {
         // mixed path: the multipole real space does not feed the solve, so
         // it runs after it, fused with the induced real space
-        launch_ind_solve(c);
+        if (!solved) launch_ind_solve(c);
         launch_polar_short(c);
         launch_polar_long(c);
         launch_torques_end(c);
@@ -136,13 +163,13 @@ void enqueue_polar(Ctx &c, bool mp_short, bool mp_long, bool ind_short, bool ind
     if (all) {
         // a full evaluation: after the solve one pass gives all structure
         // factors and one reciprocal force pass serves both terms
-        launch_ind_solve(c);
+        if (!solved) launch_ind_solve(c);
         launch_ind_short(c);
         launch_polar_long(c);
     } else {
         if (mp_long) launch_mp_long(c);
         if (c.ind_on && (ind_short || ind_long)) {
-            launch_ind_solve(c);
+            if (!solved) launch_ind_solve(c);
             if (ind_short) launch_ind_short(c);
             if (ind_long) launch_ind_long(c);
         }
@@ -185,6 +212,72 @@ void enqueue_step(Ctx &c) {
     launch_integrate(c);
 }
 
+
+// One evaluation of the selected terms at the current positions into the
+// device buffer dforce (3N doubles, used only when force is given), then the
+// forces, energies and virial copied to the host.  The pair list is kept
+// while every site stays within half the skin of its last build (the test a
+// step makes); the induced dipoles are solved once per configuration.
+int compute_forces_into(smd_ctx *x, uint32_t terms, double *dforce, double *force, double *energy,
+                        double *virial) {
+    Ctx &c = x->c;
+    CK(cudaMemsetAsync(c.status, 0, sizeof(unsigned), c.stream));
+    const bool rebuild = !c.list_built;
+    launch_nlist(c, rebuild);
+    // smd_get_pairs returns the list of the current positions: a kept list
+    // (built at earlier positions) is rebuilt there first
+    c.list_valid = rebuild ? 1 : 0;
+    CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
+    CK(cudaMemsetAsync(c.frc, 0, 3 * (size_t)c.n * sizeof(long long), c.stream));
+    const int save_vdw = c.vdw, save_ew = c.ewald_on;
+    if (!(terms & SMD_TERM_VDW)) c.vdw = VDW_NONE;
+    bool want_real = (terms & SMD_TERM_EWALD_REAL) && c.ewald_on;
+    bool want_long = (terms & SMD_TERM_EWALD_LONG) && c.ewald_on;
+    c.ewald_on = want_real ? 1 : 0;
+    launch_pair(c);
+    if (want_real) launch_intra(c);
+    c.ewald_on = save_ew;
+    if (want_long) launch_recip(c);
+    c.vdw = save_vdw;
+    const uint32_t polar = SMD_TERM_MP_SHORT | SMD_TERM_MP_LONG | SMD_TERM_IND_SHORT | SMD_TERM_IND_LONG;
+    if (c.mp_on && (terms & polar)) {
+        const bool solved = c.ind_on && c.dip_version == c.cfg_version;
+        enqueue_polar(c, terms & SMD_TERM_MP_SHORT, terms & SMD_TERM_MP_LONG, terms & SMD_TERM_IND_SHORT,
+                      terms & SMD_TERM_IND_LONG, solved);
+    }
+    if (force) launch_finalize_forces(c, dforce);
+    long long hacc[ACC_COUNT];
+    CK(cudaMemcpyAsync(hacc, c.acc, sizeof(hacc), cudaMemcpyDeviceToHost, c.stream));
+    if (force) CK(cudaMemcpyAsync(force, dforce, 3 * (size_t)c.n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    const int rs = sync_status(x);
+    if (rs) {
+        c.dip_version = 0;   // a failed evaluation leaves no usable dipoles
+        return rs;
+    }
+    if (c.mp_on && c.ind_on && (terms & (SMD_TERM_IND_SHORT | SMD_TERM_IND_LONG)))
+        c.dip_version = c.cfg_version;   // solved now, or already before
+    const bool vdw = (terms & SMD_TERM_VDW) && c.vdw != VDW_NONE;
+    if (energy) {
+        for (int q = 0; q < SMD_E_COUNT; q++) energy[q] = 0;
+        energy[SMD_E_VDW] = (double)hacc[ACC_E_VDW] * ACC_INV + (vdw ? c.e_lrc : 0.0);
+        energy[SMD_E_REAL] = (double)hacc[ACC_E_REAL] * ACC_INV;
+        energy[SMD_E_LONG] = (double)hacc[ACC_E_LONG] * ACC_INV;
+        energy[SMD_E_CORRECT] = (want_real ? c.e_self : 0.0) + (double)hacc[ACC_E_SELF] * ACC_INV;
+        energy[SMD_E_MOLCORRECT] = (double)hacc[ACC_E_INTRA] * ACC_INV;
+        energy[SMD_E_SURF] = (double)hacc[ACC_E_SURF] * ACC_INV;
+        energy[SMD_E_POL_REAL] = (double)hacc[ACC_E_POL_REAL] * ACC_INV;
+        energy[SMD_E_POL_LONG] = (double)hacc[ACC_E_POL_LONG] * ACC_INV;
+        energy[SMD_E_POL_SELF] = (double)hacc[ACC_E_POL_SELF] * ACC_INV;
+        energy[SMD_E_POL_INTRA] = (double)hacc[ACC_E_POL_INTRA] * ACC_INV;
+    }
+    if (virial) {
+        for (int q = 0; q < 9; q++) {
+            virial[q] = ((double)hacc[ACC_VIR + q] + (double)hacc[ACC_LVIR + q]) * ACC_INV;
+            if (vdw && (q == 0 || q == 4 || q == 8)) virial[q] -= c.v_lrc;
+        }
+    }
+    return SMD_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -217,6 +310,10 @@ int smd_create(int device, smd_ctx **out) {
     cudaMemset(c.status, 0, sizeof(unsigned));
     cudaMemset(c.flags, 0, 4 * sizeof(int));
     cudaMemset(c.obs, 0, sizeof(smd_observables));
+    if (device < NOALLOC_MAX_DEVICES) {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        g_live_ctx[device]++;
+    }
     *out = x;
     return SMD_OK;
 }
@@ -234,10 +331,17 @@ void smd_destroy(smd_ctx *x) {
                     c.rc.sk, c.rc.kvec, c.clen2, c.type_mp, c.type_polar, c.mu, c.qd, c.trq, c.e0,
                     c.pind, c.cgw, c.cgs, c.cg_bar, c.vpos4, c.vfixq, c.fv, c.ind_rj, c.ind_rc, c.ind_cnt,
                     c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab, c.srec, c.phist, c.cg_blk,
-                    c.upload4};
+                    c.upload4, c.fout};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c.stream) cudaStreamDestroy(c.stream);
+    if (c.device >= 0 && c.device < NOALLOC_MAX_DEVICES) {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (--g_live_ctx[c.device] <= 0) {
+            g_live_ctx[c.device] = 0;
+            g_noalloc_addr[c.device] = nullptr;   // resolved again by the next context's first call
+        }
+    }
     delete x;
 }
 
@@ -325,6 +429,7 @@ int smd_set_topology(smd_ctx *x, int n, int ntypes, const int32_t *atom_type,
     c.list_valid = 0;
     c.list_built = 0;
     c.graph_dirty = 1;
+    touch(c);
     return alloc_list(x);
 }
 
@@ -347,6 +452,7 @@ int smd_set_exclusions(smd_ctx *x, const int32_t *offsets, const int32_t *partne
     c.list_valid = 0;
     c.list_built = 0;
     c.graph_dirty = 1;
+    touch(c);
     if (ensure_ind_rows(c)) return fail(x, SMD_ERR_CUDA, "dipole-solve tensor rows: allocation failed");
     return SMD_OK;
 }
@@ -419,6 +525,7 @@ int smd_set_vdw(smd_ctx *x, int kind, const double *params, int switch_on, doubl
     }
     CK(cudaMemcpy(c.pair_par, p.data(), p.size() * sizeof(double), cudaMemcpyHostToDevice));
     c.graph_dirty = 1;
+    touch(c);
     return SMD_OK;
 }
 
@@ -445,6 +552,7 @@ int smd_set_ewald(smd_ctx *x, double alpha, double kcut, double real_cut) {
     int r = setup_recip(c);
     if (r) return fail(x, r, "smd_set_ewald: reciprocal set-up failed");
     c.graph_dirty = 1;
+    touch(c);
     return SMD_OK;
 }
 
@@ -473,6 +581,7 @@ int smd_set_buff(smd_ctx *x, const double *params, double n, double m, double de
     CK(dalloc(&c.vfixq, c.n));
     CK(dalloc(&c.fv, 3 * (size_t)c.n));
     c.graph_dirty = 1;
+    touch(c);
     return SMD_OK;
 }
 
@@ -511,7 +620,7 @@ int smd_set_multipole(smd_ctx *x, const double *type_mp, const double *polar, do
     if (r) return fail(x, r, "smd_set_multipole: solver set-up failed");
     CK(dalloc(&c.cgs, 8 + 16 * (size_t)c.cg_blocks));
     CK(cudaMemset(c.cgs, 0, (8 + 16 * (size_t)c.cg_blocks) * sizeof(double)));
-    CK(dalloc(&c.cg_bar, 1));
+    CK(dalloc(&c.cg_bar, 2));
     if (c.ind_on) {
         CK(dalloc(&c.phist, 24 * n));
         CK(cudaMemset(c.flags + 2, 0, 2 * sizeof(int)));
@@ -520,6 +629,7 @@ int smd_set_multipole(smd_ctx *x, const double *type_mp, const double *polar, do
     r = setup_recip(c);
     if (r) return fail(x, r, "smd_set_multipole: reciprocal set-up failed");
     c.graph_dirty = 1;
+    touch(c);
     return SMD_OK;
 }
 
@@ -530,6 +640,7 @@ int smd_set_solver(smd_ctx *x, double tol, int max_iter, int guess) {
     x->c.cg_max_iter = max_iter;
     x->c.cg_guess = guess;
     x->c.graph_dirty = 1;
+    touch(x->c);
     return SMD_OK;
 }
 
@@ -538,6 +649,25 @@ int smd_set_preconditioner(smd_ctx *x, int kind) {
         return fail(x, SMD_ERR_ARG, "smd_set_preconditioner: kind must be SMD_PRECOND_SITE or SMD_PRECOND_MOLECULE");
     x->c.cg_precond = kind;
     x->c.graph_dirty = 1;
+    touch(x->c);
+    return SMD_OK;
+}
+
+int smd_set_wait_limit(smd_ctx *x, double seconds) {
+    if (!x || !(seconds > 0) || seconds > 600)
+        return fail(x, SMD_ERR_ARG, "smd_set_wait_limit: the limit must lie in (0, 600] s");
+    x->c.wait_ns = (unsigned long long)(seconds * 1e9);
+    if (x->c.wait_ns == 0) x->c.wait_ns = 1;
+    x->c.graph_dirty = 1;
+    return SMD_OK;
+}
+
+int smd_test_skip_arrival(smd_ctx *x, int block) {
+    if (!x || block < -1 || (block >= 0 && block >= x->c.cg_blocks))
+        return fail(x, SMD_ERR_ARG, "smd_test_skip_arrival: block must be -1 or a block of the dipole solve");
+    x->c.test_skip_block = block;
+    x->c.graph_dirty = 1;
+    touch(x->c);
     return SMD_OK;
 }
 
@@ -580,6 +710,7 @@ int smd_set_induced(smd_ctx *x, const double *p) {
     for (int i = 0; i < n; i++)
         for (int d = 0; d < 3; d++) h[(size_t)d * n + i] = p[3 * i + d];
     CK(cudaMemcpy(c.pind, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    touch(c);
     return SMD_OK;
 }
 
@@ -592,6 +723,7 @@ int smd_mlp_init(smd_ctx *x, int capacity_frames, unsigned int seed) {
     if (r) return fail(x, r, "smd_mlp_init: allocation failed");
     c.mlp_ready = 0;
     c.graph_dirty = 1;
+    touch(c);
     return SMD_OK;
 }
 
@@ -643,6 +775,7 @@ int smd_mlp_train(smd_ctx *x, int epochs, int batch, double lr, unsigned int see
     cudaFree(dperm);
     c.mlp_ready = 1;
     c.graph_dirty = 1;
+    touch(c);
     return sync_status(x);
 }
 
@@ -717,6 +850,7 @@ int smd_set_precision(smd_ctx *x, int mode) {
     x->c.precision = mode;
     if (x->c.n > 0 && x->c.pos4) launch_fixq(x->c);
     x->c.graph_dirty = 1;
+    touch(x->c);
     return SMD_OK;
 }
 
@@ -727,12 +861,16 @@ int smd_set_tuning(smd_ctx *x, int tpp) {
         return fail(x, SMD_ERR_ARG, "smd_set_tuning: threads per site must be a power of two <= 32");
     x->c.tpp = tpp;
     x->c.graph_dirty = 1;
+    touch(x->c);
     return SMD_OK;
 }
 
 int smd_upload_positions(smd_ctx *x, const double *pos) {
     if (!x || !pos || x->c.n == 0) return fail(x, SMD_ERR_ARG, "smd_upload_positions: bad arguments");
     Ctx &c = x->c;
+    for (int i = 0; i < 3 * c.n; i++)
+        if (!std::isfinite(pos[i]))
+            return fail(x, SMD_ERR_NAN, "smd_upload_positions: non-finite coordinate of site " + std::to_string(i / 3));
     std::vector<double4> p(c.n);
     for (int i = 0; i < c.n; i++)
         p[i] = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], (double)c.h_type[i]);
@@ -752,12 +890,16 @@ int smd_upload_positions(smd_ctx *x, const double *pos) {
     launch_fixq(c);
     CK(cudaStreamSynchronize(c.stream));
     c.list_valid = 0;   // smd_get_pairs builds a fresh list from these positions
+    touch(c);
     return SMD_OK;
 }
 
 int smd_upload_velocities(smd_ctx *x, const double *vel, const double *vtminus) {
     if (!x || !vel || x->c.n == 0) return fail(x, SMD_ERR_ARG, "smd_upload_velocities: bad arguments");
     Ctx &c = x->c;
+    for (int i = 0; i < 3 * c.n; i++)
+        if (!std::isfinite(vel[i]) || (vtminus && !std::isfinite(vtminus[i])))
+            return fail(x, SMD_ERR_NAN, "smd_upload_velocities: non-finite velocity of site " + std::to_string(i / 3));
     std::vector<double4> v(c.n), vm(c.n);
     for (int i = 0; i < c.n; i++) {
         v[i] = make_double4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], 1.0 / c.h_mass[i]);
@@ -793,72 +935,11 @@ int smd_compute_forces(smd_ctx *x, uint32_t terms, double *force, double *energy
     if (!x || x->c.n == 0 || x->c.box.L[0] <= 0) return fail(x, SMD_ERR_ARG, "smd_compute_forces: system not set up");
     Ctx &c = x->c;
     CK(cudaSetDevice(c.device));
-    CK(cudaMemsetAsync(c.status, 0, sizeof(unsigned), c.stream));
-    launch_nlist(c, true);
-    c.list_valid = 1;
-    CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
-    CK(cudaMemsetAsync(c.frc, 0, 3 * (size_t)c.n * sizeof(long long), c.stream));
-    const int save_vdw = c.vdw, save_ew = c.ewald_on;
-    if (!(terms & SMD_TERM_VDW)) c.vdw = VDW_NONE;
-    bool want_real = (terms & SMD_TERM_EWALD_REAL) && c.ewald_on;
-    bool want_long = (terms & SMD_TERM_EWALD_LONG) && c.ewald_on;
-    c.ewald_on = want_real ? 1 : 0;
-    launch_pair(c);
-    if (want_real) launch_intra(c);
-    c.ewald_on = save_ew;
-    if (want_long) launch_recip(c);
-    c.vdw = save_vdw;
-    if (c.mp_on && (terms & (SMD_TERM_MP_SHORT | SMD_TERM_MP_LONG | SMD_TERM_IND_SHORT | SMD_TERM_IND_LONG)))
-        enqueue_polar(c, terms & SMD_TERM_MP_SHORT, terms & SMD_TERM_MP_LONG, terms & SMD_TERM_IND_SHORT,
-                      terms & SMD_TERM_IND_LONG);
-    double *dforce = nullptr;
-    if (force) {
-        CK(cudaMalloc(&dforce, 3 * (size_t)c.n * sizeof(double)));
-        launch_finalize_forces(c, dforce);
-    }
-    long long hacc[ACC_COUNT];
-    CK(cudaMemcpyAsync(hacc, c.acc, sizeof(hacc), cudaMemcpyDeviceToHost, c.stream));
-    if (force) CK(cudaMemcpyAsync(force, dforce, 3 * (size_t)c.n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-    int rs = sync_status(x);
-    if (dforce) cudaFree(dforce);
-    if (rs) return rs;
-    const bool vdw = (terms & SMD_TERM_VDW) && c.vdw != VDW_NONE;
-    if (energy) {
-        for (int q = 0; q < SMD_E_COUNT; q++) energy[q] = 0;
-        energy[SMD_E_VDW] = (double)hacc[ACC_E_VDW] * ACC_INV + (vdw ? c.e_lrc : 0.0);
-        energy[SMD_E_REAL] = (double)hacc[ACC_E_REAL] * ACC_INV;
-        energy[SMD_E_LONG] = (double)hacc[ACC_E_LONG] * ACC_INV;
-        energy[SMD_E_CORRECT] = (want_real ? c.e_self : 0.0) + (double)hacc[ACC_E_SELF] * ACC_INV;
-        energy[SMD_E_MOLCORRECT] = (double)hacc[ACC_E_INTRA] * ACC_INV;
-        energy[SMD_E_SURF] = (double)hacc[ACC_E_SURF] * ACC_INV;
-        energy[SMD_E_POL_REAL] = (double)hacc[ACC_E_POL_REAL] * ACC_INV;
-        energy[SMD_E_POL_LONG] = (double)hacc[ACC_E_POL_LONG] * ACC_INV;
-        energy[SMD_E_POL_SELF] = (double)hacc[ACC_E_POL_SELF] * ACC_INV;
-        energy[SMD_E_POL_INTRA] = (double)hacc[ACC_E_POL_INTRA] * ACC_INV;
-    }
-    if (virial) {
-        for (int q = 0; q < 9; q++) {
-            virial[q] = ((double)hacc[ACC_VIR + q] + (double)hacc[ACC_LVIR + q]) * ACC_INV;
-            if (vdw && (q == 0 || q == 4 || q == 8)) virial[q] -= c.v_lrc;
-        }
-    }
-    return SMD_OK;
+    if (force && !c.fout) CK(dalloc(&c.fout, 3 * (size_t)c.n));   // once per context
+    return compute_forces_into(x, terms, c.fout, force, energy, virial);
 }
 
-// ---- force evaluation without device allocation ---------------------------
-// The device output buffer of smd_compute_forces_noalloc lives in this
-// file-scope array instead of a cudaMalloc'd buffer.  Nothing in it needs to
-// start at zero: the finalize kernel writes every element a call reads back.
-// One array per process and device: calls that overlap (two threads, or two
-// contexts on one device) share it and race.
 }  // extern "C"
-
-namespace {
-constexpr int NOALLOC_MAX_SITES = 65536;
-static __device__ __align__(256) double g_noalloc_force[3 * NOALLOC_MAX_SITES];
-constexpr int NOALLOC_MAX_DEVICES = 64;
-double *g_noalloc_addr[NOALLOC_MAX_DEVICES] = {nullptr};
-}  // namespace
 
 extern "C" {
 
@@ -873,58 +954,18 @@ int smd_compute_forces_noalloc(smd_ctx *x, uint32_t terms, double *force, double
     if (c.device < 0 || c.device >= NOALLOC_MAX_DEVICES)
         return fail(x, SMD_ERR_ARG, "smd_compute_forces_noalloc: device index out of range");
     CK(cudaSetDevice(c.device));
-    if (!g_noalloc_addr[c.device]) {
-        // once per device, with that device current
-        void *a = nullptr;
-        CK(cudaGetSymbolAddress(&a, g_noalloc_force));
-        g_noalloc_addr[c.device] = (double *)a;
-    }
-    double *dforce = g_noalloc_addr[c.device];
-    CK(cudaMemsetAsync(c.status, 0, sizeof(unsigned), c.stream));
-    launch_nlist(c, true);
-    c.list_valid = 1;
-    CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
-    CK(cudaMemsetAsync(c.frc, 0, 3 * (size_t)c.n * sizeof(long long), c.stream));
-    const int save_vdw = c.vdw, save_ew = c.ewald_on;
-    if (!(terms & SMD_TERM_VDW)) c.vdw = VDW_NONE;
-    bool want_real = (terms & SMD_TERM_EWALD_REAL) && c.ewald_on;
-    bool want_long = (terms & SMD_TERM_EWALD_LONG) && c.ewald_on;
-    c.ewald_on = want_real ? 1 : 0;
-    launch_pair(c);
-    if (want_real) launch_intra(c);
-    c.ewald_on = save_ew;
-    if (want_long) launch_recip(c);
-    c.vdw = save_vdw;
-    if (c.mp_on && (terms & (SMD_TERM_MP_SHORT | SMD_TERM_MP_LONG | SMD_TERM_IND_SHORT | SMD_TERM_IND_LONG)))
-        enqueue_polar(c, terms & SMD_TERM_MP_SHORT, terms & SMD_TERM_MP_LONG, terms & SMD_TERM_IND_SHORT,
-                      terms & SMD_TERM_IND_LONG);
-    if (force) launch_finalize_forces(c, dforce);
-    long long hacc[ACC_COUNT];
-    CK(cudaMemcpyAsync(hacc, c.acc, sizeof(hacc), cudaMemcpyDeviceToHost, c.stream));
-    if (force) CK(cudaMemcpyAsync(force, dforce, 3 * (size_t)c.n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-    int rs = sync_status(x);
-    if (rs) return rs;
-    const bool vdw = (terms & SMD_TERM_VDW) && c.vdw != VDW_NONE;
-    if (energy) {
-        for (int q = 0; q < SMD_E_COUNT; q++) energy[q] = 0;
-        energy[SMD_E_VDW] = (double)hacc[ACC_E_VDW] * ACC_INV + (vdw ? c.e_lrc : 0.0);
-        energy[SMD_E_REAL] = (double)hacc[ACC_E_REAL] * ACC_INV;
-        energy[SMD_E_LONG] = (double)hacc[ACC_E_LONG] * ACC_INV;
-        energy[SMD_E_CORRECT] = (want_real ? c.e_self : 0.0) + (double)hacc[ACC_E_SELF] * ACC_INV;
-        energy[SMD_E_MOLCORRECT] = (double)hacc[ACC_E_INTRA] * ACC_INV;
-        energy[SMD_E_SURF] = (double)hacc[ACC_E_SURF] * ACC_INV;
-        energy[SMD_E_POL_REAL] = (double)hacc[ACC_E_POL_REAL] * ACC_INV;
-        energy[SMD_E_POL_LONG] = (double)hacc[ACC_E_POL_LONG] * ACC_INV;
-        energy[SMD_E_POL_SELF] = (double)hacc[ACC_E_POL_SELF] * ACC_INV;
-        energy[SMD_E_POL_INTRA] = (double)hacc[ACC_E_POL_INTRA] * ACC_INV;
-    }
-    if (virial) {
-        for (int q = 0; q < 9; q++) {
-            virial[q] = ((double)hacc[ACC_VIR + q] + (double)hacc[ACC_LVIR + q]) * ACC_INV;
-            if (vdw && (q == 0 || q == 4 || q == 8)) virial[q] -= c.v_lrc;
+    double *dforce = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[c.device]) {
+            // once per device, with that device current
+            void *a = nullptr;
+            CK(cudaGetSymbolAddress(&a, g_noalloc_force));
+            g_noalloc_addr[c.device] = (double *)a;
         }
+        dforce = g_noalloc_addr[c.device];
     }
-    return SMD_OK;
+    return compute_forces_into(x, terms, dforce, force, energy, virial);
 }
 
 int smd_get_pairs(smd_ctx *x, int32_t *pairs, int64_t cap, int64_t *count) {
@@ -990,6 +1031,7 @@ int smd_set_integrator(smd_ctx *x, const smd_integrator_params *p) {
     if (c.ip.mol_ndf <= 0) c.ip.mol_ndf = 3 * c.nmol - 3;
     c.integrator_ready = 1;
     c.graph_dirty = 1;
+    touch(c);
     return SMD_OK;
 }
 
@@ -1006,6 +1048,7 @@ int smd_set_constraints(smd_ctx *x, const double *len2) {
     CK(dalloc(&c.clen2, 3 * (size_t)c.nmol));
     CK(cudaMemcpy(c.clen2, len2, 3 * (size_t)c.nmol * sizeof(double), cudaMemcpyHostToDevice));
     c.graph_dirty = 1;
+    touch(c);
     return SMD_OK;
 }
 
@@ -1033,6 +1076,7 @@ int smd_integrator_start(smd_ctx *x) {
         launch_start_velocities(c);
     }
     c.steps_done = 0;
+    touch(c);
     return sync_status(x);
 }
 
@@ -1053,6 +1097,7 @@ int smd_run(smd_ctx *x, int nsteps) {
     }
     for (int s = 0; s < nsteps; s++) CK(cudaGraphLaunch(c.step_graph, c.stream));
     c.steps_done += nsteps;
+    if (nsteps > 0) touch(c);
     return sync_status(x);
 }
 
@@ -1135,6 +1180,7 @@ int smd_profile_stages(smd_ctx *x, int reps, double *out) {
     cudaFree(b_pos); cudaFree(b_vel); cudaFree(b_vtm); cudaFree(b_disp);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    touch(c);
     return sync_status(x);
 }
 
@@ -1183,6 +1229,7 @@ int smd_run_timed(smd_ctx *x, int nsteps, double *device_ms) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c.steps_done += nsteps;
+    if (nsteps > 0) touch(c);
     return sync_status(x);
 }
 
@@ -1204,6 +1251,7 @@ int smd_set_series_capacity(smd_ctx *x, int cap) {
         CK(cudaMemset(c.series, 0, (size_t)cap * 5 * sizeof(double)));
     }
     c.graph_dirty = 1;
+    touch(c);
     return SMD_OK;
 }
 
@@ -1355,6 +1403,7 @@ int smd_batch_autotune(smd_batch *b, int reps, int32_t *tpp_out) {
         }
         c.tpp = best_t;
         c.graph_dirty = 1;
+        touch(c);
         if (tpp_out) tpp_out[r] = best_t;
         // the step expects the full forces of the current positions
         BCK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
@@ -1391,7 +1440,10 @@ int smd_batch_run(smd_batch *b, int nsteps, double *device_ms) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
     }
-    for (smd_ctx *x : b->reps) x->c.steps_done += nsteps;
+    for (smd_ctx *x : b->reps) {
+        x->c.steps_done += nsteps;
+        if (nsteps > 0) touch(x->c);
+    }
     return batch_status(b);
 }
 

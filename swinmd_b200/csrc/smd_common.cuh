@@ -60,7 +60,9 @@ enum StatusBits {
     ST_NAN = 8,              // non-finite force or position
     ST_CELL_RANGE = 16,      // site outside the cell grid after clamping
     ST_CG_ITER = 32,         // dipole solver did not converge
-    ST_SHAKE_GEOM = 64       // SHAKE geometric failure (reference LFIntegrator.cpp:1758)
+    ST_SHAKE_GEOM = 64,      // SHAKE geometric failure (reference LFIntegrator.cpp:1758)
+    ST_WAIT_TIMEOUT = 128    // a bounded device-side wait (the dipole solve's grid
+                             // barrier) ran out: blocks not co-resident or one missing
 };
 
 // integrator scalars shared by several files (ctx->scal): 0-7 belong to the

@@ -112,7 +112,9 @@ struct Ctx {
     int cg_blocks = 0;
     int cg_precond = SMD_PRECOND_MOLECULE;  // dipole-solve preconditioner
     double *cg_blk = nullptr;       // [nmol][81] inverse molecule blocks of A
-    unsigned int *cg_bar = nullptr; // grid-barrier counter
+    unsigned int *cg_bar = nullptr; // grid barrier: [0] counter, [1] abort word of the launch
+    unsigned long long wait_ns = 1000000000ull;  // limit of one device-side barrier wait (1 s)
+    int test_skip_block = -1;       // failure-path test: solve block that never arrives
     int *ind_rj = nullptr;          // damped-tensor rows of the solve: partners [N][cap]
     void *ind_rc = nullptr;         // coefficients [N][cap] (float4 or double4)
     int *ind_cnt = nullptr;         // row lengths [N]
@@ -157,6 +159,12 @@ struct Ctx {
     int list_valid = 0;
     int list_built = 0;      // a pair list exists for the current set-up (its sites may have moved within the skin)
     double4 *upload4 = nullptr;  // staging of uploaded positions
+    double *fout = nullptr;      // [3N] device force output of smd_compute_forces, allocated once
+    // configuration version: bumped by every call that moves the sites or
+    // changes the model or the solver; smd_compute_forces solves the induced
+    // dipoles only when they were not solved for the current version
+    long long cfg_version = 1;
+    long long dip_version = 0;
     // CUDA graph of one step
     cudaGraphExec_t step_graph = nullptr;
     int graph_dirty = 1;
@@ -185,6 +193,7 @@ void launch_ind_short(Ctx &c);
 void launch_mp_mol(Ctx &c);
 bool polar_short_fused(const Ctx &c);
 void launch_polar_short(Ctx &c);
+inline void touch(Ctx &c) { c.cfg_version++; }
 void launch_ind_long(Ctx &c);
 void launch_polar_long(Ctx &c);
 void launch_torques_end(Ctx &c);

@@ -280,31 +280,48 @@ __global__ void __launch_bounds__(256) k_ind_field_f(IndArgs a, FieldMixArgs m, 
 // (A v)_i = v_i / a_i - sum_j T_ij v_j over the site's tensor row (the
 // Verlet-list neighbours and the molecule's other sites within cutoffInd)
 
-// Grid barrier with a bounded spin: every block of the (co-resident)
-// cooperative launch arrives once per phase (release add), then polls the
-// counter with acquire loads; a block that waits longer than the cap raises
-// ST_CG_ITER and returns false, and the caller stops.
+// Grid barrier with a bounded wait: every block of the (co-resident)
+// cooperative launch arrives once per phase (release add on bar[0]), then
+// polls the counter with acquire loads.  A block that has waited longer than
+// limit_ns (device global timer) raises ST_WAIT_TIMEOUT, sets this launch's
+// abort word bar[1] and returns false; blocks still waiting see the abort
+// word and return false too, and every caller then leaves the kernel.  Both
+// words are cleared before each launch, so an earlier launch's failure (or a
+// solve that ran out of iterations) never cuts a later solve short.
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned int *p) {
     unsigned v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ bool grid_barrier(unsigned int *bar, unsigned int target, unsigned int *status) {
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ bool grid_barrier(unsigned int *bar, unsigned int target, unsigned int *status,
+                             unsigned long long limit_ns) {
     __shared__ int s_ok;   // thread 0's outcome: every thread of the block takes the same branch
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
         asm volatile("red.release.gpu.global.add.u32 [%0], 1;" : : "l"(bar) : "memory");
-        unsigned int spins = 0;
+        const unsigned long long t0 = global_ns();
+        int ok = 1;
         while (ld_acquire_u32(bar) < target) {
-            __nanosleep(32);
-            if (++spins > (1u << 25)) {  // ~1 s
-                atomicOr(status, ST_CG_ITER);
+            if (ld_acquire_u32(bar + 1) != 0) {   // another block gave up
+                ok = 0;
+                break;
+            }
+            __nanosleep(64);
+            if (global_ns() - t0 > limit_ns) {
+                atomicExch(bar + 1, 1u);
+                atomicOr(status, ST_WAIT_TIMEOUT);
+                ok = 0;
                 break;
             }
         }
         __threadfence();
-        s_ok = (*(volatile unsigned int *)status & ST_CG_ITER) == 0;
+        s_ok = ok;
     }
     __syncthreads();
     return s_ok != 0;
@@ -318,7 +335,9 @@ struct CGArgs {
     void *g0, *g1;           // per-site packed copies (float4 / double4) of the start dipoles and of v
     double *part;            // partials [4][nblocks][4]
     double *scal;            // [0] iterations, [1] final rms change
-    unsigned *bar, *status;
+    unsigned *bar, *status;          // bar[0] barrier counter, bar[1] abort word
+    unsigned long long wait_ns;      // limit of one barrier wait
+    int skip_block;                  // failure-path test: this block never arrives (-1: none)
     int nblocks, max_iter, guess;
     double tol;
     const double *blk;       // [nmol][81] inverse molecule blocks of A (molecule preconditioner)
@@ -640,6 +659,10 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
     const int passes = (n + sites_per_pass - 1) / sites_per_pass;
     unsigned int phase = 0;
     double tot[4];
+    // failure-path test hook: this block leaves before its first arrival, so
+    // the other blocks' first barrier wait runs out (nothing else is skipped:
+    // it has written nothing yet)
+    if ((int)blockIdx.x == c.skip_block) return;
     // every write of a dipole component also goes to the site records, so
     // that they hold the solution when the solve ends
     auto put_p = [&](int i, int d, double v) {
@@ -671,7 +694,7 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
             g0[i] = G4{(GR)p3[0], (GR)p3[1], (GR)p3[2], (GR)0};
         }
     }
-    if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
+    if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status, c.wait_ns)) return;
     // r = E0 - A x ; u = M^-1 r ; gamma = r.u
     double vals[4] = {0, 0, 0, 0};
     for (int ps = 0; ps < passes; ps++) {
@@ -693,7 +716,7 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
     }
     if (BJ) {
         // u = B^-1 r per molecule, once every site's residual is in place
-        if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
+        if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status, c.wait_ns)) return;
         mol_tiles<G4, GR>(a, c.blk, g1, s_bv, s_bu, [&](int, int, int, int idx) { return __ldcg(&c.r[idx]); },
                           [&](int, int, int, int idx, double r, double u) {
                               c.u[idx] = u;
@@ -701,7 +724,7 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
                           });
     }
     block_partials(vals, 1, pu1, s_w);
-    if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
+    if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status, c.wait_ns)) return;
     // w = A u ; delta = w.u
     vals[0] = 0;
     for (int ps = 0; ps < passes; ps++) {
@@ -714,15 +737,20 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
         }
     }
     block_partials(vals, 1, pw1, s_w);
-    if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
+    if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status, c.wait_ns)) return;
     grid_sum(pu1, c.nblocks, 1, tot, s_w);
     double gamma = tot[0];
     grid_sum(pw1, c.nblocks, 1, tot, s_w);
     double alpha_cg = gamma / tot[0], beta = 0.0;
     int it = 0;
     double rms = 0;
+    bool conv = false;   // the RMS change fell below the tolerance (or r = 0 exactly)
     for (; it < c.max_iter; it++) {
-        if (!(gamma > 0) || !(alpha_cg > 0)) break;
+        if (!(gamma > 0)) {   // r.u = 0: the start already solves A p = E0
+            conv = gamma == 0.0;
+            break;
+        }
+        if (!(alpha_cg > 0)) break;   // breakdown (A not positive definite or non-finite)
         // U: p = u + beta p ; s = w + beta s ; x += alpha p ; r -= alpha s ;
         //    u = M^-1 r ; gamma' = r.u ; |alpha p|^2
         vals[0] = 0; vals[1] = 0;
@@ -768,11 +796,15 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
         }
         double *const pu = (it & 1) ? pu1 : pu0;
         block_partials(vals, 2, pu, s_w);
-        if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
+        if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status, c.wait_ns)) return;
         grid_sum(pu, c.nblocks, 2, tot, s_w);
         const double gamma_new = tot[0];
         rms = sqrt(tot[1] / (3.0 * n));
-        if (rms < c.tol) { it++; break; }
+        if (rms < c.tol) {
+            conv = true;
+            it++;
+            break;
+        }
         // W: w = A u ; delta' = w.u
         vals[0] = 0;
         for (int ps = 0; ps < passes; ps++) {
@@ -786,7 +818,7 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
         }
         double *const pw = (it & 1) ? pw1 : pw0;
         block_partials(vals, 1, pw, s_w);
-        if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status)) return;
+        if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status, c.wait_ns)) return;
         grid_sum(pw, c.nblocks, 1, tot, s_w);
         const double delta = tot[0];
         beta = gamma_new / gamma;
@@ -796,7 +828,7 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         c.scal[0] = it;
         c.scal[1] = rms;
-        if (it >= c.max_iter) atomicOr(c.status, ST_CG_ITER);
+        if (!conv) atomicOr(c.status, ST_CG_ITER);
     }
 }
 
@@ -1493,6 +1525,8 @@ void launch_ind_cg(Ctx &c) {
     g.g0 = c.cgw + 12 * n; g.g1 = c.cgw + 16 * n;
     g.s = c.cgw + 20 * n; g.u = c.cgw + 23 * n;
     g.part = c.cgs + 8; g.scal = c.cgs; g.bar = c.cg_bar; g.status = c.status;
+    g.wait_ns = c.wait_ns;
+    g.skip_block = c.test_skip_block;
     g.nblocks = c.cg_blocks; g.max_iter = c.cg_max_iter; g.tol = c.cg_tol;
     // 0: start from alpha E0; 1: start from the dipoles in p (previous solve or network)
     g.guess = (c.cg_guess == SMD_GUESS_PREVIOUS || learned) ? 1 : 0;
@@ -1500,7 +1534,7 @@ void launch_ind_cg(Ctx &c) {
     g.blk = c.cg_blk;
     // the mixed path's site records take the dipoles inside the solve
     g.srec = f32 && c.srec ? (float *)c.srec : nullptr;
-    cudaMemsetAsync(c.cg_bar, 0, sizeof(unsigned int), c.stream);
+    cudaMemsetAsync(c.cg_bar, 0, 2 * sizeof(unsigned int), c.stream);   // counter and abort word
     // cooperative launch: the runtime refuses it unless every block can be
     // resident at once, which the grid barrier relies on
     cudaLaunchConfig_t cfg = {};

@@ -212,6 +212,22 @@ def buff_long_range_correction(s: System, box: float) -> tuple:
 # the GPU system
 # ---------------------------------------------------------------------------
 
+def refuse_unsupported(c) -> None:
+    """Raises for configuration options the GPU path does not compute, so a
+    caller never gets different physics with a success status: the
+    surface-dipole corrections (``surfCorrect``: EwaldForce.cpp:816-937,
+    Multipole.cpp:1753-1920, Induction.cpp:2188-2380), the AMOEBA damping
+    branch of the induced real space (``dampAMOEBA``, Induction.cpp:1051-1079)
+    and the Wolf summation (WolfForce.cpp)."""
+    if c.surface_correct:
+        raise NotImplementedError("surface-dipole correction (surfCorrect) is not built on the GPU path")
+    if c.compute_multipole and c.compute_induction and c.damp_amoeba:
+        raise NotImplementedError("AMOEBA damping of the induced real space (dampAMOEBA) is not built on "
+                                  "the GPU path")
+    if c.compute_wolf:
+        raise NotImplementedError("Wolf summation (computeWolf) is not built on the GPU path")
+
+
 class GpuEnsemble:
     """One system on one GPU behind the C ABI (the role of ``Ensemble``)."""
 
@@ -221,6 +237,7 @@ class GpuEnsemble:
         self.lib = L.load()
         self.system = s = system
         self.n = s.n_atoms
+        refuse_unsupported(s.config)
         ctx = ctypes.c_void_p()
         code = self.lib.smd_create(device, ctypes.byref(ctx))
         if code != L.SMD_OK:

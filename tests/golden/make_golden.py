@@ -8,6 +8,10 @@ the CPU oracle are checked against these files; the reference itself is not
 needed to run the tests.
 
     make -C oracle && python tests/golden/make_golden.py [case ...]
+
+With no case names it makes the small cases; ``all`` adds the full-size
+benchmark configurations (polwater4096 needs about 12 GB of memory and a
+few minutes of one core).
 """
 import os
 import sys
@@ -19,9 +23,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.dirname(HERE))
 
 from swinmd_b200 import systems  # noqa: E402
 import refdump  # noqa: E402
+from conftest import pair_digest  # noqa: E402
 
 
 def lj500():
@@ -46,11 +52,39 @@ def polwater216():
     return s, [("forces",), ("run", 10)]
 
 
+# Full-size cases: the configurations the benchmark runs.  Their pair sets
+# are stored as a count and a SHA-256 of the sorted (i < j) int32 pairs
+# instead of the pairs themselves, which would take megabytes.
+def lj4000():
+    s = systems.lj_fluid(ncell=10, seed=1, n_steps=20)
+    s.config.long_correct = True
+    return s, [("forces",), ("run", 20)]
+
+
+def nacl8000_mie():
+    s = systems.nacl_melt(ncell=20, potential="mie", kmax=10, seed=1)
+    return s, [("forces",), ("mie",)]
+
+
+def spce2160():
+    s = systems.spce_water(nmol=2160, box=4.03, cutoff=1.0, kmax=9, seed=1, n_steps=20)
+    return s, [("forces",), ("run", 20)]
+
+
+def polwater4096():
+    # the benchmark's polarisable water (|n| < 18); one force evaluation with
+    # the reference's dipoles solved to its own tolerance (|r| < 1e-14)
+    s = systems.polarizable_water(nmol=4096, kmax=18, seed=1)
+    return s, [("forces",)]
+
+
 CASES = {"lj500": lj500, "nacl1000_mie": nacl1000_mie, "spce512": spce512,
          "polwater216": polwater216}
+LARGE = {"lj4000": lj4000, "nacl8000_mie": nacl8000_mie, "spce2160": spce2160,
+         "polwater4096": polwater4096}
 
 
-def pack(name, s, results):
+def pack(name, s, results, large=False):
     out = {
         "box": np.array(results["forces"]["box"]),
         "pos": s.pos.astype(np.float64),
@@ -60,10 +94,17 @@ def pack(name, s, results):
     f = results["forces"]
     for k, v in f.items():
         if k in ("pairs",):
+            if large:
+                cnt, dig = pair_digest(v.reshape(-1, 2))
+                out["pair_count"] = np.array(cnt, np.int64)
+                out["pair_sha256"] = np.array(dig)
+                continue
             p = v.astype(np.int32).reshape(-1, 2)
             p = p[np.lexsort((p[:, 1], p[:, 0]))]
             out["pairs"] = p
         elif k in ("mass", "scaled_charge", "type", "molid", "init_pos"):
+            continue
+        elif large and k in ("ind_E0", "init_vel", "mp_quad", "mp_dip"):
             continue
         else:
             out["f_" + k] = v
@@ -74,21 +115,28 @@ def pack(name, s, results):
     if "run" in results:
         for k, v in results["run"].items():
             if k.startswith(("step_", "final_", "start_")):
+                # full-size runs keep the per-step series, the final state and
+                # the small records (energies, virials)
+                if large and v.size > 64 and k not in ("final_pos", "final_vel"):
+                    continue
                 out["r_" + k] = v
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
 
 
 def main(names):
     for name in names:
-        s, modes = CASES[name]()
+        s, modes = {**CASES, **LARGE}[name]()
         with tempfile.TemporaryDirectory() as d:
             systems.write_reference_case(s, d)
             results = {}
             for m in modes:
                 results[m[0]] = refdump.run_ref(d, *m, out=f"{m[0]}.txt")
-        pack(name, s, results)
+        pack(name, s, results, large=name in LARGE)
         print(name, "ok")
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or list(CASES))
+    args = sys.argv[1:] or list(CASES)
+    if args == ["all"]:
+        args = list(CASES) + list(LARGE)
+    main(args)

@@ -1,0 +1,21 @@
+"""Options the GPU path does not compute are refused before any device
+work, instead of running with different physics (CPU only)."""
+import pytest
+
+from swinmd_b200 import engine, systems
+
+
+def _pw():
+    return systems.polarizable_water(nmol=8, kmax=3, seed=1)
+
+
+@pytest.mark.parametrize("field", ["surface_correct", "damp_amoeba", "compute_wolf"])
+def test_unsupported_options_refused(field):
+    s = _pw()
+    setattr(s.config, field, True)
+    with pytest.raises(NotImplementedError):
+        engine.refuse_unsupported(s.config)
+
+
+def test_default_options_accepted():
+    engine.refuse_unsupported(_pw().config)

@@ -1,0 +1,203 @@
+"""The benchmark configurations at full size on the GPU against the
+reference's own FP64 results for the same seeded systems
+(tests/golden/make_golden.py, full-size cases):
+
+  lj4000        LJ fluid, 4000 atoms: pair set, forces, 20 leap-frog NH steps
+  nacl8000_mie  NaCl melt, 8000 ions, Mie 14-7 + Ewald (|n| < 10): pair set,
+                each term's forces, energy and virial
+  spce2160      rigid SPC/E water, 2160 molecules, Ewald |n| < 9 + SHAKE: pair
+                set, each term, 20 steps
+  polwater4096  the benchmark's polarisable water (12 288 sites, |n| < 18):
+                pair set, each term's forces, energy and the induced dipoles
+                against the reference's tightly solved ones
+
+FP64 path: RMS relative force error <= 1e-9 (1e-10 for the pair terms); mixed
+path: <= 1e-6 per term and in total, the matched-error bound of the benchmark.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden, pair_digest, rms_rel
+from swinmd_b200 import engine, systems
+from swinmd_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+
+DIPOLE_TOL = 2.0819e-8   # 1e-6 D in e nm, the benchmark's solver tolerance
+
+
+def _lj4000():
+    s = systems.lj_fluid(ncell=10, seed=1, n_steps=20)
+    s.config.long_correct = True
+    return s
+
+
+def _nacl8000():
+    return systems.nacl_melt(ncell=20, potential="mie", kmax=10, seed=1)
+
+
+def _spce2160():
+    return systems.spce_water(nmol=2160, box=4.03, cutoff=1.0, kmax=9, seed=1, n_steps=20)
+
+
+def _polwater4096():
+    return systems.polarizable_water(nmol=4096, kmax=18, seed=1)
+
+
+def _check_inputs(s, g):
+    # the generator reproduces the fixture's configuration exactly
+    assert np.array_equal(s.pos, g["pos"])
+    assert np.array_equal(s.atom_type, g["atom_type"])
+
+
+@pytest.mark.parametrize("make,name", [(_lj4000, "lj4000"), (_nacl8000, "nacl8000_mie"),
+                                       (_spce2160, "spce2160"), (_polwater4096, "polwater4096")])
+def test_pair_sets(make, name):
+    g = golden(name)
+    s = make()
+    _check_inputs(s, g)
+    ens = engine.GpuEnsemble(s)
+    cnt, dig = pair_digest(ens.pairs())
+    ens.close()
+    assert cnt == int(g["pair_count"])
+    assert dig == str(g["pair_sha256"])
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 1e-6)])
+def test_lj4000_forces(precision, tol):
+    g = golden("lj4000")
+    ens = engine.GpuEnsemble(_lj4000(), precision=precision)
+    f, e, w = ens.compute_forces(L.TERM_VDW)
+    err = rms_rel(f, g["f_lj_force"])
+    print(precision, "lj4000 force", err)
+    assert err < tol
+    assert abs(e[L.E_VDW] - g["f_lj_energy"][0]) < max(tol, 1e-12) * abs(g["f_lj_energy"][0])
+    assert np.max(np.abs(w - g["f_lj_virial"])) < max(tol, 1e-11) * np.linalg.norm(g["f_lj_virial"])
+    ens.close()
+
+
+def test_lj4000_trajectory():
+    g = golden("lj4000")
+    ens = engine.GpuEnsemble(_lj4000())
+    lf = engine.LFIntegrator(ens, series_capacity=32)
+    lf.start()
+    lf.run(20)
+    ser = lf.series()
+    assert np.allclose(ser[:, 0], g["r_step_epot"], rtol=1e-10)
+    assert np.allclose(ser[:, 2], g["r_step_atomtemp"], rtol=1e-10)
+    assert np.allclose(ser[:, 3], g["r_step_zeta"], rtol=1e-8, atol=1e-14)
+    st = ens.state()
+    assert np.allclose(st["pos"].reshape(-1), g["r_final_pos"], rtol=0, atol=1e-10)
+    assert np.allclose(st["vel"].reshape(-1), g["r_final_vel"], rtol=0, atol=1e-9)
+    assert lf.observables().list_updates == int(g["r_step_nupdates"][-1])
+    ens.close()
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-6)])
+def test_nacl8000_terms(precision, tol):
+    g = golden("nacl8000_mie")
+    ens = engine.GpuEnsemble(_nacl8000(), precision=precision)
+    assert ens.ewald_nk() == int(g["f_ewald_nk"][0])
+    f_tot = np.zeros((ens.n, 3))
+    for term, key, slot, eidx in ((L.TERM_VDW, "m_mie", L.E_VDW, 0),
+                                  (L.TERM_EWALD_REAL, "f_ewald_short", L.E_REAL, 1),
+                                  (L.TERM_EWALD_LONG, "f_ewald_long", L.E_LONG, 2)):
+        f, e, w = ens.compute_forces(term)
+        f_tot += f
+        err = rms_rel(f, g[key + "_force"])
+        ref_e = g[key + "_energy"][eidx]
+        print(precision, key, err, e[slot], ref_e)
+        assert err < tol
+        assert abs(e[slot] - ref_e) < tol * abs(ref_e)
+    ref = sum(g[k + "_force"] for k in ("m_mie", "f_ewald_short", "f_ewald_long"))
+    assert rms_rel(f_tot, ref) < tol
+    ens.close()
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-6)])
+def test_spce2160_terms(precision, tol):
+    g = golden("spce2160")
+    ens = engine.GpuEnsemble(_spce2160(), precision=precision)
+    assert ens.ewald_nk() == int(g["f_ewald_nk"][0])
+    for term, key, slot, eidx in ((L.TERM_VDW, "f_lj", L.E_VDW, 0),
+                                  (L.TERM_EWALD_REAL, "f_ewald_short", L.E_REAL, 1),
+                                  (L.TERM_EWALD_LONG, "f_ewald_long", L.E_LONG, 2)):
+        f, e, w = ens.compute_forces(term)
+        err = rms_rel(f, g[key + "_force"])
+        ref_e = g[key + "_energy"][eidx]
+        print(precision, key, err, e[slot], ref_e)
+        assert err < tol
+        assert abs(e[slot] - ref_e) < tol * abs(ref_e)
+    ens.close()
+
+
+def test_spce2160_trajectory():
+    g = golden("spce2160")
+    ens = engine.GpuEnsemble(_spce2160())
+    lf = engine.LFIntegrator(ens, series_capacity=32)
+    lf.start()
+    lf.run(20)
+    ser = lf.series()
+    print(np.max(np.abs(ser[:, 0] / g["r_step_epot"] - 1)))
+    assert np.allclose(ser[:, 0], g["r_step_epot"], rtol=1e-8)
+    assert np.allclose(ser[:, 2], g["r_step_atomtemp"], rtol=1e-8)
+    st = ens.state()
+    assert np.allclose(st["pos"].reshape(-1), g["r_final_pos"], rtol=0, atol=1e-8)
+    ens.close()
+
+
+POL_TERMS = ((L.TERM_VDW, "f_buff", L.E_VDW, 0), (L.TERM_MP_SHORT, "f_mp_short", L.E_REAL, 1),
+             (L.TERM_MP_LONG, "f_mp_long", L.E_LONG, 2), (L.TERM_IND_SHORT, "f_ind_short", L.E_POL_REAL, 6),
+             (L.TERM_IND_LONG, "f_ind_long", L.E_POL_LONG, 7))
+
+
+@pytest.fixture(scope="module")
+def pw_golden():
+    return golden("polwater4096")
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-6)])
+def test_polwater4096_terms_tight_dipoles(pw_golden, precision, tol):
+    """Each term at full size with the dipoles solved tightly (RMS change
+    1e-13 e nm) against the reference's dipoles (its CG to |r| < 1e-14)."""
+    g = pw_golden
+    s = _polwater4096()
+    _check_inputs(s, g)
+    ens = engine.GpuEnsemble(s, precision=precision)
+    ens.set_solver(tol=1e-13, max_iter=2000)
+    f_tot = np.zeros((ens.n, 3))
+    for term, key, slot, eidx in POL_TERMS:
+        f, e, w = ens.compute_forces(term)
+        f_tot += f
+        err = rms_rel(f, g[key + "_force"])
+        ref_e = g[key + "_energy"][eidx]
+        print(precision, key, "force", err, "energy", e[slot], ref_e)
+        assert err < tol
+        assert abs(e[slot] - ref_e) < tol * abs(ref_e)
+        if term == L.TERM_IND_SHORT:
+            p_err = rms_rel(ens.polarization()["p"], g["f_ind_P"])
+            print(precision, "dipoles", p_err, ens.solver_stats())
+            assert p_err < (1e-10 if precision == "fp64" else 1e-6)
+    ref = sum(g[k + "_force"] for _, k, _, _ in POL_TERMS)
+    err = rms_rel(f_tot, ref)
+    print(precision, "total", err)
+    assert err < tol
+    ens.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_polwater4096_working_tolerance(pw_golden, precision):
+    """The benchmark's arms solve to 1e-6 D RMS: the full evaluation (both arms'
+    code path: one call for every term) stays within the matched-error bound of
+    1e-6 RMS relative against the reference's tightly solved forces."""
+    g = pw_golden
+    ens = engine.GpuEnsemble(_polwater4096(), precision=precision)
+    ens.set_solver(tol=DIPOLE_TOL, max_iter=500)
+    f, e, w = ens.compute_forces()
+    ref = sum(g[k + "_force"] for _, k, _, _ in POL_TERMS)
+    err = rms_rel(f, ref)
+    it, rms = ens.solver_stats()
+    print(precision, "full evaluation at the working tolerance", err, "iterations", it, "rms change", rms)
+    assert rms < DIPOLE_TOL
+    assert err < 1e-6
+    ens.close()
