@@ -1,17 +1,27 @@
 """Benchmark of the SwinMD B200 step: ns/day of one system on each GPU.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload polwater4096|lj4000]
+                    [--workload polwater4096|lj4000|replicas64]
 
 Default workload: rigid polarisable multipole water, 4096 molecules (12,288
-sites), the configuration the headline metric is quoted on.  Two arms are
-timed on the same system:
-  plain   FP64 pair/reciprocal/dipole arithmetic, dipole solve started from
-          the molecule-block solution M^-1 E0;
-  fast    the learned initial guess (per-site network trained beforehand, on
-          the GPU, on dipoles the solver itself converged) + the mixed path.
-Both solve the dipoles to the same tolerance (RMS change 1e-6 D).  `value`
-is the fast arm's ns/day; the plain arm and their ratio are reported beside.
+sites), the configuration the headline metric is quoted on.  The seeded
+start (random orientations) is equilibrated on the GPU first.  Arms, timed
+one after another on the same trajectory:
+  plain                  FP64 throughout, the same algorithms as the fast arm
+                         (column reciprocal passes with exact integer phases,
+                         product-form buffered 14-7), dipole solve started
+                         from the molecule-block solution M^-1 E0;
+  plain_reference_forms  the same FP64 arm with the reference's own forms
+                         (one FP64 sine/cosine per (site, k), pow() 14-7);
+  fast_first_order       mixed precision, solve started from the first-order
+                         guess p(t-1) + M^-1 (E0(t) - E0(t-1)), network off;
+  fast                   mixed precision + the learned guess (the per-site
+                         network trained beforehand, on the GPU, on dipoles the
+                         solver itself converged): the headline `value`.
+Every arm solves the dipoles to the same tolerance (RMS change 1e-6 D).  The
+line also carries the solver's iterations from each guess, each arm's force
+error against FP64 with the dipoles solved to 1e-13 e nm, pair interactions
+per second and both arms' energy drift in an NVE run from the same state.
 
 One "step" is one MD time step: pair-list check/rebuild, all forces (vdW,
 multipoles, dipole solve, induced terms), SHAKE + Nose-Hoover update and
@@ -28,6 +38,7 @@ same workload, single-threaded (the build has no MPI), bounded to one MD
 step because one step of this size takes more than a minute.
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -47,6 +58,7 @@ METRIC = "ns/day on 1 B200: learned-guess+mixed vs plain GPU path at matched for
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 DIPOLE_TOL = 2.0819e-8   # 1e-6 D in e nm
+SERIES_CAP = 4096        # per-step samples kept for the energy drift
 
 
 def workload(name, nmol=None):
@@ -355,6 +367,9 @@ def main():
     ap.add_argument("--train-epochs", type=int, default=8)
     ap.add_argument("--e2e-every", type=int, default=10)
     ap.add_argument("--cpu-sample-mols", type=int, default=1024)
+    ap.add_argument("--equilibrate", type=int, default=10000)
+    ap.add_argument("--iter-steps", type=int, default=20)
+    ap.add_argument("--drift-steps", type=int, default=2000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -387,12 +402,14 @@ def main():
     dt = s.config.timestep
     polar = args.workload == "polwater4096"
     t_setup = time.perf_counter()
-    ens = engine.GpuEnsemble(s, precision="fp64", device=local)
+    ens = engine.GpuEnsemble(s, precision="mixed", device=local)
     if polar:
-        ens.set_solver(tol=DIPOLE_TOL, max_iter=500, guess=L.GUESS_DIRECT)
-    lf = engine.LFIntegrator(ens)
+        ens.set_solver(tol=DIPOLE_TOL, max_iter=500, guess=L.GUESS_FIRST_ORDER)
+    lf = engine.LFIntegrator(ens, series_capacity=SERIES_CAP)
     lf.start()
-    lf.run(args.warmup)
+    # equilibration from the seeded start (random orientations release a lot
+    # of energy): mixed path, cheap
+    lf.run(args.equilibrate)
     l2 = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")  # 256 MB > L2
 
     train = {}
@@ -410,44 +427,125 @@ def main():
                  "epochs": args.train_epochs, "final_mse": loss,
                  "collect_s": t1 - t0, "train_s": time.perf_counter() - t1}
 
-    def arm(precision, guess):
+    clk_all = ClockSampler(local)
+    clk_all.start()
+
+    def arm(precision, guess, reference_forms=False, steps=None):
+        steps = steps or args.steps
         ens.set_precision(precision)
+        ens.set_reference_forms(reference_forms)
         if polar:
             ens.set_solver(tol=DIPOLE_TOL, max_iter=500, guess=guess)
         lf.run(args.warmup)
         if dist:
             dist.barrier()
-        lists0 = lf.observables().list_updates
-        ms = timed_steps(lf, l2, args.steps, args.chunk)
-        rebuilds = lf.observables().list_updates - lists0
+        o0 = lf.observables()
+        clk = ClockSampler(local)
+        clk.start()
+        ms = timed_steps(lf, l2, steps, args.chunk)
+        clocks = clk.stop()
+        o1 = lf.observables()
         t = torch.tensor([ms], dtype=torch.float64)
         if dist:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        iters = ens.solver_stats()[0] if polar else 0
-        return float(t[0]) / args.steps, iters, rebuilds / args.steps
+        it = ens.solver_stats() if polar else (0, 0.0)
+        ms_step = float(t[0]) / steps
+        return {"value": ns_per_day(ms_step * 1e-3, dt) * world, "ms_per_step": ms_step,
+                "solver_iterations": it[0], "dipole_rms_change_at_exit": it[1],
+                "list_rebuilds_per_step": (o1.list_updates - o0.list_updates) / steps,
+                "pairs_in_cutoff": int(o1.pairs_in_cutoff), "clocks": clocks}
 
-    plain_ms, plain_it, plain_rb = arm("fp64", L.GUESS_DIRECT)
+    # plain: FP64 throughout, the same algorithms as the fast arm (column
+    # reciprocal passes with exact integer phases, product-form 14-7), the
+    # solve started from the molecule-block solution M^-1 E0
+    plain = arm("fp64", L.GUESS_DIRECT)
     prof_plain = np.zeros(10)
     L.check(ens.ctx, ens.lib.smd_profile_stages(ens.ctx, 5, L.dptr(prof_plain)))
-    clk = ClockSampler(local)
-    clk.start()
-    fast_ms, fast_it, fast_rb = arm("mixed", L.GUESS_LEARNED if polar else L.GUESS_DIRECT)
-    clocks = clk.stop()
+    # the same FP64 arm with the reference's own forms (pow() 14-7, one FP64
+    # sine and cosine per (site, k)): what a direct GPU port of the reference
+    # arithmetic runs at
+    plain_ref = arm("fp64", L.GUESS_DIRECT, reference_forms=True, steps=max(10, args.steps // 4))
+    ens.set_reference_forms(False)
+    # fast without the network: mixed path, first-order guess
+    first_order = arm("mixed", L.GUESS_FIRST_ORDER) if polar else None
+    # fast: mixed path + learned guess (the headline)
+    fast = arm("mixed", L.GUESS_LEARNED if polar else L.GUESS_DIRECT)
+    clocks_all = clk_all.stop()
     prof = np.zeros(10)
     L.check(ens.ctx, ens.lib.smd_profile_stages(ens.ctx, 5, L.dptr(prof)))
+    value = fast["value"]
 
-    # force error of the fast arm against the FP64 evaluation, same configuration
-    ens.set_precision("fp64")
-    f64, _, _ = ens.compute_forces()
+    # iterations of the working-tolerance solve from each guess, step by step
+    iters = {}
+    if polar:
+        for name, g in (("direct", L.GUESS_DIRECT), ("previous", L.GUESS_PREVIOUS),
+                        ("first_order", L.GUESS_FIRST_ORDER), ("learned", L.GUESS_LEARNED)):
+            ens.set_solver(tol=DIPOLE_TOL, max_iter=500, guess=g)
+            lf.run(3)
+            its = []
+            for _ in range(args.iter_steps):
+                lf.run(1)
+                its.append(ens.solver_stats()[0])
+            iters[name] = {"mean": float(np.mean(its)), "min": int(min(its)), "max": int(max(its))}
+
+    # force error at matched dipole tolerance: each arm's evaluation of the
+    # current configuration against FP64 with the dipoles solved to 1e-13 e nm
+    force_err = {}
+    n = s.n_atoms
+    if polar:
+        pos_now = ens.state()["pos"].copy()
+        ens.set_precision("fp64")
+        ens.set_solver(tol=1e-13, max_iter=3000, guess=L.GUESS_DIRECT)
+        f_tight, _, _ = ens.compute_forces()
+        for name, prec, g in (("plain", "fp64", L.GUESS_DIRECT), ("fast", "mixed", L.GUESS_LEARNED)):
+            ens.set_precision(prec)
+            ens.set_solver(tol=DIPOLE_TOL, max_iter=500, guess=g)
+            ens.upload_positions(pos_now)
+            f, _, _ = ens.compute_forces()
+            force_err[name] = float(np.sqrt(((f - f_tight) ** 2).sum() / (f_tight ** 2).sum()))
+        ens.set_solver(tol=DIPOLE_TOL, max_iter=500, guess=L.GUESS_LEARNED)
+    else:
+        ens.set_precision("fp64")
+        f64, _, _ = ens.compute_forces()
+        ens.set_precision("mixed")
+        f32, _, _ = ens.compute_forces()
+        force_err["fast"] = float(np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum()))
     ens.set_precision("mixed")
-    f32, _, _ = ens.compute_forces()
-    force_err = float(np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum()))
 
-    value = ns_per_day(fast_ms * 1e-3, dt) * world
-    plain_value = ns_per_day(plain_ms * 1e-3, dt) * world
+    # energy conservation: the same state advanced without thermostat (NVE)
+    # by each arm; drift = slope of U + K over the run
+    def drift(precision, guess, steps, st0):
+        ens.set_precision(precision)
+        if polar:
+            ens.set_solver(tol=DIPOLE_TOL, max_iter=500, guess=guess)
+        ens.upload_positions(st0["pos"])
+        ens.upload_velocities(st0["vel"], st0["vtminus"])
+        lf.run(steps)
+        ser = lf.series()[-steps:]
+        h = ser[:, 0] + ser[:, 1]
+        tt = np.arange(steps) * dt * 1e-3   # ns
+        slope = float(np.polyfit(tt, h, 1)[0])
+        return {"kj_mol_per_ns": slope, "kj_mol_per_ns_per_molecule": slope / s.n_mols,
+                "rms_fluctuation_kj_mol": float(np.std(h - np.polyval(np.polyfit(tt, h, 1), tt))),
+                "steps": steps}
+    drift_steps = min(args.drift_steps, SERIES_CAP)
+    st0 = ens.state()
+    nve = lf.params
+    nve_thermo = nve.thermostat
+    nve.thermostat = L.THERMO_NONE
+    L.check(ens.ctx, ens.lib.smd_set_integrator(ens.ctx, ctypes.byref(nve)))
+    energy_drift = {"plain": drift("fp64", L.GUESS_DIRECT, drift_steps, st0),
+                    "fast": drift("mixed", L.GUESS_LEARNED if polar else L.GUESS_DIRECT, drift_steps, st0),
+                    "how": "NVE from the same state (thermostat off), slope of U + K"}
+    nve.thermostat = nve_thermo
+    L.check(ens.ctx, ens.lib.smd_set_integrator(ens.ctx, ctypes.byref(nve)))
+    ens.upload_positions(st0["pos"])
+    ens.upload_velocities(st0["vel"], st0["vtminus"])
+    ens.set_precision("mixed")
+    if polar:
+        ens.set_solver(tol=DIPOLE_TOL, max_iter=500, guess=L.GUESS_LEARNED)
 
     # --- end to end through the public API, host buffers ------------------
-    n = s.n_atoms
     pos = torch.empty(3 * n, dtype=torch.float64).pin_memory().numpy()
     vel = torch.empty(3 * n, dtype=torch.float64).pin_memory().numpy()
     st = ens.state()
@@ -455,6 +553,7 @@ def main():
     vel[:] = st["vel"].reshape(-1)
     every = args.e2e_every
     e2e_steps = max(every, (min(args.steps, 200) // every) * every)
+    lf.run(args.warmup)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -473,8 +572,7 @@ def main():
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = ns_per_day(float(te[0]) / e2e_steps * 1e-3, dt) * world
 
-    # --- roofline of the dominant stage ----------------------------------
-    import ctypes
+    # --- roofline of the reciprocal passes ---------------------------------
     kc = ctypes.c_int()
     L.check(ens.ctx, ens.lib.smd_step_kernel_count(ens.ctx, ctypes.byref(kc)))
     names = ["pair", "recip", "integrate", "list_rebuild", "frames", "mp_real", "mp_recip",
@@ -490,12 +588,11 @@ def main():
     # (FP32 SIMT work, a few MB of traffic), counted as the FP32 operations
     # of the column formulation (an FMA is 2): 33 per (site, k) in the sums
     # pass (27 per k plus the run's shared 22 over 3.7 k) and 26 in the force
-    # pass (24 per k plus the column fold, 42 over 24 k); the peak
-    # is the nominal FP32 rate of 148 SMs x 128 lanes at the measured maximum
-    # SM clock
+    # pass (24 per k plus the column fold, 42 over 24 k); the peak is the
+    # nominal FP32 rate of 148 SMs x 128 lanes at the measured maximum SM clock
     # a forced rebuild is timed, but the list is rebuilt only when a site has
     # moved half the skin: weigh it by the rebuilds seen in the timed steps
-    amortised = dict(stage_ms, list_rebuild=stage_ms["list_rebuild"] * fast_rb)
+    amortised = dict(stage_ms, list_rebuild=stage_ms["list_rebuild"] * fast["list_rebuilds_per_step"])
     dom = max(amortised, key=amortised.get)
     nk = ens.ewald_nk() if polar else 0
     flops = float(nk) * n * (33 + 26)
@@ -516,19 +613,33 @@ def main():
                              "LFIntegrator::run, one process, one core"}
 
     if rank == 0:
+        pairs = fast["pairs_in_cutoff"]
         out = {"metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": world,
-               "steps": args.steps, "warmup": args.warmup, "ms_per_step": fast_ms,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": fast["ms_per_step"],
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                "dtype": "f32 pair/reciprocal/field math, f64 solver and integrator",
-               "data": "synthetic (seeded lattice, random orientations)",
+               "data": "synthetic (seeded lattice, random orientations, equilibrated on the GPU)",
                "config": dict(desc, l2="256 MB buffer written before every chunk of "
-                              f"{args.chunk} steps", replicas=world, parallelism="replicas only"),
-               "plain": {"value": plain_value, "ms_per_step": plain_ms, "solver_iterations": plain_it,
-                         "dtype": "f64", "guess": "M^-1 E0 (molecule blocks)"},
-               "fast": {"value": value, "ms_per_step": fast_ms, "solver_iterations": fast_it,
-                        "guess": "learned" if polar else "n/a",
-                        "force_rms_rel_err_vs_fp64": force_err},
-               "speedup_fast_vs_plain": plain_ms / fast_ms,
+                              f"{args.chunk} steps", replicas=world, parallelism="replicas only",
+                              equilibration_steps=args.equilibrate),
+               "plain": dict(plain, dtype="f64", guess="M^-1 E0 (molecule blocks)",
+                             algorithms="the fast arm's: column reciprocal passes, product-form 14-7"),
+               "plain_reference_forms": dict(plain_ref, dtype="f64", guess="M^-1 E0 (molecule blocks)",
+                                             algorithms="the reference's: one FP64 sine/cosine per (site, k), "
+                                                        "pow() 14-7"),
+               "fast_first_order": first_order and dict(first_order, guess="p(t-1) + M^-1 dE0 (network off)"),
+               "fast": dict(fast, guess="learned" if polar else "n/a",
+                            force_rms_rel_err_vs_fp64_tight=force_err.get("fast")),
+               "plain_force_rms_rel_err_vs_fp64_tight": force_err.get("plain"),
+               "speedup_fast_vs_plain": plain["ms_per_step"] / fast["ms_per_step"],
+               "speedup_fast_vs_plain_reference_forms": plain_ref["ms_per_step"] / fast["ms_per_step"],
+               "speedup_learned_vs_first_order": (first_order["ms_per_step"] / fast["ms_per_step"]
+                                                  if first_order else None),
+               "solver_iterations_by_guess": iters,
+               "pair_interactions_per_s": pairs / (fast["ms_per_step"] * 1e-3),
+               "pair_interactions_note": "unordered site pairs inside the short-range cutoff per step "
+                                         "(the fast arm's) / s per step",
+               "energy_drift": energy_drift,
                "training": train,
                "e2e": {"value": e2e_value, "unit": "ns/day", "h2d_bytes_per_step": 2 * 3 * n * 8 / every,
                        "d2h_bytes_per_step": (2 * 3 * n * 8 + 512) / every,
@@ -537,13 +648,11 @@ def main():
                "gpu_launches": kc.value * args.steps,
                "kernels_per_step": kc.value,
                "stage_ms_fast": stage_ms, "stage_ms_plain": stage_plain,
-               "list_rebuilds_per_step": {"fast": fast_rb, "plain": plain_rb},
                "stage_notes": "stage_ms_* time each stage alone (list_rebuild: one forced rebuild); in the fast "
                               "arm the multipole and induced real space are one fused pass, reported under "
                               "ind_real (mp_real 0)",
-               "roofline": {"bound": "fp32", "kernel": "k_rsk_seg<2,4> + k_rforce_grp<1> (reciprocal "
-                                                      "sums and forces of the permanent + induced "
-                                                      "multipoles)",
+               "roofline": {"bound": "fp32", "kernel": "k_rsk_seg<float,2,4> + k_rforce_grp<float,1> (reciprocal "
+                                                      "sums and forces of the permanent + induced multipoles)",
                             "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                             "frac": achieved / fp32_peak if achieved else None,
                             "alg_flops_per_step": flops, "k_vectors": nk,
@@ -559,7 +668,7 @@ def main():
                                            f"({peak_src}); the file's HBM copy and bf16 GEMM rates do not "
                                            "bound these kernels",
                             "dominant_stage": dom},
-               "clocks": clocks, "cpu_baseline": cpu,
+               "clocks": clocks_all, "cpu_baseline": cpu,
                "setup_s": time.perf_counter() - t_setup}
         print(json.dumps(out))
     ens.close()

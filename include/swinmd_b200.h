@@ -75,11 +75,17 @@ enum {
 /* vdW kinds for smd_set_vdw */
 enum { SMD_VDW_NONE = 0, SMD_VDW_LJ = 1, SMD_VDW_MIE = 2, SMD_VDW_BMH = 3, SMD_VDW_BUFF = 4 };
 
-/* initial guess of the induced-dipole solve */
+/* initial guess of the induced-dipole solve (no reference counterpart: the
+ * reference starts its CG from p = 1, src/forces/Induction.cpp:2401-2467) */
 enum {
-    SMD_GUESS_DIRECT = 0,   /* p0 = alpha E0 (first-order induction) */
-    SMD_GUESS_PREVIOUS = 1, /* p0 = the previous solve's dipoles */
-    SMD_GUESS_LEARNED = 2   /* p0 from the per-site network (smd_mlp_*) */
+    SMD_GUESS_DIRECT = 0,      /* p0 = M^-1 E0: the preconditioner applied to the
+                                  permanent field (alpha E0 with the site
+                                  preconditioner) */
+    SMD_GUESS_PREVIOUS = 1,    /* p0 = the previous solve's dipoles */
+    SMD_GUESS_LEARNED = 2,     /* p0 = first-order guess + the per-site network's
+                                  correction (smd_mlp_*) */
+    SMD_GUESS_FIRST_ORDER = 3  /* p0 = p(t-1) + M^-1 (E0(t) - E0(t-1)): the learned
+                                  guess without the network */
 };
 
 /* thermostat kinds: SMD_THERMO_NOSE_HOOVER is the leap-frog integrator of
@@ -239,6 +245,16 @@ int smd_mlp_gradient(smd_ctx *ctx, const float *rows_data, int rows, float *grad
  * of the last evaluation. */
 int smd_mlp_features(smd_ctx *ctx, float *features);
 int smd_set_precision(smd_ctx *ctx, int mode);
+/* FP64 path only.  on = 1: the buffered 14-7 with pow() as
+ * BuffvdWForce::potFunc evaluates it (src/forces/BuffvdWForce.cpp:435-463)
+ * and the multipole reciprocal sums with one FP64 sine and cosine of k.r per
+ * (site, k) as Multipole::reciprocal_term and Induction::reciprocal_term do
+ * (src/forces/Multipole.cpp:951-1245, src/forces/Induction.cpp:1395-1710).
+ * on = 0 (default): the same quantities in FP64 by the algorithms the mixed
+ * path uses (integer powers as products; the column passes with exact
+ * 64-bit integer phases), which agree with the reference's forms to FP64
+ * rounding.  No reference counterpart. */
+int smd_set_reference_forms(smd_ctx *ctx, int on);
 /* Pair-kernel threads per site (1..32, power of two); 0 lets the library pick. */
 int smd_set_tuning(smd_ctx *ctx, int threads_per_site);
 

@@ -24,7 +24,7 @@ TERM_MP_SHORT, TERM_MP_LONG, TERM_IND_SHORT, TERM_IND_LONG = 8, 16, 32, 64
 E_VDW, E_REAL, E_LONG, E_CORRECT, E_MOLCORRECT, E_SURF = 0, 1, 2, 3, 4, 5
 E_POL_REAL, E_POL_LONG, E_POL_SELF, E_POL_INTRA, E_COUNT = 6, 7, 8, 9, 12
 VDW_NONE, VDW_LJ, VDW_MIE, VDW_BMH, VDW_BUFF = 0, 1, 2, 3, 4
-GUESS_DIRECT, GUESS_PREVIOUS, GUESS_LEARNED = 0, 1, 2
+GUESS_DIRECT, GUESS_PREVIOUS, GUESS_LEARNED, GUESS_FIRST_ORDER = 0, 1, 2, 3
 PRECOND_SITE, PRECOND_MOLECULE = 0, 1
 THERMO_NONE, THERMO_NOSE_HOOVER, THERMO_NH_CHAIN = 0, 1, 2
 
@@ -81,6 +81,7 @@ SIGNATURES = {
     "smd_set_ewald": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
     "smd_set_precision": (ctypes.c_int, [_P, ctypes.c_int]),
     "smd_set_tuning": (ctypes.c_int, [_P, ctypes.c_int]),
+    "smd_set_reference_forms": (ctypes.c_int, [_P, ctypes.c_int]),
     "smd_upload_positions": (ctypes.c_int, [_P, _D]),
     "smd_upload_velocities": (ctypes.c_int, [_P, _D, _D]),
     "smd_download_state": (ctypes.c_int, [_P, _D, _D, _D]),

@@ -331,7 +331,7 @@ void smd_destroy(smd_ctx *x) {
                     c.rc.sk, c.rc.kvec, c.clen2, c.type_mp, c.type_polar, c.mu, c.qd, c.trq, c.e0,
                     c.pind, c.cgw, c.cgs, c.cg_bar, c.vpos4, c.vfixq, c.fv, c.ind_rj, c.ind_rc, c.ind_cnt,
                     c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab, c.srec, c.phist, c.cg_blk,
-                    c.upload4, c.fout};
+                    c.upload4, c.fout, c.rc.kzr_d, c.rc.kcxy_d, c.rc.stab_d, c.rc.srec_d};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -634,7 +634,7 @@ int smd_set_multipole(smd_ctx *x, const double *type_mp, const double *polar, do
 }
 
 int smd_set_solver(smd_ctx *x, double tol, int max_iter, int guess) {
-    if (!x || !(tol > 0) || max_iter <= 0 || guess < 0 || guess > 2)
+    if (!x || !(tol > 0) || max_iter <= 0 || guess < 0 || guess > SMD_GUESS_FIRST_ORDER)
         return fail(x, SMD_ERR_ARG, "smd_set_solver: bad arguments");
     x->c.cg_tol = tol;
     x->c.cg_max_iter = max_iter;
@@ -849,6 +849,14 @@ int smd_set_precision(smd_ctx *x, int mode) {
         return fail(x, SMD_ERR_ARG, "smd_set_precision: unknown mode");
     x->c.precision = mode;
     if (x->c.n > 0 && x->c.pos4) launch_fixq(x->c);
+    x->c.graph_dirty = 1;
+    touch(x->c);
+    return SMD_OK;
+}
+
+int smd_set_reference_forms(smd_ctx *x, int on) {
+    if (!x || (on != 0 && on != 1)) return fail(x, SMD_ERR_ARG, "smd_set_reference_forms: on must be 0 or 1");
+    x->c.reference_forms = on;
     x->c.graph_dirty = 1;
     touch(x->c);
     return SMD_OK;
@@ -1075,6 +1083,9 @@ int smd_integrator_start(smd_ctx *x) {
         enqueue_forces(c);
         launch_start_velocities(c);
     }
+    // numUpdates counts the rebuilds of the run, not the start's
+    // (LFIntegrator.cpp:307-341): the build count restarts here
+    CK(cudaMemsetAsync(c.flags + 1, 0, sizeof(int), c.stream));
     c.steps_done = 0;
     touch(c);
     return sync_status(x);

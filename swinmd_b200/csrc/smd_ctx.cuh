@@ -50,6 +50,12 @@ struct Recip {               // Ewald reciprocal space (k half-space, k^2 < kcut
     float4 *kzr = nullptr;   // per k (kz, kz^2, 2c, 0)
     float2 *kcxy = nullptr;  // per column (kx, ky)
     float2 *stab = nullptr;  // per site phase tables [n][row]: e^{2 pi i m f / 2^32}, m < nmax + 1, per axis
+    // the FP64 column passes: (kz, kz^2, 2c, 0) per k, (kx, ky) per column,
+    // phase tables e^{2 pi i m f / 2^64} and FP64 site records [n][4]
+    double4 *kzr_d = nullptr;
+    double2 *kcxy_d = nullptr;
+    double2 *stab_d = nullptr;
+    double4 *srec_d = nullptr;
 };
 
 struct Ctx {
@@ -89,6 +95,7 @@ struct Ctx {
     PairList pl;
     Recip rc;
     int precision = SMD_PREC_FP64;
+    int reference_forms = 0;        // FP64 path: pow() buffered 14-7 and one sine/cosine per (site, k) reciprocal sums
     int want_cells = 1;
     // polarisable multipole model (Multipole / Induction / BuffvdWForce)
     int mp_on = 0, ind_on = 0;
@@ -108,7 +115,7 @@ struct Ctx {
     double *cgs = nullptr;          // CG scalars [8] and partials [4][blocks][4]
     int cg_max_iter = 500;
     double cg_tol = 2.0819e-8;      // RMS dipole change tolerance (e nm); 1e-6 D
-    int cg_guess = 0;               // 0: alpha E0, 1: previous step, 2: learned (MLP)
+    int cg_guess = 0;               // SMD_GUESS_*: 0 block solution of E0, 1 previous step, 2 learned, 3 first order
     int cg_blocks = 0;
     int cg_precond = SMD_PRECOND_MOLECULE;  // dipole-solve preconditioner
     double *cg_blk = nullptr;       // [nmol][81] inverse molecule blocks of A
@@ -204,6 +211,7 @@ int ensure_ind_rows(Ctx &c);
 // dipole-guess network (smd_mlp.cu)
 int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed);
 void launch_mlp_guess(Ctx &c);
+void launch_first_order_guess(Ctx &c);
 void launch_blk_response(Ctx &c, double *out);
 // first-order part of the learned guess: the solver's s slot of its work
 // area, which the solve writes before it first reads it

@@ -1452,9 +1452,10 @@ void launch_ind_field(Ctx &c) {
         k_ind_field<double><<<nb, 256, 0, c.stream>>>(a, R, c.status);
     // the preconditioner's inverse molecule blocks (they need this step's tensor rows)
     const bool learned = c.cg_guess == SMD_GUESS_LEARNED && c.mlp_ready;
+    const bool first_order = c.cg_guess == SMD_GUESS_FIRST_ORDER;
     if (c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk) {
-        // with the learned guess, also its first-order part
-        double *dl = learned ? guess_response(c) : nullptr;
+        // with the learned or first-order guess, also the first-order part
+        double *dl = (learned || first_order) ? guess_response(c) : nullptr;
         const int nbm = (c.nmol + MB_MOLS - 1) / MB_MOLS;
         if (f32)
             k_mol_blocks<float><<<nbm, 9 * MB_MOLS, 0, c.stream>>>(c.n, c.nmol, c.mol_off, c.mol_atoms, R,
@@ -1466,6 +1467,7 @@ void launch_ind_field(Ctx &c) {
                                                                     c.flags, dl);
     }
     if (learned) launch_mlp_guess(c);  // writes the start dipoles into p
+    else if (first_order) launch_first_order_guess(c);
 }
 
 // Response of each molecule's own block to the change of the permanent field
@@ -1529,7 +1531,7 @@ void launch_ind_cg(Ctx &c) {
     g.skip_block = c.test_skip_block;
     g.nblocks = c.cg_blocks; g.max_iter = c.cg_max_iter; g.tol = c.cg_tol;
     // 0: start from alpha E0; 1: start from the dipoles in p (previous solve or network)
-    g.guess = (c.cg_guess == SMD_GUESS_PREVIOUS || learned) ? 1 : 0;
+    g.guess = (c.cg_guess == SMD_GUESS_PREVIOUS || c.cg_guess == SMD_GUESS_FIRST_ORDER || learned) ? 1 : 0;
     const bool bj = c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk;   // blocks built by launch_ind_field
     g.blk = c.cg_blk;
     // the mixed path's site records take the dipoles inside the solve

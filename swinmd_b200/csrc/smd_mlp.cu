@@ -335,6 +335,25 @@ void launch_mlp_guess(Ctx &c) {
         c.pind);
 }
 
+// The first-order guess alone, p = p(t-1) + M^-1 (E0(t) - E0(t-1)) (M^-1 E0
+// with no stored step): the learned guess with the network's correction left
+// out, the baseline that shows what the network adds.
+__global__ void k_first_order_guess(int n, const double *dl, const double *ph, const int *flags, double *p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const V3 g = linear_guess(ph, n, flags[2], i, dl);
+    p[i] = g.x;
+    p[n + i] = g.y;
+    p[2 * n + i] = g.z;
+}
+
+void launch_first_order_guess(Ctx &c) {
+    double *dl = guess_response(c);
+    // with the molecule blocks the block kernel has just formed it
+    if (!(c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk)) launch_blk_response(c, dl);
+    k_first_order_guess<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, dl, c.phist, c.flags, c.pind);
+}
+
 int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed) {
     auto al = [](auto **p, size_t cnt) -> bool {
         if (*p) cudaFree(*p);

@@ -512,126 +512,214 @@ __global__ void __launch_bounds__(256) k_rforce_f(int n, int nk, const double4 *
 //   force   F_a = q M1_a - Q_bc M3_abc + (mu + p)_b M2_ab
 //   torque  mu x M1 - 2 g,  g_a = eps_abc (Q M2)_cb.
 constexpr int TAB_MAX = 32;     // |n| < TAB_MAX
-constexpr int TS_THREADS = 128; // runs per block, sums pass
-constexpr int TS_SITES = 128;   // sites per tile, sums pass
 constexpr int TS_SEG = 4;       // k per run, sums pass
-constexpr int CF_THREADS = 256; // sites per block, force pass
 constexpr int CF_KGROUP = 128;  // k per column group at most, force pass
 constexpr int CF_CGROUP = 64;   // columns per group at most
 
-__device__ __forceinline__ float2 table_entry(int m, unsigned f) {
-    float sn, cs;
-    sincos_phase32((int)((unsigned)m * f), sn, cs);
-    return make_float2(cs, sn);
+// The column passes in FP32 (mixed path) and FP64 (FP64 path).  FP32: the
+// phases are exact 32-bit integer phases n.(box fractions) from fixq and go
+// through sincos_phase32; running sums in FP32 within a tile or column group,
+// FP64 across them.  FP64: the phases are exact 64-bit integer phases of the
+// FP64 positions' 64-bit box fractions, sine and cosine from FP64 sincospi of
+// the phase's top 53 bits (an angle error below 1e-15 rad, where the
+// reference's k.r carries about 1e-14), all arithmetic FP64.  The FP64
+// passes hold half as many sites per tile and per block, so that their
+// tables fit shared memory with the same occupancy.
+template <typename T> struct ColT;
+template <> struct ColT<float> {
+    using T2 = float2;
+    using T4 = float4;
+    static constexpr int SUM_THREADS = 128, SUM_SITES = 128, F_THREADS = 256;
+};
+template <> struct ColT<double> {
+    using T2 = double2;
+    using T4 = double4;
+    static constexpr int SUM_THREADS = 128, SUM_SITES = 64, F_THREADS = 128;
+};
+__device__ __forceinline__ float tfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double tfma(double a, double b, double c) { return fma(a, b, c); }
+
+// 64-bit box fraction of a coordinate: (x / L mod 1) 2^64
+__device__ __forceinline__ unsigned long long frac64(double x, double invL) {
+    double f = x * invL;
+    f -= floor(f);
+    return __double2ull_rn(f * 18446744073709551616.0);
 }
+// sin and cos of 2 pi ph / 2^64
+__device__ __forceinline__ void sincos_phase64(unsigned long long ph, double &s, double &c) {
+    sincospi((double)(long long)ph * 1.0842021724855044e-19, &s, &c);   // 2^-63
+}
+
+// a site's phase source: three 32-bit (FP32) or 64-bit (FP64) box fractions
+template <typename T> struct SitePhase;
+template <> struct SitePhase<float> {
+    unsigned x, y, z;
+    __device__ __forceinline__ SitePhase(const int4 *fixq, const double4 *, const Box &, int i) {
+        const int4 f = fixq[i];
+        x = (unsigned)f.x; y = (unsigned)f.y; z = (unsigned)f.z;
+    }
+    __device__ __forceinline__ SitePhase() : x(0), y(0), z(0) {}
+    __device__ __forceinline__ unsigned ax(int a) const { return a == 0 ? x : (a == 1 ? y : z); }
+    // e^{2 pi i (nx fx + ny fy + nz fz)}
+    __device__ __forceinline__ void rot(int nx, int ny, int nz, float &sn, float &cs) const {
+        sincos_phase32((int)((unsigned)nx * x + (unsigned)ny * y + (unsigned)nz * z), sn, cs);
+    }
+    __device__ __forceinline__ static float2 entry(int m, unsigned f) {
+        float sn, cs;
+        sincos_phase32((int)((unsigned)m * f), sn, cs);
+        return make_float2(cs, sn);
+    }
+};
+template <> struct SitePhase<double> {
+    unsigned long long x, y, z;
+    __device__ __forceinline__ SitePhase(const int4 *, const double4 *pos4, const Box &b, int i) {
+        const double4 p = pos4[i];
+        x = frac64(p.x, b.inv[0]); y = frac64(p.y, b.inv[1]); z = frac64(p.z, b.inv[2]);
+    }
+    __device__ __forceinline__ SitePhase() : x(0), y(0), z(0) {}
+    __device__ __forceinline__ unsigned long long ax(int a) const { return a == 0 ? x : (a == 1 ? y : z); }
+    __device__ __forceinline__ void rot(int nx, int ny, int nz, double &sn, double &cs) const {
+        sincos_phase64((unsigned long long)(long long)nx * x + (unsigned long long)(long long)ny * y +
+                           (unsigned long long)(long long)nz * z, sn, cs);
+    }
+    __device__ __forceinline__ static double2 entry(int m, unsigned long long f) {
+        double sn, cs;
+        sincos_phase64((unsigned long long)m * f, sn, cs);
+        return make_double2(cs, sn);
+    }
+};
 
 // site tables [n][row]: X[0..nt), Y[0..nt), Z[0..nt), zero padding to an
 // even row
-__global__ void k_site_tab(int n, int nt, int row, const int4 *fixq, float2 *stab) {
+template <typename T>
+__global__ void k_site_tab(int n, int nt, int row, const int4 *fixq, const double4 *pos4, Box box,
+                           typename ColT<T>::T2 *stab) {
+    using T2 = typename ColT<T>::T2;
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (long long)n * row) return;
     const int i = (int)(e / row), r = (int)(e - (long long)i * row);
     const int ax = r / nt, m = r - ax * nt;
-    float2 v = make_float2(0.f, 0.f);
+    T2 v;
+    v.x = 0; v.y = 0;
     if (ax < 3) {
-        const int4 f = fixq[i];
-        v = table_entry(m, (unsigned)(ax == 0 ? f.x : (ax == 1 ? f.y : f.z)));
+        const SitePhase<T> f(fixq, pos4, box, i);
+        v = SitePhase<T>::entry(m, f.ax(ax));
     }
     stab[e] = v;
 }
 
+// FP64 site records of the FP64 column passes, in the layout of the mixed
+// path's FP32 records: (q, mu), (Qxx, Qxy, Qxz, Qyy), (Qyz, Qzz, px, py),
+// (pz, 0, 0, 0)
+__global__ void k_pack_srec_d(int n, const double4 *pos4, const double *tq, const double *mu, const double *qd,
+                              const double *pind, double4 *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t N = (size_t)n;
+    double4 *o = out + 4 * (size_t)i;
+    o[0] = make_double4(tq[(int)pos4[i].w] / SQC_R, mu[i], mu[N + i], mu[2 * N + i]);
+    o[1] = make_double4(qd[i], qd[N + i], qd[2 * N + i], qd[3 * N + i]);
+    o[2] = make_double4(qd[4 * N + i], qd[5 * N + i], pind ? pind[i] : 0.0, pind ? pind[N + i] : 0.0);
+    o[3] = make_double4(pind ? pind[2 * N + i] : 0.0, 0.0, 0.0, 0.0);
+}
+
 // MODE 0: permanent sums (slots 0-3); 1: induced sums (4-5); 2: all six.
 // kseg[s] = (first k, count, nx | ny << 16, first nz)
-template <int MODE, int SEG>
-__global__ void __launch_bounds__(TS_THREADS) k_rsk_seg(int n, int nk, int nseg, int nt, int row,
-                                                        const int4 *kseg, const double *kvec,
-                                                        const float2 *stab, const float4 *ssv, double *partial) {
+template <typename T, int MODE, int SEG>
+__global__ void __launch_bounds__(ColT<T>::SUM_THREADS) k_rsk_seg(int n, int nk, int nseg, int nt, int row,
+                                                                  const int4 *kseg, const double *kvec,
+                                                                  const typename ColT<T>::T2 *stab,
+                                                                  const typename ColT<T>::T4 *ssv,
+                                                                  double *partial) {
+    using T2 = typename ColT<T>::T2;
+    using T4 = typename ColT<T>::T4;
+    constexpr int THREADS = ColT<T>::SUM_THREADS, SITES = ColT<T>::SUM_SITES;
     constexpr bool PERM = MODE != 1, IND = MODE != 0;
     extern __shared__ float4 s_dyn4[];
-    float4 *s_v = s_dyn4;                              // [TS_SITES][4]
-    float2 *s_tab = (float2 *)(s_v + 4 * TS_SITES);    // [TS_SITES][row]
-    const int sid = blockIdx.x * TS_THREADS + threadIdx.x;
+    T4 *s_v = (T4 *)s_dyn4;                          // [SITES][4]
+    T2 *s_tab = (T2 *)(s_v + 4 * SITES);             // [SITES][row]
+    const int sid = blockIdx.x * THREADS + threadIdx.x;
     const bool own = sid < nseg;
     const int ch = blockIdx.y;
     const int per = (n + gridDim.y - 1) / gridDim.y;
     const int s0 = ch * per, s1 = min(n, s0 + per);
     const int4 sg = own ? kseg[sid] : make_int4(0, 0, 0, 0);
     const int nx = (short)(sg.z & 0xffff), ny = sg.z >> 16;
-    float kx = 0.f, ky = 0.f;
+    T kx = 0, ky = 0;
     if (own) {
-        kx = (float)kvec[sg.x];
-        ky = (float)kvec[nk + sg.x];
+        kx = (T)kvec[sg.x];
+        ky = (T)kvec[nk + sg.x];
     }
-    float kz[SEG], zsg[SEG];
+    T kz[SEG], zsg[SEG];
     int oz[SEG];
 #pragma unroll
     for (int j = 0; j < SEG; j++) {
         const bool v = j < sg.y;
         const int nz = sg.w + j;
-        kz[j] = v ? (float)kvec[2 * (size_t)nk + sg.x + j] : 0.f;
+        kz[j] = v ? (T)kvec[2 * (size_t)nk + sg.x + j] : (T)0;
         oz[j] = 2 * nt + (v ? (nz < 0 ? -nz : nz) : 0);
-        zsg[j] = nz < 0 ? -1.f : 1.f;
+        zsg[j] = nz < 0 ? (T)-1 : (T)1;
     }
     const int ox = nx, oy = nt + (ny < 0 ? -ny : ny);
-    const float ysg = ny < 0 ? -1.f : 1.f;
-    const float kxx = kx * kx, kxy2 = 2.f * kx * ky, kyy = ky * ky, kx2 = 2.f * kx, ky2 = 2.f * ky;
+    const T ysg = ny < 0 ? (T)-1 : (T)1;
+    const T kxx = kx * kx, kxy2 = (T)2 * kx * ky, kyy = ky * ky, kx2 = (T)2 * kx, ky2 = (T)2 * ky;
     double acc[SEG][6];
 #pragma unroll
     for (int j = 0; j < SEG; j++)
 #pragma unroll
         for (int q = 0; q < 6; q++) acc[j][q] = 0.0;
-    for (int base = s0; base < s1; base += TS_SITES) {
-        const int cnt = min(TS_SITES, s1 - base);
+    for (int base = s0; base < s1; base += SITES) {
+        const int cnt = min(SITES, s1 - base);
         __syncthreads();
         {
             // row is even, so every site's row starts on a 16-byte boundary
-            // and a tile is a whole number of float4s
+            // and a tile is a whole number of 16-byte units
             const float4 *src = (const float4 *)(stab + (size_t)base * row);
             float4 *dst = (float4 *)s_tab;
-            const int nv = cnt * row / 2;
-            for (int e = threadIdx.x; e < nv; e += TS_THREADS) dst[e] = src[e];
-            const float4 *sv = ssv + (size_t)base * 4;
-            for (int e = threadIdx.x; e < cnt * 4; e += TS_THREADS) s_v[e] = sv[e];
+            const int nv = (int)((size_t)cnt * row * sizeof(T2) / sizeof(float4));
+            for (int e = threadIdx.x; e < nv; e += THREADS) dst[e] = src[e];
+            const T4 *sv = ssv + (size_t)base * 4;
+            for (int e = threadIdx.x; e < cnt * 4; e += THREADS) s_v[e] = sv[e];
         }
         __syncthreads();
-        float t[SEG][6];
+        T t[SEG][6];
 #pragma unroll
         for (int j = 0; j < SEG; j++)
 #pragma unroll
-            for (int q = 0; q < 6; q++) t[j][q] = 0.f;
-        const float2 *tp = s_tab;
+            for (int q = 0; q < 6; q++) t[j][q] = 0;
+        const T2 *tp = s_tab;
         for (int q = 0; q < cnt; q++, tp += row) {
-            const float2 X = tp[ox], Y = tp[oy];
-            const float yi = Y.y * ysg;
-            const float xr = fmaf(X.x, Y.x, -X.y * yi), xi = fmaf(X.x, yi, X.y * Y.x);
-            float a = 0.f, b = 0.f, c = 0.f, d = 0.f, e = 0.f, pd = 0.f, pe = 0.f;
+            const T2 X = tp[ox], Y = tp[oy];
+            const T yi = Y.y * ysg;
+            const T xr = tfma(X.x, Y.x, -X.y * yi), xi = tfma(X.x, yi, X.y * Y.x);
+            T a = 0, b = 0, c = 0, d = 0, e = 0, pd = 0, pe = 0;
             if (PERM) {
-                const float4 v0 = s_v[q * 4], v1 = s_v[q * 4 + 1], v2 = s_v[q * 4 + 2];
-                a = v0.x - fmaf(v1.x, kxx, fmaf(v1.y, kxy2, v1.w * kyy));
-                b = -fmaf(v1.z, kx2, v2.x * ky2);
+                const T4 v0 = s_v[q * 4], v1 = s_v[q * 4 + 1], v2 = s_v[q * 4 + 2];
+                a = v0.x - tfma(v1.x, kxx, tfma(v1.y, kxy2, v1.w * kyy));
+                b = -tfma(v1.z, kx2, v2.x * ky2);
                 c = -v2.y;
-                d = fmaf(v0.y, kx, v0.z * ky);
+                d = tfma(v0.y, kx, v0.z * ky);
                 e = v0.w;
             }
             if (IND) {
-                const float4 v2 = s_v[q * 4 + 2], v3 = s_v[q * 4 + 3];
-                pd = fmaf(v2.z, kx, v2.w * ky);
+                const T4 v2 = s_v[q * 4 + 2], v3 = s_v[q * 4 + 3];
+                pd = tfma(v2.z, kx, v2.w * ky);
                 pe = v3.x;
             }
 #pragma unroll
             for (int j = 0; j < SEG; j++) {
-                const float2 Z = tp[oz[j]];
-                const float zi = Z.y * zsg[j];
-                const float cs = fmaf(xr, Z.x, -xi * zi), sn = fmaf(xr, zi, xi * Z.x);
+                const T2 Z = tp[oz[j]];
+                const T zi = Z.y * zsg[j];
+                const T cs = tfma(xr, Z.x, -xi * zi), sn = tfma(xr, zi, xi * Z.x);
                 if (PERM) {
-                    const float w = fmaf(kz[j], fmaf(c, kz[j], b), a);
-                    const float m = fmaf(e, kz[j], d);
-                    t[j][0] = fmaf(w, cs, t[j][0]); t[j][1] = fmaf(w, sn, t[j][1]);
-                    t[j][2] = fmaf(m, cs, t[j][2]); t[j][3] = fmaf(m, sn, t[j][3]);
+                    const T w = tfma(kz[j], tfma(c, kz[j], b), a);
+                    const T m = tfma(e, kz[j], d);
+                    t[j][0] = tfma(w, cs, t[j][0]); t[j][1] = tfma(w, sn, t[j][1]);
+                    t[j][2] = tfma(m, cs, t[j][2]); t[j][3] = tfma(m, sn, t[j][3]);
                 }
                 if (IND) {
-                    const float p = fmaf(pe, kz[j], pd);
-                    t[j][4] = fmaf(p, cs, t[j][4]); t[j][5] = fmaf(p, sn, t[j][5]);
+                    const T p = tfma(pe, kz[j], pd);
+                    t[j][4] = tfma(p, cs, t[j][4]); t[j][5] = tfma(p, sn, t[j][5]);
                 }
             }
         }
@@ -670,72 +758,80 @@ __device__ __forceinline__ int sym3(int a, int b, int c) {
 
 // kgrp[g] = (first column, columns, first k, k count); kcol[c] = (first k,
 // length, nx | ny << 16, first nz); kzr[k] = (kz, kz^2, 2c, 0)
-template <bool IND>
-__global__ void __launch_bounds__(CF_THREADS) k_rforce_grp(int n, int nk, int zs, int ngrp, const double4 *pos4,
-                                                           const int4 *fixq, const int4 *kgrp, const int4 *kcol,
-                                                           const float2 *kcxy, const float4 *kzr, const double *sk,
-                                                           const double *tq, const double *mu, const double *qd,
-                                                           const double *pind, long long *frc, long long *trq) {
+template <typename T, bool IND>
+__global__ void __launch_bounds__(ColT<T>::F_THREADS) k_rforce_grp(int n, int nk, int zs, int ngrp, Box box,
+                                                                  const double4 *pos4, const int4 *fixq,
+                                                                  const int4 *kgrp, const int4 *kcol,
+                                                                  const typename ColT<T>::T2 *kcxy,
+                                                                  const typename ColT<T>::T4 *kzr,
+                                                                  const double *sk, const double *tq,
+                                                                  const double *mu, const double *qd,
+                                                                  const double *pind, long long *frc,
+                                                                  long long *trq) {
+    using T2 = typename ColT<T>::T2;
+    using T4 = typename ColT<T>::T4;
+    constexpr int THREADS = ColT<T>::F_THREADS;
     extern __shared__ float4 s_dyn4[];
-    float4 *s_k = s_dyn4;                           // [CF_KGROUP] (U', W', kz, kz^2)
-    int4 *s_col = (int4 *)(s_k + CF_KGROUP);        // [CF_CGROUP]
-    float2 *s_cxy = (float2 *)(s_col + CF_CGROUP);  // [CF_CGROUP]
-    float2 *s_z = s_cxy + CF_CGROUP;                // [CF_THREADS][zs]
-    const int i = blockIdx.x * CF_THREADS + threadIdx.x;
+    T4 *s_k = (T4 *)s_dyn4;                        // [CF_KGROUP] (U', W', kz, kz^2)
+    int4 *s_col = (int4 *)(s_k + CF_KGROUP);       // [CF_CGROUP]
+    T2 *s_cxy = (T2 *)(s_col + CF_CGROUP);         // [CF_CGROUP]
+    T2 *s_z = s_cxy + CF_CGROUP;                   // [THREADS][zs]
+    const int i = blockIdx.x * THREADS + threadIdx.x;
     const bool own = i < n;
-    const int4 pf = own ? fixq[i] : make_int4(0, 0, 0, 0);
-    float2 *zt = s_z + threadIdx.x * zs;
-    for (int m = 0; m < zs; m++) zt[m] = table_entry(m, (unsigned)pf.z);
+    const SitePhase<T> pf = own ? SitePhase<T>(fixq, pos4, box, i) : SitePhase<T>();
+    T2 *zt = s_z + threadIdx.x * zs;
+    for (int m = 0; m < zs; m++) zt[m] = SitePhase<T>::entry(m, pf.z);
     double D1[3] = {0, 0, 0}, D2[6] = {0, 0, 0, 0, 0, 0}, D3[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     const int gper = (ngrp + gridDim.y - 1) / gridDim.y;
     const int g0 = blockIdx.y * gper, g1 = min(ngrp, g0 + gper);
     for (int g = g0; g < g1; g++) {
         const int4 gr = kgrp[g];
         __syncthreads();
-        for (int e = threadIdx.x; e < gr.w; e += CF_THREADS) {
+        for (int e = threadIdx.x; e < gr.w; e += THREADS) {
             const size_t k = (size_t)gr.z + e;
-            const float4 r = kzr[k];
+            const T4 r = kzr[k];
             double U = sk[k] - sk[3 * (size_t)nk + k], W = sk[nk + k] + sk[2 * (size_t)nk + k];
             if (IND) {
                 U -= sk[5 * (size_t)nk + k];
                 W += sk[4 * (size_t)nk + k];
             }
-            s_k[e] = make_float4((float)(r.z * U), (float)(r.z * W), r.x, r.y);
+            T4 v;
+            v.x = (T)(r.z * U); v.y = (T)(r.z * W); v.z = r.x; v.w = r.y;
+            s_k[e] = v;
         }
-        for (int e = threadIdx.x; e < gr.y; e += CF_THREADS) {
+        for (int e = threadIdx.x; e < gr.y; e += THREADS) {
             int4 cc = kcol[gr.x + e];
             cc.x -= gr.z;
             s_col[e] = cc;
             s_cxy[e] = kcxy[gr.x + e];
         }
         __syncthreads();
-        float M1[3] = {0.f, 0.f, 0.f}, M2[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        float M3[10] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        T M1[3] = {0, 0, 0}, M2[6] = {0, 0, 0, 0, 0, 0};
+        T M3[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         for (int cix = 0; cix < gr.y; cix++) {
             const int4 cc = s_col[cix];
             const int nx = (short)(cc.z & 0xffff), ny = cc.z >> 16;
-            float s0, c0;
-            sincos_phase32((int)((unsigned)nx * (unsigned)pf.x + (unsigned)ny * (unsigned)pf.y +
-                                 (unsigned)cc.w * (unsigned)pf.z), s0, c0);
-            float P0 = 0.f, P1 = 0.f, P2 = 0.f, P3 = 0.f, R0 = 0.f, R1 = 0.f, R2 = 0.f;
-            const float4 *kr = s_k + cc.x;
+            T s0, c0;
+            pf.rot(nx, ny, cc.w, s0, c0);
+            T P0 = 0, P1 = 0, P2 = 0, P3 = 0, R0 = 0, R1 = 0, R2 = 0;
+            const T4 *kr = s_k + cc.x;
             for (int m = 0; m < cc.y; m++) {
-                const float4 r = kr[m];
-                const float2 z = zt[m];
-                const float cs = fmaf(c0, z.x, -s0 * z.y), sn = fmaf(c0, z.y, s0 * z.x);
-                const float A = fmaf(sn, r.x, -cs * r.y), B = fmaf(cs, r.x, sn * r.y);
-                const float Akz = A * r.z;
-                P0 += A; P1 += Akz; P2 = fmaf(A, r.w, P2); P3 = fmaf(Akz, r.w, P3);
-                R0 += B; R1 = fmaf(B, r.z, R1); R2 = fmaf(B, r.w, R2);
+                const T4 r = kr[m];
+                const T2 z = zt[m];
+                const T cs = tfma(c0, z.x, -s0 * z.y), sn = tfma(c0, z.y, s0 * z.x);
+                const T A = tfma(sn, r.x, -cs * r.y), B = tfma(cs, r.x, sn * r.y);
+                const T Akz = A * r.z;
+                P0 += A; P1 += Akz; P2 = tfma(A, r.w, P2); P3 = tfma(Akz, r.w, P3);
+                R0 += B; R1 = tfma(B, r.z, R1); R2 = tfma(B, r.w, R2);
             }
-            const float2 kk = s_cxy[cix];
-            const float kx = kk.x, ky = kk.y, kxx = kx * kx, kxy = kx * ky, kyy = ky * ky;
-            M1[0] = fmaf(kx, P0, M1[0]); M1[1] = fmaf(ky, P0, M1[1]); M1[2] += P1;
-            M2[0] = fmaf(kxx, R0, M2[0]); M2[1] = fmaf(kxy, R0, M2[1]); M2[2] = fmaf(kx, R1, M2[2]);
-            M2[3] = fmaf(kyy, R0, M2[3]); M2[4] = fmaf(ky, R1, M2[4]); M2[5] += R2;
-            M3[0] = fmaf(kxx * kx, P0, M3[0]); M3[1] = fmaf(kxx * ky, P0, M3[1]); M3[2] = fmaf(kxx, P1, M3[2]);
-            M3[3] = fmaf(kx * kyy, P0, M3[3]); M3[4] = fmaf(kxy, P1, M3[4]); M3[5] = fmaf(kx, P2, M3[5]);
-            M3[6] = fmaf(kyy * ky, P0, M3[6]); M3[7] = fmaf(kyy, P1, M3[7]); M3[8] = fmaf(ky, P2, M3[8]);
+            const T2 kk = s_cxy[cix];
+            const T kx = kk.x, ky = kk.y, kxx = kx * kx, kxy = kx * ky, kyy = ky * ky;
+            M1[0] = tfma(kx, P0, M1[0]); M1[1] = tfma(ky, P0, M1[1]); M1[2] += P1;
+            M2[0] = tfma(kxx, R0, M2[0]); M2[1] = tfma(kxy, R0, M2[1]); M2[2] = tfma(kx, R1, M2[2]);
+            M2[3] = tfma(kyy, R0, M2[3]); M2[4] = tfma(ky, R1, M2[4]); M2[5] += R2;
+            M3[0] = tfma(kxx * kx, P0, M3[0]); M3[1] = tfma(kxx * ky, P0, M3[1]); M3[2] = tfma(kxx, P1, M3[2]);
+            M3[3] = tfma(kx * kyy, P0, M3[3]); M3[4] = tfma(kxy, P1, M3[4]); M3[5] = tfma(kx, P2, M3[5]);
+            M3[6] = tfma(kyy * ky, P0, M3[6]); M3[7] = tfma(kyy, P1, M3[7]); M3[8] = tfma(ky, P2, M3[8]);
             M3[9] += P3;
         }
 #pragma unroll
@@ -786,25 +882,32 @@ __global__ void __launch_bounds__(CF_THREADS) k_rforce_grp(int n, int nk, int zs
 }
 
 int tab_row(int nt) { return (3 * nt + 1) & ~1; }
-size_t tsum_smem(int row) { return (size_t)TS_SITES * (4 * sizeof(float4) + row * sizeof(float2)); }
+template <typename T>
+size_t tsum_smem(int row) {
+    return (size_t)ColT<T>::SUM_SITES * (4 * sizeof(typename ColT<T>::T4) + row * sizeof(typename ColT<T>::T2));
+}
 int zrow(int nmax) { return (2 * nmax + 1) | 1; }
+template <typename T>
 size_t tforce_smem(int zs) {
-    return (size_t)CF_KGROUP * sizeof(float4) + (size_t)CF_CGROUP * (sizeof(int4) + sizeof(float2)) +
-           (size_t)CF_THREADS * zs * sizeof(float2);
+    return (size_t)CF_KGROUP * sizeof(typename ColT<T>::T4) +
+           (size_t)CF_CGROUP * (sizeof(int4) + sizeof(typename ColT<T>::T2)) +
+           (size_t)ColT<T>::F_THREADS * zs * sizeof(typename ColT<T>::T2);
 }
 
-// column, run and group records of the FP32 passes, the site-table buffers
-// and the kernels' dynamic shared memory (once per k set, outside any
-// capture).  Leaves the FP32 column passes off (rc.kseg null) when the k
-// list is not column ordered with fixed (kx, ky) per column or |n| is too
-// large for the tables.
+// column, run and group records of the column passes, the site-table and
+// site-record buffers of both precisions and the kernels' dynamic shared
+// memory (once per k set, outside any capture).  Leaves the column passes
+// off (rc.kseg null) when the k list is not column ordered with fixed
+// (kx, ky) per column or |n| is too large for the tables.
 int mp_recip_prepare(Ctx &c) {
     const int nk = c.rc.nk;
-    void *old[] = {c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab};
+    void *old[] = {c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab,
+                   c.rc.kzr_d, c.rc.kcxy_d, c.rc.stab_d, c.rc.srec_d};
     for (void *p : old)
         if (p) cudaFree(p);
     c.rc.kseg = nullptr; c.rc.kcol = nullptr; c.rc.kgrp = nullptr; c.rc.kzr = nullptr;
     c.rc.kcxy = nullptr; c.rc.stab = nullptr;
+    c.rc.kzr_d = nullptr; c.rc.kcxy_d = nullptr; c.rc.stab_d = nullptr; c.rc.srec_d = nullptr;
     c.rc.nseg = c.rc.ncol = c.rc.ngrp = c.rc.row = 0;
     if (nk == 0 || c.n == 0 || c.rc.nmax + 1 > TAB_MAX || !c.srec) return 0;
     std::vector<int> kn(3 * (size_t)nk);
@@ -816,18 +919,22 @@ int mp_recip_prepare(Ctx &c) {
     std::vector<int4> col, seg, grp;
     std::vector<float2> cxy;
     std::vector<float4> kzr(nk);
+    std::vector<double2> cxy_d;
+    std::vector<double4> kzr_d(nk);
     for (int k = 0; k < nk; k++) {
         const int nx = kn[k], ny = kn[nk + k], nz = kn[2 * nk + k];
         const bool start = k == 0 || nx != kn[k - 1] || ny != kn[nk + k - 1] || nz != kn[2 * nk + k - 1] + 1;
         if (start) {
             col.push_back(make_int4(k, 0, (int)(((unsigned)nx & 0xffffu) | ((unsigned)ny << 16)), nz));
             cxy.push_back(make_float2((float)kv[k], (float)kv[nk + k]));
+            cxy_d.push_back(make_double2(kv[k], kv[nk + k]));
         } else if (kv[k] != kv[k - 1] || kv[nk + k] != kv[nk + k - 1]) {
             return 0;  // (kx, ky) varies within a column: not an orthorhombic k set
         }
         col.back().y++;
         const double kz = kv[2 * (size_t)nk + k];
         kzr[k] = make_float4((float)kz, (float)(kz * kz), (float)(2.0 * kc[k]), 0.f);
+        kzr_d[k] = make_double4(kz, kz * kz, 2.0 * kc[k], 0.0);
     }
     for (const int4 &cl : col)
         for (int j = 0; j < cl.y; j += TS_SEG)
@@ -846,8 +953,10 @@ int mp_recip_prepare(Ctx &c) {
         return cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) == cudaSuccess;
     };
     if (!put(&c.rc.kseg, seg) || !put(&c.rc.kcol, col) || !put(&c.rc.kgrp, grp) || !put(&c.rc.kzr, kzr) ||
-        !put(&c.rc.kcxy, cxy) ||
-        cudaMalloc((void **)&c.rc.stab, (size_t)c.n * row * sizeof(float2)) != cudaSuccess)
+        !put(&c.rc.kcxy, cxy) || !put(&c.rc.kzr_d, kzr_d) || !put(&c.rc.kcxy_d, cxy_d) ||
+        cudaMalloc((void **)&c.rc.stab, (size_t)c.n * row * sizeof(float2)) != cudaSuccess ||
+        cudaMalloc((void **)&c.rc.stab_d, (size_t)c.n * row * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc((void **)&c.rc.srec_d, (size_t)c.n * 4 * sizeof(double4)) != cudaSuccess)
         return SMD_ERR_CUDA;
     c.rc.nseg = (int)seg.size();
     c.rc.ncol = (int)col.size();
@@ -855,11 +964,17 @@ int mp_recip_prepare(Ctx &c) {
     c.rc.row = row;
     c.rc.tab_n = c.n;
     cudaError_t e = cudaSuccess;
-    if (!e) e = cudaFuncSetAttribute(k_rsk_seg<0, TS_SEG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(row));
-    if (!e) e = cudaFuncSetAttribute(k_rsk_seg<1, TS_SEG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(row));
-    if (!e) e = cudaFuncSetAttribute(k_rsk_seg<2, TS_SEG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsum_smem(row));
-    if (!e) e = cudaFuncSetAttribute(k_rforce_grp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tforce_smem(zs));
-    if (!e) e = cudaFuncSetAttribute(k_rforce_grp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tforce_smem(zs));
+    const cudaFuncAttribute dyn = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if (!e) e = cudaFuncSetAttribute(k_rsk_seg<float, 0, TS_SEG>, dyn, (int)tsum_smem<float>(row));
+    if (!e) e = cudaFuncSetAttribute(k_rsk_seg<float, 1, TS_SEG>, dyn, (int)tsum_smem<float>(row));
+    if (!e) e = cudaFuncSetAttribute(k_rsk_seg<float, 2, TS_SEG>, dyn, (int)tsum_smem<float>(row));
+    if (!e) e = cudaFuncSetAttribute(k_rsk_seg<double, 0, TS_SEG>, dyn, (int)tsum_smem<double>(row));
+    if (!e) e = cudaFuncSetAttribute(k_rsk_seg<double, 1, TS_SEG>, dyn, (int)tsum_smem<double>(row));
+    if (!e) e = cudaFuncSetAttribute(k_rsk_seg<double, 2, TS_SEG>, dyn, (int)tsum_smem<double>(row));
+    if (!e) e = cudaFuncSetAttribute(k_rforce_grp<float, false>, dyn, (int)tforce_smem<float>(zs));
+    if (!e) e = cudaFuncSetAttribute(k_rforce_grp<float, true>, dyn, (int)tforce_smem<float>(zs));
+    if (!e) e = cudaFuncSetAttribute(k_rforce_grp<double, false>, dyn, (int)tforce_smem<double>(zs));
+    if (!e) e = cudaFuncSetAttribute(k_rforce_grp<double, true>, dyn, (int)tforce_smem<double>(zs));
     return e == cudaSuccess ? 0 : SMD_ERR_CUDA;
 }
 
@@ -906,28 +1021,51 @@ int chunks_for(const void *kernel, int kblocks) {
     return ch < 1 ? 1 : (ch > MK_CHUNKS ? MK_CHUNKS : ch);
 }
 
+// the column passes apply: an orthorhombic k set in column order, tables
+// for the current site count
+bool column_passes(const Ctx &c) { return c.rc.kseg && c.rc.tab_n == c.n; }
+
+template <typename T, int MODE>
+int column_sums(Ctx &c, double *partial) {
+    const int nk = c.rc.nk, nt = c.rc.nmax + 1, row = c.rc.row;
+    const long long ntab = (long long)c.n * row;
+    typename ColT<T>::T2 *stab;
+    const typename ColT<T>::T4 *ssv;
+    if (sizeof(T) == 4) {
+        stab = (typename ColT<T>::T2 *)c.rc.stab;
+        ssv = (const typename ColT<T>::T4 *)c.srec;   // the frames kernel and the solve keep them current
+    } else {
+        stab = (typename ColT<T>::T2 *)c.rc.stab_d;
+        ssv = (const typename ColT<T>::T4 *)c.rc.srec_d;
+        k_pack_srec_d<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.pos4, c.type_q, c.mu, c.qd,
+                                                              c.ind_on ? c.pind : nullptr, c.rc.srec_d);
+    }
+    k_site_tab<T><<<(unsigned)((ntab + 255) / 256), 256, 0, c.stream>>>(c.n, nt, row, c.fixq, c.pos4, c.box, stab);
+    constexpr int TH = ColT<T>::SUM_THREADS;
+    const int kbt = (c.rc.nseg + TH - 1) / TH;
+    const size_t sm = tsum_smem<T>(row);
+    const int ch = sm_count() * blocks_per_sm((const void *)k_rsk_seg<T, MODE, TS_SEG>, TH, sm) / kbt;
+    const int nch = ch < 1 ? 1 : (ch > MK_CHUNKS ? MK_CHUNKS : ch);
+    k_rsk_seg<T, MODE, TS_SEG><<<dim3(kbt, nch), TH, sm, c.stream>>>(c.n, nk, c.rc.nseg, nt, row, c.rc.kseg,
+                                                                     c.rc.kvec, stab, ssv, partial);
+    return nch;
+}
+
 template <int MODE>
 void sums(Ctx &c, int slot_e, int slot_e2 = -1) {
     const int nk = c.rc.nk;
     RecipBufs B = bufs(c);
     const int kb = (nk + MK_THREADS - 1) / MK_THREADS;
     int nch;
-    if (c.precision == SMD_PREC_MIXED && c.rc.kseg && c.rc.tab_n == c.n) {
-        const int nt = c.rc.nmax + 1, row = c.rc.row;
-        const long long ntab = (long long)c.n * row;
-        k_site_tab<<<(unsigned)((ntab + 255) / 256), 256, 0, c.stream>>>(c.n, nt, row, c.fixq, c.rc.stab);
-        const int kbt = (c.rc.nseg + TS_THREADS - 1) / TS_THREADS;
-        const size_t sm = tsum_smem(row);
-        int ch = sm_count() * blocks_per_sm((const void *)k_rsk_seg<MODE, TS_SEG>, TS_THREADS, sm) / kbt;
-        nch = ch < 1 ? 1 : (ch > MK_CHUNKS ? MK_CHUNKS : ch);
-        k_rsk_seg<MODE, TS_SEG><<<dim3(kbt, nch), TS_THREADS, sm, c.stream>>>(c.n, nk, c.rc.nseg, nt, row, c.rc.kseg,
-                                                                             c.rc.kvec, c.rc.stab, c.srec,
-                                                                             B.partial);
+    if (c.precision == SMD_PREC_MIXED && column_passes(c)) {
+        nch = column_sums<float, MODE>(c, B.partial);
     } else if (c.precision == SMD_PREC_MIXED) {
         nch = chunks_for((const void *)k_rsk_partial_f<MODE>, kb);
         k_rsk_partial_f<MODE><<<dim3(kb, nch), MK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn,
                                                                           c.rc.kvec, c.type_q, c.mu, c.qd, c.pind,
                                                                           B.partial);
+    } else if (column_passes(c) && !c.reference_forms) {
+        nch = column_sums<double, MODE>(c, B.partial);
     } else {
         nch = chunks_for((const void *)k_rsk_partial<double, MODE>, kb);
         k_rsk_partial<double, MODE><<<dim3(kb, nch), MK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn,
@@ -946,21 +1084,31 @@ int ksplit_for(const void *kernel, int sblocks, int nk) {
     return ks < 1 ? 1 : (ks > tiles ? tiles : ks);
 }
 
+template <typename T, bool IND>
+void column_forces(Ctx &c, const double *sk) {
+    constexpr int TH = ColT<T>::F_THREADS;
+    const int nbs = (c.n + TH - 1) / TH;
+    const int ng = c.rc.ngrp;
+    const int zs = zrow(c.rc.nmax);
+    const size_t sm = tforce_smem<T>(zs);
+    int ks = sm_count() * blocks_per_sm((const void *)k_rforce_grp<T, IND>, TH, sm) / nbs;
+    ks = ks < 1 ? 1 : (ks > ng ? ng : ks);
+    const typename ColT<T>::T2 *kcxy = (const typename ColT<T>::T2 *)(sizeof(T) == 4 ? (void *)c.rc.kcxy
+                                                                                     : (void *)c.rc.kcxy_d);
+    const typename ColT<T>::T4 *kzr = (const typename ColT<T>::T4 *)(sizeof(T) == 4 ? (void *)c.rc.kzr
+                                                                                    : (void *)c.rc.kzr_d);
+    k_rforce_grp<T, IND><<<dim3(nbs, ks), TH, sm, c.stream>>>(c.n, c.rc.nk, zs, ng, c.box, c.pos4, c.fixq, c.rc.kgrp,
+                                                              c.rc.kcol, kcxy, kzr, sk, c.type_q, c.mu, c.qd,
+                                                              c.pind, c.frc, c.trq);
+}
+
 template <bool PERM, bool IND>
 void forces(Ctx &c) {
     const int nk = c.rc.nk;
     RecipBufs B = bufs(c);
     const int nb = (int)(((long long)c.n * F_TPS + 255) / 256);
-    if (c.precision == SMD_PREC_MIXED && PERM && c.rc.kseg && c.rc.tab_n == c.n) {
-        const int nbs = (c.n + CF_THREADS - 1) / CF_THREADS;
-        const int ng = c.rc.ngrp;
-        const int zs = zrow(c.rc.nmax);
-        const size_t sm = tforce_smem(zs);
-        int ks = sm_count() * blocks_per_sm((const void *)k_rforce_grp<IND>, CF_THREADS, sm) / nbs;
-        ks = ks < 1 ? 1 : (ks > ng ? ng : ks);
-        k_rforce_grp<IND><<<dim3(nbs, ks), CF_THREADS, sm, c.stream>>>(c.n, nk, zs, ng, c.pos4, c.fixq, c.rc.kgrp,
-                                                                      c.rc.kcol, c.rc.kcxy, c.rc.kzr, B.sk,
-                                                                      c.type_q, c.mu, c.qd, c.pind, c.frc, c.trq);
+    if (c.precision == SMD_PREC_MIXED && PERM && column_passes(c)) {
+        column_forces<float, IND>(c, B.sk);
     } else if (c.precision == SMD_PREC_MIXED) {
         if (PERM) {
             const int ks = ksplit_for((const void *)k_rforce_f<IND>, nb, nk);
@@ -973,6 +1121,8 @@ void forces(Ctx &c) {
                                                                           c.rc.kvec, c.rc.kcoef, B.sk, c.type_q,
                                                                           c.mu, c.qd, c.pind, c.frc, c.trq);
         }
+    } else if (PERM && column_passes(c) && !c.reference_forms) {
+        column_forces<double, IND>(c, B.sk);
     } else {
         const int ks = ksplit_for((const void *)k_rforce<double, PERM, IND>, nb, nk);
         k_rforce<double, PERM, IND><<<dim3(nb, ks), 256, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn,

@@ -480,14 +480,16 @@ __device__ __forceinline__ double ipow_d(double x, int k) {
     return r;
 }
 
-// Mixed path, buffered 14-7 with small integer exponents (NM = n - m and M,
-// 0 = taken at run time): r^2 exact from the box fractions, the pair
-// arithmetic in FP64 with the powers as products and the taper in its
-// well-conditioned form S = (1-t)^3 (1 + 3t + 6t^2).  Every pair quantity
+// Buffered 14-7 with small integer exponents (NM = n - m and M, 0 = taken
+// at run time), the pair arithmetic in FP64 with the powers as products and
+// the taper in its well-conditioned form S = (1-t)^3 (1 + 3t + 6t^2).
+// FIXQ (mixed path): r^2 exact from the box fractions; every pair quantity
 // carries FP64 rounding only, at a lower cost on B200 than the FP32 path's
-// error-tracking arithmetic (buff_pair_f).  Same list walk, accumulation
-// and outputs as k_pair.
-template <int TPP, int NM, int M>
+// error-tracking arithmetic (buff_pair_f).  !FIXQ (FP64 path): r from the
+// FP64 positions, minimum image as the reference's apply_pbc; the same
+// arithmetic as the reference's pow() form to FP64 rounding.  Same list
+// walk, accumulation and outputs as k_pair.
+template <int TPP, int NM, int M, bool FIXQ = true>
 __global__ void __launch_bounds__(PAIR_BLOCK) k_buff_d(PairArgs a) {
     __shared__ double s_is[MAX_TYPES * MAX_TYPES], s_ep[MAX_TYPES * MAX_TYPES];
     __shared__ double s_red[PAIR_BLOCK / 32][11];
@@ -510,22 +512,36 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_buff_d(PairArgs a) {
     int npair = 0;
     if (i < a.n) {
         const int cnt = a.nnbr[i];
-        const int4 pif = a.fixq[i];
-        const int ti = pif.w;
+        const int4 pif = FIXQ ? a.fixq[i] : make_int4(0, 0, 0, 0);
+        const double4 pid = FIXQ ? make_double4(0, 0, 0, 0) : a.pos4[i];
+        const int ti = FIXQ ? pif.w : (int)pid.w;
         for (int k = t; k < cnt; k += TPP) {
             const int raw = a.nbr[(size_t)k * a.n + i];
             const int j = raw & 0x7fffffff;
-            const int4 pj = a.fixq[j];
-            const int ix = pj.x - pif.x, iy = pj.y - pif.y, iz = pj.z - pif.z;   // r_j - r_i
-            const unsigned long long s2 = (unsigned long long)((long long)ix * ix) +
-                                          (unsigned long long)((long long)iy * iy) +
-                                          (unsigned long long)((long long)iz * iz);
-            const double r2 = (double)s2 * a.r2scale;
+            double dx, dy, dz, r2;   // r_j - r_i
+            int tj;
+            if (FIXQ) {
+                const int4 pj = a.fixq[j];
+                const int ix = pj.x - pif.x, iy = pj.y - pif.y, iz = pj.z - pif.z;
+                const unsigned long long s2 = (unsigned long long)((long long)ix * ix) +
+                                              (unsigned long long)((long long)iy * iy) +
+                                              (unsigned long long)((long long)iz * iz);
+                r2 = (double)s2 * a.r2scale;
+                dx = ix * ds0; dy = iy * ds1; dz = iz * ds2;
+                tj = pj.w;
+            } else {
+                const double4 pj = a.pos4[j];
+                dx = pbc1(pj.x - pid.x, a.box.L[0], a.box.half[0]);
+                dy = pbc1(pj.y - pid.y, a.box.L[1], a.box.half[1]);
+                dz = pbc1(pj.z - pid.z, a.box.L[2], a.box.half[2]);
+                r2 = dx * dx + dy * dy + dz * dz;
+                tj = (int)pj.w;
+            }
             if (!(r2 <= a.vdw_rc2)) continue;
             npair++;
-            const double ep = s_ep[ti * a.ntypes + pj.w];
+            const double ep = s_ep[ti * a.ntypes + tj];
             if (raw < 0 || ep == 0.0) continue;   // same molecule, or no well
-            const double is = s_is[ti * a.ntypes + pj.w];
+            const double is = s_is[ti * a.ntypes + tj];
             const double ir = rsqrt(r2), r = r2 * ir;
             const double rho = r * is;
             const double rm1 = ipow_d<(M > 1 ? M - 1 : 0)>(rho, mm - 1);
@@ -545,7 +561,6 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_buff_d(PairArgs a) {
                 en *= sv;
             }
             const double fs = -tmpf * ir;
-            const double dx = ix * ds0, dy = iy * ds1, dz = iz * ds2;
             const double fijx = -fs * dx, fijy = -fs * dy, fijz = -fs * dz;
             fx += fijx; fy += fijy; fz += fijz;
             evdw += en;
@@ -726,6 +741,14 @@ void launch_pair(Ctx &c) {
         if (!c.fixq_from_integrate) launch_fixq(c);
         if (c.ewald_on) dispatch_vdw<float, true>(c, a);
         else dispatch_vdw<float, false>(c, a);
+    } else if (buff && a.buff_int && !c.ewald_on && !a.le && !c.reference_forms) {
+        // FP64 path, integer exponents: the same product-form pass on the
+        // FP64 positions
+        const int nb = (int)(((long long)c.n * 8 + PAIR_BLOCK - 1) / PAIR_BLOCK);
+        if (c.buff_n - c.buff_m == 7 && c.buff_m == 7)
+            k_buff_d<8, 7, 7, false><<<nb, PAIR_BLOCK, 0, c.stream>>>(a);
+        else
+            k_buff_d<8, 0, 0, false><<<nb, PAIR_BLOCK, 0, c.stream>>>(a);
     } else {
         if (c.ewald_on) dispatch_vdw<double, true>(c, a);
         else dispatch_vdw<double, false>(c, a);

@@ -300,6 +300,11 @@ class GpuEnsemble:
         except Exception:
             pass
 
+    def set_reference_forms(self, on: bool):
+        """FP64 path: the reference's pow() and per-(site, k) sine forms
+        instead of the product form and the column passes."""
+        self._chk(self.lib.smd_set_reference_forms(self.ctx, int(bool(on))))
+
     def set_precision(self, precision: str):
         self.precision = precision
         self._chk(self.lib.smd_set_precision(self.ctx, L.PREC_MIXED if precision == "mixed" else L.PREC_FP64))

@@ -61,6 +61,15 @@ def lj4000():
     return s, [("forces",), ("run", 20)]
 
 
+def lj4000_jitter():
+    # the benchmark lattice starts as a perfect FCC crystal, whose forces
+    # vanish by symmetry: the full-size force check uses the same lattice with
+    # every atom displaced by up to 0.05 sigma
+    s = systems.lj_fluid(ncell=10, jitter_star=0.05, seed=1)
+    s.config.long_correct = True
+    return s, [("forces",)]
+
+
 def nacl8000_mie():
     s = systems.nacl_melt(ncell=20, potential="mie", kmax=10, seed=1)
     return s, [("forces",), ("mie",)]
@@ -80,7 +89,7 @@ def polwater4096():
 
 CASES = {"lj500": lj500, "nacl1000_mie": nacl1000_mie, "spce512": spce512,
          "polwater216": polwater216}
-LARGE = {"lj4000": lj4000, "nacl8000_mie": nacl8000_mie, "spce2160": spce2160,
+LARGE = {"lj4000": lj4000, "lj4000_jitter": lj4000_jitter, "nacl8000_mie": nacl8000_mie, "spce2160": spce2160,
          "polwater4096": polwater4096}
 
 

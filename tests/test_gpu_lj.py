@@ -71,6 +71,7 @@ def test_leapfrog_nose_hoover_trajectory():
     assert np.allclose(st["vel"].reshape(-1), g["r_final_vel"], rtol=0, atol=1e-9)
     o = lf.observables()
     assert o.step == 20
+    assert o.list_updates == int(g["r_step_nupdates"][-1])   # numUpdates: rebuilds of the run
     p_ref = g["r_step_atompressure"].reshape(-1, 9)[-1]
     assert np.allclose(np.array(o.atom_pressure), p_ref, rtol=1e-8, atol=1e-6)
 

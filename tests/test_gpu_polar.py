@@ -208,3 +208,25 @@ def test_polar_trajectory():
     assert np.allclose(ser[:, 2], g["r_step_atomtemp"], rtol=1e-7)
     st = e.state()
     assert np.allclose(st["pos"].reshape(-1), g["r_final_pos"], rtol=0, atol=1e-9)
+
+
+@pytest.mark.parametrize("reference_forms", [False, True])
+def test_fp64_forms_against_reference(reference_forms):
+    # the FP64 path by its default algorithms (column reciprocal passes with
+    # exact 64-bit phases, product-form 14-7) and by the reference's own forms
+    # (one sine/cosine per (site, k), pow()) both give the reference's forces
+    g = golden("polwater216")
+    e = engine.GpuEnsemble(_pw())
+    e.set_reference_forms(reference_forms)
+    e.set_solver(tol=1e-13, max_iter=1000)
+    for term, key in ((L.TERM_VDW, "f_buff_force"), (L.TERM_MP_LONG, "f_mp_long_force"),
+                      (L.TERM_IND_LONG, "f_ind_long_force")):
+        f, _, _ = e.compute_forces(term)
+        err = rms_rel(f, g[key].reshape(-1, 3))
+        print(reference_forms, key, err)
+        assert err < 1e-10
+    f_all, _, _ = e.compute_forces()
+    ref = sum(g[k].reshape(-1, 3) for k in ("f_buff_force", "f_mp_short_force", "f_mp_long_force",
+                                            "f_ind_short_force", "f_ind_long_force"))
+    assert rms_rel(f_all, ref) < 1e-9
+    e.close()
