@@ -275,7 +275,7 @@ static int mode_run(int nsteps, const char *out) {
         rec("start_vtminus", vm);
     }
     std::vector<double> epot, ekin, atemp, zeta, press, nupd;
-    std::vector<double> ptensor;
+    std::vector<double> ptensor, mtensor;
     double run_seconds = 0.0;
     for (int k = 0; k < nsteps; k++) {
         timespec t0, t1;
@@ -290,6 +290,7 @@ static int mode_run(int nsteps, const char *out) {
         zeta.push_back(lf->fnh);
         nupd.push_back(lf->numUpdates);
         for (int q = 0; q < 9; q++) ptensor.push_back(e->atomPressure[q]);
+        for (int q = 0; q < 9; q++) mtensor.push_back(e->molPressure[q]);
     }
     rec("step_epot", epot);
     rec("step_ekin", ekin);
@@ -297,6 +298,7 @@ static int mode_run(int nsteps, const char *out) {
     rec("step_zeta", zeta);
     rec("step_nupdates", nupd);
     rec("step_atompressure", ptensor);
+    rec("step_molpressure", mtensor);
     rec1("run_seconds", run_seconds);
     dump_state(e, "final");
     dump_forces(e, "final");
