@@ -54,6 +54,9 @@ enum {
     SMD_TERM_IND_SHORT = 32, /* Induction::compute(): dipole solve, self, real, intra */
     SMD_TERM_IND_LONG = 64,  /* Induction::compute_long() (solves the dipoles if no
                                 earlier call did for these positions) */
+    SMD_TERM_BOND = 128,     /* BondForce::compute() */
+    SMD_TERM_ANGLE = 256,    /* AngleForce::compute() */
+    SMD_TERM_UB = 512,       /* UreyBradleyForce::compute() */
     SMD_TERM_ALL = 0xffff
 };
 
@@ -69,7 +72,12 @@ enum {
     SMD_E_POL_LONG = 7,  /* myEnergy.longPolEnergy */
     SMD_E_POL_SELF = 8,  /* myEnergy.correctPolEnergy */
     SMD_E_POL_INTRA = 9, /* myEnergy.molCorrectPolEnergy */
-    SMD_E_COUNT = 12
+    SMD_E_POL_SURF = 10, /* myEnergy.surfacePolEnergy */
+    SMD_E_BOND = 11,     /* myEnergy.bondEnergy */
+    SMD_E_ANGLE = 12,    /* myEnergy.angleEnergy */
+    SMD_E_UB = 13,       /* myEnergy.ubEnergy */
+    SMD_E_TERMS = 14,    /* components summed into e_potential */
+    SMD_E_COUNT = 16
 };
 
 /* vdW kinds for smd_set_vdw */
@@ -176,6 +184,26 @@ int smd_set_ewald(smd_ctx *ctx, double alpha, double kcut, double real_cut);
 int smd_set_buff(smd_ctx *ctx, const double *params, double n, double m, double delta,
                  double gamma, double h_factor, int switch_on, double switch_dist,
                  const double *taper_c, double e_lrc, double v_lrc);
+/* Bonded terms of flexible molecules (BondForce, AngleForce,
+ * UreyBradleyForce; src/forces/BondForce.cpp:37-110, AngleForce.cpp:34-130,
+ * UreyBradleyForce.cpp:39-100).  bonds[3*nbonds] = (atom1, atom2, type),
+ * bond_params[2*type] = (r0 nm, k); angles[4*nangles] = (atom1, atom2 (the
+ * apex), atom3, type), angle_params[2*type] = (theta0 rad, k).  form: 1
+ * harmonic (U = k/2 d^2), 2 AMOEBA anharmonic (the reference's bendType 2:
+ * quartic bond, sextic-in-degrees angle).  ub_on: the harmonic H-H term
+ * k_ub (r - l0)^2 between the first and third site of every molecule.
+ * nbonds = nangles = 0 and ub_on = 0 turn the terms off. */
+int smd_set_bonded(smd_ctx *ctx, int nbonds, const int32_t *bonds, int nbond_types, const double *bond_params,
+                   int nangles, const int32_t *angles, int nangle_types, const double *angle_params, int form,
+                   int ub_on, double k_ub, double l0_ub);
+/* Surface-dipole corrections (the surfCorrect option) of the point-charge
+ * Ewald sum, the permanent multipoles and the induced dipoles
+ * (EwaldForce::surfDipoleCorrect, src/forces/EwaldForce.cpp:816-937;
+ * Multipole::surfDipoleCorrect, Multipole.cpp:1753-1920;
+ * Induction::surfDipoleCorrect, Induction.cpp:2188-2380): evaluated with
+ * SMD_TERM_EWALD_REAL, SMD_TERM_MP_SHORT and SMD_TERM_IND_SHORT as the
+ * reference evaluates them inside those terms' compute(). */
+int smd_set_surface_correct(smd_ctx *ctx, int on);
 /* Polarisable multipole model (Multipole + Induction, src/forces/Multipole.cpp,
  * src/forces/Induction.cpp) for 3-site H O H molecules.  type_mp: per type
  * local-frame dipole (3) and traceless quadrupole (xx xy xz yy yz zz) as in

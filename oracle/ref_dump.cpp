@@ -49,6 +49,9 @@
 #include "forces/EwaldForce.h"
 #include "forces/Multipole.h"
 #include "forces/Induction.h"
+#include "forces/BondForce.h"
+#include "forces/AngleForce.h"
+#include "forces/UreyBradleyForce.h"
 #undef class
 #undef private
 #undef protected
@@ -141,11 +144,11 @@ static void dump_forces(Ensemble *e, const char *tag) {
     const Energy &E = e->myEnergy;
     std::string d = std::string(tag) + "_energy";
     // order: lj real long correct molCorrect surfCorrect realPol longPol
-    //        correctPol molCorrectPol surfacePol
+    //        correctPol molCorrectPol surfacePol bond angle ub
     rec(d.c_str(), {E.ljEnergy, E.realEnergy, E.longEnergy, E.correctEnergy,
                     E.molCorrectEnergy, E.surfCorrectEnergy, E.realPolEnergy,
                     E.longPolEnergy, E.correctPolEnergy, E.molCorrectPolEnergy,
-                    E.surfacePolEnergy});
+                    E.surfacePolEnergy, E.bondEnergy, E.angleEnergy, E.ubEnergy});
 }
 
 static void header(Setup &s) {
@@ -234,6 +237,26 @@ static int mode_forces(const char *out) {
             ind.compute_long();
             dump_forces(e, "ind_long");
         }
+    }
+    // bonded terms of flexible molecules (Integrator::initialise,
+    // src/Integrator.cpp:163-190)
+    if (!c->is_constraint_on() && e->nBonds > 0) {
+        zero(e);
+        BondForce f(e);
+        f.compute();
+        dump_forces(e, "bond");
+    }
+    if (!c->is_constraint_on() && e->nAngles > 0) {
+        zero(e);
+        AngleForce f(e);
+        f.compute();
+        dump_forces(e, "angle");
+    }
+    if (c->compute_harmonic_ub()) {
+        zero(e);
+        UreyBradleyForce f(e);
+        f.compute();
+        dump_forces(e, "ub");
     }
     fclose(g_out);
     return 0;

@@ -21,8 +21,10 @@ SMD_ERR_SHAKE, SMD_ERR_NAN, SMD_ERR_CG, SMD_ERR_NO_DEVICE, SMD_ERR_TIMEOUT = 5, 
 PREC_FP64, PREC_MIXED = 0, 1
 TERM_VDW, TERM_EWALD_REAL, TERM_EWALD_LONG, TERM_ALL = 1, 2, 4, 0xFFFF
 TERM_MP_SHORT, TERM_MP_LONG, TERM_IND_SHORT, TERM_IND_LONG = 8, 16, 32, 64
+TERM_BOND, TERM_ANGLE, TERM_UB = 128, 256, 512
 E_VDW, E_REAL, E_LONG, E_CORRECT, E_MOLCORRECT, E_SURF = 0, 1, 2, 3, 4, 5
-E_POL_REAL, E_POL_LONG, E_POL_SELF, E_POL_INTRA, E_COUNT = 6, 7, 8, 9, 12
+E_POL_REAL, E_POL_LONG, E_POL_SELF, E_POL_INTRA = 6, 7, 8, 9
+E_POL_SURF, E_BOND, E_ANGLE, E_UB, E_TERMS, E_COUNT = 10, 11, 12, 13, 14, 16
 VDW_NONE, VDW_LJ, VDW_MIE, VDW_BMH, VDW_BUFF = 0, 1, 2, 3, 4
 GUESS_DIRECT, GUESS_PREVIOUS, GUESS_LEARNED, GUESS_FIRST_ORDER = 0, 1, 2, 3
 PRECOND_SITE, PRECOND_MOLECULE = 0, 1
@@ -101,6 +103,9 @@ SIGNATURES = {
     "smd_set_buff": (ctypes.c_int, [_P, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                     _D, ctypes.c_double, ctypes.c_double]),
+    "smd_set_bonded": (ctypes.c_int, [_P, ctypes.c_int, _I, ctypes.c_int, _D, ctypes.c_int, _I, ctypes.c_int, _D,
+                                      ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double]),
+    "smd_set_surface_correct": (ctypes.c_int, [_P, ctypes.c_int]),
     "smd_set_multipole": (ctypes.c_int, [_P, _D, _D, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_double]),

@@ -143,6 +143,29 @@ public:
         // (src/forces/EwaldForce.cpp:33-39)
         if (cfg->compute_ewald_force())
             check(ctx, smd_set_ewald(ctx, cfg->get_alpha(), cfg->get_k_cutoff(), cfg->get_cutoff()), "smd_set_ewald");
+        // rigid molecules: the SHAKE distances of LFIntegrator::initialise
+        // (src/integrators/LFIntegrator.cpp:141-167); they also tell the
+        // library that the intramolecular corrections are energies only
+        if (cfg->is_constraint_on()) {
+            std::vector<double> len2(3 * (size_t)e->nMols, 0.0);
+            for (int m = 0; m < e->nMols; m++) {
+                Molecule &mol = e->molecules[m];
+                if (mol.numAtoms < 2) continue;
+                const int a0 = mol.myAtoms[0]->atomID, a1 = mol.myAtoms[1]->atomID;
+                const double l01 = e->myParams->get_bond_length(a0, a1);
+                len2[3 * m] = l01 * l01;
+                if (mol.numAtoms >= 3) {
+                    const int a2 = mol.myAtoms[2]->atomID;
+                    const double l12 = e->myParams->get_bond_length(a1, a2);
+                    const double l02 = e->myParams->get_bond_length(a0, a1, a2);
+                    len2[3 * m + 1] = l12 * l12;
+                    len2[3 * m + 2] = l02 * l02;
+                } else {
+                    len2[3 * m + 1] = len2[3 * m + 2] = len2[3 * m];
+                }
+            }
+            check(ctx, smd_set_constraints(ctx, len2.data()), "smd_set_constraints");
+        }
         check(ctx, smd_set_precision(ctx, precision), "smd_set_precision");
     }
     ~GpuPath() { smd_destroy(ctx); }

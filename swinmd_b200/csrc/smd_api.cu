@@ -156,6 +156,7 @@ void enqueue_polar(Ctx &c, bool mp_short, bool mp_long, bool ind_short, bool ind
         if (!solved) launch_ind_solve(c);
         launch_polar_short(c);
         launch_polar_long(c);
+        launch_surface(c, false, true, true);
         launch_torques_end(c);
         return;
     }
@@ -174,6 +175,8 @@ void enqueue_polar(Ctx &c, bool mp_short, bool mp_long, bool ind_short, bool ind
             if (ind_long) launch_ind_long(c);
         }
     }
+    // Multipole::compute and Induction::compute add their surface terms
+    launch_surface(c, false, mp_short, ind_short && c.ind_on);
     launch_torques_end(c);
 }
 
@@ -182,8 +185,10 @@ void enqueue_forces(Ctx &c) {
     if (c.ewald_on) {
         launch_intra(c);
         launch_recip(c);
+        launch_surface(c, true, false, false);
     }
     if (c.mp_on) enqueue_polar(c, true, true, true, true);
+    if (has_bonded(c)) launch_bonded(c, true, true, true);
 }
 
 // One MD step: in the FP32 path the integrate kernel of the previous step
@@ -235,10 +240,15 @@ int compute_forces_into(smd_ctx *x, uint32_t terms, double *dforce, double *forc
     bool want_long = (terms & SMD_TERM_EWALD_LONG) && c.ewald_on;
     c.ewald_on = want_real ? 1 : 0;
     launch_pair(c);
-    if (want_real) launch_intra(c);
+    if (want_real) {
+        launch_intra(c);
+        launch_surface(c, true, false, false);   // EwaldForce::compute adds its surface term
+    }
     c.ewald_on = save_ew;
     if (want_long) launch_recip(c);
     c.vdw = save_vdw;
+    if (has_bonded(c))
+        launch_bonded(c, terms & SMD_TERM_BOND, terms & SMD_TERM_ANGLE, terms & SMD_TERM_UB);
     const uint32_t polar = SMD_TERM_MP_SHORT | SMD_TERM_MP_LONG | SMD_TERM_IND_SHORT | SMD_TERM_IND_LONG;
     if (c.mp_on && (terms & polar)) {
         const bool solved = c.ind_on && c.dip_version == c.cfg_version;
@@ -248,6 +258,9 @@ int compute_forces_into(smd_ctx *x, uint32_t terms, double *dforce, double *forc
     if (force) launch_finalize_forces(c, dforce);
     long long hacc[ACC_COUNT];
     CK(cudaMemcpyAsync(hacc, c.acc, sizeof(hacc), cudaMemcpyDeviceToHost, c.stream));
+    // a time step starts from cleared accumulators (the integrator clears
+    // them at the end of every step): leave them so for the next smd_run
+    CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
     if (force) CK(cudaMemcpyAsync(force, dforce, 3 * (size_t)c.n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     const int rs = sync_status(x);
     if (rs) {
@@ -257,19 +270,7 @@ int compute_forces_into(smd_ctx *x, uint32_t terms, double *dforce, double *forc
     if (c.mp_on && c.ind_on && (terms & (SMD_TERM_IND_SHORT | SMD_TERM_IND_LONG)))
         c.dip_version = c.cfg_version;   // solved now, or already before
     const bool vdw = (terms & SMD_TERM_VDW) && c.vdw != VDW_NONE;
-    if (energy) {
-        for (int q = 0; q < SMD_E_COUNT; q++) energy[q] = 0;
-        energy[SMD_E_VDW] = (double)hacc[ACC_E_VDW] * ACC_INV + (vdw ? c.e_lrc : 0.0);
-        energy[SMD_E_REAL] = (double)hacc[ACC_E_REAL] * ACC_INV;
-        energy[SMD_E_LONG] = (double)hacc[ACC_E_LONG] * ACC_INV;
-        energy[SMD_E_CORRECT] = (want_real ? c.e_self : 0.0) + (double)hacc[ACC_E_SELF] * ACC_INV;
-        energy[SMD_E_MOLCORRECT] = (double)hacc[ACC_E_INTRA] * ACC_INV;
-        energy[SMD_E_SURF] = (double)hacc[ACC_E_SURF] * ACC_INV;
-        energy[SMD_E_POL_REAL] = (double)hacc[ACC_E_POL_REAL] * ACC_INV;
-        energy[SMD_E_POL_LONG] = (double)hacc[ACC_E_POL_LONG] * ACC_INV;
-        energy[SMD_E_POL_SELF] = (double)hacc[ACC_E_POL_SELF] * ACC_INV;
-        energy[SMD_E_POL_INTRA] = (double)hacc[ACC_E_POL_INTRA] * ACC_INV;
-    }
+    if (energy) acc_energies(hacc, vdw ? c.e_lrc : 0.0, want_real ? c.e_self : 0.0, energy);
     if (virial) {
         for (int q = 0; q < 9; q++) {
             virial[q] = ((double)hacc[ACC_VIR + q] + (double)hacc[ACC_LVIR + q]) * ACC_INV;
@@ -331,7 +332,8 @@ void smd_destroy(smd_ctx *x) {
                     c.rc.sk, c.rc.kvec, c.clen2, c.type_mp, c.type_polar, c.mu, c.qd, c.trq, c.e0,
                     c.pind, c.cgw, c.cgs, c.cg_bar, c.vpos4, c.vfixq, c.fv, c.ind_rj, c.ind_rc, c.ind_cnt,
                     c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab, c.srec, c.phist, c.cg_blk,
-                    c.upload4, c.fout, c.rc.kzr_d, c.rc.kcxy_d, c.rc.stab_d, c.rc.srec_d};
+                    c.upload4, c.fout, c.rc.kzr_d, c.rc.kcxy_d, c.rc.stab_d, c.rc.srec_d, c.bonds, c.angles,
+                    c.bond_par, c.angle_par, c.surf_part, c.surf_tot};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -580,6 +582,63 @@ int smd_set_buff(smd_ctx *x, const double *params, double n, double m, double de
     CK(dalloc(&c.vpos4, c.n));
     CK(dalloc(&c.vfixq, c.n));
     CK(dalloc(&c.fv, 3 * (size_t)c.n));
+    c.graph_dirty = 1;
+    touch(c);
+    return SMD_OK;
+}
+
+int smd_set_bonded(smd_ctx *x, int nbonds, const int32_t *bonds, int nbond_types, const double *bond_params,
+                   int nangles, const int32_t *angles, int nangle_types, const double *angle_params, int form,
+                   int ub_on, double k_ub, double l0_ub) {
+    if (!x || x->c.n == 0 || nbonds < 0 || nangles < 0 || (nbonds && (!bonds || !bond_params || nbond_types <= 0)) ||
+        (nangles && (!angles || !angle_params || nangle_types <= 0)) || (form != 1 && form != 2))
+        return fail(x, SMD_ERR_ARG, "smd_set_bonded: bad arguments (form must be 1 harmonic or 2 AMOEBA)");
+    Ctx &c = x->c;
+    std::vector<int4> b(std::max(nbonds, 1)), g(std::max(nangles, 1));
+    for (int k = 0; k < nbonds; k++) {
+        const int a1 = bonds[3 * k], a2 = bonds[3 * k + 1], t = bonds[3 * k + 2];
+        if (a1 < 0 || a1 >= c.n || a2 < 0 || a2 >= c.n || t < 0 || t >= nbond_types)
+            return fail(x, SMD_ERR_ARG, "smd_set_bonded: bond " + std::to_string(k) + " out of range");
+        b[k] = make_int4(a1, a2, t, 0);
+    }
+    for (int k = 0; k < nangles; k++) {
+        const int a1 = angles[4 * k], a2 = angles[4 * k + 1], a3 = angles[4 * k + 2], t = angles[4 * k + 3];
+        if (a1 < 0 || a1 >= c.n || a2 < 0 || a2 >= c.n || a3 < 0 || a3 >= c.n || t < 0 || t >= nangle_types)
+            return fail(x, SMD_ERR_ARG, "smd_set_bonded: angle " + std::to_string(k) + " out of range");
+        g[k] = make_int4(a1, a2, a3, t);
+    }
+    if (ub_on)
+        for (int m = 0; m < c.nmol; m++)
+            if (c.h_mol_off[m + 1] - c.h_mol_off[m] < 3)
+                return fail(x, SMD_ERR_ARG, "smd_set_bonded: the Urey-Bradley term needs molecules of 3 sites");
+    std::vector<double2> bp(std::max(nbond_types, 1)), ap(std::max(nangle_types, 1));
+    for (int t = 0; t < nbond_types; t++) bp[t] = make_double2(bond_params[2 * t], bond_params[2 * t + 1]);
+    for (int t = 0; t < nangle_types; t++) ap[t] = make_double2(angle_params[2 * t], angle_params[2 * t + 1]);
+    CK(dalloc(&c.bonds, b.size())); CK(dalloc(&c.angles, g.size()));
+    CK(dalloc(&c.bond_par, bp.size())); CK(dalloc(&c.angle_par, ap.size()));
+    CK(cudaMemcpy(c.bonds, b.data(), b.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.angles, g.data(), g.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.bond_par, bp.data(), bp.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.angle_par, ap.data(), ap.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    c.nbond = nbonds;
+    c.nangle = nangles;
+    c.bond_form = form;
+    c.ub_on = ub_on ? 1 : 0;
+    c.ub_k = k_ub;
+    c.ub_l0 = l0_ub;
+    c.graph_dirty = 1;
+    touch(c);
+    return SMD_OK;
+}
+
+int smd_set_surface_correct(smd_ctx *x, int on) {
+    if (!x || x->c.n == 0 || (on != 0 && on != 1)) return fail(x, SMD_ERR_ARG, "smd_set_surface_correct: bad arguments");
+    Ctx &c = x->c;
+    if (on && !c.surf_part) {
+        CK(dalloc(&c.surf_part, (size_t)SURF_BLOCKS * SURF_SUMS));
+        CK(dalloc(&c.surf_tot, SURF_SUMS));
+    }
+    c.surface_on = on;
     c.graph_dirty = 1;
     touch(c);
     return SMD_OK;

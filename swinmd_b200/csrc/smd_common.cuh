@@ -49,7 +49,11 @@ enum AccSlot {
     ACC_NPAIR = 26,     // pairs inside the short-range cutoff (both directions)
     ACC_E_POL_LONG = 27,  // induced-dipole reciprocal energy
     ACC_E_POL_INTRA = 28, // induced-dipole intramolecular correction
-    ACC_COUNT = 29
+    ACC_E_POL_SURF = 29,  // induced-dipole surface correction
+    ACC_E_BOND = 30,      // bond stretching
+    ACC_E_ANGLE = 31,     // angle bending
+    ACC_E_UB = 32,        // Urey-Bradley
+    ACC_COUNT = 33
 };
 
 // ---- status word bits (ctx->status on device) --------------------------------

@@ -12,6 +12,9 @@ namespace smd {
 
 enum VdwKind { VDW_NONE = 0, VDW_LJ = 1, VDW_MIE = 2, VDW_BMH = 3, VDW_BUFF = 4 };
 
+// surface-correction reduction: blocks of partial sums and sums per block
+constexpr int SURF_BLOCKS = 64, SURF_SUMS = 11;
+
 // Per type pair parameters of the short-range pair term (ntypes^2 rows of 8).
 //   LJ : p0 sigma^2, p1 4 eps, p2 energy at the cutoff (shift), p3 unused
 //   MIE: p0 sigma, p1 Cn*eps, p2 n, p3 m
@@ -148,6 +151,17 @@ struct Ctx {
     int4 *vfixq = nullptr;          // their 32-bit box fractions
     long long *fv = nullptr;        // [3][N] forces on the virtual sites
     int has_multisite = 0;          // some molecule has more than one site
+    // bonded terms of flexible molecules (smd_bonded.cu)
+    int nbond = 0, nangle = 0, bond_form = 1, ub_on = 0;
+    double ub_k = 0, ub_l0 = 0;
+    int4 *bonds = nullptr;          // (atom1, atom2, type, 0)
+    int4 *angles = nullptr;         // (atom1, atom2, atom3, type)
+    double2 *bond_par = nullptr;    // per type (r0, k)
+    double2 *angle_par = nullptr;   // per type (theta0, k)
+    // surface-dipole corrections (smd_surface.cu)
+    int surface_on = 0;
+    double *surf_part = nullptr;    // per-block partial sums
+    double *surf_tot = nullptr;     // the sums
     double *clen2 = nullptr;        // [nmol][3] squared SHAKE distances
     int fixq_from_integrate = 0;    // step graph: integrate writes fixq
     int vdw = VDW_NONE;
@@ -205,6 +219,31 @@ void launch_ind_long(Ctx &c);
 void launch_polar_long(Ctx &c);
 void launch_torques_end(Ctx &c);
 void launch_frames(Ctx &c);
+void launch_bonded(Ctx &c, bool bond, bool angle, bool ub);
+void launch_intra_flex(Ctx &c, bool mp, bool ind);
+void launch_surface(Ctx &c, bool ewald, bool mp, bool ind);
+inline bool has_bonded(const Ctx &c) { return c.nbond > 0 || c.nangle > 0 || c.ub_on; }
+
+// the energy components of the accumulator slots (energy[SMD_E_COUNT]);
+// e_lrc and e_self are the constant tail and self energies added to the
+// vdW and self slots
+__host__ __device__ inline void acc_energies(const long long *acc, double e_lrc, double e_self, double *en) {
+    for (int q = 0; q < SMD_E_COUNT; q++) en[q] = 0.0;
+    en[SMD_E_VDW] = (double)acc[ACC_E_VDW] * ACC_INV + e_lrc;
+    en[SMD_E_REAL] = (double)acc[ACC_E_REAL] * ACC_INV;
+    en[SMD_E_LONG] = (double)acc[ACC_E_LONG] * ACC_INV;
+    en[SMD_E_CORRECT] = e_self + (double)acc[ACC_E_SELF] * ACC_INV;
+    en[SMD_E_MOLCORRECT] = (double)acc[ACC_E_INTRA] * ACC_INV;
+    en[SMD_E_SURF] = (double)acc[ACC_E_SURF] * ACC_INV;
+    en[SMD_E_POL_REAL] = (double)acc[ACC_E_POL_REAL] * ACC_INV;
+    en[SMD_E_POL_LONG] = (double)acc[ACC_E_POL_LONG] * ACC_INV;
+    en[SMD_E_POL_SELF] = (double)acc[ACC_E_POL_SELF] * ACC_INV;
+    en[SMD_E_POL_INTRA] = (double)acc[ACC_E_POL_INTRA] * ACC_INV;
+    en[SMD_E_POL_SURF] = (double)acc[ACC_E_POL_SURF] * ACC_INV;
+    en[SMD_E_BOND] = (double)acc[ACC_E_BOND] * ACC_INV;
+    en[SMD_E_ANGLE] = (double)acc[ACC_E_ANGLE] * ACC_INV;
+    en[SMD_E_UB] = (double)acc[ACC_E_UB] * ACC_INV;
+}
 void launch_buff(Ctx &c);
 int setup_cg(Ctx &c);
 int ensure_ind_rows(Ctx &c);

@@ -1356,6 +1356,86 @@ __global__ void __launch_bounds__(96) k_polar_mol(IndArgs a, long long *trq, lon
     }
 }
 
+// ---------------------------------------------------------------------------
+// forces and torques of the intramolecular corrections (flexible molecules)
+// ---------------------------------------------------------------------------
+// Without constraints the reference also applies the forces and torques of
+// its intramolecular corrections (Multipole::intraMolCorrect,
+// src/forces/Multipole.cpp:1398-1700; Induction::intraMolCorrect,
+// src/forces/Induction.cpp:1900-2140): for every excluded pair of a
+// molecule, the real-space expressions with the erf radial functions D_n in
+// place of the erfc B_n and the opposite sign, undamped.  Their energies
+// are formed by k_mp_mol / k_ind_mol / k_polar_mol with or without
+// constraints; this kernel adds the forces and torques, one thread per
+// molecule, FP64.  No virial: the reference adds none for these terms.
+__global__ void k_intra_flex(IndArgs a, long long *frc, long long *trq, int mp, int ind) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= a.nmol) return;
+    const int s0 = a.mol_off[m], ns = a.mol_off[m + 1] - s0;
+    for (int p = 0; p < ns; p++)
+        for (int q = p + 1; q < ns; q++) {
+            const int i = a.mol_atoms[s0 + p], j = a.mol_atoms[s0 + q];
+            if (!is_excluded(i, j, a.excl_off, a.excl)) continue;
+            const double4 pi = a.pos4[i], pj = a.pos4[j];
+            const V3 r = mind(pi, pj, a.box);   // r_i - r_j
+            const double r2 = dot(r, r);
+            const double qi = a.tq[(int)pi.w] / SQC, qj = a.tq[(int)pj.w] / SQC;
+            const V3 mi = ld3i(a.mu, a.n, i), mj = ld3i(a.mu, a.n, j);
+            const Q6 Qi = ldqi(a.qd, a.n, i), Qj = ldqi(a.qd, a.n, j);
+            double D[6];
+            dn_erf(r2, a.alpha, D);
+            V3 fij = v3(0, 0, 0), ti = v3(0, 0, 0), tj = v3(0, 0, 0);
+            if (mp) {
+                MPPair<double, V3> P;
+                mp_invariants(qi, mi, Qi, qj, mj, Qj, r, P);
+                const double radial = P.G[0] * D[1] + P.G[1] * D[2] + P.G[2] * D[3] + P.G[3] * D[4] + P.G[4] * D[5];
+                fij = fij + (D[1] * P.gG[1] + D[2] * P.gG[2] + D[3] * P.gG[3] + D[4] * P.gG[4] + radial * r);
+                V3 Gi[5], Gj[5];
+                mp_torque_i(qj, mi, Qi, mj, Qj, r, Gi);
+                mp_torque_i(qi, mj, Qj, mi, Qi, -r, Gj);
+                ti = ti - (D[1] * Gi[1] + D[2] * Gi[2] + D[3] * Gi[3] + D[4] * Gi[4]);
+                tj = tj - (D[1] * Gj[1] + D[2] * Gj[2] + D[3] * Gj[3] + D[4] * Gj[4]);
+            }
+            if (ind) {
+                const V3 pii = ld3i(a.p, a.n, i), pjj = ld3i(a.p, a.n, j);
+                const V3 rji = -r;
+                const double QiI = qtr(Qi), QjI = qtr(Qj);
+                const V3 Qir = qv(Qi, r), Qjrji = qv(Qj, rji);
+                const double QiRij = dot(r, Qir), QjRji = dot(r, qv(Qj, r));
+                const double pjr = dot(pjj, r), pirji = dot(pii, rji);
+                const double G1i = -qi * pjr - dot(mi, pjj);
+                const double G2i = -dot(mi, r) * pjr - 2.0 * dot(pjj, Qir) - pjr * QiI;
+                const double G3i = -pjr * QiRij;
+                const double G1j = -qj * pirji - dot(mj, pii);
+                const double G2j = -dot(mj, rji) * pirji - 2.0 * dot(pii, Qjrji) - pirji * QjI;
+                const double G3j = -pirji * QjRji;
+                const V3 gG1i = -qi * pjj;
+                const V3 gG2i = (-pjr) * mi - dot(mi, r) * pjj - 2.0 * qv(Qi, pjj) - QiI * pjj;
+                const V3 gG3i = (-QiRij) * pjj - (2 * pjr) * Qir;
+                const V3 gG1j = -qj * pii;
+                const V3 gG2j = (-pirji) * mj - dot(mj, rji) * pii - 2.0 * qv(Qj, pii) - QjI * pii;
+                const V3 gG3j = (-QjRji) * pii - (2 * pirji) * Qjrji;
+                const V3 fi = D[1] * gG1i + D[2] * gG2i + D[3] * gG3i + (G1i * D[2] + G2i * D[3] + G3i * D[4]) * r;
+                const V3 fj = D[1] * gG1j + D[2] * gG2j + D[3] * gG3j + (G1j * D[2] + G2j * D[3] + G3j * D[4]) * rji;
+                fij = fij + (fi - fj);
+                // torque coefficients as the real-space term's, for i and with i, j swapped
+                const V3 Gt1i = crs(mi, pjj);
+                const V3 Gt2i = pjr * crs(mi, r) + 2.0 * crs(Qir, pjj) + 2.0 * crs(qv(Qi, pjj), r);
+                const V3 Gt3i = (2.0 * pjr) * crs(Qir, r);
+                const V3 Gt1j = crs(mj, pii);
+                const V3 Gt2j = pirji * crs(mj, rji) + 2.0 * crs(Qjrji, pii) + 2.0 * crs(qv(Qj, pii), rji);
+                const V3 Gt3j = (2.0 * pirji) * crs(Qjrji, rji);
+                ti = ti - (D[1] * Gt1i + D[2] * Gt2i + D[3] * Gt3i);
+                tj = tj - (D[1] * Gt1j + D[2] * Gt2j + D[3] * Gt3j);
+            }
+            add_fix3_at(frc, a.n, i, fij, COU);
+            add_fix3_at(frc, a.n, j, -fij, COU);
+            add_fix3_at(trq, a.n, i, ti, COU);
+            add_fix3_at(trq, a.n, j, tj, COU);
+        }
+}
+
+
 // ring of the last 4 steps' converged dipoles and permanent fields;
 // flags[2] counts the stored steps
 // Stores the step's dipoles and permanent field in ring slot flags[2] & 3.
@@ -1390,6 +1470,14 @@ static IndArgs ind_args(Ctx &c) {
     a.box = c.box; a.cut2 = c.ind_cut2; a.a = c.thole_a; a.alpha = c.ew_alpha; a.rc2 = c.mp_rc2;
     a.e0 = c.e0; a.p = c.pind;
     return a;
+}
+
+void launch_intra_flex(Ctx &c, bool mp, bool ind) {
+    // rigid molecules (constraint lengths set): the reference applies these
+    // corrections as energies only
+    if (c.clen2 || !(mp || ind)) return;
+    k_intra_flex<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(ind_args(c), c.frc, c.trq, mp ? 1 : 0,
+                                                            ind && c.ind_on ? 1 : 0);
 }
 
 int setup_cg(Ctx &c) {
@@ -1585,6 +1673,7 @@ void launch_ind_short(Ctx &c) {
         k_ind_real<<<nb, 64, 0, c.stream>>>(A);
     }
     k_ind_mol<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(A.ia, c.trq, c.acc);
+    launch_intra_flex(c, false, true);
 }
 
 bool polar_short_fused(const Ctx &c) {
@@ -1617,6 +1706,7 @@ void launch_polar_short(Ctx &c) {
     else
         k_polar_real_f<false><<<nb, 128, 0, c.stream>>>(A);
     k_polar_mol<<<(c.nmol * PM_TPM + 95) / 96, 96, 0, c.stream>>>(A.ia, c.trq, c.acc);
+    launch_intra_flex(c, true, true);
 }
 
 }  // namespace smd

@@ -391,19 +391,10 @@ __global__ void __launch_bounds__(INT_BLOCK) k_integrate(IntArgs a) {
         o.ke_mol = 0.5 * keM;
         o.t_atom = keA / (a.atom_ndf * KB);
         o.t_mol = keM / (a.mol_ndf * KB);
-        double en[10];
-        en[SMD_E_VDW] = (double)acc[ACC_E_VDW] * ACC_INV + a.e_lrc;
-        en[SMD_E_REAL] = (double)acc[ACC_E_REAL] * ACC_INV;
-        en[SMD_E_LONG] = (double)acc[ACC_E_LONG] * ACC_INV;
-        en[SMD_E_CORRECT] = a.e_self + (double)acc[ACC_E_SELF] * ACC_INV;
-        en[SMD_E_MOLCORRECT] = (double)acc[ACC_E_INTRA] * ACC_INV;
-        en[SMD_E_SURF] = (double)acc[ACC_E_SURF] * ACC_INV;
-        en[SMD_E_POL_REAL] = (double)acc[ACC_E_POL_REAL] * ACC_INV;
-        en[SMD_E_POL_LONG] = (double)acc[ACC_E_POL_LONG] * ACC_INV;
-        en[SMD_E_POL_SELF] = (double)acc[ACC_E_POL_SELF] * ACC_INV;
-        en[SMD_E_POL_INTRA] = (double)acc[ACC_E_POL_INTRA] * ACC_INV;
+        double en[SMD_E_COUNT];
+        acc_energies(acc, a.e_lrc, a.e_self, en);
         double ep = 0;
-        for (int q = 0; q < 10; q++) {
+        for (int q = 0; q < SMD_E_COUNT; q++) {
             o.energy[q] = en[q];
             ep += en[q];
         }

@@ -420,6 +420,7 @@ void launch_mp_short(Ctx &c) {
         k_mp_real<tpp><<<nb, 128, 0, c.stream>>>(a);
     }
     launch_mp_mol(c);
+    launch_intra_flex(c, true, false);   // flexible molecules: the correction's forces and torques
 }
 
 // self energy and intramolecular correction of the multipoles

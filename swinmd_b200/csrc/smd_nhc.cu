@@ -271,18 +271,15 @@ __global__ void __launch_bounds__(NHC_BLOCK) k_nhc_second(NhcArgs a) {
         o.t_atom = keA / (a.atom_ndf * KB_N);
         o.t_mol = keM / (a.mol_ndf * KB_N);
         const long long *acc = a.acc;
-        o.energy[SMD_E_VDW] = (double)__ldcg(&acc[ACC_E_VDW]) * ACC_INV + a.e_lrc;
-        o.energy[SMD_E_REAL] = (double)__ldcg(&acc[ACC_E_REAL]) * ACC_INV;
-        o.energy[SMD_E_LONG] = (double)__ldcg(&acc[ACC_E_LONG]) * ACC_INV;
-        o.energy[SMD_E_CORRECT] = a.e_self + (double)__ldcg(&acc[ACC_E_SELF]) * ACC_INV;
-        o.energy[SMD_E_MOLCORRECT] = (double)__ldcg(&acc[ACC_E_INTRA]) * ACC_INV;
-        o.energy[SMD_E_SURF] = (double)__ldcg(&acc[ACC_E_SURF]) * ACC_INV;
-        o.energy[SMD_E_POL_REAL] = (double)__ldcg(&acc[ACC_E_POL_REAL]) * ACC_INV;
-        o.energy[SMD_E_POL_LONG] = (double)__ldcg(&acc[ACC_E_POL_LONG]) * ACC_INV;
-        o.energy[SMD_E_POL_SELF] = (double)__ldcg(&acc[ACC_E_POL_SELF]) * ACC_INV;
-        o.energy[SMD_E_POL_INTRA] = (double)__ldcg(&acc[ACC_E_POL_INTRA]) * ACC_INV;
+        long long accv[ACC_COUNT];
+        for (int q = 0; q < ACC_COUNT; q++) accv[q] = __ldcg(&acc[q]);
+        double en[SMD_E_COUNT];
+        acc_energies(accv, a.e_lrc, a.e_self, en);
         double ep = 0;
-        for (int q = 0; q < 10; q++) ep += o.energy[q];
+        for (int q = 0; q < SMD_E_COUNT; q++) {
+            o.energy[q] = en[q];
+            ep += en[q];
+        }
         o.e_potential = ep;
         const int sym[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
         for (int q = 0; q < 9; q++) {

@@ -214,13 +214,12 @@ def buff_long_range_correction(s: System, box: float) -> tuple:
 
 def refuse_unsupported(c) -> None:
     """Raises for configuration options the GPU path does not compute, so a
-    caller never gets different physics with a success status: the
-    surface-dipole corrections (``surfCorrect``: EwaldForce.cpp:816-937,
-    Multipole.cpp:1753-1920, Induction.cpp:2188-2380), the AMOEBA damping
-    branch of the induced real space (``dampAMOEBA``, Induction.cpp:1051-1079)
-    and the Wolf summation (WolfForce.cpp)."""
-    if c.surface_correct:
-        raise NotImplementedError("surface-dipole correction (surfCorrect) is not built on the GPU path")
+    caller never gets different physics with a success status: the AMOEBA
+    damping branch of the induced real space (``dampAMOEBA``,
+    Induction.cpp:1051-1079) and the Wolf summation (WolfForce.cpp)."""
+    if c.compute_ub and c.constraint:
+        # Integrator::initialise refuses the same combination (src/Integrator.cpp:178-187)
+        raise NotImplementedError("a flexible Urey-Bradley term with constraints")
     if c.compute_multipole and c.compute_induction and c.damp_amoeba:
         raise NotImplementedError("AMOEBA damping of the induced real space (dampAMOEBA) is not built on "
                                   "the GPU path")
@@ -278,6 +277,26 @@ class GpuEnsemble:
             self._chk(self.lib.smd_set_multipole(ctx, L.dptr(mp), L.dptr(pol), c.alpha, c.k_cutoff,
                                                  c.cutoff_ew, int(c.compute_induction), c.cutoff_ind,
                                                  c.a_damping))
+        # bonded terms of flexible molecules (Integrator::initialise,
+        # src/Integrator.cpp:163-190): bonds and angles without constraints,
+        # Urey-Bradley when configured
+        flexible = c.constraint == 0 and (len(s.bonds) or len(s.angles))
+        if flexible or c.compute_ub:
+            nb = len(s.bonds) if c.constraint == 0 else 0
+            na = len(s.angles) if c.constraint == 0 else 0
+            bonds = np.ascontiguousarray(np.asarray(s.bonds, np.int32).reshape(-1, 3)[:nb].reshape(-1)) \
+                if nb else np.zeros(3, np.int32)
+            angles = np.ascontiguousarray(np.asarray(s.angles, np.int32).reshape(-1, 4)[:na].reshape(-1)) \
+                if na else np.zeros(4, np.int32)
+            bp = np.ascontiguousarray([[r0, k] for (_, _, r0, k) in s.bond_params] or [[0.0, 0.0]], np.float64)
+            ap = np.ascontiguousarray([[deg * 2 * math.pi / 360.0, k] for (_, _, _, deg, k) in s.angle_params]
+                                      or [[0.0, 0.0]], np.float64)
+            self._chk(self.lib.smd_set_bonded(ctx, nb, L.iptr(bonds), max(1, len(s.bond_params)),
+                                              L.dptr(bp.reshape(-1)), na, L.iptr(angles),
+                                              max(1, len(s.angle_params)), L.dptr(ap.reshape(-1)),
+                                              int(c.bend_type), int(c.compute_ub), c.kl_ub, c.l0_ub))
+        if c.surface_correct:
+            self._chk(self.lib.smd_set_surface_correct(ctx, 1))
         self.set_precision(precision)
         if threads_per_site:
             self._chk(self.lib.smd_set_tuning(ctx, threads_per_site))

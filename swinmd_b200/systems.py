@@ -67,7 +67,11 @@ class Config:
     use_cell_list: bool = True
     constraint: int = 0              # 0 none, 1 Gaussian, 2 SHAKE
     tolerance: float = 1e-8
-    max_count: int = 1000            # SHAKE iteration cap / bending type
+    max_count: int = 1000            # SHAKE iteration cap (constraint 2)
+    bend_type: int = 1               # bond/angle form without constraints: 1 harmonic, 2 AMOEBA
+    compute_ub: bool = False         # harmonic Urey-Bradley H-H term
+    kl_ub: float = 0.0               # its force constant (kJ/mol/nm^2)
+    l0_ub: float = 0.0               # its ideal distance (nm)
     long_correct: bool = False
     switch_on: bool = True           # LJ energy shift at the cutoff
     switch_dist: float = 0.9
@@ -195,9 +199,9 @@ def write_config(cfg: Config, path: str, sysdata="sysData.in", coords="coordinat
     if c.constraint == 2:
         lines.append(f"2\t{g(c.tolerance)}\t{c.max_count}\t// SHAKE")
     else:
-        lines.append(f"{c.constraint}\t{g(c.tolerance)}\t{c.max_count}\t0.01\t// constraint")
+        lines.append(f"{c.constraint}\t{g(c.tolerance)}\t{c.bend_type}\t0.01\t// constraint, bending type")
     lines += [
-        "f\t0.0\t0.0\t// UB",
+        f"{_tf(c.compute_ub)}\t{g(c.kl_ub)}\t{g(c.l0_ub)}\t// UB",
         f"{_tf(c.long_correct)}\t{_tf(c.switch_on)}\t{g(c.switch_dist)}\t// lrc switch",
         f"{_tf(c.compute_coulomb)}\t{_tf(c.compute_ewald)}\t{_tf(c.surface_correct)}\t"
         f"{_tf(c.compute_wolf)}\t{g(c.alpha)}\t{g(c.k_cutoff)}\t// electrostatics",
@@ -272,6 +276,124 @@ def write_reference_case(s: System, directory: str) -> None:
     write_config(cfg, os.path.join(directory, "config.txt"))
     write_sysdata(s, os.path.join(directory, "sysData.in"))
     write_coordinates(s.pos, os.path.join(directory, "coordinate.in"))
+
+
+def _tf_read(tok: str) -> bool:
+    return tok.strip().lower().startswith("t")
+
+
+def read_config(path: str) -> Tuple[Config, str, str]:
+    """Reads the fields of ``config.txt`` this path uses, in the positional
+    layout ``SimConfiguration::read_config_file`` parses
+    (src/SimConfiguration.cpp:695-932): one field group per line, the rest of
+    a line ignored.  Returns the Config and the sysData / coordinate file
+    names."""
+    with open(path) as f:
+        rows = [ln.split("//")[0].split() for ln in f]
+    rows = [r for r in rows if r]
+    c = Config()
+    sysdata, coords = rows[0][0], rows[0][1]
+    c.seed = int(rows[3][1])
+    c.timestep, c.n_steps = float(rows[4][0]), int(rows[4][1])
+    c.long_steps = int(rows[5][1])
+    c.integrator = int(rows[7][0])
+    r = rows[8]
+    c.ensemble, c.temperature, c.pressure = int(r[0]), float(r[1]), float(r[2])
+    c.atom_thermo = int(r[3]) == 1
+    c.coupl_const, c.thermostat, c.baros_const = float(r[4]), r[5], float(r[6])
+    c.test_mode, c.rate = int(rows[9][0]), float(rows[9][1])
+    r = rows[10]
+    c.cutoff, c.cutoff_ew, c.k_cutoff, c.cut_buffer = float(r[0]), float(r[1]), float(r[2]), float(r[3])
+    c.density = float(rows[11][0])
+    c.use_cell_list = _tf_read(rows[13][0])
+    r = rows[14]
+    c.constraint, c.tolerance = int(r[0]), float(r[1])
+    if c.constraint == 2:
+        c.max_count = int(r[2])
+    else:
+        c.bend_type = int(r[2])
+    r = rows[15]
+    c.compute_ub, c.kl_ub, c.l0_ub = _tf_read(r[0]), float(r[1]), float(r[2])
+    r = rows[16]
+    c.long_correct, c.switch_on, c.switch_dist = _tf_read(r[0]), _tf_read(r[1]), float(r[2])
+    r = rows[17]
+    c.compute_coulomb, c.compute_ewald, c.surface_correct, c.compute_wolf = (_tf_read(x) for x in r[:4])
+    c.alpha, c.k_cutoff = float(r[4]), float(r[5])
+    r = rows[18]
+    (c.compute_multipole, c.compute_induction, c.compute_torques, c.damp_induction, c.induction_min,
+     c.damp_amoeba) = (_tf_read(x) for x in r[:6])
+    c.cutoff_ind, c.a_damping = float(r[6]), float(r[7])
+    r = rows[19]
+    c.compute_buff, c.n_buff, c.m_buff = _tf_read(r[0]), int(r[1]), int(r[2])
+    c.delta_buff, c.gamma_buff, c.h_factor = float(r[3]), float(r[4]), float(r[5])
+    r = rows[20]
+    c.compute_mie, c.n_mie, c.m_mie = _tf_read(r[0]), float(r[1]), float(r[2])
+    c.lustig = _tf_read(rows[-1][0])
+    return c, sysdata, coords
+
+
+_SYSDATA_SECTIONS = {"Size_of_system", "AtomParams", "BondParams", "AngleParams", "DihedralParams",
+                     "ImproperParams", "MolTypes", "Atoms", "Bonds", "Angles", "Dihedrals", "Impropers"}
+
+
+def read_sysdata(path: str):
+    """Reads ``sysData.in`` (``Parameters::read_sys_data``,
+    src/Parameters.cpp:76-380): atom types, bond and angle parameters,
+    molecule types and the topology sections."""
+    with open(path) as f:
+        lines = [ln.split("!")[0].strip() if not ln.lstrip().startswith("!") else ln.strip() for ln in f]
+    sec, data = None, {}
+    counts = []
+    for ln in lines:
+        if not ln:
+            continue
+        if ln.startswith("!"):
+            head = ln[1:].split()[0] if len(ln) > 1 else ""
+            if head in _SYSDATA_SECTIONS:
+                sec = head
+                data.setdefault(sec, [])
+            continue
+        if sec == "Size_of_system":
+            counts.append([int(x) for x in ln.split()[:2]])
+        elif sec is not None:
+            data[sec].append(ln.split())
+    types = []
+    for r in data.get("AtomParams", []):
+        # typeID, mass, charge, epsilon, sigma, dipole (3), quadrupole (6),
+        # polarisability, type name, atom name
+        v = [float(x) for x in r[1:15]]
+        types.append(AtomType(mass=v[0], charge=v[1], eps=v[2], sigma=v[3], dip=tuple(v[4:7]),
+                              quad=tuple(v[7:13]), polar=v[13], name=r[15] if len(r) > 15 else "X",
+                              long_name=r[16] if len(r) > 16 else "Atom"))
+    bond_params = [(int(r[1]), int(r[2]), float(r[3]), float(r[4])) for r in data.get("BondParams", [])]
+    angle_params = [(int(r[1]), int(r[2]), int(r[3]), float(r[4]), float(r[5])) for r in data.get("AngleParams", [])]
+    mol_types = [(r[2], int(r[1])) for r in data.get("MolTypes", [])]
+    atoms = np.array([[int(x) for x in r[:4]] for r in data.get("Atoms", [])], np.int64)
+    bonds = np.array([[int(x) for x in r[1:4]] for r in data.get("Bonds", [])], np.int32).reshape(-1, 3)
+    angles = np.array([[int(x) for x in r[1:5]] for r in data.get("Angles", [])], np.int32).reshape(-1, 4)
+    return types, bond_params, angle_params, mol_types, atoms, bonds, angles
+
+
+def read_reference_case(directory: str, name: str = "case") -> System:
+    """A System from a directory of the reference's own input files
+    (config.txt, its sysData file and coordinate file), so that an existing
+    SwinMD case runs on the GPU path as it is.  The cubic box follows from
+    the configured site density as in ``Ensemble::compute_bound_box``
+    (src/Ensemble.cpp:399-406)."""
+    cfg, sysdata, coords = read_config(os.path.join(directory, "config.txt"))
+    types, bp, ap, mt, atoms, bonds, angles = read_sysdata(os.path.join(directory, sysdata))
+    with open(os.path.join(directory, coords)) as f:
+        n = int(f.readline().split()[0])
+        pos = np.array([[float(x) for x in f.readline().split()[:3]] for _ in range(n)])
+    box = (n / cfg.density) ** (1.0 / 3.0)
+    mol_id = atoms[:, 2].astype(np.int32)
+    nmol = int(mol_id.max()) + 1
+    mol_type = np.zeros(nmol, np.int32)
+    mol_type[mol_id] = atoms[:, 3]
+    return System(name=name, pos=pos, box=(box, box, box), atom_types=types,
+                  atom_type=atoms[:, 1].astype(np.int32), mol_id=mol_id, mol_type_names=mt,
+                  mol_type=mol_type, config=cfg, bonds=bonds, angles=angles, bond_params=bp,
+                  angle_params=ap)
 
 
 def reference_box(s: System) -> float:

@@ -87,8 +87,20 @@ def polwater4096():
     return s, [("forces",)]
 
 
+def ref_test_nvt():
+    # the reference's own shipped case (test/: 500 flexible polarisable
+    # waters, AMOEBA bonds and angles, Urey-Bradley, buffered 14-7,
+    # multipoles, induction, surface corrections), read from its input files
+    # and run at constant volume (ensembleStatus 0) instead of NPT
+    src = os.path.join(os.environ.get("SWINMD_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference"), "test")
+    s = systems.read_reference_case(src, name="ref_test_nvt")
+    s.config.ensemble = 0
+    s.config.n_steps = 10
+    return s, [("forces",), ("run", 10)]
+
+
 CASES = {"lj500": lj500, "nacl1000_mie": nacl1000_mie, "spce512": spce512,
-         "polwater216": polwater216}
+         "polwater216": polwater216, "ref_test_nvt": ref_test_nvt}
 LARGE = {"lj4000": lj4000, "lj4000_jitter": lj4000_jitter, "nacl8000_mie": nacl8000_mie, "spce2160": spce2160,
          "polwater4096": polwater4096}
 
@@ -129,6 +141,15 @@ def pack(name, s, results, large=False):
                 if large and v.size > 64 and k not in ("final_pos", "final_vel"):
                     continue
                 out["r_" + k] = v
+    if name == "ref_test_nvt":
+        # the case itself as this project's writers emit it, so that the GPU
+        # test can rebuild the System without the reference's files
+        import tempfile
+        with tempfile.TemporaryDirectory() as d:
+            systems.write_reference_case(s, d)
+            for fn, key in (("config.txt", "case_config"), ("sysData.in", "case_sysdata"),
+                            ("coordinate.in", "case_coords")):
+                out[key] = np.array(open(os.path.join(d, fn)).read())
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
 
 

@@ -9,7 +9,7 @@ def _pw():
     return systems.polarizable_water(nmol=8, kmax=3, seed=1)
 
 
-@pytest.mark.parametrize("field", ["surface_correct", "damp_amoeba", "compute_wolf"])
+@pytest.mark.parametrize("field", ["damp_amoeba", "compute_wolf"])
 def test_unsupported_options_refused(field):
     s = _pw()
     setattr(s.config, field, True)
@@ -19,3 +19,10 @@ def test_unsupported_options_refused(field):
 
 def test_default_options_accepted():
     engine.refuse_unsupported(_pw().config)
+
+
+def test_ub_with_constraints_refused():
+    s = _pw()
+    s.config.compute_ub = True
+    with pytest.raises(NotImplementedError):
+        engine.refuse_unsupported(s.config)

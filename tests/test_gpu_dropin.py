@@ -84,3 +84,25 @@ def test_kept_list_gives_the_rebuilt_list_forces():
     assert np.array_equal(a, b)
     ens.close()
     fresh.close()
+
+
+def test_force_call_between_steps_leaves_the_run_unchanged():
+    # smd_compute_forces between smd_run calls (a sampling point) changes
+    # nothing of the trajectory or of the next steps' observables
+    def run(probe):
+        s = systems.spce_water(nmol=512, box=2.4953, cutoff=0.9, kmax=6, seed=11, n_steps=20)
+        e = engine.GpuEnsemble(s)
+        lf = engine.LFIntegrator(e, series_capacity=16)
+        lf.start()
+        lf.run(5)
+        if probe:
+            e.compute_forces(L.TERM_EWALD_LONG)
+            e.compute_forces()
+        lf.run(5)
+        out = (lf.series().copy(), e.state()["pos"].copy(), np.array(lf.observables().atom_pressure))
+        e.close()
+        return out
+    a, b = run(False), run(True)
+    assert np.array_equal(a[0], b[0])
+    assert np.array_equal(a[1], b[1])
+    assert np.array_equal(a[2], b[2])
