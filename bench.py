@@ -459,7 +459,7 @@ def main():
     # reciprocal passes with exact integer phases, product-form 14-7), the
     # solve started from the molecule-block solution M^-1 E0
     plain = arm("fp64", L.GUESS_DIRECT)
-    prof_plain = np.zeros(10)
+    prof_plain = np.zeros(12)
     L.check(ens.ctx, ens.lib.smd_profile_stages(ens.ctx, 5, L.dptr(prof_plain)))
     # the same FP64 arm with the reference's own forms (pow() 14-7, one FP64
     # sine and cosine per (site, k)): what a direct GPU port of the reference
@@ -471,7 +471,7 @@ def main():
     # fast: mixed path + learned guess (the headline)
     fast = arm("mixed", L.GUESS_LEARNED if polar else L.GUESS_DIRECT)
     clocks_all = clk_all.stop()
-    prof = np.zeros(10)
+    prof = np.zeros(12)
     L.check(ens.ctx, ens.lib.smd_profile_stages(ens.ctx, 5, L.dptr(prof)))
     value = fast["value"]
 
@@ -576,7 +576,7 @@ def main():
     kc = ctypes.c_int()
     L.check(ens.ctx, ens.lib.smd_step_kernel_count(ens.ctx, ctypes.byref(kc)))
     names = ["pair", "recip", "integrate", "list_rebuild", "frames", "mp_real", "mp_recip",
-             "dipole_solve", "ind_real", "polar_recip"]
+             "dipole_solve", "ind_real", "polar_recip", "field_rows", "pcg"]
     stage_ms = {k: float(v) for k, v in zip(names, prof)}
     stage_plain = {k: float(v) for k, v in zip(names, prof_plain)}
     peaks = dict(FALLBACK)
@@ -584,22 +584,70 @@ def main():
     if os.path.exists(PEAKS):
         peaks.update(json.load(open(PEAKS)))
         peak_src = "measured"
-    # the reciprocal sums and forces of the permanent and induced multipoles
-    # (FP32 SIMT work, a few MB of traffic), counted as the FP32 operations
-    # of the column formulation (an FMA is 2): 33 per (site, k) in the sums
-    # pass (27 per k plus the run's shared 22 over 3.7 k) and 26 in the force
-    # pass (24 per k plus the column fold, 42 over 24 k); the peak is the
-    # nominal FP32 rate of 148 SMs x 128 lanes at the measured maximum SM clock
     # a forced rebuild is timed, but the list is rebuilt only when a site has
     # moved half the skin: weigh it by the rebuilds seen in the timed steps
     amortised = dict(stage_ms, list_rebuild=stage_ms["list_rebuild"] * fast["list_rebuilds_per_step"])
+    amortised.pop("dipole_solve")   # field_rows + pcg
     dom = max(amortised, key=amortised.get)
-    nk = ens.ewald_nk() if polar else 0
-    flops = float(nk) * n * (33 + 26)
     sm_mhz = peaks.get("sm_max_mhz", 1965.0)
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
-    rstage = "polar_recip" if polar else "pair"
-    achieved = flops / (stage_ms[rstage] * 1e-3) / 1e12 if stage_ms[rstage] > 0 and flops > 0 else None
+    hbm_peak = peaks["hbm_gbs"]
+    rooflines = {}
+    nk = ens.ewald_nk() if polar else 0
+    if polar:
+        # (1) reciprocal sums and forces of the permanent + induced multipoles:
+        # FP32 operations of the column formulation (an FMA is 2): 33 per
+        # (site, k) in the sums pass (27 per k plus the run's shared 22 over
+        # 3.7 k) and 26 in the force pass (24 per k plus the column fold, 42
+        # over 24 k); bound by the FP32 SIMT rate
+        flops = float(nk) * n * (33 + 26)
+        t = stage_ms["polar_recip"] * 1e-3
+        rooflines["polar_recip"] = {
+            "bound": "fp32", "kernel": "k_rsk_seg<float,2,4> + k_rforce_grp<float,1>",
+            "achieved": flops / t / 1e12, "peak": fp32_peak, "unit": "TFLOP/s",
+            "frac": flops / t / 1e12 / fp32_peak, "alg_flops_per_launch": flops, "k_vectors": nk,
+            # DRAM bytes of one launch of each pass, from one ncu capture
+            # (dram__bytes_read.sum + dram__bytes_write.sum: 6.45 + 0 MB and 3.17 + 0 MB)
+            "traffic": 6.45e6 + 3.17e6, "ms": stage_ms["polar_recip"]}
+        # (2) fused multipole + induced real space over the solve's tensor rows:
+        # about 550 operations per directed pair (FP32 multipole algebra, FP64
+        # radial factors and force assembly), rows = both directions of every
+        # pair inside the cutoff plus the molecule's own sites
+        entries = 2.0 * fast["pairs_in_cutoff"] + 2.0 * n
+        flops = 550.0 * entries
+        t = stage_ms["ind_real"] * 1e-3
+        rooflines["fused_real"] = {
+            "bound": "fp32+fp64 issue", "kernel": "k_polar_real_f<1> (+ k_polar_mol)",
+            "achieved": flops / t / 1e12, "peak": fp32_peak, "unit": "TFLOP/s",
+            "frac": flops / t / 1e12 / fp32_peak, "alg_flops_per_launch": flops, "row_entries": entries,
+            "traffic": 17.7e6, "ms": stage_ms["ind_real"],
+            "note": "half of the work is FP64 (nominal FP64 rate 37.2 TFLOP/s); ncu: FP64 pipe 33%, FMA 28%"}
+        # (3) the PCG kernel: every product streams the FP32 tensor rows
+        # (4 B partner + 16 B coefficients per entry) and gathers the packed
+        # vector (16 B per entry); iterations + 1 products per solve
+        products = fast["solver_iterations"] + 1
+        nbytes = products * entries * (4 + 16 + 16)
+        t = stage_ms["pcg"] * 1e-3
+        rooflines["pcg"] = {
+            "bound": "hbm", "kernel": "k_ind_cg<1,1>", "achieved": nbytes / t / 1e9, "peak": hbm_peak,
+            "unit": "GB/s", "frac": nbytes / t / 1e9 / hbm_peak, "alg_bytes_per_launch": nbytes,
+            "products": products, "traffic": 150.7e6, "ms": stage_ms["pcg"],
+            "note": "rows and gathers are served mostly from L2 (126 MB); DRAM bytes from the ncu capture"}
+        # the dominant kernel: the largest device time of one kernel (the
+        # reciprocal figure covers two kernels)
+        rooflines["polar_recip"]["kernels"] = 2
+        main_kernel = max(rooflines, key=lambda k: rooflines[k]["ms"] / rooflines[k].get("kernels", 1))
+        roofline = dict(rooflines[main_kernel], which=main_kernel)
+    else:
+        pairs = fast["pairs_in_cutoff"]
+        flops = pairs * 2 * 23
+        t = stage_ms["pair"] * 1e-3
+        roofline = {"bound": "fp32", "kernel": "k_pair (LJ)", "achieved": flops / t / 1e12, "peak": fp32_peak,
+                    "unit": "TFLOP/s", "frac": flops / t / 1e12 / fp32_peak, "traffic": None, "which": "pair"}
+    roofline.update(peak_source=f"HBM: hbm_gbs of MEASURED_PEAKS.json ({peak_src}); FP32: nominal SIMT rate "
+                                "148 SMs x 128 lanes x 2 at sm_max_mhz (the file has no FP32 figure)",
+                    dominant_stage=dom,
+                    traffic_source="ncu --set full captures of the polwater4096 step (profiles/)")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and polar:
@@ -651,23 +699,8 @@ def main():
                "stage_notes": "stage_ms_* time each stage alone (list_rebuild: one forced rebuild); in the fast "
                               "arm the multipole and induced real space are one fused pass, reported under "
                               "ind_real (mp_real 0)",
-               "roofline": {"bound": "fp32", "kernel": "k_rsk_seg<float,2,4> + k_rforce_grp<float,1> (reciprocal "
-                                                      "sums and forces of the permanent + induced multipoles)",
-                            "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                            "frac": achieved / fp32_peak if achieved else None,
-                            "alg_flops_per_step": flops, "k_vectors": nk,
-                            # DRAM bytes of one launch of each pass on this workload, from one ncu
-                            # capture (dram__bytes_read.sum + dram__bytes_write.sum: 6.45 + 0 MB
-                            # and 3.17 + 0 MB); the passes read their tables from L2 and shared
-                            # memory, so they are not bound by HBM
-                            "traffic": (6.45e6 + 3.17e6) if polar else None,
-                            "traffic_unit": "bytes per step (both passes)",
-                            "traffic_source": "ncu --set full capture of the polwater4096 step "
-                                              "(profiles/polwater4096_top_kernels.md)",
-                            "peak_source": "nominal FP32 SIMT rate at sm_max_mhz of MEASURED_PEAKS.json "
-                                           f"({peak_src}); the file's HBM copy and bf16 GEMM rates do not "
-                                           "bound these kernels",
-                            "dominant_stage": dom},
+               "roofline": roofline,
+               "rooflines": rooflines,
                "clocks": clocks_all, "cpu_baseline": cpu,
                "setup_s": time.perf_counter() - t_setup}
         print(json.dumps(out))

@@ -358,8 +358,10 @@ int smd_get_series(smd_ctx *ctx, double *out, int cap, int *count);
  * real+self+intra (in the mixed precision mode the multipole and induced
  * real space are one fused pass after the solve: out[8] then holds both and
  * out[5] is 0), out[9] reciprocal structure factors and forces of the
- * permanent and induced multipoles together (out has room for 10).  Leaves
- * forces and state unchanged except for the rebuilt list. */
+ * permanent and induced multipoles together, out[10] the permanent field
+ * with the solve's tensor rows, preconditioner blocks and start dipoles,
+ * out[11] the PCG kernel alone (out has room for 12).  Leaves forces and
+ * state unchanged except for the rebuilt list. */
 int smd_profile_stages(smd_ctx *ctx, int reps, double *out);
 /* smd_run with the device time of the nsteps graph launches (CUDA events on
  * the context's stream, synchronized on both sides) returned in *device_ms. */

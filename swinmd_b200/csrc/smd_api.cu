@@ -1213,7 +1213,7 @@ int smd_profile_stages(smd_ctx *x, int reps, double *out) {
     CK(cudaMemcpyAsync(c.obs, &o_save, sizeof(o_save), cudaMemcpyHostToDevice, c.stream));
     CK(cudaMemcpyAsync(c.scal, sc_save, sizeof(sc_save), cudaMemcpyHostToDevice, c.stream));
     out[3] = timed([&] { launch_nlist(c, true); });
-    for (int q = 4; q < 10; q++) out[q] = 0.0;
+    for (int q = 4; q < 12; q++) out[q] = 0.0;
     if (c.mp_on) {
         out[4] = timed([&] { launch_frames(c); });
         const bool fused = polar_short_fused(c);
@@ -1240,6 +1240,23 @@ int smd_profile_stages(smd_ctx *x, int reps, double *out) {
             // with the fused pass the multipole real space is part of this stage
             out[8] = timed([&] { if (fused) launch_polar_short(c); else launch_ind_short(c); });
             out[9] = timed([&] { launch_polar_long(c); });
+            // the solve's two parts: the permanent field with the tensor rows,
+            // the preconditioner blocks and the start dipoles; then the PCG
+            // kernel alone, each time from the same start dipoles (a device
+            // copy of 3N doubles, about a microsecond, inside its time)
+            out[10] = timed([&] { launch_ind_field(c); });
+            {
+                const size_t pb = 3 * (size_t)c.n * sizeof(double);
+                double *p0 = nullptr;
+                CK(cudaMalloc(&p0, pb));
+                CK(cudaMemcpyAsync(p0, c.pind, pb, cudaMemcpyDeviceToDevice, c.stream));
+                out[11] = timed([&] {
+                    cudaMemcpyAsync(c.pind, p0, pb, cudaMemcpyDeviceToDevice, c.stream);
+                    launch_ind_cg(c);
+                });
+                CK(cudaStreamSynchronize(c.stream));
+                cudaFree(p0);
+            }
         }
     }
     // forces for the current positions again, accumulators clear
