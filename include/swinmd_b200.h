@@ -141,6 +141,23 @@ typedef struct {
     double shear_offset;     /* Lees-Edwards offset of the images one box up (nm) */
 } smd_observables;
 
+/* Means over the steps since the last smd_averages_reset (or the context's
+ * creation) of the observables Ensemble::accumulate averages
+ * (src/Ensemble.cpp:814-894): energies and their squares, kinetic energies,
+ * volume, and per pressure tensor (atomic, molecular) the stress figures
+ * {pressure (trace / 3), shear (XY + YX) / 2, antisymmetric (YX - XY) / 2,
+ * first normal difference XX - YY, second YY - ZZ} and the full tensor.
+ * Every step of smd_run adds its sample on the device; smd_integrator_start
+ * starts the sums afresh. */
+typedef struct {
+    int64_t samples;
+    double e_potential, e_potential_sq, e_total, e_total_sq;
+    double ke_atom, ke_atom_sq, ke_mol, ke_mol_sq, inv_ke_mol;
+    double volume, volume_sq;
+    double atom_stress[5], mol_stress[5];
+    double atom_pressure[9], mol_pressure[9];
+} smd_averages;
+
 /* ---- lifetime -------------------------------------------------------- */
 /* Creates a context on CUDA device `device` (the Simulation/Ensemble pair of
  * Simulation::setup_simulation, src/Simulation.cpp:171-263). */
@@ -296,6 +313,20 @@ int smd_upload_positions(smd_ctx *ctx, const double *pos);
 /* vel: Atom::velocity; vtminus may be NULL (then set by smd_integrator_start) */
 int smd_upload_velocities(smd_ctx *ctx, const double *vel, const double *vtminus);
 int smd_download_state(smd_ctx *ctx, double *pos, double *vel, double *vtminus);
+/* Atom::realPos, the positions without the periodic wraps (written to
+ * state.out by Integrator::write_state, src/Integrator.cpp:275-302): the
+ * positions less the box shifts each molecule has had since the last
+ * smd_upload_positions, plus the offsets an smd_upload_real_positions after
+ * that upload set (a restart's realPos). */
+int smd_download_real_positions(smd_ctx *ctx, double *real);
+int smd_upload_real_positions(smd_ctx *ctx, const double *real);
+/* The integrator's scalars (32 doubles: the Nose-Hoover zeta and its
+ * half-step value, the pending centre-of-mass correction, the chain
+ * velocities, the Lees-Edwards offset), for a restart that continues the
+ * trajectory where a checkpoint left it (the reference restarts with zeta
+ * = 0: Ensemble::set_configuration, src/Ensemble.cpp:303-317). */
+int smd_get_integrator_state(smd_ctx *ctx, double *state);
+int smd_set_integrator_state(smd_ctx *ctx, const double *state);
 
 /* ---- forces (Force::compute / compute_long, src/Force.h:59) ----------
  * Evaluates the selected terms at the current positions and returns:
@@ -340,6 +371,13 @@ int smd_set_constraints(smd_ctx *ctx, const double *len2);
 /* LFIntegrator::start (LFIntegrator.cpp:991-1174): F(0) and
  * vtMinus = v - dt/2 F/m. */
 int smd_integrator_start(smd_ctx *ctx);
+/* smd_integrator_start without LFIntegrator::start's half-step velocities:
+ * the velocities and vtMinus uploaded by smd_upload_velocities are kept, as
+ * the reference's run that does not start new takes them from state.in and
+ * vtMinus.in (LFIntegrator.cpp:187-192).  The chain integrator's scalars are
+ * reset as by smd_integrator_start; smd_set_integrator_state afterwards
+ * restores the saved ones. */
+int smd_integrator_resume(smd_ctx *ctx);
 /* LFIntegrator::run(nsteps) (LFIntegrator.cpp:252-942) without file output. */
 int smd_run(smd_ctx *ctx, int nsteps);
 int smd_get_observables(smd_ctx *ctx, smd_observables *out);
@@ -347,6 +385,21 @@ int smd_get_observables(smd_ctx *ctx, smd_observables *out);
  * atom-pressure trace/3) for the last min(nsteps, cap) steps: out[5*cap]. */
 int smd_set_series_capacity(smd_ctx *ctx, int cap);
 int smd_get_series(smd_ctx *ctx, double *out, int cap, int *count);
+
+/* ---- observables on the device ----------------------------------------- */
+int smd_averages_reset(smd_ctx *ctx);
+int smd_get_averages(smd_ctx *ctx, smd_averages *out);
+/* Radial distribution function (RDF, src/observables/RDF.cpp): histogram of
+ * every non-excluded pair closer than the smallest half box edge, per type
+ * pair, nbins bins.  Setup clears it; each sample adds the current
+ * configuration (RDF::sampling, :109-144). */
+int smd_rdf_setup(smd_ctx *ctx, int nbins);
+int smd_rdf_sample(smd_ctx *ctx);
+/* hist[ntypes][ntypes][nbins] raw counts (both type orders of every pair;
+ * may be NULL); g[npairs][nbins] the normalised RDF of each type pair
+ * t1 <= t2 in the order of RDF::write_result (:146-180; may be NULL);
+ * r_mid[nbins] the bin centres (may be NULL); *samples the samples taken. */
+int smd_rdf_get(smd_ctx *ctx, uint64_t *hist, double *g, double *r_mid, int64_t *samples);
 
 /* ---- measurement ------------------------------------------------------- */
 /* Average device time (ms, CUDA events on the context's stream) of each

@@ -11,6 +11,7 @@
 //     ref_dump run <nsteps> <out>  LFIntegrator::start() then nsteps x run(1)
 //     ref_dump mie <out>           MieForce::compute() on its own
 //     ref_dump buck <out>          BuckinghamForce::compute() on its own
+//     ref_dump rdf <out>           one RDF::sampling() of the configuration
 //
 // Setup follows Simulation::setup_simulation (src/Simulation.cpp:171-263)
 // without the output files.
@@ -52,6 +53,7 @@
 #include "forces/BondForce.h"
 #include "forces/AngleForce.h"
 #include "forces/UreyBradleyForce.h"
+#include "observables/RDF.h"
 #undef class
 #undef private
 #undef protected
@@ -338,6 +340,30 @@ static int mode_run(int nsteps, const char *out) {
     return 0;
 }
 
+// one RDF::sampling of the current configuration: the raw histogram
+// rdfTable[t1][t2][bin] (both orders of every pair), the bin count and the
+// per-type counts (src/observables/RDF.cpp:109-144)
+static int mode_rdf(const char *out) {
+    Setup s = build();
+    g_out = fopen(out, "w");
+    header(s);
+    Ensemble *e = s.ens;
+    RDF rdf(e, 1 << 30);
+    rdf.sampling();
+    const int nt = e->nAtomTypes;
+    std::vector<double> h;
+    for (int a = 0; a < nt; a++)
+        for (int b = 0; b < nt; b++)
+            for (int k = 0; k < rdf.nBins; k++) h.push_back(rdf.rdfTable[a][b][k]);
+    rec("rdf_hist", h);
+    rec1("rdf_nbins", rdf.nBins);
+    rec1("rdf_maxr", rdf.maxR);
+    std::vector<double> npt(rdf.numPerType, rdf.numPerType + nt);
+    rec("rdf_numpertype", npt);
+    fclose(g_out);
+    return 0;
+}
+
 int main(int argc, char **argv) {
     if (argc < 3) {
         fprintf(stderr, "usage: ref_dump forces|mie|buck <out> | run <nsteps> <out>\n");
@@ -346,6 +372,7 @@ int main(int argc, char **argv) {
     if (!strcmp(argv[1], "forces")) return mode_forces(argv[2]);
     if (!strcmp(argv[1], "mie") || !strcmp(argv[1], "buck")) return mode_single(argv[1], argv[2]);
     if (!strcmp(argv[1], "run") && argc >= 4) return mode_run(atoi(argv[2]), argv[3]);
+    if (!strcmp(argv[1], "rdf")) return mode_rdf(argv[2]);
     fprintf(stderr, "unknown mode\n");
     return 2;
 }

@@ -58,6 +58,15 @@ class Observables(ctypes.Structure):
                 ("shear_offset", ctypes.c_double)]
 
 
+class Averages(ctypes.Structure):
+    _fields_ = [("samples", ctypes.c_int64)] + \
+               [(k, ctypes.c_double) for k in ("e_potential", "e_potential_sq", "e_total", "e_total_sq",
+                                               "ke_atom", "ke_atom_sq", "ke_mol", "ke_mol_sq", "inv_ke_mol",
+                                               "volume", "volume_sq")] + \
+               [("atom_stress", ctypes.c_double * 5), ("mol_stress", ctypes.c_double * 5),
+                ("atom_pressure", ctypes.c_double * 9), ("mol_pressure", ctypes.c_double * 9)]
+
+
 _P = ctypes.c_void_p
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int32)
@@ -87,12 +96,17 @@ SIGNATURES = {
     "smd_upload_positions": (ctypes.c_int, [_P, _D]),
     "smd_upload_velocities": (ctypes.c_int, [_P, _D, _D]),
     "smd_download_state": (ctypes.c_int, [_P, _D, _D, _D]),
+    "smd_download_real_positions": (ctypes.c_int, [_P, _D]),
+    "smd_upload_real_positions": (ctypes.c_int, [_P, _D]),
+    "smd_get_integrator_state": (ctypes.c_int, [_P, _D]),
+    "smd_set_integrator_state": (ctypes.c_int, [_P, _D]),
     "smd_compute_forces": (ctypes.c_int, [_P, ctypes.c_uint32, _D, _D, _D]),
     "smd_get_pairs": (ctypes.c_int, [_P, _I, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "smd_ewald_nk": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
     "smd_set_integrator": (ctypes.c_int, [_P, ctypes.POINTER(IntegratorParams)]),
     "smd_set_constraints": (ctypes.c_int, [_P, _D]),
     "smd_integrator_start": (ctypes.c_int, [_P]),
+    "smd_integrator_resume": (ctypes.c_int, [_P]),
     "smd_run": (ctypes.c_int, [_P, ctypes.c_int]),
     "smd_get_observables": (ctypes.c_int, [_P, ctypes.POINTER(Observables)]),
     "smd_set_series_capacity": (ctypes.c_int, [_P, ctypes.c_int]),
@@ -106,6 +120,11 @@ SIGNATURES = {
     "smd_set_bonded": (ctypes.c_int, [_P, ctypes.c_int, _I, ctypes.c_int, _D, ctypes.c_int, _I, ctypes.c_int, _D,
                                       ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double]),
     "smd_set_surface_correct": (ctypes.c_int, [_P, ctypes.c_int]),
+    "smd_rdf_setup": (ctypes.c_int, [_P, ctypes.c_int]),
+    "smd_averages_reset": (ctypes.c_int, [_P]),
+    "smd_get_averages": (ctypes.c_int, [_P, ctypes.POINTER(Averages)]),
+    "smd_rdf_sample": (ctypes.c_int, [_P]),
+    "smd_rdf_get": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), _D, _D, ctypes.POINTER(ctypes.c_int64)]),
     "smd_set_multipole": (ctypes.c_int, [_P, _D, _D, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_double]),

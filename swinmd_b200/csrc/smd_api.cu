@@ -301,7 +301,8 @@ int smd_create(int device, smd_ctx **out) {
     }
     if (dalloc(&c.acc, ACC_COUNT) != cudaSuccess || dalloc(&c.scal, SC_NSCAL) != cudaSuccess ||
         dalloc(&c.ticket, 1) != cudaSuccess || dalloc(&c.status, 1) != cudaSuccess ||
-        dalloc(&c.flags, 4) != cudaSuccess || dalloc(&c.obs, 1) != cudaSuccess) {
+        dalloc(&c.flags, 4) != cudaSuccess || dalloc(&c.obs, 1) != cudaSuccess ||
+        dalloc(&c.avg, AVG_COUNT) != cudaSuccess) {
         delete x;
         return SMD_ERR_CUDA;
     }
@@ -311,6 +312,7 @@ int smd_create(int device, smd_ctx **out) {
     cudaMemset(c.status, 0, sizeof(unsigned));
     cudaMemset(c.flags, 0, 4 * sizeof(int));
     cudaMemset(c.obs, 0, sizeof(smd_observables));
+    cudaMemset(c.avg, 0, AVG_COUNT * sizeof(double));
     if (device < NOALLOC_MAX_DEVICES) {
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
         g_live_ctx[device]++;
@@ -333,7 +335,7 @@ void smd_destroy(smd_ctx *x) {
                     c.pind, c.cgw, c.cgs, c.cg_bar, c.vpos4, c.vfixq, c.fv, c.ind_rj, c.ind_rc, c.ind_cnt,
                     c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab, c.srec, c.phist, c.cg_blk,
                     c.upload4, c.fout, c.rc.kzr_d, c.rc.kcxy_d, c.rc.stab_d, c.rc.srec_d, c.bonds, c.angles,
-                    c.bond_par, c.angle_par, c.surf_part, c.surf_tot};
+                    c.bond_par, c.angle_par, c.surf_part, c.surf_tot, c.rdf_hist, c.avg, c.wrap};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -403,6 +405,9 @@ int smd_set_topology(smd_ctx *x, int n, int ntypes, const int32_t *atom_type,
     CK(dalloc(&c.pl.cell_atoms, n));
     int nb = (nmol + 31) / 32;   // the integrate kernels' smallest blocks
     CK(dalloc(&c.partials, (size_t)nb * 40));  // per block: NPART (35) partial sums
+    CK(dalloc(&c.wrap, 3 * (size_t)nmol));
+    CK(cudaMemset(c.wrap, 0, 3 * (size_t)nmol * sizeof(double)));
+    c.h_real_off.clear();
     CK(cudaMemcpy(c.type, atom_type, n * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.mol, mol_id, n * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.mass, mass, n * sizeof(double), cudaMemcpyHostToDevice));
@@ -448,6 +453,10 @@ int smd_set_exclusions(smd_ctx *x, const int32_t *offsets, const int32_t *partne
         if (partners[k] < 0 || partners[k] >= n) return fail(x, SMD_ERR_ARG, "smd_set_exclusions: partner out of range");
     c.h_excl_off.assign(offsets, offsets + n + 1);
     c.h_excl.assign(partners, partners + tot);
+    c.excl_intermol = 0;
+    for (int i = 0; i < n; i++)
+        for (int k = offsets[i]; k < offsets[i + 1]; k++)
+            if (c.h_mol[partners[k]] != c.h_mol[i]) c.excl_intermol = 1;
     CK(dalloc(&c.excl, std::max(tot, 1)));
     CK(cudaMemcpy(c.excl_off, offsets, (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
     if (tot) CK(cudaMemcpy(c.excl, partners, tot * sizeof(int), cudaMemcpyHostToDevice));
@@ -628,6 +637,91 @@ int smd_set_bonded(smd_ctx *x, int nbonds, const int32_t *bonds, int nbond_types
     c.ub_l0 = l0_ub;
     c.graph_dirty = 1;
     touch(c);
+    return SMD_OK;
+}
+
+int smd_rdf_setup(smd_ctx *x, int nbins) {
+    if (!x || x->c.n == 0 || x->c.box.L[0] <= 0 || nbins <= 0 ||
+        (size_t)x->c.ntypes * x->c.ntypes * nbins * sizeof(unsigned int) > 200 * 1024)
+        return fail(x, SMD_ERR_ARG, "smd_rdf_setup: nbins must be > 0 with ntypes^2 * nbins * 4 bytes <= 200 KB");
+    Ctx &c = x->c;
+    CK(cudaSetDevice(c.device));
+    const size_t nh = (size_t)c.ntypes * c.ntypes * nbins;
+    CK(dalloc(&c.rdf_hist, nh));
+    CK(cudaMemsetAsync(c.rdf_hist, 0, nh * sizeof(unsigned long long), c.stream));
+    c.rdf_nbins = nbins;
+    c.rdf_samples = 0;
+    // RDF::init (src/observables/RDF.cpp:47-55): the smallest half box edge
+    c.rdf_maxr = std::min(c.box.half[0], std::min(c.box.half[1], c.box.half[2]));
+    CK(cudaStreamSynchronize(c.stream));
+    return SMD_OK;
+}
+
+int smd_rdf_sample(smd_ctx *x) {
+    if (!x || !x->c.rdf_hist) return fail(x, SMD_ERR_ARG, "smd_rdf_sample: call smd_rdf_setup first");
+    Ctx &c = x->c;
+    CK(cudaSetDevice(c.device));
+    const int r = rdf_sample(c);
+    if (r) return fail(x, r, "smd_rdf_sample: kernel set-up failed");
+    return sync_status(x);
+}
+
+int smd_rdf_get(smd_ctx *x, uint64_t *hist, double *g, double *r_mid, int64_t *samples) {
+    if (!x || !x->c.rdf_hist) return fail(x, SMD_ERR_ARG, "smd_rdf_get: call smd_rdf_setup first");
+    Ctx &c = x->c;
+    const int nt = c.ntypes, nb = c.rdf_nbins;
+    std::vector<unsigned long long> h((size_t)nt * nt * nb);
+    CK(cudaMemcpyAsync(h.data(), c.rdf_hist, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    if (hist)
+        for (size_t k = 0; k < h.size(); k++) hist[k] = h[k];
+    if (samples) *samples = c.rdf_samples;
+    // RDF::write_result (src/observables/RDF.cpp:146-180)
+    const double dr = c.rdf_maxr / nb, vol = c.box.L[0] * c.box.L[1] * c.box.L[2];
+    const double pi4dr = 4.0 * 3.14159265358979323846 * dr / vol;
+    std::vector<double> per(nt, 0.0);
+    for (int i = 0; i < c.n; i++) per[c.h_type[i]] += 1.0;
+    int col = 0;
+    for (int t1 = 0; t1 < nt; t1++)
+        for (int t2 = t1; t2 < nt; t2++, col++)
+            for (int k = 0; k < nb; k++) {
+                const double r = k * dr + 0.5 * dr;
+                if (r_mid && col == 0) r_mid[k] = r;
+                if (!g) continue;
+                double v = ((double)h[((size_t)t1 * nt + t2) * nb + k] + (double)h[((size_t)t2 * nt + t1) * nb + k]) / pi4dr;
+                g[(size_t)col * nb + k] =
+                    c.rdf_samples ? 0.5 * v / (r * r * per[t1] * per[t2] * (double)c.rdf_samples) : 0.0;
+            }
+    return SMD_OK;
+}
+
+int smd_averages_reset(smd_ctx *x) {
+    if (!x) return SMD_ERR_ARG;
+    CK(cudaMemsetAsync(x->c.avg, 0, AVG_COUNT * sizeof(double), x->c.stream));
+    CK(cudaStreamSynchronize(x->c.stream));
+    return SMD_OK;
+}
+
+int smd_get_averages(smd_ctx *x, smd_averages *out) {
+    if (!x || !out) return SMD_ERR_ARG;
+    double s[AVG_COUNT];
+    CK(cudaMemcpyAsync(s, x->c.avg, sizeof(s), cudaMemcpyDeviceToHost, x->c.stream));
+    CK(cudaStreamSynchronize(x->c.stream));
+    const double n = s[0] > 0 ? s[0] : 1.0;
+    out->samples = (int64_t)s[0];
+    double *dst[11] = {&out->e_potential, &out->e_potential_sq, &out->e_total, &out->e_total_sq, &out->ke_atom,
+                       &out->ke_atom_sq, &out->ke_mol, &out->ke_mol_sq, &out->inv_ke_mol, &out->volume,
+                       &out->volume_sq};
+    for (int q = 0; q < 11; q++) *dst[q] = s[1 + q] / n;
+    for (int q = 0; q < 5; q++) {
+        out->atom_stress[q] = s[12 + q] / n;
+        out->mol_stress[q] = s[17 + q] / n;
+    }
+    for (int q = 0; q < 9; q++) {
+        out->atom_pressure[q] = s[22 + q] / n;
+        out->mol_pressure[q] = s[31 + q] / n;
+    }
     return SMD_OK;
 }
 
@@ -955,9 +1049,62 @@ int smd_upload_positions(smd_ctx *x, const double *pos) {
         CK(cudaMemcpyAsync(c.flags, &one, sizeof(int), cudaMemcpyHostToDevice, c.stream));
     }
     launch_fixq(c);
+    // realPos starts as these positions (smd_upload_real_positions may set it)
+    CK(cudaMemsetAsync(c.wrap, 0, 3 * (size_t)c.nmol * sizeof(double), c.stream));
+    c.h_real_off.clear();
     CK(cudaStreamSynchronize(c.stream));
     c.list_valid = 0;   // smd_get_pairs builds a fresh list from these positions
     touch(c);
+    return SMD_OK;
+}
+
+int smd_upload_real_positions(smd_ctx *x, const double *real) {
+    if (!x || !real || x->c.n == 0 || !x->c.pos4) return fail(x, SMD_ERR_ARG, "smd_upload_real_positions: bad arguments");
+    Ctx &c = x->c;
+    std::vector<double> p(3 * (size_t)c.n);
+    int r = smd_download_state(x, p.data(), nullptr, nullptr);
+    if (r) return r;
+    std::vector<double> w(3 * (size_t)c.nmol);
+    CK(cudaMemcpy(w.data(), c.wrap, w.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    c.h_real_off.assign(3 * (size_t)c.n, 0.0);
+    for (int i = 0; i < c.n; i++)
+        for (int d = 0; d < 3; d++) {
+            if (!std::isfinite(real[3 * i + d]))
+                return fail(x, SMD_ERR_NAN, "smd_upload_real_positions: non-finite coordinate");
+            c.h_real_off[3 * i + d] = real[3 * i + d] - (p[3 * i + d] - w[(size_t)d * c.nmol + c.h_mol[i]]);
+        }
+    return SMD_OK;
+}
+
+int smd_download_real_positions(smd_ctx *x, double *real) {
+    if (!x || !real || x->c.n == 0) return fail(x, SMD_ERR_ARG, "smd_download_real_positions: bad arguments");
+    Ctx &c = x->c;
+    int r = smd_download_state(x, real, nullptr, nullptr);
+    if (r) return r;
+    std::vector<double> w(3 * (size_t)c.nmol);
+    CK(cudaMemcpy(w.data(), c.wrap, w.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < c.n; i++)
+        for (int d = 0; d < 3; d++) {
+            real[3 * i + d] -= w[(size_t)d * c.nmol + c.h_mol[i]];
+            if (!c.h_real_off.empty()) real[3 * i + d] += c.h_real_off[3 * i + d];
+        }
+    return SMD_OK;
+}
+
+int smd_get_integrator_state(smd_ctx *x, double *state) {
+    if (!x || !state || !x->c.scal) return SMD_ERR_ARG;
+    CK(cudaMemcpyAsync(state, x->c.scal, SC_NSCAL * sizeof(double), cudaMemcpyDeviceToHost, x->c.stream));
+    CK(cudaStreamSynchronize(x->c.stream));
+    return SMD_OK;
+}
+
+int smd_set_integrator_state(smd_ctx *x, const double *state) {
+    if (!x || !state || !x->c.scal) return SMD_ERR_ARG;
+    for (int q = 0; q < SC_NSCAL; q++)
+        if (!std::isfinite(state[q])) return fail(x, SMD_ERR_NAN, "smd_set_integrator_state: non-finite value");
+    CK(cudaMemcpyAsync(x->c.scal, state, SC_NSCAL * sizeof(double), cudaMemcpyHostToDevice, x->c.stream));
+    CK(cudaStreamSynchronize(x->c.stream));
+    touch(x->c);
     return SMD_OK;
 }
 
@@ -1119,12 +1266,16 @@ int smd_set_constraints(smd_ctx *x, const double *len2) {
     return SMD_OK;
 }
 
-int smd_integrator_start(smd_ctx *x) {
+// new_start: LFIntegrator::start's half-step velocities from the forces;
+// otherwise the uploaded ones are kept (the run that continues from
+// state.in and vtMinus.in, LFIntegrator.cpp:187-192)
+static int integrator_begin(smd_ctx *x, bool new_start) {
     if (!x || !x->c.integrator_ready) return fail(x, SMD_ERR_ARG, "smd_integrator_start: call smd_set_integrator first");
     Ctx &c = x->c;
     CK(cudaSetDevice(c.device));
     CK(cudaMemsetAsync(c.status, 0, sizeof(unsigned), c.stream));
     CK(cudaMemsetAsync(c.obs, 0, sizeof(smd_observables), c.stream));
+    CK(cudaMemsetAsync(c.avg, 0, AVG_COUNT * sizeof(double), c.stream));   // averages of this run
     CK(cudaMemsetAsync(c.ticket, 0, sizeof(unsigned), c.stream));
     // the dipole history of the guess starts afresh (uploads keep it: the
     // solve converges to its tolerance from any start)
@@ -1140,7 +1291,7 @@ int smd_integrator_start(smd_ctx *x) {
         CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
     } else {
         enqueue_forces(c);
-        launch_start_velocities(c);
+        if (new_start) launch_start_velocities(c);
     }
     // numUpdates counts the rebuilds of the run, not the start's
     // (LFIntegrator.cpp:307-341): the build count restarts here
@@ -1149,6 +1300,10 @@ int smd_integrator_start(smd_ctx *x) {
     touch(c);
     return sync_status(x);
 }
+
+int smd_integrator_start(smd_ctx *x) { return integrator_begin(x, true); }
+
+int smd_integrator_resume(smd_ctx *x) { return integrator_begin(x, false); }
 
 int smd_run(smd_ctx *x, int nsteps) {
     if (!x || !x->c.integrator_ready || nsteps < 0) return fail(x, SMD_ERR_ARG, "smd_run: integrator not set");

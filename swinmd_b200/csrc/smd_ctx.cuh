@@ -158,6 +158,18 @@ struct Ctx {
     int4 *angles = nullptr;         // (atom1, atom2, atom3, type)
     double2 *bond_par = nullptr;    // per type (r0, k)
     double2 *angle_par = nullptr;   // per type (theta0, k)
+    // radial distribution function (smd_rdf.cu)
+    int rdf_nbins = 0;
+    long long rdf_samples = 0;
+    double rdf_maxr = 0;
+    unsigned long long *rdf_hist = nullptr;  // [ntypes][ntypes][nbins]
+    int excl_intermol = 0;          // some exclusion joins two molecules
+    // Atom::realPos bookkeeping: box shifts per molecule since the last
+    // position upload, and the uploaded offsets realPos - position
+    double *wrap = nullptr;         // [3][nmol]
+    std::vector<double> h_real_off; // [3N] (empty: realPos = position at upload)
+    // running averages of the step observables (smd_integrate.cu)
+    double *avg = nullptr;          // [AVG_COUNT] sums, updated by every step
     // surface-dipole corrections (smd_surface.cu)
     int surface_on = 0;
     double *surf_part = nullptr;    // per-block partial sums
@@ -221,8 +233,38 @@ void launch_torques_end(Ctx &c);
 void launch_frames(Ctx &c);
 void launch_bonded(Ctx &c, bool bond, bool angle, bool ub);
 void launch_intra_flex(Ctx &c, bool mp, bool ind);
+int rdf_sample(Ctx &c);
 void launch_surface(Ctx &c, bool ewald, bool mp, bool ind);
 inline bool has_bonded(const Ctx &c) { return c.nbond > 0 || c.nangle > 0 || c.ub_on; }
+
+// Running sums of the step observables (the energy and stress averages of
+// Ensemble::accumulate, src/Ensemble.cpp:814-894), added by the last block
+// of every step, in the layout of smd_averages after its sample count:
+// [0] samples, [1..11] energies, [12..21] atomic and molecular stress,
+// [22..39] atomic and molecular pressure tensors.
+constexpr int AVG_COUNT = 40;
+__device__ __forceinline__ void accumulate_averages(double *s, const smd_observables &o) {
+    if (!s) return;
+    const double et = o.e_potential + o.ke_atom;
+    s[0] += 1.0;
+    s[1] += o.e_potential; s[2] += o.e_potential * o.e_potential;
+    s[3] += et; s[4] += et * et;
+    s[5] += o.ke_atom; s[6] += o.ke_atom * o.ke_atom;
+    s[7] += o.ke_mol; s[8] += o.ke_mol * o.ke_mol;
+    s[9] += o.ke_mol != 0.0 ? 1.0 / o.ke_mol : 0.0;
+    s[10] += o.volume; s[11] += o.volume * o.volume;
+    const double *P[2] = {o.atom_pressure, o.mol_pressure};
+    for (int t = 0; t < 2; t++) {
+        const double *p = P[t];
+        double *d = s + 12 + 5 * t;
+        d[0] += (p[0] + p[4] + p[8]) / 3.0;
+        d[1] += (p[1] + p[3]) * 0.5;   // shear stress (XY + YX) / 2
+        d[2] += (p[3] - p[1]) * 0.5;   // antisymmetric part (YX - XY) / 2
+        d[3] += p[0] - p[4];           // first normal stress difference
+        d[4] += p[4] - p[8];           // second normal stress difference
+        for (int q = 0; q < 9; q++) s[22 + 9 * t + q] += p[q];
+    }
+}
 
 // the energy components of the accumulator slots (energy[SMD_E_COUNT]);
 // e_lrc and e_self are the constant tail and self energies added to the

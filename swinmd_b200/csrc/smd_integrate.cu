@@ -61,6 +61,8 @@ struct IntArgs {
     smd_observables *obs;
     double *series;
     int series_cap;
+    double *avg;           // running sums of the observables (may be null)
+    double *wrap;          // [3][nmol] box shifts applied to each molecule since the last upload
     Box box;
     double dt, temperature, tau, drmax, total_mass, volume;
     int thermostat, atom_thermo, atom_ndf, mol_ndf, write_fixq;
@@ -313,6 +315,12 @@ __global__ void __launch_bounds__(INT_BLOCK) k_integrate(IntArgs a) {
         const double wx = pbc1(cx, a.box.L[0], a.box.half[0]) - cx;
         const double wy = pbc1(cy, a.box.L[1], a.box.half[1]) - cy;
         const double wz = pbc1(cz, a.box.L[2], a.box.half[2]) - cz;
+        // the shifts so far, per molecule: Atom::realPos = position - shift
+        if (a.wrap && (wx != 0.0 || wy != 0.0 || wz != 0.0)) {
+            a.wrap[m] += wx;
+            a.wrap[a.nmol + m] += wy;
+            a.wrap[2 * a.nmol + m] += wz;
+        }
         for (int k = s; k < e; k++) {
             const int at = a.mol_atoms[k];
             double4 p = a.pos4[at];
@@ -431,6 +439,7 @@ __global__ void __launch_bounds__(INT_BLOCK) k_integrate(IntArgs a) {
             r[0] = o.e_potential; r[1] = o.ke_atom; r[2] = o.t_atom; r[3] = o.zeta;
             r[4] = (o.atom_pressure[0] + o.atom_pressure[4] + o.atom_pressure[8]) / 3.0;
         }
+        accumulate_averages(a.avg, o);
         *a.ticket = 0;
     }
     __syncthreads();
@@ -470,6 +479,8 @@ void launch_integrate(Ctx &c) {
     a.frc = c.frc; a.acc = c.acc; a.scal = c.scal; a.partials = c.partials;
     a.ticket = c.ticket; a.status = c.status; a.flags = c.flags; a.obs = c.obs;
     a.series = c.series; a.series_cap = c.series_cap;
+    a.avg = c.avg;
+    a.wrap = c.wrap;
     a.box = c.box;
     a.dt = c.ip.timestep; a.temperature = c.ip.temperature; a.tau = c.ip.coupl_const;
     a.drmax = c.pl.drmax; a.total_mass = c.total_mass;

@@ -46,6 +46,8 @@ struct NhcArgs {
     smd_observables *obs;
     double *series;
     int series_cap;
+    double *avg;           // running sums of the observables (may be null)
+    double *wrap;          // [3][nmol] box shifts applied to each molecule since the last upload
     Box box;
     double dt, kT, nf, tau, gamma, skin, volume;
     int atom_ndf, mol_ndf;
@@ -161,6 +163,12 @@ __global__ void __launch_bounds__(NHC_BLOCK) k_nhc_first(NhcArgs a) {
         if (g == 0.0) wx = 0;
         wx = pbc1(cx + wx, a.box.L[0], a.box.half[0]) - cx;
         const double wz = pbc1(cz, a.box.L[2], a.box.half[2]) - cz;
+        // the shifts so far, per molecule: Atom::realPos = position - shift
+        if (a.wrap && (wx != 0.0 || wy != 0.0 || wz != 0.0)) {
+            a.wrap[m] += wx;
+            a.wrap[a.nmol + m] += wy;
+            a.wrap[2 * a.nmol + m] += wz;
+        }
         for (int k = s0; k < s1; k++) {
             const int at = a.mol_atoms[k];
             double4 p = a.pos4[at];
@@ -301,6 +309,7 @@ __global__ void __launch_bounds__(NHC_BLOCK) k_nhc_second(NhcArgs a) {
             r[0] = o.e_potential; r[1] = o.ke_atom; r[2] = o.t_atom; r[3] = o.zeta;
             r[4] = o.atom_pressure[1];   // xy: the shear stress under SLLOD
         }
+        accumulate_averages(a.avg, o);
         *a.ticket = 0;
     }
     __syncthreads();
@@ -353,6 +362,8 @@ NhcArgs nhc_args(Ctx &c) {
     a.frc = c.frc; a.acc = c.acc; a.scal = c.scal; a.partials = c.partials;
     a.ticket = c.ticket; a.status = c.status; a.flags = c.flags; a.obs = c.obs;
     a.series = c.series; a.series_cap = c.series_cap;
+    a.avg = c.avg;
+    a.wrap = c.wrap;
     a.box = c.box;
     a.dt = c.ip.timestep; a.kT = KB_N * c.ip.temperature; a.nf = c.ip.atom_ndf; a.tau = c.ip.coupl_const;
     a.gamma = c.ip.strain_rate; a.skin = c.cut_buffer;

@@ -378,6 +378,13 @@ class GpuEnsemble:
         return {"pos": pos.reshape(-1, 3), "vel": vel.reshape(-1, 3), "vtminus": vtm.reshape(-1, 3)}
 
     # -- forces ---------------------------------------------------------
+    def real_positions(self) -> np.ndarray:
+        """Unwrapped positions (Atom::realPos): the stored positions plus the
+        box shifts the integrator applied to each molecule."""
+        real = np.zeros(3 * self.n)
+        self._chk(self.lib.smd_download_real_positions(self.ctx, L.dptr(real)))
+        return real.reshape(self.n, 3)
+
     def compute_forces(self, terms: int = L.TERM_ALL):
         f = np.zeros(3 * self.n)
         e = np.zeros(L.E_COUNT)
@@ -430,6 +437,40 @@ class GpuEnsemble:
     def set_induced(self, p: np.ndarray):
         pp = np.ascontiguousarray(p, np.float64).reshape(-1)
         self._chk(self.lib.smd_set_induced(self.ctx, L.dptr(pp)))
+
+    # -- observables on the device -------------------------------------------
+    def rdf_setup(self, nbins: int):
+        """RDF histogram of nbins bins up to the smallest half box edge
+        (``RDF``, src/observables/RDF.cpp)."""
+        self._chk(self.lib.smd_rdf_setup(self.ctx, int(nbins)))
+        self.rdf_nbins = int(nbins)
+
+    def rdf_sample(self):
+        """Adds the current configuration (``RDF::sampling``)."""
+        self._chk(self.lib.smd_rdf_sample(self.ctx))
+
+    def rdf(self):
+        """(r, g, hist, samples): bin centres, the normalised RDF of each
+        type pair t1 <= t2 (``RDF::write_result``) and the raw counts."""
+        nt = len(self.system.atom_types)
+        nb = self.rdf_nbins
+        hist = np.zeros(nt * nt * nb, np.uint64)
+        g = np.zeros(nt * (nt + 1) // 2 * nb)
+        r = np.zeros(nb)
+        cnt = ctypes.c_int64()
+        self._chk(self.lib.smd_rdf_get(self.ctx, hist.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                       L.dptr(g), L.dptr(r), ctypes.byref(cnt)))
+        return r, g.reshape(-1, nb), hist.reshape(nt, nt, nb), cnt.value
+
+    def averages(self) -> L.Averages:
+        """Means of the step observables since the integrator start or the
+        last reset (``Ensemble::accumulate``)."""
+        a = L.Averages()
+        self._chk(self.lib.smd_get_averages(self.ctx, ctypes.byref(a)))
+        return a
+
+    def reset_averages(self):
+        self._chk(self.lib.smd_averages_reset(self.ctx))
 
     # -- learned initial guess of the induced dipoles ------------------------
     def mlp_init(self, capacity_frames: int, seed: int = 1):
@@ -571,6 +612,37 @@ class LFIntegrator:
         o = L.Observables()
         L.check(self.ens.ctx, self.ens.lib.smd_get_observables(self.ens.ctx, ctypes.byref(o)))
         return o
+
+    # -- checkpoint and restart (Integrator::write_state, LFIntegrator::write_vtMinus)
+    def write_state(self, path: str, vtminus_path: Optional[str] = None):
+        """Writes state.out (positions, real positions, velocities, the
+        integrator's scalars and the box) and, when given, vtMinus.out."""
+        from . import checkpoint
+        e = self.ens
+        st = e.state()
+        real = e.real_positions()
+        scal = np.zeros(32)
+        L.check(e.ctx, e.lib.smd_get_integrator_state(e.ctx, L.dptr(scal)))
+        step = int(self.observables().step)
+        checkpoint.write_state(path, step, st["pos"], real, st["vel"], scal, (e.box, e.box, e.box))
+        if vtminus_path:
+            checkpoint.write_vtminus(vtminus_path, step, st["vtminus"])
+
+    def restart(self, path: str, vtminus_path: Optional[str] = None):
+        """Continues from state.in (and vtMinus.in): the run that does not
+        start new (Ensemble::set_configuration, src/Ensemble.cpp:303-317;
+        LFIntegrator::read_vtMinus).  Without vtMinus.in the half-step
+        velocities are the on-step ones, as the reference takes them."""
+        from . import checkpoint
+        e = self.ens
+        _, pos, real, vel, scal, _ = checkpoint.read_state(path)
+        vtm = checkpoint.read_vtminus(vtminus_path) if vtminus_path else None
+        e.upload_positions(pos)
+        L.check(e.ctx, e.lib.smd_upload_real_positions(e.ctx, L.dptr(np.ascontiguousarray(real.reshape(-1)))))
+        e.upload_velocities(vel, vtm)
+        L.check(e.ctx, e.lib.smd_integrator_resume(e.ctx))
+        if scal is not None:
+            L.check(e.ctx, e.lib.smd_set_integrator_state(e.ctx, L.dptr(np.ascontiguousarray(scal))))
 
     def series(self) -> np.ndarray:
         out = np.zeros(5 * max(self.series_capacity, 1))

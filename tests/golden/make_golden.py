@@ -33,7 +33,7 @@ from conftest import pair_digest  # noqa: E402
 def lj500():
     s = systems.lj_fluid(ncell=5, jitter_star=0.05, seed=3, n_steps=20)
     s.config.long_correct = True
-    return s, [("forces",), ("run", 20)]
+    return s, [("forces",), ("run", 20), ("rdf",)]
 
 
 def nacl1000_mie():
@@ -43,13 +43,23 @@ def nacl1000_mie():
 
 def spce512():
     s = systems.spce_water(nmol=512, box=2.4953, cutoff=0.9, kmax=6, seed=11, n_steps=20)
-    return s, [("forces",), ("run", 20)]
+    return s, [("forces",), ("run", 20), ("rdf",)]
 
 
 def polwater216():
     s = systems.polarizable_water(nmol=216, cutoff=0.9, switch=0.8, alpha=3.5, kmax=7, seed=3,
                                   n_steps=10)
     return s, [("forces",), ("run", 10)]
+
+
+def polwater216_nve():
+    # the same water without thermostat: energy conservation of the model as
+    # the reference integrates it (its total energy rises: the GPU run must
+    # follow the same curve, not a conserved one)
+    s = systems.polarizable_water(nmol=216, cutoff=0.9, switch=0.8, alpha=3.5, kmax=7, seed=3,
+                                  n_steps=80)
+    s.config.thermostat = "None"
+    return s, [("forces",), ("run", 80)]
 
 
 # Full-size cases: the configurations the benchmark runs.  Their pair sets
@@ -100,7 +110,7 @@ def ref_test_nvt():
 
 
 CASES = {"lj500": lj500, "nacl1000_mie": nacl1000_mie, "spce512": spce512,
-         "polwater216": polwater216, "ref_test_nvt": ref_test_nvt}
+         "polwater216": polwater216, "polwater216_nve": polwater216_nve, "ref_test_nvt": ref_test_nvt}
 LARGE = {"lj4000": lj4000, "lj4000_jitter": lj4000_jitter, "nacl8000_mie": nacl8000_mie, "spce2160": spce2160,
          "polwater4096": polwater4096}
 
@@ -133,6 +143,10 @@ def pack(name, s, results, large=False):
         for k, v in results["mie"].items():
             if k.startswith("mie_"):
                 out["m_" + k] = v
+    if "rdf" in results:
+        for k, v in results["rdf"].items():
+            if k.startswith("rdf_"):
+                out[k] = v
     if "run" in results:
         for k, v in results["run"].items():
             if k.startswith(("step_", "final_", "start_")):
@@ -150,6 +164,9 @@ def pack(name, s, results, large=False):
             for fn, key in (("config.txt", "case_config"), ("sysData.in", "case_sysdata"),
                             ("coordinate.in", "case_coords")):
                 out[key] = np.array(open(os.path.join(d, fn)).read())
+    if name.endswith("_nve"):
+        # the trajectory only: the forces of the start are polwater216's
+        out = {k: v for k, v in out.items() if not k.startswith("f_") and k != "pairs"}
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
 
 
