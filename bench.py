@@ -13,11 +13,15 @@ one after another on the same trajectory:
                          from the molecule-block solution M^-1 E0;
   plain_reference_forms  the same FP64 arm with the reference's own forms
                          (one FP64 sine/cosine per (site, k), pow() 14-7);
-  fast_first_order       mixed precision, solve started from the first-order
-                         guess p(t-1) + M^-1 (E0(t) - E0(t-1)), network off;
-  fast                   mixed precision + the learned guess (the per-site
-                         network trained beforehand, on the GPU, on dipoles the
-                         solver itself converged): the headline `value`.
+  fast_network_off       mixed precision, solve started from the second-order
+                         extrapolation 2 p(t-1) - p(t-2) + M^-1 (E0(t) -
+                         2 E0(t-1) + E0(t-2)): the learned guess's base with
+                         the network switched off;
+  fast                   mixed precision + the learned guess (that base plus
+                         the per-site network's correction; the network is
+                         trained beforehand, on the GPU's tensor cores, on
+                         dipoles the solver itself converged): the headline
+                         `value`.
 Every arm solves the dipoles to the same tolerance (RMS change 1e-6 D).  The
 line also carries the solver's iterations from each guess, each arm's force
 error against FP64 with the dipoles solved to 1e-13 e nm, pair interactions
@@ -362,9 +366,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="polwater4096")
     ap.add_argument("--chunk", type=int, default=100)
-    ap.add_argument("--train-frames", type=int, default=2000)
-    ap.add_argument("--train-every", type=int, default=1)
-    ap.add_argument("--train-epochs", type=int, default=8)
+    ap.add_argument("--train-frames", type=int, default=80)
+    ap.add_argument("--train-every", type=int, default=5)
+    ap.add_argument("--train-epochs", type=int, default=40)
     ap.add_argument("--e2e-every", type=int, default=10)
     ap.add_argument("--cpu-sample-mols", type=int, default=1024)
     ap.add_argument("--equilibrate", type=int, default=10000)
@@ -467,7 +471,7 @@ def main():
     plain_ref = arm("fp64", L.GUESS_DIRECT, reference_forms=True, steps=max(10, args.steps // 4))
     ens.set_reference_forms(False)
     # fast without the network: mixed path, first-order guess
-    first_order = arm("mixed", L.GUESS_FIRST_ORDER) if polar else None
+    network_off = arm("mixed", L.GUESS_EXTRAP2) if polar else None
     # fast: mixed path + learned guess (the headline)
     fast = arm("mixed", L.GUESS_LEARNED if polar else L.GUESS_DIRECT)
     clocks_all = clk_all.stop()
@@ -479,14 +483,17 @@ def main():
     iters = {}
     if polar:
         for name, g in (("direct", L.GUESS_DIRECT), ("previous", L.GUESS_PREVIOUS),
-                        ("first_order", L.GUESS_FIRST_ORDER), ("learned", L.GUESS_LEARNED)):
+                        ("first_order", L.GUESS_FIRST_ORDER), ("extrap2", L.GUESS_EXTRAP2),
+                        ("extrap3", L.GUESS_EXTRAP3), ("learned", L.GUESS_LEARNED)):
             ens.set_solver(tol=DIPOLE_TOL, max_iter=500, guess=g)
             lf.run(3)
-            its = []
+            its, first = [], []
             for _ in range(args.iter_steps):
                 lf.run(1)
                 its.append(ens.solver_stats()[0])
-            iters[name] = {"mean": float(np.mean(its)), "min": int(min(its)), "max": int(max(its))}
+                first.append(ens.solver_trace()[0])
+            iters[name] = {"mean": float(np.mean(its)), "min": int(min(its)), "max": int(max(its)),
+                           "first_update_rms": float(np.exp(np.mean(np.log(first))))}
 
     # force error at matched dipole tolerance: each arm's evaluation of the
     # current configuration against FP64 with the dipoles solved to 1e-13 e nm
@@ -675,14 +682,15 @@ def main():
                "plain_reference_forms": dict(plain_ref, dtype="f64", guess="M^-1 E0 (molecule blocks)",
                                              algorithms="the reference's: one FP64 sine/cosine per (site, k), "
                                                         "pow() 14-7"),
-               "fast_first_order": first_order and dict(first_order, guess="p(t-1) + M^-1 dE0 (network off)"),
+               "fast_network_off": network_off and dict(
+                   network_off, guess="2 p(t-1) - p(t-2) + M^-1 (E0 - 2 E0(t-1) + E0(t-2)) (network off)"),
                "fast": dict(fast, guess="learned" if polar else "n/a",
                             force_rms_rel_err_vs_fp64_tight=force_err.get("fast")),
                "plain_force_rms_rel_err_vs_fp64_tight": force_err.get("plain"),
                "speedup_fast_vs_plain": plain["ms_per_step"] / fast["ms_per_step"],
                "speedup_fast_vs_plain_reference_forms": plain_ref["ms_per_step"] / fast["ms_per_step"],
-               "speedup_learned_vs_first_order": (first_order["ms_per_step"] / fast["ms_per_step"]
-                                                  if first_order else None),
+               "speedup_learned_vs_network_off": (network_off["ms_per_step"] / fast["ms_per_step"]
+                                                  if network_off else None),
                "solver_iterations_by_guess": iters,
                "pair_interactions_per_s": pairs / (fast["ms_per_step"] * 1e-3),
                "pair_interactions_note": "unordered site pairs inside the short-range cutoff per step "

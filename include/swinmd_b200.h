@@ -90,10 +90,18 @@ enum {
                                   permanent field (alpha E0 with the site
                                   preconditioner) */
     SMD_GUESS_PREVIOUS = 1,    /* p0 = the previous solve's dipoles */
-    SMD_GUESS_LEARNED = 2,     /* p0 = first-order guess + the per-site network's
-                                  correction (smd_mlp_*) */
-    SMD_GUESS_FIRST_ORDER = 3  /* p0 = p(t-1) + M^-1 (E0(t) - E0(t-1)): the learned
-                                  guess without the network */
+    SMD_GUESS_LEARNED = 2,     /* p0 = the extrapolated guess of order
+                                  smd_mlp_set_base (default 2) + the per-site
+                                  network's correction (smd_mlp_*) */
+    SMD_GUESS_FIRST_ORDER = 3, /* p0 = p(t-1) + M^-1 (E0(t) - E0(t-1)): the learned
+                                  guess of order 1 without the network */
+    SMD_GUESS_EXTRAP2 = 4,     /* the mutual part u = p - M^-1 E0 extrapolated
+                                  linearly over the stored steps:
+                                  p0 = 2 p(t-1) - p(t-2)
+                                       + M^-1 (E0(t) - 2 E0(t-1) + E0(t-2)) */
+    SMD_GUESS_EXTRAP3 = 5      /* the same, quadratically:
+                                  p0 = 3 p(t-1) - 3 p(t-2) + p(t-3)
+                                       + M^-1 (E0(t) - 3 E0(t-1) + 3 E0(t-2) - E0(t-3)) */
 };
 
 /* thermostat kinds: SMD_THERMO_NOSE_HOOVER is the leap-frog integrator of
@@ -253,6 +261,10 @@ int smd_set_wait_limit(smd_ctx *ctx, double seconds);
 int smd_test_skip_arrival(smd_ctx *ctx, int block);
 /* Solver statistics of the last solve: iterations and final RMS change. */
 int smd_solver_stats(smd_ctx *ctx, int *iterations, double *rms_change);
+/* RMS change of the dipoles at each iteration of the last solve (the
+ * quantity the tolerance is tested on), up to 64 iterations: rms[k] for
+ * k < min(count, cap).  The first entry measures how far the start was. */
+int smd_solver_trace(smd_ctx *ctx, double *rms, int cap, int *count);
 /* Lab-frame dipoles, quadrupoles, permanent field and induced dipoles of the
  * last evaluation, per site (each pointer may be NULL): mu[3n], quad[6n]
  * (xx xy xz yy yz zz, the reference's /3 convention), e0[3n], p[3n]. */
@@ -272,6 +284,14 @@ int smd_set_induced(smd_ctx *ctx, const double *p);
 /* Allocates the network (seeded weights) and room for capacity_frames
  * configurations of training rows. */
 int smd_mlp_init(smd_ctx *ctx, int capacity_frames, unsigned int seed);
+/* The network's sizes: inputs per site (the width of smd_mlp_features and
+ * smd_mlp_eval rows; smd_mlp_gradient rows add the 3 targets) and weights
+ * (the gradient's length; smd_mlp_params adds 2 * features). */
+int smd_mlp_dims(int *features, int *params);
+/* Order (1-3) of the extrapolated guess the network corrects (SMD_GUESS_
+ * FIRST_ORDER, EXTRAP2, EXTRAP3 without it).  Part of the trained model: set
+ * it before smd_mlp_collect. */
+int smd_mlp_set_base(smd_ctx *ctx, int order);
 /* Appends the current configuration's rows (features and the converged
  * dipoles of the last force evaluation); needs two stored time steps. */
 int smd_mlp_collect(smd_ctx *ctx);

@@ -26,7 +26,7 @@ E_VDW, E_REAL, E_LONG, E_CORRECT, E_MOLCORRECT, E_SURF = 0, 1, 2, 3, 4, 5
 E_POL_REAL, E_POL_LONG, E_POL_SELF, E_POL_INTRA = 6, 7, 8, 9
 E_POL_SURF, E_BOND, E_ANGLE, E_UB, E_TERMS, E_COUNT = 10, 11, 12, 13, 14, 16
 VDW_NONE, VDW_LJ, VDW_MIE, VDW_BMH, VDW_BUFF = 0, 1, 2, 3, 4
-GUESS_DIRECT, GUESS_PREVIOUS, GUESS_LEARNED, GUESS_FIRST_ORDER = 0, 1, 2, 3
+GUESS_DIRECT, GUESS_PREVIOUS, GUESS_LEARNED, GUESS_FIRST_ORDER, GUESS_EXTRAP2, GUESS_EXTRAP3 = 0, 1, 2, 3, 4, 5
 PRECOND_SITE, PRECOND_MOLECULE = 0, 1
 THERMO_NONE, THERMO_NOSE_HOOVER, THERMO_NH_CHAIN = 0, 1, 2
 
@@ -131,11 +131,14 @@ SIGNATURES = {
     "smd_set_solver": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
     "smd_set_preconditioner": (ctypes.c_int, [_P, ctypes.c_int]),
     "smd_solver_stats": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), _D]),
+    "smd_solver_trace": (ctypes.c_int, [_P, _D, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "smd_set_wait_limit": (ctypes.c_int, [_P, ctypes.c_double]),
     "smd_test_skip_arrival": (ctypes.c_int, [_P, ctypes.c_int]),
     "smd_get_polarization": (ctypes.c_int, [_P, _D, _D, _D, _D]),
     "smd_set_induced": (ctypes.c_int, [_P, _D]),
     "smd_mlp_init": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_uint]),
+    "smd_mlp_dims": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "smd_mlp_set_base": (ctypes.c_int, [_P, ctypes.c_int]),
     "smd_mlp_collect": (ctypes.c_int, [_P]),
     "smd_mlp_train": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_uint, _D]),
     "smd_mlp_params": (ctypes.c_int, [_P, _F, _F, ctypes.POINTER(ctypes.c_int)]),

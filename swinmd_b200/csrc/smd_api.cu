@@ -771,8 +771,8 @@ int smd_set_multipole(smd_ctx *x, const double *type_mp, const double *polar, do
     CK(cudaMemset(c.e0, 0, 3 * n * sizeof(double)));
     int r = setup_cg(c);
     if (r) return fail(x, r, "smd_set_multipole: solver set-up failed");
-    CK(dalloc(&c.cgs, 8 + 16 * (size_t)c.cg_blocks));
-    CK(cudaMemset(c.cgs, 0, (8 + 16 * (size_t)c.cg_blocks) * sizeof(double)));
+    CK(dalloc(&c.cgs, CG_SCAL + CG_TRACE + 16 * (size_t)c.cg_blocks));
+    CK(cudaMemset(c.cgs, 0, (CG_SCAL + CG_TRACE + 16 * (size_t)c.cg_blocks) * sizeof(double)));
     CK(dalloc(&c.cg_bar, 2));
     if (c.ind_on) {
         CK(dalloc(&c.phist, 24 * n));
@@ -787,7 +787,7 @@ int smd_set_multipole(smd_ctx *x, const double *type_mp, const double *polar, do
 }
 
 int smd_set_solver(smd_ctx *x, double tol, int max_iter, int guess) {
-    if (!x || !(tol > 0) || max_iter <= 0 || guess < 0 || guess > SMD_GUESS_FIRST_ORDER)
+    if (!x || !(tol > 0) || max_iter <= 0 || guess < 0 || guess > SMD_GUESS_EXTRAP3)
         return fail(x, SMD_ERR_ARG, "smd_set_solver: bad arguments");
     x->c.cg_tol = tol;
     x->c.cg_max_iter = max_iter;
@@ -831,6 +831,17 @@ int smd_solver_stats(smd_ctx *x, int *iterations, double *rms_change) {
     CK(cudaStreamSynchronize(x->c.stream));
     if (iterations) *iterations = (int)s[0];
     if (rms_change) *rms_change = s[1];
+    return SMD_OK;
+}
+
+int smd_solver_trace(smd_ctx *x, double *rms, int cap, int *count) {
+    if (!x || !x->c.cgs || !count || (cap > 0 && !rms)) return fail(x, SMD_ERR_ARG, "smd_solver_trace: bad arguments");
+    double s[CG_SCAL + CG_TRACE];
+    CK(cudaMemcpyAsync(s, x->c.cgs, sizeof(s), cudaMemcpyDeviceToHost, x->c.stream));
+    CK(cudaStreamSynchronize(x->c.stream));
+    const int it = std::min((int)s[0], CG_TRACE);
+    for (int k = 0; k < std::min(it, cap); k++) rms[k] = s[CG_SCAL + k];
+    *count = it;
     return SMD_OK;
 }
 
@@ -880,6 +891,20 @@ int smd_mlp_init(smd_ctx *x, int capacity_frames, unsigned int seed) {
     return SMD_OK;
 }
 
+int smd_mlp_dims(int *features, int *params) {
+    if (features) *features = mlp_nfeat();
+    if (params) *params = mlp_nparam();
+    return SMD_OK;
+}
+
+int smd_mlp_set_base(smd_ctx *x, int order) {
+    if (!x || order < 1 || order > 3) return fail(x, SMD_ERR_ARG, "smd_mlp_set_base: order must be 1, 2 or 3");
+    x->c.mlp_base = order;
+    x->c.graph_dirty = 1;
+    touch(x->c);
+    return SMD_OK;
+}
+
 int smd_mlp_collect(smd_ctx *x) {
     if (!x || !x->c.mlp_data) return fail(x, SMD_ERR_ARG, "smd_mlp_collect: call smd_mlp_init first");
     Ctx &c = x->c;
@@ -915,15 +940,10 @@ int smd_mlp_train(smd_ctx *x, int epochs, int batch, double lr, unsigned int see
     }
     if (loss) {  // mean-squared error over (up to) the first max-batch rows of the last order
         const int b = (int)std::min<long long>(rows, mlp_max_batch());
-        launch_mlp_step(c, dperm, 0, b, 0.f, c.mlp_part + (size_t)64 * mlp_nparam() + 64);
-        std::vector<float> lp(64);
-        const int nb = (b + 255) / 256;
-        CK(cudaMemcpyAsync(lp.data(), c.mlp_part + (size_t)64 * mlp_nparam(), nb * sizeof(float),
-                           cudaMemcpyDeviceToHost, c.stream));
-        CK(cudaStreamSynchronize(c.stream));
-        double t = 0;
-        for (int q = 0; q < nb; q++) t += lp[q];
-        *loss = t;
+        if (mlp_batch_loss(c, dperm, b, loss)) {
+            cudaFree(dperm);
+            return fail(x, SMD_ERR_CUDA, "smd_mlp_train: loss evaluation failed");
+        }
     }
     cudaFree(dperm);
     c.mlp_ready = 1;

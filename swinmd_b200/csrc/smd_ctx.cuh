@@ -13,6 +13,8 @@ namespace smd {
 enum VdwKind { VDW_NONE = 0, VDW_LJ = 1, VDW_MIE = 2, VDW_BMH = 3, VDW_BUFF = 4 };
 
 // surface-correction reduction: blocks of partial sums and sums per block
+constexpr int CG_SCAL = 8;     // iterations, final RMS change, ...
+constexpr int CG_TRACE = 64;   // RMS change of each iteration of the last solve
 constexpr int SURF_BLOCKS = 64, SURF_SUMS = 11;
 
 // Per type pair parameters of the short-range pair term (ntypes^2 rows of 8).
@@ -115,7 +117,7 @@ struct Ctx {
     double *pind = nullptr;         // [3][N] induced dipoles
     float4 *srec = nullptr;         // [N][4] mixed path, FP32: (q, mu), (Qxx, Qxy, Qxz, Qyy), (Qyz, Qzz, px, py), (pz, 0, 0, 0)
     double *cgw = nullptr;          // CG work: r, w, p [3][N] each, alpha [N], two gather copies [N][4], s, u [3][N]
-    double *cgs = nullptr;          // CG scalars [8] and partials [4][blocks][4]
+    double *cgs = nullptr;          // CG scalars [CG_SCAL], trace [CG_TRACE], partials [4][blocks][4]
     int cg_max_iter = 500;
     double cg_tol = 2.0819e-8;      // RMS dipole change tolerance (e nm); 1e-6 D
     int cg_guess = 0;               // SMD_GUESS_*: 0 block solution of E0, 1 previous step, 2 learned, 3 first order
@@ -134,6 +136,7 @@ struct Ctx {
     double *frame = nullptr;        // [9][N] site axes u, v, w (lab frame)
     // per-site network giving the initial induced dipoles (smd_mlp.cu)
     int mlp_ready = 0;
+    int mlp_base = 2;                // order of the extrapolated guess the network corrects
     float *mlp_w = nullptr;         // parameters, MLP_NPARAM floats
     float *mlp_m = nullptr, *mlp_v = nullptr;  // Adam moments
     float *mlp_part = nullptr;      // per-block gradient partials
@@ -293,10 +296,21 @@ int ensure_ind_rows(Ctx &c);
 int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed);
 void launch_mlp_guess(Ctx &c);
 void launch_first_order_guess(Ctx &c);
-void launch_blk_response(Ctx &c, double *out);
+void launch_blk_response(Ctx &c, double *out, int order, double *out_prev);
+// order of the extrapolated guess of the solver's guess mode (0: none)
+inline int guess_order(const Ctx &c) {
+    return c.cg_guess == SMD_GUESS_FIRST_ORDER ? 1
+           : c.cg_guess == SMD_GUESS_EXTRAP2   ? 2
+           : c.cg_guess == SMD_GUESS_EXTRAP3   ? 3
+                                               : 0;
+}
 // first-order part of the learned guess: the solver's s slot of its work
 // area, which the solve writes before it first reads it
 inline double *guess_response(Ctx &c) { return c.cgw + 20 * (size_t)c.n; }
+// M^-1 (E0(t-1) - E0(t-2)), the network's input (the solve's residual
+// buffer, free until the solve starts)
+inline double *guess_response_prev(Ctx &c) { return c.cgw; }
+int mlp_batch_loss(Ctx &c, const unsigned int *perm, int batch, double *loss);
 void launch_mlp_features(Ctx &c);
 void launch_mlp_collect(Ctx &c);
 void launch_mlp_norm(Ctx &c);

@@ -477,14 +477,15 @@ __device__ V3 amul(const CGArgs &c, int i, int t, const G4 *g) {
 // so that the solve's loads of one entry coalesce.
 constexpr int MB_MOLS = 32;
 // With dl given, the same threads also form the blocks' response to the
-// change of the permanent field since the last stored step,
-// dl = M_m^-1 (E0(t) - E0(t-1)) (M_m^-1 E0 when none is stored), the first-order
-// part of the learned guess (as k_blk_response does from the stored blocks).
+// permanent field's difference of the extrapolated guess of the given order,
+// dl = M_m^-1 (E0(t) - sum_j w_j E0(t-j)) (M_m^-1 E0 when no step is stored;
+// as k_blk_response does from the stored blocks).
 template <typename TS>
 __global__ void __launch_bounds__(9 * MB_MOLS) k_mol_blocks(int n, int nmol, const int *mol_off, const int *mol_atoms,
                                                             TRows R, const double *polar, const double4 *pos4,
                                                             double *blk, const double *e0, const double *ph,
-                                                            const int *flags, double *dl) {
+                                                            const int *flags, double *dl, int order,
+                                                            double *dlp) {
     using TS4 = typename std::conditional<sizeof(TS) == 4, float4, double4>::type;
     __shared__ double s_piv[MB_MOLS][9];
     __shared__ int s_bad[MB_MOLS];
@@ -570,7 +571,7 @@ __global__ void __launch_bounds__(9 * MB_MOLS) k_mol_blocks(int n, int nmol, con
         double de = 0.0;
         if (i >= 0) {
             const size_t idx = (size_t)x * n + i;
-            de = e0[idx] - (cnt >= 1 ? ph[(size_t)((cnt - 1) & 3) * 6 * n + 3 * (size_t)n + idx] : 0.0);
+            de = hist_diff_e(ph, n, cnt, order, idx, e0[idx]);
         }
         s_de[lm][r] = de;
         __syncthreads();
@@ -579,6 +580,23 @@ __global__ void __launch_bounds__(9 * MB_MOLS) k_mol_blocks(int n, int nmol, con
 #pragma unroll
             for (int c = 0; c < 9; c++) u += row[c] * s_de[lm][c];
             dl[(size_t)x * n + i] = u;
+        }
+        if (dlp) {   // the last step's response, M_m^-1 (E0(t-1) - E0(t-2))
+            __syncthreads();
+            double dp = 0.0;
+            if (i >= 0 && cnt >= 2) {
+                const size_t idx = (size_t)x * n + i;
+                dp = ph[(size_t)((cnt - 1) & 3) * 6 * n + 3 * (size_t)n + idx] -
+                     ph[(size_t)((cnt - 2) & 3) * 6 * n + 3 * (size_t)n + idx];
+            }
+            s_de[lm][r] = dp;
+            __syncthreads();
+            if (i >= 0) {
+                double u = 0.0;
+#pragma unroll
+                for (int c = 0; c < 9; c++) u += row[c] * s_de[lm][c];
+                dlp[(size_t)x * n + i] = u;
+            }
         }
     }
 }
@@ -800,6 +818,7 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
         grid_sum(pu, c.nblocks, 2, tot, s_w);
         const double gamma_new = tot[0];
         rms = sqrt(tot[1] / (3.0 * n));
+        if (blockIdx.x == 0 && threadIdx.x == 0 && it < CG_TRACE) c.scal[CG_SCAL + it] = rms;
         if (rms < c.tol) {
             conv = true;
             it++;
@@ -1540,40 +1559,41 @@ void launch_ind_field(Ctx &c) {
         k_ind_field<double><<<nb, 256, 0, c.stream>>>(a, R, c.status);
     // the preconditioner's inverse molecule blocks (they need this step's tensor rows)
     const bool learned = c.cg_guess == SMD_GUESS_LEARNED && c.mlp_ready;
-    const bool first_order = c.cg_guess == SMD_GUESS_FIRST_ORDER;
+    const bool first_order = guess_order(c) > 0 && !learned;
+    const int order = learned ? c.mlp_base : guess_order(c);
     if (c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk) {
-        // with the learned or first-order guess, also the first-order part
+        // with the learned or extrapolated guess, also the blocks' responses
         double *dl = (learned || first_order) ? guess_response(c) : nullptr;
+        double *dlp = learned ? guess_response_prev(c) : nullptr;
         const int nbm = (c.nmol + MB_MOLS - 1) / MB_MOLS;
         if (f32)
             k_mol_blocks<float><<<nbm, 9 * MB_MOLS, 0, c.stream>>>(c.n, c.nmol, c.mol_off, c.mol_atoms, R,
                                                                    c.type_polar, c.pos4, c.cg_blk, c.e0, c.phist,
-                                                                   c.flags, dl);
+                                                                   c.flags, dl, order, dlp);
         else
             k_mol_blocks<double><<<nbm, 9 * MB_MOLS, 0, c.stream>>>(c.n, c.nmol, c.mol_off, c.mol_atoms, R,
                                                                     c.type_polar, c.pos4, c.cg_blk, c.e0, c.phist,
-                                                                    c.flags, dl);
+                                                                    c.flags, dl, order, dlp);
     }
     if (learned) launch_mlp_guess(c);  // writes the start dipoles into p
     else if (first_order) launch_first_order_guess(c);
 }
 
-// Response of each molecule's own block to the change of the permanent field
-// since the last stored step, out = M_m^-1 (E0(t) - E0(t-1)) (M_m^-1 E0(t)
-// when no step is stored), nine threads per molecule; with the site
-// preconditioner the block is diag(alpha).  It is the first-order part of
-// the learned guess.
+// Response of each molecule's own block to the permanent field's difference
+// of the extrapolated guess of the given order, out = M_m^-1 (E0(t) -
+// sum_j w_j E0(t-j)) (M_m^-1 E0(t) when no step is stored), nine threads per
+// molecule; with the site preconditioner the block is diag(alpha).
 constexpr int RESP_MOLS = 32;
 __global__ void __launch_bounds__(9 * RESP_MOLS) k_blk_response(int n, int nmol, const int *mol_off,
                                                                const int *mol_atoms, const double *blk,
                                                                const double *polar, const double4 *pos4,
                                                                const double *e0, const double *ph,
-                                                               const int *flags, double *out) {
+                                                               const int *flags, double *out, int order,
+                                                               double *out_prev) {
     __shared__ double s_v[9 * RESP_MOLS];
     const int ml = threadIdx.x / 9, e = threadIdx.x - 9 * ml, q = e / 3, d = e - 3 * q;
     const int m = blockIdx.x * RESP_MOLS + ml;
     const int cnt = flags[2];
-    const double *eprev = cnt >= 1 ? ph + (size_t)((cnt - 1) & 3) * 6 * n + 3 * (size_t)n : nullptr;
     int ns = 0, i = -1;
     if (m < nmol) {
         const int s0 = mol_off[m];
@@ -1581,22 +1601,32 @@ __global__ void __launch_bounds__(9 * RESP_MOLS) k_blk_response(int n, int nmol,
         if (q < ns) i = mol_atoms[s0 + q];
     }
     const size_t idx = (size_t)d * n + i;
-    s_v[threadIdx.x] = i >= 0 ? e0[idx] - (eprev ? eprev[idx] : 0.0) : 0.0;
+    s_v[threadIdx.x] = i >= 0 ? hist_diff_e(ph, n, cnt, order, idx, e0[idx]) : 0.0;
     __syncthreads();
-    if (i < 0) return;
-    double u = 0.0;
-    if (blk) {
-        for (int col = 0; col < 3 * ns; col++) u += blk[(size_t)(e * 9 + col) * nmol + m] * s_v[9 * ml + col];
-    } else {
-        u = fmax(1e-8, polar[(int)pos4[i].w]) * s_v[threadIdx.x];
-    }
-    out[idx] = u;
+    auto apply = [&]() {
+        double u = 0.0;
+        if (blk) {
+            for (int col = 0; col < 3 * ns; col++) u += blk[(size_t)(e * 9 + col) * nmol + m] * s_v[9 * ml + col];
+        } else {
+            u = fmax(1e-8, polar[(int)pos4[i].w]) * s_v[threadIdx.x];
+        }
+        return u;
+    };
+    if (i >= 0) out[idx] = apply();
+    if (!out_prev) return;   // block-uniform
+    __syncthreads();
+    s_v[threadIdx.x] = i >= 0 && cnt >= 2 ? ph[(size_t)((cnt - 1) & 3) * 6 * n + 3 * (size_t)n + idx] -
+                                                ph[(size_t)((cnt - 2) & 3) * 6 * n + 3 * (size_t)n + idx]
+                                          : 0.0;
+    __syncthreads();
+    if (i >= 0) out_prev[idx] = apply();
 }
 
-void launch_blk_response(Ctx &c, double *out) {
+void launch_blk_response(Ctx &c, double *out, int order, double *out_prev) {
     const double *blk = c.cg_precond == SMD_PRECOND_MOLECULE ? c.cg_blk : nullptr;
     k_blk_response<<<(c.nmol + RESP_MOLS - 1) / RESP_MOLS, 9 * RESP_MOLS, 0, c.stream>>>(
-        c.n, c.nmol, c.mol_off, c.mol_atoms, blk, c.type_polar, c.pos4, c.e0, c.phist, c.flags, out);
+        c.n, c.nmol, c.mol_off, c.mol_atoms, blk, c.type_polar, c.pos4, c.e0, c.phist, c.flags, out, order,
+        out_prev);
 }
 
 // the PCG solve from the start dipoles, then the site records' new dipoles
@@ -1614,12 +1644,12 @@ void launch_ind_cg(Ctx &c) {
     g.r = c.cgw; g.z = c.cgw + 3 * n; g.v = c.cgw + 6 * n; g.al = c.cgw + 9 * n;
     g.g0 = c.cgw + 12 * n; g.g1 = c.cgw + 16 * n;
     g.s = c.cgw + 20 * n; g.u = c.cgw + 23 * n;
-    g.part = c.cgs + 8; g.scal = c.cgs; g.bar = c.cg_bar; g.status = c.status;
+    g.part = c.cgs + CG_SCAL + CG_TRACE; g.scal = c.cgs; g.bar = c.cg_bar; g.status = c.status;
     g.wait_ns = c.wait_ns;
     g.skip_block = c.test_skip_block;
     g.nblocks = c.cg_blocks; g.max_iter = c.cg_max_iter; g.tol = c.cg_tol;
     // 0: start from alpha E0; 1: start from the dipoles in p (previous solve or network)
-    g.guess = (c.cg_guess == SMD_GUESS_PREVIOUS || c.cg_guess == SMD_GUESS_FIRST_ORDER || learned) ? 1 : 0;
+    g.guess = (c.cg_guess == SMD_GUESS_PREVIOUS || guess_order(c) > 0 || learned) ? 1 : 0;
     const bool bj = c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk;   // blocks built by launch_ind_field
     g.blk = c.cg_blk;
     // the mixed path's site records take the dipoles inside the solve

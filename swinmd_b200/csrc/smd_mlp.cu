@@ -2,13 +2,14 @@
 //
 // The induced dipoles are solved to the same tolerance from whatever start
 // the solver is given; this guess only brings the start closer, so the solve
-// needs fewer iterations.  The guess is the previous step's converged
-// dipoles moved by the linear response to the change of the permanent field,
-// pl = p(t-1) + alpha (E0(t) - E0(t-1)), plus a correction the network
-// predicts (the mutual induction the first-order response leaves out).
-// Each time step stores its converged dipoles and permanent field.
+// needs fewer iterations.  The guess is an extrapolation of the stored
+// steps' dipoles (order 1-3, smd_mlp_set_base: the mutual part p - M^-1 E0 of
+// the last steps carried forward, with the molecule blocks' response to this
+// step's permanent field), plus a correction the network predicts from the
+// site's own descriptors.  Each time step stores its converged dipoles and
+// permanent field in a ring of four.
 //
-// Inputs (F = 20 per site, in the site's own axes u, v, w, so invariant under
+// Inputs (F = 24 per site, in the site's own axes u, v, w, so invariant under
 // rotation of the system):
 //   0-2   permanent field E0(t) at the site
 //   3     |E0(t)|
@@ -16,26 +17,45 @@
 //   7-12  E0(t) at the molecule's two other sites
 //   13-15 p(t-1)
 //   16-18 p(t-1) - p(t-2)
-//   19    site type (O = 1, H = 0)
-// Output (3): 1e5 (p - pl) in the site axes.
-// Network: F -> 64 -> 64 -> 3, tanh hidden activations, FP32 weights.
-// Training (on rows the solver itself produced): mean-squared error, Adam,
-// forward and backward on the GPU with one thread per row; weight gradients
-// are reduced within a warp by shuffles, then per block in shared memory,
-// then over blocks in a fixed order by the Adam kernel.
+//   19-21 the mutual increment of the last step,
+//         p(t-1) - p(t-2) - M^-1 (E0(t-1) - E0(t-2))
+//   22    |E0(t) - E0(t-1)|
+//   23    site type (O = 1, H = 0)
+// Output (3): 1e5 (p - guess) in the site axes.
+// Network: F -> 64 -> 64 -> 3, tanh hidden activations; FP32 master
+// weights (Adam), BF16 operands of the two wide layers on the tensor cores
+// (mma.sync m16n8k16, FP32 accumulation), the 64 -> 3 output layer in FP32.
+//
+// Every kernel works in warps of 16 rows (sites or training rows): a warp's
+// 16 x 64 hidden activations stay in mma accumulator fragments, and the
+// accumulator layout of one layer is the operand layout of the next, so the
+// two hidden layers chain in registers.  Training runs the backward pass the
+// same way (the input gradient of layer 2 is one more mma against W2^T) and
+// forms the weight gradients as mma over the block's 64 rows, from
+// transposed BF16 tiles in shared memory.  Every sum runs in a fixed order
+// (fragments, then shuffles, then warps, then blocks in the Adam kernel), so
+// training is deterministic.
 #include <cmath>
+#include <cstdint>
 #include <vector>
+#include <cuda_bf16.h>
 #include "smd_ctx.cuh"
 #include "smd_polar.cuh"
 
 namespace smd {
 
-constexpr int MF = 20, MH = 64, MO = 3;
+constexpr int MF = 24, MH = 64, MO = 3;
 constexpr int OW1 = 0, OB1 = OW1 + MH * MF, OW2 = OB1 + MH, OB2 = OW2 + MH * MH, OW3 = OB2 + MH,
               OB3 = OW3 + MO * MH, MLP_NPARAM = OB3 + MO;
 constexpr float TARGET_SCALE = 1.0e5f;
-constexpr int MLP_THREADS = 256;
-constexpr int MLP_MAX_BLOCKS = 64;
+constexpr int KP = 32;                        // input width padded to two k-steps of 16
+constexpr int SX = KP + 8;                    // row stride (bf16) of 32-wide tiles
+constexpr int SW = MH + 8;                    // row stride (bf16) of 64-wide tiles
+constexpr int MLP_WARPS = 4, MLP_TB = 32 * MLP_WARPS;
+constexpr int MLP_CHUNK = 16 * MLP_WARPS;     // rows per block pass
+constexpr int MLP_MAX_BLOCKS = 128;
+constexpr int MLP_MAX_BATCH = 65536;
+static_assert(MF <= KP && MH % 16 == 0, "tile shapes");
 
 // ---------------------------------------------------------------------------
 // features and targets
@@ -58,31 +78,40 @@ __device__ __forceinline__ V3 hist_e(const double *ph, int n, int cnt, int k, in
     return v3(h[i], h[n + i], h[2 * n + i]);
 }
 
-// first-order guess: the previous dipoles moved by dl, the response of the
-// molecule's block to the change of the permanent field (k_blk_response;
-// dl = M^-1 E0 when nothing is stored)
-__device__ __forceinline__ V3 linear_guess(const double *ph, int n, int cnt, int i, const double *dl) {
-    const V3 r = v3(dl[i], dl[n + i], dl[2 * n + i]);
-    if (cnt < 1) return r;
-    return hist_p(ph, n, cnt, 1, i) + r;
+// extrapolated guess of the given order: the stored dipoles' extrapolation
+// plus dl, the molecule block's response to the permanent field's
+// difference of the same order (k_blk_response; dl = M^-1 E0 when nothing is
+// stored)
+__device__ __forceinline__ V3 linear_guess(const double *ph, int n, int cnt, int i, const double *dl, int order) {
+    return v3(dl[i] + hist_base_p(ph, n, cnt, order, i), dl[n + i] + hist_base_p(ph, n, cnt, order, n + i),
+              dl[2 * n + i] + hist_base_p(ph, n, cnt, order, 2 * (size_t)n + i));
 }
 
-// the F inputs of site i (one thread)
+// the F inputs of site i (one thread); dlp = M^-1 (E0(t-1) - E0(t-2))
 __device__ __forceinline__ void site_features(int i, int n, int cnt, const int *mol, const int *mol_off,
                                               const int *mol_atoms, const double4 *pos4, const double *frame,
-                                              const double *e0, const double *ph, float (&f)[MF]) {
+                                              const double *e0, const double *ph, const double *dlp,
+                                              float (&f)[MF]) {
     const V3 E = v3(e0[i], e0[n + i], e0[2 * n + i]);
     const V3 El = in_axes(frame, n, i, E);
     f[0] = (float)El.x; f[1] = (float)El.y; f[2] = (float)El.z;
     f[3] = (float)len(E);
-    for (int q = 4; q < 19; q++) f[q] = 0.f;
+#pragma unroll
+    for (int q = 4; q < MF - 1; q++) f[q] = 0.f;
+    if (cnt >= 1) {
+        const V3 dE = E - hist_e(ph, n, cnt, 1, i);
+        const V3 dEl = in_axes(frame, n, i, dE);
+        const V3 p1 = in_axes(frame, n, i, hist_p(ph, n, cnt, 1, i));
+        f[4] = (float)dEl.x; f[5] = (float)dEl.y; f[6] = (float)dEl.z;
+        f[13] = (float)p1.x; f[14] = (float)p1.y; f[15] = (float)p1.z;
+        f[22] = (float)len(dE);
+    }
     if (cnt >= 2) {
-        const V3 dE = in_axes(frame, n, i, E - hist_e(ph, n, cnt, 1, i));
-        const V3 p1 = hist_p(ph, n, cnt, 1, i);
-        const V3 pl = in_axes(frame, n, i, p1), dp = in_axes(frame, n, i, p1 - hist_p(ph, n, cnt, 2, i));
-        f[4] = (float)dE.x; f[5] = (float)dE.y; f[6] = (float)dE.z;
-        f[13] = (float)pl.x; f[14] = (float)pl.y; f[15] = (float)pl.z;
-        f[16] = (float)dp.x; f[17] = (float)dp.y; f[18] = (float)dp.z;
+        const V3 dp = hist_p(ph, n, cnt, 1, i) - hist_p(ph, n, cnt, 2, i);
+        const V3 dpl = in_axes(frame, n, i, dp);
+        const V3 mut = in_axes(frame, n, i, dp - v3(dlp[i], dlp[n + i], dlp[2 * n + i]));
+        f[16] = (float)dpl.x; f[17] = (float)dpl.y; f[18] = (float)dpl.z;
+        f[19] = (float)mut.x; f[20] = (float)mut.y; f[21] = (float)mut.z;
     }
     int q = 7;
     const int m = mol[i];
@@ -92,28 +121,29 @@ __device__ __forceinline__ void site_features(int i, int n, int cnt, const int *
         const V3 Ej = in_axes(frame, n, i, v3(e0[j], e0[n + j], e0[2 * n + j]));
         f[q++] = (float)Ej.x; f[q++] = (float)Ej.y; f[q++] = (float)Ej.z;
     }
-    f[19] = (int)pos4[i].w == 0 ? 0.f : 1.f;
+    f[MF - 1] = (int)pos4[i].w == 0 ? 0.f : 1.f;
 }
 
 __global__ void k_mlp_features(int n, const int *mol, const int *mol_off, const int *mol_atoms,
                                const double4 *pos4, const double *frame, const double *e0, const double *ph,
-                               const int *flags, float *x) {
+                               const double *dlp, const int *flags, float *x) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float f[MF];
-    site_features(i, n, flags[2], mol, mol_off, mol_atoms, pos4, frame, e0, ph, f);
+    site_features(i, n, flags[2], mol, mol_off, mol_atoms, pos4, frame, e0, ph, dlp, f);
     for (int k = 0; k < MF; k++) x[(size_t)i * MF + k] = f[k];
 }
 
 // appends (features, target) rows of the current configuration: the target
-// is what the network should add to the first-order guess (needs 2 stored steps)
+// is what the network should add to the extrapolated guess (needs 2 stored
+// steps)
 __global__ void k_mlp_collect(int n, const float *x, const double *frame, const double *p, const double *dl,
-                              const double *ph, const int *flags, float *data, long long row0) {
+                              const double *ph, const int *flags, float *data, long long row0, int order) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float *row = data + (size_t)(row0 + i) * (MF + MO);
     for (int k = 0; k < MF; k++) row[k] = x[(size_t)i * MF + k];
-    const V3 pl = linear_guess(ph, n, flags[2], i, dl);
+    const V3 pl = linear_guess(ph, n, flags[2], i, dl, order);
     const V3 dt = in_axes(frame, n, i, v3(p[i], p[n + i], p[2 * n + i]) - pl);
     row[MF] = (float)dt.x * TARGET_SCALE;
     row[MF + 1] = (float)dt.y * TARGET_SCALE;
@@ -123,7 +153,7 @@ __global__ void k_mlp_collect(int n, const float *x, const double *frame, const 
 // feature mean and 1/std over the collected rows (one block, fixed order)
 __global__ void k_mlp_norm(long long rows, const float *data, float *norm) {
     __shared__ double s1[MF][8], s2[MF][8];
-    const int f = threadIdx.x % MF, part = threadIdx.x / MF;  // 8 parts x 20 features = 160 threads
+    const int f = threadIdx.x % MF, part = threadIdx.x / MF;  // 8 parts x F features
     double a = 0, b = 0;
     if (part < 8)
         for (long long r = part; r < rows; r += 8) {
@@ -144,162 +174,416 @@ __global__ void k_mlp_norm(long long rows, const float *data, float *norm) {
 }
 
 // ---------------------------------------------------------------------------
-// forward / backward
+// tensor-core building blocks
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void mlp_forward(const float *W, const float *xn, float h1[MH], float y[MO]) {
-    for (int k = 0; k < MH; k++) {
-        float z = W[OB1 + k];
-        for (int f = 0; f < MF; f++) z = fmaf(W[OW1 + k * MF + f], xn[f], z);
-        h1[k] = tanhf(z);
-    }
-    for (int o = 0; o < MO; o++) y[o] = W[OB3 + o];
-    for (int j = 0; j < MH; j++) {
-        float z = W[OB2 + j];
-        for (int k = 0; k < MH; k++) z = fmaf(W[OW2 + j * MH + k], h1[k], z);
-        const float h2 = tanhf(z);
-        for (int o = 0; o < MO; o++) y[o] = fmaf(W[OW3 + o * MH + j], h2, y[o]);
-    }
+// two floats as one register of two BF16 (the lower index in the low half)
+__device__ __forceinline__ uint32_t pack2(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t *>(&v);
+}
+__device__ __forceinline__ uint32_t ld2(const __nv_bfloat16 *p) { return *reinterpret_cast<const uint32_t *>(p); }
+
+// D += A (16 x 16, row) B (16 x 8, col), BF16 operands, FP32 accumulators.
+// Fragments (g = lane / 4, t = lane % 4): a0 = A[g][2t..], a1 = A[g+8][2t..],
+// a2 = A[g][2t+8..], a3 = A[g+8][2t+8..]; b0 = B[2t..][g], b1 = B[2t+8..][g];
+// d0,d1 = D[g][2t, 2t+1], d2,d3 = D[g+8][2t, 2t+1].
+__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// Inference with MLP_ITPP threads per site, features computed in the same
-// kernel (one thread per site, while the block stages the weights).  Each
-// thread computes MH / MLP_ITPP hidden units of each layer; weights and
-// activations sit in shared memory in rows padded to a multiple of four
-// floats, read as float4 with four partial sums per unit (the two operands
-// of four multiply-adds in two 16-byte loads); the three outputs are summed
-// over the site's threads by shuffles.
-constexpr int MLP_ITPP = 4;
-constexpr int MLP_IBLOCK = 128;
-constexpr int MLP_ISITES = MLP_IBLOCK / MLP_ITPP;
-constexpr int HP = MH + 4;   // padded row of hidden activations / of W2
-static_assert(MF % 4 == 0 && MH % 4 == 0 && OW2 % 4 == 0, "float4 rows");
-__device__ __forceinline__ float dot4(const float4 *w, const float4 *h, int cnt4, float z) {
-    float z1 = 0.f, z2 = 0.f, z3 = 0.f;
-#pragma unroll
-    for (int k = 0; k < cnt4; k++) {
-        const float4 a = w[k], b = h[k];
-        z = fmaf(a.x, b.x, z); z1 = fmaf(a.y, b.y, z1); z2 = fmaf(a.z, b.z, z2); z3 = fmaf(a.w, b.w, z3);
-    }
-    return (z + z1) + (z2 + z3);
+// A fragments of 16-wide k-step ks from a row-major BF16 tile (stride ld)
+__device__ __forceinline__ void frag_a(uint32_t (&a)[4], const __nv_bfloat16 *tile, int ld, int ks, int g, int t) {
+    const __nv_bfloat16 *p = tile + g * ld + ks * 16 + 2 * t;
+    a[0] = ld2(p);
+    a[1] = ld2(p + 8 * ld);
+    a[2] = ld2(p + 8);
+    a[3] = ld2(p + 8 * ld + 8);
 }
-__global__ void __launch_bounds__(MLP_IBLOCK) k_mlp_infer(int n, const int *mol, const int *mol_off,
-                                                          const int *mol_atoms, const double4 *pos4,
-                                                          const double *e0, const float *norm, const float *Wg,
-                                                          const double *frame, const double *dl,
-                                                          const double *ph, const int *flags, double *p) {
-    __shared__ __align__(16) float sW1[MH * MF];
-    __shared__ __align__(16) float sW2[MH * HP];
-    __shared__ __align__(16) float sX[MLP_ISITES][MF];
-    __shared__ __align__(16) float sH1[MLP_ISITES][HP];
-    __shared__ float sB1[MH], sB2[MH], sW3[MO * MH], sB3[MO];
-    const int cnt = flags[2];
-    {
-        const float4 *g1 = (const float4 *)(Wg + OW1), *g2 = (const float4 *)(Wg + OW2);
-        for (int k = threadIdx.x; k < MH * MF / 4; k += blockDim.x) ((float4 *)sW1)[k] = g1[k];
-        for (int k = threadIdx.x; k < MH * MH / 4; k += blockDim.x) {
-            const int j = k / (MH / 4), c4 = k - j * (MH / 4);
-            *(float4 *)&sW2[j * HP + 4 * c4] = g2[k];
+// A fragments of k-step kk taken from accumulator fragments of the previous
+// layer (n-tiles 2 kk and 2 kk + 1): the layouts coincide
+__device__ __forceinline__ void frag_chain(uint32_t (&a)[4], const float (&h)[8][4], int kk) {
+    a[0] = pack2(h[2 * kk][0], h[2 * kk][1]);
+    a[1] = pack2(h[2 * kk][2], h[2 * kk][3]);
+    a[2] = pack2(h[2 * kk + 1][0], h[2 * kk + 1][1]);
+    a[3] = pack2(h[2 * kk + 1][2], h[2 * kk + 1][3]);
+}
+
+// weights in shared memory: W1[j][f] (f zero-padded to KP), W2[j][k],
+// FP32 biases and output layer
+struct MlpW {
+    __nv_bfloat16 w1[MH * SX];
+    __nv_bfloat16 w2[MH * SW];
+    float b1[MH], b2[MH], w3[MO * MH], b3[4];
+};
+
+// every thread of the block takes part; w2t (optional): W2^T[k][j]
+__device__ __forceinline__ void load_weights(MlpW &S, const float *W, __nv_bfloat16 *w2t) {
+    for (int k = threadIdx.x; k < MH * KP; k += blockDim.x) {
+        const int j = k / KP, f = k - j * KP;
+        S.w1[j * SX + f] = __float2bfloat16_rn(f < MF ? W[OW1 + j * MF + f] : 0.f);
+    }
+    for (int k = threadIdx.x; k < MH * MH; k += blockDim.x) {
+        const int j = k / MH, q = k - j * MH;
+        const __nv_bfloat16 v = __float2bfloat16_rn(W[OW2 + k]);
+        S.w2[j * SW + q] = v;
+        if (w2t) w2t[q * SW + j] = v;
+    }
+    for (int k = threadIdx.x; k < MH; k += blockDim.x) { S.b1[k] = W[OB1 + k]; S.b2[k] = W[OB2 + k]; }
+    for (int k = threadIdx.x; k < MO * MH; k += blockDim.x) S.w3[k] = W[OW3 + k];
+    if (threadIdx.x < MO) S.b3[threadIdx.x] = W[OB3 + threadIdx.x];
+}
+
+// the two hidden layers of one warp's 16 rows (normalised BF16 inputs in
+// xs, row stride SX): h1, h2 after tanh, as accumulator fragments
+__device__ __forceinline__ void warp_hidden(const MlpW &S, const __nv_bfloat16 *xs, float (&h1)[8][4],
+                                            float (&h2)[8][4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+        const float b0 = S.b1[nt * 8 + 2 * t], b1 = S.b1[nt * 8 + 2 * t + 1];
+        h1[nt][0] = b0; h1[nt][1] = b1; h1[nt][2] = b0; h1[nt][3] = b1;
+    }
+#pragma unroll
+    for (int ks = 0; ks < KP / 16; ks++) {
+        uint32_t a[4];
+        frag_a(a, xs, SX, ks, g, t);
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const __nv_bfloat16 *b = S.w1 + (nt * 8 + g) * SX + ks * 16 + 2 * t;
+            mma16816(h1[nt], a, ld2(b), ld2(b + 8));
         }
     }
-    for (int k = threadIdx.x; k < MO * MH; k += blockDim.x) sW3[k] = Wg[OW3 + k];
-    for (int k = threadIdx.x; k < MH; k += blockDim.x) { sB1[k] = Wg[OB1 + k]; sB2[k] = Wg[OB2 + k]; }
-    if (threadIdx.x < MO) sB3[threadIdx.x] = Wg[OB3 + threadIdx.x];
-    if (threadIdx.x < MLP_ISITES) {
-        const int is = blockIdx.x * MLP_ISITES + threadIdx.x;
-        float f[MF];
-        if (is < n) site_features(is, n, cnt, mol, mol_off, mol_atoms, pos4, frame, e0, ph, f);
 #pragma unroll
-        for (int k = 0; k < MF; k++) sX[threadIdx.x][k] = is < n ? (f[k] - norm[k]) * norm[MF + k] : 0.f;
+    for (int nt = 0; nt < 8; nt++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) h1[nt][q] = tanhf(h1[nt][q]);
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+        const float b0 = S.b2[nt * 8 + 2 * t], b1 = S.b2[nt * 8 + 2 * t + 1];
+        h2[nt][0] = b0; h2[nt][1] = b1; h2[nt][2] = b0; h2[nt][3] = b1;
     }
-    const int ls = threadIdx.x / MLP_ITPP, t = threadIdx.x % MLP_ITPP;
-    const int i = blockIdx.x * MLP_ISITES + ls;
-    const bool own = i < n;
-    __syncthreads();
-    for (int j = t; j < MH; j += MLP_ITPP)
-        sH1[ls][j] = tanhf(dot4((const float4 *)&sW1[j * MF], (const float4 *)sX[ls], MF / 4, sB1[j]));
-    __syncthreads();
-    float y0 = 0.f, y1 = 0.f, y2 = 0.f;
-    for (int j = t; j < MH; j += MLP_ITPP) {
-        const float h2 = tanhf(dot4((const float4 *)&sW2[j * HP], (const float4 *)sH1[ls], MH / 4, sB2[j]));
-        y0 = fmaf(sW3[j], h2, y0);
-        y1 = fmaf(sW3[MH + j], h2, y1);
-        y2 = fmaf(sW3[2 * MH + j], h2, y2);
+#pragma unroll
+    for (int kk = 0; kk < MH / 16; kk++) {
+        uint32_t a[4];
+        frag_chain(a, h1, kk);
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const __nv_bfloat16 *b = S.w2 + (nt * 8 + g) * SW + kk * 16 + 2 * t;
+            mma16816(h2[nt], a, ld2(b), ld2(b + 8));
+        }
     }
-    y0 = group_sum<MLP_ITPP>(y0) + sB3[0];
-    y1 = group_sum<MLP_ITPP>(y1) + sB3[1];
-    y2 = group_sum<MLP_ITPP>(y2) + sB3[2];
-    if (!own || t != 0) return;
-    V3 g = linear_guess(ph, n, cnt, i, dl);
-    if (cnt >= 2) {
-        const V3 u = axis(frame, n, i, 0), v = axis(frame, n, i, 1), w = axis(frame, n, i, 2);
-        g = g + (y0 / TARGET_SCALE) * u + (y1 / TARGET_SCALE) * v + (y2 / TARGET_SCALE) * w;
-    }
-    p[i] = g.x;
-    p[n + i] = g.y;
-    p[2 * n + i] = g.z;
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) h2[nt][q] = tanhf(h2[nt][q]);
 }
 
-// gradient of the batch loss (1/(3B)) sum (y - t)^2 ; rows idx[r0 .. r0+B)
-__device__ __forceinline__ void acc_grad(float *g, int k, float v) {
-    v = warp_sum(v);
-    if ((threadIdx.x & 31) == 0) atomicAdd(&g[k], v);
-}
-
-__global__ void __launch_bounds__(MLP_THREADS) k_mlp_grad(long long r0, int batch, long long rows,
-                                                          const unsigned int *perm, const float *data,
-                                                          const float *norm, const float *Wg, float *part,
-                                                          float *loss_part) {
-    extern __shared__ float sm[];
-    float *W = sm, *G = sm + MLP_NPARAM;
-    for (int k = threadIdx.x; k < MLP_NPARAM; k += blockDim.x) { W[k] = Wg[k]; G[k] = 0.f; }
-    __syncthreads();
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = r < batch;
-    float xn[MF], h1[MH], dh1[MH], y[MO], dy[MO];
-    float loss = 0.f;
-    long long row = valid ? (long long)perm[(r0 + r) % rows] : 0;
-    const float *d = data + row * (MF + MO);
-    for (int f = 0; f < MF; f++) xn[f] = valid ? (d[f] - norm[f]) * norm[MF + f] : 0.f;
-    mlp_forward(W, xn, h1, y);
-    const float scale = 2.f / (3.f * (float)batch);
+// output layer in FP32: y of rows g (lo) and g + 8 (hi), in every lane of
+// the row's quad
+__device__ __forceinline__ void warp_out(const MlpW &S, const float (&h2)[8][4], float (&lo)[MO], float (&hi)[MO]) {
+    const int t = threadIdx.x & 3;
+#pragma unroll
     for (int o = 0; o < MO; o++) {
-        const float e = valid ? y[o] - d[MF + o] : 0.f;
-        loss += e * e;
-        dy[o] = scale * e;
-        acc_grad(G, OB3 + o, dy[o]);
+        float a = 0.f, b = 0.f;
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const float w0 = S.w3[o * MH + nt * 8 + 2 * t], w1 = S.w3[o * MH + nt * 8 + 2 * t + 1];
+            a = fmaf(w0, h2[nt][0], fmaf(w1, h2[nt][1], a));
+            b = fmaf(w0, h2[nt][2], fmaf(w1, h2[nt][3], b));
+        }
+        a += __shfl_xor_sync(0xffffffffu, a, 1);
+        a += __shfl_xor_sync(0xffffffffu, a, 2);
+        b += __shfl_xor_sync(0xffffffffu, b, 1);
+        b += __shfl_xor_sync(0xffffffffu, b, 2);
+        lo[o] = a + S.b3[o];
+        hi[o] = b + S.b3[o];
     }
-    for (int k = 0; k < MH; k++) dh1[k] = 0.f;
-    for (int j = 0; j < MH; j++) {
-        float z = W[OB2 + j];
-        for (int k = 0; k < MH; k++) z = fmaf(W[OW2 + j * MH + k], h1[k], z);
-        const float h2 = tanhf(z);
-        float dh2 = 0.f;
+}
+
+// sum over the 8 row groups of a warp (lanes with equal t)
+__device__ __forceinline__ float rows_sum(float v) {
+    v += __shfl_xor_sync(0xffffffffu, v, 4);
+    v += __shfl_xor_sync(0xffffffffu, v, 8);
+    v += __shfl_xor_sync(0xffffffffu, v, 16);
+    return v;
+}
+
+// normalised input f of a raw feature row as BF16 (zero past the F inputs)
+__device__ __forceinline__ __nv_bfloat16 norm_in(const float *row, const float *norm, int f, bool ok) {
+    return __float2bfloat16_rn(ok && f < MF ? (row[f] - norm[f]) * norm[MF + f] : 0.f);
+}
+
+// ---------------------------------------------------------------------------
+// inference: the start dipoles of the solve
+// ---------------------------------------------------------------------------
+// One block = 4 warps = 64 sites.  The first 64 threads compute one site's
+// features each into a BF16 tile, the warps run the network on 16 sites
+// each, and the same 64 threads add the correction to the extrapolated guess.
+__global__ void __launch_bounds__(MLP_TB) k_mlp_infer(int n, const int *mol, const int *mol_off,
+                                                      const int *mol_atoms, const double4 *pos4, const double *e0,
+                                                      const float *norm, const float *Wg, const double *frame,
+                                                      const double *dl, const double *dlp, const double *ph,
+                                                      const int *flags, double *p, int order) {
+    __shared__ __align__(16) MlpW S;
+    __shared__ __align__(16) __nv_bfloat16 sX[MLP_CHUNK * SX];
+    __shared__ float sY[MLP_CHUNK][MO];
+    load_weights(S, Wg, nullptr);
+    const int cnt = flags[2];
+    const int i = blockIdx.x * MLP_CHUNK + threadIdx.x;
+    if (threadIdx.x < MLP_CHUNK) {
+        float f[MF];
+        if (i < n) site_features(i, n, cnt, mol, mol_off, mol_atoms, pos4, frame, e0, ph, dlp, f);
+#pragma unroll
+        for (int k = 0; k < KP; k++) {
+            float v = 0.f;
+            if (k < MF && i < n) v = (f[k < MF ? k : 0] - norm[k < MF ? k : 0]) * norm[MF + (k < MF ? k : 0)];
+            sX[threadIdx.x * SX + k] = __float2bfloat16_rn(v);
+        }
+    }
+    __syncthreads();
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    float h1[8][4], h2[8][4], lo[MO], hi[MO];
+    warp_hidden(S, sX + 16 * w * SX, h1, h2);
+    warp_out(S, h2, lo, hi);
+    if (t == 0)
         for (int o = 0; o < MO; o++) {
-            dh2 = fmaf(W[OW3 + o * MH + j], dy[o], dh2);
-            acc_grad(G, OW3 + o * MH + j, dy[o] * h2);
+            sY[16 * w + g][o] = lo[o];
+            sY[16 * w + g + 8][o] = hi[o];
         }
-        const float dz2 = dh2 * (1.f - h2 * h2);
-        acc_grad(G, OB2 + j, dz2);
-        for (int k = 0; k < MH; k++) {
-            acc_grad(G, OW2 + j * MH + k, dz2 * h1[k]);
-            dh1[k] = fmaf(W[OW2 + j * MH + k], dz2, dh1[k]);
-        }
+    __syncthreads();
+    if (threadIdx.x >= MLP_CHUNK || i >= n) return;
+    V3 gs = linear_guess(ph, n, cnt, i, dl, order);
+    if (cnt >= 2) {
+        const V3 u = axis(frame, n, i, 0), v = axis(frame, n, i, 1), ww = axis(frame, n, i, 2);
+        const float *y = sY[threadIdx.x];
+        gs = gs + (y[0] / TARGET_SCALE) * u + (y[1] / TARGET_SCALE) * v + (y[2] / TARGET_SCALE) * ww;
     }
-    for (int k = 0; k < MH; k++) {
-        const float dz1 = dh1[k] * (1.f - h1[k] * h1[k]);
-        acc_grad(G, OB1 + k, dz1);
-        for (int f = 0; f < MF; f++) acc_grad(G, OW1 + k * MF + f, dz1 * xn[f]);
+    p[i] = gs.x;
+    p[n + i] = gs.y;
+    p[2 * n + i] = gs.z;
+}
+
+// network output for given raw feature rows (the checker's entry)
+__global__ void __launch_bounds__(MLP_TB) k_mlp_eval(int rows, const float *x, const float *norm, const float *Wg,
+                                                     float *y) {
+    __shared__ __align__(16) MlpW S;
+    __shared__ __align__(16) __nv_bfloat16 sX[MLP_CHUNK * SX];
+    load_weights(S, Wg, nullptr);
+    const int r0 = blockIdx.x * MLP_CHUNK;
+    for (int k = threadIdx.x; k < MLP_CHUNK * KP; k += blockDim.x) {
+        const int r = k / KP, f = k - r * KP;
+        const bool ok = r0 + r < rows;
+        sX[r * SX + f] = norm_in(x + (size_t)(ok ? r0 + r : 0) * MF, norm, f, ok);
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < MLP_NPARAM; k += blockDim.x) part[(size_t)blockIdx.x * MLP_NPARAM + k] = G[k];
-    loss = warp_sum(loss);
-    __shared__ float s_l[MLP_THREADS / 32];
-    if ((threadIdx.x & 31) == 0) s_l[threadIdx.x >> 5] = loss;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    float h1[8][4], h2[8][4], lo[MO], hi[MO];
+    warp_hidden(S, sX + 16 * w * SX, h1, h2);
+    warp_out(S, h2, lo, hi);
+    if (t != 0) return;
+    const int ra = r0 + 16 * w + g, rb = ra + 8;
+    for (int o = 0; o < MO; o++) {
+        if (ra < rows) y[(size_t)ra * MO + o] = lo[o];
+        if (rb < rows) y[(size_t)rb * MO + o] = hi[o];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// training: gradient of the batch loss (1/(3B)) sum (y - t)^2
+// ---------------------------------------------------------------------------
+// Block b takes rows [b per, (b + 1) per) of the batch (per a multiple of 64)
+// in passes of 64 rows.  Per pass each warp runs the forward and backward of
+// its 16 rows in registers and writes the BF16 tiles the weight gradients
+// need transposed (rows innermost) into shared memory; then warp w forms the
+// gradient rows 16 w .. 16 w + 15 of W2 (64 x 64) and of W1 (64 x 32) as
+// mma over the 64 rows, accumulating across passes in registers.  Bias and
+// output-layer gradients are column sums (shuffles over a warp's rows, then
+// per-warp slots in shared memory).  The block writes its partial gradient
+// and loss; k_mlp_adam adds the blocks in order.
+struct GradSmem {
+    MlpW S;
+    __nv_bfloat16 w2t[MH * SW];        // W2^T[k][j]
+    __nv_bfloat16 x[MLP_CHUNK * SX];   // normalised inputs [row][f]
+    __nv_bfloat16 xt[KP * SW];         // [f][row]
+    __nv_bfloat16 h1t[MH * SW];        // [k][row]
+    __nv_bfloat16 d2t[MH * SW];        // dL/dz2 [j][row]
+    __nv_bfloat16 d1t[MH * SW];        // dL/dz1 [k][row]
+    float tgt[MLP_CHUNK][4];           // targets, [3] = 1 for a row of the batch
+    float acc[MLP_WARPS][2 * MH + MO * MH + 4];   // db1, db2, dW3, db3 per warp
+    float loss[MLP_WARPS];
+};
+constexpr int GA_B1 = 0, GA_B2 = MH, GA_W3 = 2 * MH, GA_B3 = 2 * MH + MO * MH, GA_N = 2 * MH + MO * MH + 4;
+
+__global__ void __launch_bounds__(MLP_TB) k_mlp_grad(long long r0, int batch, int per, long long rows,
+                                                     const unsigned int *perm, const float *data, const float *norm,
+                                                     const float *Wg, float *part, float *loss_part) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    GradSmem &G = *reinterpret_cast<GradSmem *>(smraw);
+    load_weights(G.S, Wg, G.w2t);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    for (int k = lane; k < GA_N; k += 32) G.acc[w][k] = 0.f;
+    float lsum = 0.f;
+    float gW2[8][4], gW1[KP / 8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) gW2[nt][q] = 0.f;
+#pragma unroll
+    for (int nt = 0; nt < KP / 8; nt++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) gW1[nt][q] = 0.f;
+    const float scale = 2.f / (3.f * (float)batch);
+    const int b0 = blockIdx.x * per, b1 = min(batch, b0 + per);
+    for (int c0 = b0; c0 < b1; c0 += MLP_CHUNK) {
+        __syncthreads();   // the previous pass's tiles have been read
+        if (threadIdx.x < MLP_CHUNK) {
+            const int r = c0 + threadIdx.x;
+            const bool ok = r < b1;
+            const float *d = data + (ok ? (size_t)perm[(r0 + r) % rows] : 0) * (MF + MO);
+            for (int f = 0; f < KP; f++) {
+                const __nv_bfloat16 v = norm_in(d, norm, f, ok);
+                G.x[threadIdx.x * SX + f] = v;
+                G.xt[f * SW + threadIdx.x] = v;
+            }
+            for (int o = 0; o < MO; o++) G.tgt[threadIdx.x][o] = ok ? d[MF + o] : 0.f;
+            G.tgt[threadIdx.x][3] = ok ? 1.f : 0.f;
+        }
+        __syncthreads();
+        const int ra = 16 * w + g, rb = ra + 8;   // this lane's rows in the pass
+        float h1[8][4], h2[8][4], lo[MO], hi[MO];
+        warp_hidden(G.S, G.x + 16 * w * SX, h1, h2);
+        warp_out(G.S, h2, lo, hi);
+        float da[MO], db[MO];   // dL/dy of rows ra, rb
+        for (int o = 0; o < MO; o++) {
+            const float ea = G.tgt[ra][3] != 0.f ? lo[o] - G.tgt[ra][o] : 0.f;
+            const float eb = G.tgt[rb][3] != 0.f ? hi[o] - G.tgt[rb][o] : 0.f;
+            if (t == 0) lsum += ea * ea + eb * eb;
+            da[o] = scale * ea;
+            db[o] = scale * eb;
+        }
+        // output layer: dW3[o][j] = sum_rows dy_o h2_j, db3 = sum_rows dy
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++)
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const int col = nt * 8 + 2 * t + q;
+                for (int o = 0; o < MO; o++) {
+                    const float v = rows_sum(da[o] * h2[nt][q] + db[o] * h2[nt][q + 2]);
+                    if (g == 0) G.acc[w][GA_W3 + o * MH + col] += v;
+                }
+            }
+        for (int o = 0; o < MO; o++) {
+            const float v = rows_sum(da[o] + db[o]);
+            if (lane == 0) G.acc[w][GA_B3 + o] += v;
+        }
+        // dz2 = (W3^T dy) (1 - h2^2), in h2's fragments
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int col = nt * 8 + 2 * t + (q & 1);
+                float s = 0.f;
+                for (int o = 0; o < MO; o++) s = fmaf(G.S.w3[o * MH + col], q < 2 ? da[o] : db[o], s);
+                h2[nt][q] = s * (1.f - h2[nt][q] * h2[nt][q]);
+            }
+        // dz1 = (W2^T dz2) (1 - h1^2): one more mma per tile against W2^T
+        float d1[8][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) d1[nt][q] = 0.f;
+#pragma unroll
+        for (int kk = 0; kk < MH / 16; kk++) {
+            uint32_t a[4];
+            frag_chain(a, h2, kk);
+#pragma unroll
+            for (int nt = 0; nt < 8; nt++) {
+                const __nv_bfloat16 *b = G.w2t + (nt * 8 + g) * SW + kk * 16 + 2 * t;
+                mma16816(d1[nt], a, ld2(b), ld2(b + 8));
+            }
+        }
+        // bias gradients, and the transposed tiles of dz2, h1, dz1
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++)
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const int col = nt * 8 + 2 * t + q;
+                const float e1a = d1[nt][q] * (1.f - h1[nt][q] * h1[nt][q]);
+                const float e1b = d1[nt][q + 2] * (1.f - h1[nt][q + 2] * h1[nt][q + 2]);
+                const float s2 = rows_sum(h2[nt][q] + h2[nt][q + 2]);
+                const float s1 = rows_sum(e1a + e1b);
+                if (g == 0) {
+                    G.acc[w][GA_B2 + col] += s2;
+                    G.acc[w][GA_B1 + col] += s1;
+                }
+                G.d2t[col * SW + ra] = __float2bfloat16_rn(h2[nt][q]);
+                G.d2t[col * SW + rb] = __float2bfloat16_rn(h2[nt][q + 2]);
+                G.h1t[col * SW + ra] = __float2bfloat16_rn(h1[nt][q]);
+                G.h1t[col * SW + rb] = __float2bfloat16_rn(h1[nt][q + 2]);
+                G.d1t[col * SW + ra] = __float2bfloat16_rn(e1a);
+                G.d1t[col * SW + rb] = __float2bfloat16_rn(e1b);
+            }
+        __syncthreads();
+        // weight gradients over the pass's 64 rows: dW2 = dz2^T h1, dW1 = dz1^T x
+#pragma unroll
+        for (int ks = 0; ks < MLP_CHUNK / 16; ks++) {
+            uint32_t a[4];
+            frag_a(a, G.d2t + 16 * w * SW, SW, ks, g, t);
+#pragma unroll
+            for (int nt = 0; nt < 8; nt++) {
+                const __nv_bfloat16 *b = G.h1t + (nt * 8 + g) * SW + ks * 16 + 2 * t;
+                mma16816(gW2[nt], a, ld2(b), ld2(b + 8));
+            }
+            frag_a(a, G.d1t + 16 * w * SW, SW, ks, g, t);
+#pragma unroll
+            for (int nt = 0; nt < KP / 8; nt++) {
+                const __nv_bfloat16 *b = G.xt + (nt * 8 + g) * SW + ks * 16 + 2 * t;
+                mma16816(gW1[nt], a, ld2(b), ld2(b + 8));
+            }
+        }
+    }
+    // the block's partial gradient
+    float *out = part + (size_t)blockIdx.x * MLP_NPARAM;
+    const int ja = 16 * w + g, jb = ja + 8;
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+        const int k = nt * 8 + 2 * t;
+        out[OW2 + ja * MH + k] = gW2[nt][0];
+        out[OW2 + ja * MH + k + 1] = gW2[nt][1];
+        out[OW2 + jb * MH + k] = gW2[nt][2];
+        out[OW2 + jb * MH + k + 1] = gW2[nt][3];
+    }
+#pragma unroll
+    for (int nt = 0; nt < KP / 8; nt++) {
+        const int f = nt * 8 + 2 * t;
+        if (f < MF) {
+            out[OW1 + ja * MF + f] = gW1[nt][0];
+            out[OW1 + jb * MF + f] = gW1[nt][2];
+        }
+        if (f + 1 < MF) {
+            out[OW1 + ja * MF + f + 1] = gW1[nt][1];
+            out[OW1 + jb * MF + f + 1] = gW1[nt][3];
+        }
+    }
+    lsum = rows_sum(lsum);
+    if (lane == 0) G.loss[w] = lsum;
     __syncthreads();
+    for (int k = threadIdx.x; k < GA_B3 + MO; k += blockDim.x) {
+        float s = 0.f;
+        for (int q = 0; q < MLP_WARPS; q++) s += G.acc[q][k];
+        if (k < GA_B2) out[OB1 + k] = s;
+        else if (k < GA_W3) out[OB2 + k - GA_B2] = s;
+        else if (k < GA_B3) out[OW3 + k - GA_W3] = s;
+        else out[OB3 + k - GA_B3] = s;
+    }
     if (threadIdx.x == 0) {
-        float t = 0;
-        for (int q = 0; q < MLP_THREADS / 32; q++) t += s_l[q];
-        loss_part[blockIdx.x] = t / (3.f * (float)batch);
+        float s = 0.f;
+        for (int q = 0; q < MLP_WARPS; q++) s += G.loss[q];
+        loss_part[blockIdx.x] = s / (3.f * (float)batch);
     }
 }
 
@@ -321,27 +605,35 @@ __global__ void k_mlp_adam(int nblocks, const float *part, float *W, float *m, f
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
+// the blocks' responses the guess and the features use: dl (the base order's
+// field difference) and dlp (the last step's)
+static void responses(Ctx &c, int order) {
+    launch_blk_response(c, guess_response(c), order, guess_response_prev(c));
+}
+
 void launch_mlp_features(Ctx &c) {
+    responses(c, c.mlp_base);
     k_mlp_features<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.mol, c.mol_off, c.mol_atoms, c.pos4, c.frame,
-                                                            c.e0, c.phist, c.flags, c.mlp_x);
+                                                            c.e0, c.phist, guess_response_prev(c), c.flags,
+                                                            c.mlp_x);
 }
 
 void launch_mlp_guess(Ctx &c) {
-    double *dl = guess_response(c);
-    // with the molecule blocks the block kernel has just formed it
-    if (!(c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk)) launch_blk_response(c, dl);
-    k_mlp_infer<<<(c.n + MLP_ISITES - 1) / MLP_ISITES, MLP_IBLOCK, 0, c.stream>>>(
-        c.n, c.mol, c.mol_off, c.mol_atoms, c.pos4, c.e0, c.mlp_norm, c.mlp_w, c.frame, dl, c.phist, c.flags,
-        c.pind);
+    // with the molecule blocks the block kernel has just formed both
+    if (!(c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk)) responses(c, c.mlp_base);
+    k_mlp_infer<<<(c.n + MLP_CHUNK - 1) / MLP_CHUNK, MLP_TB, 0, c.stream>>>(
+        c.n, c.mol, c.mol_off, c.mol_atoms, c.pos4, c.e0, c.mlp_norm, c.mlp_w, c.frame, guess_response(c),
+        guess_response_prev(c), c.phist, c.flags, c.pind, c.mlp_base);
 }
 
-// The first-order guess alone, p = p(t-1) + M^-1 (E0(t) - E0(t-1)) (M^-1 E0
-// with no stored step): the learned guess with the network's correction left
-// out, the baseline that shows what the network adds.
-__global__ void k_first_order_guess(int n, const double *dl, const double *ph, const int *flags, double *p) {
+// The extrapolated guess alone (order 1: p = p(t-1) + M^-1 (E0(t) - E0(t-1)),
+// M^-1 E0 with no stored step): the learned guess with the network's
+// correction left out, the baseline that shows what the network adds.
+__global__ void k_first_order_guess(int n, const double *dl, const double *ph, const int *flags, double *p,
+                                    int order) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const V3 g = linear_guess(ph, n, flags[2], i, dl);
+    const V3 g = linear_guess(ph, n, flags[2], i, dl, order);
     p[i] = g.x;
     p[n + i] = g.y;
     p[2 * n + i] = g.z;
@@ -349,9 +641,10 @@ __global__ void k_first_order_guess(int n, const double *dl, const double *ph, c
 
 void launch_first_order_guess(Ctx &c) {
     double *dl = guess_response(c);
+    const int order = guess_order(c);
     // with the molecule blocks the block kernel has just formed it
-    if (!(c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk)) launch_blk_response(c, dl);
-    k_first_order_guess<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, dl, c.phist, c.flags, c.pind);
+    if (!(c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk)) launch_blk_response(c, dl, order, nullptr);
+    k_first_order_guess<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, dl, c.phist, c.flags, c.pind, order);
 }
 
 int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed) {
@@ -361,10 +654,13 @@ int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed) {
         return cudaMalloc((void **)p, (cnt ? cnt : 1) * sizeof(**p)) == cudaSuccess;
     };
     if (!al(&c.mlp_w, MLP_NPARAM) || !al(&c.mlp_m, MLP_NPARAM) || !al(&c.mlp_v, MLP_NPARAM) ||
-        // block partials, per-block losses, then room for one gradient
-        !al(&c.mlp_part, (size_t)(MLP_MAX_BLOCKS + 1) * MLP_NPARAM + MLP_MAX_BLOCKS) ||
+        // block partials, per-block losses
+        !al(&c.mlp_part, (size_t)MLP_MAX_BLOCKS * MLP_NPARAM + MLP_MAX_BLOCKS) ||
         !al(&c.mlp_norm, 2 * MF) || !al(&c.mlp_x, (size_t)c.n * MF) ||
         !al(&c.mlp_data, (size_t)cap_rows * (MF + MO)))
+        return SMD_ERR_CUDA;
+    if (cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GradSmem)) !=
+        cudaSuccess)
         return SMD_ERR_CUDA;
     // Glorot-uniform weights from a 32-bit LCG (seeded), zero biases
     std::vector<float> w(MLP_NPARAM, 0.f);
@@ -390,46 +686,61 @@ int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed) {
 }
 
 void launch_mlp_collect(Ctx &c) {
-    launch_mlp_features(c);
-    double *dl = guess_response(c);
-    launch_blk_response(c, dl);   // the blocks of the solve that produced p
-    k_mlp_collect<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.mlp_x, c.frame, c.pind, dl, c.phist, c.flags,
-                                                           c.mlp_data, c.mlp_rows);
+    launch_mlp_features(c);   // also the responses, from the blocks of the solve that produced p
+    k_mlp_collect<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.mlp_x, c.frame, c.pind, guess_response(c),
+                                                           c.phist, c.flags, c.mlp_data, c.mlp_rows, c.mlp_base);
 }
 
 void launch_mlp_norm(Ctx &c) {
-    k_mlp_norm<<<1, 160, 0, c.stream>>>(c.mlp_rows, c.mlp_data, c.mlp_norm);
+    k_mlp_norm<<<1, 8 * MF, 0, c.stream>>>(c.mlp_rows, c.mlp_data, c.mlp_norm);
 }
 
-// one optimisation step over rows perm[r0 .. r0 + batch); grad_only: write
-// the batch gradient into grad_out instead of updating the weights
+// blocks of one optimisation step over a batch, and the rows each takes (a
+// multiple of the 64-row pass)
+static int step_blocks(int batch, int &per) {
+    int nb = (batch + MLP_CHUNK - 1) / MLP_CHUNK;
+    if (nb > MLP_MAX_BLOCKS) nb = MLP_MAX_BLOCKS;
+    per = (batch + nb - 1) / nb;
+    per = (per + MLP_CHUNK - 1) / MLP_CHUNK * MLP_CHUNK;
+    return (batch + per - 1) / per;
+}
+
+// one optimisation step over rows perm[r0 .. r0 + batch); grad_out: write
+// the batch gradient there instead of updating the weights
 void launch_mlp_step(Ctx &c, const unsigned int *perm, long long r0, int batch, float lr, float *grad_out) {
-    const int nb = (batch + MLP_THREADS - 1) / MLP_THREADS;
-    const size_t smem = 2 * MLP_NPARAM * sizeof(float);
-    k_mlp_grad<<<nb, MLP_THREADS, smem, c.stream>>>(r0, batch, c.mlp_rows, perm, c.mlp_data, c.mlp_norm,
-                                                    c.mlp_w, c.mlp_part,
-                                                    c.mlp_part + (size_t)MLP_MAX_BLOCKS * MLP_NPARAM);
+    int per = 0;
+    const int nb = step_blocks(batch, per);
+    k_mlp_grad<<<nb, MLP_TB, sizeof(GradSmem), c.stream>>>(r0, batch, per, c.mlp_rows, perm, c.mlp_data,
+                                                          c.mlp_norm, c.mlp_w, c.mlp_part,
+                                                          c.mlp_part + (size_t)MLP_MAX_BLOCKS * MLP_NPARAM);
     if (!grad_out) c.mlp_t++;
     k_mlp_adam<<<(MLP_NPARAM + 255) / 256, 256, 0, c.stream>>>(nb, c.mlp_part, c.mlp_w, c.mlp_m, c.mlp_v, lr,
                                                                c.mlp_t, grad_out);
 }
 
-int mlp_nparam() { return MLP_NPARAM; }
-int mlp_nfeat() { return MF; }
-int mlp_max_batch() { return MLP_MAX_BLOCKS * MLP_THREADS; }
-
-// network output for given feature rows (checker entry: x raw features)
-__global__ void k_mlp_eval(int rows, const float *x, const float *norm, const float *W, float *y) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= rows) return;
-    float xn[MF], h1[MH], yy[MO];
-    for (int f = 0; f < MF; f++) xn[f] = (x[(size_t)r * MF + f] - norm[f]) * norm[MF + f];
-    mlp_forward(W, xn, h1, yy);
-    for (int o = 0; o < MO; o++) y[(size_t)r * MO + o] = yy[o];
+// mean-squared error of the rows perm[0 .. batch) (weights unchanged)
+int mlp_batch_loss(Ctx &c, const unsigned int *perm, int batch, double *loss) {
+    int per = 0;
+    const int nb = step_blocks(batch, per);
+    float *lpart = c.mlp_part + (size_t)MLP_MAX_BLOCKS * MLP_NPARAM;
+    k_mlp_grad<<<nb, MLP_TB, sizeof(GradSmem), c.stream>>>(0, batch, per, c.mlp_rows, perm, c.mlp_data,
+                                                          c.mlp_norm, c.mlp_w, c.mlp_part, lpart);
+    std::vector<float> lp(nb);
+    if (cudaMemcpyAsync(lp.data(), lpart, nb * sizeof(float), cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+        cudaStreamSynchronize(c.stream) != cudaSuccess)
+        return SMD_ERR_CUDA;
+    double t = 0;
+    for (int q = 0; q < nb; q++) t += lp[q];
+    *loss = t;
+    return 0;
 }
 
+int mlp_nparam() { return MLP_NPARAM; }
+int mlp_nfeat() { return MF; }
+int mlp_max_batch() { return MLP_MAX_BATCH; }
+
 void launch_mlp_eval(Ctx &c, int rows, const float *x, float *y) {
-    k_mlp_eval<<<(rows + 127) / 128, 128, 0, c.stream>>>(rows, x, c.mlp_norm, c.mlp_w, y);
+    k_mlp_eval<<<(rows + MLP_CHUNK - 1) / MLP_CHUNK, MLP_TB, 0, c.stream>>>(rows, x, c.mlp_norm, c.mlp_w, y);
 }
 
 }  // namespace smd

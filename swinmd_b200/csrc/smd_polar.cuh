@@ -19,6 +19,28 @@ __device__ __forceinline__ V3 crs(V3 a, V3 b) {
 }
 __device__ __forceinline__ double len(V3 a) { return sqrt(dot(a, a)); }
 
+// Extrapolation over the dipole history ring ph ([4][6][N]: p x y z, E0 x y
+// z per stored step, slot (count - k) & 3 for step t - k): with k = min(order,
+// cnt) steps and the alternating binomial weights w_j (1; 2, -1; 3, -3, 1),
+// the guess is sum_j w_j p(t-j) + M^-1 (E0(t) - sum_j w_j E0(t-j)), the mutual
+// part p - M^-1 E0 of the stored steps extrapolated to t (weights sum to 1).
+// idx = axis * n + site.
+__device__ __forceinline__ double hist_w(int k, int j) {
+    return k == 1 ? 1.0 : (k == 2 ? (j == 1 ? 2.0 : -1.0) : (j == 2 ? -3.0 : (j == 1 ? 3.0 : 1.0)));
+}
+__device__ __forceinline__ double hist_base_p(const double *ph, int n, int cnt, int order, size_t idx) {
+    const int k = min(order, cnt);
+    double s = 0.0;
+    for (int j = 1; j <= k; j++) s += hist_w(k, j) * ph[(size_t)((cnt - j) & 3) * 6 * n + idx];
+    return s;
+}
+__device__ __forceinline__ double hist_diff_e(const double *ph, int n, int cnt, int order, size_t idx, double e0) {
+    const int k = min(order, cnt);
+    double s = e0;
+    for (int j = 1; j <= k; j++) s -= hist_w(k, j) * ph[(size_t)((cnt - j) & 3) * 6 * n + 3 * (size_t)n + idx];
+    return s;
+}
+
 struct Q6 {
     double xx, xy, xz, yy, yz, zz;
 };

@@ -427,6 +427,13 @@ class GpuEnsemble:
         self._chk(self.lib.smd_solver_stats(self.ctx, ctypes.byref(it), ctypes.byref(rms)))
         return it.value, rms.value
 
+    def solver_trace(self) -> np.ndarray:
+        """RMS dipole change of each iteration of the last solve."""
+        out = np.zeros(64)
+        cnt = ctypes.c_int()
+        self._chk(self.lib.smd_solver_trace(self.ctx, L.dptr(out), 64, ctypes.byref(cnt)))
+        return out[:min(cnt.value, 64)]
+
     def polarization(self):
         n = self.n
         mu, q, e0, p = np.zeros(3 * n), np.zeros(6 * n), np.zeros(3 * n), np.zeros(3 * n)
@@ -476,6 +483,10 @@ class GpuEnsemble:
     def mlp_init(self, capacity_frames: int, seed: int = 1):
         self._chk(self.lib.smd_mlp_init(self.ctx, capacity_frames, seed))
 
+    def mlp_set_base(self, order: int):
+        """Order (1-3) of the extrapolated guess the network corrects."""
+        self._chk(self.lib.smd_mlp_set_base(self.ctx, int(order)))
+
     def mlp_collect(self):
         self._chk(self.lib.smd_mlp_collect(self.ctx))
 
@@ -492,22 +503,31 @@ class GpuEnsemble:
         self._chk(self.lib.smd_mlp_params(self.ctx, L.fptr(out), L.fptr(s), ctypes.byref(cnt)))
         return out
 
+    def mlp_dims(self):
+        """(inputs per site, weights) of the network."""
+        f, p = ctypes.c_int(), ctypes.c_int()
+        self._chk(self.lib.smd_mlp_dims(ctypes.byref(f), ctypes.byref(p)))
+        return f.value, p.value
+
     def mlp_eval(self, feats: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(feats, np.float32)
+        if x.ndim != 2 or x.shape[1] != self.mlp_dims()[0]:
+            raise ValueError(f"mlp_eval: rows of {self.mlp_dims()[0]} features expected")
         y = np.zeros((x.shape[0], 3), np.float32)
         self._chk(self.lib.smd_mlp_eval(self.ctx, L.fptr(x), x.shape[0], L.fptr(y)))
         return y
 
     def mlp_gradient(self, rows: np.ndarray) -> np.ndarray:
         r = np.ascontiguousarray(rows, np.float32)
-        cnt = ctypes.c_int()
-        self._chk(self.lib.smd_mlp_params(self.ctx, None, None, ctypes.byref(cnt)))
-        g = np.zeros(cnt.value - 40, np.float32)
+        nf, npar = self.mlp_dims()
+        if r.ndim != 2 or r.shape[1] != nf + 3:
+            raise ValueError(f"mlp_gradient: rows of {nf} features and 3 targets expected")
+        g = np.zeros(npar, np.float32)
         self._chk(self.lib.smd_mlp_gradient(self.ctx, L.fptr(r), r.shape[0], L.fptr(g)))
         return g
 
     def mlp_features(self) -> np.ndarray:
-        f = np.zeros((self.n, 20), np.float32)
+        f = np.zeros((self.n, self.mlp_dims()[0]), np.float32)
         self._chk(self.lib.smd_mlp_features(self.ctx, L.fptr(f)))
         return f
 
