@@ -33,8 +33,10 @@ enum {
     SMD_ERR_NAN = 6,          /* non-finite force or position */
     SMD_ERR_CG = 7,           /* dipole solve did not converge */
     SMD_ERR_NO_DEVICE = 8,    /* no CUDA device / extension unusable */
-    SMD_ERR_TIMEOUT = 9       /* a bounded device-side wait ran out (the dipole
+    SMD_ERR_TIMEOUT = 9,      /* a bounded device-side wait ran out (the dipole
                                  solve's grid barrier; see smd_set_wait_limit) */
+    SMD_ERR_BOX = 10          /* the barostat shrank the box below the cell grid's
+                                 reach (run again from smd_integrator_start) */
 };
 
 /* arithmetic of the pair, reciprocal and dipole-field kernels */
@@ -384,6 +386,18 @@ int smd_ewald_nk(smd_ctx *ctx, int *nk);
 
 /* ---- integration (LFIntegrator, src/integrators/LFIntegrator.cpp) ------ */
 int smd_set_integrator(smd_ctx *ctx, const smd_integrator_params *p);
+/* Isotropic barostat of the reference's NpT run (NHIntegrator with
+ * ensemble 1, src/integrators/NHIntegrator.cpp:276-694, chain :1814-1912):
+ * the chain integrator (SMD_THERMO_NH_CHAIN) then carries vlog with mass
+ * W = (Nf + 1) kT BarosConst^2 and scales positions and box each step.
+ * pressure is the config's value (divided by 1.66053904042716 into
+ * kJ/mol/nm^3 as Integrator.cpp:44 does).  The barostat reads the virial
+ * pressure as the reference does with computeLustig on.  Pair terms
+ * (LJ, Mie, Buckingham) in FP64 only, without constraints; other set-ups
+ * are refused at smd_integrator_start.  on = 0 switches it off. */
+int smd_set_barostat(smd_ctx *ctx, double pressure, double baros_const, int on);
+/* Current box edges (the barostat's, when it runs). */
+int smd_get_box(smd_ctx *ctx, double *edges);
 /* SHAKE targets (LFIntegrator::initialise, LFIntegrator.cpp:141-167):
  * len2[3*m + k] = squared length of the k-th cyclic distance of molecule m
  * (sites 0-1, 1-2, 2-0 of a 3-site molecule; 0-1, 1-2 of a chain). */

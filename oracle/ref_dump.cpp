@@ -12,6 +12,7 @@
 //     ref_dump mie <out>           MieForce::compute() on its own
 //     ref_dump buck <out>          BuckinghamForce::compute() on its own
 //     ref_dump rdf <out>           one RDF::sampling() of the configuration
+//     ref_dump nhrun <nsteps> <out> NHIntegrator::start() then nsteps x run(1)
 //
 // Setup follows Simulation::setup_simulation (src/Simulation.cpp:171-263)
 // without the output files.
@@ -43,6 +44,7 @@
 #include "SimConfiguration.h"
 #include "Integrator.h"
 #include "integrators/LFIntegrator.h"
+#include "integrators/NHIntegrator.h"
 #include "forces/LJForce.h"
 #include "forces/MieForce.h"
 #include "forces/BuckinghamForce.h"
@@ -340,6 +342,45 @@ static int mode_run(int nsteps, const char *out) {
     return 0;
 }
 
+// NHIntegrator (the chain, with the barostat when the config asks for
+// ensemble 1): its start, then nsteps x run(1), with the chain and barostat
+// variables after every step
+static int mode_nhrun(int nsteps, const char *out) {
+    Setup s = build();
+    g_out = fopen(out, "w");
+    header(s);
+    Ensemble *e = s.ens;
+    NHIntegrator *nh = new NHIntegrator(e, s.cfg);  // runs start(): F(0)
+    std::vector<double> epot, ekin, atemp, vol, boxl, vlog, vnh, molvirt, molpt, ptensor;
+    for (int k = 0; k < nsteps; k++) {
+        nh->run(1);
+        const Energy &E = e->myEnergy;
+        epot.push_back(E.totEnergy);
+        ekin.push_back(E.atomKinEnergy);
+        atemp.push_back(e->atomTemp);
+        boxl.push_back(e->boxLx);
+        vol.push_back(e->boxLx * e->boxLy * e->boxLz);
+        vlog.push_back(nh->vlog);
+        for (int q = 0; q < 4; q++) vnh.push_back(nh->vnh[q]);
+        molvirt.push_back(nh->molVirt);
+        molpt.push_back(nh->molPt);
+        for (int q = 0; q < 9; q++) ptensor.push_back(e->atomPressure[q]);
+    }
+    rec("nh_epot", epot);
+    rec("nh_ekin", ekin);
+    rec("nh_atomtemp", atemp);
+    rec("nh_boxl", boxl);
+    rec("nh_volume", vol);
+    rec("nh_vlog", vlog);
+    rec("nh_vnh", vnh);
+    rec("nh_molvirt", molvirt);
+    rec("nh_molpt", molpt);
+    rec("nh_atompressure", ptensor);
+    dump_state(e, "nh_final");
+    fclose(g_out);
+    return 0;
+}
+
 // one RDF::sampling of the current configuration: the raw histogram
 // rdfTable[t1][t2][bin] (both orders of every pair), the bin count and the
 // per-type counts (src/observables/RDF.cpp:109-144)
@@ -373,6 +414,7 @@ int main(int argc, char **argv) {
     if (!strcmp(argv[1], "mie") || !strcmp(argv[1], "buck")) return mode_single(argv[1], argv[2]);
     if (!strcmp(argv[1], "run") && argc >= 4) return mode_run(atoi(argv[2]), argv[3]);
     if (!strcmp(argv[1], "rdf")) return mode_rdf(argv[2]);
+    if (!strcmp(argv[1], "nhrun") && argc >= 4) return mode_nhrun(atoi(argv[2]), argv[3]);
     fprintf(stderr, "unknown mode\n");
     return 2;
 }

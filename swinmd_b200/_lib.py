@@ -15,9 +15,9 @@ LIB_PATH = os.path.join(HERE, "libswinmd_b200.so")
 SMD_OK = 0
 ERRORS = {1: "SMD_ERR_ARG", 2: "SMD_ERR_CUDA", 3: "SMD_ERR_LIST_OVERFLOW", 4: "SMD_ERR_NH_ITER",
           5: "SMD_ERR_SHAKE", 6: "SMD_ERR_NAN", 7: "SMD_ERR_CG", 8: "SMD_ERR_NO_DEVICE",
-          9: "SMD_ERR_TIMEOUT"}
+          9: "SMD_ERR_TIMEOUT", 10: "SMD_ERR_BOX"}
 SMD_ERR_ARG, SMD_ERR_CUDA, SMD_ERR_LIST_OVERFLOW, SMD_ERR_NH_ITER = 1, 2, 3, 4
-SMD_ERR_SHAKE, SMD_ERR_NAN, SMD_ERR_CG, SMD_ERR_NO_DEVICE, SMD_ERR_TIMEOUT = 5, 6, 7, 8, 9
+SMD_ERR_SHAKE, SMD_ERR_NAN, SMD_ERR_CG, SMD_ERR_NO_DEVICE, SMD_ERR_TIMEOUT, SMD_ERR_BOX = 5, 6, 7, 8, 9, 10
 PREC_FP64, PREC_MIXED = 0, 1
 TERM_VDW, TERM_EWALD_REAL, TERM_EWALD_LONG, TERM_ALL = 1, 2, 4, 0xFFFF
 TERM_MP_SHORT, TERM_MP_LONG, TERM_IND_SHORT, TERM_IND_LONG = 8, 16, 32, 64
@@ -104,6 +104,8 @@ SIGNATURES = {
     "smd_get_pairs": (ctypes.c_int, [_P, _I, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "smd_ewald_nk": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
     "smd_set_integrator": (ctypes.c_int, [_P, ctypes.POINTER(IntegratorParams)]),
+    "smd_set_barostat": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, ctypes.c_int]),
+    "smd_get_box": (ctypes.c_int, [_P, _D]),
     "smd_set_constraints": (ctypes.c_int, [_P, _D]),
     "smd_integrator_start": (ctypes.c_int, [_P]),
     "smd_integrator_resume": (ctypes.c_int, [_P]),

@@ -56,6 +56,7 @@ cudaError_t dalloc(T **p, size_t count) {
 }
 
 int status_to_code(unsigned st) {
+    if (st & ST_BOX) return SMD_ERR_BOX;   // first: what follows it may stem from it
     if (st & ST_LIST_OVERFLOW) return SMD_ERR_LIST_OVERFLOW;
     if (st & ST_NAN) return SMD_ERR_NAN;
     if (st & (ST_SHAKE_ITER | ST_SHAKE_GEOM)) return SMD_ERR_SHAKE;
@@ -66,6 +67,7 @@ int status_to_code(unsigned st) {
 }
 
 const char *status_text(unsigned st) {
+    if (st & ST_BOX) return "the barostat shrank the box below the cell grid's reach";
     if (st & ST_LIST_OVERFLOW) return "pair list overflow: a site has more neighbours than the list holds";
     if (st & ST_NAN) return "non-finite position";
     if (st & ST_SHAKE_GEOM) return "SHAKE geometric failure";
@@ -82,15 +84,19 @@ void setup_grid(Ctx &c, int use_cells) {
     CellGrid &g = c.grid;
     double len = c.cutoff + c.cut_buffer;
     g.use_cells = use_cells;
+    for (int d = 0; d < 3; d++) g.L0[d] = c.box.L[d];
+    // with the barostat the cells are laid out for a box 10 % smaller, so
+    // that the 27-cell stencil still covers the list radius as it shrinks
+    const double room = c.npt ? 0.9 : 1.0;
     for (int d = 0; d < 3; d++)
-        if (len <= 0 || len > c.box.L[d] / 3.0) g.use_cells = 0;
+        if (len <= 0 || len > room * c.box.L[d] / 3.0) g.use_cells = 0;
     if (!g.use_cells) {
         g.ncell = 0;
         for (int d = 0; d < 3; d++) { g.n[d] = 0; g.len[d] = g.rlen[d] = g.origin[d] = 0; }
         return;
     }
     for (int d = 0; d < 3; d++) {
-        g.n[d] = (int)(c.box.L[d] / len);
+        g.n[d] = (int)(room * c.box.L[d] / len);
         g.len[d] = c.box.L[d] / g.n[d];
         g.rlen[d] = 1.0 / g.len[d];
         g.origin[d] = -c.box.L[d] / 2.0;
@@ -481,7 +487,33 @@ int smd_set_box(smd_ctx *x, double lx, double ly, double lz) {
         int r = setup_recip(c);
         if (r) return fail(x, r, "smd_set_box: reciprocal set-up failed");
     }
+    if (c.dbox) CK(cudaMemcpy(c.dbox, &c.box, sizeof(Box), cudaMemcpyHostToDevice));
     return alloc_list(x);
+}
+
+int smd_set_barostat(smd_ctx *x, double pressure, double baros_const, int on) {
+    if (!x || (on && !(baros_const > 0)) || !std::isfinite(pressure))
+        return fail(x, SMD_ERR_ARG, "smd_set_barostat: BarosConst must be > 0");
+    Ctx &c = x->c;
+    c.npt = on ? 1 : 0;
+    c.npt_press = pressure / 1.66053904042716;   // Integrator.cpp:44
+    c.npt_tau = baros_const;
+    if (on && !c.dbox) CK(dalloc(&c.dbox, 1));
+    if (c.dbox) CK(cudaMemcpy(c.dbox, &c.box, sizeof(Box), cudaMemcpyHostToDevice));
+    setup_grid(c, c.want_cells);
+    return alloc_list(x);
+}
+
+int smd_get_box(smd_ctx *x, double *edges) {
+    if (!x || !edges) return SMD_ERR_ARG;
+    Ctx &c = x->c;
+    Box b = c.box;
+    if (c.npt && c.dbox) {
+        CK(cudaStreamSynchronize(c.stream));
+        CK(cudaMemcpy(&b, c.dbox, sizeof(Box), cudaMemcpyDeviceToHost));
+    }
+    for (int d = 0; d < 3; d++) edges[d] = b.L[d];
+    return SMD_OK;
 }
 
 int smd_set_pairlist(smd_ctx *x, double cutoff, double cut_buffer, int use_cells) {
@@ -1300,11 +1332,35 @@ static int integrator_begin(smd_ctx *x, bool new_start) {
     // the dipole history of the guess starts afresh (uploads keep it: the
     // solve converges to its tolerance from any start)
     CK(cudaMemsetAsync(c.flags + 2, 0, 2 * sizeof(int), c.stream));   // step count and the push's ticket
+    if (c.npt) {
+        // NHIntegrator's NpT run: pair terms only (the reciprocal sums keep
+        // their k-vectors of one box), no constraints (the reference stops
+        // there too, NHIntegrator.cpp:604-607), FP64
+        if (c.ip.thermostat != SMD_THERMO_NH_CHAIN || c.ip.strain_rate != 0.0 || c.ewald_on || c.mp_on ||
+            has_bonded(c) || c.precision != SMD_PREC_FP64 || c.vdw == VDW_BUFF)
+            return fail(x, SMD_ERR_ARG,
+                        "smd_integrator_start: the barostat runs with the chain integrator on pair terms in FP64");
+        CK(cudaMemcpy(c.dbox, &c.box, sizeof(Box), cudaMemcpyHostToDevice));
+        setup_grid(c, c.want_cells);
+        int r = alloc_list(x);
+        if (r) return r;
+        const double vol = c.box.L[0] * c.box.L[1] * c.box.L[2];
+        c.npt_lrc_k = c.e_lrc * vol;
+        c.npt_smin = 0.0;
+        if (c.grid.use_cells)
+            for (int d = 0; d < 3; d++)
+                c.npt_smin = std::max(c.npt_smin, c.grid.n[d] * (c.cutoff + c.cut_buffer) / c.box.L[d]);
+    }
     launch_nlist(c, true);
     c.list_valid = 1;
     CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
     if (c.ip.thermostat == SMD_THERMO_NH_CHAIN) {
         launch_nhc_start(c);   // delta = 0 before the first list and forces
+        // the barostat at rest; molVirt = -P until the first forces
+        // (Integrator.cpp:44-46), vlog = 0 (NHIntegrator.cpp:120)
+        const double bs[5] = {0.0, c.npt ? -c.npt_press : 0.0, 1.0, c.ip.timestep,
+                              c.box.L[0] * c.box.L[1] * c.box.L[2]};
+        CK(cudaMemcpyAsync(c.scal + SC_VLOG, bs, sizeof(bs), cudaMemcpyHostToDevice, c.stream));
         launch_nlist(c, true);
         CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
         enqueue_forces(c);
@@ -1325,6 +1381,18 @@ int smd_integrator_start(smd_ctx *x) { return integrator_begin(x, true); }
 
 int smd_integrator_resume(smd_ctx *x) { return integrator_begin(x, false); }
 
+// after barostat steps: the host copy of the box and the tail correction
+// follow the device's (the cell grid stays laid out for the box it was
+// built for; the kernels scale it)
+static void sync_npt_box(Ctx &c) {
+    Box b;
+    if (cudaMemcpy(&b, c.dbox, sizeof(Box), cudaMemcpyDeviceToHost) != cudaSuccess) return;
+    c.box = b;
+    const double vol = b.L[0] * b.L[1] * b.L[2];
+    c.e_lrc = c.npt_lrc_k / vol;
+    c.v_lrc = -2.0 * c.e_lrc;
+}
+
 int smd_run(smd_ctx *x, int nsteps) {
     if (!x || !x->c.integrator_ready || nsteps < 0) return fail(x, SMD_ERR_ARG, "smd_run: integrator not set");
     Ctx &c = x->c;
@@ -1343,7 +1411,9 @@ int smd_run(smd_ctx *x, int nsteps) {
     for (int s = 0; s < nsteps; s++) CK(cudaGraphLaunch(c.step_graph, c.stream));
     c.steps_done += nsteps;
     if (nsteps > 0) touch(c);
-    return sync_status(x);
+    int r = sync_status(x);
+    if (c.npt) sync_npt_box(c);
+    return r;
 }
 
 int smd_profile_stages(smd_ctx *x, int reps, double *out) {
@@ -1492,7 +1562,9 @@ int smd_run_timed(smd_ctx *x, int nsteps, double *device_ms) {
     cudaEventDestroy(e1);
     c.steps_done += nsteps;
     if (nsteps > 0) touch(c);
-    return sync_status(x);
+    int r = sync_status(x);
+    if (c.npt) sync_npt_box(c);
+    return r;
 }
 
 int smd_get_observables(smd_ctx *x, smd_observables *out) {

@@ -65,8 +65,9 @@ enum StatusBits {
     ST_CELL_RANGE = 16,      // site outside the cell grid after clamping
     ST_CG_ITER = 32,         // dipole solver did not converge
     ST_SHAKE_GEOM = 64,      // SHAKE geometric failure (reference LFIntegrator.cpp:1758)
-    ST_WAIT_TIMEOUT = 128    // a bounded device-side wait (the dipole solve's grid
+    ST_WAIT_TIMEOUT = 128,   // a bounded device-side wait (the dipole solve's grid
                              // barrier) ran out: blocks not co-resident or one missing
+    ST_BOX = 256             // the barostat shrank the box below what the cell grid covers
 };
 
 // integrator scalars shared by several files (ctx->scal): 0-7 belong to the
@@ -78,6 +79,11 @@ enum ScalShared {
     SC_LE = 14,      // Lees-Edwards offset delta (nm), in [0, Lx)
     SC_LE_B = 15,    // delta at the last pair-list build
     SC_DRMAX = 16,   // displacement^2 limit of the current step's list test
+    SC_VLOG = 17,    // barostat velocity vlog (NHIntegrator)
+    SC_MOLVIRT = 18, // molVirt: minus the virial pressure of the last forces
+    SC_X2 = 19,      // exp(dt vlog): position and box scale of the step
+    SC_POLY = 20,    // exp(dt vlog / 2) sinh-series dt: velocity factor of the drift
+    SC_VOL = 21,     // volume of the current box
     SC_NSCAL = 32
 };
 

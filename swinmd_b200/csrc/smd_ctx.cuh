@@ -26,6 +26,7 @@ struct CellGrid {
     int n[3];
     int ncell;
     double len[3], rlen[3], origin[3];
+    double L0[3];       // the box the grid was laid out for (the barostat scales it)
 };
 
 struct PairList {
@@ -184,6 +185,13 @@ struct Ctx {
     double vdw_rc2 = 1.0, sw_rs2 = 0.0, sw_c1 = 0, sw_c2 = 0, sw_c3 = 0;
     int switch_on = 0;
     double e_lrc = 0, v_lrc = 0;
+    // isotropic barostat of the chain integrator (NHIntegrator's NpT run)
+    int npt = 0;
+    double npt_press = 0;           // target pressure, kJ/mol/nm^3
+    double npt_tau = 0;             // BarosConst (ps)
+    double npt_lrc_k = 0;           // tail-correction energy x volume
+    double npt_smin = 0;            // smallest box scale the cell grid covers
+    Box *dbox = nullptr;            // the box on the device while the barostat runs
     int ewald_on = 0;
     double ew_alpha = 0, ew_kcut = 0, ew_rc2 = 0, e_self = 0;
     int long_steps = 1;

@@ -3,9 +3,18 @@
 //
 // Chain: NHIntegrator::chain (src/integrators/NHIntegrator.cpp:1814-1912),
 // 4 links, nc = 5 multiple steps, Suzuki-Yoshida weights (1/(2 - 2^(1/3)),
-// 1 - 2 w, w), Q_0 = Nf kT tau^2, Q_k = kT tau^2 (:113-119).  The reference's
-// integrator always couples its barostat (vlog); here that degree of freedom
-// is removed (vlog = 0, Nf kT in the first link) for constant-volume runs.
+// 1 - 2 w, w), Q_0 = Nf kT tau^2, Q_k = kT tau^2 (:113-119).  With the
+// barostat (smd_set_barostat: the reference's NpT run) the chain carries the
+// isotropic MTK degree of freedom vlog with mass W = (Nf + 1) kT tau_P^2
+// (:119): G_0 = 2 K + W vlog^2 - (Nf + 1) kT, G_log = (2 K (1 + 3/Nf) +
+// 3 V (P_vir - P)) / W, and the velocity scale exp(-(v_1 + (1 + 3/Nf) vlog)
+// dt/2); the drift is r' = r e^(2h) + v e^h S(h) dt with h = vlog dt/2 and
+// S the sinh(h)/h series to h^8, and the box edges scale by e^(2h)
+// (:390-419).  P_vir is the reference's -molVirt of the previous forces
+// (:382, :635): the Lustig volume derivative of the pair energy,
+// sum r du/dr / 3V, minus that of the tail correction (LJForce.cpp:136-250,
+// 297-327), the trace of the pair virial here.  Without the barostat vlog
+// stays 0 and the first link sees Nf kT: constant volume.
 // Step order as NHIntegrator::run (:380-408, :628-644):
 //   k_nhc_chain   chain half step on the kinetic energy of v (one thread),
 //                 Lees-Edwards offset delta += g Ly dt, the list test limit
@@ -52,16 +61,25 @@ struct NhcArgs {
     double dt, kT, nf, tau, gamma, skin, volume;
     int atom_ndf, mol_ndf;
     double e_lrc, v_lrc, e_self;
+    // barostat (npt): the box on the device, target pressure, W, the tail
+    // correction's energy times volume, the smallest box scale the cell
+    // grid covers and the box it was built for
+    int npt;
+    Box *dbox;
+    double press, wbar, lrc_k, smin, L0[3];
 };
 
-// one chain half step; returns the velocity scale (vnh in scal[SC_VNH..+3])
-__device__ double chain_half(double *vnh, double ekin, const NhcArgs &a) {
+// one chain half step; returns the velocity scale (vnh in scal[SC_VNH..+3]);
+// with the barostat also vlog, driven by the virial pressure pvir
+__device__ double chain_half(double *vnh, double ekin, const NhcArgs &a, double &vlog, double pvir, double vol) {
     double qnh[4];
     for (int k = 0; k < 4; k++) qnh[k] = a.kT * a.tau * a.tau;
     qnh[0] *= a.nf;
     const double w0 = 1.0 / (2.0 - cbrt(2.0));
     const double wj[3] = {w0, 1.0 - 2.0 * w0, w0};
     const int nc = 5;
+    const double gkt = a.npt ? (a.nf + 1.0) * a.kT : a.nf * a.kT;
+    const double odnf = 1.0 + 3.0 / a.nf, diff = pvir - a.press;
     double scale = 1.0, g[4];
     for (int i = 0; i < nc; i++)
         for (int j = 0; j < 3; j++) {
@@ -75,13 +93,25 @@ __device__ double chain_half(double *vnh, double ekin, const NhcArgs &a) {
             g[1] = (qnh[0] * vnh[0] * vnh[0] - a.kT) / qnh[1];
             ex = exp(-vnh[2] * dts8);
             vnh[1] = ex * (vnh[1] * ex + g[1] * dts4);
-            g[0] = (2.0 * ekin - a.nf * a.kT) / qnh[0];
+            g[0] = (2.0 * ekin + (a.npt ? a.wbar * vlog * vlog : 0.0) - gkt) / qnh[0];
             ex = exp(-vnh[1] * dts8);
             vnh[0] = ex * (vnh[0] * ex + g[0] * dts4);
-            ex = exp(-vnh[0] * dts2);
+            if (a.npt) {
+                const double glog = (2.0 * ekin * odnf + 3.0 * vol * diff) / a.wbar;
+                ex = exp(-vnh[0] * dts8);
+                vlog = ex * (vlog * ex + glog * dts4);
+                ex = exp(-(vnh[0] + vlog * odnf) * dts2);
+            } else {
+                ex = exp(-vnh[0] * dts2);
+            }
             scale *= ex;
             ekin = ekin * ex * ex;
-            g[0] = (2.0 * ekin - a.nf * a.kT) / qnh[0];
+            if (a.npt) {
+                const double glog = (2.0 * ekin * odnf + 3.0 * vol * diff) / a.wbar;
+                ex = exp(-vnh[0] * dts8);
+                vlog = ex * (vlog * ex + glog * dts4);
+            }
+            g[0] = (2.0 * ekin + (a.npt ? a.wbar * vlog * vlog : 0.0) - gkt) / qnh[0];
             ex = exp(-vnh[1] * dts8);
             vnh[0] = ex * (vnh[0] * ex + g[0] * dts4);
             g[1] = (qnh[0] * vnh[0] * vnh[0] - a.kT) / qnh[1];
@@ -100,9 +130,30 @@ __global__ void k_nhc_chain(NhcArgs a) {
     if (threadIdx.x != 0) return;
     double vnh[4];
     for (int k = 0; k < 4; k++) vnh[k] = a.scal[SC_VNH + k];
-    const double s = chain_half(vnh, a.scal[SC_EKIN], a);
+    double vlog = a.scal[SC_VLOG];
+    const double s = chain_half(vnh, a.scal[SC_EKIN], a, vlog, -a.scal[SC_MOLVIRT], a.scal[SC_VOL]);
     for (int k = 0; k < 4; k++) a.scal[SC_VNH + k] = vnh[k];
     a.scal[SC_SCALE] = s;
+    if (a.npt) {
+        // the drift's factors and the scaled box (NHIntegrator.cpp:390-419)
+        a.scal[SC_VLOG] = vlog;
+        const double term = 0.5 * a.dt * vlog, ex = exp(term), ex2 = ex * ex, arg2 = term * term;
+        const double e2 = 1.0 / 6.0, e4 = e2 / 20.0, e6 = e4 / 42.0, e8 = e6 / 72.0;
+        const double poly = ex * (1.0 + arg2 * (e2 + arg2 * (e4 + arg2 * (e6 + arg2 * e8)))) * a.dt;
+        a.scal[SC_X2] = ex2;
+        a.scal[SC_POLY] = poly;
+        Box b = *a.dbox;
+        bool small = false;
+        for (int d = 0; d < 3; d++) {
+            b.L[d] *= ex2;
+            b.half[d] = 0.5 * b.L[d];
+            b.inv[d] = 1.0 / b.L[d];
+            small |= b.L[d] < a.smin * a.L0[d];
+        }
+        *a.dbox = b;
+        a.scal[SC_VOL] = b.L[0] * b.L[1] * b.L[2];
+        if (small) atomicOr(a.status, ST_BOX);
+    }
     double lim = 0.5 * a.skin;
     if (a.gamma != 0.0) {
         const double Lx = a.box.L[0];
@@ -129,6 +180,8 @@ __global__ void __launch_bounds__(NHC_BLOCK) k_nhc_first(NhcArgs a) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     const double s = a.scal[SC_SCALE], delta = a.scal[SC_LE], drmax = a.scal[SC_DRMAX];
     const double hdt = 0.5 * a.dt, g = a.gamma;
+    const Box bx = a.npt ? *a.dbox : a.box;
+    const double x2 = a.npt ? a.scal[SC_X2] : 1.0, poly = a.npt ? a.scal[SC_POLY] : a.dt;
     bool rebuild = false, bad = false;
     if (m < a.nmol) {
         const int s0 = a.mol_off[m], s1 = a.mol_off[m + 1];
@@ -141,9 +194,18 @@ __global__ void __launch_bounds__(NHC_BLOCK) k_nhc_first(NhcArgs a) {
             if (g != 0.0) v.x -= g * hdt * v.y;
             v.x += hdt * v.w * f.x; v.y += hdt * v.w * f.y; v.z += hdt * v.w * f.z;
             double4 p = a.pos4[at];
-            const double drx = a.dt * v.x + g * a.dt * (p.y + hdt * v.y);
-            const double dry = a.dt * v.y, drz = a.dt * v.z;
-            p.x += drx; p.y += dry; p.z += drz;
+            double drx, dry, drz;
+            if (a.npt) {
+                // r' = r e^(2h) + v e^h S(h) dt
+                drx = (p.x * x2 + v.x * poly) - p.x;
+                dry = (p.y * x2 + v.y * poly) - p.y;
+                drz = (p.z * x2 + v.z * poly) - p.z;
+                p.x = p.x * x2 + v.x * poly; p.y = p.y * x2 + v.y * poly; p.z = p.z * x2 + v.z * poly;
+            } else {
+                drx = a.dt * v.x + g * a.dt * (p.y + hdt * v.y);
+                dry = a.dt * v.y; drz = a.dt * v.z;
+                p.x += drx; p.y += dry; p.z += drz;
+            }
             double4 d = a.disp4[at];
             d.x += drx; d.y += dry; d.z += drz;
             if (d.x * d.x + d.y * d.y + d.z * d.z > drmax) rebuild = true;
@@ -158,11 +220,11 @@ __global__ void __launch_bounds__(NHC_BLOCK) k_nhc_first(NhcArgs a) {
         cx /= M; cy /= M; cz /= M;
         // wrap the centre of mass: y first (Lees-Edwards), then x and z
         double wx = 0, wy = 0;
-        if (cy >= a.box.half[1]) { wy = -a.box.L[1]; wx = -delta; }
-        else if (cy < -a.box.half[1]) { wy = a.box.L[1]; wx = delta; }
+        if (cy >= bx.half[1]) { wy = -bx.L[1]; wx = -delta; }
+        else if (cy < -bx.half[1]) { wy = bx.L[1]; wx = delta; }
         if (g == 0.0) wx = 0;
-        wx = pbc1(cx + wx, a.box.L[0], a.box.half[0]) - cx;
-        const double wz = pbc1(cz, a.box.L[2], a.box.half[2]) - cz;
+        wx = pbc1(cx + wx, bx.L[0], bx.half[0]) - cx;
+        const double wz = pbc1(cz, bx.L[2], bx.half[2]) - cz;
         // the shifts so far, per molecule: Atom::realPos = position - shift
         if (a.wrap && (wx != 0.0 || wy != 0.0 || wz != 0.0)) {
             a.wrap[m] += wx;
@@ -266,9 +328,23 @@ __global__ void __launch_bounds__(NHC_BLOCK) k_nhc_second(NhcArgs a) {
     if (threadIdx.x == 0) {
         double vnh[4];
         for (int k = 0; k < 4; k++) vnh[k] = a.scal[SC_VNH + k];
-        const double s = chain_half(vnh, 0.5 * tot[Q_KE], a);
+        double vlog = a.scal[SC_VLOG];
+        const double vol = a.npt ? a.scal[SC_VOL] : a.volume;
+        const double s = chain_half(vnh, 0.5 * tot[Q_KE], a, vlog, -a.scal[SC_MOLVIRT], vol);
         for (int k = 0; k < 4; k++) a.scal[SC_VNH + k] = vnh[k];
         a.scal[SC_SCALE] = s;
+        // the tail correction of this volume (LJForce::long_range_correct,
+        // recomputed every evaluation in NpT: E = K / V, virial -2 E, dU/dV = -2 E / V)
+        const double e_lrc = a.npt ? a.lrc_k / vol : a.e_lrc;
+        const double v_lrc = a.npt ? -2.0 * e_lrc : a.v_lrc;
+        if (a.npt) {
+            a.scal[SC_VLOG] = vlog;
+            // molVirt = -(sum r du/dr) / 3V + dU_lrc/dV (NHIntegrator.cpp:635)
+            double tr = 0.0;
+            for (int q = 0; q < 9; q += 4)
+                tr += ((double)__ldcg(&a.acc[ACC_VIR + q]) + (double)__ldcg(&a.acc[ACC_LVIR + q])) * ACC_INV;
+            a.scal[SC_MOLVIRT] = -tr / (3.0 * vol) + v_lrc / vol;
+        }
         const double s2 = s * s;
         const double keA = tot[Q_KE] * s2, keM = tot[Q_KEM] * s2;
         a.scal[SC_EKIN] = 0.5 * keA;
@@ -282,7 +358,7 @@ __global__ void __launch_bounds__(NHC_BLOCK) k_nhc_second(NhcArgs a) {
         long long accv[ACC_COUNT];
         for (int q = 0; q < ACC_COUNT; q++) accv[q] = __ldcg(&acc[q]);
         double en[SMD_E_COUNT];
-        acc_energies(accv, a.e_lrc, a.e_self, en);
+        acc_energies(accv, e_lrc, a.e_self, en);
         double ep = 0;
         for (int q = 0; q < SMD_E_COUNT; q++) {
             o.energy[q] = en[q];
@@ -292,12 +368,12 @@ __global__ void __launch_bounds__(NHC_BLOCK) k_nhc_second(NhcArgs a) {
         const int sym[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
         for (int q = 0; q < 9; q++) {
             double vir = ((double)__ldcg(&acc[ACC_VIR + q]) + (double)__ldcg(&acc[ACC_LVIR + q])) * ACC_INV;
-            if (q == 0 || q == 4 || q == 8) vir -= a.v_lrc;
-            o.mol_pressure[q] = (tot[Q_MP + sym[q]] * s2 + vir - tot[Q_MC + q]) / a.volume;
-            o.atom_pressure[q] = (tot[Q_AP + sym[q]] * s2 + vir) / a.volume;
+            if (q == 0 || q == 4 || q == 8) vir -= v_lrc;
+            o.mol_pressure[q] = (tot[Q_MP + sym[q]] * s2 + vir - tot[Q_MC + q]) / vol;
+            o.atom_pressure[q] = (tot[Q_AP + sym[q]] * s2 + vir) / vol;
             o.virial[q] = vir;
         }
-        o.volume = a.volume;
+        o.volume = vol;
         o.shear_offset = a.scal[SC_LE];
         o.step += 1;
         o.list_updates = a.flags[1];
@@ -370,6 +446,13 @@ NhcArgs nhc_args(Ctx &c) {
     a.volume = c.box.L[0] * c.box.L[1] * c.box.L[2];
     a.atom_ndf = c.ip.atom_ndf; a.mol_ndf = c.ip.mol_ndf;
     a.e_lrc = c.e_lrc; a.v_lrc = c.v_lrc; a.e_self = c.e_self;
+    a.npt = c.npt;
+    a.dbox = c.dbox;
+    a.press = c.npt_press;
+    a.wbar = (c.ip.atom_ndf + 1.0) * a.kT * c.npt_tau * c.npt_tau;
+    a.lrc_k = c.npt_lrc_k;
+    a.smin = c.npt_smin;
+    for (int d = 0; d < 3; d++) a.L0[d] = c.grid.L0[d];
     return a;
 }
 }  // namespace

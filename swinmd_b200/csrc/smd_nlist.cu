@@ -19,12 +19,14 @@
 
 namespace smd {
 
-__device__ __forceinline__ int ref_cell(const double4 &p, const CellGrid &g) {
+// sc: the box edges over the ones the grid was laid out for (1 but under
+// the barostat, which scales positions and box together)
+__device__ __forceinline__ int ref_cell(const double4 &p, const CellGrid &g, const double (&sc)[3]) {
     int c[3];
     const double pp[3] = {p.x, p.y, p.z};
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-        double delta = pp[d] - g.origin[d];
+        double delta = sc[d] == 1.0 ? pp[d] - g.origin[d] : pp[d] / sc[d] - g.origin[d];
         int x = (int)(delta * g.rlen[d]);
         if (x >= g.n[d]) x = g.n[d] - 1;
         else if (x < 0) x = 0;
@@ -34,12 +36,15 @@ __device__ __forceinline__ int ref_cell(const double4 &p, const CellGrid &g) {
 }
 
 __global__ void k_bin(int n, const double4 *__restrict__ pos4, CellGrid g, int *cell_of,
-                      int *cell_slot, int *cell_count, double4 *disp4, const int *flags) {
+                      int *cell_slot, int *cell_count, double4 *disp4, const int *flags, const Box *dbox) {
     if (!flags[0]) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (g.use_cells) {
-        int c = ref_cell(pos4[i], g);
+        double sc[3] = {1.0, 1.0, 1.0};
+        if (dbox)
+            for (int d = 0; d < 3; d++) sc[d] = dbox->L[d] / g.L0[d];
+        int c = ref_cell(pos4[i], g, sc);
         cell_of[i] = c;
         cell_slot[i] = atomicAdd(&cell_count[c], 1);
     }
@@ -127,6 +132,7 @@ struct BuildArgs {
     unsigned int *status;
     const int *flags;
     const double *le;   // Lees-Edwards offset on the device, or null
+    const Box *dbox;    // the box on the device (barostat), or null: box
 };
 
 // r^2 of the reference's pair test, without contraction into FMA
@@ -147,6 +153,7 @@ __device__ __forceinline__ double ref_r2(const double4 &a, const double4 &b, con
 // One warp per site i; candidates are tested 32 at a time and appended in
 // candidate order (ballot + popc), so the row order is deterministic.
 __device__ void build_site(const BuildArgs &a, int i, int lane) {
+    const Box box = a.dbox ? *a.dbox : a.box;
     const double4 pi = a.pos4[i];
     const int mi = a.mol[i];
     const int e0 = a.excl_off[i], e1 = a.excl_off[i + 1];
@@ -157,7 +164,7 @@ __device__ void build_site(const BuildArgs &a, int i, int lane) {
         bool take = valid && j != i;
         // the distance test first: only the few candidates inside the list
         // radius read the exclusion list
-        if (take) take = ref_r2(pi, a.pos4[j], a.box, pbc, le && pbc, delta) < a.rl2;
+        if (take) take = ref_r2(pi, a.pos4[j], box, pbc, le && pbc, delta) < a.rl2;
         if (take) {
             for (int e = e0; e < e1; e++)
                 if (a.excl[e] == j) { take = false; break; }
@@ -234,6 +241,7 @@ __global__ void k_build(BuildArgs a) {
 constexpr int BS_SITES = 16, BS_STAGE = 1024;
 __global__ void __launch_bounds__(BS_SITES * 32) k_build_staged(BuildArgs a) {
     if (!a.flags[0]) return;
+    const Box box = a.dbox ? *a.dbox : a.box;
     __shared__ double s_x[BS_STAGE], s_y[BS_STAGE], s_z[BS_STAGE];
     __shared__ int s_j[BS_STAGE], s_m[BS_STAGE];
     __shared__ int s_cell[BS_SITES], s_cs[27], s_off[28], s_nc[27];
@@ -303,7 +311,7 @@ __global__ void __launch_bounds__(BS_SITES * 32) k_build_staged(BuildArgs a) {
             bool take = valid && j != i;
             if (take) {
                 const double4 pj = make_double4(s_x[kk], s_y[kk], s_z[kk], 0.0);
-                take = ref_r2(pi, pj, a.box, mj >= 0, false, 0.0) < a.rl2;
+                take = ref_r2(pi, pj, box, mj >= 0, false, 0.0) < a.rl2;
             }
             if (take)
                 for (int q = e0; q < e1; q++)
@@ -345,7 +353,7 @@ void launch_nlist(Ctx &c, bool force_rebuild) {
     int nb = (c.n + T - 1) / T;
     if (c.grid.use_cells) {
         k_bin<<<nb, T, 0, c.stream>>>(c.n, c.pos4, c.grid, c.pl.cell_of, c.pl.cell_slot,
-                                      c.pl.cell_count, c.disp4, c.flags);
+                                      c.pl.cell_count, c.disp4, c.flags, c.npt ? c.dbox : nullptr);
         k_scan<<<1, 1024, 0, c.stream>>>(c.grid.ncell, c.pl.cell_count, c.pl.cell_start, c.flags);
         k_fill<<<nb, T, 0, c.stream>>>(c.n, c.pl.cell_of, c.pl.cell_slot, c.pl.cell_start,
                                        c.pl.cell_atoms, c.flags);
@@ -355,7 +363,7 @@ void launch_nlist(Ctx &c, bool force_rebuild) {
                                              c.flags);
     } else {
         k_bin<<<nb, T, 0, c.stream>>>(c.n, c.pos4, c.grid, c.pl.cell_of, c.pl.cell_slot,
-                                      c.pl.cell_count, c.disp4, c.flags);
+                                      c.pl.cell_count, c.disp4, c.flags, nullptr);
     }
     BuildArgs a;
     a.n = c.n; a.max_nbr = c.pl.max_nbr; a.pos4 = c.pos4; a.mol = c.mol;
@@ -363,6 +371,7 @@ void launch_nlist(Ctx &c, bool force_rebuild) {
     a.cell_start = c.pl.cell_start; a.cell_atoms = c.pl.cell_atoms; a.g = c.grid; a.box = c.box;
     a.rl2 = c.pl.rl2; a.nbr = c.pl.nbr; a.nnbr = c.pl.nnbr; a.status = c.status; a.flags = c.flags;
     a.le = c.ip.strain_rate != 0.0 && c.integrator_ready ? c.scal + SC_LE : nullptr;
+    a.dbox = c.npt ? c.dbox : nullptr;
     if (c.grid.use_cells && !a.le) {
         k_build_staged<<<(c.n + BS_SITES - 1) / BS_SITES, BS_SITES * 32, 0, c.stream>>>(a);
     } else {

@@ -49,6 +49,7 @@ struct PairArgs {
     float bswf, bwinv;  // taper start and 1/(cutoff - start), FP32 path
     int buff_int;       // n - m and m are small positive integers
     const double *le;   // Lees-Edwards offset on the device (planar shear), or null
+    const Box *dbox;    // the box on the device (barostat, FP64 path), or null: box
     long long *frc;
     long long *acc;
 };
@@ -319,8 +320,9 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_pair(PairArgs a) {
     const int gt = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = gt / TPP;
     const int t = gt % TPP;
+    const Box box = a.dbox ? *a.dbox : a.box;
     const double le_d = a.le ? *a.le : 0.0;
-    const unsigned le_f = a.le ? le_frac(le_d, a.box.inv[0]) : 0u;
+    const unsigned le_f = a.le ? le_frac(le_d, box.inv[0]) : 0u;
     double fx = 0, fy = 0, fz = 0;
     R evdw = 0, ereal = 0;
     int npair = 0;
@@ -349,12 +351,12 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_pair(PairArgs a) {
                 const double4 pj = a.pos4[j];
                 if (a.le) {
                     double ex = pj.x - pi64.x, ey = pj.y - pi64.y, ez = pj.z - pi64.z;
-                    min_image_le(ex, ey, ez, a.box, le_d);
+                    min_image_le(ex, ey, ez, box, le_d);
                     dx = ex; dy = ey; dz = ez;
                 } else {
-                    dx = pbc1(pj.x - pi64.x, a.box.L[0], a.box.half[0]);
-                    dy = pbc1(pj.y - pi64.y, a.box.L[1], a.box.half[1]);
-                    dz = pbc1(pj.z - pi64.z, a.box.L[2], a.box.half[2]);
+                    dx = pbc1(pj.x - pi64.x, box.L[0], box.half[0]);
+                    dy = pbc1(pj.y - pi64.y, box.L[1], box.half[1]);
+                    dz = pbc1(pj.z - pi64.z, box.L[2], box.half[2]);
                 }
                 r2 = dx * dx + dy * dy + dz * dz;
                 tj = (int)pj.w;
@@ -710,6 +712,7 @@ void launch_pair(Ctx &c) {
     a.ew_rc2 = c.ew_rc2;
     a.frc = c.frc; a.acc = c.acc;
     a.le = c.ip.strain_rate != 0.0 && c.integrator_ready ? c.scal + SC_LE : nullptr;
+    a.dbox = c.npt ? c.dbox : nullptr;
     a.bn = c.buff_n; a.bm = c.buff_m; a.bdelta = c.buff_delta; a.bgamma = c.buff_gamma;
     for (int q = 0; q < 6; q++) a.bc[q] = c.buff_c[q];
     a.bsw2 = c.buff_sw * c.buff_sw;

@@ -615,6 +615,13 @@ class LFIntegrator:
         if series_capacity:
             L.check(ensemble.ctx, ensemble.lib.smd_set_series_capacity(ensemble.ctx, series_capacity))
         self.series_capacity = series_capacity
+        # the NpT ensemble (ensemble 1): the barostat of NHIntegrator; the
+        # leap-frog integrator's own NpT branch is not built
+        npt = int(c.ensemble) == 1
+        if npt and p.thermostat != L.THERMO_NH_CHAIN:
+            raise NotImplementedError("NpT runs with the chain integrator (NHIntegrator) only")
+        L.check(ensemble.ctx, ensemble.lib.smd_set_barostat(ensemble.ctx, float(c.pressure),
+                                                            float(c.baros_const), int(npt)))
 
     def start(self):
         L.check(self.ens.ctx, self.ens.lib.smd_integrator_start(self.ens.ctx))
@@ -674,12 +681,33 @@ class LFIntegrator:
 
 class NHIntegrator(LFIntegrator):
     """Velocity-Verlet integrator with the 4-link Nose-Hoover chain of
-    ``NHIntegrator::chain`` (src/integrators/NHIntegrator.cpp:1814-1912) at
-    constant volume, and SLLOD planar Couette shear with Lees-Edwards images
-    when the configuration asks for it (testMode 2, ``rate``).  ``start()``
-    computes F(0) and the chain's starting kinetic energy."""
+    ``NHIntegrator::chain`` (src/integrators/NHIntegrator.cpp:1814-1912):
+    with the isotropic barostat of the reference's NpT run when the
+    configuration asks for ensemble 1 (``NHIntegrator::run``, :276-694), at
+    constant volume otherwise, and SLLOD planar Couette shear with
+    Lees-Edwards images when the configuration asks for it (testMode 2,
+    ``rate``).  ``start()`` computes F(0) and the chain's starting kinetic
+    energy."""
 
     thermostat_kind = L.THERMO_NH_CHAIN
+
+    def box(self):
+        """Current box edges (nm)."""
+        out = np.zeros(3)
+        L.check(self.ens.ctx, self.ens.lib.smd_get_box(self.ens.ctx, L.dptr(out)))
+        return out
+
+    def barostat_state(self):
+        """(vlog, molVirt, volume) after the last step."""
+        scal = np.zeros(32)
+        L.check(self.ens.ctx, self.ens.lib.smd_get_integrator_state(self.ens.ctx, L.dptr(scal)))
+        return float(scal[17]), float(scal[18]), float(scal[21])
+
+    def chain_state(self):
+        """The four chain velocities vnh after the last step."""
+        scal = np.zeros(32)
+        L.check(self.ens.ctx, self.ens.lib.smd_get_integrator_state(self.ens.ctx, L.dptr(scal)))
+        return scal[8:12].copy()
 
 
 class BuffvdWForce(GpuForce):

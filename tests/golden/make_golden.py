@@ -52,6 +52,21 @@ def polwater216():
     return s, [("forces",), ("run", 10)]
 
 
+def lj500_npt():
+    # NHIntegrator's NpT run (chain + isotropic barostat, Lustig virial
+    # pressure) near the state's own pressure; 25 steps of 4 fs keep every
+    # atom within half the skin of the start's list, which the reference's
+    # NpT loop never rebuilds.  The tail correction is recomputed at every
+    # step's volume (with the checker build's zero start of its accumulator)
+    s = systems.lj_fluid(ncell=5, jitter_star=0.05, seed=3, n_steps=25)
+    c = s.config
+    c.long_correct = True
+    c.ensemble, c.pressure, c.baros_const, c.coupl_const = 1, -240.0, 1.0, 0.5
+    c.lustig = True
+    c.timestep = 0.004
+    return s, [("forces",), ("nhrun", 25)]
+
+
 def polwater216_nve():
     # the same water without thermostat: energy conservation of the model as
     # the reference integrates it (its total energy rises: the GPU run must
@@ -109,7 +124,7 @@ def ref_test_nvt():
     return s, [("forces",), ("run", 10)]
 
 
-CASES = {"lj500": lj500, "nacl1000_mie": nacl1000_mie, "spce512": spce512,
+CASES = {"lj500": lj500, "lj500_npt": lj500_npt, "nacl1000_mie": nacl1000_mie, "spce512": spce512,
          "polwater216": polwater216, "polwater216_nve": polwater216_nve, "ref_test_nvt": ref_test_nvt}
 LARGE = {"lj4000": lj4000, "lj4000_jitter": lj4000_jitter, "nacl8000_mie": nacl8000_mie, "spce2160": spce2160,
          "polwater4096": polwater4096}
@@ -143,6 +158,10 @@ def pack(name, s, results, large=False):
         for k, v in results["mie"].items():
             if k.startswith("mie_"):
                 out["m_" + k] = v
+    if "nhrun" in results:
+        for k, v in results["nhrun"].items():
+            if k.startswith("nh_"):
+                out[k] = v
     if "rdf" in results:
         for k, v in results["rdf"].items():
             if k.startswith("rdf_"):
@@ -164,7 +183,7 @@ def pack(name, s, results, large=False):
             for fn, key in (("config.txt", "case_config"), ("sysData.in", "case_sysdata"),
                             ("coordinate.in", "case_coords")):
                 out[key] = np.array(open(os.path.join(d, fn)).read())
-    if name.endswith("_nve"):
+    if name.endswith(("_nve", "_npt")):
         # the trajectory only: the forces of the start are polwater216's
         out = {k: v for k, v in out.items() if not k.startswith("f_") and k != "pairs"}
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
