@@ -59,6 +59,7 @@ enum {
     SMD_TERM_BOND = 128,     /* BondForce::compute() */
     SMD_TERM_ANGLE = 256,    /* AngleForce::compute() */
     SMD_TERM_UB = 512,       /* UreyBradleyForce::compute() */
+    SMD_TERM_WOLF = 1024,    /* WolfForce::compute() (energy into SMD_E_REAL) */
     SMD_TERM_ALL = 0xffff
 };
 
@@ -395,6 +396,16 @@ int smd_set_integrator(smd_ctx *ctx, const smd_integrator_params *p);
  * pressure as the reference does with computeLustig on.  Pair terms
  * (LJ, Mie, Buckingham) in FP64 only, without constraints; other set-ups
  * are refused at smd_integrator_start.  on = 0 switches it off. */
+/* Wolf summation of the point charges instead of Ewald (WolfForce,
+ * src/forces/WolfForce.cpp:100-260; computeWolf): every listed pair within
+ * the cutoff adds q_i q_j (erfc(a r)/r - erfc(a rc)/rc) to the energy and
+ * the force factor shifted by its value at the cutoff.  msite (n entries,
+ * or null): 1 where a site's charge sits on the displaced site of
+ * WolfForce::DummyPosition (the reference flags the type-1 site of every
+ * "WAT" molecule), d_op its distance from the molecule's second site in nm
+ * (R_OP over F_Length in the reference).  The charge term then runs as a
+ * second FP64 pass; without displaced sites it is fused into the pair pass. */
+int smd_set_wolf(smd_ctx *ctx, double alpha, double cutoff, const int *msite, double d_op);
 int smd_set_barostat(smd_ctx *ctx, double pressure, double baros_const, int on);
 /* Current box edges (the barostat's, when it runs). */
 int smd_get_box(smd_ctx *ctx, double *edges);

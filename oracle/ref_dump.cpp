@@ -50,6 +50,7 @@
 #include "forces/BuckinghamForce.h"
 #include "forces/BuffvdWForce.h"
 #include "forces/EwaldForce.h"
+#include "forces/WolfForce.h"
 #include "forces/Multipole.h"
 #include "forces/Induction.h"
 #include "forces/BondForce.h"
@@ -191,6 +192,12 @@ static int mode_forces(const char *out) {
         LJForce f(e);
         f.compute();
         dump_forces(e, "lj");
+    }
+    if (c->compute_wolf()) {
+        zero(e);
+        WolfForce f(e);
+        f.compute();
+        dump_forces(e, "wolf");
     }
     if (c->compute_ewald_force()) {
         zero(e);

@@ -240,8 +240,9 @@ int compute_forces_into(smd_ctx *x, uint32_t terms, double *dforce, double *forc
     c.list_valid = rebuild ? 1 : 0;
     CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));
     CK(cudaMemsetAsync(c.frc, 0, 3 * (size_t)c.n * sizeof(long long), c.stream));
-    const int save_vdw = c.vdw, save_ew = c.ewald_on;
+    const int save_vdw = c.vdw, save_ew = c.ewald_on, save_wolf = c.wolf_on;
     if (!(terms & SMD_TERM_VDW)) c.vdw = VDW_NONE;
+    if (!(terms & SMD_TERM_WOLF)) c.wolf_on = 0;
     bool want_real = (terms & SMD_TERM_EWALD_REAL) && c.ewald_on;
     bool want_long = (terms & SMD_TERM_EWALD_LONG) && c.ewald_on;
     c.ewald_on = want_real ? 1 : 0;
@@ -251,6 +252,7 @@ int compute_forces_into(smd_ctx *x, uint32_t terms, double *dforce, double *forc
         launch_surface(c, true, false, false);   // EwaldForce::compute adds its surface term
     }
     c.ewald_on = save_ew;
+    c.wolf_on = save_wolf;
     if (want_long) launch_recip(c);
     c.vdw = save_vdw;
     if (has_bonded(c))
@@ -341,7 +343,8 @@ void smd_destroy(smd_ctx *x) {
                     c.pind, c.cgw, c.cgs, c.cg_bar, c.vpos4, c.vfixq, c.fv, c.ind_rj, c.ind_rc, c.ind_cnt,
                     c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab, c.srec, c.phist, c.cg_blk,
                     c.upload4, c.fout, c.rc.kzr_d, c.rc.kcxy_d, c.rc.stab_d, c.rc.srec_d, c.bonds, c.angles,
-                    c.bond_par, c.angle_par, c.surf_part, c.surf_tot, c.rdf_hist, c.avg, c.wrap};
+                    c.bond_par, c.angle_par, c.surf_part, c.surf_tot, c.rdf_hist, c.avg, c.wrap,
+                    c.wolf_msite, c.wpos4, c.dbox};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -489,6 +492,33 @@ int smd_set_box(smd_ctx *x, double lx, double ly, double lz) {
     }
     if (c.dbox) CK(cudaMemcpy(c.dbox, &c.box, sizeof(Box), cudaMemcpyHostToDevice));
     return alloc_list(x);
+}
+
+int smd_set_wolf(smd_ctx *x, double alpha, double cutoff, const int *msite, double d_op) {
+    if (!x || !(alpha > 0) || !(cutoff > 0) || x->c.n == 0 || x->c.ewald_on)
+        return fail(x, SMD_ERR_ARG, "smd_set_wolf: set the topology first; alpha, cutoff > 0; not with Ewald");
+    Ctx &c = x->c;
+    std::vector<int> flag(c.n, 0);
+    int any = 0;
+    if (msite)
+        for (int i = 0; i < c.n; i++) {
+            flag[i] = msite[i] ? 1 : 0;
+            any |= flag[i];
+            if (flag[i] && c.h_mol_off[c.h_mol[i] + 1] - c.h_mol_off[c.h_mol[i]] != 3)
+                return fail(x, SMD_ERR_ARG, "smd_set_wolf: a displaced charge site needs a 3-site molecule");
+        }
+    if (any && !(d_op > 0)) return fail(x, SMD_ERR_ARG, "smd_set_wolf: d_op must be > 0");
+    CK(dalloc(&c.wolf_msite, (size_t)c.n));
+    CK(cudaMemcpy(c.wolf_msite, flag.data(), c.n * sizeof(int), cudaMemcpyHostToDevice));
+    if (any) CK(dalloc(&c.wpos4, (size_t)c.n));
+    c.wolf_on = 1;
+    c.wolf_alpha = alpha;
+    c.wolf_rc = cutoff;
+    c.wolf_d = d_op;
+    c.wolf_msites = any;
+    c.graph_dirty = 1;
+    touch(c);
+    return SMD_OK;
 }
 
 int smd_set_barostat(smd_ctx *x, double pressure, double baros_const, int on) {
@@ -1337,7 +1367,7 @@ static int integrator_begin(smd_ctx *x, bool new_start) {
         // their k-vectors of one box), no constraints (the reference stops
         // there too, NHIntegrator.cpp:604-607), FP64
         if (c.ip.thermostat != SMD_THERMO_NH_CHAIN || c.ip.strain_rate != 0.0 || c.ewald_on || c.mp_on ||
-            has_bonded(c) || c.precision != SMD_PREC_FP64 || c.vdw == VDW_BUFF)
+            has_bonded(c) || c.precision != SMD_PREC_FP64 || c.vdw == VDW_BUFF || c.wolf_on)
             return fail(x, SMD_ERR_ARG,
                         "smd_integrator_start: the barostat runs with the chain integrator on pair terms in FP64");
         CK(cudaMemcpy(c.dbox, &c.box, sizeof(Box), cudaMemcpyHostToDevice));

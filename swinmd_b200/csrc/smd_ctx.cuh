@@ -185,6 +185,12 @@ struct Ctx {
     double vdw_rc2 = 1.0, sw_rs2 = 0.0, sw_c1 = 0, sw_c2 = 0, sw_c3 = 0;
     int switch_on = 0;
     double e_lrc = 0, v_lrc = 0;
+    // Wolf summation of the charges (WolfForce)
+    int wolf_on = 0;
+    double wolf_alpha = 0, wolf_rc = 0, wolf_d = 0;
+    int wolf_msites = 0;            // some charge sits on a displaced site
+    int *wolf_msite = nullptr;      // per site: 1 if its charge is displaced
+    double4 *wpos4 = nullptr;       // charge-site positions
     // isotropic barostat of the chain integrator (NHIntegrator's NpT run)
     int npt = 0;
     double npt_press = 0;           // target pressure, kJ/mol/nm^3

@@ -50,6 +50,10 @@ struct PairArgs {
     int buff_int;       // n - m and m are small positive integers
     const double *le;   // Lees-Edwards offset on the device (planar shear), or null
     const Box *dbox;    // the box on the device (barostat, FP64 path), or null: box
+    // Wolf summation (WolfForce::real_term): the charge term's energy and
+    // force shifts at the cutoff (0 for Ewald)
+    double wolf_e, wolf_f;
+    int second;         // a pass after another pair pass: add forces, count no pairs
     long long *frc;
     long long *acc;
 };
@@ -393,15 +397,15 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_pair(PairArgs a) {
             else
                 vdw_pair<R, VDW>(r2, e, fs, &s_par[(ti * a.ntypes + tj) * 4], a, same);
             evdw += e;
-            npair += (r2 <= R(a.vdw_rc2) || (EWALD && r2 < R(a.ew_rc2))) ? 1 : 0;
+            npair += (!a.second && (r2 <= R(a.vdw_rc2) || (EWALD && r2 < R(a.ew_rc2)))) ? 1 : 0;
             if (EWALD) {
                 if (r2 < R(a.ew_rc2)) {
                     const R qij = qi * s_q[tj];
                     const R r = sqrt(r2);
                     const R ee = erfc(R(a.alpha) * r) / r;
                     const R ff = (ee + R(a.alpha2pi) * exp(-R(a.alpha2) * r2)) / r2;
-                    ereal += qij * ee;
-                    fs += qij * ff;
+                    ereal += qij * (ee - R(a.wolf_e));
+                    fs += qij * (ff - R(a.wolf_f));
                 }
             }
             const R fijx = -fs * dx, fijy = -fs * dy, fijz = -fs * dz;
@@ -416,9 +420,15 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_pair(PairArgs a) {
     fy = group_sum<TPP>(fy);
     fz = group_sum<TPP>(fz);
     if (i < a.n && t == 0) {
-        a.frc[i] = to_fix(fx, FRC_SCALE);
-        a.frc[a.n + i] = to_fix(fy, FRC_SCALE);
-        a.frc[2 * a.n + i] = to_fix(fz, FRC_SCALE);
+        if (a.second) {   // this thread owns site i's entries: a plain add
+            a.frc[i] += to_fix(fx, FRC_SCALE);
+            a.frc[a.n + i] += to_fix(fy, FRC_SCALE);
+            a.frc[2 * a.n + i] += to_fix(fz, FRC_SCALE);
+        } else {
+            a.frc[i] = to_fix(fx, FRC_SCALE);
+            a.frc[a.n + i] = to_fix(fy, FRC_SCALE);
+            a.frc[2 * a.n + i] = to_fix(fz, FRC_SCALE);
+        }
     }
     // energies and virial: warp, then block, then one fixed-point atomic each
     double v[8] = {(double)evdw, (double)ereal, (double)vxx, (double)vxy,
@@ -640,6 +650,27 @@ __global__ void k_fixq(int n, const double4 *pos4, int4 *fixq, Box b) {
                         (int)p.w);
 }
 
+// Charge sites of the Wolf summation (WolfForce::DummyPosition,
+// src/forces/WolfForce.cpp:60-80): a flagged site (the O of a "WAT"
+// molecule) carries its charge at r_2 + d (r_mid - r_2)/|r_mid - r_2|, with
+// r_2 the molecule's second site, r_mid the midpoint of its first and third
+// and d the reference's R_OP in nm; other sites stay.  The displacement is
+// taken without minimum image, as the reference takes it.
+__global__ void k_wolf_sites(int n, const int *mol, const int *mol_off, const int *mol_atoms, const int *msite,
+                             const double4 *pos4, double d, double4 *vpos4) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 p = pos4[i];
+    if (msite[i]) {
+        const int s0 = mol_off[mol[i]];
+        const double4 a = pos4[mol_atoms[s0]], o = pos4[mol_atoms[s0 + 1]], b = pos4[mol_atoms[s0 + 2]];
+        const double rx = 0.5 * (b.x + a.x) - o.x, ry = 0.5 * (b.y + a.y) - o.y, rz = 0.5 * (b.z + a.z) - o.z;
+        const double f = d / sqrt(rx * rx + ry * ry + rz * rz);
+        p.x = o.x + f * rx; p.y = o.y + f * ry; p.z = o.z + f * rz;
+    }
+    vpos4[i] = p;
+}
+
 // Virtual sites of the buffered 14-7 term (BuffvdWForce::VirtualPositions,
 // src/forces/BuffvdWForce.cpp:358-385): a type-0 (H) site moves to
 // f r_H + (1 - f) r_O, with O the molecule's second site; others stay.
@@ -695,6 +726,17 @@ void launch_fixq(Ctx &c) {
     k_fixq<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.pos4, c.fixq, c.box);
 }
 
+// WolfForce::real_term's shifts: e(rc) = erfc(a rc)/rc and the force term
+// (e(rc)/rc + 2a/sqrt(pi) exp(-a^2 rc^2)/rc)/rc, subtracted from every pair's
+// energy and force factor
+static void wolf_shifts(const Ctx &c, double &we, double &wf) {
+    const double rc = c.wolf_rc, al = c.wolf_alpha;
+    const double eR = erfc(al * rc) / rc;
+    const double Rc = eR / rc + 2.0 * al / 1.7724538509055160273 * exp(-al * al * rc * rc) / rc;
+    we = eR;
+    wf = Rc / rc;
+}
+
 void launch_pair(Ctx &c) {
     PairArgs a;
     a.n = c.n; a.max_nbr = c.pl.max_nbr; a.ntypes = c.ntypes;
@@ -713,6 +755,17 @@ void launch_pair(Ctx &c) {
     a.frc = c.frc; a.acc = c.acc;
     a.le = c.ip.strain_rate != 0.0 && c.integrator_ready ? c.scal + SC_LE : nullptr;
     a.dbox = c.npt ? c.dbox : nullptr;
+    a.wolf_e = a.wolf_f = 0.0;
+    a.second = 0;
+    // Wolf in the pair pass itself when every charge sits on its atom
+    const bool wolf_here = c.wolf_on && !c.wolf_msites;
+    if (wolf_here) {
+        a.alpha = c.wolf_alpha; a.alpha2 = c.wolf_alpha * c.wolf_alpha;
+        a.alpha2pi = 2.0 * c.wolf_alpha / 1.7724538509055160273;
+        a.ew_rc2 = c.wolf_rc * c.wolf_rc;
+        wolf_shifts(c, a.wolf_e, a.wolf_f);
+    }
+    const bool elec = c.ewald_on || wolf_here;
     a.bn = c.buff_n; a.bm = c.buff_m; a.bdelta = c.buff_delta; a.bgamma = c.buff_gamma;
     for (int q = 0; q < 6; q++) a.bc[q] = c.buff_c[q];
     a.bsw2 = c.buff_sw * c.buff_sw;
@@ -742,7 +795,7 @@ void launch_pair(Ctx &c) {
             k_buff_d<8, 0, 0><<<nb, PAIR_BLOCK, 0, c.stream>>>(a);
     } else if (c.precision == SMD_PREC_MIXED) {
         if (!c.fixq_from_integrate) launch_fixq(c);
-        if (c.ewald_on) dispatch_vdw<float, true>(c, a);
+        if (elec) dispatch_vdw<float, true>(c, a);
         else dispatch_vdw<float, false>(c, a);
     } else if (buff && a.buff_int && !c.ewald_on && !a.le && !c.reference_forms) {
         // FP64 path, integer exponents: the same product-form pass on the
@@ -753,8 +806,25 @@ void launch_pair(Ctx &c) {
         else
             k_buff_d<8, 0, 0, false><<<nb, PAIR_BLOCK, 0, c.stream>>>(a);
     } else {
-        if (c.ewald_on) dispatch_vdw<double, true>(c, a);
+        if (elec) dispatch_vdw<double, true>(c, a);
         else dispatch_vdw<double, false>(c, a);
+    }
+    if (c.wolf_on && c.wolf_msites) {
+        // charges on displaced sites: a second FP64 pass of the charge term
+        // alone over the same list, on the charge sites' positions, adding
+        // its forces to the atoms that own them (the reference applies a
+        // displaced site's force to its atom unchanged)
+        k_wolf_sites<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.mol, c.mol_off, c.mol_atoms, c.wolf_msite,
+                                                               c.pos4, c.wolf_d, c.wpos4);
+        PairArgs w = a;
+        w.pos4 = c.wpos4;
+        w.frc = c.frc;
+        w.alpha = c.wolf_alpha; w.alpha2 = c.wolf_alpha * c.wolf_alpha;
+        w.alpha2pi = 2.0 * c.wolf_alpha / 1.7724538509055160273;
+        w.ew_rc2 = c.wolf_rc * c.wolf_rc;
+        wolf_shifts(c, w.wolf_e, w.wolf_f);
+        w.second = 1;
+        dispatch_tpp<double, VDW_NONE, true>(c, w);
     }
     if (buff)
         k_buff_distribute<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.mol, c.mol_off, c.mol_atoms, c.pos4,

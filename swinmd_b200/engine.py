@@ -212,19 +212,25 @@ def buff_long_range_correction(s: System, box: float) -> tuple:
 # the GPU system
 # ---------------------------------------------------------------------------
 
+# R_OP / F_Length of WolfForce.h:38, 45, 51 (0.505783 Bohr in nm)
+WOLF_R_OP_NM = 0.505783 / (1.0e-9 / 5.29189379e-11)
+
+
 def refuse_unsupported(c) -> None:
     """Raises for configuration options the GPU path does not compute, so a
     caller never gets different physics with a success status: the AMOEBA
     damping branch of the induced real space (``dampAMOEBA``,
-    Induction.cpp:1051-1079) and the Wolf summation (WolfForce.cpp)."""
+    Induction.cpp:1051-1079) and Wolf with another electrostatic method."""
     if c.compute_ub and c.constraint:
         # Integrator::initialise refuses the same combination (src/Integrator.cpp:178-187)
         raise NotImplementedError("a flexible Urey-Bradley term with constraints")
     if c.compute_multipole and c.compute_induction and c.damp_amoeba:
         raise NotImplementedError("AMOEBA damping of the induced real space (dampAMOEBA) is not built on "
                                   "the GPU path")
-    if c.compute_wolf:
-        raise NotImplementedError("Wolf summation (computeWolf) is not built on the GPU path")
+    if c.compute_wolf and (c.compute_ewald or c.compute_multipole):
+        # the reference stops on more than one electrostatic method
+        # (LFIntegrator.cpp:1027, 1058)
+        raise NotImplementedError("Wolf together with Ewald or multipoles")
 
 
 class GpuEnsemble:
@@ -260,6 +266,13 @@ class GpuEnsemble:
         self._setup_vdw()
         if c.compute_ewald:
             self._chk(self.lib.smd_set_ewald(ctx, c.alpha, c.k_cutoff, c.cutoff))
+        elif c.compute_wolf:
+            # WolfForce: the type-1 site of a "WAT" molecule carries its charge
+            # R_OP (in Bohr, WolfForce.h:38) along the bisector
+            names = [s.mol_type_names[t][0] for t in s.mol_type]
+            msite = np.ascontiguousarray([1 if names[s.mol_id[i]] == "WAT" and s.atom_type[i] == 1 else 0
+                                          for i in range(s.n_atoms)], np.int32)
+            self._chk(self.lib.smd_set_wolf(ctx, c.alpha, c.cutoff, L.iptr(msite), WOLF_R_OP_NM))
         if c.constraint == 2:
             from .systems import constraint_lengths
             cl = np.ascontiguousarray(constraint_lengths(s).reshape(-1))

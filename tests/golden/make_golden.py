@@ -67,6 +67,21 @@ def lj500_npt():
     return s, [("forces",), ("nhrun", 25)]
 
 
+def spce512_wolf():
+    # Wolf summation instead of Ewald; the O charge of every "WAT" molecule
+    # sits on WolfForce's displaced site
+    s = systems.spce_water(nmol=512, box=2.4953, cutoff=0.9, kmax=6, seed=11)
+    s.config.compute_ewald, s.config.compute_wolf, s.config.alpha = False, True, 2.0
+    return s, [("forces",)]
+
+
+def nacl1000_wolf():
+    # ions (no displaced sites): the charge term fused into the pair pass
+    s = systems.nacl_melt(ncell=10, potential="mie", kmax=6, seed=5)
+    s.config.compute_ewald, s.config.compute_wolf, s.config.alpha = False, True, 2.5
+    return s, [("forces",)]
+
+
 def polwater216_nve():
     # the same water without thermostat: energy conservation of the model as
     # the reference integrates it (its total energy rises: the GPU run must
@@ -125,7 +140,7 @@ def ref_test_nvt():
 
 
 CASES = {"lj500": lj500, "lj500_npt": lj500_npt, "nacl1000_mie": nacl1000_mie, "spce512": spce512,
-         "polwater216": polwater216, "polwater216_nve": polwater216_nve, "ref_test_nvt": ref_test_nvt}
+         "polwater216": polwater216, "spce512_wolf": spce512_wolf, "nacl1000_wolf": nacl1000_wolf, "polwater216_nve": polwater216_nve, "ref_test_nvt": ref_test_nvt}
 LARGE = {"lj4000": lj4000, "lj4000_jitter": lj4000_jitter, "nacl8000_mie": nacl8000_mie, "spce2160": spce2160,
          "polwater4096": polwater4096}
 
@@ -183,6 +198,9 @@ def pack(name, s, results, large=False):
             for fn, key in (("config.txt", "case_config"), ("sysData.in", "case_sysdata"),
                             ("coordinate.in", "case_coords")):
                 out[key] = np.array(open(os.path.join(d, fn)).read())
+    if name.endswith("_wolf"):
+        out = {k: v for k, v in out.items() if not k.startswith("f_") or k.startswith("f_wolf_")}
+        out.pop("pairs", None)
     if name.endswith(("_nve", "_npt")):
         # the trajectory only: the forces of the start are polwater216's
         out = {k: v for k, v in out.items() if not k.startswith("f_") and k != "pairs"}

@@ -11,6 +11,7 @@ def _pw():
 
 @pytest.mark.parametrize("field", ["damp_amoeba", "compute_wolf"])
 def test_unsupported_options_refused(field):
+    # (Wolf is built, but not together with the multipoles)
     s = _pw()
     setattr(s.config, field, True)
     with pytest.raises(NotImplementedError):
