@@ -84,7 +84,7 @@ enum {
 };
 
 /* vdW kinds for smd_set_vdw */
-enum { SMD_VDW_NONE = 0, SMD_VDW_LJ = 1, SMD_VDW_MIE = 2, SMD_VDW_BMH = 3, SMD_VDW_BUFF = 4 };
+enum { SMD_VDW_NONE = 0, SMD_VDW_LJ = 1, SMD_VDW_MIE = 2, SMD_VDW_BMH = 3, SMD_VDW_BUFF = 4, SMD_VDW_SAAP = 5 };
 
 /* initial guess of the induced-dipole solve (no reference counterpart: the
  * reference starts its CG from p = 1, src/forces/Induction.cpp:2401-2467) */
@@ -405,6 +405,13 @@ int smd_set_integrator(smd_ctx *ctx, const smd_integrator_params *p);
  * "WAT" molecule), d_op its distance from the molecule's second site in nm
  * (R_OP over F_Length in the reference).  The charge term then runs as a
  * second FP64 pass; without displaced sites it is fused into the pair pass. */
+/* SAAP pair potential (SAAPForce::compute, src/forces/SAAPForce.cpp:54-230)
+ * as the vdW term: U = (a0 e^(a1 r)/r + a2 e^(a3 r) + a4) / (1 + a5 r^6)
+ * between sites of different molecules within the cutoff, with the
+ * reference's 5th-order switch as SAAPForce applies it.  table: ntypes^2
+ * rows of (a0, a1, a2, a3, a4, a5).  No tail correction (the reference's is
+ * for its three-type CO2 table only). */
+int smd_set_saap(smd_ctx *ctx, const double *table, int switch_on, double switch_dist2);
 int smd_set_wolf(smd_ctx *ctx, double alpha, double cutoff, const int *msite, double d_op);
 int smd_set_barostat(smd_ctx *ctx, double pressure, double baros_const, int on);
 /* Current box edges (the barostat's, when it runs). */

@@ -11,6 +11,7 @@
 //     ref_dump run <nsteps> <out>  LFIntegrator::start() then nsteps x run(1)
 //     ref_dump mie <out>           MieForce::compute() on its own
 //     ref_dump buck <out>          BuckinghamForce::compute() on its own
+//     ref_dump saap <out>          SAAPForce::compute() on its own (three atom types)
 //     ref_dump rdf <out>           one RDF::sampling() of the configuration
 //     ref_dump nhrun <nsteps> <out> NHIntegrator::start() then nsteps x run(1)
 //
@@ -48,6 +49,7 @@
 #include "forces/LJForce.h"
 #include "forces/MieForce.h"
 #include "forces/BuckinghamForce.h"
+#include "forces/SAAPForce.h"
 #include "forces/BuffvdWForce.h"
 #include "forces/EwaldForce.h"
 #include "forces/WolfForce.h"
@@ -283,6 +285,22 @@ static int mode_single(const char *which, const char *out) {
         MieForce f(e);
         f.compute();
         dump_forces(e, "mie");
+    } else if (!strcmp(which, "saap")) {
+        // SAAPForce with its built-in three-type table (SAAPForce.h); the
+        // table is recorded so that the GPU side runs the same parameters
+        SAAPForce f(e);
+        f.compute();
+        dump_forces(e, "saap");
+        std::vector<double> tab;
+// (WolfForce.h defines a macro of the first field's name)
+#pragma push_macro("Aa0")
+#undef Aa0
+        for (int k = 0; k < e->nAtomTypes * e->nAtomTypes; k++) {
+            const SAAPParam &q = f.saapParams[k];
+            for (double v : {q.Aa0, q.Aa1, q.Aa2, q.Aa3, q.Aa4, q.Aa5}) tab.push_back(v);
+        }
+#pragma pop_macro("Aa0")
+        rec("saap_params", tab);
     } else {
         BuckinghamForce f(e);
         f.compute();
@@ -418,7 +436,8 @@ int main(int argc, char **argv) {
         return 2;
     }
     if (!strcmp(argv[1], "forces")) return mode_forces(argv[2]);
-    if (!strcmp(argv[1], "mie") || !strcmp(argv[1], "buck")) return mode_single(argv[1], argv[2]);
+    if (!strcmp(argv[1], "mie") || !strcmp(argv[1], "buck") || !strcmp(argv[1], "saap"))
+        return mode_single(argv[1], argv[2]);
     if (!strcmp(argv[1], "run") && argc >= 4) return mode_run(atoi(argv[2]), argv[3]);
     if (!strcmp(argv[1], "rdf")) return mode_rdf(argv[2]);
     if (!strcmp(argv[1], "nhrun") && argc >= 4) return mode_nhrun(atoi(argv[2]), argv[3]);

@@ -344,7 +344,7 @@ void smd_destroy(smd_ctx *x) {
                     c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab, c.srec, c.phist, c.cg_blk,
                     c.upload4, c.fout, c.rc.kzr_d, c.rc.kcxy_d, c.rc.stab_d, c.rc.srec_d, c.bonds, c.angles,
                     c.bond_par, c.angle_par, c.surf_part, c.surf_tot, c.rdf_hist, c.avg, c.wrap,
-                    c.wolf_msite, c.wpos4, c.dbox};
+                    c.wolf_msite, c.wpos4, c.dbox, c.saap};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -492,6 +492,25 @@ int smd_set_box(smd_ctx *x, double lx, double ly, double lz) {
     }
     if (c.dbox) CK(cudaMemcpy(c.dbox, &c.box, sizeof(Box), cudaMemcpyHostToDevice));
     return alloc_list(x);
+}
+
+int smd_set_saap(smd_ctx *x, const double *table, int switch_on, double switch_dist2) {
+    if (!x || !table || x->c.ntypes == 0) return fail(x, SMD_ERR_ARG, "smd_set_saap: set the topology first");
+    Ctx &c = x->c;
+    const int nt = c.ntypes;
+    for (int k = 0; k < 6 * nt * nt; k++)
+        if (!std::isfinite(table[k])) return fail(x, SMD_ERR_NAN, "smd_set_saap: non-finite parameter");
+    // the switch constants as smd_set_vdw forms them (no parameters of its own)
+    int r = smd_set_vdw(x, SMD_VDW_NONE, nullptr, switch_on, switch_dist2, 0.0, 0.0);
+    if (r) return r;
+    CK(dalloc(&c.saap, (size_t)6 * nt * nt));
+    CK(cudaMemcpy(c.saap, table, (size_t)6 * nt * nt * sizeof(double), cudaMemcpyHostToDevice));
+    c.vdw = VDW_SAAP;
+    // with the switch off the kernel never reads sw_rs2; with it on,
+    // smd_set_vdw has set it for a non-LJ kind
+    c.graph_dirty = 1;
+    touch(c);
+    return SMD_OK;
 }
 
 int smd_set_wolf(smd_ctx *x, double alpha, double cutoff, const int *msite, double d_op) {
@@ -1367,7 +1386,8 @@ static int integrator_begin(smd_ctx *x, bool new_start) {
         // their k-vectors of one box), no constraints (the reference stops
         // there too, NHIntegrator.cpp:604-607), FP64
         if (c.ip.thermostat != SMD_THERMO_NH_CHAIN || c.ip.strain_rate != 0.0 || c.ewald_on || c.mp_on ||
-            has_bonded(c) || c.precision != SMD_PREC_FP64 || c.vdw == VDW_BUFF || c.wolf_on)
+            has_bonded(c) || c.precision != SMD_PREC_FP64 || c.vdw == VDW_BUFF || c.vdw == VDW_SAAP ||
+            c.wolf_on)
             return fail(x, SMD_ERR_ARG,
                         "smd_integrator_start: the barostat runs with the chain integrator on pair terms in FP64");
         CK(cudaMemcpy(c.dbox, &c.box, sizeof(Box), cudaMemcpyHostToDevice));

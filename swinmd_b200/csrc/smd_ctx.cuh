@@ -10,7 +10,7 @@
 
 namespace smd {
 
-enum VdwKind { VDW_NONE = 0, VDW_LJ = 1, VDW_MIE = 2, VDW_BMH = 3, VDW_BUFF = 4 };
+enum VdwKind { VDW_NONE = 0, VDW_LJ = 1, VDW_MIE = 2, VDW_BMH = 3, VDW_BUFF = 4, VDW_SAAP = 5 };
 
 // surface-correction reduction: blocks of partial sums and sums per block
 constexpr int CG_SCAL = 8;     // iterations, final RMS change, ...
@@ -185,6 +185,7 @@ struct Ctx {
     double vdw_rc2 = 1.0, sw_rs2 = 0.0, sw_c1 = 0, sw_c2 = 0, sw_c3 = 0;
     int switch_on = 0;
     double e_lrc = 0, v_lrc = 0;
+    double *saap = nullptr;         // SAAP pair parameters a0..a5 per type pair
     // Wolf summation of the charges (WolfForce)
     int wolf_on = 0;
     double wolf_alpha = 0, wolf_rc = 0, wolf_d = 0;

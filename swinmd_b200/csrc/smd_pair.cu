@@ -54,6 +54,7 @@ struct PairArgs {
     // force shifts at the cutoff (0 for Ewald)
     double wolf_e, wolf_f;
     int second;         // a pass after another pair pass: add forces, count no pairs
+    const double *saap; // SAAP a0..a5 per type pair
     long long *frc;
     long long *acc;
 };
@@ -140,6 +141,35 @@ __device__ __forceinline__ void vdw_pair(R r2, R &e, R &fs, const R *p, const Pa
                 e *= sv;
             }
         }
+    }
+}
+
+// SAAPForce::compute (src/forces/SAAPForce.cpp:140-200): with N = a0 e^(a1 r)/r
+// + a2 e^(a3 r) + a4 and D = 1 + a5 r^6, U = N/D and the reference's tmpf =
+// U'/r; it takes r_ij = r_i - r_j, so in this kernel's convention (f_ij =
+// -fs (r_j - r_i)) fs = -tmpf, and its switch, tmpf s - U ds, becomes
+// fs s + U ds.
+template <typename R>
+__device__ __forceinline__ void saap_pair(R r2, R &e, R &fs, const double *q, const PairArgs &a, bool same) {
+    e = R(0);
+    fs = R(0);
+    if (same || !(r2 <= R(a.vdw_rc2))) return;
+    const R a0 = R(q[0]), a1 = R(q[1]), a2 = R(q[2]), a3 = R(q[3]), a4 = R(q[4]), a5 = R(q[5]);
+    const R r = sqrt(r2), r_1 = R(1) / r, rij_2 = r_1 * r_1;
+    const R ex1 = exp(a1 * r), ex3 = exp(a3 * r);
+    const R num = a0 * r_1 * ex1 + a2 * ex3 + a4;
+    const R den = R(1) + a5 * r2 * r2 * r2;
+    e = num / den;
+    const R tmpf = (-a0 * rij_2 * ex1 + a0 * a1 * r_1 * ex1 + a2 * a3 * ex3) * r_1 / den -
+                   R(6) * a5 * r2 * r2 * num / (den * den);
+    fs = -tmpf;
+    if (a.switch_on && r2 > R(a.sw_rs2)) {
+        const R c = R(a.vdw_rc2) - r2;
+        const R c4 = c * (R(2) * r2 + R(a.sw_c2));
+        const R sv = c * c4 * R(a.sw_c1);
+        const R dsv = R(a.sw_c3) * (c * c - c4);
+        fs = fs * sv + e * dsv;
+        e *= sv;
     }
 }
 
@@ -394,6 +424,8 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_pair(PairArgs a) {
             else if (sizeof(R) == 4 && (VDW == VDW_MIE || VDW == VDW_BMH))
                 vdw_pair_f<VDW>((float)r2, r2c, *(float *)&e, *(float *)&fs,
                                 (const float *)&s_par[(ti * a.ntypes + tj) * 4], a, same);
+            else if (VDW == VDW_SAAP)
+                saap_pair<R>(r2, e, fs, a.saap + (size_t)(ti * a.ntypes + tj) * 6, a, same);
             else
                 vdw_pair<R, VDW>(r2, e, fs, &s_par[(ti * a.ntypes + tj) * 4], a, same);
             evdw += e;
@@ -637,6 +669,7 @@ static void dispatch_vdw(Ctx &c, const PairArgs &a) {
         case VDW_MIE: dispatch_tpp<R, VDW_MIE, EWALD>(c, a); break;
         case VDW_BMH: dispatch_tpp<R, VDW_BMH, EWALD>(c, a); break;
         case VDW_BUFF: dispatch_tpp<R, VDW_BUFF, EWALD>(c, a); break;
+        case VDW_SAAP: dispatch_tpp<R, VDW_SAAP, EWALD>(c, a); break;
         default: dispatch_tpp<R, VDW_NONE, EWALD>(c, a); break;
     }
 }
@@ -757,6 +790,7 @@ void launch_pair(Ctx &c) {
     a.dbox = c.npt ? c.dbox : nullptr;
     a.wolf_e = a.wolf_f = 0.0;
     a.second = 0;
+    a.saap = c.saap;
     // Wolf in the pair pass itself when every charge sits on its atom
     const bool wolf_here = c.wolf_on && !c.wolf_msites;
     if (wolf_here) {

@@ -337,6 +337,15 @@ class GpuEnsemble:
         instead of the product form and the column passes."""
         self._chk(self.lib.smd_set_reference_forms(self.ctx, int(bool(on))))
 
+    def set_saap(self, table: np.ndarray, switch_on: bool = False, switch_dist: float = 0.0):
+        """The SAAP pair potential as the vdW term (SAAPForce): table rows
+        (a0 .. a5) per type pair, ntypes^2 of them."""
+        t = np.ascontiguousarray(table, np.float64).reshape(-1)
+        nt = len(self.system.atom_types)
+        if t.size != 6 * nt * nt:
+            raise ValueError(f"set_saap: {nt * nt} rows of 6 parameters expected")
+        self._chk(self.lib.smd_set_saap(self.ctx, L.dptr(t), int(switch_on), float(switch_dist) ** 2))
+
     def set_precision(self, precision: str):
         self.precision = precision
         self._chk(self.lib.smd_set_precision(self.ctx, L.PREC_MIXED if precision == "mixed" else L.PREC_FP64))

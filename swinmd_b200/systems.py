@@ -471,6 +471,18 @@ def nacl_bmh_tables():
     return {"A": A, "rho": np.full((2, 2), _TF_RHO), "C": C, "D": D}
 
 
+def three_type_fluid(ncell: int = 5, seed: int = 3) -> System:
+    """The jittered LJ lattice with its atoms cycled over three types of
+    equal parameters (O, C, B): a system for pair potentials whose tables
+    are written for three types, such as the reference's SAAP table."""
+    s = lj_fluid(ncell=ncell, jitter_star=0.05, seed=seed)
+    base = s.atom_types[0]
+    s.atom_types = [AtomType(base.mass, 0.0, base.eps, base.sigma, name=nm, long_name=nm) for nm in ("O", "C", "B")]
+    s.atom_type = (np.arange(s.n_atoms) % 3).astype(np.int32)
+    s.name = f"tri{s.n_atoms}"
+    return s
+
+
 def nacl_melt(ncell: int = 20, density_gcc: float = 1.55, temperature: float = 1200.0,
               seed: int = 1, jitter: float = 0.02, cutoff: float = 1.1, skin: float = 0.1,
               alpha: float = 2.8, kmax: int = 10, potential: str = "bmh",

@@ -82,6 +82,12 @@ def nacl1000_wolf():
     return s, [("forces",)]
 
 
+def saap500():
+    # SAAPForce with the reference's own three-type table
+    s = systems.three_type_fluid(ncell=5, seed=3)
+    return s, [("forces",), ("saap",)]
+
+
 def polwater216_nve():
     # the same water without thermostat: energy conservation of the model as
     # the reference integrates it (its total energy rises: the GPU run must
@@ -140,7 +146,7 @@ def ref_test_nvt():
 
 
 CASES = {"lj500": lj500, "lj500_npt": lj500_npt, "nacl1000_mie": nacl1000_mie, "spce512": spce512,
-         "polwater216": polwater216, "spce512_wolf": spce512_wolf, "nacl1000_wolf": nacl1000_wolf, "polwater216_nve": polwater216_nve, "ref_test_nvt": ref_test_nvt}
+         "polwater216": polwater216, "spce512_wolf": spce512_wolf, "saap500": saap500, "nacl1000_wolf": nacl1000_wolf, "polwater216_nve": polwater216_nve, "ref_test_nvt": ref_test_nvt}
 LARGE = {"lj4000": lj4000, "lj4000_jitter": lj4000_jitter, "nacl8000_mie": nacl8000_mie, "spce2160": spce2160,
          "polwater4096": polwater4096}
 
@@ -173,6 +179,10 @@ def pack(name, s, results, large=False):
         for k, v in results["mie"].items():
             if k.startswith("mie_"):
                 out["m_" + k] = v
+    if "saap" in results:
+        for k, v in results["saap"].items():
+            if k.startswith("saap_"):
+                out["s_" + k] = v
     if "nhrun" in results:
         for k, v in results["nhrun"].items():
             if k.startswith("nh_"):
@@ -198,6 +208,9 @@ def pack(name, s, results, large=False):
             for fn, key in (("config.txt", "case_config"), ("sysData.in", "case_sysdata"),
                             ("coordinate.in", "case_coords")):
                 out[key] = np.array(open(os.path.join(d, fn)).read())
+    if name.startswith("saap"):
+        out = {k: v for k, v in out.items() if not k.startswith("f_")}
+        out.pop("pairs", None)
     if name.endswith("_wolf"):
         out = {k: v for k, v in out.items() if not k.startswith("f_") or k.startswith("f_wolf_")}
         out.pop("pairs", None)
