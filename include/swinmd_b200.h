@@ -411,6 +411,12 @@ int smd_set_integrator(smd_ctx *ctx, const smd_integrator_params *p);
  * reference's 5th-order switch as SAAPForce applies it.  table: ntypes^2
  * rows of (a0, a1, a2, a3, a4, a5).  No tail correction (the reference's is
  * for its three-type CO2 table only). */
+/* Lustig's volume derivatives of the LJ term at the current positions
+ * (LJForce::compute with computeLustig: Ensemble::myLustig.ljUlus, ljdUlus,
+ * ljd2Ulus, src/forces/LJForce.cpp:136-150, 230-247): out[0] = U, out[1] =
+ * dU/dV, out[2] = d2U/dV2, tail correction included; under constraints the
+ * pair term takes r_ij . R_ij with R_ij the molecules' centre difference. */
+int smd_lustig_lj(smd_ctx *ctx, double *out);
 int smd_set_saap(smd_ctx *ctx, const double *table, int switch_on, double switch_dist2);
 int smd_set_wolf(smd_ctx *ctx, double alpha, double cutoff, const int *msite, double d_op);
 int smd_set_barostat(smd_ctx *ctx, double pressure, double baros_const, int on);

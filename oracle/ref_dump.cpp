@@ -194,6 +194,10 @@ static int mode_forces(const char *out) {
         LJForce f(e);
         f.compute();
         dump_forces(e, "lj");
+        if (c->compute_lustig()) {
+            const Lustig &L = e->myLustig;
+            rec("lustig_lj", std::vector<double>{L.ljUlus, L.ljdUlus, L.ljd2Ulus});
+        }
     }
     if (c->compute_wolf()) {
         zero(e);
@@ -327,7 +331,7 @@ static int mode_run(int nsteps, const char *out) {
         rec("start_vtminus", vm);
     }
     std::vector<double> epot, ekin, atemp, zeta, press, nupd;
-    std::vector<double> ptensor, mtensor;
+    std::vector<double> ptensor, mtensor, lus;
     double run_seconds = 0.0;
     for (int k = 0; k < nsteps; k++) {
         timespec t0, t1;
@@ -335,6 +339,13 @@ static int mode_run(int nsteps, const char *out) {
         lf->run(1);
         clock_gettime(CLOCK_MONOTONIC, &t1);
         run_seconds += (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec);
+        if (s.cfg->compute_lustig()) {
+            // the LJ term's Lustig values of this step's forces (evaluated
+            // at the positions the previous step left, with its centres)
+            const Lustig &L = e->myLustig;
+            for (double v : {L.ljUlus, L.ljdUlus, L.ljd2Ulus}) lus.push_back(v);
+            if (k == 0) dump_state(e, "step_after1");
+        }
         const Energy &E = e->myEnergy;
         epot.push_back(E.totEnergy);
         ekin.push_back(E.atomKinEnergy);
@@ -344,6 +355,7 @@ static int mode_run(int nsteps, const char *out) {
         for (int q = 0; q < 9; q++) ptensor.push_back(e->atomPressure[q]);
         for (int q = 0; q < 9; q++) mtensor.push_back(e->molPressure[q]);
     }
+    if (!lus.empty()) rec("step_lustig", lus);
     rec("step_epot", epot);
     rec("step_ekin", ekin);
     rec("step_atomtemp", atemp);

@@ -494,6 +494,15 @@ int smd_set_box(smd_ctx *x, double lx, double ly, double lz) {
     return alloc_list(x);
 }
 
+int smd_lustig_lj(smd_ctx *x, double *out) {
+    if (!x || !out || x->c.vdw != VDW_LJ) return fail(x, SMD_ERR_ARG, "smd_lustig_lj: the vdW term is not LJ");
+    Ctx &c = x->c;
+    CK(cudaSetDevice(c.device));
+    int r = lustig_lj(c, out);
+    if (r) return fail(x, r, "smd_lustig_lj: evaluation failed");
+    return sync_status(x);
+}
+
 int smd_set_saap(smd_ctx *x, const double *table, int switch_on, double switch_dist2) {
     if (!x || !table || x->c.ntypes == 0) return fail(x, SMD_ERR_ARG, "smd_set_saap: set the topology first");
     Ctx &c = x->c;

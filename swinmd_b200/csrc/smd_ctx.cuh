@@ -312,6 +312,7 @@ int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed);
 void launch_mlp_guess(Ctx &c);
 void launch_first_order_guess(Ctx &c);
 void launch_blk_response(Ctx &c, double *out, int order, double *out_prev);
+int lustig_lj(Ctx &c, double *out);
 // order of the extrapolated guess of the solver's guess mode (0: none)
 inline int guess_order(const Ctx &c) {
     return c.cg_guess == SMD_GUESS_FIRST_ORDER ? 1

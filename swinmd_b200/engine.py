@@ -337,6 +337,13 @@ class GpuEnsemble:
         instead of the product form and the column passes."""
         self._chk(self.lib.smd_set_reference_forms(self.ctx, int(bool(on))))
 
+    def lustig_lj(self) -> np.ndarray:
+        """(U, dU/dV, d2U/dV2) of the LJ term at the current positions
+        (Ensemble::myLustig.ljUlus, ljdUlus, ljd2Ulus)."""
+        out = np.zeros(3)
+        self._chk(self.lib.smd_lustig_lj(self.ctx, L.dptr(out)))
+        return out
+
     def set_saap(self, table: np.ndarray, switch_on: bool = False, switch_dist: float = 0.0):
         """The SAAP pair potential as the vdW term (SAAPForce): table rows
         (a0 .. a5) per type pair, ntypes^2 of them."""

@@ -82,6 +82,22 @@ def nacl1000_wolf():
     return s, [("forces",)]
 
 
+def lj500_lustig():
+    # Lustig's volume derivatives of the LJ energy (LJForce.cpp:136-250)
+    s, _ = lj500()
+    s.config.lustig = True
+    return s, [("forces",)]
+
+
+def spce512_lustig():
+    # the same with constraints: r_ij . R_ij with the molecules' centres,
+    # which the reference fills in during a step; so from a run: the second
+    # step's values at the positions the first step left
+    s = systems.spce_water(nmol=512, box=2.4953, cutoff=0.9, kmax=6, seed=11, n_steps=2)
+    s.config.lustig = True
+    return s, [("forces",), ("run", 2)]
+
+
 def saap500():
     # SAAPForce with the reference's own three-type table
     s = systems.three_type_fluid(ncell=5, seed=3)
@@ -146,7 +162,8 @@ def ref_test_nvt():
 
 
 CASES = {"lj500": lj500, "lj500_npt": lj500_npt, "nacl1000_mie": nacl1000_mie, "spce512": spce512,
-         "polwater216": polwater216, "spce512_wolf": spce512_wolf, "saap500": saap500, "nacl1000_wolf": nacl1000_wolf, "polwater216_nve": polwater216_nve, "ref_test_nvt": ref_test_nvt}
+         "polwater216": polwater216, "spce512_wolf": spce512_wolf, "saap500": saap500,
+         "lj500_lustig": lj500_lustig, "spce512_lustig": spce512_lustig, "nacl1000_wolf": nacl1000_wolf, "polwater216_nve": polwater216_nve, "ref_test_nvt": ref_test_nvt}
 LARGE = {"lj4000": lj4000, "lj4000_jitter": lj4000_jitter, "nacl8000_mie": nacl8000_mie, "spce2160": spce2160,
          "polwater4096": polwater4096}
 
@@ -208,6 +225,10 @@ def pack(name, s, results, large=False):
             for fn, key in (("config.txt", "case_config"), ("sysData.in", "case_sysdata"),
                             ("coordinate.in", "case_coords")):
                 out[key] = np.array(open(os.path.join(d, fn)).read())
+    if name.endswith("_lustig"):
+        out = {k: v for k, v in out.items() if not k.startswith(("f_", "r_")) or
+               k in ("f_lustig_lj", "f_lj_energy", "r_step_lustig", "r_step_after1_pos")}
+        out.pop("pairs", None)
     if name.startswith("saap"):
         out = {k: v for k, v in out.items() if not k.startswith("f_")}
         out.pop("pairs", None)
