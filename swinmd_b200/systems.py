@@ -544,19 +544,34 @@ def _place_waters(nmol, L, r_oh, theta_deg, rng, masses, min_dist=0.2):
     body -= com
     idx = np.stack(np.meshgrid(np.arange(g), np.arange(g), np.arange(g), indexing="ij"), -1).reshape(-1, 3)
     order = rng.permutation(len(idx))[:nmol]
-    centres = (idx[np.sort(order)] + 0.5) * a - L / 2
+    cells = idx[np.sort(order)]
+    centres = (cells + 0.5) * a - L / 2
+    # molecules outside the 27 surrounding grid points sit two or more grid
+    # spacings away, so with every site within R of its centre they never
+    # come within min_dist: only the placed neighbours are tested
+    R = float(np.sqrt((body ** 2).sum(1)).max())
+    near = 2.0 * a - 2.0 * R >= min_dist
+    owner = {}
     pos = np.zeros((nmol, 3, 3))
     for m in range(nmol):
+        if near:
+            ci = cells[m]
+            prev_ids = [owner[key] for key in
+                        {tuple((ci + (dx, dy, dz)) % g) for dx in (-1, 0, 1) for dy in (-1, 0, 1) for dz in (-1, 0, 1)}
+                        if key in owner]
         for _ in range(200):
             cand = centres[m] + body @ _random_rotation(rng).T
             if m == 0:
                 break
-            prev = pos[:m].reshape(-1, 3)
+            prev = pos[sorted(prev_ids)].reshape(-1, 3) if near else pos[:m].reshape(-1, 3)
+            if len(prev) == 0:
+                break
             d = cand[:, None, :] - prev[None, :, :]
             d -= L * np.round(d / L)
             if np.sqrt((d ** 2).sum(-1)).min() >= min_dist:
                 break
         pos[m] = cand
+        owner[tuple(cells[m])] = m
     return pos.reshape(-1, 3)
 
 
@@ -643,6 +658,23 @@ def constraint_lengths(s: System) -> np.ndarray:
     out[:, 0] = l1 * l1
     out[:, 1] = l2 * l2
     out[:, 2] = l3 * l3
+    return out
+
+
+def water_replica_set(count: int = 64, n_min: int = 500, n_max: int = 8000, seed: int = 1,
+                      n_steps: int = 5000) -> list:
+    """Independent rigid SPC/E-like waters (LJ + Ewald, SHAKE, Nose-Hoover)
+    for batched runs: molecule counts log-uniform in [n_min, n_max], boxes at
+    the density of the 2160-molecule case (4.03 nm), |n| < kmax with kmax
+    scaled with the box from 9 at 4.03 nm, one seed each.  At zero shear:
+    Ewald under shear is not built."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for r in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
+        box = 4.03 * (n / 2160.0) ** (1.0 / 3.0)
+        kmax = max(5, int(round(9 * box / 4.03)))
+        out.append(spce_water(nmol=n, box=box, cutoff=1.0, kmax=kmax, seed=seed * 1000 + r, n_steps=n_steps))
     return out
 
 

@@ -53,3 +53,32 @@ def test_autotune_and_run():
         e.set_precision("mixed")
         assert np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum()) < 1e-6
     batch.close()
+
+
+def test_water_batch_matches_single_runs():
+    # LJ + Ewald water replicas (SHAKE, leap-frog Nose-Hoover) in one graph
+    # give each replica its own trajectory
+    reps = systems.water_replica_set(count=3, n_min=300, n_max=900, seed=4, n_steps=20)
+
+    def build():
+        out = []
+        for s in reps:
+            e = engine.GpuEnsemble(s, precision="mixed")
+            lf = engine.LFIntegrator(e)
+            lf.start()
+            out.append((e, lf))
+        return out
+
+    alone = build()
+    for _, lf in alone:
+        lf.run(10)
+    together = build()
+    batch = engine.ReplicaBatch([e for e, _ in together])
+    batch.run(10)
+    for (ea, la), (eb, lb) in zip(alone, together):
+        a, b = ea.state(), eb.state()
+        assert np.array_equal(a["pos"], b["pos"]) and np.array_equal(a["vel"], b["vel"])
+        assert la.observables().e_potential == lb.observables().e_potential
+    batch.close()
+    for e, _ in alone + together:
+        e.close()
