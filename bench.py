@@ -407,9 +407,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="polwater4096")
     ap.add_argument("--chunk", type=int, default=100)
-    ap.add_argument("--train-frames", type=int, default=80)
-    ap.add_argument("--train-every", type=int, default=5)
-    ap.add_argument("--train-epochs", type=int, default=40)
+    ap.add_argument("--train-frames", type=int, default=2000)
+    ap.add_argument("--train-every", type=int, default=1)
+    ap.add_argument("--train-epochs", type=int, default=8)
     ap.add_argument("--e2e-every", type=int, default=10)
     ap.add_argument("--cpu-sample-mols", type=int, default=1024)
     ap.add_argument("--equilibrate", type=int, default=10000)
