@@ -7,15 +7,24 @@
 //                          reference's Ensemble / Parameters /
 //                          SimConfiguration objects (Simulation::setup_simulation,
 //                          src/Simulation.cpp:171-263)
-//   GpuLJForce             LJForce::compute (src/forces/LJForce.cpp:58-255)
-//   GpuEwaldForce          EwaldForce::compute / compute_long
-//                          (src/forces/EwaldForce.cpp:127-196)
-//   GpuForceLFIntegrator   the reference's own LFIntegrator (leap-frog, Nose-Hoover,
-//                          SHAKE on the host) driving the GPU force objects: the
-//                          pointers Integrator::initialise filled
-//                          (src/Integrator.cpp:111-203) are swapped for the
-//                          GPU ones, and LFIntegrator::run calls them as
-//                          before (src/integrators/LFIntegrator.cpp:387-458)
+//   GpuNonbonded<Base>     every non-bonded term the configuration enables
+//                          (LJForce or BuffvdWForce, EwaldForce or Multipole +
+//                          Induction, their surface terms), evaluated in two
+//                          calls per step (short range, reciprocal space),
+//                          standing in the slot of Base = LJForce or
+//                          BuffvdWForce, the one force object
+//                          LFIntegrator::run always calls
+//                          (src/integrators/LFIntegrator.cpp:387-400)
+//   GpuForceLFIntegrator   the reference's own LFIntegrator (leap-frog,
+//                          Nose-Hoover, SHAKE, bonded terms on the host)
+//                          driving it: the vdW pointer Integrator::initialise
+//                          filled (src/Integrator.cpp:111-203) is swapped for
+//                          the GPU object and the electrostatic branches of
+//                          LFIntegrator::run (:411-458) are switched off, as
+//                          the GPU object already computed those terms.
+//                          (EwaldForce::compute_long, Multipole::compute_long
+//                          and Induction::compute_long are not virtual, so a
+//                          derived object in their slots would not be called.)
 //
 // Every GPU force object honours the output conventions of the class it
 // replaces: forces add into Atom::force, energies are assigned into
@@ -43,8 +52,11 @@
 #include "Parameters.h"
 #include "SimConfiguration.h"
 #include "integrators/LFIntegrator.h"
+#include "forces/BuffvdWForce.h"
 #include "forces/EwaldForce.h"
+#include "forces/Induction.h"
 #include "forces/LJForce.h"
+#include "forces/Multipole.h"
 
 namespace swinmd_gpu {
 
@@ -86,6 +98,82 @@ inline void lj_tail(Ensemble *e, double *e_lrc, double *v_lrc) {
     *v_lrc = -2.0 * *e_lrc;
 }
 
+// BuffvdWForce::set_buff_param (src/forces/BuffvdWForce.cpp:392-433): per
+// type pair the cubic-mean sigma and the HHG epsilon; a pair with a zero
+// epsilon gets sigma 1e-7 and epsilon 0.  tab: nt * nt * 2 (sigma, eps).
+inline void buff_table(Ensemble *e, std::vector<double> &tab) {
+    const int nt = e->nAtomTypes;
+    tab.assign((size_t)nt * nt * 2, 0.0);
+    for (int a = 0; a < nt; a++)
+        for (int b = 0; b < nt; b++) {
+            const AtomParam &pa = e->myParams->atomParams[a], &pb = e->myParams->atomParams[b];
+            double *t = &tab[2 * (a * nt + b)];
+            if (pa.eps == 0.0 || pb.eps == 0.0) {
+                t[0] = 0.0000001;
+                t[1] = 0.0;
+                continue;
+            }
+            const double si2 = pa.sigma * pa.sigma, sj2 = pb.sigma * pb.sigma;
+            const double es = std::sqrt(pa.eps) + std::sqrt(pb.eps);
+            t[0] = (si2 * pa.sigma + sj2 * pb.sigma) / (si2 + sj2);
+            t[1] = (4.0 * pa.eps * pb.eps) / (es * es);
+        }
+}
+
+// BuffvdWForce::potFunc (BuffvdWForce.cpp:435-463): energy and dU/dr
+inline void buff_pot(double r, double sigma, double eps, double n, double m, double delta, double gamma,
+                     double &u, double &f) {
+    if (eps == 0.0) { u = f = 0.0; return; }
+    const double inv = 1.0 / sigma, rho = r * inv;
+    const double rho_m = std::pow(rho, m), rho_m1 = std::pow(rho, m - 1.0), nm = n - m;
+    const double par1 = (1.0 + delta) / (rho + delta), par2 = (1.0 + gamma) / (rho_m + gamma);
+    const double p1 = std::pow(par1, nm);
+    u = eps * p1 * (par2 - 2.0);
+    f = -eps * nm * p1 * (par2 - 2.0) * inv / (rho + delta) - eps * p1 * par2 * m * rho_m1 * inv / (rho_m + gamma);
+}
+
+// BuffvdWForce::long_range_correct (BuffvdWForce.cpp:468-601): the trapezoid
+// rule with 2^20 intervals of r^2 U and r^3 U' from the cutoff to 5000 nm,
+// averaged over the type pairs of all atoms
+inline void buff_tail(Ensemble *e, const std::vector<double> &tab, double *e_lrc, double *v_lrc) {
+    SimConfiguration *c = e->myConfig;
+    const int nt = e->nAtomTypes, n = e->nAtoms;
+    std::vector<long long> count(nt, 0);
+    for (int i = 0; i < n; i++) count[e->atoms[i].atomType]++;
+    const double rc = c->get_cutoff(), vol = e->boxLx * e->boxLy * e->boxLz;
+    const double nb = c->get_nBuff_param(), mb = c->get_mBuff_param();
+    const double db = c->get_deltaBuff_param(), gb = c->get_gammaBuff_param();
+    const long long intervals = 1LL << 20;
+    const double h = (5000.0 - rc) / (double)intervals;
+    double U = 0.0, P = 0.0;
+    long long npair = 0;
+    for (int a = 0; a < nt; a++)
+        for (int b = a; b < nt; b++) {
+            const long long nij = a != b ? count[a] * count[b] : (long long)(count[a] * (count[a] - 1) * 0.5);
+            npair += nij;
+            const double sig = tab[2 * (a * nt + b)], eps = tab[2 * (a * nt + b) + 1];
+            double u, f;
+            buff_pot(rc, sig, eps, nb, mb, db, gb, u, f);
+            double su = 0.5 * h * rc * rc * u, sp = 0.5 * h * rc * rc * rc * f;
+            for (long long k = 1; k < intervals; k++) {
+                const double r = rc + (double)k * h;
+                buff_pot(r, sig, eps, nb, mb, db, gb, u, f);
+                su += h * r * r * u;
+                sp += h * r * r * r * f;
+            }
+            buff_pot(5000.0, sig, eps, nb, mb, db, gb, u, f);
+            su += 0.5 * h * 5000.0 * 5000.0 * u;
+            sp += 0.5 * h * 5000.0 * 5000.0 * 5000.0 * f;
+            U += (double)nij * su;
+            P += (double)nij * sp;
+        }
+    if (npair <= 0) { *e_lrc = *v_lrc = 0.0; return; }
+    U /= (double)npair;
+    P /= (double)npair;
+    *e_lrc = 2.0 * M_PI * (double)n * (double)n / vol * U;
+    *v_lrc = 2.0 * M_PI * (double)n * (double)n / (vol * vol) * P / 3.0 * vol;
+}
+
 class GpuPath {
 public:
     smd_ctx *ctx = nullptr;
@@ -122,23 +210,65 @@ public:
         check(ctx, smd_set_box(ctx, e->boxLx, e->boxLy, e->boxLz), "smd_set_box");
         check(ctx, smd_set_pairlist(ctx, cfg->get_cutoff(), cfg->get_cutBuff(), e->useCellPairList ? 1 : 0),
               "smd_set_pairlist");
-        if (cfg->compute_buffamoeba() || cfg->compute_multipol() || cfg->compute_wolf() ||
-            cfg->compute_surf_correct())
-            ERRORMSG("swinmd_gpu: this adapter carries the LJ and point-charge Ewald terms");
-        // LJForce: sigma^2 and 4 eps per type pair (Parameters::set_lj_param)
+        if (cfg->compute_wolf())
+            ERRORMSG("swinmd_gpu: this adapter carries LJ, buffered 14-7, Ewald and the multipole model");
         const int nt = e->nAtomTypes;
-        std::vector<double> lj((size_t)nt * nt * 4, 0.0);
-        for (int a = 0; a < nt; a++)
-            for (int b = 0; b < nt; b++) {
-                const LJPairParam p = e->myParams->get_lj_parameter(a, b);
-                lj[4 * (a * nt + b)] = p.sigma;
-                lj[4 * (a * nt + b) + 1] = p.eps;
-            }
-        double e_lrc = 0.0, v_lrc = 0.0;
-        if (cfg->use_long_correct()) lj_tail(e, &e_lrc, &v_lrc);
         const double sd = cfg->get_switch_distance();
-        check(ctx, smd_set_vdw(ctx, SMD_VDW_LJ, lj.data(), cfg->is_switch_on() ? 1 : 0, sd * sd, e_lrc, v_lrc),
-              "smd_set_vdw");
+        if (cfg->compute_buffamoeba()) {
+            // BuffvdWForce: mixed table, taper from the switch distance to
+            // the cutoff (BuffvdWForce.cpp:60-73), tail correction
+            std::vector<double> tab;
+            buff_table(e, tab);
+            const double rc = cfg->get_cutoff(), rc2 = rc * rc, sd2 = sd * sd, off = rc - sd;
+            const double den = off * off * off * off * off;
+            const double taper[6] = {rc * rc2 * (rc2 - 5.0 * rc * sd + 10.0 * sd2) / den, -30.0 * rc2 * sd2 / den,
+                                     30.0 * (rc2 * sd + rc * sd2) / den, -10.0 * (rc2 + 4.0 * rc * sd + sd2) / den,
+                                     15.0 * (rc + sd) / den, -6.0 / den};
+            double e_lrc = 0.0, v_lrc = 0.0;
+            if (cfg->use_long_correct()) buff_tail(e, tab, &e_lrc, &v_lrc);
+            check(ctx, smd_set_buff(ctx, tab.data(), cfg->get_nBuff_param(), cfg->get_mBuff_param(),
+                                    cfg->get_deltaBuff_param(), cfg->get_gammaBuff_param(),
+                                    cfg->get_hfactor_reduction(), cfg->is_switch_on() ? 1 : 0, sd, taper, e_lrc,
+                                    v_lrc),
+                  "smd_set_buff");
+        } else {
+            // LJForce: sigma^2 and 4 eps per type pair (Parameters::set_lj_param)
+            std::vector<double> lj((size_t)nt * nt * 4, 0.0);
+            for (int a = 0; a < nt; a++)
+                for (int b = 0; b < nt; b++) {
+                    const LJPairParam p = e->myParams->get_lj_parameter(a, b);
+                    lj[4 * (a * nt + b)] = p.sigma;
+                    lj[4 * (a * nt + b) + 1] = p.eps;
+                }
+            double e_lrc = 0.0, v_lrc = 0.0;
+            if (cfg->use_long_correct()) lj_tail(e, &e_lrc, &v_lrc);
+            check(ctx, smd_set_vdw(ctx, SMD_VDW_LJ, lj.data(), cfg->is_switch_on() ? 1 : 0, sd * sd, e_lrc, v_lrc),
+                  "smd_set_vdw");
+        }
+        if (cfg->compute_multipol()) {
+            // Multipole / Induction: per type local-frame dipole, quadrupole
+            // and polarisability (Parameters' AtomParam), Ewald and
+            // induction cutoffs, Thole a; the dipoles solved far below the
+            // reference's own stopping point (|r| < 1e-14)
+            std::vector<double> mpv((size_t)nt * 9), pol(nt);
+// (NccForce.h defines a macro named after AtomParam's polarisability field)
+#pragma push_macro("polar")
+#undef polar
+            for (int t = 0; t < nt; t++) {
+                const AtomParam &ap = e->myParams->atomParams[t];
+                const double v[9] = {ap.dipx, ap.dipy, ap.dipz, ap.quadxx, ap.quadxy, ap.quadxz,
+                                     ap.quadyy, ap.quadyz, ap.quadzz};
+                for (int k = 0; k < 9; k++) mpv[9 * t + k] = v[k];
+                pol[t] = ap.polar;
+            }
+#pragma pop_macro("polar")
+            check(ctx, smd_set_multipole(ctx, mpv.data(), pol.data(), cfg->get_alpha(), cfg->get_k_cutoff(),
+                                         cfg->get_cutoffEw(), cfg->compute_induction() ? 1 : 0,
+                                         cfg->get_cutoffInd(), cfg->get_adamping()),
+                  "smd_set_multipole");
+            check(ctx, smd_set_solver(ctx, 1e-13, 3000, SMD_GUESS_DIRECT), "smd_set_solver");
+        }
+        if (cfg->compute_surf_correct()) check(ctx, smd_set_surface_correct(ctx, 1), "smd_set_surface_correct");
         // EwaldForce: alpha, |k| cutoff and the real-space cutoff
         // (src/forces/EwaldForce.cpp:33-39)
         if (cfg->compute_ewald_force())
@@ -203,51 +333,61 @@ public:
     }
 };
 
-class GpuLJForce : public LJForce {
+// The non-bonded terms of the step in the slot of Base (LJForce or
+// BuffvdWForce).  Forces add into Atom::force; energies are assigned into the
+// myEnergy fields the replaced classes assign; the short-range virial goes
+// into Ensemble::virial with the reference's sign, and the reciprocal virial
+// into Ensemble::longVirial components 0..7, as EwaldForce::compute_long and
+// Multipole::compute_long + Induction::compute_long leave them.
+template <class Base>
+class GpuNonbonded : public Base {
     GpuPath *path;
+    uint32_t short_terms = SMD_TERM_VDW, long_terms = 0;
 
 public:
-    GpuLJForce(Ensemble *e, GpuPath *p) : LJForce(e), path(p) {}
-    void compute() override {
-        double en[SMD_E_COUNT], w[9];
-        path->evaluate(SMD_TERM_VDW, en, w);
-        path->add_forces();
-        energy = en[SMD_E_VDW];
-        myEnsemble->myEnergy.ljEnergy = energy;
-        for (int k = 0; k < 9; k++) {
-            virial[k] = -w[k];
-            myEnsemble->virial[k] += w[k];
+    GpuNonbonded(Ensemble *e, GpuPath *p) : Base(e), path(p) {
+        SimConfiguration *c = e->myConfig;
+        if (c->compute_ewald_force()) {
+            short_terms |= SMD_TERM_EWALD_REAL;
+            long_terms |= SMD_TERM_EWALD_LONG;
+        } else if (c->compute_multipol()) {
+            short_terms |= SMD_TERM_MP_SHORT;
+            long_terms |= SMD_TERM_MP_LONG;
+            if (c->compute_induction()) {
+                short_terms |= SMD_TERM_IND_SHORT;
+                long_terms |= SMD_TERM_IND_LONG;
+            }
         }
     }
-};
-
-class GpuEwaldForce : public EwaldForce {
-    GpuPath *path;
-
-public:
-    GpuEwaldForce(Ensemble *e, GpuPath *p) : EwaldForce(e), path(p) {}
-    // real space, intramolecular correction, self and net-charge energies
     void compute() override {
         double en[SMD_E_COUNT], w[9];
-        path->evaluate(SMD_TERM_EWALD_REAL, en, w);
+        Energy &E = this->myEnsemble->myEnergy;
+        path->evaluate(short_terms, en, w);
         path->add_forces();
-        myEnsemble->myEnergy.realEnergy = en[SMD_E_REAL];
-        myEnsemble->myEnergy.correctEnergy = en[SMD_E_CORRECT];
-        myEnsemble->myEnergy.molCorrectEnergy = en[SMD_E_MOLCORRECT];
-        myEnsemble->myEnergy.surfCorrectEnergy = 0.0;
-        energy = en[SMD_E_REAL] + en[SMD_E_CORRECT] + en[SMD_E_MOLCORRECT];
-        for (int k = 0; k < 9; k++) {
-            virial[k] = -w[k];
-            myEnsemble->virial[k] += w[k];
+        this->energy = en[SMD_E_VDW];
+        E.ljEnergy = en[SMD_E_VDW];   // tail correction included
+        if (short_terms & (SMD_TERM_EWALD_REAL | SMD_TERM_MP_SHORT)) {
+            E.realEnergy = en[SMD_E_REAL];
+            E.correctEnergy = en[SMD_E_CORRECT];
+            E.molCorrectEnergy = en[SMD_E_MOLCORRECT];
+            E.surfCorrectEnergy = en[SMD_E_SURF];
         }
-    }
-    // reciprocal space: forces into Atom::force, as reciprocal_term adds them
-    void compute_long() {
-        double en[SMD_E_COUNT], w[9];
-        path->evaluate(SMD_TERM_EWALD_LONG, en, w);
+        if (short_terms & SMD_TERM_IND_SHORT) {
+            E.realPolEnergy = en[SMD_E_POL_REAL];
+            E.correctPolEnergy = en[SMD_E_POL_SELF];
+            E.molCorrectPolEnergy = en[SMD_E_POL_INTRA];
+            E.surfacePolEnergy = en[SMD_E_POL_SURF];
+        }
+        for (int k = 0; k < 9; k++) {
+            this->virial[k] = -w[k];
+            this->myEnsemble->virial[k] += w[k];
+        }
+        if (!long_terms) return;
+        path->evaluate(long_terms, en, w);
         path->add_forces();
-        myEnsemble->myEnergy.longEnergy = en[SMD_E_LONG];
-        for (int k = 0; k < 8; k++) myEnsemble->longVirial[k] = w[k];
+        E.longEnergy = en[SMD_E_LONG];
+        if (long_terms & SMD_TERM_IND_LONG) E.longPolEnergy = en[SMD_E_POL_LONG];
+        for (int k = 0; k < 8; k++) this->myEnsemble->longVirial[k] = w[k];
     }
 };
 
@@ -258,15 +398,23 @@ public:
 class GpuForceLFIntegrator : public LFIntegrator {
 public:
     GpuForceLFIntegrator(Ensemble *e, SimConfiguration *c, GpuPath *p) : LFIntegrator(e, c) {
-        Force *old_lj = ljForce;
-        ljForce = new GpuLJForce(e, p);
-        for (Force *&f : forceGroup)
-            if (f == old_lj) f = ljForce;
-        delete old_lj;
-        if (ewaldForce) {
-            delete ewaldForce;
-            ewaldForce = new GpuEwaldForce(e, p);
+        if (buffForce) {
+            Force *old = buffForce;
+            buffForce = new GpuNonbonded<BuffvdWForce>(e, p);
+            for (Force *&f : forceGroup)
+                if (f == old) f = buffForce;
+            delete old;
+        } else {
+            Force *old = ljForce;
+            ljForce = new GpuNonbonded<LJForce>(e, p);
+            for (Force *&f : forceGroup)
+                if (f == old) f = ljForce;
+            delete old;
         }
+        // the GPU object computes the electrostatic terms too
+        computeEwald = false;
+        computeMultipole = false;
+        computeInduction = false;
     }
     double zeta() const { return fnh; }
     int list_updates() const { return numUpdates; }

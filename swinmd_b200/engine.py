@@ -769,6 +769,38 @@ class Induction(GpuForce):
         return f
 
 
+class WolfForce(GpuForce):
+    """``WolfForce::compute`` (src/forces/WolfForce.cpp:100-260): the charges'
+    damped, shifted real-space sum (energy into realEnergy)."""
+    terms = L.TERM_WOLF
+    energy_index = L.E_REAL
+
+
+class SAAPForce(GpuForce):
+    """``SAAPForce::compute`` (src/forces/SAAPForce.cpp:54-230), once the
+    ensemble carries a SAAP table (``GpuEnsemble.set_saap``)."""
+    terms = L.TERM_VDW
+    energy_index = L.E_VDW
+
+
+class BondForce(GpuForce):
+    """``BondForce::compute`` (src/forces/BondForce.cpp:37-110)."""
+    terms = L.TERM_BOND
+    energy_index = L.E_BOND
+
+
+class AngleForce(GpuForce):
+    """``AngleForce::compute`` (src/forces/AngleForce.cpp:34-130)."""
+    terms = L.TERM_ANGLE
+    energy_index = L.E_ANGLE
+
+
+class UreyBradleyForce(GpuForce):
+    """``UreyBradleyForce::compute`` (src/forces/UreyBradleyForce.cpp:39-100)."""
+    terms = L.TERM_UB
+    energy_index = L.E_UB
+
+
 class ReplicaBatch:
     """Independent replicas (``GpuEnsemble`` objects with their integrators
     started) advanced by one CUDA graph per step (``smd_batch_*``)."""
