@@ -212,6 +212,11 @@ public:
               "smd_set_pairlist");
         if (cfg->compute_wolf())
             ERRORMSG("swinmd_gpu: this adapter carries LJ, buffered 14-7, Ewald and the multipole model");
+        // molecule kinds with their own branches in the electrostatic terms
+        // (the dummy charge site of "MCY", the damping of "BBV")
+        for (int m = 0; m < e->nMols; m++)
+            if (!std::strcmp(e->molecules[m].molName, "MCY") || !std::strcmp(e->molecules[m].molName, "BBV"))
+                ERRORMSG("swinmd_gpu: MCY and BBV molecules are not built on the GPU path");
         const int nt = e->nAtomTypes;
         const double sd = cfg->get_switch_distance();
         if (cfg->compute_buffamoeba()) {

@@ -233,6 +233,18 @@ def refuse_unsupported(c) -> None:
         raise NotImplementedError("Wolf together with Ewald or multipoles")
 
 
+def refuse_unsupported_molecules(s: System) -> None:
+    """Raises for molecule kinds whose special cases the GPU path does not
+    carry: "MCY" (its O charge moved to a dummy site in Ewald, Multipole and
+    Induction, e.g. EwaldForce.cpp:99-125, Multipole.cpp:143-160), "BBV" (its
+    own Coulomb damping and SHAKE, Multipole.cpp:639, LFIntegrator::shakeBBV)
+    and "CO2" (LFIntegrator::shakeCFR)."""
+    names = {nm for nm, _ in s.mol_type_names}
+    bad = sorted(names & {"MCY", "BBV", "CO2"})
+    if bad:
+        raise NotImplementedError(f"molecule kinds {bad} are not built on the GPU path")
+
+
 class GpuEnsemble:
     """One system on one GPU behind the C ABI (the role of ``Ensemble``)."""
 
@@ -243,6 +255,7 @@ class GpuEnsemble:
         self.system = s = system
         self.n = s.n_atoms
         refuse_unsupported(s.config)
+        refuse_unsupported_molecules(s)
         ctx = ctypes.c_void_p()
         code = self.lib.smd_create(device, ctypes.byref(ctx))
         if code != L.SMD_OK:

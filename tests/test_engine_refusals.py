@@ -27,3 +27,12 @@ def test_ub_with_constraints_refused():
     s.config.compute_ub = True
     with pytest.raises(NotImplementedError):
         engine.refuse_unsupported(s.config)
+
+
+@pytest.mark.parametrize("name", ["MCY", "BBV", "CO2"])
+def test_unsupported_molecule_kinds_refused(name):
+    s = _pw()
+    s.mol_type_names = [(name, 3)]
+    with pytest.raises(NotImplementedError):
+        engine.refuse_unsupported_molecules(s)
+    engine.refuse_unsupported_molecules(_pw())   # "WAT" is built
