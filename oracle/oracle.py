@@ -227,3 +227,108 @@ def water_md(system, pos, vel, box, nsteps):
                        ep.ctypes.data_as(_D), tt.ctypes.data_as(_D), zz.ctypes.data_as(_D))
     assert r == 0, r
     return {"pos": pos.reshape(-1, 3), "vel": vel.reshape(-1, 3), "epot": ep, "temp": tt, "zeta": zz}
+
+
+def _bonded_tables(system):
+    """bonds [nb][3], (r0, k) per bond type; angles [na][4], (t0 rad, k) per type."""
+    import math
+    bonds = np.ascontiguousarray(system.bonds, np.int32).reshape(-1, 3)
+    angles = np.ascontiguousarray(system.angles, np.int32).reshape(-1, 4)
+    bpar = np.array([[r0, k] for (_, _, r0, k) in system.bond_params] or [[0.0, 0.0]], np.float64)
+    apar = np.array([[math.radians(t0), k] for (_, _, _, t0, k) in system.angle_params] or [[0.0, 0.0]],
+                    np.float64)
+    return bonds, bpar, angles, apar
+
+
+def _flex_args(system, box):
+    c = system.config
+    s2, e4 = system.lj_table()
+    L = np.array(box if np.ndim(box) else [box] * 3, np.float64)
+    q = system.scaled_charges()
+    off, flat = _excl_csr(system)
+    bonds, bpar, angles, apar = _bonded_tables(system)
+    ns = system.mol_type_names[0][1]
+    return c, s2, e4, L, q, off, flat, bonds, bpar, angles, apar, ns
+
+
+def flex_le_forces(system, pos, box, delta):
+    """Forces, per-term energies and virial of a flexible point-charge model
+    (LJ, Ewald real / sheared reciprocal / intramolecular, bonds, angles)
+    with Lees-Edwards images at offset delta; see or_flex_le_forces."""
+    lb = lib()
+    lb.or_flex_le_forces.restype = None
+    lb.or_flex_le_forces.argtypes = [ctypes.c_int, ctypes.c_int, _D, _I, _I, _D, _D, ctypes.c_double,
+                                     ctypes.c_int, _D, _D, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                     ctypes.c_double, _I, _I, ctypes.c_int, _I, _D, ctypes.c_int, _I, _D,
+                                     _D, _D, _D]
+    c, s2, e4, L, q, off, flat, bonds, bpar, angles, apar, ns = _flex_args(system, box)
+    n = system.n_atoms
+    f = np.zeros(3 * n)
+    w = np.zeros(9)
+    e = np.zeros(7)
+    lb.or_flex_le_forces(n, ns, d(pos), i32(system.atom_type), i32(system.mol_id), d(q), d(L), float(delta),
+                         len(system.atom_types), d(s2), d(e4), c.cutoff, int(c.switch_on), c.alpha, c.k_cutoff,
+                         i32(off), i32(flat), len(bonds), i32(bonds), d(bpar), len(angles), i32(angles), d(apar),
+                         f.ctypes.data_as(_D), w.ctypes.data_as(_D), e.ctypes.data_as(_D))
+    return {"force": f.reshape(-1, 3), "virial": w, "vdw": e[0], "real": e[1], "long": e[2], "intra": e[3],
+            "bond": e[4], "angle": e[5], "nk": int(e[6])}
+
+
+def ewald_recip_le(system, pos, box, delta, alpha=None, kcut=None):
+    """Reciprocal Ewald energy, forces and long virial in the sheared cell."""
+    lb = lib()
+    lb.or_ewald_recip_le.restype = ctypes.c_double
+    lb.or_ewald_recip_le.argtypes = [ctypes.c_int, _D, _D, _D, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, _D, _D, ctypes.POINTER(ctypes.c_int)]
+    c = system.config
+    L = np.array(box if np.ndim(box) else [box] * 3, np.float64)
+    n = system.n_atoms
+    f = np.zeros(3 * n)
+    w = np.zeros(9)
+    nk = ctypes.c_int()
+    e = lb.or_ewald_recip_le(n, d(pos), d(system.scaled_charges()), d(L), float(delta),
+                             c.alpha if alpha is None else alpha, c.k_cutoff if kcut is None else kcut,
+                             f.ctypes.data_as(_D), w.ctypes.data_as(_D), ctypes.byref(nk))
+    return {"energy": e, "force": f.reshape(-1, 3), "virial": w, "nk": nk.value}
+
+
+def ewald_real_le(system, pos, box, delta, alpha=None, rc=None):
+    lb = lib()
+    lb.or_ewald_real_le.restype = ctypes.c_double
+    lb.or_ewald_real_le.argtypes = [ctypes.c_int, _D, _D, _I, _D, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, _D, _D]
+    c = system.config
+    L = np.array(box if np.ndim(box) else [box] * 3, np.float64)
+    n = system.n_atoms
+    f = np.zeros(3 * n)
+    w = np.zeros(9)
+    e = lb.or_ewald_real_le(n, d(pos), d(system.scaled_charges()), i32(system.mol_id), d(L), float(delta),
+                            c.alpha if alpha is None else alpha, c.cutoff if rc is None else rc,
+                            f.ctypes.data_as(_D), w.ctypes.data_as(_D))
+    return {"energy": e, "force": f.reshape(-1, 3), "virial": w}
+
+
+def flex_nhc_md(system, pos, vel, box, nsteps, strain_rate=0.0, ndf=None):
+    """Chain / SLLOD velocity-Verlet MD of a flexible point-charge model with
+    molecules wrapped by their centres; see or_flex_nhc_md."""
+    lb = lib()
+    lb.or_flex_nhc_md.restype = ctypes.c_int
+    lb.or_flex_nhc_md.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, _I, _I, _D, _D, ctypes.c_int, _D, _D,
+                                  ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double, _I, _I,
+                                  ctypes.c_int, _I, _D, ctypes.c_int, _I, _D, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D]
+    c, s2, e4, L, q, off, flat, bonds, bpar, angles, apar, ns = _flex_args(system, box)
+    n = system.n_atoms
+    pos = np.array(pos, np.float64).reshape(-1).copy()
+    vel = np.array(vel, np.float64).reshape(-1).copy()
+    out = [np.zeros(nsteps) for _ in range(5)]
+    ndf = 3 * n - 3 if ndf is None else ndf
+    r = lb.or_flex_nhc_md(n, ns, pos.ctypes.data_as(_D), vel.ctypes.data_as(_D), d(system.masses()),
+                          i32(system.atom_type), i32(system.mol_id), d(q), d(L), len(system.atom_types), d(s2),
+                          d(e4), c.cutoff, int(c.switch_on), c.alpha, c.k_cutoff, i32(off), i32(flat),
+                          len(bonds), i32(bonds), d(bpar), len(angles), i32(angles), d(apar), c.timestep,
+                          c.temperature, c.coupl_const, strain_rate, ndf, nsteps,
+                          *[o.ctypes.data_as(_D) for o in out])
+    assert r == 0, r
+    return {"pos": pos.reshape(-1, 3), "vel": vel.reshape(-1, 3), "epot": out[0], "temp": out[1],
+            "vnh0": out[2], "pxy": out[3], "delta": out[4]}

@@ -638,3 +638,253 @@ double or_lj_le_forces(int n, const double *pos, const int32_t *type, const doub
                        const double *sig2, const double *eps4, double rc, int shift, double *f, double *w) {
     return lj_le_forces(n, pos, type, L, delta, nt, sig2, eps4, rc, shift, f, w);
 }
+
+/* ----------------------------------------------------------------------
+ * Point-charge Ewald sums in the Lees-Edwards (sliding brick) cell, and
+ * the chain/SLLOD MD of flexible point-charge molecules that uses them.
+ * No reference code: the reference has no shear.  The images of the box
+ * under planar Couette shear with offset d are the lattice a1 = (Lx, 0, 0),
+ * a2 = (d, Ly, 0), a3 = (0, 0, Lz); its reciprocal vectors give
+ * k(n) = 2 pi (nx / Lx, (ny - nx d / Lx) / Ly, nz / Lz).  The reciprocal
+ * sum is the reference's (EwaldForce::set_up + reciprocal_term,
+ * src/forces/EwaldForce.cpp:198-257, 529-698) over the half space of n with
+ * |k| < kcut for that lattice; d and d + Lx describe the same lattice, so
+ * d is first reduced to [-Lx/2, Lx/2].  Parity unpinned: checked by the
+ * properties of the lattice sum (independence of alpha, of d -> d + Lx, the
+ * unsheared sum at d = 0, forces as the energy's derivative).
+ * ---------------------------------------------------------------------- */
+double or_ewald_recip_le(int n, const double *pos, const double *q, const double *L, double delta,
+                         double alpha, double kcut, double *f, double *w, int *nk_out) {
+    double kc2 = kcut * kcut, aR4 = 1.0 / (4.0 * alpha * alpha);
+    double dd = delta - L[0] * floor(delta / L[0] + 0.5), t = dd / L[0];
+    int nmax[3];
+    for (int d = 0; d < 3; d++) nmax[d] = (int)(kcut * L[d] / (2 * OR_PI));
+    int nyr = nmax[1] + nmax[0] + 1;   /* |ny - nx t| < kcut Ly / 2 pi for every |t| <= 1/2 */
+    double vol = L[0] * L[1] * L[2], pi4V = 4.0 * OR_PI * (1.0 / vol), pi8V = 2.0 * pi4V;
+    double *sc = (double *)malloc(sizeof(double) * 2 * (n > 0 ? n : 1)), pe = 0;
+    int nk = 0;
+    for (int nx = 0; nx <= nmax[0]; nx++)
+        for (int ny = -nyr; ny <= nyr; ny++)
+            for (int nz = -nmax[2]; nz <= nmax[2]; nz++) {
+                if (!(nx > 0 || (nx == 0 && ny > 0) || (nx == 0 && ny == 0 && nz > 0))) continue;
+                double k[3] = {2.0 * OR_PI * nx / L[0], 2.0 * OR_PI * (ny - nx * t) / L[1],
+                               2.0 * OR_PI * nz / L[2]};
+                double k2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
+                if (!(k2 < kc2)) continue;
+                nk++;
+                double expK = exp(-k2 * aR4) / k2, ss = 0, cs = 0;
+                for (int i = 0; i < n; i++) {
+                    double a = pos[3 * i] * k[0] + pos[3 * i + 1] * k[1] + pos[3 * i + 2] * k[2];
+                    sc[2 * i] = q[i] * sin(a);
+                    sc[2 * i + 1] = q[i] * cos(a);
+                    ss += sc[2 * i];
+                    cs += sc[2 * i + 1];
+                }
+                double e = pi4V * expK * (ss * ss + cs * cs);
+                pe += e;
+                double coeff = 2.0 * (aR4 + 1.0 / k2);
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) w[3 * a + b] += (a == b ? e : 0.0) - e * coeff * k[a] * k[b];
+                double b = pi8V * expK;
+                for (int i = 0; i < n; i++) {
+                    double val = b * (sc[2 * i] * cs - sc[2 * i + 1] * ss);
+                    for (int d = 0; d < 3; d++) f[3 * i + d] += k[d] * val;
+                }
+            }
+    free(sc);
+    if (nk_out) *nk_out = nk;
+    return pe;
+}
+
+/* Ewald real space with Lees-Edwards images: q_i q_j erfc(a r)/r over all
+ * pairs of different molecules within rc (EwaldForce::real_term,
+ * EwaldForce.cpp:296-527, whose pair list holds no same-molecule pair of a
+ * water).  Adds forces and the virial, returns the energy. */
+double or_ewald_real_le(int n, const double *pos, const double *q, const int32_t *mol, const double *L,
+                        double delta, double alpha, double rc, double *f, double *w) {
+    double rc2 = rc * rc, a2 = alpha * alpha, a2pi = 2.0 * alpha / OR_SQRT_PI, energy = 0;
+    for (int i = 0; i < n; i++)
+        for (int j = i + 1; j < n; j++) {
+            if (mol[i] == mol[j]) continue;
+            double d[3] = {pos[3 * j] - pos[3 * i], pos[3 * j + 1] - pos[3 * i + 1],
+                           pos[3 * j + 2] - pos[3 * i + 2]};
+            pbc_le(d, L, delta);
+            double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+            if (!(r2 < rc2)) continue;
+            double qij = q[i] * q[j], r = sqrt(r2);
+            double e = erfc(alpha * r) / r;
+            double fs = (e + a2pi * exp(-a2 * r2)) / r2;
+            energy += qij * e;
+            double fij[3] = {-qij * fs * d[0], -qij * fs * d[1], -qij * fs * d[2]};
+            for (int k = 0; k < 3; k++) { f[3 * i + k] += fij[k]; f[3 * j + k] -= fij[k]; }
+            vir_add(w, fij, d);
+        }
+    return energy;
+}
+
+/* Harmonic bonds and angles (BondForce::compute, BondForce.cpp:37-110;
+ * AngleForce::compute, AngleForce.cpp:34-130): U = k/2 (r - r0)^2 and
+ * k/2 (t - t0)^2 (t0 in radians), cos t clamped at -0.9999999.  Each class
+ * adds f_a r_b of its own vectors (r12 = r1 - r2; r2 - r1 and r2 - r3 for
+ * the angle) to a local virial that it subtracts from Ensemble::virial,
+ * which is what w receives.  bonds: [nb][3] (a1 a2 type), bpar [type][2]
+ * (r0, k); angles: [na][4] (a1 apex a3 type), apar [type][2] (t0, k). */
+void or_bonded(int nb, const int32_t *bonds, const double *bpar, int na, const int32_t *angles,
+               const double *apar, const double *pos, const double *L, double *f, double *w,
+               double *e_bond, double *e_angle) {
+    double eb = 0, ea = 0;
+    for (int b = 0; b < nb; b++) {
+        int i = bonds[3 * b], j = bonds[3 * b + 1], t = bonds[3 * b + 2];
+        double x[3] = {pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1], pos[3 * i + 2] - pos[3 * j + 2]};
+        pbc(x, L);
+        double r = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]), dr = r - bpar[2 * t], k = bpar[2 * t + 1];
+        eb += 0.5 * k * dr * dr;
+        double s = -k * dr / r;
+        for (int p = 0; p < 3; p++) {
+            f[3 * i + p] += s * x[p];
+            f[3 * j + p] -= s * x[p];
+            for (int c = 0; c < 3; c++) w[3 * p + c] -= s * x[p] * x[c];
+        }
+    }
+    for (int a = 0; a < na; a++) {
+        int i1 = angles[4 * a], i2 = angles[4 * a + 1], i3 = angles[4 * a + 2], t = angles[4 * a + 3];
+        double r12[3], r32[3];
+        for (int p = 0; p < 3; p++) {
+            r12[p] = pos[3 * i2 + p] - pos[3 * i1 + p];
+            r32[p] = pos[3 * i2 + p] - pos[3 * i3 + p];
+        }
+        pbc(r12, L);
+        pbc(r32, L);
+        double d12r = 1.0 / sqrt(r12[0] * r12[0] + r12[1] * r12[1] + r12[2] * r12[2]);
+        double d32r = 1.0 / sqrt(r32[0] * r32[0] + r32[1] * r32[1] + r32[2] * r32[2]);
+        double cs = (r12[0] * r32[0] + r12[1] * r32[1] + r12[2] * r32[2]) * d12r * d32r;
+        if (cs < -0.9999999) cs = -0.9999999;
+        double isn = 1.0 / sqrt(1.0 - cs * cs), diff = acos(cs) - apar[2 * t], k = apar[2 * t + 1];
+        ea += 0.5 * k * diff * diff;
+        double v = k * diff;
+        for (int p = 0; p < 3; p++) {
+            double u12 = r12[p] * d12r, u32 = r32[p] * d32r;
+            double f1 = v * d12r * isn * (u12 * cs - r32[p] * d32r);
+            double f3 = v * d32r * isn * (u32 * cs - r12[p] * d12r);
+            f[3 * i1 + p] += f1;
+            f[3 * i2 + p] -= f1 + f3;
+            f[3 * i3 + p] += f3;
+            for (int c = 0; c < 3; c++) w[3 * p + c] -= f1 * r12[c] + f3 * r32[c];
+        }
+    }
+    *e_bond = eb;
+    *e_angle = ea;
+}
+
+/* All terms of a flexible point-charge model at offset delta: LJ (shifted at
+ * rc when shift, every pair of different molecules), Ewald real space,
+ * reciprocal space in the sheared cell, the intramolecular erf correction
+ * with its forces (molecules of ns consecutive sites, excluded pairs from
+ * off/ex), bonds and angles.  e[7] = {vdw, real, long, intra, bond, angle,
+ * k count}; f and w are overwritten; w holds Ensemble::virial + longVirial. */
+void or_flex_le_forces(int n, int ns, const double *pos, const int32_t *type, const int32_t *mol,
+                       const double *q, const double *L, double delta, int nt, const double *sig2,
+                       const double *eps4, double rc, int shift, double alpha, double kcut,
+                       const int32_t *off, const int32_t *ex, int nb, const int32_t *bonds, const double *bpar,
+                       int na, const int32_t *angles, const double *apar, double *f, double *w, double *e) {
+    double *ft = (double *)malloc(sizeof(double) * 3 * n), wt[9];
+    int nk = 0;
+    e[0] = lj_le_forces(n, pos, type, L, delta, nt, sig2, eps4, rc, shift, f, w);
+    e[1] = or_ewald_real_le(n, pos, q, mol, L, delta, alpha, rc, f, w);
+    memset(ft, 0, sizeof(double) * 3 * n);
+    memset(wt, 0, sizeof(wt));
+    e[2] = or_ewald_recip_le(n, pos, q, L, delta, alpha, kcut, ft, wt, &nk);
+    for (int k = 0; k < 3 * n; k++) f[k] += ft[k];
+    for (int k = 0; k < 9; k++) w[k] += wt[k];
+    e[3] = or_ewald_intra(n / ns, ns, pos, q, L, alpha, off, ex, 0, f);
+    or_bonded(nb, bonds, bpar, na, angles, apar, pos, L, f, w, &e[4], &e[5]);
+    e[6] = nk;
+    free(ft);
+}
+
+/* The chain / SLLOD velocity-Verlet of or_lj_nhc_md for flexible molecules
+ * with the forces of or_flex_le_forces, each molecule wrapped by its centre
+ * of mass (y first, moving x by -/+ delta under shear; then x and z).
+ * Outputs per step: the sum of the force terms' energies, 2 KE / (Nf kB),
+ * the first chain velocity, P_xy = (sum m v_x v_y + W_xy) / V and delta. */
+int or_flex_nhc_md(int n, int ns, double *pos, double *vel, const double *mass, const int32_t *type,
+                   const int32_t *mol, const double *q, const double *L, int nt, const double *sig2,
+                   const double *eps4, double rc, int shift, double alpha, double kcut, const int32_t *off,
+                   const int32_t *ex, int nb, const int32_t *bonds, const double *bpar, int na,
+                   const int32_t *angles, const double *apar, double dt, double T, double tau, double gamma,
+                   int ndf, int nsteps, double *out_epot, double *out_temp, double *out_vnh0, double *out_pxy,
+                   double *out_delta) {
+    double *f = (double *)malloc(sizeof(double) * 3 * n);
+    double w[9], e[7];
+    const double kT = OR_KB * T, nf = (double)ndf, vol = L[0] * L[1] * L[2];
+    double qnh[4], vnh[4] = {0, 0, 0, 0};
+    for (int k = 0; k < 4; k++) qnh[k] = kT * tau * tau;
+    qnh[0] *= nf;
+    double delta = 0.0;
+    const int nmol = n / ns;
+    or_flex_le_forces(n, ns, pos, type, mol, q, L, delta, nt, sig2, eps4, rc, shift, alpha, kcut, off, ex, nb,
+                      bonds, bpar, na, angles, apar, f, w, e);
+    for (int s = 0; s < nsteps; s++) {
+        double ekin = 0;
+        for (int i = 0; i < n; i++)
+            ekin += 0.5 * mass[i] * (vel[3 * i] * vel[3 * i] + vel[3 * i + 1] * vel[3 * i + 1] + vel[3 * i + 2] * vel[3 * i + 2]);
+        double sc = nhc_half(vnh, qnh, ekin, kT, nf, dt);
+        delta = fmod(delta + gamma * L[1] * dt, L[0]);
+        if (delta < 0) delta += L[0];
+        for (int i = 0; i < n; i++) {
+            double *v = &vel[3 * i], *r = &pos[3 * i], mr = 1.0 / mass[i];
+            for (int k = 0; k < 3; k++) v[k] *= sc;
+            v[0] -= gamma * 0.5 * dt * v[1];
+            for (int k = 0; k < 3; k++) v[k] += 0.5 * dt * mr * f[3 * i + k];
+            r[0] += dt * v[0] + gamma * dt * (r[1] + 0.5 * dt * v[1]);
+            r[1] += dt * v[1];
+            r[2] += dt * v[2];
+        }
+        for (int m = 0; m < nmol; m++) {
+            double c[3] = {0, 0, 0}, M = 0, sh[3] = {0, 0, 0};
+            for (int a = 0; a < ns; a++) {
+                int i = m * ns + a;
+                for (int k = 0; k < 3; k++) c[k] += mass[i] * pos[3 * i + k];
+                M += mass[i];
+            }
+            for (int k = 0; k < 3; k++) c[k] /= M;
+            if (c[1] >= L[1] / 2.0) { sh[1] = -L[1]; sh[0] = -delta; }
+            else if (c[1] < -L[1] / 2.0) { sh[1] = L[1]; sh[0] = delta; }
+            if (gamma == 0.0) sh[0] = 0.0;
+            double cx = c[0] + sh[0], cz = c[2];
+            while (cx >= L[0] / 2.0) cx -= L[0];
+            while (cx < -L[0] / 2.0) cx += L[0];
+            while (cz >= L[2] / 2.0) cz -= L[2];
+            while (cz < -L[2] / 2.0) cz += L[2];
+            sh[0] = cx - c[0];
+            sh[2] = cz - c[2];
+            for (int a = 0; a < ns; a++)
+                for (int k = 0; k < 3; k++) pos[3 * (m * ns + a) + k] += sh[k];
+        }
+        or_flex_le_forces(n, ns, pos, type, mol, q, L, delta, nt, sig2, eps4, rc, shift, alpha, kcut, off, ex,
+                          nb, bonds, bpar, na, angles, apar, f, w, e);
+        out_epot[s] = e[0] + e[1] + e[2] + e[3] + e[4] + e[5];
+        ekin = 0;
+        double kxy = 0;
+        for (int i = 0; i < n; i++) {
+            double *v = &vel[3 * i], mr = 1.0 / mass[i];
+            for (int k = 0; k < 3; k++) v[k] += 0.5 * dt * mr * f[3 * i + k];
+            v[0] -= gamma * 0.5 * dt * v[1];
+            ekin += 0.5 * mass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        }
+        sc = nhc_half(vnh, qnh, ekin, kT, nf, dt);
+        ekin = 0;
+        for (int i = 0; i < n; i++) {
+            double *v = &vel[3 * i];
+            for (int k = 0; k < 3; k++) v[k] *= sc;
+            ekin += 0.5 * mass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            kxy += mass[i] * v[0] * v[1];
+        }
+        out_temp[s] = 2.0 * ekin / (nf * OR_KB);
+        out_vnh0[s] = vnh[0];
+        out_pxy[s] = (kxy + w[1]) / vol;
+        out_delta[s] = delta;
+    }
+    free(f);
+    return 0;
+}

@@ -344,7 +344,7 @@ void smd_destroy(smd_ctx *x) {
                     c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab, c.srec, c.phist, c.cg_blk,
                     c.upload4, c.fout, c.rc.kzr_d, c.rc.kcxy_d, c.rc.stab_d, c.rc.srec_d, c.bonds, c.angles,
                     c.bond_par, c.angle_par, c.surf_part, c.surf_tot, c.rdf_hist, c.avg, c.wrap,
-                    c.wolf_msite, c.wpos4, c.dbox, c.saap};
+                    c.wolf_msite, c.wpos4, c.dbox, c.saap, c.rc.nk_dev};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -1321,8 +1321,8 @@ int smd_get_pairs(smd_ctx *x, int32_t *pairs, int64_t cap, int64_t *count) {
 
 int smd_ewald_nk(smd_ctx *x, int *nk) {
     if (!x || !nk) return SMD_ERR_ARG;
-    *nk = x->c.rc.nk;
-    return SMD_OK;
+    const int r = recip_nk(x->c, nk);
+    return r ? fail(x, r, "smd_ewald_nk: reading the k count failed") : SMD_OK;
 }
 
 int smd_set_integrator(smd_ctx *x, const smd_integrator_params *p) {
@@ -1343,17 +1343,25 @@ int smd_set_integrator(smd_ctx *x, const smd_integrator_params *p) {
     if (p->strain_rate != 0.0) {
         if (p->thermostat != SMD_THERMO_NH_CHAIN)
             return fail(x, SMD_ERR_ARG, "smd_set_integrator: SLLOD shear runs with the chain integrator");
-        if (x->c.ewald_on || x->c.mp_on || x->c.vdw == VDW_BUFF)
+        if (x->c.mp_on || x->c.vdw == VDW_BUFF || x->c.surface_on)
             return fail(x, SMD_ERR_ARG,
-                        "smd_set_integrator: SLLOD shear supports the LJ / Mie / BMH pair terms only");
+                        "smd_set_integrator: SLLOD shear supports the LJ / Mie / BMH pair terms, point-charge "
+                        "Ewald and bonded terms (no multipoles, buffered 14-7 or surface correction)");
     }
     Ctx &c = x->c;
+    const bool was_sheared = c.integrator_ready && c.ip.strain_rate != 0.0;
     c.ip = *p;
     // the sheared cell search moves a 4-cell x window across the y boundary
     if (p->strain_rate != 0.0 && c.grid.use_cells && c.grid.n[0] < 4) c.grid.use_cells = 0;
     if (c.ip.atom_ndf <= 0) c.ip.atom_ndf = 3 * c.n - 3;
     if (c.ip.mol_ndf <= 0) c.ip.mol_ndf = 3 * c.nmol - 3;
     c.integrator_ready = 1;
+    // the point-charge reciprocal sum under shear takes its k list from the
+    // offset (and back to the fixed list without shear)
+    if (c.ewald_on && (was_sheared || p->strain_rate != 0.0)) {
+        const int r = setup_recip(c);
+        if (r) return fail(x, r, "smd_set_integrator: reciprocal set-up failed");
+    }
     c.graph_dirty = 1;
     touch(c);
     return SMD_OK;
@@ -1410,6 +1418,9 @@ static int integrator_begin(smd_ctx *x, bool new_start) {
             for (int d = 0; d < 3; d++)
                 c.npt_smin = std::max(c.npt_smin, c.grid.n[d] * (c.cutoff + c.cut_buffer) / c.box.L[d]);
     }
+    if (c.ip.strain_rate != 0.0 && (c.mp_on || c.vdw == VDW_BUFF || c.surface_on))
+        return fail(x, SMD_ERR_ARG,
+                    "smd_integrator_start: SLLOD shear takes no multipoles, buffered 14-7 or surface correction");
     launch_nlist(c, true);
     c.list_valid = 1;
     CK(cudaMemsetAsync(c.acc, 0, ACC_COUNT * sizeof(long long), c.stream));

@@ -47,6 +47,12 @@ struct Recip {               // Ewald reciprocal space (k half-space, k^2 < kcut
     long long *sk = nullptr; // [2][nk] structure factor, fixed point (SK_SCALE)
     double *kvec = nullptr;  // [3][nk] k in 1/nm
     int nmax = 0;            // largest |n| of any component
+    // sheared cell (SLLOD, point charges): the k list depends on the
+    // Lees-Edwards offset, so it is rebuilt on the device before every
+    // evaluation; nk is then the candidate capacity and nk_dev the count
+    int le = 0;
+    int le_nx = 0, le_ny = 0, le_nz = 0;   // candidates nx 0..le_nx, ny - round(nx t) and nz within +-le_ny, +-le_nz
+    int *nk_dev = nullptr;
     // FP32 passes of the polarisable model (built once per k set; the k list
     // is ordered column by column, nz ascending by one within a column)
     int nseg = 0, ncol = 0, ngrp = 0, row = 0, tab_n = 0;
@@ -306,6 +312,7 @@ __host__ __device__ inline void acc_energies(const long long *acc, double e_lrc,
 }
 void launch_buff(Ctx &c);
 int setup_cg(Ctx &c);
+int recip_nk(Ctx &c, int *nk);
 int ensure_ind_rows(Ctx &c);
 // dipole-guess network (smd_mlp.cu)
 int mlp_alloc(Ctx &c, long long cap_rows, unsigned int seed);

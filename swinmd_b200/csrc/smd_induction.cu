@@ -603,15 +603,17 @@ __global__ void __launch_bounds__(9 * MB_MOLS) k_mol_blocks(int n, int nmol, con
 
 // u = B_m^-1 v for every molecule, nine threads per molecule (thread e of a
 // molecule owns component e = 3 q + d, site q, axis d) in tiles of
-// CG_THREADS / 9 molecules per block; the components meet in shared memory.
+// at most CG_THREADS / 9 molecules, spread over the whole grid; the
+// components meet in shared memory.
 // in(m, e, i, idx) gives (and may update) component e of v, out(...) takes
 // u's component; the packed copy pk of u (one G4 per site) is written here.
 // Block-uniform loop: every thread of the block reaches each barrier.
 template <typename G4, typename GR, class FIn, class FOut>
 __device__ __forceinline__ void mol_tiles(const IndArgs &a, const double *blk, G4 *pk, double *s_v, double *s_u,
                                           FIn &&in, FOut &&out) {
-    constexpr int TM = CG_THREADS / 9;
     const int n = a.n, nmol = a.nmol;
+    // molecules per tile: spread over every block of the grid
+    const int TM = max(1, min(CG_THREADS / 9, (nmol + (int)gridDim.x - 1) / (int)gridDim.x));
     const int ml = threadIdx.x / 9, e = threadIdx.x - 9 * ml, q = e / 3, d = e - 3 * q;
     for (int m0 = blockIdx.x * TM; m0 < nmol; m0 += gridDim.x * TM) {
         const int m = m0 + ml;

@@ -14,6 +14,17 @@
 // exact 32-bit integer sum of n_a times the sites' 32-bit box fractions (the
 // wrap mod 2^32 is the wrap mod 2 pi), so the FP32 sine and cosine see an
 // argument in [-pi, pi) with no reduction error.
+//
+// Sheared cell (SLLOD with Lees-Edwards images; no reference code): the
+// images of the box with offset d form the lattice a1 = (Lx, 0, 0),
+// a2 = (d, Ly, 0), a3 = (0, 0, Lz), whose reciprocal vectors give
+// k(n) = 2 pi (nx / Lx, (ny - nx t) / Ly, nz / Lz), t = d / Lx, with d
+// reduced to [-Lx/2, Lx/2] (d and d + Lx are the same lattice).  The sums are
+// those above over the half space of n with |k| < kcut for that lattice, so
+// the k list changes with d: k_le_kset rebuilds it on the device before every
+// evaluation, in the order of the unsheared list (nx, ny, nz ascending), and
+// the passes read the live count from the device.  The phase is
+// n.(fractional coordinates): x's fraction becomes (x - d y / Ly) / Lx.
 #include <cmath>
 #include <vector>
 #include <algorithm>
@@ -39,21 +50,103 @@ __device__ __forceinline__ void sincos_phase(int ph, float &s, float &c) {
     c = fmaf(-b, sh, ch);
 }
 
-// partial[ch][2][nk]
+// the Lees-Edwards offset reduced to [-Lx/2, Lx/2]
+__device__ __forceinline__ double le_reduced(const double *le, const Box &b) {
+    const double d = le ? *le : 0.0;
+    return d - b.L[0] * floor(d * b.inv[0] + 0.5);
+}
+
+// sheared cell: the 32-bit fraction of x - dd y / Ly along a1
+__device__ __forceinline__ int le_xfrac(const double4 &p, double dd, const Box &b) {
+    return frac32(p.x - dd * (p.y * b.inv[1]), b.inv[0]);
+}
+
+// The k list of the sheared cell (one block): candidates (nx, m, nz) with
+// nx in [0, nxm], m in [-nyr, nyr], nz in [-nzm, nzm] and ny = m + rint(nx t)
+// cover every n with |k| < kcut (|ny - nx t| <= kcut Ly / 2 pi and
+// |nx t - rint(nx t)| <= 1/2).  Each thread takes a contiguous run of
+// candidates, counts its members, and after a block-wide exclusive scan
+// writes them in candidate order: nx, then ny, then nz ascending.
+constexpr int KSET_THREADS = 1024;
+__global__ void __launch_bounds__(KSET_THREADS) k_le_kset(int nxm, int nyr, int nzm, Box box, const double *le,
+                                                          double kc2, double aR4, double pi4V, int cap, int *kn,
+                                                          double *kvec, double *kcoef, int *nk_out) {
+    __shared__ int s_w[KSET_THREADS / 32];
+    const double PI2 = 6.283185307179586476925;
+    const double t = le_reduced(le, box) * box.inv[0];
+    const int nys = 2 * nyr + 1, nzs = 2 * nzm + 1;
+    const int total = (nxm + 1) * nys * nzs;
+    const int per = (total + KSET_THREADS - 1) / KSET_THREADS;
+    const int c0 = min(total, (int)threadIdx.x * per), c1 = min(total, c0 + per);
+    auto member = [&](int ci, int &nx, int &ny, int &nz, double &kx, double &ky, double &kz, double &k2) {
+        nx = ci / (nys * nzs);
+        const int r = ci - nx * nys * nzs;
+        const int m = r / nzs - nyr;
+        nz = r - (m + nyr) * nzs - nzm;
+        ny = m + (int)rint(nx * t);
+        if (!(nx > 0 || (nx == 0 && ny > 0) || (nx == 0 && ny == 0 && nz > 0))) return false;
+        kx = PI2 * nx * box.inv[0];
+        ky = PI2 * (ny - nx * t) * box.inv[1];
+        kz = PI2 * nz * box.inv[2];
+        k2 = kx * kx + ky * ky + kz * kz;
+        return k2 < kc2;
+    };
+    int cnt = 0;
+    for (int ci = c0; ci < c1; ci++) {
+        int nx, ny, nz;
+        double kx, ky, kz, k2;
+        if (member(ci, nx, ny, nz, kx, ky, kz, k2)) cnt++;
+    }
+    // exclusive scan of cnt over the block
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int inc = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
+    }
+    if (lane == 31) s_w[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        int v = s_w[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += u;
+        }
+        s_w[lane] = v;   // inclusive totals per warp
+    }
+    __syncthreads();
+    int k = inc - cnt + (w > 0 ? s_w[w - 1] : 0);
+    if (threadIdx.x == KSET_THREADS - 1) *nk_out = k + cnt;
+    for (int ci = c0; ci < c1 && k < cap; ci++) {
+        int nx, ny, nz;
+        double kx, ky, kz, k2;
+        if (!member(ci, nx, ny, nz, kx, ky, kz, k2)) continue;
+        kn[k] = nx; kn[cap + k] = ny; kn[2 * cap + k] = nz;
+        kvec[k] = kx; kvec[cap + k] = ky; kvec[2 * cap + k] = kz;
+        kcoef[k] = pi4V * (exp(-k2 * aR4) / k2);
+        k++;
+    }
+}
+
+// partial[ch][2][nk]; nk is the stride of the k arrays, *nkd (when given)
+// the live count; le (sheared cell) the device offset
 template <typename R>
-__global__ void __launch_bounds__(RK_THREADS) k_sk_partial(int n, int nk, const double4 *pos4,
+__global__ void __launch_bounds__(RK_THREADS) k_sk_partial(int n, int nk, const int *nkd, const double4 *pos4,
                                                            const int4 *fixq, const int *kn,
                                                            const double *kvec, const double *tq,
-                                                           double *partial) {
+                                                           Box box, const double *le, double *partial) {
     __shared__ double4 s_p[RK_THREADS];
     __shared__ int4 s_f[RK_THREADS];
     const int k = blockIdx.x * RK_THREADS + threadIdx.x;
+    const int nkv = nkd ? *nkd : nk;
+    if ((int)(blockIdx.x * RK_THREADS) >= nkv) return;   // block-uniform: no k of this block is live
     const int ch = blockIdx.y;
     const int per = (n + RK_CHUNKS - 1) / RK_CHUNKS;
     const int s0 = ch * per, s1 = min(n, s0 + per);
+    const double dd = le ? le_reduced(le, box) : 0.0;
     int nx = 0, ny = 0, nz = 0;
     double kx = 0, ky = 0, kz = 0;
-    if (k < nk) {
+    if (k < nkv) {
         nx = kn[k]; ny = kn[nk + k]; nz = kn[2 * nk + k];
         kx = kvec[k]; ky = kvec[nk + k]; kz = kvec[2 * nk + k];
     }
@@ -62,12 +155,17 @@ __global__ void __launch_bounds__(RK_THREADS) k_sk_partial(int n, int nk, const 
         const int i = base + threadIdx.x;
         __syncthreads();
         if (i < s1) {
-            if (sizeof(R) == 8) s_p[threadIdx.x] = pos4[i];
-            else s_f[threadIdx.x] = fixq[i];
+            if (sizeof(R) == 8) {
+                s_p[threadIdx.x] = pos4[i];
+            } else {
+                int4 f = fixq[i];
+                if (le) f.x = le_xfrac(pos4[i], dd, box);
+                s_f[threadIdx.x] = f;
+            }
         }
         __syncthreads();
         const int cnt = min(RK_THREADS, s1 - base);
-        if (k < nk) {
+        if (k < nkv) {
             for (int q = 0; q < cnt; q++) {
                 R s, c, qi;
                 if (sizeof(R) == 8) {
@@ -91,18 +189,20 @@ __global__ void __launch_bounds__(RK_THREADS) k_sk_partial(int n, int nk, const 
             }
         }
     }
-    if (k < nk) {
+    if (k < nkv) {
         partial[(size_t)ch * 2 * nk + k] = cs;
         partial[(size_t)ch * 2 * nk + nk + k] = sn;
     }
 }
 
 // S(k) in fixed chunk order; energy and long virial per k.
-__global__ void k_sk_reduce(int nk, const double *partial, const double *kcoef, const double *kvec,
+__global__ void k_sk_reduce(int nk, const int *nkd, const double *partial, const double *kcoef, const double *kvec,
                             double alphaR4, double *sk, long long *acc) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nkv = nkd ? *nkd : nk;
+    if ((int)(blockIdx.x * blockDim.x) >= nkv) return;   // block-uniform
     double e = 0, vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
-    if (k < nk) {
+    if (k < nkv) {
         double cs = 0, sn = 0;
         for (int ch = 0; ch < RK_CHUNKS; ch++) {
             cs += partial[(size_t)ch * 2 * nk + k];
@@ -145,11 +245,11 @@ __global__ void k_sk_reduce(int nk, const double *partial, const double *kcoef, 
 
 // Per-site reciprocal force; RF_TPS threads split the k set.
 template <typename R>
-__global__ void __launch_bounds__(256) k_recip_force(int n, int nk, const double4 *pos4,
+__global__ void __launch_bounds__(256) k_recip_force(int n, int nk, const int *nkd, const double4 *pos4,
                                                      const int4 *fixq, const int *kn,
                                                      const double *kvec, const double *kcoef,
-                                                     const double *sk, const double *tq,
-                                                     long long *frc) {
+                                                     const double *sk, const double *tq, Box box,
+                                                     const double *le, long long *frc) {
     __shared__ int s_n[3][256];
     // k vectors, prefactors and S(k) stay FP64; only the phase and its
     // sine/cosine follow R (the FP32 path's cost is in sincospif)
@@ -162,13 +262,18 @@ __global__ void __launch_bounds__(256) k_recip_force(int n, int nk, const double
     R qi = 0;
     if (i < n) {
         if (sizeof(R) == 8) { p64 = pos4[i]; qi = (R)tq[(int)p64.w]; }
-        else { pf = fixq[i]; qi = (R)tq[pf.w]; }
+        else {
+            pf = fixq[i];
+            if (le) pf.x = le_xfrac(pos4[i], le_reduced(le, box), box);
+            qi = (R)tq[pf.w];
+        }
     }
+    const int nkv = nkd ? *nkd : nk;
     double fx = 0, fy = 0, fz = 0;
-    for (int base = 0; base < nk; base += 256) {
+    for (int base = 0; base < nkv; base += 256) {
         __syncthreads();
         const int k = base + threadIdx.x;
-        if (k < nk) {
+        if (k < nkv) {
             s_n[0][threadIdx.x] = kn[k]; s_n[1][threadIdx.x] = kn[nk + k]; s_n[2][threadIdx.x] = kn[2 * nk + k];
             s_k[0][threadIdx.x] = kvec[k]; s_k[1][threadIdx.x] = kvec[nk + k];
             s_k[2][threadIdx.x] = kvec[2 * nk + k];
@@ -177,7 +282,7 @@ __global__ void __launch_bounds__(256) k_recip_force(int n, int nk, const double
             s_s[threadIdx.x] = sk[nk + k];
         }
         __syncthreads();
-        const int cnt = min(256, nk - base);
+        const int cnt = min(256, nkv - base);
         if (i < n) {
             double ax = 0, ay = 0, az = 0;
             for (int q = t; q < cnt; q += RF_TPS) {
@@ -214,9 +319,39 @@ __global__ void __launch_bounds__(256) k_recip_force(int n, int nk, const double
     }
 }
 
+// sheared cell: capacity for every candidate of k_le_kset
+static int setup_recip_le(Ctx &c) {
+    const double PI = 3.14159265358979323846;
+    const double kCut = c.ew_kcut;
+    c.rc.le_nx = (int)(kCut * c.box.L[0] / (2 * PI));
+    c.rc.le_ny = (int)(kCut * c.box.L[1] / (2 * PI)) + 1;
+    c.rc.le_nz = (int)(kCut * c.box.L[2] / (2 * PI));
+    const long long cap = (long long)(c.rc.le_nx + 1) * (2 * c.rc.le_ny + 1) * (2 * c.rc.le_nz + 1);
+    if (cap > (1 << 26)) return SMD_ERR_ARG;
+    const int nk = (int)cap;
+    c.rc.nk = nk;
+    c.rc.nmax = std::max(c.rc.le_nx + c.rc.le_ny, c.rc.le_nz);
+    auto realloc = [](auto **p, size_t cnt) -> bool {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+        return cudaMalloc((void **)p, (cnt ? cnt : 1) * sizeof(**p)) == cudaSuccess;
+    };
+    if (!realloc(&c.rc.kn, 3 * (size_t)nk) || !realloc(&c.rc.kvec, 3 * (size_t)nk) ||
+        !realloc(&c.rc.kcoef, (size_t)nk) || !realloc(&c.rc.sk, 6 * (size_t)nk * RK_CHUNKS + 6 * (size_t)nk) ||
+        !realloc(&c.rc.nk_dev, 1))
+        return SMD_ERR_CUDA;
+    if (cudaMemset(c.rc.nk_dev, 0, sizeof(int)) != cudaSuccess) return SMD_ERR_CUDA;
+    c.rc.le = 1;
+    c.graph_dirty = 1;
+    return 0;
+}
+
 int setup_recip(Ctx &c) {
     const double PI = 3.14159265358979323846;
     if (!(c.ewald_on || c.mp_on) || c.box.L[0] <= 0) return 0;
+    // SLLOD shear with the point-charge sum: the k list follows the offset
+    if (c.ewald_on && !c.mp_on && c.integrator_ready && c.ip.strain_rate != 0.0) return setup_recip_le(c);
+    c.rc.le = 0;
     const double kCut = c.ew_kcut, kCut2 = kCut * kCut;
     const double alpha2 = c.ew_alpha * c.ew_alpha, alphaR4 = 1.0 / (4.0 * alpha2);
     const int nxMax = (int)(kCut * c.box.L[0] / (2 * PI));
@@ -270,6 +405,16 @@ int setup_recip(Ctx &c) {
     return c.mp_on ? mp_recip_prepare(c) : 0;
 }
 
+// the live k count (the sheared cell's list is built on the device)
+int recip_nk(Ctx &c, int *nk) {
+    if (!c.rc.le) {
+        *nk = c.rc.nk;
+        return 0;
+    }
+    if (cudaStreamSynchronize(c.stream) != cudaSuccess) return SMD_ERR_CUDA;
+    return cudaMemcpy(nk, c.rc.nk_dev, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : SMD_ERR_CUDA;
+}
+
 void launch_recip(Ctx &c) {
     const int nk = c.rc.nk;
     if (nk == 0) return;
@@ -277,24 +422,35 @@ void launch_recip(Ctx &c) {
     double *partial = (double *)c.rc.sk;
     double *sk = partial + (size_t)2 * nk * RK_CHUNKS;
     const double alphaR4 = 1.0 / (4.0 * c.ew_alpha * c.ew_alpha);
+    // sheared cell: the offset is the integrator's (zero before it starts)
+    const bool le = c.rc.le && c.integrator_ready && c.ip.strain_rate != 0.0;
+    const double *led = le ? c.scal + SC_LE : nullptr;
+    const int *nkd = c.rc.le ? c.rc.nk_dev : nullptr;
+    if (c.rc.le) {
+        const double vol = c.box.L[0] * c.box.L[1] * c.box.L[2];
+        k_le_kset<<<1, KSET_THREADS, 0, c.stream>>>(c.rc.le_nx, c.rc.le_ny, c.rc.le_nz, c.box, led,
+                                                    c.ew_kcut * c.ew_kcut, alphaR4,
+                                                    4.0 * 3.14159265358979323846 * (1.0 / vol), nk, c.rc.kn,
+                                                    c.rc.kvec, c.rc.kcoef, c.rc.nk_dev);
+    }
     dim3 g1((nk + RK_THREADS - 1) / RK_THREADS, RK_CHUNKS);
     const bool mixed = c.precision == SMD_PREC_MIXED;
     if (mixed) {
-        k_sk_partial<float><<<g1, RK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn,
-                                                             c.rc.kvec, c.type_q, partial);
+        k_sk_partial<float><<<g1, RK_THREADS, 0, c.stream>>>(c.n, nk, nkd, c.pos4, c.fixq, c.rc.kn,
+                                                             c.rc.kvec, c.type_q, c.box, led, partial);
     } else {
-        k_sk_partial<double><<<g1, RK_THREADS, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn,
-                                                              c.rc.kvec, c.type_q, partial);
+        k_sk_partial<double><<<g1, RK_THREADS, 0, c.stream>>>(c.n, nk, nkd, c.pos4, c.fixq, c.rc.kn,
+                                                              c.rc.kvec, c.type_q, c.box, led, partial);
     }
-    k_sk_reduce<<<(nk + 255) / 256, 256, 0, c.stream>>>(nk, partial, c.rc.kcoef, c.rc.kvec,
+    k_sk_reduce<<<(nk + 255) / 256, 256, 0, c.stream>>>(nk, nkd, partial, c.rc.kcoef, c.rc.kvec,
                                                         alphaR4, sk, c.acc);
     const int nb = (int)(((long long)c.n * RF_TPS + 255) / 256);
     if (mixed) {
-        k_recip_force<float><<<nb, 256, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,
-                                                       c.rc.kcoef, sk, c.type_q, c.frc);
+        k_recip_force<float><<<nb, 256, 0, c.stream>>>(c.n, nk, nkd, c.pos4, c.fixq, c.rc.kn, c.rc.kvec,
+                                                       c.rc.kcoef, sk, c.type_q, c.box, led, c.frc);
     } else {
-        k_recip_force<double><<<nb, 256, 0, c.stream>>>(c.n, nk, c.pos4, c.fixq, c.rc.kn,
-                                                        c.rc.kvec, c.rc.kcoef, sk, c.type_q, c.frc);
+        k_recip_force<double><<<nb, 256, 0, c.stream>>>(c.n, nk, nkd, c.pos4, c.fixq, c.rc.kn,
+                                                        c.rc.kvec, c.rc.kcoef, sk, c.type_q, c.box, led, c.frc);
     }
 }
 

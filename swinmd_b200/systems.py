@@ -604,6 +604,40 @@ def spce_water(nmol: int = 2160, box: float = 4.03, seed: int = 1, temperature: 
                   bond_params=[(0, 1, 0.1, 345000.0)], angle_params=[(0, 1, 0, 109.47, 383.0)])
 
 
+def spce_flexible(nmol: int = 343, box: float = None, seed: int = 1, temperature: float = 298.0,
+                  cutoff: float = 0.9, skin: float = 0.1, alpha: float = 3.1, kmax: int = None,
+                  dt: float = 0.0005, tau: float = 0.1, strain_rate: float = 0.0,
+                  n_steps: int = 1000) -> System:
+    """Flexible SPC/E-like water for the chain integrator: the charges, LJ
+    and geometry of ``spce_water`` held by harmonic O-H bonds
+    (k = 345000 kJ/mol/nm^2) and a harmonic H-O-H angle (383 kJ/mol/rad^2)
+    instead of constraints, at the 2160-molecule case's density, |n| < kmax
+    (default: 9 scaled with the box), each molecule whole around its centre
+    of mass, and SLLOD planar Couette shear at ``strain_rate`` (1/ps)."""
+    if box is None:
+        box = 4.03 * (nmol / 2160.0) ** (1.0 / 3.0)
+    if kmax is None:
+        kmax = max(4, int(round(9 * box / 4.03)))
+    s = spce_water(nmol=nmol, box=box, seed=seed, temperature=temperature, cutoff=cutoff, skin=skin,
+                   alpha=alpha, kmax=kmax, dt=dt, n_steps=n_steps)
+    # whole molecules: each H next to its O, then the molecule shifted by
+    # the image of its centre of mass
+    pos = s.pos.reshape(nmol, 3, 3).copy()
+    pos -= box * np.round((pos - pos[:, 1:2, :]) / box)
+    mass = np.array([1.008, 15.9994, 1.008])
+    com = (pos * mass[None, :, None]).sum(1) / mass.sum()
+    pos = pos + (_wrap(com, box) - com)[:, None, :]
+    c = s.config
+    c.constraint = 0
+    c.bend_type = 1
+    c.thermostat = "NoseHoover"
+    c.coupl_const = tau
+    c.long_correct = False
+    c.test_mode = 2 if strain_rate else 0
+    c.rate = strain_rate
+    return s.replace(name=f"spcf{nmol}", pos=pos.reshape(-1, 3))
+
+
 def polarizable_water(nmol: int = 4096, density_gcc: float = 0.997, seed: int = 1,
                       temperature: float = 298.0, cutoff: float = 0.9, skin: float = 0.1,
                       switch: float = 0.8, alpha: float = 3.5, kmax: int = 20, dt: float = 0.001,
