@@ -1,7 +1,8 @@
 """Benchmark of the SwinMD B200 step: ns/day of one system on each GPU.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload polwater4096|lj4000|replicas64|water_replicas64]
+                    [--workload polwater4096|lj4000|replicas64|water_replicas64|
+                                water_shear_replicas64]
 
 Default workload: rigid polarisable multipole water, 4096 molecules (12,288
 sites), the configuration the headline metric is quoted on.  The seeded
@@ -161,7 +162,7 @@ def cpu_reference(s, steps, timeout=1800):
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
-    if args.workload in ("replicas64", "water_replicas64"):
+    if args.workload in REPLICA_WORKLOADS:
         return run_reference_replicas(args, world)
     s, desc = workload(args.workload)
     # the reference's dense dipole matrix makes one polwater4096 step take
@@ -194,8 +195,10 @@ def run_reference_replicas(args, world):
     if not os.path.exists(refdump.REF_DUMP):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_dump is not built"}))
         return
-    water = args.workload == "water_replicas64"
-    reps = systems.water_replica_set(count=64, seed=1) if water else systems.replica_set(count=64, seed=1)
+    water = args.workload != "replicas64"
+    flexible = args.workload == "water_shear_replicas64"
+    reps = (systems.water_replica_set(count=64, seed=1, flexible=flexible) if water
+            else systems.replica_set(count=64, seed=1))
     cores = max(1, min(64, os.cpu_count() or 1))
     steps = max(1, min(args.steps, 5 if water else 50))
 
@@ -211,9 +214,7 @@ def run_reference_replicas(args, world):
         sps = list(ex.map(one, reps[:cores]))
     dt = reps[0].config.timestep
     v = sum(ns_per_day(x, dt) for x in sps)
-    metric = ("aggregate ns/day of 64 batched LJ/Ewald water replicas (uneven sizes, per-replica seeds and "
-              "Nose-Hoover thermostats)" if water else
-              "aggregate ns/day of 64 batched LJ replicas (uneven sizes, per-replica shear and Nose-Hoover chain)")
+    metric = REPLICA_METRICS[args.workload]
     print(json.dumps({
         "metric": metric,
         "value": v, "unit": "ns/day", "impl": "reference", "n_gpus": world, "steps": steps, "warmup": 0,
@@ -221,8 +222,20 @@ def run_reference_replicas(args, world):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": {"workload": args.workload},
         "cpu_baseline": {"value": v, "unit": "ns/day", "cores": cores, "kind": "reference",
                          "sample": f"{cores} concurrent SwinMD processes (one per core), {steps} steps "
-                                   "each of the first replicas at zero shear, LFIntegrator::run"},
+                                   "each of the first replicas at zero shear (the reference has no SLLOD), "
+                                   "LFIntegrator::run"},
         "e2e": {"value": v, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+REPLICA_WORKLOADS = ("replicas64", "water_replicas64", "water_shear_replicas64")
+REPLICA_METRICS = {
+    "replicas64": "aggregate ns/day of 64 batched LJ replicas (uneven sizes, per-replica shear and Nose-Hoover "
+                  "chain)",
+    "water_replicas64": "aggregate ns/day of 64 batched LJ/Ewald water replicas (uneven sizes, per-replica seeds "
+                        "and Nose-Hoover thermostats)",
+    "water_shear_replicas64": "aggregate ns/day of 64 batched LJ/Ewald water replicas (uneven sizes, per-replica "
+                              "strain rates and Nose-Hoover chains)",
+}
 
 
 def run_replicas(args, rank, world, local):
@@ -230,17 +243,21 @@ def run_replicas(args, rank, world, local):
     all replicas and ranks.  replicas64: LJ fluids (sizes log-uniform
     500-8000 atoms, strain rates uniform 0-0.2 reduced, own Nose-Hoover
     chains); water_replicas64: rigid LJ + Ewald waters (500-8000 molecules,
-    own seeds and Nose-Hoover thermostats, SHAKE, zero shear)."""
+    own seeds and Nose-Hoover thermostats, SHAKE, zero shear);
+    water_shear_replicas64: flexible LJ + Ewald waters (500-8000 molecules,
+    strain rates uniform 0-0.2 reduced under SLLOD with the sheared Ewald
+    sum, own Nose-Hoover chains)."""
     import torch
     from swinmd_b200 import engine, systems
     torch.cuda.set_device(local)
-    water = args.workload == "water_replicas64"
-    reps = (systems.water_replica_set(count=64, seed=1 + rank) if water
+    water = args.workload != "replicas64"
+    flexible = args.workload == "water_shear_replicas64"
+    reps = (systems.water_replica_set(count=64, seed=1 + rank, flexible=flexible) if water
             else systems.replica_set(count=64, seed=1 + rank))
     ens, integ = [], []
     for s in reps:
         e = engine.GpuEnsemble(s, precision="mixed", device=local)
-        nh = engine.LFIntegrator(e) if water else engine.NHIntegrator(e)
+        nh = engine.LFIntegrator(e) if water and not flexible else engine.NHIntegrator(e)
         nh.start()
         ens.append(e)
         integ.append(nh)
@@ -319,13 +336,18 @@ def run_replicas(args, rank, world, local):
     peak = 148 * 128 * 2 * 1.965e9 / 1e12
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and water:
-        sample = systems.spce_water(nmol=512, box=2.4953, cutoff=0.9, kmax=6, seed=11, n_steps=20)
+        if flexible:
+            sample = systems.spce_flexible(nmol=512, box=2.4953, cutoff=0.9, kmax=6, seed=11, n_steps=20)
+        else:
+            sample = systems.spce_water(nmol=512, box=2.4953, cutoff=0.9, kmax=6, seed=11, n_steps=20)
         sps = cpu_reference(sample, 20)
         if sps:
+            kind = "flexible" if flexible else "rigid"
             cpu = {"value": ns_per_day(sps, sample.config.timestep), "unit": "ns/day", "cores": 1,
                    "kind": "reference",
-                   "sample": "20 steps of one 512-molecule water with SwinMD's own LFIntegrator::run, "
-                             "one process, one core; 64 such processes on 64 cores would give 64x this"}
+                   "sample": f"20 steps of one 512-molecule {kind} water at zero shear (the reference has "
+                             "no SLLOD) with SwinMD's own LFIntegrator::run, one process, one core; 64 such "
+                             "processes on 64 cores would give 64x this"}
     elif rank == 0 and not args.no_cpu_baseline:
         sample = systems.lj_fluid(ncell=8, seed=5, n_steps=50)
         sample.config.long_correct = True
@@ -335,11 +357,38 @@ def run_replicas(args, rank, world, local):
                    "sample": "50 steps of one 2048-atom replica at zero shear with SwinMD's own "
                              "LFIntegrator::run (the reference has no SLLOD), one process, one core; "
                              "64 such processes on 64 cores would give 64x this"}
-    if rank == 0 and water:
+    if rank == 0 and flexible:
+        nmol = sum(s.n_mols for s in reps)
+        rates = [s.config.rate for s in reps]
+        print(json.dumps({
+            "metric": REPLICA_METRICS[args.workload],
+            "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 pair and reciprocal math on exact fractions, f64 bonded terms and integrator",
+            "data": "synthetic (seeded lattices, random orientations, Maxwell-Boltzmann velocities)",
+            "config": {"workload": f"water_shear_replicas64: 64 flexible SPC/E-like waters, {nmol} molecules "
+                                   "in total, sizes log-uniform 500-8000 molecules at 0.997 g/cm3, harmonic "
+                                   "O-H bonds and H-O-H angle, LJ on O + Ewald (alpha 3.1/nm, rc 1.0 nm, kmax "
+                                   "scaled with the box from 9 at 4.03 nm; the sheared cell's k list rebuilt "
+                                   "every step), SLLOD with Lees-Edwards images at strain rates uniform 0-0.2 "
+                                   "reduced (sigma_O sqrt(m/eps_O) = 1.666 ps), NH chain 298 K tau 0.1 ps, "
+                                   "dt 0.5 fs; one CUDA graph per step over all replicas",
+                       "replicas": len(reps) * world, "l2": "256 MB buffer written before every chunk",
+                       "parallelism": "replicas only",
+                       "strain_rate_per_ps": {"min": min(rates), "max": max(rates)}},
+            "autotuned_threads_per_site": [int(x) for x in tpp],
+            "force_rms_rel_err_vs_fp64": {"max": max(errs), "median": float(np.median(errs))},
+            "e2e": {"value": e2e, "unit": "ns/day", "h2d_bytes_per_step": natoms * 6 * 8 / every,
+                    "d2h_bytes_per_step": natoms * 9 * 8 / every},
+            "gpu_launches": launches * args.steps,
+            "roofline": {"bound": "fp32", "kernel": "k_pair (LJ + Ewald real) over the whole step",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": None, "peak_source": "nominal FP32 SIMT rate at the measured max SM clock"},
+            "clocks": clocks, "cpu_baseline": cpu}))
+    elif rank == 0 and water:
         nmol = sum(s.n_mols for s in reps)
         print(json.dumps({
-            "metric": "aggregate ns/day of 64 batched LJ/Ewald water replicas (uneven sizes, per-replica "
-                      "seeds and Nose-Hoover thermostats)",
+            "metric": REPLICA_METRICS[args.workload],
             "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 pair and reciprocal math on exact fractions, f64 SHAKE and integrator",
@@ -362,8 +411,7 @@ def run_replicas(args, rank, world, local):
             "clocks": clocks, "cpu_baseline": cpu}))
     elif rank == 0:
         print(json.dumps({
-            "metric": "aggregate ns/day of 64 batched LJ replicas (uneven sizes, per-replica shear and "
-                      "Nose-Hoover chain)",
+            "metric": REPLICA_METRICS[args.workload],
             "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 pair math on exact fractions, f64 integrator",
@@ -433,7 +481,7 @@ def main():
         if dist:
             dist.destroy_process_group()
         return
-    if args.workload in ("replicas64", "water_replicas64"):
+    if args.workload in REPLICA_WORKLOADS:
         run_replicas(args, rank, world, local)
         if dist:
             dist.destroy_process_group()

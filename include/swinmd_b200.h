@@ -129,7 +129,11 @@ typedef struct {
     int atom_ndf;          /* degrees of freedom (Integrator.cpp:22-27) */
     int mol_ndf;
     double strain_rate;    /* SLLOD planar Couette rate du_x/dy (1/ps); 0: equilibrium.
-                              Needs SMD_THERMO_NH_CHAIN and short-range terms only */
+                              Needs SMD_THERMO_NH_CHAIN; takes the pair terms,
+                              the point-charge Ewald sum (over the sheared cell's
+                              k list, rebuilt on the device every evaluation)
+                              and bonded terms, not multipoles, the buffered
+                              14-7 or the surface correction */
 } smd_integrator_params;
 
 /* Per-step observables the reference keeps in Ensemble/Integrator members. */

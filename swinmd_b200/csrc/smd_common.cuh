@@ -142,6 +142,22 @@ __device__ __forceinline__ int frac32(double x, double invL) {
     return (int)(unsigned int)(v & 0xffffffffLL);
 }
 
+// Box fractions of a site for the FP32 path.  Under Lees-Edwards images (le)
+// a site outside [-Ly/2, Ly/2) in y (molecules are wrapped whole, by their
+// centre, so a site can stick out) is first taken to its image inside,
+// which moves x by -/+ delta per box crossed in y: the fractions then belong
+// to an image of the site, as le_dx_frac requires of both partners.
+__device__ __forceinline__ int4 site_frac(double4 p, const Box &b, bool le, double delta) {
+    if (le) {
+        const double w = floor(p.y * b.inv[1] + 0.5);
+        if (w != 0.0) {
+            p.y -= w * b.L[1];
+            p.x -= w * delta;
+        }
+    }
+    return make_int4(frac32(p.x, b.inv[0]), frac32(p.y, b.inv[1]), frac32(p.z, b.inv[2]), (int)p.w);
+}
+
 // Warp helpers ---------------------------------------------------------------
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {

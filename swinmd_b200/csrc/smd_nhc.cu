@@ -238,9 +238,7 @@ __global__ void __launch_bounds__(NHC_BLOCK) k_nhc_first(NhcArgs a) {
                 p.x += wx; p.y += wy; p.z += wz;
                 a.pos4[at] = p;
             }
-            if (a.write_fixq)
-                a.fixq[at] = make_int4(frac32(p.x, a.box.inv[0]), frac32(p.y, a.box.inv[1]),
-                                       frac32(p.z, a.box.inv[2]), (int)p.w);
+            if (a.write_fixq) a.fixq[at] = site_frac(p, a.box, g != 0.0, delta);
         }
     }
     if (__any_sync(0xffffffffu, rebuild) && (threadIdx.x & 31) == 0) atomicOr(&a.flags[0], 1);

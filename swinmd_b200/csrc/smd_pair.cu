@@ -674,13 +674,12 @@ static void dispatch_vdw(Ctx &c, const PairArgs &a) {
     }
 }
 
-// Converts FP64 master positions to box fractions for the FP32 path.
-__global__ void k_fixq(int n, const double4 *pos4, int4 *fixq, Box b) {
+// Converts FP64 master positions to box fractions for the FP32 path (le:
+// the Lees-Edwards offset on the device under shear, else null).
+__global__ void k_fixq(int n, const double4 *pos4, int4 *fixq, Box b, const double *le) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    double4 p = pos4[i];
-    fixq[i] = make_int4(frac32(p.x, b.inv[0]), frac32(p.y, b.inv[1]), frac32(p.z, b.inv[2]),
-                        (int)p.w);
+    fixq[i] = site_frac(pos4[i], b, le != nullptr, le ? *le : 0.0);
 }
 
 // Charge sites of the Wolf summation (WolfForce::DummyPosition,
@@ -756,7 +755,8 @@ __global__ void k_buff_distribute(int n, const int *mol, const int *mol_off, con
 }
 
 void launch_fixq(Ctx &c) {
-    k_fixq<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.pos4, c.fixq, c.box);
+    const double *le = c.ip.strain_rate != 0.0 && c.integrator_ready ? c.scal + SC_LE : nullptr;
+    k_fixq<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.pos4, c.fixq, c.box, le);
 }
 
 // WolfForce::real_term's shifts: e(rc) = erfc(a rc)/rc and the force term

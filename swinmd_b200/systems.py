@@ -695,20 +695,33 @@ def constraint_lengths(s: System) -> np.ndarray:
     return out
 
 
+# time unit of the water model's LJ reduced units: sigma_O sqrt(m_water / eps_O) (ps)
+WATER_TAU = 0.3166 * math.sqrt(18.0154 / 0.650)
+
+
 def water_replica_set(count: int = 64, n_min: int = 500, n_max: int = 8000, seed: int = 1,
-                      n_steps: int = 5000) -> list:
-    """Independent rigid SPC/E-like waters (LJ + Ewald, SHAKE, Nose-Hoover)
-    for batched runs: molecule counts log-uniform in [n_min, n_max], boxes at
-    the density of the 2160-molecule case (4.03 nm), |n| < kmax with kmax
-    scaled with the box from 9 at 4.03 nm, one seed each.  At zero shear:
-    Ewald under shear is not built."""
+                      n_steps: int = 5000, flexible: bool = False, rate_max_star: float = 0.2) -> list:
+    """Independent SPC/E-like waters (LJ on O + Ewald) for batched runs:
+    molecule counts log-uniform in [n_min, n_max], boxes at the density of
+    the 2160-molecule case (4.03 nm), |n| < kmax with kmax scaled with the
+    box from 9 at 4.03 nm, rc 1.0 nm, one seed each.  Rigid (default): SHAKE
+    and the leap-frog Nose-Hoover thermostat at zero shear.  flexible: bonds
+    and angle (``spce_flexible``, dt 0.5 fs), each with its own strain rate
+    uniform in [0, rate_max_star] reduced units (1 / WATER_TAU) for SLLOD and
+    its own Nose-Hoover chain."""
     rng = np.random.default_rng(seed)
     out = []
     for r in range(count):
         n = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
         box = 4.03 * (n / 2160.0) ** (1.0 / 3.0)
         kmax = max(5, int(round(9 * box / 4.03)))
-        out.append(spce_water(nmol=n, box=box, cutoff=1.0, kmax=kmax, seed=seed * 1000 + r, n_steps=n_steps))
+        if flexible:
+            rate = float(rng.uniform(0.0, rate_max_star)) / WATER_TAU
+            out.append(spce_flexible(nmol=n, box=box, cutoff=1.0, kmax=kmax, seed=seed * 1000 + r,
+                                     strain_rate=rate, n_steps=n_steps))
+        else:
+            out.append(spce_water(nmol=n, box=box, cutoff=1.0, kmax=kmax, seed=seed * 1000 + r,
+                                  n_steps=n_steps))
     return out
 
 

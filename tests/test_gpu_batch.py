@@ -82,3 +82,36 @@ def test_water_batch_matches_single_runs():
     batch.close()
     for e, _ in alone + together:
         e.close()
+
+
+def test_sheared_water_batch_matches_single_runs():
+    # flexible LJ + Ewald water replicas with their own strain rates (SLLOD,
+    # the sheared cell's k list) and Nose-Hoover chains in one graph
+    reps = systems.water_replica_set(count=3, n_min=300, n_max=900, seed=6, n_steps=20, flexible=True,
+                                     rate_max_star=4.0)
+    assert len({s.config.rate for s in reps}) == 3 and min(s.config.rate for s in reps) > 0
+
+    def build():
+        out = []
+        for s in reps:
+            e = engine.GpuEnsemble(s, precision="mixed")
+            nh = engine.NHIntegrator(e)
+            nh.start()
+            out.append((e, nh))
+        return out
+
+    alone = build()
+    for _, nh in alone:
+        nh.run(20)
+    together = build()
+    batch = engine.ReplicaBatch([e for e, _ in together])
+    batch.run(20)
+    for (ea, la), (eb, lb) in zip(alone, together):
+        a, b = ea.state(), eb.state()
+        assert np.array_equal(a["pos"], b["pos"]) and np.array_equal(a["vel"], b["vel"])
+        oa, ob = la.observables(), lb.observables()
+        assert oa.e_potential == ob.e_potential
+        assert oa.shear_offset == ob.shear_offset and oa.shear_offset > 0
+    batch.close()
+    for e, _ in alone + together:
+        e.close()

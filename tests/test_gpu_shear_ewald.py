@@ -18,7 +18,19 @@ RATE = 5.0   # 1/ps: moves the offset by about 0.1 nm in 40 steps of 0.5 fs
 
 
 def _sys(rate=RATE, nmol=343):
-    return systems.spce_flexible(nmol=nmol, seed=2, strain_rate=rate)
+    """The seeded waters sit on a grid whose outer layer keeps clear of the
+    box faces; shifted in y by a part of the grid spacing and wrapped by
+    their centres, some molecules straddle the y faces, so that sites stick
+    out of the box (the case the sheared images must get right)."""
+    s = systems.spce_flexible(nmol=nmol, seed=2, strain_rate=rate)
+    L = s.box[1]
+    a = L / int(np.ceil(nmol ** (1.0 / 3.0) - 1e-9))
+    pos = s.pos.reshape(-1, 3, 3) + np.array([0.0, 0.45 * a, 0.0])
+    m = np.array([1.008, 15.9994, 1.008])
+    com = (pos * m[None, :, None]).sum(1) / m.sum()
+    pos += (com - L * np.floor(com / L + 0.5) - com)[:, None, :]
+    s.pos = pos.reshape(-1, 3)
+    return s
 
 
 def rms_rel(a, b):
@@ -56,6 +68,9 @@ def test_sheared_forces_match_oracle(precision, tol):
     ens.set_precision(precision)
     f, e, w = ens.compute_forces()
     st = ens.state()
+    # molecules are wrapped whole, so some sites stick out of the box in y:
+    # the FP32 path must take them to their Lees-Edwards image
+    assert (np.abs(st["pos"][:, 1]) >= 0.5 * s.box[1]).any()
     ref = oracle.flex_le_forces(s, st["pos"], s.box[0], delta)
     assert ens.ewald_nk() == ref["nk"]
     err = rms_rel(f, ref["force"])
