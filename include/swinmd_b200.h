@@ -421,6 +421,33 @@ int smd_set_integrator(smd_ctx *ctx, const smd_integrator_params *p);
  * dU/dV, out[2] = d2U/dV2, tail correction included; under constraints the
  * pair term takes r_ij . R_ij with R_ij the molecules' centre difference. */
 int smd_lustig_lj(smd_ctx *ctx, double *out);
+/* Every field of Ensemble::myLustig (src/Ensemble.h:77-108) at the current
+ * configuration, as the reference's force terms write them during a step:
+ * the LJ (LJForce.cpp:136-250) or buffered 14-7 (BuffvdWForce.cpp:244-335)
+ * values, the point-charge Ewald sums' real, intramolecular, surface and
+ * reciprocal derivatives (EwaldForce.cpp:129-192, 405-411, 596-675,
+ * 770-790, 850-863), the multipoles' (Multipole.cpp:163-240 with the torque
+ * mapping's dU/dV, :1946-2134), the induced dipoles' (Induction.cpp:486-590),
+ * and bonds and Urey-Bradley (BondForce.cpp:86-105,
+ * UreyBradleyForce.cpp:76-95).  Positions with constraints use the
+ * molecules' centres of mass as the reference does (r_ij . R_ij and the
+ * reciprocal centre-of-mass sums).  Evaluated in FP64 whatever the precision
+ * mode; the induced dipoles are solved at the solver's settings first.
+ * out[SMD_LUSTIG_COUNT] in the struct's order (SMD_LUS_*); fields no term
+ * writes (inducEn, inducDeriv, intravirPolCorrect, the second derivatives
+ * the reference leaves at zero) come back 0, and so does virialcorrect,
+ * which LFIntegrator forms after the position update from one step's forces
+ * and the next step's positions (LFIntegrator.cpp:819-836).  Refused (SMD_ERR_ARG) with
+ * Wolf, Mie, BMH or SAAP pair terms and in a sheared cell. */
+enum {
+    SMD_LUS_LJ_U = 0, SMD_LUS_LJ_DU, SMD_LUS_LJ_D2U, SMD_LUS_VIRCORRECT, SMD_LUS_INTRAVIR,
+    SMD_LUS_LONG, SMD_LUS_REAL, SMD_LUS_REAL2, SMD_LUS_LONG2, SMD_LUS_SURF, SMD_LUS_SURF2,
+    SMD_LUS_INDUC_EN, SMD_LUS_INDUC, SMD_LUS_MOL, SMD_LUS_MOL2, SMD_LUS_BOND, SMD_LUS_BOND2,
+    SMD_LUS_POL_INTRAVIR, SMD_LUS_POL_LONG, SMD_LUS_POL_REAL, SMD_LUS_POL_REAL2, SMD_LUS_POL_LONG2,
+    SMD_LUS_POL_SURF, SMD_LUS_POL_SURF2, SMD_LUS_POL_MOL, SMD_LUS_POL_MOL2, SMD_LUS_POL_SELF,
+    SMD_LUS_UB, SMD_LUS_UB2, SMD_LUSTIG_COUNT
+};
+int smd_lustig(smd_ctx *ctx, double *out);
 int smd_set_saap(smd_ctx *ctx, const double *table, int switch_on, double switch_dist2);
 int smd_set_wolf(smd_ctx *ctx, double alpha, double cutoff, const int *msite, double d_op);
 int smd_set_barostat(smd_ctx *ctx, double pressure, double baros_const, int on);

@@ -331,7 +331,7 @@ static int mode_run(int nsteps, const char *out) {
         rec("start_vtminus", vm);
     }
     std::vector<double> epot, ekin, atemp, zeta, press, nupd;
-    std::vector<double> ptensor, mtensor, lus;
+    std::vector<double> ptensor, mtensor, lus, lus_all, molvirt, molpt;
     double run_seconds = 0.0;
     for (int k = 0; k < nsteps; k++) {
         timespec t0, t1;
@@ -344,8 +344,16 @@ static int mode_run(int nsteps, const char *out) {
             // at the positions the previous step left, with its centres)
             const Lustig &L = e->myLustig;
             for (double v : {L.ljUlus, L.ljdUlus, L.ljd2Ulus}) lus.push_back(v);
+            // every field of Ensemble::myLustig in declaration order (each
+            // force term writes its own fields during the step)
+            const double *all = reinterpret_cast<const double *>(&L);
+            static_assert(sizeof(Lustig) == 29 * sizeof(double), "Lustig layout");
+            lus_all.insert(lus_all.end(), all, all + 29);
             if (k == 0) dump_state(e, "step_after1");
         }
+        // the step's Lustig virial and pressure (LFIntegrator.cpp:731-741)
+        molvirt.push_back(lf->molVirt);
+        molpt.push_back(lf->molPt);
         const Energy &E = e->myEnergy;
         epot.push_back(E.totEnergy);
         ekin.push_back(E.atomKinEnergy);
@@ -356,6 +364,9 @@ static int mode_run(int nsteps, const char *out) {
         for (int q = 0; q < 9; q++) mtensor.push_back(e->molPressure[q]);
     }
     if (!lus.empty()) rec("step_lustig", lus);
+    if (!lus_all.empty()) rec("step_lustig_all", lus_all);
+    rec("step_molvirt", molvirt);
+    rec("step_molpt", molpt);
     rec("step_epot", epot);
     rec("step_ekin", ekin);
     rec("step_atomtemp", atemp);

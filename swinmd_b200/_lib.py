@@ -22,6 +22,12 @@ PREC_FP64, PREC_MIXED = 0, 1
 TERM_VDW, TERM_EWALD_REAL, TERM_EWALD_LONG, TERM_ALL = 1, 2, 4, 0xFFFF
 TERM_MP_SHORT, TERM_MP_LONG, TERM_IND_SHORT, TERM_IND_LONG = 8, 16, 32, 64
 TERM_BOND, TERM_ANGLE, TERM_UB, TERM_WOLF = 128, 256, 512, 1024
+# fields of Ensemble::myLustig in declaration order (SMD_LUS_*)
+LUSTIG_FIELDS = ("ljUlus", "ljdUlus", "ljd2Ulus", "virialcorrect", "intravirCorrect", "longDeriv",
+                 "realDeriv", "realSecDeriv", "longSecDeriv", "surfDeriv", "surfSecDeriv", "inducEn",
+                 "inducDeriv", "molDeriv", "molSecDeriv", "BondDeriv", "BondSecDeriv", "intravirPolCorrect",
+                 "longPolDeriv", "realPolDeriv", "realSecPolDeriv", "longSecPolDeriv", "surfPolDeriv",
+                 "surfSecPolDeriv", "molPolDeriv", "molSecPolDeriv", "selfPolDeriv", "ubDeriv", "ubSecDeriv")
 E_VDW, E_REAL, E_LONG, E_CORRECT, E_MOLCORRECT, E_SURF = 0, 1, 2, 3, 4, 5
 E_POL_REAL, E_POL_LONG, E_POL_SELF, E_POL_INTRA = 6, 7, 8, 9
 E_POL_SURF, E_BOND, E_ANGLE, E_UB, E_TERMS, E_COUNT = 10, 11, 12, 13, 14, 16
@@ -105,6 +111,7 @@ SIGNATURES = {
     "smd_ewald_nk": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
     "smd_set_integrator": (ctypes.c_int, [_P, ctypes.POINTER(IntegratorParams)]),
     "smd_lustig_lj": (ctypes.c_int, [_P, _D]),
+    "smd_lustig": (ctypes.c_int, [_P, _D]),
     "smd_set_saap": (ctypes.c_int, [_P, _D, ctypes.c_int, ctypes.c_double]),
     "smd_set_wolf": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, _I, ctypes.c_double]),
     "smd_set_barostat": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, ctypes.c_int]),

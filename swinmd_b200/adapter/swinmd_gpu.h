@@ -327,6 +327,34 @@ public:
         check(ctx, smd_compute_forces(ctx, terms, frc.data(), energy, virial), "smd_compute_forces");
     }
 
+    // Ensemble::myLustig as the replaced classes leave it after a step's
+    // force calls (smd_lustig, FP64): the electrostatic fields every step
+    // (EwaldForce, Multipole and Induction write theirs unconditionally), the
+    // buffered 14-7's U and dU/dV every step and its d2U/dV2 with
+    // computeLustig (BuffvdWForce.cpp:326-336), the LJ fields with
+    // computeLustig only (LJForce.cpp:136-250).  The bonded fields belong to
+    // the host's own BondForce / UreyBradleyForce and virialcorrect to the
+    // integrator; they are left alone.  `lustig = false` skips the
+    // evaluation (the fields then keep their last values).
+    bool lustig = true;
+    void fill_lustig(bool compute_lustig, bool buff) {
+        static_assert(sizeof(Lustig) == SMD_LUSTIG_COUNT * sizeof(double), "Lustig layout");
+        double v[SMD_LUSTIG_COUNT];
+        sync_positions();
+        check(ctx, smd_lustig(ctx, v), "smd_lustig");
+        double *L = reinterpret_cast<double *>(&ens->myLustig);
+        for (int q = 0; q < SMD_LUSTIG_COUNT; q++) {
+            if (q == SMD_LUS_VIRCORRECT || q == SMD_LUS_BOND || q == SMD_LUS_BOND2 || q == SMD_LUS_UB ||
+                q == SMD_LUS_UB2)
+                continue;
+            if (q == SMD_LUS_LJ_U || q == SMD_LUS_LJ_DU || q == SMD_LUS_LJ_D2U) {
+                const bool always = buff && q != SMD_LUS_LJ_D2U;
+                if (!always && !compute_lustig) continue;
+            }
+            L[q] = v[q];
+        }
+    }
+
     // adds the forces of the last evaluation into Atom::force
     void add_forces() {
         for (int i = 0; i < ens->nAtoms; i++) {
@@ -387,12 +415,16 @@ public:
             this->virial[k] = -w[k];
             this->myEnsemble->virial[k] += w[k];
         }
-        if (!long_terms) return;
-        path->evaluate(long_terms, en, w);
-        path->add_forces();
-        E.longEnergy = en[SMD_E_LONG];
-        if (long_terms & SMD_TERM_IND_LONG) E.longPolEnergy = en[SMD_E_POL_LONG];
-        for (int k = 0; k < 8; k++) this->myEnsemble->longVirial[k] = w[k];
+        if (long_terms) {
+            path->evaluate(long_terms, en, w);
+            path->add_forces();
+            E.longEnergy = en[SMD_E_LONG];
+            if (long_terms & SMD_TERM_IND_LONG) E.longPolEnergy = en[SMD_E_POL_LONG];
+            for (int k = 0; k < 8; k++) this->myEnsemble->longVirial[k] = w[k];
+        }
+        if (path->lustig)
+            path->fill_lustig(this->myEnsemble->myConfig->compute_lustig(),
+                              this->myEnsemble->myConfig->compute_buffamoeba());
     }
 };
 
@@ -422,6 +454,8 @@ public:
         computeInduction = false;
     }
     double zeta() const { return fnh; }
+    // the step's Lustig pressure (LFIntegrator.cpp:731-741)
+    double lustig_pressure() const { return molPt; }
     int list_updates() const { return numUpdates; }
 };
 

@@ -344,7 +344,7 @@ void smd_destroy(smd_ctx *x) {
                     c.rc.kseg, c.rc.kcol, c.rc.kgrp, c.rc.kzr, c.rc.kcxy, c.rc.stab, c.srec, c.phist, c.cg_blk,
                     c.upload4, c.fout, c.rc.kzr_d, c.rc.kcxy_d, c.rc.stab_d, c.rc.srec_d, c.bonds, c.angles,
                     c.bond_par, c.angle_par, c.surf_part, c.surf_tot, c.rdf_hist, c.avg, c.wrap,
-                    c.wolf_msite, c.wpos4, c.dbox, c.saap, c.rc.nk_dev};
+                    c.wolf_msite, c.wpos4, c.dbox, c.saap, c.rc.nk_dev, c.lus_com, c.lus_buf};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -500,6 +500,20 @@ int smd_lustig_lj(smd_ctx *x, double *out) {
     CK(cudaSetDevice(c.device));
     int r = lustig_lj(c, out);
     if (r) return fail(x, r, "smd_lustig_lj: evaluation failed");
+    return sync_status(x);
+}
+
+int smd_lustig(smd_ctx *x, double *out) {
+    if (!x || !out || x->c.n == 0 || x->c.box.L[0] <= 0) return fail(x, SMD_ERR_ARG, "smd_lustig: system not set up");
+    Ctx &c = x->c;
+    if (c.wolf_on || c.rc.le || (c.vdw != VDW_NONE && c.vdw != VDW_LJ && c.vdw != VDW_BUFF))
+        return fail(x, SMD_ERR_ARG,
+                    "smd_lustig: built for the LJ and buffered 14-7 terms, Ewald sums, multipoles, induced "
+                    "dipoles and bonded terms (no Wolf, Mie, BMH, SAAP or sheared cell)");
+    CK(cudaSetDevice(c.device));
+    CK(cudaMemsetAsync(c.status, 0, sizeof(unsigned), c.stream));
+    int r = lustig_all(c, out);
+    if (r) return fail(x, r, "smd_lustig: evaluation failed");
     return sync_status(x);
 }
 

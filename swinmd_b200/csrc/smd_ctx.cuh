@@ -222,6 +222,10 @@ struct Ctx {
     // dipoles only when they were not solved for the current version
     long long cfg_version = 1;
     long long dip_version = 0;
+    // scratch of the on-demand volume derivatives (smd_lustig.cu)
+    double4 *lus_com = nullptr;     // [nmol] molecular centres of mass
+    double *lus_buf = nullptr;      // per-block / per-k partial sums
+    size_t lus_cap = 0;
     // CUDA graph of one step
     cudaGraphExec_t step_graph = nullptr;
     int graph_dirty = 1;
@@ -320,6 +324,11 @@ void launch_mlp_guess(Ctx &c);
 void launch_first_order_guess(Ctx &c);
 void launch_blk_response(Ctx &c, double *out, int order, double *out_prev);
 int lustig_lj(Ctx &c, double *out);
+int lustig_all(Ctx &c, double *out);
+void launch_mp_real_only(Ctx &c);
+void launch_ind_real_only(Ctx &c);
+void launch_ind_self_only(Ctx &c);
+void launch_intra_flex_lus(Ctx &c, bool mp, bool ind, double *fr_mol);
 // order of the extrapolated guess of the solver's guess mode (0: none)
 inline int guess_order(const Ctx &c) {
     return c.cg_guess == SMD_GUESS_FIRST_ORDER ? 1

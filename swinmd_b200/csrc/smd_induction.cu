@@ -1389,10 +1389,13 @@ __global__ void __launch_bounds__(96) k_polar_mol(IndArgs a, long long *trq, lon
 // are formed by k_mp_mol / k_ind_mol / k_polar_mol with or without
 // constraints; this kernel adds the forces and torques, one thread per
 // molecule, FP64.  No virial: the reference adds none for these terms.
-__global__ void k_intra_flex(IndArgs a, long long *frc, long long *trq, int mp, int ind) {
+// fr_mol (may be null): per molecule, sum f_ij . r_ij over its pairs (the
+// volume derivative's share, Multipole.cpp:1514, Induction.cpp:2013)
+__global__ void k_intra_flex(IndArgs a, long long *frc, long long *trq, int mp, int ind, double *fr_mol) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= a.nmol) return;
     const int s0 = a.mol_off[m], ns = a.mol_off[m + 1] - s0;
+    double fr = 0;
     for (int p = 0; p < ns; p++)
         for (int q = p + 1; q < ns; q++) {
             const int i = a.mol_atoms[s0 + p], j = a.mol_atoms[s0 + q];
@@ -1453,7 +1456,9 @@ __global__ void k_intra_flex(IndArgs a, long long *frc, long long *trq, int mp, 
             add_fix3_at(frc, a.n, j, -fij, COU);
             add_fix3_at(trq, a.n, i, ti, COU);
             add_fix3_at(trq, a.n, j, tj, COU);
+            fr += dot(fij, r);
         }
+    if (fr_mol) fr_mol[m] = fr;
 }
 
 
@@ -1498,7 +1503,28 @@ void launch_intra_flex(Ctx &c, bool mp, bool ind) {
     // corrections as energies only
     if (c.clen2 || !(mp || ind)) return;
     k_intra_flex<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(ind_args(c), c.frc, c.trq, mp ? 1 : 0,
-                                                            ind && c.ind_on ? 1 : 0);
+                                                            ind && c.ind_on ? 1 : 0, nullptr);
+}
+
+// the same pass with each molecule's sum f_ij . r_ij in fr_mol[nmol]
+// (flexible molecules; the volume derivatives' intramolecular share)
+void launch_intra_flex_lus(Ctx &c, bool mp, bool ind, double *fr_mol) {
+    if (c.clen2 || !(mp || ind)) return;
+    k_intra_flex<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(ind_args(c), c.frc, c.trq, mp ? 1 : 0,
+                                                            ind && c.ind_on ? 1 : 0, fr_mol);
+}
+
+// FP64 induced real space alone, and the induced self term alone (the
+// volume derivatives take each one's virial and torques on their own)
+void launch_ind_real_only(Ctx &c) {
+    IndRealArgs A;
+    A.ia = ind_args(c);
+    A.frc = c.frc; A.trq = c.trq; A.acc = c.acc;
+    k_ind_real<<<(int)(((long long)c.n * 8 + 63) / 64), 64, 0, c.stream>>>(A);
+}
+
+void launch_ind_self_only(Ctx &c) {
+    k_ind_mol<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(ind_args(c), c.trq, c.acc);
 }
 
 int setup_cg(Ctx &c) {

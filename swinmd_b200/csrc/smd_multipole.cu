@@ -423,6 +423,16 @@ void launch_mp_short(Ctx &c) {
     launch_intra_flex(c, true, false);   // flexible molecules: the correction's forces and torques
 }
 
+// the FP64 real-space pair pass alone (the volume derivative of
+// Multipole::real_term takes its virial and torques on their own)
+void launch_mp_real_only(Ctx &c) {
+    MPArgs a;
+    a.n = c.n; a.nbr = c.pl.nbr; a.nnbr = c.pl.nnbr; a.pos4 = c.pos4; a.mu = c.mu; a.qd = c.qd;
+    a.tq = c.type_q; a.box = c.box; a.alpha = c.ew_alpha; a.rc2 = c.mp_rc2;
+    a.frc = c.frc; a.trq = c.trq; a.acc = c.acc;
+    k_mp_real<8><<<(int)(((long long)c.n * 8 + 127) / 128), 128, 0, c.stream>>>(a);
+}
+
 // self energy and intramolecular correction of the multipoles
 void launch_mp_mol(Ctx &c) {
     k_mp_mol<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.n, c.mol_off, c.mol_atoms, c.excl_off,

@@ -216,6 +216,20 @@ def buff_long_range_correction(s: System, box: float) -> tuple:
 WOLF_R_OP_NM = 0.505783 / (1.0e-9 / 5.29189379e-11)
 
 
+def lustig_molvirt(fields: dict, volume: float, tb_energy: float = 0.0) -> float:
+    """The Lustig virial of LFIntegrator::run (molVirt,
+    src/integrators/LFIntegrator.cpp:731-734) from the fields of
+    GpuEnsemble.lustig(); the pressure it reports is then
+    2 K / 3V - molVirt with K the molecular kinetic energy under
+    constraints and the atomic one otherwise (:736-741)."""
+    f = fields
+    V = volume
+    return (f["ljdUlus"] + f["inducDeriv"] - 3.0 * tb_energy / V + f["surfDeriv"] + f["molDeriv"]
+            + f["surfPolDeriv"] + f["molPolDeriv"]
+            + (f["longDeriv"] + f["realDeriv"] + f["ubDeriv"] + f["BondDeriv"] + f["longPolDeriv"]
+               + f["realPolDeriv"] + f["selfPolDeriv"]) / (3.0 * V))
+
+
 def refuse_unsupported(c) -> None:
     """Raises for configuration options the GPU path does not compute, so a
     caller never gets different physics with a success status: the AMOEBA
@@ -356,6 +370,13 @@ class GpuEnsemble:
         out = np.zeros(3)
         self._chk(self.lib.smd_lustig_lj(self.ctx, L.dptr(out)))
         return out
+
+    def lustig(self) -> dict:
+        """Every field of Ensemble::myLustig at the current configuration
+        (FP64), keyed by the reference's field names."""
+        out = np.zeros(len(L.LUSTIG_FIELDS))
+        self._chk(self.lib.smd_lustig(self.ctx, L.dptr(out)))
+        return dict(zip(L.LUSTIG_FIELDS, out.tolist()))
 
     def set_saap(self, table: np.ndarray, switch_on: bool = False, switch_dist: float = 0.0):
         """The SAAP pair potential as the vdW term (SAAPForce): table rows

@@ -53,7 +53,7 @@ int main(int argc, char **argv) {
     swinmd_gpu::GpuPath path(ens, precision);
     swinmd_gpu::GpuForceLFIntegrator *lf = new swinmd_gpu::GpuForceLFIntegrator(ens, cfg, &path);
     g_out = fopen(argv[2], "w");
-    std::vector<double> epot, ekin, atemp, zeta, nupd, ptensor;
+    std::vector<double> epot, ekin, atemp, zeta, nupd, ptensor, molpt;
     for (int k = 0; k < nsteps; k++) {
         lf->run(1);
         const Energy &E = ens->myEnergy;
@@ -63,6 +63,7 @@ int main(int argc, char **argv) {
         zeta.push_back(lf->zeta());
         nupd.push_back(lf->list_updates());
         for (int q = 0; q < 9; q++) ptensor.push_back(ens->atomPressure[q]);
+        molpt.push_back(lf->lustig_pressure());
     }
     rec("step_epot", epot);
     rec("step_ekin", ekin);
@@ -70,6 +71,7 @@ int main(int argc, char **argv) {
     rec("step_zeta", zeta);
     rec("step_nupdates", nupd);
     rec("step_atompressure", ptensor);
+    rec("step_molpt", molpt);
     const int n = ens->nAtoms;
     std::vector<double> p(3 * n), v(3 * n);
     for (int i = 0; i < n; i++) {

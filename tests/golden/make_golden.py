@@ -98,6 +98,49 @@ def spce512_lustig():
     return s, [("forces",), ("run", 2)]
 
 
+# Every field of Ensemble::myLustig (Ensemble.h:77-108) as the reference's
+# force terms write it during a step: two steps of LFIntegrator, the second
+# step's values belonging to the positions (and molecular centres) the first
+# step left.  One case per branch of the terms' derivative code: atoms
+# (no constraints), flexible molecules (intramolecular forces, bonds),
+# rigid molecules (r_ij . R_ij, the reciprocal centre-of-mass terms), the
+# polarisable model and the reference's own flexible polarisable case.
+def nacl1000_lustig():
+    # point charges + LJ on ions, surface term on (EwaldForce, LJForce)
+    s = systems.nacl_melt(ncell=10, potential="lj", kmax=6, seed=5, n_steps=2)
+    s.config.lustig = True
+    s.config.surface_correct = True
+    return s, [("forces",), ("run", 2)]
+
+
+def spcf216_lustig():
+    # flexible SPC/E-like water: harmonic bonds and angle, Ewald with the
+    # intramolecular correction's forces
+    s = systems.spce_flexible(nmol=216, seed=4, n_steps=2)
+    s.config.lustig = True
+    s.config.surface_correct = True
+    s.config.thermostat = "NoseHoover"
+    return s, [("forces",), ("run", 2)]
+
+
+def polwater216_lustig():
+    # rigid polarisable multipole water with the surface terms
+    s = systems.polarizable_water(nmol=216, cutoff=0.9, switch=0.8, alpha=3.5, kmax=7, seed=3,
+                                  n_steps=2)
+    s.config.lustig = True
+    s.config.surface_correct = True
+    return s, [("forces",), ("run", 2)]
+
+
+def ref_test_lustig():
+    # the reference's shipped flexible polarisable case (bonds, angles,
+    # Urey-Bradley, buffered 14-7, multipoles, induction, surface terms)
+    s, _ = ref_test_nvt()
+    s.config.n_steps = 2
+    s.config.lustig = True
+    return s, [("forces",), ("run", 2)]
+
+
 def saap500():
     # SAAPForce with the reference's own three-type table
     s = systems.three_type_fluid(ncell=5, seed=3)
@@ -163,7 +206,9 @@ def ref_test_nvt():
 
 CASES = {"lj500": lj500, "lj500_npt": lj500_npt, "nacl1000_mie": nacl1000_mie, "spce512": spce512,
          "polwater216": polwater216, "spce512_wolf": spce512_wolf, "saap500": saap500,
-         "lj500_lustig": lj500_lustig, "spce512_lustig": spce512_lustig, "nacl1000_wolf": nacl1000_wolf, "polwater216_nve": polwater216_nve, "ref_test_nvt": ref_test_nvt}
+         "lj500_lustig": lj500_lustig, "spce512_lustig": spce512_lustig, "nacl1000_wolf": nacl1000_wolf, "polwater216_nve": polwater216_nve, "ref_test_nvt": ref_test_nvt,
+         "nacl1000_lustig": nacl1000_lustig, "spcf216_lustig": spcf216_lustig,
+         "polwater216_lustig": polwater216_lustig, "ref_test_lustig": ref_test_lustig}
 LARGE = {"lj4000": lj4000, "lj4000_jitter": lj4000_jitter, "nacl8000_mie": nacl8000_mie, "spce2160": spce2160,
          "polwater4096": polwater4096}
 
@@ -227,7 +272,9 @@ def pack(name, s, results, large=False):
                 out[key] = np.array(open(os.path.join(d, fn)).read())
     if name.endswith("_lustig"):
         out = {k: v for k, v in out.items() if not k.startswith(("f_", "r_")) or
-               k in ("f_lustig_lj", "f_lj_energy", "r_step_lustig", "r_step_after1_pos")}
+               k in ("f_lustig_lj", "f_lj_energy", "r_step_lustig", "r_step_lustig_all",
+                     "r_step_molvirt", "r_step_molpt", "r_step_after1_pos", "r_step_epot",
+                     "r_start_vtminus")}
         out.pop("pairs", None)
     if name.startswith("saap"):
         out = {k: v for k, v in out.items() if not k.startswith("f_")}

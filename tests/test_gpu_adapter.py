@@ -42,6 +42,11 @@ def test_reference_integrator_with_gpu_forces(tmp_path):
     # all nine components: the adapter copies the reciprocal virial as
     # EwaldForce::compute_long does (components 0..7)
     assert np.allclose(out["step_atompressure"], g["r_step_atompressure"], rtol=1e-7, atol=1e-6)
+    # the Lustig pressure LFIntegrator reports (LFIntegrator.cpp:731-741)
+    # from the myLustig fields the GPU object filled; from the second step,
+    # as the reference's first step reads molecular centres no step has set
+    print(out["step_molpt"] - g["r_step_molpt"])
+    assert np.allclose(out["step_molpt"][1:], g["r_step_molpt"][1:], rtol=1e-7, atol=1e-6)
     assert np.allclose(out["final_pos"], g["r_final_pos"], rtol=0, atol=1e-8)
     assert np.allclose(out["final_vel"], g["r_final_vel"], rtol=0, atol=1e-6)
 
@@ -65,4 +70,6 @@ def test_reference_integrator_with_gpu_polarisable_water(tmp_path):
     print(np.max(np.abs(out["step_epot"] / g["r_step_epot"] - 1)))
     assert np.allclose(out["step_epot"], g["r_step_epot"], rtol=1e-7)
     assert np.allclose(out["step_atomtemp"], g["r_step_atomtemp"], rtol=1e-7)
+    print(out["step_molpt"] - g["r_step_molpt"])
+    assert np.allclose(out["step_molpt"][1:], g["r_step_molpt"][1:], rtol=1e-6, atol=1e-5)
     assert np.allclose(out["final_pos"], g["r_final_pos"], rtol=0, atol=1e-9)
