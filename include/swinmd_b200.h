@@ -437,8 +437,9 @@ int smd_lustig_lj(smd_ctx *ctx, double *out);
  * writes (inducEn, inducDeriv, intravirPolCorrect, the second derivatives
  * the reference leaves at zero) come back 0, and so does virialcorrect,
  * which LFIntegrator forms after the position update from one step's forces
- * and the next step's positions (LFIntegrator.cpp:819-836).  Refused (SMD_ERR_ARG) with
- * Wolf, Mie, BMH or SAAP pair terms and in a sheared cell. */
+ * and the next step's positions (LFIntegrator.cpp:819-836).  The Wolf sum's
+ * realDeriv/realSecDeriv follow WolfForce.cpp:200-244.  Refused
+ * (SMD_ERR_ARG) with Mie, BMH or SAAP pair terms and in a sheared cell. */
 enum {
     SMD_LUS_LJ_U = 0, SMD_LUS_LJ_DU, SMD_LUS_LJ_D2U, SMD_LUS_VIRCORRECT, SMD_LUS_INTRAVIR,
     SMD_LUS_LONG, SMD_LUS_REAL, SMD_LUS_REAL2, SMD_LUS_LONG2, SMD_LUS_SURF, SMD_LUS_SURF2,

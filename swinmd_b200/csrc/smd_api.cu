@@ -506,10 +506,10 @@ int smd_lustig_lj(smd_ctx *x, double *out) {
 int smd_lustig(smd_ctx *x, double *out) {
     if (!x || !out || x->c.n == 0 || x->c.box.L[0] <= 0) return fail(x, SMD_ERR_ARG, "smd_lustig: system not set up");
     Ctx &c = x->c;
-    if (c.wolf_on || c.rc.le || (c.vdw != VDW_NONE && c.vdw != VDW_LJ && c.vdw != VDW_BUFF))
+    if (c.rc.le || (c.vdw != VDW_NONE && c.vdw != VDW_LJ && c.vdw != VDW_BUFF))
         return fail(x, SMD_ERR_ARG,
-                    "smd_lustig: built for the LJ and buffered 14-7 terms, Ewald sums, multipoles, induced "
-                    "dipoles and bonded terms (no Wolf, Mie, BMH, SAAP or sheared cell)");
+                    "smd_lustig: built for the LJ and buffered 14-7 terms, Ewald and Wolf sums, multipoles, "
+                    "induced dipoles and bonded terms (no Mie, BMH, SAAP or sheared cell)");
     CK(cudaSetDevice(c.device));
     CK(cudaMemsetAsync(c.status, 0, sizeof(unsigned), c.stream));
     int r = lustig_all(c, out);

@@ -325,6 +325,7 @@ void launch_first_order_guess(Ctx &c);
 void launch_blk_response(Ctx &c, double *out, int order, double *out_prev);
 int lustig_lj(Ctx &c, double *out);
 int lustig_all(Ctx &c, double *out);
+void launch_wolf_sites(Ctx &c);
 void launch_mp_real_only(Ctx &c);
 void launch_ind_real_only(Ctx &c);
 void launch_ind_self_only(Ctx &c);

@@ -133,6 +133,7 @@ int lustig_lj(Ctx &c, double *out) {
 //       (:1133, :1386-1389), molPolDeriv (:2013), surfPolDeriv/
 //       surfSecPolDeriv (:2270-2290), longPolDeriv/longSecPolDeriv
 //       (:1597-1613, :1686-1690, :1742-1745)
+//   Wolf sum (WolfForce)             realDeriv/realSecDeriv (:200-244)
 //   buffered 14-7 (BuffvdWForce)     ljUlus, ljdUlus (:244, :326-330)
 //   bonds, Urey-Bradley              BondDeriv/BondSecDeriv (BondForce.cpp:86-87),
 //                                    ubDeriv/ubSecDeriv (UreyBradleyForce.cpp:76-77)
@@ -228,6 +229,52 @@ __global__ void __launch_bounds__(LU_THREADS) k_lus_ewald_real(int n, const int 
             const double f = (erfc(alpha * r) / r + a2pi * ex) / r2;
             v[0] += -qij * f * rr;
             v[1] += qij * (2.0 * f + 2.0 * a2pi * a2 * ex) * rr * rr / r2 + 2.0 * qij * f * rr;
+        }
+    }
+    lu_block_out<2>(v, out);
+}
+
+// WolfForce::real_term's derivatives (WolfForce.cpp:200-244) over the full
+// list of charge-site positions (the displaced O sites of "WAT" molecules
+// where the sum puts them): with the sum shifted at the cutoff Rc,
+//   f   = (erfc(a r)/r + a2pi e^{-a^2 r^2}) / r^2 - R / Rc,
+//         R = erfc(a Rc)/Rc^2 + a2pi e^{-a^2 Rc^2} / Rc
+//   dv2 = (2 dv + 2 a2pi a^2 e^{-a^2 r^2}) / r^2 - (2 R / Rc + 2 a2pi a^2 e^{-a^2 Rc^2}) / Rc^2
+//   realDeriv    += -q_ij f (r_ij . R_ij)
+//   realSecDeriv += q_ij dv2 (r_ij . R_ij)^2 + 2 q_ij f (r_ij . R_ij)
+// with R_ij the molecules' centres' difference in every case.
+__global__ void __launch_bounds__(LU_THREADS) k_lus_wolf(int n, const int *nbr, const int *nnbr,
+                                                         const double4 *qpos4, const int *mol,
+                                                         const double4 *com, const double *tq, Box box,
+                                                         double rc, double alpha, double *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[2] = {0, 0};
+    if (i < n) {
+        const double4 pi = qpos4[i];
+        const double qi = tq[(int)pi.w];
+        const double4 ci = com[mol[i]];
+        const double a2 = alpha * alpha, a2pi = 2.0 * alpha / LU_SQRTPI, rc2 = rc * rc;
+        const double eR = erfc(alpha * rc) / rc;
+        const double Rc = eR / rc + a2pi * exp(-a2 * rc2) / rc;
+        const double d2c = (2.0 * Rc / rc + 2.0 * a2pi * a2 * exp(-a2 * rc2)) / rc2;
+        for (int k = 0; k < nnbr[i]; k++) {
+            const int j = nbr[(size_t)k * n + i] & 0x7fffffff;
+            const double4 pj = qpos4[j];
+            double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+            lu_min(dx, dy, dz, box);
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            if (!(r2 < rc2)) continue;
+            const double4 cj = com[mol[j]];
+            double mx = cj.x - ci.x, my = cj.y - ci.y, mz = cj.z - ci.z;
+            lu_min(mx, my, mz, box);
+            const double rr = dx * mx + dy * my + dz * mz;
+            const double qij = qi * tq[(int)pj.w];
+            const double r = sqrt(r2), ex = exp(-a2 * r2);
+            const double dv = (erfc(alpha * r) / r + a2pi * ex) / r2;
+            const double f = dv - Rc / rc;
+            const double dv2 = (2.0 * dv + 2.0 * a2pi * a2 * ex) / r2 - d2c;
+            v[0] += -qij * f * rr;
+            v[1] += qij * dv2 * rr * rr + 2.0 * qij * f * rr;
         }
     }
     lu_block_out<2>(v, out);
@@ -601,7 +648,7 @@ int lus_recip(Ctx &c, int constrained, double *d1, double *d2) {
 // out[SMD_LUSTIG_COUNT]: the fields of Ensemble::myLustig in declaration order
 int lustig_all(Ctx &c, double *out) {
     for (int q = 0; q < SMD_LUSTIG_COUNT; q++) out[q] = 0;
-    if (c.wolf_on || (c.vdw != VDW_NONE && c.vdw != VDW_LJ && c.vdw != VDW_BUFF) || c.rc.le) return SMD_ERR_ARG;
+    if ((c.vdw != VDW_NONE && c.vdw != VDW_LJ && c.vdw != VDW_BUFF) || c.rc.le) return SMD_ERR_ARG;
     // partials: 2 per k, LU_NSUM per site block, 4 per bond block, one per
     // molecule (the intramolecular pass)
     const size_t need = std::max<size_t>({(size_t)2 * std::max(c.rc.nk, 1),
@@ -686,6 +733,20 @@ int lustig_all(Ctx &c, double *out) {
             out[SMD_LUS_SURF2] = surf2(qr, qR);
         }
         if ((r = lus_recip<0>(c, constrained, &out[SMD_LUS_LONG], &out[SMD_LUS_LONG2]))) return done(r);
+    }
+    // ---- the Wolf sum of the charges
+    if (c.wolf_on) {
+        const double4 *qp = c.pos4;
+        if (c.wolf_msites) {
+            launch_wolf_sites(c);
+            qp = c.wpos4;
+        }
+        k_lus_wolf<<<nbs, LU_THREADS, 0, c.stream>>>(c.n, c.pl.nbr, c.pl.nnbr, qp, c.mol, c.lus_com, c.type_q, c.box,
+                                                      c.wolf_rc, c.wolf_alpha, c.lus_buf);
+        double t[2];
+        if ((r = lus_fetch(c, nbs, 2, t))) return done(r);
+        out[SMD_LUS_REAL] = 0.5 * t[0];
+        out[SMD_LUS_REAL2] = 0.5 * t[1];
     }
     // ---- multipoles and induced dipoles (each part's torques on their own)
     if (c.mp_on) {

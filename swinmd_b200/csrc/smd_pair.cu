@@ -703,6 +703,13 @@ __global__ void k_wolf_sites(int n, const int *mol, const int *mol_off, const in
     vpos4[i] = p;
 }
 
+// the charge-site positions of the Wolf sum into c.wpos4 (every site; the
+// displaced ones moved as above)
+void launch_wolf_sites(Ctx &c) {
+    k_wolf_sites<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.mol, c.mol_off, c.mol_atoms, c.wolf_msite,
+                                                           c.pos4, c.wolf_d, c.wpos4);
+}
+
 // Virtual sites of the buffered 14-7 term (BuffvdWForce::VirtualPositions,
 // src/forces/BuffvdWForce.cpp:358-385): a type-0 (H) site moves to
 // f r_H + (1 - f) r_O, with O the molecule's second site; others stay.

@@ -132,6 +132,15 @@ def polwater216_lustig():
     return s, [("forces",), ("run", 2)]
 
 
+def spce512_wolf_lustig():
+    # the Wolf sum with displaced O charge sites (WolfForce, realDeriv with
+    # the molecules' centres)
+    s = systems.spce_water(nmol=512, box=2.4953, cutoff=0.9, kmax=6, seed=11, n_steps=2)
+    s.config.compute_ewald, s.config.compute_wolf, s.config.alpha = False, True, 2.0
+    s.config.lustig = True
+    return s, [("forces",), ("run", 2)]
+
+
 def ref_test_lustig():
     # the reference's shipped flexible polarisable case (bonds, angles,
     # Urey-Bradley, buffered 14-7, multipoles, induction, surface terms)
@@ -208,7 +217,8 @@ CASES = {"lj500": lj500, "lj500_npt": lj500_npt, "nacl1000_mie": nacl1000_mie, "
          "polwater216": polwater216, "spce512_wolf": spce512_wolf, "saap500": saap500,
          "lj500_lustig": lj500_lustig, "spce512_lustig": spce512_lustig, "nacl1000_wolf": nacl1000_wolf, "polwater216_nve": polwater216_nve, "ref_test_nvt": ref_test_nvt,
          "nacl1000_lustig": nacl1000_lustig, "spcf216_lustig": spcf216_lustig,
-         "polwater216_lustig": polwater216_lustig, "ref_test_lustig": ref_test_lustig}
+         "polwater216_lustig": polwater216_lustig, "ref_test_lustig": ref_test_lustig,
+         "spce512_wolf_lustig": spce512_wolf_lustig}
 LARGE = {"lj4000": lj4000, "lj4000_jitter": lj4000_jitter, "nacl8000_mie": nacl8000_mie, "spce2160": spce2160,
          "polwater4096": polwater4096}
 
@@ -279,7 +289,7 @@ def pack(name, s, results, large=False):
     if name.startswith("saap"):
         out = {k: v for k, v in out.items() if not k.startswith("f_")}
         out.pop("pairs", None)
-    if name.endswith("_wolf"):
+    if name.endswith("_wolf"):  # (the Wolf Lustig case ends in _lustig)
         out = {k: v for k, v in out.items() if not k.startswith("f_") or k.startswith("f_wolf_")}
         out.pop("pairs", None)
     if name.endswith(("_nve", "_npt")):

@@ -127,3 +127,13 @@ def test_lustig_all_reference_case(tmp_path):
     ens.set_solver(tol=1e-13, max_iter=1000)
     _compare(ens, golden("ref_test_lustig"), rtol=1e-7)
     ens.close()
+
+
+def test_lustig_all_wolf():
+    # the Wolf sum with the O charges on WolfForce's displaced sites
+    s = systems.spce_water(nmol=512, box=2.4953, cutoff=0.9, kmax=6, seed=11, n_steps=2)
+    s.config.compute_ewald, s.config.compute_wolf, s.config.alpha = False, True, 2.0
+    s.config.lustig = True
+    ens = engine.GpuEnsemble(s)
+    _compare(ens, golden("spce512_wolf_lustig"))
+    ens.close()
