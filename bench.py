@@ -725,7 +725,8 @@ def main():
         nbytes = products * entries * (4 + 16 + 16)
         t = stage_ms["pcg"] * 1e-3
         rooflines["pcg"] = {
-            "bound": "hbm", "kernel": "k_ind_cg<1,1>", "achieved": nbytes / t / 1e9, "peak": hbm_peak,
+            "bound": "hbm", "kernel": "k_ind_pcg_pipe (pipelined PCG, molecule blocks)",
+            "achieved": nbytes / t / 1e9, "peak": hbm_peak,
             "unit": "GB/s", "frac": nbytes / t / 1e9 / hbm_peak, "alg_bytes_per_launch": nbytes,
             "products": products, "traffic": 150.7e6, "ms": stage_ms["pcg"],
             "note": "rows and gathers are served mostly from L2 (126 MB); DRAM bytes from the ncu capture"}

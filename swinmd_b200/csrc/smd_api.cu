@@ -866,7 +866,7 @@ int smd_set_multipole(smd_ctx *x, const double *type_mp, const double *polar, do
     CK(cudaMemcpy(c.type_polar, polar, c.ntypes * sizeof(double), cudaMemcpyHostToDevice));
     const size_t n = c.n;
     CK(dalloc(&c.mu, 3 * n)); CK(dalloc(&c.qd, 6 * n)); CK(dalloc(&c.trq, 3 * n));
-    CK(dalloc(&c.e0, 3 * n)); CK(dalloc(&c.pind, 3 * n)); CK(dalloc(&c.cgw, 26 * n));
+    CK(dalloc(&c.e0, 3 * n)); CK(dalloc(&c.pind, 3 * n)); CK(dalloc(&c.cgw, 35 * n));
     CK(dalloc(&c.frame, 9 * n));
     CK(dalloc(&c.cg_blk, 81 * (size_t)c.nmol));
     CK(cudaMemset(c.pind, 0, 3 * n * sizeof(double)));
@@ -875,8 +875,9 @@ int smd_set_multipole(smd_ctx *x, const double *type_mp, const double *polar, do
     CK(cudaMemset(c.e0, 0, 3 * n * sizeof(double)));
     int r = setup_cg(c);
     if (r) return fail(x, r, "smd_set_multipole: solver set-up failed");
-    CK(dalloc(&c.cgs, CG_SCAL + CG_TRACE + 16 * (size_t)c.cg_blocks));
-    CK(cudaMemset(c.cgs, 0, (CG_SCAL + CG_TRACE + 16 * (size_t)c.cg_blocks) * sizeof(double)));
+    const size_t cgb = (size_t)std::max(c.cg_blocks, c.pp_blocks);
+    CK(dalloc(&c.cgs, CG_SCAL + CG_TRACE + 16 * cgb));
+    CK(cudaMemset(c.cgs, 0, (CG_SCAL + CG_TRACE + 16 * cgb) * sizeof(double)));
     CK(dalloc(&c.cg_bar, 2));
     if (c.ind_on) {
         CK(dalloc(&c.phist, 24 * n));
@@ -905,6 +906,14 @@ int smd_set_preconditioner(smd_ctx *x, int kind) {
     if (!x || (kind != SMD_PRECOND_SITE && kind != SMD_PRECOND_MOLECULE))
         return fail(x, SMD_ERR_ARG, "smd_set_preconditioner: kind must be SMD_PRECOND_SITE or SMD_PRECOND_MOLECULE");
     x->c.cg_precond = kind;
+    x->c.graph_dirty = 1;
+    touch(x->c);
+    return SMD_OK;
+}
+
+int smd_set_solver_pipelined(smd_ctx *x, int on) {
+    if (!x) return fail(x, SMD_ERR_ARG, "smd_set_solver_pipelined: null context");
+    x->c.cg_pipelined = on ? 1 : 0;
     x->c.graph_dirty = 1;
     touch(x->c);
     return SMD_OK;

@@ -342,6 +342,7 @@ struct CGArgs {
     double tol;
     const double *blk;       // [nmol][81] inverse molecule blocks of A (molecule preconditioner)
     float *srec;             // mixed path: site records (16 floats per site, p at 10..12), kept current
+    double *w, *m, *q;       // [3][N] the pipelined form's w = A u, m = M^-1 w, q = M^-1 s
 };
 
 // fixed-order block sums, every block computes the same totals: each thread
@@ -845,6 +846,188 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
         beta = gamma_new / gamma;
         alpha_cg = gamma_new / (delta - beta * gamma_new / alpha_cg);
         gamma = gamma_new;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        c.scal[0] = it;
+        c.scal[1] = rms;
+        if (!conv) atomicOr(c.status, ST_CG_ITER);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pipelined preconditioned CG: one grid barrier per iteration
+// ---------------------------------------------------------------------------
+// The mixed path's solve with the molecule blocks, in the pipelined form of
+// Ghysels and Vanroose (2014, Parallel Computing 40: 224-238): with
+// m = M^-1 w and n = A m carried along, the recurrences
+//   z = n + beta z, q = m + beta q, s = w + beta s, p = u + beta p,
+//   x += alpha p,  r -= alpha s,  u -= alpha q,  w -= alpha z
+// keep u = M^-1 r and w = A u without a second product.  Both inner
+// products of the next iteration (gamma = r.u, delta = w.u) and the RMS
+// change come out of the pass that also forms the next m = M^-1 w, so one
+// grid barrier per iteration remains instead of two; alpha and beta are
+// those of standard PCG in exact arithmetic, and the solve stops on the
+// same RMS change.  Each block owns whole molecules (PP_MOLS per pass; the
+// sites of molecule k are 3k .. 3k + 2), so applying the molecule blocks
+// needs only its own sites and a block barrier.  Start: x0 (M^-1 E0 or the
+// dipoles given), r0 = E0 - A x0, u0 = M^-1 r0, w0 = A u0, m0 = M^-1 w0,
+// with three grid barriers.  The packed FP32 copies the products gather
+// alternate between g0 and g1, and the partial sums between two buffers, by
+// iteration parity.
+constexpr int PP_MOLS = 8, PP_SITES = 3 * PP_MOLS, PP_THREADS = PP_SITES * CG_TPP;   // 192 threads
+constexpr double PP_MIN_TOL = 1e-9;   // e nm: below it the single-reduction form runs
+
+__global__ void __launch_bounds__(PP_THREADS, 4) k_ind_pcg_pipe(CGArgs c) {
+    __shared__ double s_w[PP_THREADS / 32][4];
+    __shared__ double s_in[3 * PP_SITES], s_out[3 * PP_SITES];
+    const IndArgs &a = c.ia;
+    const int n = a.n, nmol = a.nmol;
+    float4 *const gb[2] = {(float4 *)c.g0, (float4 *)c.g1};
+    double *const pa[2] = {c.part, c.part + 4 * c.nblocks};
+    // lane group sl of CG_TPP lanes per site; lanes d < 3 of a group own the
+    // site's component d in the vector updates
+    const int sl = threadIdx.x / CG_TPP, t = threadIdx.x - CG_TPP * sl, d = t;
+    const int groups = (nmol + PP_MOLS - 1) / PP_MOLS;
+    const int passes = (groups + (int)gridDim.x - 1) / (int)gridDim.x;
+    unsigned int phase = 0;
+    // failure-path test hook, as in k_ind_cg
+    if ((int)blockIdx.x == c.skip_block) return;
+    auto put_p = [&](int i, int dd, double v) {
+        a.p[dd * n + i] = v;
+        if (c.srec) c.srec[16 * (size_t)i + 10 + dd] = (float)v;
+    };
+    // this lane group's site in pass ps, or -1
+    auto site_of = [&](int ps) {
+        const int gi = blockIdx.x + ps * (int)gridDim.x;
+        const int i = gi * PP_SITES + sl;
+        return (gi < groups && i < n) ? i : -1;
+    };
+    // s_out = M^-1 s_in for the pass's molecules (s_in[3 sl + d] written by
+    // the component lanes; the inverse blocks are stored entry-major); then
+    // the site's packed copy for the products' gathers
+    auto precond = [&](int ps, int i, float4 *pk) {
+        __syncthreads();
+        if (threadIdx.x < 9 * PP_MOLS) {
+            const int ml = threadIdx.x / 9, e = threadIdx.x - 9 * ml;
+            const int mo = (blockIdx.x + ps * (int)gridDim.x) * PP_MOLS + ml;
+            double u = 0.0;
+            if (mo < nmol)
+                for (int col = 0; col < 9; col++) u += __ldcg(&c.blk[(size_t)(e * 9 + col) * nmol + mo]) * s_in[9 * ml + col];
+            s_out[threadIdx.x] = u;
+        }
+        __syncthreads();
+        if (t == 0 && i >= 0)
+            pk[i] = make_float4((float)s_out[3 * sl], (float)s_out[3 * sl + 1], (float)s_out[3 * sl + 2], 0.f);
+    };
+    auto matvec = [&](int i, const float4 *g) {
+        V3 v = i >= 0 ? amul<float4, float>(c, i, t, g) : v3(0, 0, 0);
+        v.x = group_sum<CG_TPP>(v.x); v.y = group_sum<CG_TPP>(v.y); v.z = group_sum<CG_TPP>(v.z);
+        return d == 0 ? v.x : (d == 1 ? v.y : v.z);   // the lane's component (every lane holds the sum)
+    };
+    // x0
+    for (int ps = 0; ps < passes; ps++) {
+        const int i = site_of(ps);
+        if (t == 0 && i >= 0) c.al[i] = fmax(1e-8, a.polar[(int)a.pos4[i].w]);
+        if (c.guess == 0) {
+            if (d < 3) s_in[3 * sl + d] = i >= 0 ? a.e0[d * n + i] : 0.0;
+            precond(ps, i, gb[0]);
+            if (d < 3 && i >= 0) put_p(i, d, s_out[3 * sl + d]);
+        } else {
+            if (d < 3 && i >= 0) put_p(i, d, a.p[d * n + i]);
+            if (t == 0 && i >= 0)
+                gb[0][i] = make_float4((float)a.p[i], (float)a.p[n + i], (float)a.p[2 * n + i], 0.f);
+        }
+    }
+    if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status, c.wait_ns)) return;
+    // r0 = E0 - A x0 ; u0 = M^-1 r0
+    for (int ps = 0; ps < passes; ps++) {
+        const int i = site_of(ps);
+        const double ax = matvec(i, gb[0]);
+        if (d < 3) {
+            const double r = i >= 0 ? a.e0[d * n + i] - ax : 0.0;
+            if (i >= 0) c.r[d * n + i] = r;
+            s_in[3 * sl + d] = r;
+        }
+        precond(ps, i, gb[1]);
+        if (d < 3 && i >= 0) c.u[d * n + i] = s_out[3 * sl + d];
+    }
+    if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status, c.wait_ns)) return;
+    // w0 = A u0 ; m0 = M^-1 w0 ; gamma = r0.u0, delta = w0.u0
+    double vals[4] = {0, 0, 0, 0};
+    for (int ps = 0; ps < passes; ps++) {
+        const int i = site_of(ps);
+        const double au = matvec(i, gb[1]);
+        if (d < 3) {
+            if (i >= 0) {
+                const int idx = d * n + i;
+                c.w[idx] = au;
+                const double u = c.u[idx];
+                vals[0] += c.r[idx] * u;
+                vals[1] += au * u;
+            }
+            s_in[3 * sl + d] = i >= 0 ? au : 0.0;
+        }
+        precond(ps, i, gb[0]);
+        if (d < 3 && i >= 0) c.m[d * n + i] = s_out[3 * sl + d];
+    }
+    block_partials(vals, 2, pa[0], s_w);
+    if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status, c.wait_ns)) return;
+    double tot[4];
+    grid_sum(pa[0], c.nblocks, 2, tot, s_w);
+    double gamma = tot[0], alpha_cg = tot[0] / tot[1], beta = 0.0;
+    int it = 0, cur = 0;   // gb[cur] holds the m the next product gathers
+    double rms = 0;
+    bool conv = false;
+    for (; it < c.max_iter; it++) {
+        if (!(gamma > 0)) {   // r.u = 0: the start already solves A p = E0
+            conv = gamma == 0.0;
+            break;
+        }
+        if (!(alpha_cg > 0)) break;   // breakdown (A not positive definite or non-finite)
+        vals[0] = 0; vals[1] = 0; vals[2] = 0;
+        for (int ps = 0; ps < passes; ps++) {
+            const int i = site_of(ps);
+            const double nv = matvec(i, gb[cur]);
+            if (d < 3) {
+                double wn = 0.0;
+                if (i >= 0) {
+                    const int idx = d * n + i;
+                    const double zv = nv + (it ? beta * c.z[idx] : 0.0);
+                    const double qv = c.m[idx] + (it ? beta * c.q[idx] : 0.0);
+                    const double sv = c.w[idx] + (it ? beta * c.s[idx] : 0.0);
+                    const double pv = c.u[idx] + (it ? beta * c.v[idx] : 0.0);
+                    c.z[idx] = zv; c.q[idx] = qv; c.s[idx] = sv; c.v[idx] = pv;
+                    const double dp = alpha_cg * pv;
+                    put_p(i, d, a.p[idx] + dp);
+                    const double rn = c.r[idx] - alpha_cg * sv;
+                    const double un = c.u[idx] - alpha_cg * qv;
+                    wn = c.w[idx] - alpha_cg * zv;
+                    c.r[idx] = rn; c.u[idx] = un; c.w[idx] = wn;
+                    vals[0] += rn * un;
+                    vals[1] += wn * un;
+                    vals[2] += dp * dp;
+                }
+                s_in[3 * sl + d] = wn;
+            }
+            precond(ps, i, gb[cur ^ 1]);
+            if (d < 3 && i >= 0) c.m[d * n + i] = s_out[3 * sl + d];
+        }
+        double *const pp = pa[(it + 1) & 1];
+        block_partials(vals, 3, pp, s_w);
+        if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status, c.wait_ns)) return;
+        grid_sum(pp, c.nblocks, 3, tot, s_w);
+        rms = sqrt(tot[2] / (3.0 * n));
+        if (blockIdx.x == 0 && threadIdx.x == 0 && it < CG_TRACE) c.scal[CG_SCAL + it] = rms;
+        if (rms < c.tol) {
+            conv = true;
+            it++;
+            break;
+        }
+        const double gamma_new = tot[0], delta = tot[1];
+        beta = gamma_new / gamma;
+        alpha_cg = gamma_new / (delta - beta * gamma_new / alpha_cg);
+        gamma = gamma_new;
+        cur ^= 1;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         c.scal[0] = it;
@@ -1543,6 +1726,20 @@ int setup_cg(Ctx &c) {
     int maxb = per_sm * prop.multiProcessorCount;
     c.cg_blocks = want < maxb ? want : maxb;
     if (c.cg_blocks < 1) c.cg_blocks = 1;
+    // the pipelined form: every molecule three sites, molecule k's at 3k .. 3k + 2
+    bool ok = c.nmol > 0 && c.n == 3 * c.nmol;
+    for (int m = 0; ok && m <= c.nmol; m++) ok = c.h_mol_off[m] == 3 * m;
+    for (int k = 0; ok && k < c.n; k++) ok = c.h_mol_atoms[k] == k;
+    c.pp_blocks = 0;
+    if (ok) {
+        int v = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, (const void *)k_ind_pcg_pipe, PP_THREADS, 0) !=
+            cudaSuccess)
+            return SMD_ERR_CUDA;
+        const int groups = (c.nmol + PP_MOLS - 1) / PP_MOLS;
+        const int mb = v * prop.multiProcessorCount;
+        c.pp_blocks = groups < mb ? groups : mb;
+    }
     return 0;
 }
 
@@ -1694,7 +1891,16 @@ void launch_ind_cg(Ctx &c) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (f32 && bj)
+    g.w = c.cgw + 26 * n; g.m = c.cgw + 29 * n; g.q = c.cgw + 32 * n;
+    // the pipelined recurrences drift by rounding, which limits the change
+    // they can resolve: tight tolerances (the checkers' 1e-13) keep the
+    // single-reduction form
+    if (f32 && bj && c.pp_blocks > 0 && c.cg_pipelined && c.cg_tol >= PP_MIN_TOL) {
+        g.nblocks = c.pp_blocks;
+        cfg.gridDim = dim3(c.pp_blocks);
+        cfg.blockDim = dim3(PP_THREADS);
+        cudaLaunchKernelEx(&cfg, k_ind_pcg_pipe, g);
+    } else if (f32 && bj)
         cudaLaunchKernelEx(&cfg, k_ind_cg<true, true>, g);
     else if (f32)
         cudaLaunchKernelEx(&cfg, k_ind_cg<true, false>, g);

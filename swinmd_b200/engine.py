@@ -476,6 +476,11 @@ class GpuEnsemble:
         self._chk(self.lib.smd_ewald_nk(self.ctx, ctypes.byref(nk)))
         return nk.value
 
+    def set_solver_pipelined(self, on: bool):
+        """Mixed path with molecule blocks: the pipelined PCG (one grid
+        barrier per iteration, the default) or the single-reduction form."""
+        self._chk(self.lib.smd_set_solver_pipelined(self.ctx, int(bool(on))))
+
     def set_solver(self, tol: float = 2.0819e-8, max_iter: int = 500, guess: int = L.GUESS_DIRECT,
                    precond: int = None):
         """Dipole solve settings; precond (L.PRECOND_SITE / L.PRECOND_MOLECULE,

@@ -4,7 +4,7 @@ BuffvdWForce / Multipole / Induction / LFIntegrator results."""
 import numpy as np
 import pytest
 
-from conftest import golden
+from conftest import golden, rms_rel
 from swinmd_b200 import engine, systems
 from swinmd_b200 import _lib as L
 
@@ -230,3 +230,26 @@ def test_fp64_forms_against_reference(reference_forms):
                                             "f_ind_short_force", "f_ind_long_force"))
     assert rms_rel(f_all, ref) < 1e-9
     e.close()
+
+
+@pytest.mark.parametrize("nmol,kmax", [(216, 7), (4096, 18)])
+def test_pipelined_solve_matches_single_reduction(nmol, kmax):
+    """The mixed path's pipelined PCG (one grid barrier per iteration) and
+    the single-reduction form solve the same system at the working dipole
+    tolerance: the same iterations within one, forces within the tolerance's
+    own effect, both well inside the 1e-6 bound."""
+    if nmol == 216:
+        s = systems.polarizable_water(nmol=216, cutoff=0.9, switch=0.8, alpha=3.5, kmax=7, seed=3)
+    else:
+        s = systems.polarizable_water(nmol=nmol, kmax=kmax, seed=1)
+    ens = engine.GpuEnsemble(s, precision="mixed")
+    out = {}
+    for pipe in (False, True):
+        ens.set_solver_pipelined(pipe)
+        ens.set_solver(tol=2.0819e-8, max_iter=500)
+        f, e, _ = ens.compute_forces()
+        out[pipe] = (f, e, ens.solver_stats()[0])
+    print(out[False][2], out[True][2], rms_rel(out[True][0], out[False][0]))
+    assert abs(out[True][2] - out[False][2]) <= 1
+    assert rms_rel(out[True][0], out[False][0]) < 2e-7
+    ens.close()
