@@ -256,18 +256,18 @@ int smd_set_solver(smd_ctx *ctx, double tol, int max_iter, int guess);
 #define SMD_PRECOND_SITE 0
 #define SMD_PRECOND_MOLECULE 1
 int smd_set_preconditioner(smd_ctx *ctx, int kind);
-/* (no reference counterpart) Form of the mixed path's solve with the
- * molecule-block preconditioner: on (the default) the pipelined PCG of
- * Ghysels and Vanroose (one grid barrier per iteration, w = A u and
- * m = M^-1 w kept by recurrence), off the single-reduction form of
- * Chronopoulos and Gear (two barriers).  The same alpha, beta and stopping
+/* (no reference counterpart) Form of the solve with the molecule-block
+ * preconditioner: mode 1 (the default) runs the pipelined PCG of Ghysels
+ * and Vanroose (one grid barrier per iteration, w = A u and m = M^-1 w kept
+ * by recurrence) in the mixed path, mode 2 in both precisions (in FP64 the
+ * single-reduction form is the faster one), mode 0 never: the
+ * single-reduction form of Chronopoulos and Gear (two barriers).  The same alpha, beta and stopping
  * test in exact arithmetic.  The pipelined form needs every molecule to be
  * three sites, molecule k's at sites 3k .. 3k + 2, and a tolerance of at
  * least 1e-9 e nm (its recurrences drift by rounding: on the polarisable
  * water it reaches 2e-10 and stalls near 1e-10); other
- * layouts, tighter tolerances and the FP64 path use the single-reduction
- * form. */
-int smd_set_solver_pipelined(smd_ctx *ctx, int on);
+ * layouts and tighter tolerances use the single-reduction form. */
+int smd_set_solver_pipelined(smd_ctx *ctx, int mode);
 /* Limit (seconds, default 1) of every bounded device-side wait: the dipole
  * solve's grid barrier.  A wait that runs out makes the solve leave, sets
  * SMD_ERR_TIMEOUT and keeps the context usable.  No reference counterpart

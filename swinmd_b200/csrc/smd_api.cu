@@ -913,7 +913,8 @@ int smd_set_preconditioner(smd_ctx *x, int kind) {
 
 int smd_set_solver_pipelined(smd_ctx *x, int on) {
     if (!x) return fail(x, SMD_ERR_ARG, "smd_set_solver_pipelined: null context");
-    x->c.cg_pipelined = on ? 1 : 0;
+    if (on < 0 || on > 2) return fail(x, SMD_ERR_ARG, "smd_set_solver_pipelined: mode must be 0, 1 or 2");
+    x->c.cg_pipelined = on;
     x->c.graph_dirty = 1;
     touch(x->c);
     return SMD_OK;

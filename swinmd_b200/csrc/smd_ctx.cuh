@@ -130,7 +130,7 @@ struct Ctx {
     int cg_guess = 0;               // SMD_GUESS_*: 0 block solution of E0, 1 previous step, 2 learned, 3 first order
     int cg_blocks = 0;
     int pp_blocks = 0;              // grid of the pipelined solve (0: the layout does not allow it)
-    int cg_pipelined = 1;           // mixed path with molecule blocks: pipelined form (one barrier per iteration)
+    int cg_pipelined = 1;           // pipelined solve (molecule blocks): 0 never, 1 mixed path, 2 both precisions
     int cg_precond = SMD_PRECOND_MOLECULE;  // dipole-solve preconditioner
     double *cg_blk = nullptr;       // [nmol][81] inverse molecule blocks of A
     unsigned int *cg_bar = nullptr; // grid barrier: [0] counter, [1] abort word of the launch

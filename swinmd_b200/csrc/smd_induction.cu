@@ -857,7 +857,7 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
 // ---------------------------------------------------------------------------
 // Pipelined preconditioned CG: one grid barrier per iteration
 // ---------------------------------------------------------------------------
-// The mixed path's solve with the molecule blocks, in the pipelined form of
+// The solve with the molecule blocks (either precision), in the pipelined form of
 // Ghysels and Vanroose (2014, Parallel Computing 40: 224-238): with
 // m = M^-1 w and n = A m carried along, the recurrences
 //   z = n + beta z, q = m + beta q, s = w + beta s, p = u + beta p,
@@ -877,12 +877,15 @@ __global__ void __launch_bounds__(CG_THREADS, 3) k_ind_cg(CGArgs c) {
 constexpr int PP_MOLS = 8, PP_SITES = 3 * PP_MOLS, PP_THREADS = PP_SITES * CG_TPP;   // 192 threads
 constexpr double PP_MIN_TOL = 1e-9;   // e nm: below it the single-reduction form runs
 
+template <bool F32>
 __global__ void __launch_bounds__(PP_THREADS, 4) k_ind_pcg_pipe(CGArgs c) {
+    using G4 = typename std::conditional<F32, float4, double4>::type;
+    using GR = typename std::conditional<F32, float, double>::type;
     __shared__ double s_w[PP_THREADS / 32][4];
     __shared__ double s_in[3 * PP_SITES], s_out[3 * PP_SITES];
     const IndArgs &a = c.ia;
     const int n = a.n, nmol = a.nmol;
-    float4 *const gb[2] = {(float4 *)c.g0, (float4 *)c.g1};
+    G4 *const gb[2] = {(G4 *)c.g0, (G4 *)c.g1};
     double *const pa[2] = {c.part, c.part + 4 * c.nblocks};
     // lane group sl of CG_TPP lanes per site; lanes d < 3 of a group own the
     // site's component d in the vector updates
@@ -905,7 +908,7 @@ __global__ void __launch_bounds__(PP_THREADS, 4) k_ind_pcg_pipe(CGArgs c) {
     // s_out = M^-1 s_in for the pass's molecules (s_in[3 sl + d] written by
     // the component lanes; the inverse blocks are stored entry-major); then
     // the site's packed copy for the products' gathers
-    auto precond = [&](int ps, int i, float4 *pk) {
+    auto precond = [&](int ps, int i, G4 *pk) {
         __syncthreads();
         if (threadIdx.x < 9 * PP_MOLS) {
             const int ml = threadIdx.x / 9, e = threadIdx.x - 9 * ml;
@@ -917,10 +920,10 @@ __global__ void __launch_bounds__(PP_THREADS, 4) k_ind_pcg_pipe(CGArgs c) {
         }
         __syncthreads();
         if (t == 0 && i >= 0)
-            pk[i] = make_float4((float)s_out[3 * sl], (float)s_out[3 * sl + 1], (float)s_out[3 * sl + 2], 0.f);
+            pk[i] = G4{(GR)s_out[3 * sl], (GR)s_out[3 * sl + 1], (GR)s_out[3 * sl + 2], (GR)0};
     };
-    auto matvec = [&](int i, const float4 *g) {
-        V3 v = i >= 0 ? amul<float4, float>(c, i, t, g) : v3(0, 0, 0);
+    auto matvec = [&](int i, const G4 *g) {
+        V3 v = i >= 0 ? amul<G4, GR>(c, i, t, g) : v3(0, 0, 0);
         v.x = group_sum<CG_TPP>(v.x); v.y = group_sum<CG_TPP>(v.y); v.z = group_sum<CG_TPP>(v.z);
         return d == 0 ? v.x : (d == 1 ? v.y : v.z);   // the lane's component (every lane holds the sum)
     };
@@ -935,7 +938,7 @@ __global__ void __launch_bounds__(PP_THREADS, 4) k_ind_pcg_pipe(CGArgs c) {
         } else {
             if (d < 3 && i >= 0) put_p(i, d, a.p[d * n + i]);
             if (t == 0 && i >= 0)
-                gb[0][i] = make_float4((float)a.p[i], (float)a.p[n + i], (float)a.p[2 * n + i], 0.f);
+                gb[0][i] = G4{(GR)a.p[i], (GR)a.p[n + i], (GR)a.p[2 * n + i], (GR)0};
         }
     }
     if (!grid_barrier(c.bar, (++phase) * c.nblocks, c.status, c.wait_ns)) return;
@@ -1733,9 +1736,13 @@ int setup_cg(Ctx &c) {
     c.pp_blocks = 0;
     if (ok) {
         int v = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, (const void *)k_ind_pcg_pipe, PP_THREADS, 0) !=
-            cudaSuccess)
+        int v2 = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, (const void *)k_ind_pcg_pipe<true>, PP_THREADS, 0) !=
+                cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v2, (const void *)k_ind_pcg_pipe<false>, PP_THREADS, 0) !=
+                cudaSuccess)
             return SMD_ERR_CUDA;
+        v = v2 < v ? v2 : v;
         const int groups = (c.nmol + PP_MOLS - 1) / PP_MOLS;
         const int mb = v * prop.multiProcessorCount;
         c.pp_blocks = groups < mb ? groups : mb;
@@ -1895,11 +1902,17 @@ void launch_ind_cg(Ctx &c) {
     // the pipelined recurrences drift by rounding, which limits the change
     // they can resolve: tight tolerances (the checkers' 1e-13) keep the
     // single-reduction form
-    if (f32 && bj && c.pp_blocks > 0 && c.cg_pipelined && c.cg_tol >= PP_MIN_TOL) {
+    // mode 1 (the default): the mixed path only; in FP64 the single-reduction
+    // form is the faster one (double4 gathers; 0.450 against 0.480 ms on
+    // polwater4096); mode 2: both precisions
+    if (bj && c.pp_blocks > 0 && c.cg_pipelined >= (f32 ? 1 : 2) && c.cg_tol >= PP_MIN_TOL) {
         g.nblocks = c.pp_blocks;
         cfg.gridDim = dim3(c.pp_blocks);
         cfg.blockDim = dim3(PP_THREADS);
-        cudaLaunchKernelEx(&cfg, k_ind_pcg_pipe, g);
+        if (f32)
+            cudaLaunchKernelEx(&cfg, k_ind_pcg_pipe<true>, g);
+        else
+            cudaLaunchKernelEx(&cfg, k_ind_pcg_pipe<false>, g);
     } else if (f32 && bj)
         cudaLaunchKernelEx(&cfg, k_ind_cg<true, true>, g);
     else if (f32)

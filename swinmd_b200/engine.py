@@ -476,10 +476,12 @@ class GpuEnsemble:
         self._chk(self.lib.smd_ewald_nk(self.ctx, ctypes.byref(nk)))
         return nk.value
 
-    def set_solver_pipelined(self, on: bool):
-        """Mixed path with molecule blocks: the pipelined PCG (one grid
-        barrier per iteration, the default) or the single-reduction form."""
-        self._chk(self.lib.smd_set_solver_pipelined(self.ctx, int(bool(on))))
+    def set_solver_pipelined(self, mode: int):
+        """Solve with molecule blocks at tolerances >= 1e-9 e nm: the
+        pipelined PCG (one grid barrier per iteration) in the mixed path
+        (mode 1, the default), in both precisions (2), or never (0: the
+        single-reduction form)."""
+        self._chk(self.lib.smd_set_solver_pipelined(self.ctx, int(mode)))
 
     def set_solver(self, tol: float = 2.0819e-8, max_iter: int = 500, guess: int = L.GUESS_DIRECT,
                    precond: int = None):

@@ -4,7 +4,7 @@ BuffvdWForce / Multipole / Induction / LFIntegrator results."""
 import numpy as np
 import pytest
 
-from conftest import golden, rms_rel
+from conftest import golden
 from swinmd_b200 import engine, systems
 from swinmd_b200 import _lib as L
 
@@ -232,20 +232,21 @@ def test_fp64_forms_against_reference(reference_forms):
     e.close()
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
 @pytest.mark.parametrize("nmol,kmax", [(216, 7), (4096, 18)])
-def test_pipelined_solve_matches_single_reduction(nmol, kmax):
-    """The mixed path's pipelined PCG (one grid barrier per iteration) and
-    the single-reduction form solve the same system at the working dipole
+def test_pipelined_solve_matches_single_reduction(nmol, kmax, precision):
+    """The pipelined PCG (one grid barrier per iteration) and the
+    single-reduction form solve the same system at the working dipole
     tolerance: the same iterations within one, forces within the tolerance's
     own effect, both well inside the 1e-6 bound."""
     if nmol == 216:
         s = systems.polarizable_water(nmol=216, cutoff=0.9, switch=0.8, alpha=3.5, kmax=7, seed=3)
     else:
         s = systems.polarizable_water(nmol=nmol, kmax=kmax, seed=1)
-    ens = engine.GpuEnsemble(s, precision="mixed")
+    ens = engine.GpuEnsemble(s, precision=precision)
     out = {}
     for pipe in (False, True):
-        ens.set_solver_pipelined(pipe)
+        ens.set_solver_pipelined(2 if pipe else 0)
         ens.set_solver(tol=2.0819e-8, max_iter=500)
         f, e, _ = ens.compute_forces()
         out[pipe] = (f, e, ens.solver_stats()[0])
