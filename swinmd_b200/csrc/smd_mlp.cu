@@ -239,6 +239,20 @@ __device__ __forceinline__ void load_weights(MlpW &S, const float *W, __nv_bfloa
 
 // the two hidden layers of one warp's 16 rows (normalised BF16 inputs in
 // xs, row stride SX): h1, h2 after tanh, as accumulator fragments
+// the hidden activation: tanhf, or with FAST the hardware approximation
+// (tanh.approx.f32, relative error about 2^-11, below the BF16 rounding the
+// next layer applies to it); training and the checker's entry use tanhf
+template <bool FAST>
+__device__ __forceinline__ float act(float x) {
+    if (FAST) {
+        float y;
+        asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+        return y;
+    }
+    return tanhf(x);
+}
+
+template <bool FAST = false>
 __device__ __forceinline__ void warp_hidden(const MlpW &S, const __nv_bfloat16 *xs, float (&h1)[8][4],
                                             float (&h2)[8][4]) {
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -260,7 +274,7 @@ __device__ __forceinline__ void warp_hidden(const MlpW &S, const __nv_bfloat16 *
 #pragma unroll
     for (int nt = 0; nt < 8; nt++)
 #pragma unroll
-        for (int q = 0; q < 4; q++) h1[nt][q] = tanhf(h1[nt][q]);
+        for (int q = 0; q < 4; q++) h1[nt][q] = act<FAST>(h1[nt][q]);
 #pragma unroll
     for (int nt = 0; nt < 8; nt++) {
         const float b0 = S.b2[nt * 8 + 2 * t], b1 = S.b2[nt * 8 + 2 * t + 1];
@@ -279,7 +293,7 @@ __device__ __forceinline__ void warp_hidden(const MlpW &S, const __nv_bfloat16 *
 #pragma unroll
     for (int nt = 0; nt < 8; nt++)
 #pragma unroll
-        for (int q = 0; q < 4; q++) h2[nt][q] = tanhf(h2[nt][q]);
+        for (int q = 0; q < 4; q++) h2[nt][q] = act<FAST>(h2[nt][q]);
 }
 
 // output layer in FP32: y of rows g (lo) and g + 8 (hi), in every lane of
@@ -347,7 +361,7 @@ __global__ void __launch_bounds__(MLP_TB) k_mlp_infer(int n, const int *mol, con
     __syncthreads();
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     float h1[8][4], h2[8][4], lo[MO], hi[MO];
-    warp_hidden(S, sX + 16 * w * SX, h1, h2);
+    warp_hidden<true>(S, sX + 16 * w * SX, h1, h2);
     warp_out(S, h2, lo, hi);
     if (t == 0)
         for (int o = 0; o < MO; o++) {
