@@ -26,7 +26,9 @@ one after another on the same trajectory:
 Every arm solves the dipoles to the same tolerance (RMS change 1e-6 D).  The
 line also carries the solver's iterations from each guess, each arm's force
 error against FP64 with the dipoles solved to 1e-13 e nm, pair interactions
-per second and both arms' energy drift in an NVE run from the same state.
+per second and both arms' energy drift in an NVE run from the same state
+(10^4 steps), with the same drift of the rigid SPC/E water configuration in
+both precisions.
 
 One "step" is one MD time step: pair-list check/rebuild, all forces (vdW,
 multipoles, dipole solve, induced terms), SHAKE + Nose-Hoover update and
@@ -63,7 +65,7 @@ METRIC = "ns/day on 1 B200: learned-guess+mixed vs plain GPU path at matched for
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 DIPOLE_TOL = 2.0819e-8   # 1e-6 D in e nm
-SERIES_CAP = 4096        # per-step samples kept for the energy drift
+SERIES_CAP = 10000       # per-step samples kept for the energy drift
 
 
 def workload(name, nmol=None):
@@ -434,6 +436,49 @@ def run_replicas(args, rank, world, local):
     batch.close()
 
 
+def spce_drift(steps, equilibrate=2000):
+    """NVE energy drift of rigid SPC/E water (2160 molecules in a 4.03 nm
+    box, LJ on O, Ewald alpha 3.1/nm with |n| < 9, SHAKE tolerance 1e-8,
+    dt 2 fs) in FP64 and in the mixed path from the same state, equilibrated
+    with the Nose-Hoover thermostat first; and the mixed path's RMS relative
+    force error against FP64 at that state."""
+    from swinmd_b200 import engine, systems
+    from swinmd_b200 import _lib as L
+    s = systems.spce_water(nmol=2160, box=4.03, cutoff=1.0, kmax=9, seed=1)
+    ens = engine.GpuEnsemble(s, precision="mixed")
+    lf = engine.LFIntegrator(ens, series_capacity=SERIES_CAP)
+    lf.start()
+    lf.run(equilibrate)
+    st0 = ens.state()
+    ens.set_precision("fp64")
+    f64, _, _ = ens.compute_forces()
+    ens.set_precision("mixed")
+    f32, _, _ = ens.compute_forces()
+    err = float(np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum()))
+    nve = lf.params
+    nve.thermostat = L.THERMO_NONE
+    L.check(ens.ctx, ens.lib.smd_set_integrator(ens.ctx, ctypes.byref(nve)))
+    dt = s.config.timestep
+    steps = min(steps, SERIES_CAP)
+    out = {"workload": "spce2160: rigid SPC/E water, 2160 molecules, 4.03 nm box, LJ (O) + Ewald "
+                       "alpha=3.1/nm |n|<9, rc=1.0 nm, SHAKE tol 1e-8, dt=2 fs, NVE after "
+                       f"{equilibrate} Nose-Hoover steps at 298 K",
+           "force_rms_rel_err_vs_fp64": err}
+    for name, prec in (("plain", "fp64"), ("fast", "mixed")):
+        ens.set_precision(prec)
+        ens.upload_positions(st0["pos"])
+        ens.upload_velocities(st0["vel"], st0["vtminus"])
+        lf.run(steps)
+        ser = lf.series()[-steps:]
+        h = ser[:, 0] + ser[:, 1]
+        tt = np.arange(steps) * dt * 1e-3   # ns
+        fit = np.polyfit(tt, h, 1)
+        out[name] = {"kj_mol_per_ns": float(fit[0]), "kj_mol_per_ns_per_molecule": float(fit[0]) / s.n_mols,
+                     "rms_fluctuation_kj_mol": float(np.std(h - np.polyval(fit, tt))), "steps": steps}
+    ens.close()
+    return out
+
+
 def timed_steps(lf, l2, steps, chunk):
     import torch
     total = 0.0
@@ -462,7 +507,7 @@ def main():
     ap.add_argument("--cpu-sample-mols", type=int, default=1024)
     ap.add_argument("--equilibrate", type=int, default=10000)
     ap.add_argument("--iter-steps", type=int, default=20)
-    ap.add_argument("--drift-steps", type=int, default=2000)
+    ap.add_argument("--drift-steps", type=int, default=10000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -641,6 +686,11 @@ def main():
     if polar:
         ens.set_solver(tol=DIPOLE_TOL, max_iter=500, guess=L.GUESS_LEARNED)
 
+    # energy drift of the rigid water of the SPC/E configuration (2160
+    # molecules, LJ + Ewald |n| < 9, SHAKE): both precisions from the same
+    # equilibrated state, NVE, and the mixed path's force error against FP64
+    drift_c3 = spce_drift(args.drift_steps) if polar and world == 1 else None
+
     # --- end to end through the public API, host buffers ------------------
     pos = torch.empty(3 * n, dtype=torch.float64).pin_memory().numpy()
     vel = torch.empty(3 * n, dtype=torch.float64).pin_memory().numpy()
@@ -786,6 +836,7 @@ def main():
                "pair_interactions_note": "unordered site pairs inside the short-range cutoff per step "
                                          "(the fast arm's) / s per step",
                "energy_drift": energy_drift,
+               "energy_drift_spce2160": drift_c3,
                "training": train,
                "e2e": {"value": e2e_value, "unit": "ns/day", "h2d_bytes_per_step": 2 * 3 * n * 8 / every,
                        "d2h_bytes_per_step": (2 * 3 * n * 8 + 512) / every,

@@ -81,37 +81,46 @@ __global__ void k_lustig_lj(int n, const int *nbr, const int *nnbr, const double
     }
 }
 
+// grows the evaluation's scratch (the context owns it; freed with the context)
+static int lus_reserve(Ctx &c, size_t doubles) {
+    if (!c.lus_com) {
+        if (cudaMalloc(&c.lus_com, (size_t)c.nmol * sizeof(double4)) != cudaSuccess) return SMD_ERR_CUDA;
+    }
+    if (doubles > c.lus_cap) {
+        if (c.lus_buf) cudaFree(c.lus_buf);
+        c.lus_buf = nullptr;
+        c.lus_cap = 0;
+        if (cudaMalloc(&c.lus_buf, doubles * sizeof(double)) != cudaSuccess) return SMD_ERR_CUDA;
+        c.lus_cap = doubles;
+    }
+    return SMD_OK;
+}
+
 int lustig_lj(Ctx &c, double *out) {
     if (c.vdw != VDW_LJ) return SMD_ERR_ARG;
-    double *mass = nullptr;
-    double4 *com = nullptr;
-    long long *acc = nullptr;
-    auto done = [&](int r) {
-        cudaFree(mass); cudaFree(com); cudaFree(acc);
-        return r;
-    };
-    if (cudaMalloc(&mass, c.n * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&com, c.nmol * sizeof(double4)) != cudaSuccess ||
-        cudaMalloc(&acc, 3 * sizeof(long long)) != cudaSuccess)
-        return done(SMD_ERR_CUDA);
-    cudaMemcpyAsync(mass, c.h_mass.data(), c.n * sizeof(double), cudaMemcpyHostToDevice, c.stream);
+    // the three fixed-point sums in the context's scratch (no allocation
+    // after the first call)
+    int r = lus_reserve(c, 3);
+    if (r) return r;
+    long long *acc = reinterpret_cast<long long *>(c.lus_buf);
     cudaMemsetAsync(acc, 0, 3 * sizeof(long long), c.stream);
     launch_nlist(c, !c.list_built);
-    k_mol_com<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.mol_off, c.mol_atoms, c.pos4, mass, com);
-    k_lustig_lj<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.pl.nbr, c.pl.nnbr, c.pos4, c.mol, com, c.pair_par,
-                                                         c.ntypes, c.box, c.vdw_rc2, c.switch_on,
+    k_mol_com<<<(c.nmol + 127) / 128, 128, 0, c.stream>>>(c.nmol, c.mol_off, c.mol_atoms, c.pos4, c.mass,
+                                                         c.lus_com);
+    k_lustig_lj<<<(c.n + 127) / 128, 128, 0, c.stream>>>(c.n, c.pl.nbr, c.pl.nnbr, c.pos4, c.mol, c.lus_com,
+                                                         c.pair_par, c.ntypes, c.box, c.vdw_rc2, c.switch_on,
                                                          c.clen2 != nullptr, acc);
     long long h[3];
     if (cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
         cudaStreamSynchronize(c.stream) != cudaSuccess)
-        return done(SMD_ERR_CUDA);
+        return SMD_ERR_CUDA;
     const double V = c.box.L[0] * c.box.L[1] * c.box.L[2];
     const double su = 0.5 * (double)h[0] / LUS_SCALE, s1 = 0.5 * (double)h[1] / LUS_SCALE,
                  s2 = 0.5 * (double)h[2] / LUS_SCALE;
     out[0] = su + c.e_lrc;
     out[1] = -s1 / (3.0 * V) - 2.0 * c.e_lrc / V;
     out[2] = s2 / (9.0 * V * V) + 6.0 * c.e_lrc / (V * V);
-    return done(SMD_OK);
+    return SMD_OK;
 }
 
 // ===========================================================================
@@ -559,21 +568,6 @@ __global__ void __launch_bounds__(LU_THREADS) k_lus_bonded(int nbond, const int4
 }
 
 namespace {
-
-// grows the evaluation's scratch (the context owns it; freed with the context)
-int lus_reserve(Ctx &c, size_t doubles) {
-    if (!c.lus_com) {
-        if (cudaMalloc(&c.lus_com, (size_t)c.nmol * sizeof(double4)) != cudaSuccess) return SMD_ERR_CUDA;
-    }
-    if (doubles > c.lus_cap) {
-        if (c.lus_buf) cudaFree(c.lus_buf);
-        c.lus_buf = nullptr;
-        c.lus_cap = 0;
-        if (cudaMalloc(&c.lus_buf, doubles * sizeof(double)) != cudaSuccess) return SMD_ERR_CUDA;
-        c.lus_cap = doubles;
-    }
-    return SMD_OK;
-}
 
 // the first cnt * nv partials, summed per value in block order
 int lus_fetch(Ctx &c, int cnt, int nv, double *tot) {
