@@ -509,6 +509,8 @@ def main():
     ap.add_argument("--iter-steps", type=int, default=20)
     ap.add_argument("--drift-steps", type=int, default=10000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mlp-tensor-path", type=int, default=1, choices=[0, 1],
+                    help="network inference on tcgen05 128-row tiles (1) or warp-level mma.sync tiles (0)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -554,6 +556,7 @@ def main():
     if polar:
         # training rows: the solver's own converged dipoles along the trajectory
         ens.mlp_init(capacity_frames=args.train_frames, seed=1)
+        ens.mlp_set_tensor_path(args.mlp_tensor_path)
         t0 = time.perf_counter()
         for _ in range(args.train_frames):
             lf.run(args.train_every)
@@ -563,6 +566,7 @@ def main():
         loss = ens.mlp_train(epochs=args.train_epochs, batch=16384, lr=2e-3)
         train = {"frames": args.train_frames, "rows": args.train_frames * s.n_atoms,
                  "epochs": args.train_epochs, "final_mse": loss,
+                 "inference": "tcgen05" if args.mlp_tensor_path else "mma.sync",
                  "collect_s": t1 - t0, "train_s": time.perf_counter() - t1}
 
     clk_all = ClockSampler(local)

@@ -34,7 +34,8 @@ enum {
     SMD_ERR_CG = 7,           /* dipole solve did not converge */
     SMD_ERR_NO_DEVICE = 8,    /* no CUDA device / extension unusable */
     SMD_ERR_TIMEOUT = 9,      /* a bounded device-side wait ran out (the dipole
-                                 solve's grid barrier; see smd_set_wait_limit) */
+                                 solve's grid barrier, see smd_set_wait_limit; the
+                                 network's tensor-core completion wait) */
     SMD_ERR_BOX = 10          /* the barostat shrank the box below the cell grid's
                                  reach (run again from smd_integrator_start) */
 };
@@ -268,6 +269,14 @@ int smd_set_preconditioner(smd_ctx *ctx, int kind);
  * water it reaches 2e-10 and stalls near 1e-10); other
  * layouts and tighter tolerances use the single-reduction form. */
 int smd_set_solver_pipelined(smd_ctx *ctx, int mode);
+/* (no reference counterpart) Tensor-core path of the learned guess's
+ * network (inference in the step and smd_mlp_eval): path 1 (the default)
+ * runs the two hidden layers as 128-row tiles on the tcgen05 tensor cores
+ * (BF16 operands in shared memory, FP32 accumulators in tensor memory),
+ * path 0 as 16-row warp-level mma.sync tiles.  Both round the inputs and the
+ * first hidden layer to BF16 and accumulate in FP32; their outputs agree to
+ * FP32 summation order.  Training always uses the warp-level tiles. */
+int smd_mlp_set_tensor_path(smd_ctx *ctx, int path);
 /* Limit (seconds, default 1) of every bounded device-side wait: the dipole
  * solve's grid barrier.  A wait that runs out makes the solve leave, sets
  * SMD_ERR_TIMEOUT and keeps the context usable.  No reference counterpart

@@ -920,6 +920,15 @@ int smd_set_solver_pipelined(smd_ctx *x, int on) {
     return SMD_OK;
 }
 
+int smd_mlp_set_tensor_path(smd_ctx *x, int path) {
+    if (!x) return fail(x, SMD_ERR_ARG, "smd_mlp_set_tensor_path: null context");
+    if (path < 0 || path > 1) return fail(x, SMD_ERR_ARG, "smd_mlp_set_tensor_path: path must be 0 or 1");
+    x->c.mlp_tc = path;
+    x->c.graph_dirty = 1;
+    touch(x->c);
+    return SMD_OK;
+}
+
 int smd_set_wait_limit(smd_ctx *x, double seconds) {
     if (!x || !(seconds > 0) || seconds > 600)
         return fail(x, SMD_ERR_ARG, "smd_set_wait_limit: the limit must lie in (0, 600] s");

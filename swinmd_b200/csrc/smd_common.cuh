@@ -66,7 +66,8 @@ enum StatusBits {
     ST_CG_ITER = 32,         // dipole solver did not converge
     ST_SHAKE_GEOM = 64,      // SHAKE geometric failure (reference LFIntegrator.cpp:1758)
     ST_WAIT_TIMEOUT = 128,   // a bounded device-side wait (the dipole solve's grid
-                             // barrier) ran out: blocks not co-resident or one missing
+                             // barrier, the network's tensor-core mbarrier) ran out:
+                             // blocks not co-resident, one missing, or no commit
     ST_BOX = 256             // the barostat shrank the box below what the cell grid covers
 };
 

@@ -146,6 +146,7 @@ struct Ctx {
     // per-site network giving the initial induced dipoles (smd_mlp.cu)
     int mlp_ready = 0;
     int mlp_base = 2;                // order of the extrapolated guess the network corrects
+    int mlp_tc = 1;                  // inference and evaluation: 1 tcgen05 tiles of 128 rows, 0 warp-level mma.sync
     float *mlp_w = nullptr;         // parameters, MLP_NPARAM floats
     float *mlp_m = nullptr, *mlp_v = nullptr;  // Adam moments
     float *mlp_part = nullptr;      // per-block gradient partials

@@ -617,6 +617,235 @@ __global__ void k_mlp_adam(int nblocks, const float *part, float *W, float *m, f
 }
 
 // ---------------------------------------------------------------------------
+// the two hidden layers on the 5th-generation tensor cores (tcgen05)
+// ---------------------------------------------------------------------------
+// One CTA of 128 threads takes 128 rows (sites or feature rows), thread r
+// row r: one M = 128 tile.  The BF16 inputs, the layer-1 activations and
+// both weight matrices sit in shared memory in the unswizzled K-major
+// layout of the tensor cores' operands (8-row x 16-byte core matrices, the
+// 8-row groups 128 B apart, the 8-element K chunks R x 16 B apart for an
+// R-row tile); one elected thread issues tcgen05.mma (kind::f16: BF16
+// operands, FP32 accumulation in tensor memory, N = 64, K = 16 per
+// instruction) and commits to an mbarrier; every thread then reads its own
+// row of the accumulator (tensor-memory lane r) with tcgen05.ld, adds the
+// bias, applies the activation and writes the BF16 row the next layer
+// reads.  Layer 1 takes tensor-memory columns 0-63, layer 2 64-127; the
+// 64 -> 3 output layer runs in FP32 in registers.  The mbarrier waits are
+// bounded: a wait that runs out sets ST_WAIT_TIMEOUT and the row's output is
+// zero.
+constexpr int TC_ROWS = 128;
+
+// byte offset of element (row, k) of an R-row K-major tile
+__host__ __device__ __forceinline__ uint32_t tc_ofs(int row, int k, int R) {
+    return (uint32_t)(((k >> 3) * (R >> 3) + (row >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+// shared-memory matrix descriptor (start, leading = K-chunk, stride = 8-row
+// group byte offsets; version 1; no swizzle)
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr & 0x3FFFF) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
+}
+
+struct TcSmem {
+    __align__(1024) unsigned char x[TC_ROWS * KP * 2];   // inputs
+    __align__(1024) unsigned char h[TC_ROWS * MH * 2];   // layer-1 activations
+    __align__(1024) unsigned char w1[MH * KP * 2];
+    __align__(1024) unsigned char w2[MH * MH * 2];
+    float b1[MH], b2[MH], w3[MO * MH], b3[4];
+    __align__(8) unsigned long long mbar;
+    unsigned int tbase;
+    // keeps the footprint above a fifth of the SM's shared memory: at most
+    // four CTAs per SM, whose 4 x 128 tensor-memory columns all fit, so no
+    // tcgen05.alloc has to wait for another CTA's release
+    unsigned char pad[7 * 1024];
+};
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                 "l"(da), "l"(db), "r"(idesc), "r"(acc));
+}
+
+// waits for the mbarrier's given phase (bounded); false if it ran out
+__device__ __forceinline__ bool tc_wait(uint32_t mb, uint32_t phase) {
+    uint32_t done = 0;
+    for (int it = 0; it < (1 << 22) && !done; it++)
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done) : "r"(mb), "r"(phase) : "memory");
+    return done != 0;
+}
+
+// 16 consecutive FP32 columns of this thread's tensor-memory lane
+__device__ __forceinline__ void tc_ld16(uint32_t addr, float (&v)[16]) {
+    uint32_t u[16];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]), "=r"(u[7]),
+                   "=r"(u[8]), "=r"(u[9]), "=r"(u[10]), "=r"(u[11]), "=r"(u[12]), "=r"(u[13]), "=r"(u[14]), "=r"(u[15])
+                 : "r"(addr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; j++) v[j] = __uint_as_float(u[j]);
+}
+
+// 8 values as one 16-byte row of a core matrix (BF16, round to nearest)
+__device__ __forceinline__ void tc_st8(unsigned char *dst, const float *v) {
+    uint4 u;
+    uint32_t *w = &u.x;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+        w[j] = *reinterpret_cast<const uint32_t *>(&b2);
+    }
+    *reinterpret_cast<uint4 *>(dst) = u;
+}
+
+// the weights of the network into the operand layouts
+__device__ __forceinline__ void tc_load_weights(TcSmem &S, const float *W) {
+    // one 16-byte core-matrix row (8 inputs of output j) per store
+    for (int k = threadIdx.x; k < MH * (KP / 8); k += blockDim.x) {
+        const int j = k / (KP / 8), f0 = 8 * (k - j * (KP / 8));
+        float v[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) v[e] = f0 + e < MF ? W[OW1 + j * MF + f0 + e] : 0.f;
+        tc_st8(S.w1 + tc_ofs(j, f0, MH), v);
+    }
+    for (int k = threadIdx.x; k < MH * (MH / 8); k += blockDim.x) {
+        const int j = k / (MH / 8), q0 = 8 * (k - j * (MH / 8));
+        float v[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) v[e] = W[OW2 + j * MH + q0 + e];
+        tc_st8(S.w2 + tc_ofs(j, q0, MH), v);
+    }
+    for (int k = threadIdx.x; k < MH; k += blockDim.x) { S.b1[k] = W[OB1 + k]; S.b2[k] = W[OB2 + k]; }
+    for (int k = threadIdx.x; k < MO * MH; k += blockDim.x) S.w3[k] = W[OW3 + k];
+    if (threadIdx.x < MO) S.b3[threadIdx.x] = W[OB3 + threadIdx.x];
+}
+
+// S.x holds this CTA's 128 input rows; y = the network's output for the
+// thread's row.  Every thread of the 128 calls it.
+template <bool FAST>
+__device__ void tc_forward(TcSmem &S, float (&y)[MO], unsigned int *status) {
+    const int tid = threadIdx.x, w = tid >> 5;
+    const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&S.mbar);
+    if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb));
+    if (w == 0) {
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&S.tbase);
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(128));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    // the operand tiles written by the threads, visible to the tensor cores
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = S.tbase;
+    // kind::f16: F32 accumulator, BF16 A and B, both K-major, N = 64, M = 128
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(MH >> 3) << 17) |
+                           ((uint32_t)(TC_ROWS >> 4) << 24);
+    const uint32_t x0 = (uint32_t)__cvta_generic_to_shared(S.x), h0 = (uint32_t)__cvta_generic_to_shared(S.h);
+    const uint32_t w10 = (uint32_t)__cvta_generic_to_shared(S.w1), w20 = (uint32_t)__cvta_generic_to_shared(S.w2);
+    constexpr uint32_t LA = (TC_ROWS / 8) * 128, LB = (MH / 8) * 128;   // K-chunk strides
+    if (tid == 0) {
+        for (int ks = 0; ks < KP / 16; ks++)
+            tc_mma(tmem, tc_desc(x0 + ks * 2 * LA, LA, 128), tc_desc(w10 + ks * 2 * LB, LB, 128), idesc, ks > 0);
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mb)
+                     : "memory");
+    }
+    bool ok = tc_wait(mb, 0);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t lane_base = tmem + ((uint32_t)(32 * w) << 16);
+    if (ok)
+        for (int c0 = 0; c0 < MH; c0 += 16) {
+            float v[16];
+            tc_ld16(lane_base + c0, v);
+#pragma unroll
+            for (int j = 0; j < 16; j++) v[j] = act<FAST>(v[j] + S.b1[c0 + j]);
+            tc_st8(S.h + tc_ofs(tid, c0, TC_ROWS), v);
+            tc_st8(S.h + tc_ofs(tid, c0 + 8, TC_ROWS), v + 8);
+        }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) {
+        for (int ks = 0; ks < MH / 16; ks++)
+            tc_mma(tmem + MH, tc_desc(h0 + ks * 2 * LA, LA, 128), tc_desc(w20 + ks * 2 * LB, LB, 128), idesc, ks > 0);
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mb)
+                     : "memory");
+    }
+    ok = tc_wait(mb, 1) && ok;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    for (int o = 0; o < MO; o++) y[o] = 0.f;
+    if (ok) {
+        for (int o = 0; o < MO; o++) y[o] = S.b3[o];
+        for (int c0 = 0; c0 < MH; c0 += 16) {
+            float v[16];
+            tc_ld16(lane_base + MH + c0, v);
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                const float hj = act<FAST>(v[j] + S.b2[c0 + j]);
+                for (int o = 0; o < MO; o++) y[o] = fmaf(S.w3[o * MH + c0 + j], hj, y[o]);
+            }
+        }
+    } else if (tid == 0) {
+        atomicOr(status, ST_WAIT_TIMEOUT);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (w == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128));
+}
+
+// the learned start on the tensor cores: k_mlp_infer's inputs and output
+__global__ void __launch_bounds__(TC_ROWS) k_mlp_infer_tc(int n, const int *mol, const int *mol_off,
+                                                          const int *mol_atoms, const double4 *pos4,
+                                                          const double *e0, const float *norm, const float *Wg,
+                                                          const double *frame, const double *dl, const double *dlp,
+                                                          const double *ph, const int *flags, double *p, int order,
+                                                          unsigned int *status) {
+    __shared__ TcSmem S;
+    tc_load_weights(S, Wg);
+    const int cnt = flags[2];
+    const int i = blockIdx.x * TC_ROWS + threadIdx.x;
+    float f[MF];
+    if (i < n) site_features(i, n, cnt, mol, mol_off, mol_atoms, pos4, frame, e0, ph, dlp, f);
+    float v[KP];
+#pragma unroll
+    for (int k = 0; k < KP; k++)
+        v[k] = (k < MF && i < n) ? (f[k < MF ? k : 0] - norm[k < MF ? k : 0]) * norm[MF + (k < MF ? k : 0)] : 0.f;
+#pragma unroll
+    for (int k = 0; k < KP; k += 8) tc_st8(S.x + tc_ofs(threadIdx.x, k, TC_ROWS), v + k);
+    float y[MO];
+    tc_forward<true>(S, y, status);
+    if (i >= n) return;
+    V3 gs = linear_guess(ph, n, cnt, i, dl, order);
+    if (cnt >= 2) {
+        const V3 u = axis(frame, n, i, 0), v = axis(frame, n, i, 1), ww = axis(frame, n, i, 2);
+        gs = gs + (y[0] / TARGET_SCALE) * u + (y[1] / TARGET_SCALE) * v + (y[2] / TARGET_SCALE) * ww;
+    }
+    p[i] = gs.x;
+    p[n + i] = gs.y;
+    p[2 * n + i] = gs.z;
+}
+
+// the network's output for raw feature rows on the tensor cores (tanhf, as
+// k_mlp_eval)
+__global__ void __launch_bounds__(TC_ROWS) k_mlp_eval_tc(int rows, const float *x, const float *norm, const float *Wg,
+                                                         float *y, unsigned int *status) {
+    __shared__ TcSmem S;
+    tc_load_weights(S, Wg);
+    const int r = blockIdx.x * TC_ROWS + threadIdx.x;
+    const bool ok = r < rows;
+    for (int k = 0; k < KP; k++)
+        *(__nv_bfloat16 *)(S.x + tc_ofs(threadIdx.x, k, TC_ROWS)) = norm_in(x + (size_t)(ok ? r : 0) * MF, norm, k, ok);
+    float out[MO];
+    tc_forward<false>(S, out, status);
+    if (ok)
+        for (int o = 0; o < MO; o++) y[(size_t)r * MO + o] = out[o];
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 // the blocks' responses the guess and the features use: dl (the base order's
@@ -635,9 +864,14 @@ void launch_mlp_features(Ctx &c) {
 void launch_mlp_guess(Ctx &c) {
     // with the molecule blocks the block kernel has just formed both
     if (!(c.cg_precond == SMD_PRECOND_MOLECULE && c.cg_blk)) responses(c, c.mlp_base);
-    k_mlp_infer<<<(c.n + MLP_CHUNK - 1) / MLP_CHUNK, MLP_TB, 0, c.stream>>>(
-        c.n, c.mol, c.mol_off, c.mol_atoms, c.pos4, c.e0, c.mlp_norm, c.mlp_w, c.frame, guess_response(c),
-        guess_response_prev(c), c.phist, c.flags, c.pind, c.mlp_base);
+    if (c.mlp_tc)
+        k_mlp_infer_tc<<<(c.n + TC_ROWS - 1) / TC_ROWS, TC_ROWS, 0, c.stream>>>(
+            c.n, c.mol, c.mol_off, c.mol_atoms, c.pos4, c.e0, c.mlp_norm, c.mlp_w, c.frame, guess_response(c),
+            guess_response_prev(c), c.phist, c.flags, c.pind, c.mlp_base, c.status);
+    else
+        k_mlp_infer<<<(c.n + MLP_CHUNK - 1) / MLP_CHUNK, MLP_TB, 0, c.stream>>>(
+            c.n, c.mol, c.mol_off, c.mol_atoms, c.pos4, c.e0, c.mlp_norm, c.mlp_w, c.frame, guess_response(c),
+            guess_response_prev(c), c.phist, c.flags, c.pind, c.mlp_base);
 }
 
 // The extrapolated guess alone (order 1: p = p(t-1) + M^-1 (E0(t) - E0(t-1)),
@@ -754,7 +988,11 @@ int mlp_nfeat() { return MF; }
 int mlp_max_batch() { return MLP_MAX_BATCH; }
 
 void launch_mlp_eval(Ctx &c, int rows, const float *x, float *y) {
-    k_mlp_eval<<<(rows + MLP_CHUNK - 1) / MLP_CHUNK, MLP_TB, 0, c.stream>>>(rows, x, c.mlp_norm, c.mlp_w, y);
+    if (c.mlp_tc)
+        k_mlp_eval_tc<<<(rows + TC_ROWS - 1) / TC_ROWS, TC_ROWS, 0, c.stream>>>(rows, x, c.mlp_norm, c.mlp_w, y,
+                                                                              c.status);
+    else
+        k_mlp_eval<<<(rows + MLP_CHUNK - 1) / MLP_CHUNK, MLP_TB, 0, c.stream>>>(rows, x, c.mlp_norm, c.mlp_w, y);
 }
 
 }  // namespace smd

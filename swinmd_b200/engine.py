@@ -483,6 +483,11 @@ class GpuEnsemble:
         single-reduction form)."""
         self._chk(self.lib.smd_set_solver_pipelined(self.ctx, int(mode)))
 
+    def mlp_set_tensor_path(self, path: int):
+        """Network inference and evaluation on tcgen05 128-row tiles (1, the
+        default) or warp-level mma.sync tiles (0)."""
+        self._chk(self.lib.smd_mlp_set_tensor_path(self.ctx, int(path)))
+
     def set_solver(self, tol: float = 2.0819e-8, max_iter: int = 500, guess: int = L.GUESS_DIRECT,
                    precond: int = None):
         """Dipole solve settings; precond (L.PRECOND_SITE / L.PRECOND_MOLECULE,

@@ -125,3 +125,59 @@ def test_learned_guess_small_system_converges_to_same_dipoles():
     print("iterations direct", it_direct, "learned", it_learned)
     assert np.sqrt(np.mean((p_learned - p_direct) ** 2)) < 1e-7
     assert it_learned < it_direct
+
+
+@pytest.mark.parametrize("rows", [1, 127, 130, 1000])
+def test_tensor_paths_agree(rows):
+    # tcgen05 128-row tiles (the default) and the warp-level mma.sync tiles,
+    # on ragged row counts: the same BF16 operands, FP32 sums in another
+    # order, so the two agree far inside the BF16 checker's bound
+    ens = engine.GpuEnsemble(_pw())
+    ens.mlp_init(capacity_frames=4, seed=11)
+    ens.compute_forces(L.TERM_IND_SHORT)
+    feats = ens.mlp_features()
+    params = ens.mlp_params()
+    params[M.NPARAM:M.NPARAM + M.F] = feats.mean(0)
+    params[M.NPARAM + M.F:] = 1.0 / (feats.std(0) + 1e-3)
+    ens.mlp_params(set_to=params)
+    x = np.ascontiguousarray(np.resize(feats, (rows, feats.shape[1])))
+    y_tc = ens.mlp_eval(x)
+    ens.mlp_set_tensor_path(0)
+    y_ws = ens.mlp_eval(x)
+    ens.mlp_set_tensor_path(1)
+    y_bf, _ = M.forward(params, x, bf16=True)
+    scale = 1 + np.abs(y_bf).max()
+    print("tcgen05 vs mma.sync", np.max(np.abs(y_tc - y_ws)) / scale, "vs bf16 checker",
+          np.max(np.abs(y_tc - y_bf)) / scale)
+    assert np.max(np.abs(y_tc - y_ws)) < 2e-3 * scale
+    assert np.max(np.abs(y_tc - y_bf)) < 2e-3 * scale
+    with pytest.raises(L.SmdError):
+        ens.mlp_set_tensor_path(2)
+    ens.close()
+
+
+def test_learned_guess_same_on_both_tensor_paths():
+    s = _pw(seed=9)
+    ens = engine.GpuEnsemble(s)
+    ens.set_solver(tol=2.0819e-8, max_iter=500, guess=L.GUESS_DIRECT)
+    lf = engine.LFIntegrator(ens)
+    lf.start()
+    lf.run(2)
+    ens.mlp_init(capacity_frames=20, seed=5)
+    for _ in range(20):
+        lf.run(2)
+        ens.compute_forces(L.TERM_IND_SHORT)
+        ens.mlp_collect()
+    ens.mlp_train(epochs=10, batch=2048, lr=2e-3)
+    lf.run(3)
+    ens.set_solver(tol=2.0819e-8, max_iter=500, guess=L.GUESS_LEARNED)
+    out = {}
+    for path in (1, 0):
+        ens.mlp_set_tensor_path(path)
+        ens.compute_forces(L.TERM_IND_SHORT)
+        out[path] = (ens.solver_trace()[0], ens.solver_stats()[0], ens.polarization()["p"])
+    print("first update", out[1][0], out[0][0], "iterations", out[1][1], out[0][1])
+    assert abs(out[1][0] - out[0][0]) <= 1e-2 * out[0][0]
+    assert abs(out[1][1] - out[0][1]) <= 1
+    assert np.sqrt(np.mean((out[1][2] - out[0][2]) ** 2)) < 1e-7
+    ens.close()
