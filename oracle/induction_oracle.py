@@ -388,7 +388,7 @@ def induced_correct_energies(pos, q, dip, quad, p, box, alpha, mol_id):
     return e_self, -0.5 * intra * COULOMBS
 
 
-def induced_real_energy(pos, q, dip, quad, p, polar, box, alpha, a, cutoff, mol_id):
+def induced_real_energy(pos, q, dip, quad, p, polar, box, alpha, a, cutoff, mol_id, amoeba=False):
     """The reference's realPolEnergy (Induction.cpp:985-1075, Thole damping
     applied to the Ewald B_n, not the AMOEBA form): for every pair of sites
     of different molecules within the real-space cutoff
@@ -396,7 +396,13 @@ def induced_real_energy(pos, q, dip, quad, p, polar, box, alpha, a, cutoff, mol_
     with the invariants of induced_correct_energies, u^3 = r^3 / sqrt(a_i a_j),
     e = exp(-a u^3), l3 = 1 - e, g3 = 3 a u^3 e / r^2, g5 = 3 (a u^3)^2 e / r^2,
         B1d = B1 l3,  B2d = B2 l3 + B1 g3,  B3d = B3 l3 + 2 B2 g3 + B1 (g3 - 3 g5) / r^2
-    and the erfc-based B_n of multipole_real_energy."""
+    and the erfc-based B_n of multipole_real_energy.
+
+    amoeba=True is the reference's dampAMOEBA branch (Induction.cpp:1051-1084,
+    Tinker's form): pairs of one molecule (excluded, s = 0) are summed too,
+    and with l5 = 1 - (1 + a u^3) e, l7 = 1 - (1 + a u^3 + 3 (a u^3)^2 / 5) e,
+        B1d = B1 + (1 - s l3) / r^3,  B2d = B2 - 3 (1 - s l5) / r^5,
+        B3d = B3 + 15 (1 - s l7) / r^7."""
     from scipy.special import erfc
     pos = np.asarray(pos, np.float64)
     box = np.asarray(box, np.float64)
@@ -415,8 +421,11 @@ def induced_real_energy(pos, q, dip, quad, p, polar, box, alpha, a, cutoff, mol_
         j = np.arange(i + 1, n)
         r = min_image(pos[i] - pos[j], box)
         r2 = np.einsum("ij,ij->i", r, r)
-        keep = (r2 < cutoff * cutoff) & (mol[j] != mol[i])
+        keep = r2 < cutoff * cutoff
+        if not amoeba:
+            keep &= mol[j] != mol[i]
         j, r, r2 = j[keep], r[keep], r2[keep]
+        sc = (mol[j] != mol[i]).astype(np.float64)
         if len(j) == 0:
             continue
         rr = np.sqrt(r2)
@@ -430,9 +439,17 @@ def induced_real_energy(pos, q, dip, quad, p, polar, box, alpha, a, cutoff, mol_
         l3 = 1.0 - e
         g3 = 3.0 * au3 * e / r2
         g5 = 3.0 * au3 * au3 * e / r2
-        B1d = B1 * l3
-        B2d = B2 * l3 + B1 * g3
-        B3d = B3 * l3 + 2.0 * B2 * g3 + B1 * (g3 - 3.0 * g5) / r2
+        if amoeba:
+            l5 = 1.0 - (1.0 + au3) * e
+            l7 = 1.0 - (1.0 + au3 + 0.6 * au3 * au3) * e
+            ir3 = 1.0 / (r2 * rr)
+            B1d = B1 + (1.0 - sc * l3) * ir3
+            B2d = B2 - (1.0 - sc * l5) * 3.0 * ir3 / r2
+            B3d = B3 + (1.0 - sc * l7) * 15.0 * ir3 / (r2 * r2)
+        else:
+            B1d = B1 * l3
+            B2d = B2 * l3 + B1 * g3
+            B3d = B3 * l3 + 2.0 * B2 * g3 + B1 * (g3 - 3.0 * g5) / r2
         Qi_r = (Q[i] @ r.T).T
         Qj_r = np.einsum("kab,kb->ka", Q[j], r)
         rQir = np.einsum("ka,ka->k", r, Qi_r)

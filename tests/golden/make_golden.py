@@ -52,6 +52,14 @@ def polwater216():
     return s, [("forces",), ("run", 10)]
 
 
+def polwater216_amoeba():
+    # the induced real space damped as Tinker's AMOEBA (dampAMOEBA,
+    # Induction.cpp:1051-1079): the same configuration as polwater216
+    s, _ = polwater216()
+    s.config.damp_amoeba = True
+    return s, [("forces",)]
+
+
 def lj500_npt():
     # NHIntegrator's NpT run (chain + isotropic barostat, Lustig virial
     # pressure) near the state's own pressure; 25 steps of 4 fs keep every
@@ -214,7 +222,7 @@ def ref_test_nvt():
 
 
 CASES = {"lj500": lj500, "lj500_npt": lj500_npt, "nacl1000_mie": nacl1000_mie, "spce512": spce512,
-         "polwater216": polwater216, "spce512_wolf": spce512_wolf, "saap500": saap500,
+         "polwater216": polwater216, "polwater216_amoeba": polwater216_amoeba, "spce512_wolf": spce512_wolf, "saap500": saap500,
          "lj500_lustig": lj500_lustig, "spce512_lustig": spce512_lustig, "nacl1000_wolf": nacl1000_wolf, "polwater216_nve": polwater216_nve, "ref_test_nvt": ref_test_nvt,
          "nacl1000_lustig": nacl1000_lustig, "spcf216_lustig": spcf216_lustig,
          "polwater216_lustig": polwater216_lustig, "ref_test_lustig": ref_test_lustig,
@@ -291,6 +299,10 @@ def pack(name, s, results, large=False):
         out.pop("pairs", None)
     if name.endswith("_wolf"):  # (the Wolf Lustig case ends in _lustig)
         out = {k: v for k, v in out.items() if not k.startswith("f_") or k.startswith("f_wolf_")}
+        out.pop("pairs", None)
+    if name.endswith("_amoeba"):
+        # the induced terms only: the rest is polwater216's
+        out = {k: v for k, v in out.items() if not k.startswith("f_") or k.startswith(("f_ind_", "f_mp_dip", "f_mp_quad"))}
         out.pop("pairs", None)
     if name.endswith(("_nve", "_npt")):
         # the trajectory only: the forces of the start are polwater216's

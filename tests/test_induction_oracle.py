@@ -113,6 +113,21 @@ def test_induced_correct_energies_match_reference():
     assert abs(e_intra - ref[9]) < 1e-12 * abs(ref[9])
 
 
+def test_induced_real_energy_amoeba_matches_reference():
+    """The dampAMOEBA branch (fixture polwater216_amoeba: the same
+    configuration and dipoles, the induced real space damped as Tinker's)."""
+    g0, s, polar = _case()
+    g = golden("polwater216_amoeba")
+    assert np.array_equal(g["f_ind_P"], g0["f_ind_P"])
+    q = np.array([s.atom_types[k].charge for k in g["atom_type"]])
+    e = induction_oracle.induced_real_energy(g["pos"], q, g["f_mp_dip"], g["f_mp_quad"], g["f_ind_P"], polar,
+                                             g["box"], s.config.alpha, s.config.a_damping, s.config.cutoff_ew,
+                                             g["mol_id"], amoeba=True)
+    ref = g["f_ind_short_energy"][6]
+    print(e, ref, g0["f_ind_short_energy"][6])
+    assert abs(e - ref) < 1e-12 * abs(ref)
+
+
 def test_induced_real_energy_matches_reference():
     """Thole-damped Ewald real-space energy of the induced dipoles (from the
     reference's converged dipoles) against its realPolEnergy."""
