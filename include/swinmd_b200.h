@@ -277,6 +277,14 @@ int smd_set_solver_pipelined(smd_ctx *ctx, int mode);
  * first hidden layer to BF16 and accumulate in FP32; their outputs agree to
  * FP32 summation order.  Training always uses the warp-level tiles. */
 int smd_mlp_set_tensor_path(smd_ctx *ctx, int path);
+/* Damping of the induced real-space energy, forces and torques, as the
+ * reference's Config flag dampAmoeba selects (Induction.cpp:1051-1079):
+ * form 0 (the default) multiplies the Ewald B_n by Thole's factors and skips
+ * excluded pairs, form 1 is Tinker's AMOEBA form, which adds (1 - s l_n)
+ * times the bare 1/r^n terms with the exclusion scale s inside, so excluded
+ * pairs contribute.  The dipole solve is the same for both.  The mixed path
+ * takes the unfused real-space kernels under form 1; smd_lustig refuses it. */
+int smd_set_induction_damping(smd_ctx *ctx, int form);
 /* Limit (seconds, default 1) of every bounded device-side wait: the dipole
  * solve's grid barrier.  A wait that runs out makes the solve leave, sets
  * SMD_ERR_TIMEOUT and keeps the context usable.  No reference counterpart

@@ -114,6 +114,7 @@ SIGNATURES = {
     "smd_lustig": (ctypes.c_int, [_P, _D]),
     "smd_set_solver_pipelined": (ctypes.c_int, [_P, ctypes.c_int]),
     "smd_mlp_set_tensor_path": (ctypes.c_int, [_P, ctypes.c_int]),
+    "smd_set_induction_damping": (ctypes.c_int, [_P, ctypes.c_int]),
     "smd_set_saap": (ctypes.c_int, [_P, _D, ctypes.c_int, ctypes.c_double]),
     "smd_set_wolf": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, _I, ctypes.c_double]),
     "smd_set_barostat": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, ctypes.c_int]),

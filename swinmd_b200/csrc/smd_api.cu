@@ -505,6 +505,8 @@ int smd_lustig_lj(smd_ctx *x, double *out) {
 
 int smd_lustig(smd_ctx *x, double *out) {
     if (!x || !out || x->c.n == 0 || x->c.box.L[0] <= 0) return fail(x, SMD_ERR_ARG, "smd_lustig: system not set up");
+    if (x->c.ind_amoeba && x->c.ind_on)
+        return fail(x, SMD_ERR_ARG, "smd_lustig: the AMOEBA-damped induced real space has no volume derivatives here");
     Ctx &c = x->c;
     if (c.rc.le || (c.vdw != VDW_NONE && c.vdw != VDW_LJ && c.vdw != VDW_BUFF))
         return fail(x, SMD_ERR_ARG,
@@ -915,6 +917,15 @@ int smd_set_solver_pipelined(smd_ctx *x, int on) {
     if (!x) return fail(x, SMD_ERR_ARG, "smd_set_solver_pipelined: null context");
     if (on < 0 || on > 2) return fail(x, SMD_ERR_ARG, "smd_set_solver_pipelined: mode must be 0, 1 or 2");
     x->c.cg_pipelined = on;
+    x->c.graph_dirty = 1;
+    touch(x->c);
+    return SMD_OK;
+}
+
+int smd_set_induction_damping(smd_ctx *x, int form) {
+    if (!x) return fail(x, SMD_ERR_ARG, "smd_set_induction_damping: null context");
+    if (form < 0 || form > 1) return fail(x, SMD_ERR_ARG, "smd_set_induction_damping: form must be 0 or 1");
+    x->c.ind_amoeba = form;
     x->c.graph_dirty = 1;
     touch(x->c);
     return SMD_OK;

@@ -114,6 +114,7 @@ struct Ctx {
     double mp_rc2 = 0;              // real-space cutoff^2 (cutoffEw)
     double ind_cut2 = 0;            // cutoffInd^2
     double thole_a = 0.39;
+    int ind_amoeba = 0;              // induced real space: 0 Thole-damped B_n, 1 Tinker's AMOEBA form
     double *type_mp = nullptr;      // [ntypes][9] local dipole (3) + quadrupole (6)
     double *type_polar = nullptr;   // [ntypes] polarisabilities (nm^3)
     std::vector<double> h_type_polar;

@@ -54,6 +54,7 @@ struct IndArgs {
     Box box;
     double cut2, a, alpha, rc2;
     double *e0, *p;
+    int amoeba;   // induced real space damped as Tinker's AMOEBA (dampAMOEBA)
 };
 
 // ---------------------------------------------------------------------------
@@ -1104,6 +1105,85 @@ __device__ __forceinline__ void ind_pair(double qi, V3 mi, const Q6 &Qi, V3 pi_,
     o.tau = scale * (B1d * Gt1 + B2d * Gt2 + B3d * Gt3);
 }
 
+// The dampAMOEBA branch (Induction.cpp:1051-1079, Tinker's form; the
+// minimisation terms G1ip, G2ip with the undamped-by-exclusion factors):
+//   B1d = B1 + (1 - s l3)/r^3, B2d = B2 - 3 (1 - s l5)/r^5, B3d = B3 + 15 (1 - s l7)/r^7
+// and their radial gradients gB1..gB3 in place of B2d..B4d.  The exclusion
+// scale s sits inside the factors, so excluded pairs contribute.
+struct IndRadA {
+    double c1, c2, c3;    // B1d, B2d, B3d
+    double g1, g2, g3;    // gradB1, gradB2, gradB3
+    double cp, gp1, gp2;  // B2du, gradB1u, gradB2u (s = 1)
+};
+
+__device__ __forceinline__ void ind_radial_amoeba(double rr, double ir2, const double *B, double ipp, double a,
+                                                  double s, IndRadA &R) {
+    const double au3 = a * rr * rr * rr * ipp, e = exp(-au3), a2u6 = au3 * au3, a3u9 = a2u6 * au3;
+    const double l3 = 1.0 - e, l5 = 1.0 - (1.0 + au3) * e, l7 = 1.0 - (1.0 + au3 + 0.6 * a2u6) * e;
+    const double gl3 = 3.0 * au3 * e * ir2, gl5 = 3.0 * a2u6 * e * ir2;
+    const double gl7 = (-3.0 * a2u6 + 9.0 * a3u9) * e * (0.2 * ir2);
+    const double ir3 = ir2 / rr, ir5 = 3.0 * ir3 * ir2, ir7 = 5.0 * ir5 * ir2, ir9 = 7.0 * ir7 * ir2;
+    R.c1 = B[1] + (1.0 - s * l3) * ir3;
+    R.c2 = B[2] - (1.0 - s * l5) * ir5;
+    R.c3 = B[3] + (1.0 - s * l7) * ir7;
+    R.g1 = B[2] - s * gl3 * ir3 - (1.0 - s * l3) * ir5;
+    R.g2 = B[3] + s * gl5 * ir5 + (1.0 - s * l5) * ir7;
+    R.g3 = B[4] - s * gl7 * ir7 - (1.0 - s * l7) * ir9;
+    R.cp = B[2] - (1.0 - l5) * ir5;
+    R.gp1 = B[2] - gl3 * ir3 - (1.0 - l3) * ir5;
+    R.gp2 = B[3] + gl5 * ir5 + (1.0 - l5) * ir7;
+}
+
+__device__ __forceinline__ V3 as_v3(V3 v) { return v; }
+__device__ __forceinline__ V3 as_v3(F3 v) { return to_v3(v); }
+
+// energy, force and torque of the pair from its angular algebra (FP64 or
+// FP32 members) and the AMOEBA radial factors
+template <class AL>
+__device__ __forceinline__ void ind_pair_amoeba(const AL &A, V3 r, const IndRadA &R, IndPairOut &o) {
+    o.e = 0.5 * (((double)A.G1i + A.G1j) * R.c1 + ((double)A.G2i + A.G2j) * R.c2 + ((double)A.G3i + A.G3j) * R.c3);
+    const V3 fi = -(R.c1 * as_v3(A.gG1i) + R.c2 * as_v3(A.gG2i) + R.c3 * as_v3(A.gG3i) + R.cp * as_v3(A.gG2ip)) -
+                  (A.G1i * R.g1 + A.G2i * R.g2 + A.G3i * R.g3 + A.G1ip * R.gp1 + A.G2ip * R.gp2) * r;
+    const V3 fj = -(R.c1 * as_v3(A.gG1j) + R.c2 * as_v3(A.gG2j) + R.c3 * as_v3(A.gG3j) + R.cp * as_v3(A.gG2jp)) -
+                  (A.G1j * R.g1 + A.G2j * R.g2 + A.G3j * R.g3) * (-r);
+    o.fij = fi - fj;
+    o.tau = R.c1 * as_v3(A.Gt1) + R.c2 * as_v3(A.Gt2) + R.c3 * as_v3(A.Gt3);
+}
+
+// the angular algebra of the pair in FP64 (members as IndAlgF's)
+struct IndAlgD {
+    double G1i, G2i, G3i, G1j, G2j, G3j, G1ip, G2ip;
+    V3 gG1i, gG2i, gG3i, gG1j, gG2j, gG3j, gG2ip, gG2jp, Gt1, Gt2, Gt3;
+};
+
+__device__ __forceinline__ void ind_algebra_d(double qi, V3 mi, const Q6 &Qi, V3 pi_, double qj, V3 mj,
+                                              const Q6 &Qj, V3 pj_, V3 r, IndAlgD &A) {
+    const V3 rji = -r;
+    const double QiI = qtr(Qi), QjI = qtr(Qj);
+    const V3 Qir = qv(Qi, r), Qjrji = qv(Qj, rji);
+    const double QiRij = dot(r, Qir), QjRji = dot(r, qv(Qj, r));
+    const double pjr = dot(pj_, r), pirji = dot(pi_, rji);
+    A.G1i = -qi * pjr - dot(mi, pj_);
+    A.G2i = -dot(mi, r) * pjr - 2.0 * dot(pj_, Qir) - pjr * QiI;
+    A.G3i = -pjr * QiRij;
+    A.G1j = -qj * pirji - dot(mj, pi_);
+    A.G2j = -dot(mj, rji) * pirji - 2.0 * dot(pi_, Qjrji) - pirji * QjI;
+    A.G3j = -pirji * QjRji;
+    A.gG1i = (-qi) * pj_;
+    A.gG2i = (-pjr) * mi - dot(mi, r) * pj_ - 2.0 * qv(Qi, pj_) - QiI * pj_;
+    A.gG3i = (-QiRij) * pj_ - (2.0 * pjr) * Qir;
+    A.gG1j = (-qj) * pi_;
+    A.gG2j = (-pirji) * mj - dot(mj, rji) * pi_ - 2.0 * qv(Qj, pi_) - QjI * pi_;
+    A.gG3j = (-QjRji) * pi_ - (2.0 * pirji) * Qjrji;
+    A.G1ip = -dot(pi_, pj_);
+    A.G2ip = -dot(pi_, r) * pjr;
+    A.gG2ip = (-pjr) * pi_;
+    A.gG2jp = (-pirji) * pj_;
+    A.Gt1 = crs(mi, pj_);
+    A.Gt2 = pjr * crs(mi, r) + 2.0 * crs(Qir, pj_) + 2.0 * crs(qv(Qi, pj_), r);
+    A.Gt3 = (2.0 * pjr) * crs(Qir, r);
+}
+
 // Mixed path: the same terms with the angular algebra (G, their gradients
 // and the torque coefficients) in FP32 and the radial Ewald / Thole factors,
 // the energy and the force assembly in FP64.
@@ -1203,8 +1283,19 @@ __global__ void __launch_bounds__(64) k_ind_real(IndRealArgs A) {
             const double r2 = dot(r, r);
             if (!(r2 < a.rc2)) return;
             IndPairOut o;
-            ind_pair(qi, mi, Qi, pii, a.tq[(int)pj.w] / SQC, ld3i(a.mu, a.n, j), ldqi(a.qd, a.n, j),
-                     ld3i(a.p, a.n, j), r, r2, poli, a.polar[(int)pj.w], a.a, a.alpha, scale, o);
+            if (a.amoeba) {
+                IndAlgD al;
+                ind_algebra_d(qi, mi, Qi, pii, a.tq[(int)pj.w] / SQC, ld3i(a.mu, a.n, j), ldqi(a.qd, a.n, j),
+                              ld3i(a.p, a.n, j), r, al);
+                double B[6];
+                bn_erfc(r2, a.alpha, B);
+                IndRadA R;
+                ind_radial_amoeba(sqrt(r2), 1.0 / r2, B, 1.0 / sqrt(poli * a.polar[(int)pj.w]), a.a, scale, R);
+                ind_pair_amoeba(al, r, R, o);
+            } else {
+                ind_pair(qi, mi, Qi, pii, a.tq[(int)pj.w] / SQC, ld3i(a.mu, a.n, j), ldqi(a.qd, a.n, j),
+                         ld3i(a.p, a.n, j), r, r2, poli, a.polar[(int)pj.w], a.a, a.alpha, scale, o);
+            }
             en += o.e;
             f = f + o.fij;
             tau = tau + o.tau;
@@ -1283,7 +1374,15 @@ __global__ void __launch_bounds__(64) k_ind_real_f(IndRealArgs A) {
             IndAlgF al;
             ind_algebra_f(qi, mi, Qi, pii, j0.x, f3(j0.y, j0.z, j0.w), Qj, f3(j2.z, j2.w, j3.x), rf, al);
             IndPairOut o;
-            ind_pair_mixed(al, r, r2, poli, a.polar[fj.w], a.a, a.alpha, scale, o);
+            if (a.amoeba) {
+                double B[6];
+                bn_erfc(r2, a.alpha, B);
+                IndRadA R;
+                ind_radial_amoeba(sqrt(r2), 1.0 / r2, B, 1.0 / sqrt(poli * a.polar[fj.w]), a.a, scale, R);
+                ind_pair_amoeba(al, r, R, o);
+            } else {
+                ind_pair_mixed(al, r, r2, poli, a.polar[fj.w], a.a, a.alpha, scale, o);
+            }
             en += o.e;
             f = f + o.fij;
             tau = tau + o.tau;
@@ -1681,6 +1780,7 @@ static IndArgs ind_args(Ctx &c) {
     a.pos4 = c.pos4; a.tq = c.type_q; a.polar = c.type_polar; a.mu = c.mu; a.qd = c.qd;
     a.box = c.box; a.cut2 = c.ind_cut2; a.a = c.thole_a; a.alpha = c.ew_alpha; a.rc2 = c.mp_rc2;
     a.e0 = c.e0; a.p = c.pind;
+    a.amoeba = c.ind_amoeba;
     return a;
 }
 
@@ -1955,7 +2055,7 @@ void launch_ind_short(Ctx &c) {
 
 bool polar_short_fused(const Ctx &c) {
     const bool cubic = c.box.L[0] == c.box.L[1] && c.box.L[1] == c.box.L[2];
-    return c.precision == SMD_PREC_MIXED && cubic && c.srec && c.ind_on;
+    return c.precision == SMD_PREC_MIXED && cubic && c.srec && c.ind_on && !c.ind_amoeba;
 }
 
 // Both real-space polarisable terms after the dipole solve: one fused pass

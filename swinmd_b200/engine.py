@@ -232,15 +232,11 @@ def lustig_molvirt(fields: dict, volume: float, tb_energy: float = 0.0) -> float
 
 def refuse_unsupported(c) -> None:
     """Raises for configuration options the GPU path does not compute, so a
-    caller never gets different physics with a success status: the AMOEBA
-    damping branch of the induced real space (``dampAMOEBA``,
-    Induction.cpp:1051-1079) and Wolf with another electrostatic method."""
+    caller never gets different physics with a success status: Wolf with
+    another electrostatic method."""
     if c.compute_ub and c.constraint:
         # Integrator::initialise refuses the same combination (src/Integrator.cpp:178-187)
         raise NotImplementedError("a flexible Urey-Bradley term with constraints")
-    if c.compute_multipole and c.compute_induction and c.damp_amoeba:
-        raise NotImplementedError("AMOEBA damping of the induced real space (dampAMOEBA) is not built on "
-                                  "the GPU path")
     if c.compute_wolf and (c.compute_ewald or c.compute_multipole):
         # the reference stops on more than one electrostatic method
         # (LFIntegrator.cpp:1027, 1058)
@@ -317,6 +313,8 @@ class GpuEnsemble:
             self._chk(self.lib.smd_set_multipole(ctx, L.dptr(mp), L.dptr(pol), c.alpha, c.k_cutoff,
                                                  c.cutoff_ew, int(c.compute_induction), c.cutoff_ind,
                                                  c.a_damping))
+            # Config dampAmoeba (Induction.cpp:52): Tinker's damping form
+            self._chk(self.lib.smd_set_induction_damping(ctx, int(bool(c.damp_amoeba))))
         # bonded terms of flexible molecules (Integrator::initialise,
         # src/Integrator.cpp:163-190): bonds and angles without constraints,
         # Urey-Bradley when configured

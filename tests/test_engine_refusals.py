@@ -9,7 +9,7 @@ def _pw():
     return systems.polarizable_water(nmol=8, kmax=3, seed=1)
 
 
-@pytest.mark.parametrize("field", ["damp_amoeba", "compute_wolf"])
+@pytest.mark.parametrize("field", ["compute_wolf"])
 def test_unsupported_options_refused(field):
     # (Wolf is built, but not together with the multipoles)
     s = _pw()
